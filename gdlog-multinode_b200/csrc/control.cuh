@@ -1,0 +1,164 @@
+// control.cuh — per-iteration bookkeeping kernels of the device-side loop,
+// plus the load-path helpers (pack, digest).
+//
+// LIE::fixpoint_loop (src/lie.cu:26-274) drives the loop from the host with
+// a cudaDeviceSynchronize after almost every step.  Here the loop state is
+// on the device: k_begin opens an iteration, k_commit closes it (swaps the
+// rebuilt FULL/DELTA in, writes the per-iteration log line, decides
+// termination exactly as src/lie.cu:208-215 does) and, when the iteration
+// runs inside a CUDA graph while-node, sets the node's condition.
+#pragma once
+
+#include "common.cuh"
+
+namespace gdl {
+
+constexpr int kMaxOps = 64;
+
+struct LieDev {
+  int n_update, n_static, n_tmp, n_ops;
+  int update[kMaxRels];
+  int statics[kMaxRels];
+  int tmps[kMaxRels];
+  u32 once[kMaxOps];          // RelationalCopy::copied (committed)
+  u32 once_pending[kMaxOps];  // set by this iteration's copies
+  u64 *trace;                 // [trace rows][n_update][3]
+};
+
+__global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
+  if (ctl_stop(ctl) || threadIdx.x != 0) return;
+  for (int i = 0; i < L->n_update; i++) {
+    RelDev &r = rels[L->update[i]];
+    r.w_full_vis = r.full_vis;
+    r.w_delta_vis = r.delta_vis;
+    r.newt.n = 0;
+  }
+  for (int i = 0; i < L->n_static; i++) {
+    RelDev &r = rels[L->statics[i]];
+    r.w_full_vis = r.full_vis;
+    r.w_delta_vis = r.delta_vis;
+  }
+  for (int i = 0; i < L->n_tmp; i++) {
+    RelDev &r = rels[L->tmps[i]];
+    r.w_full_vis = r.full_vis;
+    r.w_delta_vis = r.delta_vis;
+    r.newt.n = 0;
+  }
+  for (int i = 0; i < L->n_ops; i++) L->once_pending[i] = 0;
+}
+
+template <class T>
+__device__ __forceinline__ void dswap(T &a, T &b) {
+  T t = a;
+  a = b;
+  b = t;
+}
+
+__global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
+  if (threadIdx.x != 0) return;
+  bool stop = ctl->done | ctl->pause | ctl->overflow | ctl->timeout;
+  if (!stop) {
+    const u64 it = ctl->iteration;
+    const u64 row = it - ctl->trace_base;
+    bool fixpoint = true;
+    for (int i = 0; i < L->n_update; i++) {
+      RelDev &r = rels[L->update[i]];
+      u64 *tr = (L->trace && row < ctl->trace_rows) ? L->trace + (row * L->n_update + i) * 3 : 0;
+      if (r.c_newt_n == 0) {
+        // src/lie.cu:114-121: no new tuple -> a fresh, empty DELTA.
+        r.delta.n = 0;
+        r.delta_vis = 1;
+        r.full_vis = r.w_full_vis;
+        if (tr) {
+          tr[0] = kNoTrace;
+          tr[1] = 0;
+          tr[2] = r.full.n;
+        }
+      } else {
+        dswap(r.delta, r.delta_next);
+        dswap(r.delta_idx, r.delta_idx_next);
+        r.delta_vis = 1;
+        if (r.delta.n) {
+          // flush_delta (src/relation.cu:405-521): FULL := FULL ∪ DELTA.
+          dswap(r.full, r.full_next);
+          dswap(r.full_idx, r.full_idx_next);
+          r.full_vis = 1;
+          fixpoint = false;
+        } else {
+          r.full_vis = r.w_full_vis;
+        }
+        if (tr) {
+          tr[0] = r.delta.n;
+          tr[1] = r.delta.n;
+          tr[2] = r.full.n;
+        }
+      }
+      r.newt.n = 0;
+      r.c_newt_n = 0;
+    }
+    for (int i = 0; i < L->n_static; i++) {
+      RelDev &r = rels[L->statics[i]];
+      r.full_vis = r.w_full_vis;
+      r.delta_vis = r.w_delta_vis;
+    }
+    for (int i = 0; i < L->n_tmp; i++) {
+      RelDev &r = rels[L->tmps[i]];
+      r.newt.n = 0;  // src/lie.cu:85-87
+    }
+    for (int i = 0; i < L->n_ops; i++) L->once[i] |= L->once_pending[i];
+    const u64 next = it + 1;
+    ctl->iteration = next;
+    ctl->generation = ctl->generation + 1;
+    if (fixpoint || next > ctl->max_iteration)
+      ctl->done = 1;
+    else if (next >= ctl->stop_at)
+      ctl->pause = 1;
+    __threadfence();
+    stop = ctl->done | ctl->pause;
+  }
+  if (ctl->cond_set) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
+}
+
+// Pack host-layout rows (two u64 columns) into keys; raise bit 0 of *bad if
+// a column does not fit 32 bits.  *maxv receives the largest column value.
+__global__ void k_pack_rows(const u64 *rows, u64 n, u64 *keys, u64 *maxv, u32 *bad) {
+  u64 m = 0;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    u64 c0 = rows[2 * i], c1 = rows[2 * i + 1];
+    if ((c0 | c1) >> 32) atomicOr(bad, 1u);
+    keys[i] = make_key((u32)c0, (u32)c1);
+    m = max(m, max(c0, c1));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(maxv, m);
+}
+
+// Unpack keys into host-layout rows.
+__global__ void k_unpack_rows(const u64 *keys, u64 n, u64 *rows) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    u64 k = keys[i];
+    rows[2 * i] = key_c0(k);
+    rows[2 * i + 1] = key_c1(k);
+  }
+}
+
+// Digest of sorted keys: sum over i of a hash of (i, c0, c1).
+__global__ void k_digest(const u64 *keys, u64 n, u64 *acc) {
+  u64 s = 0;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    u64 k = keys[i];
+    u64 h = mix64(i);
+    h = mix64(h ^ (u64)key_c0(k));
+    h = mix64(h ^ (u64)key_c1(k));
+    s += h;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
+}
+
+}  // namespace gdl

@@ -1,0 +1,1291 @@
+// engine.cu — host side of the B200 fixpoint engine and its C-ABI
+// (include/gdlog_b200.h).
+//
+// The engine mirrors the reference's object model (Relation with
+// FULL/DELTA/NEWT, LIE with update/static/tmp relations and an ordered list
+// of RA operators; include/relation.cuh:257-300, include/lie.cuh:11-65) but
+// runs a LIE's semi-naive loop as a fixed sequence of kernels per iteration
+// whose sizes are all device-resident:
+//
+//   k_begin                      open the iteration (working counts)
+//   per op:  k_join_count + k_join_mat[_pred]   (RelationalJoin)
+//            k_copy                             (RelationalCopy / ACopy)
+//   per update relation:
+//            k_sort_hist + k_sort_pass x P      (onesweep radix sort NEWT)
+//            k_merge_diff                       (dedup, NEWT \ FULL, FULL ∪ Δ)
+//            k_index_build (FULL, DELTA)        (only indexes some op probes)
+//   k_commit                     swap in, log, decide termination
+//
+// That sequence is captured once into a CUDA graph as the body of a
+// conditional while-node; k_commit sets the node's condition, so a whole
+// batch of iterations runs from one graph launch with no host round trip.
+// The host looks at the loop state only between batches: to grow buffers
+// after a capacity overflow (the iteration is then rerun from committed
+// state) or to finish.
+#include "../../include/gdlog_b200.h"
+
+#include "common.cuh"
+#include "control.cuh"
+#include "index.cuh"
+#include "join.cuh"
+#include "merge.cuh"
+#include "sort.cuh"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace gdl;
+
+namespace {
+
+constexpr u64 kMinCap = 1ull << 16;
+constexpr int kIdentityMaxBits = 22;
+constexpr u64 kMaxRows = (1ull << 30) - 4096;  // sort status keeps 30 bits
+
+u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
+u64 next_pow2(u64 x) {
+  u64 p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+int bits_for(u64 v) {
+  int b = 1;
+  while (b < 64 && (v >> b)) b++;
+  return b;
+}
+
+struct OpHost {
+  int kind;  // 0 join, 1 copy, 2 acopy
+  int inner = -1, inner_ver = GDL_FULL, outer = -1, outer_ver = GDL_DELTA, out = -1;
+  Sel2 sel{0, 1};
+  Pred pred{0, 0, 0};
+};
+
+struct LieHost {
+  std::vector<int> update, statics, tmps;
+  std::vector<OpHost> ops;
+  long long max_iteration = 2147483647LL;  // include/lie.cuh:30 (INT_MAX)
+  bool reload_full = true;                 // include/lie.cuh:29
+  bool trace_on = true;
+  LieDev *d_lie = nullptr;
+  JoinRec *d_joinrec = nullptr;  // [kMaxOps]
+  std::vector<uint64_t> trace;   // 5 words per record
+  double ms = 0;
+  u64 kernels = 0, iterations = 0, retries = 0, graph_launches = 0;
+  cudaGraphExec_t gexec = nullptr;
+  unsigned long long cond_handle = 0;
+  bool graph_dirty = true;
+  int kernels_per_iter = 0;
+};
+
+struct RelHost {
+  std::string name;
+  int arity = 2, icols = 1, dep = 0;
+  bool index_flag = true, tmp_flag = false;
+  // FULL's raw buffer in load order (the reference's data_raw); the first
+  // |FULL| rows of it become DELTA at the start of a LIE
+  // (copy_relation_container, src/relation.cu:764-795).
+  u64 *raw = nullptr;
+  u64 raw_n = 0;
+  bool raw_is_full = true;
+  bool delta_sorted = true;
+};
+
+}  // namespace
+
+struct gdl_engine {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t s = nullptr;
+  bool own_stream = false;
+  std::string err;
+  std::vector<RelHost> rels;
+  std::vector<RelDev> h;  // host mirror of the device relation table
+  RelDev *d_rels = nullptr;
+  Ctl *d_ctl = nullptr;
+  Ctl *h_ctl = nullptr;  // pinned
+  int kbits = 1;         // bits of the largest column value loaded
+  u64 max_value = 0;
+  std::vector<LieHost> lies;
+  // scratch
+  u64 *sort_buf = nullptr;
+  u64 sort_cap = 0;
+  u32 *sort_offsets = nullptr, *sort_counters = nullptr, *sort_status = nullptr;
+  u64 sort_status_tiles = 0;
+  int sort_status_passes = 0;
+  u64 *crow_off = nullptr, *crow_key = nullptr;
+  u32 *crow_start = nullptr, *crow_len = nullptr;
+  u64 crow_cap = 0;
+  Lb lb_cnt{}, lb_nz{}, lb_merge{};
+  u64 lb_join_tiles = 0, lb_merge_tiles = 0;
+  LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
+  DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
+  u64 *d_u64 = nullptr;       // [4] small device scalars
+  u32 *d_u32 = nullptr;       // [4]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  u64 kernels_launched = 0;
+  bool broken = false;  // a bounded wait gave up or a bounds check fired
+};
+
+namespace {
+
+gdl_status fail(gdl_engine *e, gdl_status code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  e->err = buf;
+  return code;
+}
+
+#define CK(e, call)                                                                   \
+  do {                                                                                \
+    cudaError_t _r = (call);                                                          \
+    if (_r != cudaSuccess)                                                            \
+      return fail((e), _r == cudaErrorMemoryAllocation ? GDL_E_NOMEM : GDL_E_CUDA,    \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_r), __FILE__, \
+                  __LINE__);                                                          \
+  } while (0)
+
+#define TRY(x)                     \
+  do {                             \
+    gdl_status _s = (x);           \
+    if (_s != GDL_OK) return _s;   \
+  } while (0)
+
+gdl_status dalloc(gdl_engine *e, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  CK(e, cudaMallocAsync(p, bytes, e->s));
+  return GDL_OK;
+}
+void dfree(gdl_engine *e, void *p) {
+  if (p) cudaFreeAsync(p, e->s);
+}
+
+// Grow array `a` to hold at least `need` elements; keep its contents.
+gdl_status ensure_arr(gdl_engine *e, DArr &a, u64 need, bool keep) {
+  if (a.cap >= need && a.ptr) return GDL_OK;
+  u64 cap = std::max<u64>({need, kMinCap, a.cap + a.cap / 2});
+  cap = round_up(cap, 2);
+  if (cap > kMaxRows) cap = std::max<u64>(need, kMaxRows);
+  if (need > kMaxRows)
+    return fail(e, GDL_E_UNSUPPORTED, "relation of %llu tuples exceeds the %llu-tuple limit",
+                (unsigned long long)need, (unsigned long long)kMaxRows);
+  u64 *p = nullptr;
+  TRY(dalloc(e, (void **)&p, cap * sizeof(u64)));
+  if (keep && a.n) CK(e, cudaMemcpyAsync(p, a.ptr, a.n * sizeof(u64), cudaMemcpyDeviceToDevice, e->s));
+  dfree(e, a.ptr);
+  a.ptr = p;
+  a.cap = cap;
+  if (!keep) a.n = std::min(a.n, cap);
+  return GDL_OK;
+}
+
+// Size an index for arrays of capacity `cap`.
+gdl_status ensure_index(gdl_engine *e, Index &ix, u64 cap) {
+  u32 mode;
+  u64 slots;
+  if (e->kbits <= kIdentityMaxBits) {
+    mode = 0;
+    slots = 1ull << e->kbits;
+  } else {
+    mode = 1;
+    u64 distinct = std::min<u64>(cap, 1ull << std::min(e->kbits, 40));
+    slots = next_pow2(std::max<u64>(2 * distinct, 1024));
+  }
+  if (ix.slots && ix.hash_mode == mode && ix.mask + 1 >= slots) return GDL_OK;
+  dfree(e, ix.slots);
+  TRY(dalloc(e, (void **)&ix.slots, slots * sizeof(uint4)));
+  CK(e, cudaMemsetAsync(ix.slots, 0, slots * sizeof(uint4), e->s));
+  ix.mask = slots - 1;
+  ix.hash_mode = mode;
+  ix.epoch = 0;
+  return GDL_OK;
+}
+
+gdl_status pull(gdl_engine *e) {
+  if (e->rels.empty()) return GDL_OK;
+  CK(e, cudaMemcpyAsync(e->h.data(), e->d_rels, e->rels.size() * sizeof(RelDev),
+                        cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  return GDL_OK;
+}
+gdl_status push(gdl_engine *e) {
+  if (e->rels.empty()) return GDL_OK;
+  CK(e, cudaMemcpyAsync(e->d_rels, e->h.data(), e->rels.size() * sizeof(RelDev),
+                        cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  return GDL_OK;
+}
+
+int grid_for(gdl_engine *e, u64 work, u64 per_block, int per_sm) {
+  u64 g = (work + per_block - 1) / per_block;
+  u64 lim = (u64)e->sms * per_sm;
+  if (g > lim) g = lim;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+int sort_passes(const gdl_engine *e) { return std::max(1, (2 * e->kbits + 7) / 8); }
+
+// ---------------------------------------------------------------------------
+// Scratch sizing
+// ---------------------------------------------------------------------------
+gdl_status ensure_lb(gdl_engine *e, Lb &lb, u64 &have, u64 tiles) {
+  if (have >= tiles) return GDL_OK;
+  tiles = std::max<u64>(tiles + tiles / 2, 1024);
+  dfree(e, lb.flag);
+  dfree(e, lb.agg);
+  dfree(e, lb.inc);
+  TRY(dalloc(e, (void **)&lb.flag, tiles * sizeof(u32)));
+  TRY(dalloc(e, (void **)&lb.agg, tiles * sizeof(u64)));
+  TRY(dalloc(e, (void **)&lb.inc, tiles * sizeof(u64)));
+  CK(e, cudaMemsetAsync(lb.flag, 0, tiles * sizeof(u32), e->s));
+  have = tiles;
+  return GDL_OK;
+}
+
+gdl_status ensure_scratch(gdl_engine *e) {
+  u64 max_cap = 0, max_full = 0, max_newt = 0;
+  for (size_t i = 0; i < e->rels.size(); i++) {
+    const RelDev &r = e->h[i];
+    max_cap = std::max({max_cap, r.full.cap, r.delta.cap, r.newt.cap, r.delta_next.cap});
+    max_full = std::max({max_full, r.full.cap, r.full_next.cap});
+    max_newt = std::max({max_newt, r.newt.cap});
+  }
+  max_newt = std::max(max_newt, e->sort_cap);
+  // sort
+  if (e->sort_cap < max_newt || !e->sort_buf) {
+    dfree(e, e->sort_buf);
+    e->sort_cap = std::max<u64>(max_newt, kMinCap);
+    TRY(dalloc(e, (void **)&e->sort_buf, e->sort_cap * sizeof(u64)));
+  }
+  const u64 tiles = e->sort_cap / kSortTile + 2;
+  const int passes = std::max(sort_passes(e), 1);
+  if (tiles > e->sort_status_tiles || passes > e->sort_status_passes || !e->sort_status) {
+    dfree(e, e->sort_status);
+    e->sort_status_tiles = tiles;
+    e->sort_status_passes = std::max(passes, 4);
+    TRY(dalloc(e, (void **)&e->sort_status,
+               (u64)e->sort_status_passes * tiles * kRadix * sizeof(u32)));
+  }
+  if (!e->sort_offsets) {
+    TRY(dalloc(e, (void **)&e->sort_offsets, kMaxPasses * kRadix * sizeof(u32)));
+    TRY(dalloc(e, (void **)&e->sort_counters, (kMaxPasses + 1) * sizeof(u32)));
+    CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kRadix * sizeof(u32), e->s));
+    CK(e, cudaMemsetAsync(e->sort_counters, 0, (kMaxPasses + 1) * sizeof(u32), e->s));
+  }
+  // join records
+  if (e->crow_cap < max_cap || !e->crow_off) {
+    u64 c = std::max<u64>(max_cap, kMinCap);
+    dfree(e, e->crow_off);
+    dfree(e, e->crow_key);
+    dfree(e, e->crow_start);
+    dfree(e, e->crow_len);
+    TRY(dalloc(e, (void **)&e->crow_off, (c + 1) * sizeof(u64)));
+    TRY(dalloc(e, (void **)&e->crow_key, c * sizeof(u64)));
+    TRY(dalloc(e, (void **)&e->crow_start, c * sizeof(u32)));
+    TRY(dalloc(e, (void **)&e->crow_len, c * sizeof(u32)));
+    e->crow_cap = c;
+  }
+  TRY(ensure_lb(e, e->lb_cnt, e->lb_join_tiles, e->crow_cap / kJoinTile + 2));
+  u64 jt = e->lb_join_tiles;
+  TRY(ensure_lb(e, e->lb_nz, jt, e->lb_join_tiles));
+  TRY(ensure_lb(e, e->lb_merge, e->lb_merge_tiles, (max_full + max_newt) / kMergeTile + 2));
+  return GDL_OK;
+}
+
+// Put the device control block in a runnable state (no stop flags, no
+// graph condition) keeping the build generation.
+gdl_status reset_ctl(gdl_engine *e) {
+  Ctl c;
+  CK(e, cudaMemcpyAsync(&c, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  const u64 g = c.generation;
+  memset(&c, 0, sizeof c);
+  c.generation = g + 1;
+  c.max_iteration = ~0ull;
+  c.stop_at = ~0ull;
+  CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
+  return GDL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel launchers
+// ---------------------------------------------------------------------------
+void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, int *kcount) {
+  SortArgs a;
+  a.keys = d_keys;
+  a.buf0 = buf0;
+  a.buf1 = e->sort_buf;
+  a.cap = std::min(cap, e->sort_cap);
+  a.kbits = e->kbits;
+  a.passes = sort_passes(e);
+  a.offsets = e->sort_offsets;
+  a.status = e->sort_status;
+  a.max_tiles = e->sort_status_tiles;
+  a.counters = e->sort_counters;
+  a.ctl = e->d_ctl;
+  int gh = grid_for(e, cap, (u64)kSortTile * 4, 2);
+  int gp = grid_for(e, cap, kSortTile, 4);
+  k_sort_hist<<<gh, kSortBlock, kSortSmemBytes, e->s>>>(a);
+  for (int p = 0; p < a.passes; p++) k_sort_pass<<<gp, kSortBlock, kSortSmemBytes, e->s>>>(a, p);
+  *kcount += 1 + a.passes;
+}
+
+u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e->sort_buf : buf0; }
+
+// FULL := unique(sort(keys[0..n))) for a load; DELTA/NEWT cleared.
+gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
+  RelHost &rh = e->rels[rel];
+  TRY(pull(e));
+  RelDev &r = e->h[rel];
+  // raw := keys in load order
+  if (rh.raw && !rh.raw_is_full) dfree(e, rh.raw);
+  rh.raw = nullptr;
+  rh.raw_n = n;
+  rh.raw_is_full = false;
+  if (n) {
+    TRY(dalloc(e, (void **)&rh.raw, n * sizeof(u64)));
+    CK(e, cudaMemcpyAsync(rh.raw, keys_dev, n * sizeof(u64), cudaMemcpyDeviceToDevice, e->s));
+  }
+  r.full.n = 0;
+  r.delta.n = 0;
+  r.newt.n = 0;
+  r.full_vis = r.delta_vis = r.w_full_vis = r.w_delta_vis = 1;
+  r.full_idx.epoch = r.full_idx_next.epoch = r.delta_idx.epoch = r.delta_idx_next.epoch = 0;
+  TRY(ensure_arr(e, r.full, n, false));
+  TRY(ensure_arr(e, r.full_next, n, false));
+  if (n) {
+    // sort a copy in the NEWT buffer, then dedup it into FULL
+    TRY(ensure_arr(e, r.newt, n, false));
+    TRY(ensure_arr(e, r.delta_next, n, false));
+    TRY(ensure_scratch(e));
+    CK(e, cudaMemcpyAsync(r.newt.ptr, keys_dev, n * sizeof(u64), cudaMemcpyDeviceToDevice, e->s));
+    r.newt.n = n;
+    TRY(push(e));
+    TRY(reset_ctl(e));
+    int kc = 0;
+    launch_sort(e, &e->d_rels[rel].newt, r.newt.ptr, r.newt.cap, &kc);
+    MergeArgs m;
+    m.newt = &e->d_rels[rel].newt;
+    m.a = sorted_location(e, r.newt.ptr);
+    // B = empty FULL
+    m.full = &e->d_rels[rel].full;
+    m.full_next = &e->d_rels[rel].full_next;
+    m.delta_next = &e->d_rels[rel].delta_next;
+    m.c_newt_n = &e->d_rels[rel].c_newt_n;
+    m.rec = &e->recs[2];
+    m.lb = e->lb_merge;
+    m.ctl = e->d_ctl;
+    m.rel = rel;
+    k_merge_diff<<<grid_for(e, n, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, e->s>>>(m);
+    CK(e, cudaGetLastError());
+    TRY(pull(e));
+    Ctl c2;
+    CK(e, cudaMemcpyAsync(&c2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    CK(e, cudaStreamSynchronize(e->s));
+    if (c2.timeout || c2.oob || c2.overflow)
+      return fail(e, GDL_E_TIMEOUT, "load of %s: device check failed (timeout=%u oob=%u overflow=%u)",
+                  rh.name.c_str(), c2.timeout, c2.oob, c2.overflow);
+    std::swap(r.full, r.full_next);
+    r.newt.n = 0;
+    r.delta_next.n = 0;
+    r.c_newt_n = 0;
+  }
+  TRY(push(e));
+  return GDL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One iteration of a LIE
+// ---------------------------------------------------------------------------
+struct Plan {
+  std::vector<char> full_idx, delta_idx;  // per relation: index needed
+};
+
+Plan make_plan(gdl_engine *e, const LieHost &L) {
+  Plan p;
+  p.full_idx.assign(e->rels.size(), 0);
+  p.delta_idx.assign(e->rels.size(), 0);
+  for (const OpHost &op : L.ops)
+    if (op.kind == 0) (op.inner_ver == GDL_DELTA ? p.delta_idx : p.full_idx)[op.inner] = 1;
+  return p;
+}
+
+void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, int *kc) {
+  cudaStream_t s = e->s;
+  RelDev *R = e->d_rels;
+  k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl);
+  (*kc)++;
+  for (size_t oi = 0; oi < L.ops.size(); oi++) {
+    const OpHost &op = L.ops[oi];
+    if (op.kind == 0) {
+      JoinArgs a;
+      const RelDev &oh = e->h[op.outer];
+      if (op.outer_ver == GDL_DELTA) {
+        a.outer = &R[op.outer].delta;
+        a.outer_vis = &R[op.outer].w_delta_vis;
+      } else if (op.outer_ver == GDL_FULL) {
+        a.outer = &R[op.outer].full;
+        a.outer_vis = &R[op.outer].w_full_vis;
+      } else {
+        a.outer = &R[op.outer].newt;
+        a.outer_vis = nullptr;
+      }
+      if (op.inner_ver == GDL_DELTA) {
+        a.inner = &R[op.inner].delta;
+        a.inner_vis = &R[op.inner].w_delta_vis;
+        a.inner_idx = &R[op.inner].delta_idx;
+      } else {  // FULL (a NEWT inner reads FULL, src/join.cu:14-19)
+        a.inner = &R[op.inner].full;
+        a.inner_vis = &R[op.inner].w_full_vis;
+        a.inner_idx = &R[op.inner].full_idx;
+      }
+      a.out_newt = &R[op.out].newt;
+      a.sel = op.sel;
+      a.pred = op.pred;
+      a.op = L.d_joinrec + oi;
+      a.rec = &e->recs[0];
+      a.lb_cnt = e->lb_cnt;
+      a.lb_nz = e->lb_nz;
+      a.crow_off = e->crow_off;
+      a.crow_start = e->crow_start;
+      a.crow_len = e->crow_len;
+      a.crow_key = e->crow_key;
+      a.crow_cap = e->crow_cap;
+      a.ctl = e->d_ctl;
+      a.out_rel = op.out;
+      u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
+                                oh.newt.cap});
+      k_join_count<<<grid_for(e, outer_cap, kJoinTile, 4), kJoinBlock, 0, s>>>(a);
+      JoinArgs b = a;
+      b.rec = &e->recs[1];
+      const u64 out_cap = e->h[op.out].newt.cap;
+      if (op.pred.kind)
+        k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b);
+      else
+        k_join_mat<<<grid_for(e, out_cap, kMatTile, 8), kMatBlock, 0, s>>>(b);
+      *kc += 2;
+    } else {
+      CopyArgs c;
+      const RelDev &sh = e->h[op.inner];
+      if (op.kind == 2) {
+        c.src = &R[op.inner].newt;
+        c.src_vis = nullptr;
+      } else if (op.inner_ver == GDL_DELTA) {
+        c.src = &R[op.inner].delta;
+        c.src_vis = &R[op.inner].w_delta_vis;
+      } else {
+        c.src = &R[op.inner].full;
+        c.src_vis = &R[op.inner].w_full_vis;
+      }
+      c.dest = &R[op.out].newt;
+      c.sel = op.sel;
+      bool once = op.kind == 1 && op.inner_ver == GDL_FULL;
+      c.once = once ? &L.d_lie->once[oi] : nullptr;
+      c.once_pending = once ? &L.d_lie->once_pending[oi] : nullptr;
+      c.rec = &e->recs[3];
+      c.ctl = e->d_ctl;
+      c.dest_rel = op.out;
+      c.replace = op.kind == 2;
+      u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
+      k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c);
+      (*kc)++;
+    }
+  }
+  for (int r : L.update) {
+    const RelDev &rh = e->h[r];
+    launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
+    MergeArgs m;
+    m.newt = &R[r].newt;
+    m.a = sorted_location(e, rh.newt.ptr);
+    m.full = &R[r].full;
+    m.full_next = &R[r].full_next;
+    m.delta_next = &R[r].delta_next;
+    m.c_newt_n = &R[r].c_newt_n;
+    m.rec = &e->recs[2];
+    m.lb = e->lb_merge;
+    m.ctl = e->d_ctl;
+    m.rel = r;
+    u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
+    k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m);
+    (*kc)++;
+    if (plan.full_idx[r]) {
+      u64 c = std::max(rh.full.cap, rh.full_next.cap);
+      k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
+          &R[r].full_next, &R[r].full_idx_next, &R[r].delta_next, e->d_ctl);
+      (*kc)++;
+    }
+    if (plan.delta_idx[r]) {
+      u64 c = std::max(rh.delta.cap, rh.delta_next.cap);
+      k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
+          &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl);
+      (*kc)++;
+    }
+  }
+  k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl);
+  (*kc)++;
+}
+
+gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
+  if (L.gexec) {
+    cudaGraphExecDestroy(L.gexec);
+    L.gexec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(e, cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t r = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (r != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(e, GDL_E_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(r));
+  }
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  r = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+  if (r != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(e, GDL_E_CUDA, "cudaGraphAddNode(conditional): %s", cudaGetErrorString(r));
+  }
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  CK(e, cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal));
+  int kc = 0;
+  enqueue_iteration(e, L, plan, &kc);
+  cudaGraph_t captured = nullptr;
+  r = cudaStreamEndCapture(e->s, &captured);
+  if (r != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(e, GDL_E_CUDA, "capture of the iteration failed: %s", cudaGetErrorString(r));
+  }
+  r = cudaGraphInstantiate(&L.gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (r != cudaSuccess) return fail(e, GDL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(r));
+  L.cond_handle = (unsigned long long)h;
+  L.kernels_per_iter = kc;
+  L.graph_dirty = false;
+  return GDL_OK;
+}
+
+// Grow the buffers an overflow asked for.
+gdl_status grow_after_overflow(gdl_engine *e, const Ctl &c) {
+  TRY(pull(e));
+  for (size_t i = 0; i < e->rels.size(); i++) {
+    RelDev &r = e->h[i];
+    u64 nn = c.need[need_index((int)i, kNeedNewt)];
+    u64 nf = c.need[need_index((int)i, kNeedFull)];
+    u64 nd = c.need[need_index((int)i, kNeedDelta)];
+    if (nn) {
+      TRY(ensure_arr(e, r.newt, nn + nn / 2, false));
+      if (r.delta_next.cap < r.newt.cap) {
+        TRY(ensure_arr(e, r.delta, r.newt.cap, true));
+        TRY(ensure_arr(e, r.delta_next, r.newt.cap, false));
+      }
+    }
+    if (nf) {
+      TRY(ensure_arr(e, r.full, nf + nf / 2, true));
+      TRY(ensure_arr(e, r.full_next, nf + nf / 2, false));
+      TRY(ensure_index(e, r.full_idx, r.full.cap));
+      TRY(ensure_index(e, r.full_idx_next, r.full_next.cap));
+    }
+    if (nd) {
+      TRY(ensure_arr(e, r.delta, nd + nd / 2, true));
+      TRY(ensure_arr(e, r.delta_next, nd + nd / 2, false));
+      TRY(ensure_index(e, r.delta_idx, r.delta.cap));
+      TRY(ensure_index(e, r.delta_idx_next, r.delta_next.cap));
+    }
+  }
+  TRY(ensure_scratch(e));
+  TRY(push(e));
+  return GDL_OK;
+}
+
+gdl_status validate_rel(gdl_engine *e, int r) {
+  const RelHost &h = e->rels[r];
+  if (h.arity != 2 || h.icols != 1 || h.dep != 0)
+    return fail(e, GDL_E_UNSUPPORTED,
+                "relation %s: only arity 2, index_column_size 1, dependent_column_size 0 "
+                "are supported",
+                h.name.c_str());
+  return GDL_OK;
+}
+
+gdl_status build_index_now(gdl_engine *e, int r, bool delta) {
+  RelDev &h = e->h[r];
+  DArr &a = delta ? h.delta : h.full;
+  Index &ix = delta ? h.delta_idx : h.full_idx;
+  Index &ixn = delta ? h.delta_idx_next : h.full_idx_next;
+  TRY(ensure_index(e, ix, a.cap));
+  TRY(ensure_index(e, ixn, delta ? h.delta_next.cap : h.full_next.cap));
+  TRY(push(e));
+  k_index_build<<<grid_for(e, a.n, kIndexBlock, 8), kIndexBlock, 0, e->s>>>(
+      delta ? &e->d_rels[r].delta : &e->d_rels[r].full,
+      delta ? &e->d_rels[r].delta_idx : &e->d_rels[r].full_idx, nullptr, e->d_ctl);
+  CK(e, cudaGetLastError());
+  TRY(pull(e));
+  return GDL_OK;
+}
+
+gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
+  if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
+  if ((int)L.ops.size() > kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops in one LIE");
+  std::vector<char> is_update(e->rels.size(), 0), is_tmp(e->rels.size(), 0);
+  for (int r : L.update) is_update[r] = 1;
+  for (int r : L.tmps) is_tmp[r] = 1;
+  for (int r : L.update) TRY(validate_rel(e, r));
+  for (int r : L.statics) TRY(validate_rel(e, r));
+  for (int r : L.tmps) TRY(validate_rel(e, r));
+  for (const OpHost &op : L.ops) {
+    TRY(validate_rel(e, op.inner));
+    if (op.outer >= 0) TRY(validate_rel(e, op.outer));
+    TRY(validate_rel(e, op.out));
+    if (!is_update[op.out] && !is_tmp[op.out])
+      return fail(e, GDL_E_UNSUPPORTED,
+                  "op output %s is neither an update nor a tmp relation of the LIE",
+                  e->rels[op.out].name.c_str());
+  }
+  const Plan plan = make_plan(e, L);
+  TRY(reset_ctl(e));
+  TRY(pull(e));
+  // Setup (src/lie.cu:49-59): DELTA := the first |FULL| rows of FULL's raw
+  // buffer; capacities for the loop.
+  for (int r : L.update) {
+    RelDev &h = e->h[r];
+    RelHost &rh = e->rels[r];
+    if (!h.full_vis) h.full.n = 0;  // tuple_full gets tuple_counts rows
+    const u64 take = rh.raw_is_full ? h.full.n : std::min(h.full.n, rh.raw_n);
+    const u64 base = std::max<u64>(2 * h.full.n, kMinCap);
+    TRY(ensure_arr(e, h.full, base, true));
+    TRY(ensure_arr(e, h.full_next, h.full.cap, false));
+    TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, base), false));
+    TRY(ensure_arr(e, h.delta, std::max<u64>(take, h.newt.cap), false));
+    TRY(ensure_arr(e, h.delta_next, h.delta.cap, false));
+    if (take)
+      CK(e, cudaMemcpyAsync(h.delta.ptr, rh.raw_is_full ? h.full.ptr : rh.raw, take * sizeof(u64),
+                            cudaMemcpyDeviceToDevice, e->s));
+    h.delta.n = take;
+    h.delta_vis = 1;
+    rh.delta_sorted = rh.raw_is_full;
+    h.newt.n = 0;
+  }
+  for (int r : L.tmps) {
+    RelDev &h = e->h[r];
+    TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, kMinCap), false));
+    h.newt.n = 0;
+  }
+  TRY(ensure_scratch(e));
+  TRY(push(e));
+  // An unsorted DELTA (raw load order) used as a join inner is sorted and
+  // deduplicated first (the reference's index walk is undefined there).
+  for (int r : L.update) {
+    if (plan.delta_idx[r] && !e->rels[r].delta_sorted && e->h[r].delta.n) {
+      RelDev &h = e->h[r];
+      const u64 n = h.delta.n;
+      TRY(ensure_arr(e, h.newt, n, false));
+      CK(e, cudaMemcpyAsync(h.newt.ptr, h.delta.ptr, n * sizeof(u64), cudaMemcpyDeviceToDevice, e->s));
+      u64 *keys = h.newt.ptr;
+      h.newt.n = n;
+      TRY(push(e));
+      int kc = 0;
+      launch_sort(e, &e->d_rels[r].newt, keys, h.newt.cap, &kc);
+      TRY(pull(e));
+      CK(e, cudaMemcpyAsync(h.delta.ptr, sorted_location(e, keys), n * sizeof(u64),
+                            cudaMemcpyDeviceToDevice, e->s));
+      // unique in place on the host side is not needed: duplicates in an
+      // index run only repeat outputs, which the later dedup removes.
+      h.newt.n = 0;
+      e->rels[r].delta_sorted = true;
+      TRY(push(e));
+    }
+  }
+  // Indexes every join of this LIE probes.
+  for (size_t r = 0; r < e->rels.size(); r++) {
+    if (plan.full_idx[r]) TRY(build_index_now(e, (int)r, false));
+    if (plan.delta_idx[r]) TRY(build_index_now(e, (int)r, true));
+  }
+  // Device LIE description.
+  LieDev ld;
+  CK(e, cudaMemcpyAsync(&ld, L.d_lie, sizeof(LieDev), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  ld.n_update = (int)L.update.size();
+  ld.n_static = (int)L.statics.size();
+  ld.n_tmp = (int)L.tmps.size();
+  ld.n_ops = (int)L.ops.size();
+  for (size_t i = 0; i < L.update.size(); i++) ld.update[i] = L.update[i];
+  for (size_t i = 0; i < L.statics.size(); i++) ld.statics[i] = L.statics[i];
+  for (size_t i = 0; i < L.tmps.size(); i++) ld.tmps[i] = L.tmps[i];
+  // trace buffer: rows for one batch
+  const u64 trace_rows = 256;
+  if (!ld.trace) TRY(dalloc(e, (void **)&ld.trace, trace_rows * kMaxRels * 3 * sizeof(u64)));
+  CK(e, cudaMemcpyAsync(L.d_lie, &ld, sizeof(LieDev), cudaMemcpyHostToDevice, e->s));
+  // Control block.
+  Ctl c;
+  CK(e, cudaMemcpyAsync(&c, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  const u64 generation = c.generation;
+  memset(&c, 0, sizeof c);
+  c.generation = generation + 1;
+  c.max_iteration = L.max_iteration < 0 ? 0 : (u64)L.max_iteration;
+  c.trace_rows = trace_rows;
+  L.trace.clear();
+  L.retries = 0;
+  L.graph_launches = 0;
+  L.kernels = 0;
+  L.graph_dirty = true;
+  const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr;
+  CK(e, cudaEventRecord(e->ev0, e->s));
+  u64 batch = 4;
+  while (true) {
+    c.pause = 0;
+    c.stop_at = c.iteration + (use_graph ? std::min<u64>(trace_rows, 1u << 20) : batch);
+    c.trace_base = c.iteration;
+    if (use_graph && L.graph_dirty) TRY(build_graph(e, L, plan));
+    c.cond_set = use_graph ? 1 : 0;
+    c.cond_handle = use_graph ? L.cond_handle : 0;
+    CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
+    const u64 it0 = c.iteration;
+    if (use_graph) {
+      CK(e, cudaGraphLaunch(L.gexec, e->s));
+      L.graph_launches++;
+    } else {
+      for (u64 k = 0; k < std::min<u64>(batch, trace_rows); k++) {
+        int kc = 0;
+        enqueue_iteration(e, L, plan, &kc);
+        L.kernels_per_iter = kc;
+      }
+      CK(e, cudaGetLastError());
+    }
+    CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    CK(e, cudaStreamSynchronize(e->s));
+    c = *e->h_ctl;
+    const u64 ran = c.iteration - it0;
+    L.kernels += (ran + (c.overflow ? 1 : 0)) * (u64)L.kernels_per_iter;
+    if (L.trace_on && ran) {
+      std::vector<u64> rows(ran * L.update.size() * 3);
+      CK(e, cudaMemcpyAsync(rows.data(), ld.trace, rows.size() * sizeof(u64),
+                            cudaMemcpyDeviceToHost, e->s));
+      CK(e, cudaStreamSynchronize(e->s));
+      for (u64 t = 0; t < ran; t++)
+        for (size_t i = 0; i < L.update.size(); i++) {
+          const u64 *x = &rows[(t * L.update.size() + i) * 3];
+          L.trace.insert(L.trace.end(), {it0 + t, (u64)L.update[i], x[0], x[1], x[2]});
+        }
+    }
+    if (c.timeout || c.oob) {
+      e->broken = true;
+      return fail(e, GDL_E_TIMEOUT,
+                  "device-side check failed in iteration %llu (timeout=%u, dropped writes=%u)",
+                  (unsigned long long)c.iteration, c.timeout, c.oob);
+    }
+    if (c.overflow) {
+      TRY(grow_after_overflow(e, c));
+      c.overflow = 0;
+      memset(c.need, 0, sizeof c.need);
+      L.retries++;
+      L.graph_dirty = true;
+      continue;
+    }
+    if (c.done) break;
+    batch = std::min<u64>(batch * 2, 64);
+  }
+  CK(e, cudaEventRecord(e->ev1, e->s));
+  CK(e, cudaEventSynchronize(e->ev1));
+  float ms = 0;
+  CK(e, cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+  L.ms = ms;
+  L.iterations = c.iteration;
+  e->kernels_launched += L.kernels;
+  // Finish (src/lie.cu:217-260).
+  TRY(pull(e));
+  for (int r : L.update) {
+    RelDev &h = e->h[r];
+    RelHost &rh = e->rels[r];
+    if (L.reload_full) {
+      // FULL becomes flat, sorted and indexed; it is now its own raw buffer.
+      if (rh.raw && !rh.raw_is_full) dfree(e, rh.raw);
+      rh.raw = nullptr;
+      rh.raw_is_full = true;
+      rh.raw_n = h.full.n;
+      h.full_vis = 1;
+      h.delta.n = 0;
+      h.delta_vis = 1;
+      h.newt.n = 0;
+    }
+  }
+  TRY(push(e));
+  *out_iters = c.iteration;
+  return GDL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+const char *gdl_version(void) { return "gdlog-b200 0.1 (sm_100a)"; }
+
+const char *gdl_status_string(gdl_status s) {
+  switch (s) {
+    case GDL_OK: return "ok";
+    case GDL_E_INVALID: return "invalid argument";
+    case GDL_E_CUDA: return "CUDA error";
+    case GDL_E_NOMEM: return "out of device memory";
+    case GDL_E_UNSUPPORTED: return "unsupported";
+    case GDL_E_TIMEOUT: return "device-side wait or check failed";
+    case GDL_E_CAPACITY: return "buffer too small";
+  }
+  return "unknown status";
+}
+
+const char *gdl_last_error(const gdl_engine *e) { return e ? e->err.c_str() : "null engine"; }
+
+gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
+  if (!out) return GDL_E_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GDL_E_CUDA;
+  if (device < 0 || device >= ndev) return GDL_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return GDL_E_CUDA;
+  gdl_engine *e = new gdl_engine;
+  e->device = device;
+  cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device);
+  if (stream) {
+    e->s = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking) != cudaSuccess) {
+      delete e;
+      return GDL_E_CUDA;
+    }
+    e->own_stream = true;
+  }
+  auto bad = [&](cudaError_t r) {
+    if (r == cudaSuccess) return false;
+    e->err = cudaGetErrorString(r);
+    return true;
+  };
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    u64 thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  if (bad(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSortSmemBytes)) ||
+      bad(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSortSmemBytes)) ||
+      bad(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kMergeSmemBytes)) ||
+      bad(cudaMalloc(&e->d_rels, kMaxRels * sizeof(RelDev))) ||
+      bad(cudaMalloc(&e->d_ctl, sizeof(Ctl))) || bad(cudaMallocHost(&e->h_ctl, sizeof(Ctl))) ||
+      bad(cudaMalloc(&e->recs, 8 * sizeof(LaunchRec))) ||
+      bad(cudaMalloc(&e->d_tmp, 4 * sizeof(DArr))) || bad(cudaMalloc(&e->d_u64, 4 * sizeof(u64))) ||
+      bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) || bad(cudaEventCreate(&e->ev0)) ||
+      bad(cudaEventCreate(&e->ev1)) ||
+      bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
+      bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
+      bad(cudaMemsetAsync(e->recs, 0, 8 * sizeof(LaunchRec), e->s)) ||
+      bad(cudaStreamSynchronize(e->s))) {
+    gdl_engine_destroy(e);
+    return GDL_E_CUDA;
+  }
+  *out = e;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_destroy(gdl_engine *e) {
+  if (!e) return GDL_OK;
+  cudaSetDevice(e->device);
+  if (e->s) cudaStreamSynchronize(e->s);
+  for (size_t i = 0; i < e->rels.size(); i++) {
+    RelDev &r = e->h[i];
+    for (DArr *a : {&r.full, &r.full_next, &r.delta, &r.delta_next, &r.newt}) cudaFree(a->ptr);
+    for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
+      cudaFree(x->slots);
+    if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFree(e->rels[i].raw);
+  }
+  for (LieHost &L : e->lies) {
+    if (L.gexec) cudaGraphExecDestroy(L.gexec);
+    if (L.d_lie) {
+      LieDev ld;
+      if (cudaMemcpy(&ld, L.d_lie, sizeof ld, cudaMemcpyDeviceToHost) == cudaSuccess)
+        cudaFree(ld.trace);
+      cudaFree(L.d_lie);
+    }
+    cudaFree(L.d_joinrec);
+  }
+  for (void *p : {(void *)e->sort_buf, (void *)e->sort_offsets, (void *)e->sort_counters,
+                  (void *)e->sort_status, (void *)e->crow_off, (void *)e->crow_key,
+                  (void *)e->crow_start, (void *)e->crow_len, (void *)e->lb_cnt.flag,
+                  (void *)e->lb_cnt.agg, (void *)e->lb_cnt.inc, (void *)e->lb_nz.flag,
+                  (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
+                  (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->recs,
+                  (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
+                  (void *)e->d_ctl})
+    if (p) cudaFree(p);
+  if (e->h_ctl) cudaFreeHost(e->h_ctl);
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->own_stream && e->s) cudaStreamDestroy(e->s);
+  delete e;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_sync(gdl_engine *e) {
+  if (!e) return GDL_E_INVALID;
+  CK(e, cudaStreamSynchronize(e->s));
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_create(gdl_engine *e, const char *name, int32_t arity, int32_t icols,
+                               int32_t dep, int32_t index_flag, int32_t tmp_flag, int32_t *out) {
+  if (!e || !out) return GDL_E_INVALID;
+  if ((int)e->rels.size() >= kMaxRels) return fail(e, GDL_E_UNSUPPORTED, "too many relations");
+  if (arity < 1 || icols < 1 || icols > arity || dep < 0 || dep >= arity)
+    return fail(e, GDL_E_INVALID, "bad arity/index/dependent column sizes");
+  if (arity != 2) return fail(e, GDL_E_UNSUPPORTED, "arity %d not supported (arity 2 only)", arity);
+  cudaSetDevice(e->device);
+  RelHost rh;
+  rh.name = name ? name : "";
+  rh.arity = arity;
+  rh.icols = icols;
+  rh.dep = dep;
+  rh.index_flag = index_flag != 0;
+  rh.tmp_flag = tmp_flag != 0;
+  e->rels.push_back(rh);
+  RelDev d;
+  memset(&d, 0, sizeof d);
+  d.full_vis = d.delta_vis = d.w_full_vis = d.w_delta_vis = 1;
+  e->h.push_back(d);
+  *out = (int32_t)e->rels.size() - 1;
+  TRY(pull(e));  // keep the mirror coherent, then write the new entry
+  e->h.back() = d;
+  TRY(push(e));
+  return GDL_OK;
+}
+
+#define CHECK_REL(e, r)                                                        \
+  do {                                                                          \
+    if (!(e)) return GDL_E_INVALID;                                             \
+    if ((r) < 0 || (r) >= (int)(e)->rels.size())                                \
+      return fail((e), GDL_E_INVALID, "bad relation id %d", (int)(r));          \
+    cudaSetDevice((e)->device);                                                 \
+  } while (0)
+#define CHECK_LIE(e, l)                                                        \
+  do {                                                                          \
+    if (!(e)) return GDL_E_INVALID;                                             \
+    if ((l) < 0 || (l) >= (int)(e)->lies.size())                                \
+      return fail((e), GDL_E_INVALID, "bad lie id %d", (int)(l));               \
+    cudaSetDevice((e)->device);                                                 \
+  } while (0)
+
+static gdl_status load_common(gdl_engine *e, int32_t rel, const uint64_t *rows, uint64_t n,
+                              bool on_device) {
+  if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
+  if (n > kMaxRows) return fail(e, GDL_E_UNSUPPORTED, "too many rows");
+  if (n == 0) return load_keys(e, rel, nullptr, 0);
+  u64 *d_rows = nullptr, *d_keys = nullptr;
+  if (on_device) {
+    d_rows = (u64 *)rows;
+  } else {
+    TRY(dalloc(e, (void **)&d_rows, n * 2 * sizeof(u64)));
+    CK(e, cudaMemcpyAsync(d_rows, rows, n * 2 * sizeof(u64), cudaMemcpyHostToDevice, e->s));
+  }
+  TRY(dalloc(e, (void **)&d_keys, n * sizeof(u64)));
+  CK(e, cudaMemsetAsync(e->d_u64, 0, sizeof(u64), e->s));
+  CK(e, cudaMemsetAsync(e->d_u32, 0, sizeof(u32), e->s));
+  k_pack_rows<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(d_rows, n, d_keys, e->d_u64, e->d_u32);
+  CK(e, cudaGetLastError());
+  u64 maxv = 0;
+  u32 badv = 0;
+  CK(e, cudaMemcpyAsync(&maxv, e->d_u64, sizeof maxv, cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaMemcpyAsync(&badv, e->d_u32, sizeof badv, cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  if (!on_device) dfree(e, d_rows);
+  if (badv) {
+    dfree(e, d_keys);
+    return fail(e, GDL_E_UNSUPPORTED, "column values must be below 2^32");
+  }
+  e->max_value = std::max(e->max_value, maxv);
+  e->kbits = std::max(e->kbits, bits_for(e->max_value));
+  gdl_status s = load_keys(e, rel, d_keys, n);
+  dfree(e, d_keys);
+  return s;
+}
+
+gdl_status gdl_relation_load(gdl_engine *e, int32_t rel, const uint64_t *rows, uint64_t n) {
+  CHECK_REL(e, rel);
+  if (n && !rows) return fail(e, GDL_E_INVALID, "null rows");
+  return load_common(e, rel, rows, n, false);
+}
+
+gdl_status gdl_relation_load_device(gdl_engine *e, int32_t rel, const uint64_t *rows, uint64_t n) {
+  CHECK_REL(e, rel);
+  if (n && !rows) return fail(e, GDL_E_INVALID, "null rows");
+  return load_common(e, rel, rows, n, true);
+}
+
+static gdl_status version_view(gdl_engine *e, int rel, int ver, const u64 **ptr, u64 *n,
+                               bool *sorted) {
+  TRY(pull(e));
+  const RelDev &r = e->h[rel];
+  *sorted = true;
+  if (ver == GDL_FULL) {
+    *ptr = r.full.ptr;
+    *n = r.full_vis ? r.full.n : 0;
+  } else if (ver == GDL_DELTA) {
+    *ptr = r.delta.ptr;
+    *n = r.delta_vis ? r.delta.n : 0;
+    *sorted = e->rels[rel].delta_sorted;
+  } else if (ver == GDL_NEWT) {
+    *ptr = r.newt.ptr;
+    *n = r.newt.n;
+    *sorted = false;
+  } else {
+    return fail(e, GDL_E_INVALID, "bad version %d", ver);
+  }
+  return GDL_OK;
+}
+
+static gdl_status host_rows(gdl_engine *e, int rel, int ver, std::vector<u64> &keys) {
+  const u64 *p = nullptr;
+  u64 n = 0;
+  bool sorted;
+  TRY(version_view(e, rel, ver, &p, &n, &sorted));
+  keys.resize(n);
+  if (n) CK(e, cudaMemcpyAsync(keys.data(), p, n * sizeof(u64), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  if (!sorted) {
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  }
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_size(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *out) {
+  CHECK_REL(e, rel);
+  if (!out) return GDL_E_INVALID;
+  if (ver == GDL_NEWT) {
+    std::vector<u64> k;
+    TRY(host_rows(e, rel, ver, k));
+    *out = k.size();
+    return GDL_OK;
+  }
+  const u64 *p = nullptr;
+  u64 n = 0;
+  bool sorted;
+  TRY(version_view(e, rel, ver, &p, &n, &sorted));
+  *out = n;
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *rows,
+                               uint64_t cap, uint64_t *out_n) {
+  CHECK_REL(e, rel);
+  if (!out_n) return GDL_E_INVALID;
+  std::vector<u64> k;
+  TRY(host_rows(e, rel, ver, k));
+  *out_n = k.size();
+  if (k.size() > cap) return fail(e, GDL_E_CAPACITY, "export needs %zu rows", k.size());
+  if (k.size() && !rows) return GDL_E_INVALID;
+  for (size_t i = 0; i < k.size(); i++) {
+    rows[2 * i] = key_c0(k[i]);
+    rows[2 * i + 1] = key_c1(k[i]);
+  }
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *out) {
+  CHECK_REL(e, rel);
+  if (!out) return GDL_E_INVALID;
+  const u64 *p = nullptr;
+  u64 n = 0;
+  bool sorted;
+  TRY(version_view(e, rel, ver, &p, &n, &sorted));
+  u64 acc = 0;
+  if (!sorted) {
+    std::vector<u64> k;
+    TRY(host_rows(e, rel, ver, k));
+    for (size_t i = 0; i < k.size(); i++) {
+      u64 h = mix64(i);
+      h = mix64(h ^ (u64)key_c0(k[i]));
+      h = mix64(h ^ (u64)key_c1(k[i]));
+      acc += h;
+    }
+    *out = mix64(acc ^ (u64)k.size());
+    return GDL_OK;
+  }
+  CK(e, cudaMemsetAsync(e->d_u64, 0, sizeof(u64), e->s));
+  if (n) k_digest<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(p, n, e->d_u64);
+  CK(e, cudaGetLastError());
+  CK(e, cudaMemcpyAsync(&acc, e->d_u64, sizeof acc, cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  *out = mix64(acc ^ n);
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_create(gdl_engine *e, int32_t *out) {
+  if (!e || !out) return GDL_E_INVALID;
+  cudaSetDevice(e->device);
+  LieHost L;
+  CK(e, cudaMalloc(&L.d_lie, sizeof(LieDev)));
+  CK(e, cudaMemset(L.d_lie, 0, sizeof(LieDev)));
+  CK(e, cudaMalloc(&L.d_joinrec, kMaxOps * sizeof(JoinRec)));
+  CK(e, cudaMemset(L.d_joinrec, 0, kMaxOps * sizeof(JoinRec)));
+  e->lies.push_back(L);
+  *out = (int32_t)e->lies.size() - 1;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_relation(gdl_engine *e, int32_t lie, int32_t rel, int32_t static_flag) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, rel);
+  LieHost &L = e->lies[lie];
+  (static_flag ? L.statics : L.update).push_back(rel);
+  L.graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_tmp_relation(gdl_engine *e, int32_t lie, int32_t rel) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, rel);
+  e->lies[lie].tmps.push_back(rel);
+  e->lies[lie].graph_dirty = true;
+  return GDL_OK;
+}
+
+static gdl_status decode_sel(gdl_engine *e, const int32_t *gen, int32_t len, bool join, Sel2 *s) {
+  if (!gen || len != 2) return fail(e, GDL_E_INVALID, "gen must have 2 entries (arity 2)");
+  int v[2];
+  for (int j = 0; j < 2; j++) {
+    int g = gen[j];
+    if (g == GDL_INNER(0) || g == GDL_INNER(1))
+      v[j] = g;
+    else if (join && (g == GDL_OUTER(0) || g == GDL_OUTER(1)))
+      v[j] = 2 + (g - 16);
+    else
+      return fail(e, GDL_E_INVALID, "gen entry %d out of range", g);
+  }
+  s->s0 = v[0];
+  s->s1 = v[1];
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_join(gdl_engine *e, int32_t lie, int32_t inner, int32_t inner_ver,
+                            int32_t outer, int32_t outer_ver, int32_t output, const int32_t *gen,
+                            int32_t gen_len, int32_t pred_kind, int32_t pa, int32_t pb) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, inner);
+  CHECK_REL(e, outer);
+  CHECK_REL(e, output);
+  if (inner_ver < 0 || inner_ver > 2 || outer_ver < 0 || outer_ver > 2)
+    return fail(e, GDL_E_INVALID, "bad version");
+  if (pred_kind < GDL_PRED_NONE || pred_kind > GDL_PRED_GE)
+    return fail(e, GDL_E_INVALID, "bad predicate");
+  if (pred_kind && (pa < 0 || pa > 1 || pb < 0 || pb > 1))
+    return fail(e, GDL_E_INVALID, "predicate column out of range");
+  if ((int)e->lies[lie].ops.size() >= kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops");
+  OpHost op;
+  op.kind = 0;
+  op.inner = inner;
+  op.inner_ver = inner_ver;
+  op.outer = outer;
+  op.outer_ver = outer_ver;
+  op.out = output;
+  TRY(decode_sel(e, gen, gen_len, true, &op.sel));
+  op.pred = Pred{pred_kind, pa, pb};
+  e->lies[lie].ops.push_back(op);
+  e->lies[lie].graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_copy(gdl_engine *e, int32_t lie, int32_t src, int32_t src_ver, int32_t dest,
+                            const int32_t *gen, int32_t gen_len) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, src);
+  CHECK_REL(e, dest);
+  if (src_ver != GDL_DELTA && src_ver != GDL_FULL)
+    return fail(e, GDL_E_INVALID, "copy source must be DELTA or FULL");
+  if ((int)e->lies[lie].ops.size() >= kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops");
+  OpHost op;
+  op.kind = 1;
+  op.inner = src;
+  op.inner_ver = src_ver;
+  op.out = dest;
+  TRY(decode_sel(e, gen, gen_len, false, &op.sel));
+  e->lies[lie].ops.push_back(op);
+  e->lies[lie].graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_acopy(gdl_engine *e, int32_t lie, int32_t src, int32_t dest,
+                             const int32_t *gen, int32_t gen_len) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, src);
+  CHECK_REL(e, dest);
+  if ((int)e->lies[lie].ops.size() >= kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops");
+  OpHost op;
+  op.kind = 2;
+  op.inner = src;
+  op.inner_ver = GDL_NEWT;
+  op.out = dest;
+  TRY(decode_sel(e, gen, gen_len, false, &op.sel));
+  e->lies[lie].ops.push_back(op);
+  e->lies[lie].graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_set_max_iteration(gdl_engine *e, int32_t lie, int64_t m) {
+  CHECK_LIE(e, lie);
+  e->lies[lie].max_iteration = m;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_set_reload_full(gdl_engine *e, int32_t lie, int32_t flag) {
+  CHECK_LIE(e, lie);
+  e->lies[lie].reload_full = flag != 0;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_set_trace(gdl_engine *e, int32_t lie, int32_t flag) {
+  CHECK_LIE(e, lie);
+  e->lies[lie].trace_on = flag != 0;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_fixpoint(gdl_engine *e, int32_t lie, uint64_t *out) {
+  CHECK_LIE(e, lie);
+  uint64_t dummy;
+  return fixpoint(e, e->lies[lie], out ? out : &dummy);
+}
+
+gdl_status gdl_lie_trace(gdl_engine *e, int32_t lie, uint64_t *rec, uint64_t cap, uint64_t *out_n) {
+  CHECK_LIE(e, lie);
+  const std::vector<uint64_t> &t = e->lies[lie].trace;
+  uint64_t n = t.size() / 5;
+  if (out_n) *out_n = n;
+  if (rec) memcpy(rec, t.data(), std::min(n, cap) * 5 * sizeof(uint64_t));
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out, int32_t n_out) {
+  CHECK_LIE(e, lie);
+  const LieHost &L = e->lies[lie];
+  double v[5] = {L.ms, (double)L.kernels, (double)L.iterations, (double)L.retries,
+                 (double)L.graph_launches};
+  for (int i = 0; i < n_out && i < 5; i++) out[i] = v[i];
+  return GDL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+"""ctypes binding of the engine's C-ABI (include/gdlog_b200.h).
+
+Mirrors the reference's operator API for the semi-naive path, so that a
+program reads like the reference drivers (test/tc.cu, test/sg.cu,
+test/cspa.cu):
+
+    eng = Engine("gpu")
+    path = eng.relation("path_2__1_2", index_flag=False)
+    eng.load(path, edges)                         # load_relation
+    lie = eng.lie()                               # LIE(grid, block)
+    lie.add_relations(edge, static=True)          # LIE::add_relations
+    lie.add_join(edge, FULL, path, DELTA, path,   # RelationalJoin(...)
+                 gen=(INNER(1), OUTER(1)))
+    iterations = lie.fixpoint()                   # LIE::fixpoint_loop
+
+The same class drives the CPU oracle (``Engine("oracle")``, test
+infrastructure) through its mirror C-ABI, so tests run one program on both.
+The GPU backend fails loudly when its shared library is missing: there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+GPU_LIB = os.path.join(HERE, "lib", "libgdlog_b200.so")
+ORACLE_LIB = os.path.join(REPO, "oracle", "liboracle.so")
+
+DELTA, FULL, NEWT = 0, 1, 2
+PRED_NONE, PRED_NE, PRED_EQ, PRED_LT, PRED_LE, PRED_GT, PRED_GE = range(7)
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "UNSUPPORTED",
+          5: "TIMEOUT", 6: "CAPACITY"}
+
+
+def INNER(c: int) -> int:
+    return c
+
+
+def OUTER(c: int) -> int:
+    return 16 + c
+
+
+def SRC(c: int) -> int:
+    return c
+
+
+class GdlError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_I = C.c_int32
+_U64 = C.c_uint64
+_PU64 = C.POINTER(C.c_uint64)
+_PI = C.POINTER(C.c_int32)
+
+# (name, argtypes) shared by both prefixes; engine pointer first.
+_SIGS = {
+    "relation_create": [_P, C.c_char_p, _I, _I, _I, _I, _I, _PI],
+    "relation_load": [_P, _I, _PU64, _U64],
+    "relation_size": [_P, _I, _I, _PU64],
+    "relation_export": [_P, _I, _I, _PU64, _U64, _PU64],
+    "relation_digest": [_P, _I, _I, _PU64],
+    "lie_create": [_P, _PI],
+    "lie_add_relation": [_P, _I, _I, _I],
+    "lie_add_tmp_relation": [_P, _I, _I],
+    "lie_add_join": [_P, _I, _I, _I, _I, _I, _I, _PI, _I, _I, _I, _I],
+    "lie_add_copy": [_P, _I, _I, _I, _I, _PI, _I],
+    "lie_add_acopy": [_P, _I, _I, _I, _PI, _I],
+    "lie_set_max_iteration": [_P, _I, C.c_int64],
+    "lie_set_reload_full": [_P, _I, _I],
+    "lie_fixpoint": [_P, _I, _PU64],
+    "lie_trace": [_P, _I, _PU64, _U64, _PU64],
+}
+
+_libs: dict = {}
+
+
+def load_library(kind: str) -> C.CDLL:
+    """Open the GPU engine ("gpu") or the CPU oracle ("oracle") library."""
+    if kind in _libs:
+        return _libs[kind]
+    path = GPU_LIB if kind == "gpu" else ORACLE_LIB
+    if not os.path.exists(path):
+        raise GdlError(4, f"{kind} library not built: {path} (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    pre = "gdl_" if kind == "gpu" else "orc_"
+    for name, args in _SIGS.items():
+        f = getattr(lib, pre + name)
+        f.argtypes = args
+        f.restype = _I
+    if kind == "gpu":
+        lib.gdl_engine_create.argtypes = [_I, _P, C.POINTER(_P)]
+        lib.gdl_engine_create.restype = _I
+        lib.gdl_engine_destroy.argtypes = [_P]
+        lib.gdl_engine_destroy.restype = _I
+        lib.gdl_last_error.argtypes = [_P]
+        lib.gdl_last_error.restype = C.c_char_p
+        lib.gdl_version.restype = C.c_char_p
+        lib.gdl_lie_stats.argtypes = [_P, _I, C.POINTER(C.c_double), _I]
+        lib.gdl_lie_stats.restype = _I
+        lib.gdl_lie_set_trace.argtypes = [_P, _I, _I]
+        lib.gdl_lie_set_trace.restype = _I
+        lib.gdl_engine_sync.argtypes = [_P]
+        lib.gdl_engine_sync.restype = _I
+        lib.gdl_relation_load_device.argtypes = [_P, _I, _P, _U64]
+        lib.gdl_relation_load_device.restype = _I
+    else:
+        lib.orc_engine_create.argtypes = [_I, _I, C.POINTER(_P)]
+        lib.orc_engine_create.restype = _I
+        lib.orc_engine_destroy.argtypes = [_P]
+        lib.orc_engine_destroy.restype = _I
+        lib.orc_last_error.argtypes = [_P]
+        lib.orc_last_error.restype = C.c_char_p
+        lib.orc_threads.argtypes = [_P]
+        lib.orc_threads.restype = _I
+        lib.orc_lie_seconds.argtypes = [_P, _I, C.POINTER(C.c_double)]
+        lib.orc_lie_seconds.restype = _I
+    _libs[kind] = lib
+    return lib
+
+
+class Relation:
+    """Handle of a declared relation (include/relation.cuh:257-300)."""
+
+    def __init__(self, eng: "Engine", rid: int, name: str, arity: int):
+        self.eng, self.id, self.name, self.arity = eng, rid, name, arity
+
+    def size(self, version: int = FULL) -> int:
+        return self.eng.size(self, version)
+
+    def rows(self, version: int = FULL) -> np.ndarray:
+        return self.eng.export(self, version)
+
+    def digest(self, version: int = FULL) -> int:
+        return self.eng.digest(self, version)
+
+    def __repr__(self):
+        return f"Relation({self.name!r}, id={self.id})"
+
+
+class Lie:
+    """LIE (include/lie.cuh:11-65)."""
+
+    def __init__(self, eng: "Engine", lid: int):
+        self.eng, self.id = eng, lid
+        self.iterations = None
+
+    def _call(self, name, *args):
+        return self.eng._call(name, *args)
+
+    def add_relations(self, rel: Relation, static: bool) -> None:
+        self._call("lie_add_relation", self.id, rel.id, int(bool(static)))
+
+    def add_tmp_relation(self, rel: Relation) -> None:
+        self._call("lie_add_tmp_relation", self.id, rel.id)
+
+    def add_join(self, inner: Relation, inner_ver: int, outer: Relation, outer_ver: int,
+                 output: Relation, gen, pred=None) -> None:
+        g = (C.c_int32 * len(gen))(*gen)
+        kind, a, b = pred if pred else (PRED_NONE, 0, 0)
+        self._call("lie_add_join", self.id, inner.id, inner_ver, outer.id, outer_ver,
+                   output.id, g, len(gen), kind, a, b)
+
+    def add_copy(self, src: Relation, src_ver: int, dest: Relation, gen) -> None:
+        g = (C.c_int32 * len(gen))(*gen)
+        self._call("lie_add_copy", self.id, src.id, src_ver, dest.id, g, len(gen))
+
+    def add_acopy(self, src: Relation, dest: Relation, gen) -> None:
+        g = (C.c_int32 * len(gen))(*gen)
+        self._call("lie_add_acopy", self.id, src.id, dest.id, g, len(gen))
+
+    @property
+    def max_iteration(self):
+        return None
+
+    @max_iteration.setter
+    def max_iteration(self, m: int) -> None:
+        self._call("lie_set_max_iteration", self.id, int(m))
+
+    def set_reload_full(self, flag: bool) -> None:
+        self._call("lie_set_reload_full", self.id, int(bool(flag)))
+
+    reload_full_flag = property(None, set_reload_full)
+
+    def set_trace(self, flag: bool) -> None:
+        if self.eng.kind == "gpu":
+            self.eng._check(self.eng.lib.gdl_lie_set_trace(self.eng.h, self.id, int(bool(flag))))
+
+    def fixpoint(self) -> int:
+        out = C.c_uint64(0)
+        self._call("lie_fixpoint", self.id, C.byref(out))
+        self.iterations = int(out.value)
+        return self.iterations
+
+    def trace(self) -> np.ndarray:
+        n = C.c_uint64(0)
+        self._call("lie_trace", self.id, None, 0, C.byref(n))
+        buf = np.zeros(int(n.value) * 5, dtype=np.uint64)
+        self._call("lie_trace", self.id, buf.ctypes.data_as(_PU64), n.value, C.byref(n))
+        return buf.reshape(-1, 5)
+
+    def stats(self) -> dict:
+        if self.eng.kind != "gpu":
+            s = C.c_double(0)
+            self.eng._check(self.eng.lib.orc_lie_seconds(self.eng.h, self.id, C.byref(s)))
+            return {"ms": s.value * 1e3}
+        out = (C.c_double * 5)()
+        self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 5))
+        return {"ms": out[0], "kernels": int(out[1]), "iterations": int(out[2]),
+                "retries": int(out[3]), "graph_launches": int(out[4])}
+
+
+class Engine:
+    """One engine (GPU: one CUDA stream on one device; oracle: CPU threads)."""
+
+    def __init__(self, kind: str = "gpu", device: int = 0, threads: int = 0,
+                 max_arity: int = 2, stream: int | None = None):
+        if kind not in ("gpu", "oracle"):
+            raise ValueError(kind)
+        self.kind = kind
+        self.lib = load_library(kind)
+        self.pre = "gdl_" if kind == "gpu" else "orc_"
+        h = _P()
+        if kind == "gpu":
+            code = self.lib.gdl_engine_create(device, stream, C.byref(h))
+            if code:
+                raise GdlError(code, "gdl_engine_create failed (no CUDA device?)")
+        else:
+            code = self.lib.orc_engine_create(max_arity, threads, C.byref(h))
+            if code:
+                raise GdlError(code, "orc_engine_create failed")
+        self.h = h
+        self.relations: list[Relation] = []
+
+    def close(self) -> None:
+        if self.h:
+            getattr(self.lib, self.pre + "engine_destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def threads(self) -> int:
+        return int(self.lib.orc_threads(self.h)) if self.kind == "oracle" else 0
+
+    def last_error(self) -> str:
+        msg = getattr(self.lib, self.pre + "last_error")(self.h)
+        return msg.decode() if msg else ""
+
+    def _check(self, code: int) -> None:
+        if code:
+            raise GdlError(code, self.last_error())
+
+    def _call(self, name, *args):
+        self._check(getattr(self.lib, self.pre + name)(self.h, *args))
+
+    # -- relations ---------------------------------------------------------
+    def relation(self, name: str, arity: int = 2, index_column_size: int = 1,
+                 dependent_column_size: int = 0, index_flag: bool = True,
+                 tmp_flag: bool = False) -> Relation:
+        rid = C.c_int32(-1)
+        self._call("relation_create", name.encode(), arity, index_column_size,
+                   dependent_column_size, int(index_flag), int(tmp_flag), C.byref(rid))
+        r = Relation(self, rid.value, name, arity)
+        self.relations.append(r)
+        return r
+
+    def load(self, rel: Relation, rows) -> None:
+        """load_relation: rows is an (n, arity) array of non-negative ints."""
+        if rows is None:
+            self._call("relation_load", rel.id, None, 0)
+            return
+        a = np.ascontiguousarray(np.asarray(rows), dtype=np.uint64)
+        if a.size == 0:
+            self._call("relation_load", rel.id, None, 0)
+            return
+        if a.ndim != 2 or a.shape[1] != rel.arity:
+            raise ValueError(f"rows must be (n, {rel.arity})")
+        self._call("relation_load", rel.id, a.ctypes.data_as(_PU64), a.shape[0])
+
+    def size(self, rel: Relation, version: int = FULL) -> int:
+        out = C.c_uint64(0)
+        self._call("relation_size", rel.id, version, C.byref(out))
+        return int(out.value)
+
+    def export(self, rel: Relation, version: int = FULL) -> np.ndarray:
+        n = self.size(rel, version)
+        buf = np.zeros((max(n, 1), rel.arity), dtype=np.uint64)
+        out = C.c_uint64(0)
+        self._call("relation_export", rel.id, version, buf.ctypes.data_as(_PU64), n,
+                   C.byref(out))
+        return buf[: int(out.value)]
+
+    def digest(self, rel: Relation, version: int = FULL) -> int:
+        out = C.c_uint64(0)
+        self._call("relation_digest", rel.id, version, C.byref(out))
+        return int(out.value)
+
+    def lie(self) -> Lie:
+        lid = C.c_int32(-1)
+        self._call("lie_create", C.byref(lid))
+        return Lie(self, lid.value)
+
+    def sync(self) -> None:
+        if self.kind == "gpu":
+            self._check(self.lib.gdl_engine_sync(self.h))
+
+
+def digest_rows(rows: np.ndarray) -> int:
+    """Host restatement of gdl_relation_digest over already-sorted rows."""
+    M = (1 << 64) - 1
+
+    def mix(x):
+        x = (x + 0x9E3779B97F4A7C15) & M
+        x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & M
+        x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & M
+        return x ^ (x >> 31)
+
+    s = 0
+    for i, row in enumerate(rows.tolist()):
+        h = mix(i)
+        for c in row:
+            h = mix(h ^ c)
+        s = (s + h) & M
+    return mix(s ^ len(rows))

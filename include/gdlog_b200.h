@@ -1,0 +1,192 @@
+/*
+ * gdlog_b200.h — C-ABI of the B200-native Datalog fixpoint engine.
+ *
+ * This is the drop-in boundary for the semi-naive fixpoint path of the
+ * slog GPU backend (harp-lab/gdlog-multinode).  Every entry point below
+ * replaces one piece of that project's C++ operator API; the citation on
+ * each names the reference interface (file:line, paths relative to the
+ * reference project root).  The C++ drop-in headers in include/gdlog/
+ * (Relation, load_relation, LIE, RelationalJoin/Copy/ACopy) are written on
+ * top of these calls.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, int32 ids.  No CUDA, no torch.
+ *  - Every call returns gdl_status; GDL_OK == 0.  The reference aborts the
+ *    process on any CUDA error (include/exception.cuh:9-18); here the
+ *    failure is returned and gdl_last_error() holds a one-line message.
+ *  - Tuples are rows of `arity` unsigned 64-bit columns (the reference's
+ *    column_type, include/tuple.cuh:5-10), row-major, on the host unless a
+ *    function says "device".  The engine stores arity-2 relations packed as
+ *    one 64-bit key (c0 << 32 | c1), which is order-preserving for column
+ *    values below 2^32; larger values are rejected with GDL_E_UNSUPPORTED.
+ *  - Hooks.  The reference passes __device__ function pointers
+ *    (tuple_generator_hook / tuple_copy_hook / tuple_predicate,
+ *    include/tuple.cuh:23-25).  Across a C-ABI they are described instead
+ *    as column selections: gen[j] names the source of output column j,
+ *    GDL_INNER(c) or GDL_OUTER(c) for a join, GDL_SRC(c) for a copy.
+ *    A predicate compares two columns of the generated tuple.
+ *  - One engine owns one CUDA stream; calls on one engine are not
+ *    thread-safe.  Device memory is owned by the engine.
+ */
+#ifndef GDLOG_B200_H
+#define GDLOG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gdl_status;
+#define GDL_OK 0
+#define GDL_E_INVALID 1     /* bad argument, id or state                 */
+#define GDL_E_CUDA 2        /* a CUDA runtime call failed                */
+#define GDL_E_NOMEM 3       /* device allocation failed                  */
+#define GDL_E_UNSUPPORTED 4 /* arity/values/hook shape not supported     */
+#define GDL_E_TIMEOUT 5     /* a bounded device-side wait gave up        */
+#define GDL_E_CAPACITY 6    /* a caller-provided buffer is too small     */
+
+/* RelationVersion (include/relation.cuh:13): same numeric order. */
+#define GDL_DELTA 0
+#define GDL_FULL 1
+#define GDL_NEWT 2
+
+/* Column-selection encoding of a hook's output column. */
+#define GDL_INNER(c) (c)
+#define GDL_OUTER(c) (16 + (c))
+#define GDL_SRC(c) (c)
+
+/* Predicate on the generated tuple t: t[a] <op> t[b]. */
+#define GDL_PRED_NONE 0
+#define GDL_PRED_NE 1
+#define GDL_PRED_EQ 2
+#define GDL_PRED_LT 3
+#define GDL_PRED_LE 4
+#define GDL_PRED_GT 5
+#define GDL_PRED_GE 6
+
+typedef struct gdl_engine gdl_engine;
+
+/* Library identification (no reference counterpart). */
+const char *gdl_version(void);
+const char *gdl_status_string(gdl_status s);
+/* Message of the last failing call on `e` (never NULL). */
+const char *gdl_last_error(const gdl_engine *e);
+
+/* Create an engine on CUDA device `device`.  `stream` is a cudaStream_t or
+ * NULL (the engine then creates its own non-blocking stream).  Replaces the
+ * implicit device/legacy-stream state that every reference call assumes
+ * (src/relation.cu, src/lie.cu: legacy stream + cudaDeviceSynchronize). */
+gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out);
+gdl_status gdl_engine_destroy(gdl_engine *e);
+
+/* Declare a relation.  Replaces `new Relation()` plus the field writes the
+ * drivers make before loading (include/relation.cuh:257-300; index_flag as
+ * set at test/tc.cu:108, tmp_flag as in load_relation's last argument,
+ * src/relation.cu:815-824). */
+gdl_status gdl_relation_create(gdl_engine *e, const char *name, int32_t arity,
+                               int32_t index_column_size,
+                               int32_t dependent_column_size,
+                               int32_t index_flag, int32_t tmp_flag,
+                               int32_t *out_rel);
+
+/* load_relation (src/relation.cu:815-838): copy `rows` host rows into FULL,
+ * sort, deduplicate, index.  rows == 0 (host_rows may be NULL) gives an
+ * empty relation, as at test/sg.cu:126-127.  Reloading replaces FULL and
+ * clears DELTA and NEWT. */
+gdl_status gdl_relation_load(gdl_engine *e, int32_t rel,
+                             const uint64_t *host_rows, uint64_t rows);
+
+/* Same as gdl_relation_load with the rows already in device memory
+ * (load_relation_container with gpu_data_flag, src/relation.cu:547-548). */
+gdl_status gdl_relation_load_device(gdl_engine *e, int32_t rel,
+                                    const uint64_t *device_rows, uint64_t rows);
+
+/* Container->tuple_counts of one version (GHashRelContainer::tuple_counts,
+ * include/relation.cuh:60); the drivers read full->tuple_counts after the
+ * fixpoint (test/tc.cu:138). */
+gdl_status gdl_relation_size(gdl_engine *e, int32_t rel, int32_t version,
+                             uint64_t *out_rows);
+
+/* Copy one version's tuples to the host, sorted lexicographically over all
+ * columns (the order of include/tuple.cuh:106-126).  Fails with
+ * GDL_E_CAPACITY (and sets *out_rows) if cap_rows is too small.  The
+ * reference has no export; its printers (src/print.cu) are debug only. */
+gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t version,
+                               uint64_t *host_rows, uint64_t cap_rows,
+                               uint64_t *out_rows);
+
+/* Order-sensitive 64-bit digest of one version's sorted tuples, computed on
+ * the device (no reference counterpart; used for bit-exact parity of large
+ * results without copying them to the host). */
+gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t version,
+                               uint64_t *out_digest);
+
+/* LIE(grid, block) (include/lie.cuh:11-65, src/lie.cu:13-24). */
+gdl_status gdl_lie_create(gdl_engine *e, int32_t *out_lie);
+/* LIE::add_relations (src/lie.cu:15-22). */
+gdl_status gdl_lie_add_relation(gdl_engine *e, int32_t lie, int32_t rel,
+                                int32_t static_flag);
+/* LIE::add_tmp_relation (src/lie.cu:24). */
+gdl_status gdl_lie_add_tmp_relation(gdl_engine *e, int32_t lie, int32_t rel);
+
+/* LIE::add_ra(RelationalJoin(...)) (include/relational_algebra.cuh:18-57,
+ * src/join.cu:12-270).  gen has gen_len == arity(output) entries. */
+gdl_status gdl_lie_add_join(gdl_engine *e, int32_t lie, int32_t inner,
+                            int32_t inner_version, int32_t outer,
+                            int32_t outer_version, int32_t output,
+                            const int32_t *gen, int32_t gen_len,
+                            int32_t pred_kind, int32_t pred_a, int32_t pred_b);
+
+/* LIE::add_ra(RelationalCopy(...)) (include/relational_algebra.cuh:63-82,
+ * src/copy.cu:12-95).  As in the reference the predicate is not applied
+ * (src/relation.cu:390-403), so none is taken. */
+gdl_status gdl_lie_add_copy(gdl_engine *e, int32_t lie, int32_t src,
+                            int32_t src_version, int32_t dest,
+                            const int32_t *gen, int32_t gen_len);
+
+/* LIE::add_ra(RelationalACopy(...)) (include/relational_algebra.cuh:90-109,
+ * src/acopy.cu:12-50). */
+gdl_status gdl_lie_add_acopy(gdl_engine *e, int32_t lie, int32_t src,
+                             int32_t dest, const int32_t *gen, int32_t gen_len);
+
+/* LIE::max_iteration / LIE::reload_full_flag (include/lie.cuh:29-30). */
+gdl_status gdl_lie_set_max_iteration(gdl_engine *e, int32_t lie,
+                                     int64_t max_iteration);
+gdl_status gdl_lie_set_reload_full(gdl_engine *e, int32_t lie, int32_t flag);
+
+/* LIE::fixpoint_loop (src/lie.cu:26-274).  *out_iterations receives the
+ * loop-pass count, including the final empty pass (the reference's
+ * iteration_counter after the loop). */
+gdl_status gdl_lie_fixpoint(gdl_engine *e, int32_t lie,
+                            uint64_t *out_iterations);
+
+/* Per-iteration log of the last fixpoint: one record per (iteration,
+ * update relation) with the three numbers the reference prints at
+ * src/lie.cu:193-197 (dedup new tuples, delta size, full count); dedup is
+ * UINT64_MAX for the "no new tuple added" branch (src/lie.cu:114-121).
+ * Records are 5 uint64: iteration, relation id, dedup, delta, full.
+ * Returns the number of records in *out_records (always), copies at most
+ * cap_records. */
+gdl_status gdl_lie_trace(gdl_engine *e, int32_t lie, uint64_t *records,
+                         uint64_t cap_records, uint64_t *out_records);
+
+/* Enable/disable the per-iteration trace (it costs one small device->host
+ * copy per iteration at the end of the fixpoint, not per iteration). */
+gdl_status gdl_lie_set_trace(gdl_engine *e, int32_t lie, int32_t flag);
+
+/* Timing and launch accounting of the last fixpoint on this engine:
+ * out[0] = fixpoint device milliseconds, out[1] = kernels launched,
+ * out[2] = iterations, out[3] = capacity retries, out[4] = graph launches.
+ * n_out is the number of doubles the caller provides. */
+gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out,
+                         int32_t n_out);
+
+/* Block until all work queued on the engine's stream has finished. */
+gdl_status gdl_engine_sync(gdl_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GDLOG_B200_H */

@@ -1,0 +1,210 @@
+"""GPU parity: the CUDA engine, called through its C-ABI, against the oracle.
+
+Bit-exact on every count: result sizes, loop-pass counts, the per-iteration
+(dedup, delta, full) log of src/lie.cu:193-197 and the order-sensitive
+digest of the sorted result tuples.  Small workloads are compared with the
+committed golden fixtures; the full-size ones (64x64 grid TC, R-MAT scale
+14 SG) with their golden digests and with size-independent properties
+(sortedness, uniqueness) of the exported rows.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import programs as P
+import workloads as W
+from gdlog_b200 import (DELTA, FULL, INNER, NEWT, OUTER, PRED_GT, PRED_LT, PRED_NE, SRC, Engine,
+                        GdlError)
+from test_oracle import GOLDEN, SMALL, build_workload
+
+pytestmark = pytest.mark.gpu
+
+
+def summarize(r):
+    return {
+        "sizes": {k: v.size() for k, v in r.relations.items()},
+        "digests": {k: hex(v.digest()) for k, v in r.relations.items()},
+        "iterations": r.iterations,
+        "traces": {k: lie.trace().tolist() for k, lie in r.lies.items()},
+    }
+
+
+def run_both(prog, *args):
+    with Engine("gpu") as g:
+        got = summarize(prog(g, *args, sync=g.sync))
+    with Engine("oracle") as o:
+        want = summarize(prog(o, *args))
+    return got, want
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_small_workloads_match_golden(name):
+    prog, args = build_workload(name)
+    with Engine("gpu") as g:
+        got = summarize(prog(g, *args, sync=g.sync))
+    want = GOLDEN["workloads"][name]
+    assert got["sizes"] == want["sizes"]
+    assert got["iterations"] == want["iterations"]
+    assert got["digests"] == want["digests"]
+    assert got["traces"] == want["traces"]
+
+
+def test_grid_tc_64x64():
+    want = GOLDEN["workloads"]["tc_grid_64x64"]
+    with Engine("gpu") as g:
+        r = P.tc(g, W.grid_edges(64, 64), sync=g.sync)
+        assert r.output.size() == 4322304
+        assert r.iterations["tc"] == 126
+        assert hex(r.output.digest()) == want["digests"]["path"]
+        assert r.lies["tc"].trace().tolist() == want["traces"]["tc"]
+
+
+def test_sg_rmat_scale14_full_size():
+    want = GOLDEN["workloads"]["sg_rmat_s14_40000_s14"]
+    with Engine("gpu") as g:
+        r = P.sg(g, W.rmat_edges(14, 40000, seed=14), sync=g.sync)
+        assert r.output.size() == want["sizes"]["sg"]
+        assert r.iterations == want["iterations"]
+        assert hex(r.output.digest()) == want["digests"]["sg"]
+        rows = r.output.rows()
+        key = (rows[:, 0] << np.uint64(32)) | rows[:, 1]
+        assert (np.diff(key.astype(np.int64)) > 0).all()  # sorted, unique
+        assert (rows[:, 0] != rows[:, 1]).all()
+
+
+def test_graph_and_stream_paths_agree():
+    e = W.layered_dag(20, 12, 7)
+    os.environ["GDLOG_NO_GRAPH"] = "1"
+    try:
+        with Engine("gpu") as g:
+            a = summarize(P.tc(g, e, sync=g.sync))
+    finally:
+        del os.environ["GDLOG_NO_GRAPH"]
+    with Engine("gpu") as g:
+        b = summarize(P.tc(g, e, sync=g.sync))
+    assert a == b
+
+
+def test_duplicate_and_unsorted_input():
+    e = W.layered_dag(10, 9, 3)
+    noisy = np.concatenate([e[::-1], e[: len(e) // 2]])
+    got, want = run_both(P.tc, noisy)
+    assert got == want
+
+
+def test_empty_relation():
+    e = np.zeros((0, 2), dtype=np.uint64)
+    got, want = run_both(P.tc, e)
+    assert got == want
+    assert got["sizes"]["path"] == 0
+
+
+def test_large_ids_hashed_index():
+    """Column values above the identity-index range use the hashed index."""
+    e = W.layered_dag(12, 10, 5) * np.uint64(40503) + np.uint64(3_000_000_000)
+    got, want = run_both(P.tc, e)
+    assert got == want
+
+
+def test_values_above_32_bits_rejected():
+    with Engine("gpu") as g:
+        r = g.relation("x")
+        with pytest.raises(GdlError):
+            g.load(r, np.array([[1 << 33, 1]], dtype=np.uint64))
+
+
+def test_max_iteration_cap():
+    e = W.grid_edges(12, 12)
+    for cap in (0, 1, 5):
+        res = []
+        for kind in ("gpu", "oracle"):
+            with Engine(kind) as eng:
+                path = eng.relation("path", index_flag=False)
+                edge = eng.relation("edge")
+                eng.load(path, e)
+                eng.load(edge, W.reverse(e))
+                lie = eng.lie()
+                lie.set_reload_full(False)
+                lie.add_relations(edge, True)
+                lie.add_relations(path, False)
+                lie.add_join(edge, FULL, path, DELTA, path, P.REORDER_PATH)
+                lie.max_iteration = cap
+                it = lie.fixpoint()
+                res.append((it, path.size(), path.digest(), lie.trace().tolist()))
+        assert res[0] == res[1], cap
+
+
+def empty_inner_program(eng):
+    """A join whose inner is empty zeroes the outer's count
+    (src/join.cu:38-45); a Copy from an empty source zeroes the dest NEWT
+    (src/copy.cu:24-27)."""
+    a = eng.relation("a")
+    b = eng.relation("b")
+    c = eng.relation("c")
+    eng.load(a, np.array([[1, 2], [2, 3], [3, 4]], dtype=np.uint64))
+    eng.load(b, None)
+    eng.load(c, np.array([[5, 6]], dtype=np.uint64))
+    lie = eng.lie()
+    lie.add_relations(b, True)
+    lie.add_relations(a, False)
+    lie.add_relations(c, False)
+    lie.add_join(b, FULL, a, DELTA, a, (INNER(1), OUTER(1)))
+    lie.add_copy(a, DELTA, c, (SRC(1), SRC(0)))
+    lie.add_join(a, FULL, a, DELTA, c, (OUTER(0), INNER(1)))
+    it = lie.fixpoint()
+    return it, a.size(), c.size(), c.digest(), lie.trace().tolist()
+
+
+def test_empty_inner_quirk():
+    with Engine("gpu") as g:
+        got = empty_inner_program(g)
+    with Engine("oracle") as o:
+        want = empty_inner_program(o)
+    assert got == want
+
+
+@pytest.mark.parametrize("kind", [PRED_NE, PRED_LT, PRED_GT])
+def test_predicates(kind):
+    e = W.rmat_edges(7, 300, seed=9)
+
+    def prog(eng, sync=None):
+        edge = eng.relation("edge")
+        out = eng.relation("out", index_flag=False)
+        eng.load(edge, e)
+        eng.load(out, None)
+        lie = eng.lie()
+        lie.add_relations(edge, True)
+        lie.add_relations(out, False)
+        lie.add_join(edge, FULL, edge, FULL, out, (INNER(1), OUTER(1)), pred=(kind, 0, 1))
+        it = lie.fixpoint()
+        return it, out.size(), out.digest()
+
+    with Engine("gpu") as g:
+        got = prog(g)
+    with Engine("oracle") as o:
+        want = prog(o)
+    assert got == want
+
+
+def test_relation_export_roundtrip():
+    rows = np.array([[7, 1], [0, 9], [7, 0], [0, 9]], dtype=np.uint64)
+    with Engine("gpu") as g:
+        r = g.relation("x")
+        g.load(r, rows)
+        assert r.size() == 3
+        assert r.rows().tolist() == [[0, 9], [7, 0], [7, 1]]
+
+
+def test_repeated_fixpoints_on_one_engine():
+    """Engine state (scratch buffers, index epochs, look-back generations)
+    carries over correctly from one program to the next."""
+    with Engine("gpu") as g:
+        outs = []
+        for seed in (1, 2, 3):
+            prog, args = build_workload(f"sg_rmat_s8_600_s{seed}")
+            outs.append(summarize(prog(g, *args, sync=g.sync)))
+    for seed, got in zip((1, 2, 3), outs):
+        want = GOLDEN["workloads"][f"sg_rmat_s8_600_s{seed}"]
+        assert got["sizes"] == want["sizes"] and got["digests"] == want["digests"]
