@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Datalog fixpoint engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sg_rmat_s14|tc_grid_64|cspa_v300]
+
+Default workload: same generation on an R-MAT graph of scale 14 (16,384
+nodes), 40,000 directed edges, a,b,c,d = .57,.19,.19,.05, seed 14, self loops
+and duplicates removed; the reference's SG program (test/sg.cu:93-191: an
+init LIE, then the recursive LIE with a tmp relation).  One step = both
+fixpoints of that program over one synthetic input.
+
+Metric: derived tuples per second = |sg| / fixpoint seconds.
+  value  device time of the fixpoint loops (CUDA events on the engine's
+         stream) with the input relations already loaded in HBM;
+  e2e    the same metric through the public API from host buffers:
+         host->device copy and load of the edges, both fixpoints, and the
+         device->host read of the result's size and digest, every step.
+The roofline object is the dominant kernel family of one extra profiled
+step (an event pair around every launch) against the measured HBM copy
+bandwidth.  cpu_baseline times the CPU oracle (a C++/OpenMP restatement of
+the reference's semi-naive loop) on all host cores.
+
+--impl reference runs that same CPU implementation as the reference arm
+(the reference's own CPU path, its Souffle programs, cannot be built
+offline; its CUDA engine is timed separately as a GPU baseline).
+Under torchrun every rank runs one replica of the workload (the single
+fixpoint does not shard); value sums the ranks' tuples over the slowest
+rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "gdlog-multinode_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+import programs as P  # noqa: E402
+import workloads as W  # noqa: E402
+
+WORKLOADS = {
+    "sg_rmat_s14": dict(
+        prog=P.sg, make=lambda: (W.rmat_edges(14, 40000, seed=14),),
+        desc="same generation, R-MAT scale 14 (16,384 nodes), 40,000 edges, "
+             "a,b,c,d=.57,.19,.19,.05, seed 14"),
+    "tc_grid_64": dict(
+        prog=P.tc, make=lambda: (W.grid_edges(64, 64),),
+        desc="transitive closure, 64x64 directed grid, 8,064 edges"),
+    "sg_rmat_s13": dict(
+        prog=P.sg, make=lambda: (W.rmat_edges(13, 20000, seed=14),),
+        desc="same generation, R-MAT scale 13 (8,192 nodes), 20,000 edges, "
+             "a,b,c,d=.57,.19,.19,.05, seed 14 (profiling case)"),
+    "cspa_v300": dict(
+        prog=P.cspa, make=lambda: W.cspa_facts(300, 600, 225, seed=3),
+        desc="CSPA, 300 variables, 600 assign, 225 dereference, Zipf(1.1) sources, seed 3"),
+}
+
+
+def derived(result) -> int:
+    return sum(r.size() for r in result.relations.values())
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def oracle_run(wl: dict, inputs, threads: int = 0):
+    """One run of the workload on the CPU oracle: (fixpoint seconds, tuples)."""
+    from gdlog_b200 import Engine
+    with Engine("oracle", threads=threads) as eng:
+        r = wl["prog"](eng, *inputs)
+        secs = sum(lie.stats()["ms"] for lie in r.lies.values()) / 1e3
+        return secs, derived(r), eng.threads
+
+
+def traffic_for(kind: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch from the committed ncu summary of this kernel
+    family, scaled by algorithmic bytes (capture of a smaller case)."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    rec = json.load(open(p)).get(kind)
+    if not rec or not rec.get("alg_bytes"):
+        return None
+    return rec["dram_bytes"] / rec["alg_bytes"] * alg_bytes_per_launch
+
+
+def reference_gpu(workload: str):
+    """Fixpoint seconds of the reference CUDA engine on this workload, as
+    recorded by tests/golden/make_ref_gpu.py on a B200."""
+    key = {"sg_rmat_s14": "sg_rmat_s14_40000_s14", "tc_grid_64": "tc_grid_64x64",
+           "cspa_v300": "cspa_v300_s3"}.get(workload)
+    p = os.path.join(REPO, "tests", "golden", "ref_gpu.json")
+    if not os.path.exists(p):
+        return None
+    rec = json.load(open(p)).get(key)
+    if not rec or "seconds" not in rec:
+        return None
+    t = sum(rec["sizes"].values())
+    return {"seconds": rec["seconds"], "value": t / rec["seconds"], "unit": "tuples/s",
+            "source": "reference CUDA engine built from its own sources, same input, B200"}
+
+
+def run_ours(a) -> None:
+    import torch
+    from gdlog_b200 import DeviceRows, Engine
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    wl = WORKLOADS[a.workload]
+    inputs = wl["make"]()
+    stream = torch.cuda.Stream(device=dev)
+    eng = Engine("gpu", device=local, stream=stream.cuda_stream)
+    dev_inputs = [DeviceRows(torch.from_numpy(x.astype(np.int64)).to(dev)) for x in inputs]
+    pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in inputs]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def device_step():
+        eng.clear()
+        with torch.cuda.stream(stream):
+            flush.fill_(1)  # L2 flush between steps (256 MB > 126 MB L2)
+        r = wl["prog"](eng, *dev_inputs)
+        st = [lie.stats() for lie in r.lies.values()]
+        return sum(s["ms"] for s in st), derived(r), sum(s["kernels"] for s in st)
+
+    n_out = [0]
+
+    def e2e_step():
+        eng.clear()
+        r = wl["prog"](eng, *pinned)
+        out = [(rel.size(), rel.digest()) for rel in r.relations.values()]
+        n_out[0] = len(out)
+        return sum(n for n, _ in out)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+    if a.single:
+        ms, t, k = device_step()
+        print(json.dumps({"single_step_ms": ms, "tuples": t, "launches": k}), flush=True)
+        eng.close()
+        return
+    for _ in range(a.warmup):
+        device_step()
+    e2e_step()
+    barrier()
+    ms_total, tuples, kernels = 0.0, 0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(a.steps):
+            ms, t, k = device_step()
+            ms_total += ms
+            tuples += t
+            kernels += k
+        barrier()
+        # e2e: public API from pinned host buffers, events on the engine stream
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2e_tuples = 0
+        e0.record(stream)
+        for _ in range(a.steps):
+            e2e_tuples += e2e_step()
+        e1.record(stream)
+        barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    # profiled step: an event pair around every launch
+    eng.profile_reset()
+    eng.set_profile(True)
+    device_step()
+    eng.set_profile(False)
+    prof = eng.profile()
+    eng.close()
+
+    vals = torch.tensor([ms_total, float(tuples), e2e_ms, float(e2e_tuples)], dtype=torch.float64,
+                        device=dev)
+    if dist:
+        mx = vals.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = vals.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_total, e2e_ms = mx[0].item(), mx[2].item()
+        tuples, e2e_tuples = sm[1].item(), sm[3].item()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = measured_peaks()
+    kind, rec = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    per_launch_ms = rec["ms"] / max(rec["launches"], 1)
+    per_launch_bytes = rec["bytes"] / max(rec["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else 0.0
+    tr = traffic_for(kind, per_launch_bytes)
+    line = {
+        "metric": "derived tuples/s (SG fixpoint)" if a.workload == "sg_rmat_s14"
+        else "derived tuples/s", "value": tuples / (ms_total / 1e3), "unit": "tuples/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "program": wl["prog"].__name__,
+                   "tuples_per_step": tuples / a.steps / world,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "flushed between steps (256 MB write); relations exceed L2"},
+        "e2e": {"value": e2e_tuples / (e2e_ms / 1e3), "unit": "tuples/s",
+                "h2d_bytes_per_step": int(sum(x.nbytes for x in pinned)),
+                "d2h_bytes_per_step": 16 * n_out[0]},
+        "gpu_launches": int(kernels),
+        "roofline": {"bound": "hbm", "kernel": kind, "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": tr,
+                     "alg_bytes_per_launch": per_launch_bytes,
+                     "ms_per_launch": per_launch_ms, "launches": rec["launches"],
+                     "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4),
+                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] else None}
+                    for k, v in prof.items() if v["launches"]},
+        "clocks": clocks.summary(),
+    }
+    ref = reference_gpu(a.workload)
+    if ref:
+        line["reference_gpu"] = ref
+    if world == 1 and not a.no_cpu_baseline:
+        secs, t, threads = oracle_run(wl, inputs)
+        line["cpu_baseline"] = {"value": t / secs, "unit": "tuples/s", "cores": threads,
+                                "kind": "port",
+                                "sample": "one full run of the same workload on the CPU oracle"}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(a) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    wl = WORKLOADS[a.workload]
+    inputs = wl["make"]()
+    secs0, _, _ = oracle_run(wl, inputs)  # one warm-up run (CPU caches, page faults)
+    budget = 240.0
+    steps = max(1, min(a.steps, int(budget // max(secs0, 1e-3))))
+    total, tuples, threads = 0.0, 0, 0
+    for _ in range(steps):
+        s, t, threads = oracle_run(wl, inputs)
+        total += s
+        tuples += t
+    v = tuples / total
+    print(json.dumps({
+        "impl": "reference", "metric": "derived tuples/s (SG fixpoint)"
+        if a.workload == "sg_rmat_s14" else "derived tuples/s",
+        "value": v, "unit": "tuples/s", "n_gpus": world, "steps": a.steps,
+        "steps_timed": steps, "warmup": a.warmup, "warmup_timed_out": max(a.warmup - 1, 0),
+        "ms_per_step": total / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "program": wl["prog"].__name__,
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full run(s) of the workload, after one warm-up run"},
+        "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sg_rmat_s14", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single", action="store_true",
+                    help="run one device step and exit (for profiler captures)")
+    a = ap.parse_args()
+    if a.warmup < 3 and a.impl == "ours":
+        a.warmup = 3
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

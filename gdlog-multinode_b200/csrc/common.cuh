@@ -84,7 +84,27 @@ struct Ctl {
   u64 trace_rows;    // capacity of the trace buffer in iterations
   unsigned long long cond_handle;  // cudaGraphConditionalHandle (while node)
   u64 need[3 * kMaxRels + 4];      // capacities needed after an overflow
+  u64 prof[16];                    // algorithmic bytes moved, per ProfKind
 };
+
+// Kernel families for the per-kernel accounting.  Every kernel adds the
+// algorithmic bytes of its launch (what the operation must read and write,
+// not what this implementation happens to move) to Ctl::prof[kind].
+enum ProfKind {
+  kPSortHist = 0,  // k_sort_hist: 8n (16n when the whole sort is one tile)
+  kPSortPass,      // k_sort_pass: 16n per digit pass
+  kPMerge,         // k_merge_diff: 8(|NEWT|+|FULL|) read + 8(|U|+|D|) written
+  kPIndex,         // k_index_build: 8n read + 16 per run inserted
+  kPJoinCount,     // k_join_count: 8|outer| read + 16|outer| probe
+  kPJoinMat,       // k_join_mat[_pred]: 16 per output + 24 per matched outer row
+  kPCopy,          // k_copy: 16 per tuple
+  kPControl,       // k_begin / k_commit: 0
+  kPKinds
+};
+
+__device__ __forceinline__ void prof_add(Ctl *c, int kind, u64 bytes) {
+  if (bytes) atomicAdd(&c->prof[kind], bytes);
+}
 
 enum NeedSlot { kNeedNewt = 0, kNeedFull = 1, kNeedDelta = 2 };
 __host__ __device__ inline int need_index(int rel, int kind) { return 3 * rel + kind; }

@@ -58,6 +58,16 @@ int bits_for(u64 v) {
   return b;
 }
 
+// Launch accounting of one enqueue: kernels per ProfKind.
+struct Counts {
+  int total = 0;
+  int kind[kPKinds] = {};
+  void add(int k) {
+    total++;
+    kind[k]++;
+  }
+};
+
 struct OpHost {
   int kind;  // 0 join, 1 copy, 2 acopy
   int inner = -1, inner_ver = GDL_FULL, outer = -1, outer_ver = GDL_DELTA, out = -1;
@@ -79,7 +89,7 @@ struct LieHost {
   cudaGraphExec_t gexec = nullptr;
   unsigned long long cond_handle = 0;
   bool graph_dirty = true;
-  int kernels_per_iter = 0;
+  Counts per_iter;  // launches of one enqueued iteration
 };
 
 struct RelHost {
@@ -121,7 +131,7 @@ struct gdl_engine {
   u32 *crow_start = nullptr, *crow_len = nullptr;
   u64 crow_cap = 0;
   Lb lb_cnt{}, lb_nz{}, lb_merge{};
-  u64 lb_join_tiles = 0, lb_merge_tiles = 0;
+  u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
   LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
   u64 *d_u64 = nullptr;       // [4] small device scalars
@@ -129,6 +139,19 @@ struct gdl_engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   u64 kernels_launched = 0;
   bool broken = false;  // a bounded wait gave up or a bounds check fired
+  // Per-kernel accounting of fixpoint loops (gdl_engine_profile).  With
+  // `profile` set, loops run launch by launch with an event pair around
+  // every kernel instead of from the captured graph.
+  bool profile = false;
+  double prof_ms[kPKinds] = {};
+  u64 prof_launches[kPKinds] = {};
+  u64 prof_bytes[kPKinds] = {};
+  std::vector<cudaEvent_t> ev_pool;
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
 };
 
 namespace {
@@ -234,6 +257,53 @@ int grid_for(gdl_engine *e, u64 work, u64 per_block, int per_sm) {
 
 int sort_passes(const gdl_engine *e) { return std::max(1, (2 * e->kbits + 7) / 8); }
 
+cudaEvent_t take_event(gdl_engine *e) {
+  cudaEvent_t ev = nullptr;
+  if (!e->ev_pool.empty()) {
+    ev = e->ev_pool.back();
+    e->ev_pool.pop_back();
+  } else if (cudaEventCreate(&ev) != cudaSuccess) {
+    ev = nullptr;
+  }
+  return ev;
+}
+
+// Event pair around one launch when profiling (no-op otherwise).
+cudaEvent_t prof_begin(gdl_engine *e) {
+  if (!e->profile) return nullptr;
+  cudaEvent_t a = take_event(e);
+  if (a) cudaEventRecord(a, e->s);
+  return a;
+}
+void prof_end(gdl_engine *e, int kind, cudaEvent_t a) {
+  if (!a) return;
+  cudaEvent_t b = take_event(e);
+  if (!b) {
+    e->ev_pool.push_back(a);
+    return;
+  }
+  cudaEventRecord(b, e->s);
+  e->pending.push_back({kind, a, b});
+}
+// After a stream synchronize: fold the recorded pairs into prof_ms.
+void prof_collect(gdl_engine *e) {
+  for (auto &p : e->pending) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) e->prof_ms[p.kind] += ms;
+    e->ev_pool.push_back(p.a);
+    e->ev_pool.push_back(p.b);
+  }
+  e->pending.clear();
+}
+
+#define PLAUNCH(cnt, kind, ...)                \
+  do {                                         \
+    cudaEvent_t _pe = prof_begin(e);           \
+    __VA_ARGS__;                               \
+    prof_end(e, (kind), _pe);                  \
+    (cnt)->add(kind);                          \
+  } while (0)
+
 // ---------------------------------------------------------------------------
 // Scratch sizing
 // ---------------------------------------------------------------------------
@@ -294,9 +364,8 @@ gdl_status ensure_scratch(gdl_engine *e) {
     TRY(dalloc(e, (void **)&e->crow_len, c * sizeof(u32)));
     e->crow_cap = c;
   }
-  TRY(ensure_lb(e, e->lb_cnt, e->lb_join_tiles, e->crow_cap / kJoinTile + 2));
-  u64 jt = e->lb_join_tiles;
-  TRY(ensure_lb(e, e->lb_nz, jt, e->lb_join_tiles));
+  TRY(ensure_lb(e, e->lb_cnt, e->lb_cnt_tiles, e->crow_cap / kJoinTile + 2));
+  TRY(ensure_lb(e, e->lb_nz, e->lb_nz_tiles, e->crow_cap / kJoinTile + 2));
   TRY(ensure_lb(e, e->lb_merge, e->lb_merge_tiles, (max_full + max_newt) / kMergeTile + 2));
   return GDL_OK;
 }
@@ -319,7 +388,7 @@ gdl_status reset_ctl(gdl_engine *e) {
 // ---------------------------------------------------------------------------
 // Kernel launchers
 // ---------------------------------------------------------------------------
-void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, int *kcount) {
+void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *kc) {
   SortArgs a;
   a.keys = d_keys;
   a.buf0 = buf0;
@@ -334,9 +403,9 @@ void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, int *kco
   a.ctl = e->d_ctl;
   int gh = grid_for(e, cap, (u64)kSortTile * 4, 2);
   int gp = grid_for(e, cap, kSortTile, 4);
-  k_sort_hist<<<gh, kSortBlock, kSortSmemBytes, e->s>>>(a);
-  for (int p = 0; p < a.passes; p++) k_sort_pass<<<gp, kSortBlock, kSortSmemBytes, e->s>>>(a, p);
-  *kcount += 1 + a.passes;
+  PLAUNCH(kc, kPSortHist, k_sort_hist<<<gh, kSortBlock, kSortSmemBytes, e->s>>>(a));
+  for (int p = 0; p < a.passes; p++)
+    PLAUNCH(kc, kPSortPass, k_sort_pass<<<gp, kSortBlock, kSortSmemBytes, e->s>>>(a, p));
 }
 
 u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e->sort_buf : buf0; }
@@ -371,7 +440,7 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     r.newt.n = n;
     TRY(push(e));
     TRY(reset_ctl(e));
-    int kc = 0;
+    Counts kc;
     launch_sort(e, &e->d_rels[rel].newt, r.newt.ptr, r.newt.cap, &kc);
     MergeArgs m;
     m.newt = &e->d_rels[rel].newt;
@@ -419,11 +488,10 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   return p;
 }
 
-void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, int *kc) {
+void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
-  k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl);
-  (*kc)++;
+  PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (op.kind == 0) {
@@ -464,15 +532,17 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, int *kc) {
       a.out_rel = op.out;
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
-      k_join_count<<<grid_for(e, outer_cap, kJoinTile, 4), kJoinBlock, 0, s>>>(a);
+      PLAUNCH(kc, kPJoinCount,
+              k_join_count<<<grid_for(e, outer_cap, kJoinTile, 4), kJoinBlock, 0, s>>>(a));
       JoinArgs b = a;
       b.rec = &e->recs[1];
       const u64 out_cap = e->h[op.out].newt.cap;
       if (op.pred.kind)
-        k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b);
+        PLAUNCH(kc, kPJoinMat,
+                k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b));
       else
-        k_join_mat<<<grid_for(e, out_cap, kMatTile, 8), kMatBlock, 0, s>>>(b);
-      *kc += 2;
+        PLAUNCH(kc, kPJoinMat,
+                k_join_mat<<<grid_for(e, out_cap, kMatTile, 8), kMatBlock, 0, s>>>(b));
     } else {
       CopyArgs c;
       const RelDev &sh = e->h[op.inner];
@@ -496,8 +566,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, int *kc) {
       c.dest_rel = op.out;
       c.replace = op.kind == 2;
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
-      k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c);
-      (*kc)++;
+      PLAUNCH(kc, kPCopy, k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c));
     }
   }
   for (int r : L.update) {
@@ -515,23 +584,22 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, int *kc) {
     m.ctl = e->d_ctl;
     m.rel = r;
     u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
-    k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m);
-    (*kc)++;
+    PLAUNCH(kc, kPMerge,
+            k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m));
     if (plan.full_idx[r]) {
       u64 c = std::max(rh.full.cap, rh.full_next.cap);
-      k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
-          &R[r].full_next, &R[r].full_idx_next, &R[r].delta_next, e->d_ctl);
-      (*kc)++;
+      PLAUNCH(kc, kPIndex,
+              k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
+                  &R[r].full_next, &R[r].full_idx_next, &R[r].delta_next, e->d_ctl));
     }
     if (plan.delta_idx[r]) {
       u64 c = std::max(rh.delta.cap, rh.delta_next.cap);
-      k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
-          &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl);
-      (*kc)++;
+      PLAUNCH(kc, kPIndex,
+              k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
+                  &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl));
     }
   }
-  k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl);
-  (*kc)++;
+  PLAUNCH(kc, kPControl, k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
 }
 
 gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
@@ -561,7 +629,7 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   cudaGraph_t body = p.conditional.phGraph_out[0];
   CK(e, cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal));
-  int kc = 0;
+  Counts kc;
   enqueue_iteration(e, L, plan, &kc);
   cudaGraph_t captured = nullptr;
   r = cudaStreamEndCapture(e->s, &captured);
@@ -573,7 +641,7 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   cudaGraphDestroy(g);
   if (r != cudaSuccess) return fail(e, GDL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(r));
   L.cond_handle = (unsigned long long)h;
-  L.kernels_per_iter = kc;
+  L.per_iter = kc;
   L.graph_dirty = false;
   return GDL_OK;
 }
@@ -656,6 +724,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
                   e->rels[op.out].name.c_str());
   }
   const Plan plan = make_plan(e, L);
+  // The timed span is the whole call, as the reference's drivers time the
+  // whole fixpoint_loop (test/tc.cu:120-140): setup, loop and finish.
+  CK(e, cudaEventRecord(e->ev0, e->s));
   TRY(reset_ctl(e));
   TRY(pull(e));
   // Setup (src/lie.cu:49-59): DELTA := the first |FULL| rows of FULL's raw
@@ -697,7 +768,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       u64 *keys = h.newt.ptr;
       h.newt.n = n;
       TRY(push(e));
-      int kc = 0;
+      Counts kc;
       launch_sort(e, &e->d_rels[r].newt, keys, h.newt.cap, &kc);
       TRY(pull(e));
       CK(e, cudaMemcpyAsync(h.delta.ptr, sorted_location(e, keys), n * sizeof(u64),
@@ -743,8 +814,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   L.graph_launches = 0;
   L.kernels = 0;
   L.graph_dirty = true;
-  const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr;
-  CK(e, cudaEventRecord(e->ev0, e->s));
+  const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr && !e->profile;
   u64 batch = 4;
   while (true) {
     c.pause = 0;
@@ -755,22 +825,33 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     c.cond_handle = use_graph ? L.cond_handle : 0;
     CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
     const u64 it0 = c.iteration;
+    u64 enqueued = 0;
     if (use_graph) {
       CK(e, cudaGraphLaunch(L.gexec, e->s));
       L.graph_launches++;
     } else {
-      for (u64 k = 0; k < std::min<u64>(batch, trace_rows); k++) {
-        int kc = 0;
+      // Profiling enqueues one iteration at a time, so that no launch of an
+      // iteration past the fixpoint enters the per-kernel times.
+      const u64 nb = e->profile ? 1 : std::min<u64>(batch, trace_rows);
+      for (u64 k = 0; k < nb; k++) {
+        Counts kc;
         enqueue_iteration(e, L, plan, &kc);
-        L.kernels_per_iter = kc;
+        L.per_iter = kc;
+        enqueued++;
       }
       CK(e, cudaGetLastError());
     }
     CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
     CK(e, cudaStreamSynchronize(e->s));
+    prof_collect(e);
     c = *e->h_ctl;
     const u64 ran = c.iteration - it0;
-    L.kernels += (ran + (c.overflow ? 1 : 0)) * (u64)L.kernels_per_iter;
+    // In a graph, the body runs once per committed iteration plus once for
+    // an iteration that overflowed; on the stream, every enqueued
+    // iteration launches (those past the fixpoint return at once).
+    const u64 bodies = use_graph ? ran + (c.overflow ? 1 : 0) : enqueued;
+    L.kernels += bodies * (u64)L.per_iter.total;
+    for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += bodies * (u64)L.per_iter.kind[k];
     if (L.trace_on && ran) {
       std::vector<u64> rows(ran * L.update.size() * 3);
       CK(e, cudaMemcpyAsync(rows.data(), ld.trace, rows.size() * sizeof(u64),
@@ -806,6 +887,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   L.ms = ms;
   L.iterations = c.iteration;
   e->kernels_launched += L.kernels;
+  for (int k = 0; k < kPKinds; k++) e->prof_bytes[k] += c.prof[k];
   // Finish (src/lie.cu:217-260).
   TRY(pull(e));
   for (int r : L.update) {
@@ -904,16 +986,16 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
   return GDL_OK;
 }
 
-gdl_status gdl_engine_destroy(gdl_engine *e) {
-  if (!e) return GDL_OK;
-  cudaSetDevice(e->device);
-  if (e->s) cudaStreamSynchronize(e->s);
+// Free every relation and LIE of the engine (device arrays return to the
+// stream-ordered pool, so a following program reuses them cheaply).
+static void release_program(gdl_engine *e) {
   for (size_t i = 0; i < e->rels.size(); i++) {
     RelDev &r = e->h[i];
-    for (DArr *a : {&r.full, &r.full_next, &r.delta, &r.delta_next, &r.newt}) cudaFree(a->ptr);
+    for (DArr *a : {&r.full, &r.full_next, &r.delta, &r.delta_next, &r.newt})
+      if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
-      cudaFree(x->slots);
-    if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFree(e->rels[i].raw);
+      if (x->slots) cudaFreeAsync(x->slots, e->s);
+    if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
   }
   for (LieHost &L : e->lies) {
     if (L.gexec) cudaGraphExecDestroy(L.gexec);
@@ -925,6 +1007,30 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
     }
     cudaFree(L.d_joinrec);
   }
+  cudaStreamSynchronize(e->s);
+  e->rels.clear();
+  e->h.clear();
+  e->lies.clear();
+  e->kbits = 1;
+  e->max_value = 0;
+}
+
+gdl_status gdl_engine_clear(gdl_engine *e) {
+  if (!e) return GDL_E_INVALID;
+  cudaSetDevice(e->device);
+  if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
+  CK(e, cudaStreamSynchronize(e->s));
+  release_program(e);
+  CK(e, cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_destroy(gdl_engine *e) {
+  if (!e) return GDL_OK;
+  cudaSetDevice(e->device);
+  if (e->s) cudaStreamSynchronize(e->s);
+  release_program(e);
   for (void *p : {(void *)e->sort_buf, (void *)e->sort_offsets, (void *)e->sort_counters,
                   (void *)e->sort_status, (void *)e->crow_off, (void *)e->crow_key,
                   (void *)e->crow_start, (void *)e->crow_len, (void *)e->lb_cnt.flag,
@@ -937,6 +1043,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  prof_collect(e);
+  for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
   if (e->own_stream && e->s) cudaStreamDestroy(e->s);
   delete e;
   return GDL_OK;
@@ -1276,6 +1384,42 @@ gdl_status gdl_lie_trace(gdl_engine *e, int32_t lie, uint64_t *rec, uint64_t cap
   uint64_t n = t.size() / 5;
   if (out_n) *out_n = n;
   if (rec) memcpy(rec, t.data(), std::min(n, cap) * 5 * sizeof(uint64_t));
+  return GDL_OK;
+}
+
+static const char *const kProfNames[kPKinds] = {"sort_hist", "sort_pass",  "merge_diff",
+                                                 "index_build", "join_count", "join_mat",
+                                                 "copy",      "control"};
+
+int32_t gdl_profile_kinds(void) { return kPKinds; }
+
+const char *gdl_profile_kind_name(int32_t kind) {
+  return kind >= 0 && kind < kPKinds ? kProfNames[kind] : "";
+}
+
+gdl_status gdl_engine_set_profile(gdl_engine *e, int32_t flag) {
+  if (!e) return GDL_E_INVALID;
+  e->profile = flag != 0;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_profile(gdl_engine *e, double *out, int32_t n_out) {
+  if (!e || (n_out && !out)) return GDL_E_INVALID;
+  for (int k = 0; k < kPKinds; k++) {
+    const double v[3] = {(double)e->prof_launches[k], e->prof_ms[k], (double)e->prof_bytes[k]};
+    for (int j = 0; j < 3; j++)
+      if (3 * k + j < n_out) out[3 * k + j] = v[j];
+  }
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_profile_reset(gdl_engine *e) {
+  if (!e) return GDL_E_INVALID;
+  for (int k = 0; k < kPKinds; k++) {
+    e->prof_ms[k] = 0;
+    e->prof_launches[k] = 0;
+    e->prof_bytes[k] = 0;
+  }
   return GDL_OK;
 }
 

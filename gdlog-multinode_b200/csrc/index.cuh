@@ -110,14 +110,20 @@ __global__ void __launch_bounds__(kIndexBlock) k_index_build(const DArr *arr, In
   const Index local = *ix;
   if (blockIdx.x == 0 && threadIdx.x == 0) ix->epoch = epoch;
   const u64 *keys = arr->ptr;
+  u32 inserted = 0;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
     u64 k = keys[i];
     if (i == 0 || key_c0(keys[i - 1]) != key_c0(k)) {
       u64 e = run_end(keys, n, i);
       index_insert(local, epoch, key_c0(k), (u32)i, (u32)(e - i), ctl);
+      inserted++;
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  if ((threadIdx.x & 31) == 0)
+    prof_add(ctl, kPIndex, 16ull * inserted + (blockIdx.x == 0 && threadIdx.x == 0 ? 8 * n : 0));
 }
 
 }  // namespace gdl

@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
       const u64 total = sm.cnt_base + tot_cnt, nc = sm.nz_base + tot_nz;
       a.op->total = total;
       a.op->nc = nc;
+      prof_add(a.ctl, kPJoinCount, 24 * n_outer);
       if (nc < a.crow_cap + 1) a.crow_off[nc] = total;
       // The overflow is recorded in the op and raised by the next kernel:
       // ctl flags must not change while blocks of this launch may still
@@ -276,6 +277,7 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat(JoinArgs a) {
   if (launch_rec_finish(a.rec) && threadIdx.x == 0) {
     a.op->base = base;
     a.out_newt->n = base + ((total + 1) & ~1ull);
+    prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
   }
 }
 
@@ -326,6 +328,7 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_pred(JoinArgs a) {
     }
     a.op->base = base;
     a.out_newt->n = base + ((total + 1) & ~1ull);
+    prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
   }
 }
 
@@ -380,6 +383,7 @@ __global__ void __launch_bounds__(kMatBlock) k_copy(CopyArgs c) {
   if (launch_rec_finish(c.rec) && threadIdx.x == 0) {
     c.dest->n = need;
     if (c.once_pending) *c.once_pending = 1;
+    prof_add(c.ctl, kPCopy, 16 * n);
   }
 }
 

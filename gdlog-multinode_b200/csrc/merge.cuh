@@ -167,6 +167,8 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_diff(MergeArgs m) {
           m.full_next->n = (prefix & 0xFFFFFFFFull) + tot_u;
           m.delta_next->n = (prefix >> 32) + tot_d;
           *m.c_newt_n = na;
+          prof_add(m.ctl, kPMerge,
+                   8 * (na + nb) + 8 * ((prefix & 0xFFFFFFFFull) + tot_u + (prefix >> 32) + tot_d));
         }
       }
     }

@@ -171,6 +171,8 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   if (ctl_stop(a.ctl)) return;
   const u64 n = a.keys->n;
   if (n == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    prof_add(a.ctl, kPSortHist, n <= (u64)kSortTile ? 16 * n : 8 * n);
   if (n <= (u64)kSortTile) {
     if (blockIdx.x == 0) small_sort(a, n, sm);
     return;
@@ -235,6 +237,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) 
   u64 *dst = (pass & 1) ? a.buf0 : a.buf1;
   u32 *status = a.status + (u64)pass * a.max_tiles * kRadix;
   const u32 *offs = a.offsets + pass * kRadix;
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(a.ctl, kPSortPass, 16 * n);
   while (true) {
     __syncthreads();
     if (threadIdx.x == 0) sm.tile = (long long)atomicAdd(&a.counters[pass], 1u);

@@ -111,6 +111,18 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_engine_sync.restype = _I
         lib.gdl_relation_load_device.argtypes = [_P, _I, _P, _U64]
         lib.gdl_relation_load_device.restype = _I
+        lib.gdl_engine_clear.argtypes = [_P]
+        lib.gdl_engine_clear.restype = _I
+        lib.gdl_profile_kinds.argtypes = []
+        lib.gdl_profile_kinds.restype = _I
+        lib.gdl_profile_kind_name.argtypes = [_I]
+        lib.gdl_profile_kind_name.restype = C.c_char_p
+        lib.gdl_engine_set_profile.argtypes = [_P, _I]
+        lib.gdl_engine_set_profile.restype = _I
+        lib.gdl_engine_profile.argtypes = [_P, C.POINTER(C.c_double), _I]
+        lib.gdl_engine_profile.restype = _I
+        lib.gdl_engine_profile_reset.argtypes = [_P]
+        lib.gdl_engine_profile_reset.restype = _I
     else:
         lib.orc_engine_create.argtypes = [_I, _I, C.POINTER(_P)]
         lib.orc_engine_create.restype = _I
@@ -118,12 +130,45 @@ def load_library(kind: str) -> C.CDLL:
         lib.orc_engine_destroy.restype = _I
         lib.orc_last_error.argtypes = [_P]
         lib.orc_last_error.restype = C.c_char_p
+        lib.orc_engine_clear.argtypes = [_P]
+        lib.orc_engine_clear.restype = _I
         lib.orc_threads.argtypes = [_P]
         lib.orc_threads.restype = _I
         lib.orc_lie_seconds.argtypes = [_P, _I, C.POINTER(C.c_double)]
         lib.orc_lie_seconds.restype = _I
     _libs[kind] = lib
     return lib
+
+
+class DeviceRows:
+    """Rows already in device memory: a contiguous (n, 2) tensor of 64-bit
+    integers (any object with data_ptr() and shape, e.g. a torch tensor).
+    Keeps the tensor alive; `reversed()` gives the column-swapped twin."""
+
+    def __init__(self, tensor, reversed_tensor=None):
+        if tensor.dim() != 2 or tensor.shape[1] != 2 or tensor.element_size() != 8:
+            raise ValueError("DeviceRows needs an (n, 2) tensor of 64-bit integers")
+        self.t = tensor.contiguous()
+        self._rev = reversed_tensor
+
+    @property
+    def ptr(self) -> int:
+        return self.t.data_ptr()
+
+    @property
+    def n(self) -> int:
+        return int(self.t.shape[0])
+
+    @property
+    def nbytes(self) -> int:
+        return self.n * 16
+
+    def reversed(self) -> "DeviceRows":
+        if self._rev is None:
+            self._rev = DeviceRows(self.t.flip(1).contiguous(), self.t)
+        elif not isinstance(self._rev, DeviceRows):
+            self._rev = DeviceRows(self._rev, self.t)
+        return self._rev
 
 
 class Relation:
@@ -283,7 +328,11 @@ class Engine:
         return r
 
     def load(self, rel: Relation, rows) -> None:
-        """load_relation: rows is an (n, arity) array of non-negative ints."""
+        """load_relation: rows is an (n, arity) array of non-negative ints,
+        or DeviceRows already in this engine's device memory."""
+        if isinstance(rows, DeviceRows):
+            self.load_device(rel, rows.ptr, rows.n)
+            return
         if rows is None:
             self._call("relation_load", rel.id, None, 0)
             return
@@ -321,6 +370,37 @@ class Engine:
     def sync(self) -> None:
         if self.kind == "gpu":
             self._check(self.lib.gdl_engine_sync(self.h))
+
+    def clear(self) -> None:
+        """Drop every relation and LIE; keep buffers and the memory pool."""
+        if self.kind == "gpu":
+            self._check(self.lib.gdl_engine_clear(self.h))
+        else:
+            self._check(self.lib.orc_engine_clear(self.h))
+        self.relations = []
+
+    def load_device(self, rel: Relation, ptr: int, n_rows: int) -> None:
+        """load_relation from rows already in device memory (n_rows x 2 u64)."""
+        self._check(self.lib.gdl_relation_load_device(self.h, rel.id, C.c_void_p(ptr), n_rows))
+
+    # -- per-kernel accounting (GPU only) -----------------------------------
+    def set_profile(self, flag: bool) -> None:
+        self._check(self.lib.gdl_engine_set_profile(self.h, int(bool(flag))))
+
+    def profile_reset(self) -> None:
+        self._check(self.lib.gdl_engine_profile_reset(self.h))
+
+    def profile(self) -> dict:
+        """{kernel family: {"launches", "ms", "bytes"}}."""
+        k = self.lib.gdl_profile_kinds()
+        out = (C.c_double * (3 * k))()
+        self._check(self.lib.gdl_engine_profile(self.h, out, 3 * k))
+        res = {}
+        for i in range(k):
+            name = self.lib.gdl_profile_kind_name(i).decode()
+            res[name] = {"launches": int(out[3 * i]), "ms": out[3 * i + 1],
+                         "bytes": int(out[3 * i + 2])}
+        return res
 
 
 def digest_rows(rows: np.ndarray) -> int:

@@ -141,9 +141,12 @@ def dag_batch(n_instances: int = 384, seed: int = 2024, l_range=(8, 128),
     return out
 
 
-def reverse(edges: np.ndarray) -> np.ndarray:
+def reverse(edges):
     """(u,v) -> (v,u), the host-side reversal the drivers do before loading
-    (test/tc.cu:97-101)."""
+    (test/tc.cu:97-101).  Device-resident rows (gdlog_b200.DeviceRows)
+    return their reversed twin, also on the device."""
+    if hasattr(edges, "reversed"):
+        return edges.reversed()
     return np.ascontiguousarray(edges[:, ::-1])
 
 

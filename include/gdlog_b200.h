@@ -80,6 +80,12 @@ const char *gdl_last_error(const gdl_engine *e);
 gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out);
 gdl_status gdl_engine_destroy(gdl_engine *e);
 
+/* Drop every relation and LIE of the engine, keeping its stream, scratch
+ * buffers and memory pool, so the next program starts without device
+ * allocation cost.  Relation and LIE ids restart at 0.  The reference has
+ * no counterpart (its drivers leak relations at exit, test/tc.cu:80-149). */
+gdl_status gdl_engine_clear(gdl_engine *e);
+
 /* Declare a relation.  Replaces `new Relation()` plus the field writes the
  * drivers make before loading (include/relation.cuh:257-300; index_flag as
  * set at test/tc.cu:108, tmp_flag as in load_relation's last argument,
@@ -184,6 +190,24 @@ gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out,
 
 /* Block until all work queued on the engine's stream has finished. */
 gdl_status gdl_engine_sync(gdl_engine *e);
+
+/* Per-kernel accounting of the fixpoint loops run on this engine (the
+ * reference threads a float detail_time[] through RelationalJoin and
+ * accumulates phase times in LIE::fixpoint_loop, include/
+ * relational_algebra.cuh:43-44, src/lie.cu:28-45; this replaces it).
+ * Kernels are grouped in gdl_profile_kinds() families named by
+ * gdl_profile_kind_name().  gdl_engine_profile writes, per family k,
+ * out[3k] = launches, out[3k+1] = device milliseconds (measured only while
+ * profiling is on: loops then run launch by launch with a CUDA event pair
+ * around each kernel instead of from the captured graph), out[3k+2] =
+ * algorithmic bytes (what the operation must read and write; counted by
+ * the kernels themselves, always on).  Totals accumulate until
+ * gdl_engine_profile_reset. */
+int32_t gdl_profile_kinds(void);
+const char *gdl_profile_kind_name(int32_t kind);
+gdl_status gdl_engine_set_profile(gdl_engine *e, int32_t flag);
+gdl_status gdl_engine_profile(gdl_engine *e, double *out, int32_t n_out);
+gdl_status gdl_engine_profile_reset(gdl_engine *e);
 
 #ifdef __cplusplus
 }

@@ -466,22 +466,38 @@ struct Engine final : EngineBase {
 
 struct orc_engine {
   std::unique_ptr<EngineBase> impl;
+  int32_t max_arity = 2;
 };
+
+static EngineBase *make_impl(int32_t max_arity) {
+  switch (max_arity) {
+    case 1:
+    case 2: return new Engine<2>;
+    case 3: return new Engine<3>;
+    case 4: return new Engine<4>;
+    default: return nullptr;
+  }
+}
 
 extern "C" {
 
 int32_t orc_engine_create(int32_t max_arity, int32_t threads, orc_engine **out) {
   if (!out) return E_INVALID;
+  EngineBase *impl = make_impl(max_arity);
+  if (!impl) return E_UNSUPPORTED;
   auto *e = new orc_engine;
-  switch (max_arity) {
-    case 1:
-    case 2: e->impl.reset(new Engine<2>); break;
-    case 3: e->impl.reset(new Engine<3>); break;
-    case 4: e->impl.reset(new Engine<4>); break;
-    default: delete e; return E_UNSUPPORTED;
-  }
+  e->impl.reset(impl);
+  e->max_arity = max_arity;
   e->impl->threads = threads > 0 ? threads : omp_get_max_threads();
   *out = e;
+  return OK;
+}
+
+int32_t orc_engine_clear(orc_engine *e) {
+  if (!e) return E_INVALID;
+  const int32_t threads = e->impl->threads;
+  e->impl.reset(make_impl(e->max_arity));
+  e->impl->threads = threads;
   return OK;
 }
 

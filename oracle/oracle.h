@@ -29,6 +29,8 @@ typedef struct orc_engine orc_engine;
  * threads to use (<= 0: all available). */
 int32_t orc_engine_create(int32_t max_arity, int32_t threads, orc_engine **out);
 int32_t orc_engine_destroy(orc_engine *e);
+/* Drop every relation and LIE (mirrors gdl_engine_clear). */
+int32_t orc_engine_clear(orc_engine *e);
 const char *orc_last_error(const orc_engine *e);
 int32_t orc_threads(const orc_engine *e);
 

@@ -202,3 +202,23 @@ def test_workload_shapes():
     assert ((dag[:, 1] // 7) == (dag[:, 0] // 7) + 1).all()
     batch = W.dag_batch(16)
     assert all(8 <= L <= 128 and 16 <= Wd <= 256 for L, Wd, _ in batch)
+
+
+def test_reference_cuda_build_agrees_with_oracle():
+    """The reference's own CUDA engine (compiled unmodified from its
+    sources, run on a B200 by tests/golden/make_ref_gpu.py) gives the same
+    sizes, loop-pass counts and digests of the sorted result as the
+    oracle's golden fixtures."""
+    path = os.path.join(HERE, "golden", "ref_gpu.json")
+    ref = json.load(open(path))
+    checked = 0
+    for name, rec in ref.items():
+        if "error" in rec or name not in GOLDEN["workloads"]:
+            continue
+        want = GOLDEN["workloads"][name]
+        assert rec["sizes"] == want["sizes"], name
+        assert rec["iterations"] == want["iterations"], name
+        assert rec["digests"] == want["digests"], name
+        assert rec["sorted"], name
+        checked += 1
+    assert checked >= 4
