@@ -201,12 +201,16 @@ def run_ours(a) -> None:
     pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in inputs]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    host = {"setup_ms": 0.0, "grow_ms": 0.0, "graph_ms": 0.0, "retries": 0}
+
     def device_step():
         eng.clear()
         with torch.cuda.stream(stream):
             flush.fill_(1)  # L2 flush between steps (256 MB > 126 MB L2)
         r = wl["prog"](eng, *dev_inputs)
         st = [lie.stats() for lie in r.lies.values()]
+        for key in host:
+            host[key] += sum(s[key] for s in st)
         return sum(s["ms"] for s in st), derived(r), sum(s["kernels"] for s in st)
 
     n_out = [0]
@@ -233,6 +237,8 @@ def run_ours(a) -> None:
     e2e_step()
     barrier()
     ms_total, tuples, kernels = 0.0, 0, 0
+    for key in host:
+        host[key] = 0
     with ClockSampler(local) as clocks:
         for _ in range(a.steps):
             ms, t, k = device_step()
@@ -249,6 +255,7 @@ def run_ours(a) -> None:
         e1.record(stream)
         barrier()
     e2e_ms = e0.elapsed_time(e1)
+    host_per_step = {k: v / a.steps for k, v in host.items()}
     # profiled step: an event pair around every launch
     eng.profile_reset()
     eng.set_profile(True)
@@ -299,6 +306,7 @@ def run_ours(a) -> None:
                         "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] else None}
                     for k, v in prof.items() if v["launches"]},
         "clocks": clocks.summary(),
+        "host_ms_per_step": host_per_step,
     }
     ref = reference_gpu(a.workload)
     if ref:

@@ -32,6 +32,7 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -47,6 +48,9 @@ constexpr int kIdentityMaxBits = 22;
 constexpr u64 kMaxRows = (1ull << 30) - 4096;  // sort status keeps 30 bits
 
 u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
+double host_ms_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
 u64 next_pow2(u64 x) {
   u64 p = 1;
   while (p < x) p <<= 1;
@@ -86,6 +90,9 @@ struct LieHost {
   std::vector<uint64_t> trace;   // 5 words per record
   double ms = 0;
   u64 kernels = 0, iterations = 0, retries = 0, graph_launches = 0;
+  // host wall milliseconds of the last fixpoint: setup, capacity growth
+  // (including re-runs), graph capture + instantiation
+  double setup_ms = 0, grow_ms = 0, graph_ms = 0;
   cudaGraphExec_t gexec = nullptr;
   unsigned long long cond_handle = 0;
   bool graph_dirty = true;
@@ -131,6 +138,7 @@ struct gdl_engine {
   u32 *crow_start = nullptr, *crow_len = nullptr;
   u64 crow_cap = 0;
   Lb lb_cnt{}, lb_nz{}, lb_merge{};
+  u64 *merge_parts = nullptr;  // [lb_merge_tiles + 1]
   u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
   LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
@@ -366,7 +374,12 @@ gdl_status ensure_scratch(gdl_engine *e) {
   }
   TRY(ensure_lb(e, e->lb_cnt, e->lb_cnt_tiles, e->crow_cap / kJoinTile + 2));
   TRY(ensure_lb(e, e->lb_nz, e->lb_nz_tiles, e->crow_cap / kJoinTile + 2));
+  const u64 had = e->lb_merge_tiles;
   TRY(ensure_lb(e, e->lb_merge, e->lb_merge_tiles, (max_full + max_newt) / kMergeTile + 2));
+  if (!e->merge_parts || had != e->lb_merge_tiles) {
+    dfree(e, e->merge_parts);
+    TRY(dalloc(e, (void **)&e->merge_parts, (e->lb_merge_tiles + 1) * sizeof(u64)));
+  }
   return GDL_OK;
 }
 
@@ -452,8 +465,11 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     m.c_newt_n = &e->d_rels[rel].c_newt_n;
     m.rec = &e->recs[2];
     m.lb = e->lb_merge;
+    m.parts = e->merge_parts;
+    m.parts_cap = e->lb_merge_tiles + 1;
     m.ctl = e->d_ctl;
     m.rel = rel;
+    k_merge_partition<<<grid_for(e, n / kMergeTile + 2, 256, 8), 256, 0, e->s>>>(m);
     k_merge_diff<<<grid_for(e, n, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, e->s>>>(m);
     CK(e, cudaGetLastError());
     TRY(pull(e));
@@ -581,9 +597,13 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
     m.c_newt_n = &R[r].c_newt_n;
     m.rec = &e->recs[2];
     m.lb = e->lb_merge;
+    m.parts = e->merge_parts;
+    m.parts_cap = e->lb_merge_tiles + 1;
     m.ctl = e->d_ctl;
     m.rel = r;
     u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
+    PLAUNCH(kc, kPMerge,
+            k_merge_partition<<<grid_for(e, mcap / kMergeTile + 2, 256, 8), 256, 0, s>>>(m));
     PLAUNCH(kc, kPMerge,
             k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m));
     if (plan.full_idx[r]) {
@@ -727,6 +747,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   // The timed span is the whole call, as the reference's drivers time the
   // whole fixpoint_loop (test/tc.cu:120-140): setup, loop and finish.
   CK(e, cudaEventRecord(e->ev0, e->s));
+  const auto t_setup = std::chrono::steady_clock::now();
   TRY(reset_ctl(e));
   TRY(pull(e));
   // Setup (src/lie.cu:49-59): DELTA := the first |FULL| rows of FULL's raw
@@ -811,6 +832,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   c.trace_rows = trace_rows;
   L.trace.clear();
   L.retries = 0;
+  L.grow_ms = L.graph_ms = 0;
+  L.setup_ms = host_ms_since(t_setup);
   L.graph_launches = 0;
   L.kernels = 0;
   L.graph_dirty = true;
@@ -820,7 +843,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     c.pause = 0;
     c.stop_at = c.iteration + (use_graph ? std::min<u64>(trace_rows, 1u << 20) : batch);
     c.trace_base = c.iteration;
-    if (use_graph && L.graph_dirty) TRY(build_graph(e, L, plan));
+    if (use_graph && L.graph_dirty) {
+      const auto tg = std::chrono::steady_clock::now();
+      TRY(build_graph(e, L, plan));
+      L.graph_ms += host_ms_since(tg);
+    }
     c.cond_set = use_graph ? 1 : 0;
     c.cond_handle = use_graph ? L.cond_handle : 0;
     CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
@@ -870,7 +897,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
                   (unsigned long long)c.iteration, c.timeout, c.oob);
     }
     if (c.overflow) {
+      const auto tg = std::chrono::steady_clock::now();
       TRY(grow_after_overflow(e, c));
+      L.grow_ms += host_ms_since(tg);
       c.overflow = 0;
       memset(c.need, 0, sizeof c.need);
       L.retries++;
@@ -1036,7 +1065,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->crow_start, (void *)e->crow_len, (void *)e->lb_cnt.flag,
                   (void *)e->lb_cnt.agg, (void *)e->lb_cnt.inc, (void *)e->lb_nz.flag,
                   (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
-                  (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->recs,
+                  (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->merge_parts,
+                  (void *)e->recs,
                   (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
                   (void *)e->d_ctl})
     if (p) cudaFree(p);
@@ -1426,9 +1456,10 @@ gdl_status gdl_engine_profile_reset(gdl_engine *e) {
 gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out, int32_t n_out) {
   CHECK_LIE(e, lie);
   const LieHost &L = e->lies[lie];
-  double v[5] = {L.ms, (double)L.kernels, (double)L.iterations, (double)L.retries,
-                 (double)L.graph_launches};
-  for (int i = 0; i < n_out && i < 5; i++) out[i] = v[i];
+  double v[8] = {L.ms,      (double)L.kernels,        (double)L.iterations,
+                 (double)L.retries, (double)L.graph_launches, L.setup_ms,
+                 L.grow_ms, L.graph_ms};
+  for (int i = 0; i < n_out && i < 8; i++) out[i] = v[i];
   return GDL_OK;
 }
 

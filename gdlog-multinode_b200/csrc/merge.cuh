@@ -34,6 +34,8 @@ struct MergeArgs {
   u64 *c_newt_n;      // RelDev::c_newt_n of the relation
   LaunchRec *rec;
   Lb lb;
+  u64 *parts;     // [tiles + 1] A-split of every tile boundary (k_merge_partition)
+  u64 parts_cap;
   Ctl *ctl;
   int rel;
 };
@@ -49,6 +51,28 @@ __device__ __forceinline__ u64 merge_path(const u64 *A, u64 na, const u64 *B, u6
       hi = mid;
   }
   return lo;
+}
+
+__device__ __forceinline__ bool merge_fits(const MergeArgs &m, u64 na, u64 nb) {
+  return na + nb <= m.full_next->cap && na <= m.delta_next->cap;
+}
+
+// Split points of the merged sequence at every tile boundary, one thread
+// per boundary, so that no CTA of k_merge_diff waits on a serial search
+// through global memory.
+__global__ void __launch_bounds__(256) k_merge_partition(MergeArgs m) {
+  if (ctl_stop(m.ctl)) return;
+  const u64 na = m.newt->n, nb = m.full->n;
+  if (na == 0 || !merge_fits(m, na, nb)) return;  // k_merge_diff handles both
+  const u64 total = na + nb;
+  const u64 tiles = (total + kMergeTile - 1) / kMergeTile;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t <= tiles;
+       t += (u64)gridDim.x * blockDim.x) {
+    if (t < m.parts_cap)
+      m.parts[t] = merge_path(m.a, na, m.full->ptr, nb, min(t * (u64)kMergeTile, total));
+    else
+      atomicOr(&m.ctl->oob, 512u);
+  }
 }
 
 struct MergeSmem {
@@ -75,7 +99,7 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_diff(MergeArgs m) {
     }
     return;
   }
-  if (na + nb > m.full_next->cap || na > m.delta_next->cap) {
+  if (!merge_fits(m, na, nb)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       atomicMax(&m.ctl->need[need_index(m.rel, kNeedFull)], na + nb);
       atomicMax(&m.ctl->need[need_index(m.rel, kNeedDelta)], na);
@@ -96,8 +120,9 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_diff(MergeArgs m) {
     const u64 d0 = (u64)tile * kMergeTile;
     const u64 d1 = min(d0 + kMergeTile, total);
     if (threadIdx.x == 0) {
-      u64 i0 = merge_path(A, na, B, nb, d0);
-      u64 i1 = merge_path(A, na, B, nb, d1);
+      const bool ok = (u64)tile + 1 < m.parts_cap;
+      u64 i0 = ok ? m.parts[tile] : merge_path(A, na, B, nb, d0);
+      u64 i1 = ok ? m.parts[tile + 1] : merge_path(A, na, B, nb, d1);
       sm.a0 = i0;
       sm.a1 = i1;
       sm.b0 = d0 - i0;

@@ -256,10 +256,11 @@ class Lie:
             s = C.c_double(0)
             self.eng._check(self.eng.lib.orc_lie_seconds(self.eng.h, self.id, C.byref(s)))
             return {"ms": s.value * 1e3}
-        out = (C.c_double * 5)()
-        self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 5))
+        out = (C.c_double * 8)()
+        self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 8))
         return {"ms": out[0], "kernels": int(out[1]), "iterations": int(out[2]),
-                "retries": int(out[3]), "graph_launches": int(out[4])}
+                "retries": int(out[3]), "graph_launches": int(out[4]), "setup_ms": out[5],
+                "grow_ms": out[6], "graph_ms": out[7]}
 
 
 class Engine:

@@ -183,7 +183,9 @@ gdl_status gdl_lie_set_trace(gdl_engine *e, int32_t lie, int32_t flag);
 
 /* Timing and launch accounting of the last fixpoint on this engine:
  * out[0] = fixpoint device milliseconds, out[1] = kernels launched,
- * out[2] = iterations, out[3] = capacity retries, out[4] = graph launches.
+ * out[2] = iterations, out[3] = capacity retries, out[4] = graph launches,
+ * out[5] = host setup ms, out[6] = host ms growing buffers after capacity
+ * overflows, out[7] = host ms capturing and instantiating graphs.
  * n_out is the number of doubles the caller provides. */
 gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out,
                          int32_t n_out);
