@@ -66,6 +66,11 @@ struct RelDev {
   u64 c_newt_n;  // NEWT count seen by the last merge step (0: empty branch)
   u32 sorted_in_scratch;
   u32 pad;
+  // Dense form (dense.cuh): FULL bitmap, its next version, NEWT bitmap.
+  u32 *bmF, *bmF_next, *bmG;
+  u64 f_count;     // |FULL'| when the FULL list is not rebuilt every iteration
+  u32 dense;       // the running LIE keeps this relation as bitmaps
+  u32 full_lazy;   // FULL's list is materialised only when the LIE ends
 };
 
 // Loop control of a running fixpoint (one per engine, device memory).
@@ -97,8 +102,9 @@ enum ProfKind {
   kPIndex,         // k_index_build: 8n read + 16 per run inserted
   kPJoinCount,     // k_join_count: 8|outer| read + 16|outer| probe
   kPJoinMat,       // k_join_mat[_pred]: 16 per output + 24 per matched outer row
-  kPCopy,          // k_copy: 16 per tuple
+  kPCopy,          // k_copy: 16 per tuple; dense copies 8 per source tuple
   kPControl,       // k_begin / k_commit: 0
+  kPBitmap,        // dense scans: bitmap words read/written + 8 per key listed
   kPKinds
 };
 

@@ -64,6 +64,8 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
     for (int i = 0; i < L->n_update; i++) {
       RelDev &r = rels[L->update[i]];
       u64 *tr = (L->trace && row < ctl->trace_rows) ? L->trace + (row * L->n_update + i) * 3 : 0;
+      // Dense form: the scan wrote FULL | NEWT into bmF_next (dense.cuh).
+      if (r.dense) dswap(r.bmF, r.bmF_next);
       if (r.c_newt_n == 0) {
         // src/lie.cu:114-121: no new tuple -> a fresh, empty DELTA.
         r.delta.n = 0;
@@ -80,8 +82,12 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
         r.delta_vis = 1;
         if (r.delta.n) {
           // flush_delta (src/relation.cu:405-521): FULL := FULL ∪ DELTA.
-          dswap(r.full, r.full_next);
-          dswap(r.full_idx, r.full_idx_next);
+          if (r.dense && r.full_lazy) {
+            r.full.n = r.f_count;  // the list is written when the LIE ends
+          } else {
+            dswap(r.full, r.full_next);
+            dswap(r.full_idx, r.full_idx_next);
+          }
           r.full_vis = 1;
           fixpoint = false;
         } else {

@@ -1,0 +1,431 @@
+// dense.cuh — bitmap form of relation versions over a small key domain.
+//
+// When every column value is below 2^dk with 2*dk <= 30, the whole key
+// domain of an arity-2 relation is 2^(2dk) bits (at most 128 MB), and a
+// version of the relation can be held as a bitmap whose bit v is the tuple
+// (v >> dk, v & (2^dk - 1)).  Bit order is the reference's tuple order
+// (include/tuple.cuh:106-126), so compacting a bitmap gives the sorted,
+// deduplicated tuple list directly.  This replaces, for such domains, the
+// sort -> unique -> set_difference -> merge sequence of the reference's
+// update step (src/lie.cu:122-185, src/relation.cu:405-521, src/join.cu:
+// 160-225):
+//   * joins and copies test-and-set bits of the output relation's NEWT
+//     bitmap G (atomicOr, aggregated per warp), so the raw join output --
+//     often tens of times larger than its distinct tuples -- is never
+//     written to memory;
+//   * one streaming pass over (G, F) per relation then yields DELTA =
+//     G & ~F and FULL' = F | G as sorted lists, the next FULL bitmap, and
+//     the run index of FULL' from per-row popcounts.
+// Each scan is two kernels: k_bm_count computes per-tile counts and their
+// exclusive prefixes (decoupled look-back) and checks the output
+// capacities; k_bm_write writes.  Nothing but idempotent bit-sets happens
+// before a capacity check, so an iteration that overflows can be re-run.
+#pragma once
+
+#include "common.cuh"
+#include "index.cuh"
+#include "join.cuh"
+
+namespace gdl {
+
+constexpr int kBmBlock = 256;
+constexpr int kBmWordsPerThread = 8;
+constexpr int kBmTileWords = kBmBlock * kBmWordsPerThread;  // 2048 words = 65536 keys
+constexpr int kDenseMaxDomainBits = 30;
+
+__device__ __forceinline__ u64 dense_vkey(u64 key, int dk) {
+  return ((u64)key_c0(key) << dk) | (u64)key_c1(key);
+}
+__device__ __forceinline__ u64 dense_key(u64 vkey, int dk) {
+  return make_key((u32)(vkey >> dk), (u32)(vkey & ((1ull << dk) - 1)));
+}
+// Bit sets are bounds-checked against the bitmap size: a key outside the
+// domain is dropped and recorded in Ctl::oob instead of being written.
+__device__ __forceinline__ void bm_set(u32 *bm, u64 words, u64 vkey, Ctl *ctl) {
+  if ((vkey >> 5) < words)
+    atomicOr(bm + (vkey >> 5), 1u << (vkey & 31));
+  else
+    atomicOr(&ctl->oob, 8192u);
+}
+
+// Expressions a scan can compact, over the word pair (g, f).
+enum BmExpr { kBmNone = 0, kBmDelta = 1, kBmUnion = 2 };
+__device__ __forceinline__ u32 bm_eval(int ex, u32 g, u32 f) {
+  return ex == kBmDelta ? (g & ~f) : ex == kBmUnion ? (f | g) : 0u;
+}
+
+struct BmScanRec {
+  u64 total_a, total_b;  // list sizes
+  u64 pop_g;             // popcount of g (accumulated, reset by k_bm_write)
+  u32 overflow;
+  u32 pad;
+};
+
+struct BmScanArgs {
+  const u32 *g;    // NEWT bitmap (may be null: all zero)
+  const u32 *f;    // FULL bitmap (may be null: all zero)
+  u32 *f_next;     // if set: receives f | g
+  // If set, g / f / f_next are this relation's bmG / bmF / bmF_next, read
+  // from the device descriptor when the kernel starts: k_commit swaps bmF
+  // and bmF_next on the device, so pointers captured in a graph would go
+  // stale.
+  const RelDev *rd;
+  u64 words;       // bitmap words (multiple of kBmTileWords or smaller)
+  int dk;          // bits per column
+  int ex_a, ex_b;  // expressions for list a and list b
+  DArr *list_a;    // output lists (sorted keys); null when ex is kBmNone
+  DArr *list_b;
+  Index *idx_b;    // if set: run index of list b (identity addressing)
+  u64 *count_b;    // if set: receives total_b (FULL count without a list)
+  u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
+  int need_a, need_b;  // need slots to raise on overflow (-1: none)
+  u64 *tile_prefix;    // [tiles] packed exclusive prefix (a << 32 | b)
+  u64 tiles_cap;
+  BmScanRec *rec;
+  LaunchRec *lrec;
+  Lb lb;
+  Ctl *ctl;
+};
+
+__device__ __forceinline__ u64 bm_tiles(u64 words) {
+  return (words + kBmTileWords - 1) / kBmTileWords;
+}
+
+// Pass 1: per-tile counts, exclusive prefixes by decoupled look-back, and
+// the capacity check (recorded in rec->overflow for k_bm_write to raise).
+__global__ void __launch_bounds__(kBmBlock) k_bm_count(BmScanArgs a) {
+  __shared__ u64 s_scan[kBmBlock / 32];
+  __shared__ long long s_tile;
+  if (ctl_stop(a.ctl)) return;
+  const u64 tiles = bm_tiles(a.words);
+  if (tiles > a.tiles_cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->oob, 1024u);
+    return;
+  }
+  if (a.rd) {
+    a.g = a.rd->bmG;
+    a.f = a.rd->bmF;
+    a.f_next = a.rd->bmF_next;
+  }
+  const u32 gen = a.lrec->gen;
+  u64 my_g = 0;
+  while (true) {
+    const long long tile = grab_tile(a.lrec, &s_tile);
+    if (tile >= (long long)tiles) break;
+    const u64 w0 = (u64)tile * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 ca = 0, cb = 0;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u64 w = w0 + i;
+      if (w < a.words) {
+        const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
+        ca += __popc(bm_eval(a.ex_a, g, f));
+        cb += __popc(bm_eval(a.ex_b, g, f));
+        my_g += __popc(g);
+      }
+    }
+    u64 tot;
+    block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, s_scan, &tot);
+    if (threadIdx.x < 32) {
+      u64 prefix = 0;
+      if (tile == 0) {
+        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, true, tot);
+      } else {
+        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, false, tot);
+        prefix = lb_warp_prefix(a.lb, tile, gen, a.ctl);
+        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, true, prefix + tot);
+      }
+      if (threadIdx.x == 0) {
+        a.tile_prefix[tile] = prefix;
+        if ((u64)tile == tiles - 1) {
+          const u64 ta = (prefix + tot) >> 32, tb = (prefix + tot) & 0xFFFFFFFFull;
+          a.rec->total_a = ta;
+          a.rec->total_b = tb;
+          bool over = false;
+          if (a.list_a && ta > a.list_a->cap) {
+            over = true;
+            if (a.need_a >= 0) atomicMax(&a.ctl->need[a.need_a], ta);
+          }
+          if (a.list_b && tb > a.list_b->cap) {
+            over = true;
+            if (a.need_b >= 0) atomicMax(&a.ctl->need[a.need_b], tb);
+          }
+          a.rec->overflow = over;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_g += __shfl_xor_sync(0xffffffffu, my_g, o);
+  if ((threadIdx.x & 31) == 0 && my_g) atomicAdd(&a.rec->pop_g, my_g);
+  launch_rec_finish(a.lrec);
+}
+
+// Pass 2: write list a, list b (+ its index) and f_next.
+struct BmWriteSmem {
+  u32 off_b[kBmTileWords + 1];  // exclusive offsets of list b per word
+  u64 scan_tmp[kBmBlock / 32];
+};
+
+__global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
+  __shared__ BmWriteSmem sm;
+  if (ctl_stop(a.ctl)) return;
+  if (a.rec->overflow) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.rec->pop_g = 0;
+      atomicExch(&a.ctl->overflow, 1u);
+    }
+    return;
+  }
+  const u64 tiles = bm_tiles(a.words);
+  if (tiles > a.tiles_cap) return;
+  if (a.rd) {
+    a.g = a.rd->bmG;
+    a.f = a.rd->bmF;
+    a.f_next = a.rd->bmF_next;
+  }
+  const int row_shift = a.dk - 5;  // words per row = 2^row_shift (dk >= 5)
+  const u32 epoch = (u32)(a.ctl->generation + 1);
+  const Index ix = a.idx_b ? *a.idx_b : Index{};
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.idx_b) a.idx_b->epoch = epoch;
+  u64 *la = a.list_a ? a.list_a->ptr : nullptr;
+  u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
+  const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const u64 prefix = a.tile_prefix[tile];
+    const u64 wt = tile * kBmTileWords;
+    const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
+    u32 ca = 0, cb = 0;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u64 w = w0 + i;
+      u32 g = 0, f = 0;
+      if (w < a.words) {
+        g = a.g ? a.g[w] : 0u;
+        f = a.f ? a.f[w] : 0u;
+        if (a.f_next) a.f_next[w] = f | g;
+      }
+      ea[i] = bm_eval(a.ex_a, g, f);
+      eb[i] = bm_eval(a.ex_b, g, f);
+      ca += __popc(ea[i]);
+      cb += __popc(eb[i]);
+    }
+    u64 tot;
+    const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
+    u64 pa = (prefix >> 32) + (ex >> 32);
+    u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
+    u32 ob = (u32)(ex & 0xFFFFFFFFull);
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u64 vbase = (w0 + i) << 5;
+      if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
+      ob += __popc(eb[i]);
+      u32 x = ea[i];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        if (pa < cap_a)
+          la[pa] = dense_key(vbase + b, a.dk);
+        else
+          atomicOr(&a.ctl->oob, 2048u);
+        pa++;
+      }
+      x = eb[i];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        if (pb < cap_b)
+          lb[pb] = dense_key(vbase + b, a.dk);
+        else
+          atomicOr(&a.ctl->oob, 4096u);
+        pb++;
+      }
+    }
+    if (a.idx_b) {
+      if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
+      __syncthreads();
+      // One slot per non-empty row of the tile: {c0, epoch, start, len}.
+      const u64 row_words = 1ull << row_shift;
+      const u64 rows = kBmTileWords >> row_shift;
+      for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
+        const u64 lw = r << row_shift;  // first word of the row in the tile
+        if (wt + lw >= a.words) break;
+        const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
+        if (len) {
+          const u32 c0 = (u32)((wt + lw) >> row_shift);
+          const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
+          index_insert(ix, epoch, c0, start, len, a.ctl);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
+    if (a.list_a) a.list_a->n = a.rec->total_a;
+    if (a.list_b) a.list_b->n = a.rec->total_b;
+    if (a.count_b) *a.count_b = a.rec->total_b;
+    if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
+    a.rec->pop_g = 0;
+    prof_add(a.ctl, kPBitmap,
+             a.words * 4 * ((a.g ? 2 : 0) + (a.f ? 2 : 0) + (a.f_next ? 1 : 0)) +
+                 8 * (a.rec->total_a + a.rec->total_b));
+  }
+}
+
+// Zero a bitmap.  With `only_if_empty`, only when *only_if_empty == 0 (the
+// copy of an empty source empties its destination NEWT, src/copy.cu:24-27).
+__global__ void __launch_bounds__(256) k_bm_clear(u32 *bm, u64 words, const DArr *only_if_empty,
+                                                  const u32 *vis, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  if (only_if_empty && eff_count(only_if_empty, vis) != 0) return;
+  uint4 *p = reinterpret_cast<uint4 *>(bm);
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < words / 4;
+       i += (u64)gridDim.x * blockDim.x)
+    p[i] = make_uint4(0, 0, 0, 0);
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, words * 4);
+}
+
+// Set the bits of a key list (FULL at the start of a LIE).
+__global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm, u64 words, int dk,
+                                                      Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u64 n = list->n;
+  const u64 *k = list->ptr;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    bm_set(bm, words, dense_vkey(k[i], dk), ctl);
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
+}
+
+// Warp-aggregated bit set: lanes whose words are equal and adjacent OR their
+// bits together and the last lane of each run issues one atomicOr.  Lanes
+// with word == ~0 set nothing.
+__device__ __forceinline__ void bm_set_warp(u32 *bm, u64 words, u64 word, u32 bits, Ctl *ctl) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 ob = __shfl_up_sync(0xffffffffu, bits, o);
+    const u64 ow = __shfl_up_sync(0xffffffffu, word, o);
+    if (lane >= o && ow == word) bits |= ob;
+  }
+  const u64 nw = __shfl_down_sync(0xffffffffu, word, 1);
+  const bool last = lane == 31 || nw != word;
+  if (last && word != ~0ull && bits) {
+    if (word < words)
+      atomicOr(bm + word, bits);
+    else
+      atomicOr(&ctl->oob, 8192u);
+  }
+}
+
+// RelationalJoin materialisation into the output's NEWT bitmap.  Balanced
+// over candidate positions exactly as k_join_mat; consecutive lanes take
+// consecutive positions, so the outputs of one outer row (one c0, ascending
+// c1) fall into few bitmap words and are set with few atomics.
+__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_bm, u64 out_words,
+                                                           int dk) {
+  __shared__ MatSmem sm;
+  if (ctl_stop(a.ctl)) return;
+  const u64 total = a.op->total;
+  const u64 nc = a.op->nc;
+  if (total == 0) return;
+  const u64 *inner = a.inner->ptr;
+  const u64 tiles = (total + kMatTile - 1) / kMatTile;
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const u64 p0 = tile * kMatTile;
+    const u64 p1 = min(p0 + kMatTile, total);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u64 lo = 0, hi = nc;
+      while (hi - lo > 1) {
+        u64 mid = (lo + hi) >> 1;
+        if (a.crow_off[mid] <= p0)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      sm.k0 = lo;
+      sm.nrec = (u32)min((u64)kMatTile, nc - lo);
+    }
+    __syncthreads();
+    const u64 k0 = sm.k0;
+    const u32 m = sm.nrec;
+    for (u32 i = threadIdx.x; i <= m; i += blockDim.x) {
+      sm.off[i] = a.crow_off[k0 + i];
+      if (i < m) {
+        sm.start[i] = a.crow_start[k0 + i];
+        sm.key[i] = a.crow_key[k0 + i];
+      }
+    }
+    __syncthreads();
+    for (u64 q = 0; q < (u64)kMatTile; q += blockDim.x) {
+      const u64 p = p0 + q + threadIdx.x;
+      u64 word = ~0ull;
+      u32 bits = 0;
+      if (p < p1) {
+        const u32 r = find_rec(sm.off, m, p);
+        const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+        if (pred_ok(a.pred, t)) {
+          const u64 v = dense_vkey(t, dk);
+          word = v >> 5;
+          bits = 1u << (v & 31);
+        }
+      }
+      bm_set_warp(out_bm, out_words, word, bits, a.ctl);
+    }
+  }
+  if (launch_rec_finish(a.rec) && threadIdx.x == 0)
+    prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
+}
+
+// RelationalCopy into the destination's NEWT bitmap (src/copy.cu:12-95).
+// An empty source empties the destination NEWT (src/copy.cu:24-27).
+__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, u32 *dest_bm, u64 dest_words,
+                                                 int dk) {
+  if (ctl_stop(c.ctl)) return;
+  if (c.once && *c.once) return;
+  const u64 n = eff_count(c.src, c.src_vis);
+  if (n == 0) {
+    uint4 *p = reinterpret_cast<uint4 *>(dest_bm);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < dest_words / 4;
+         i += (u64)gridDim.x * blockDim.x)
+      p[i] = make_uint4(0, 0, 0, 0);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c.once_pending) *c.once_pending = 1;
+    return;
+  }
+  const u64 *src = c.src->ptr;
+  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+    const u64 i = i0 + threadIdx.x;
+    u64 word = ~0ull;
+    u32 bits = 0;
+    if (i < n) {
+      const u64 v = dense_vkey(gen_join(c.sel, src[i], 0), dk);
+      word = v >> 5;
+      bits = 1u << (v & 31);
+    }
+    bm_set_warp(dest_bm, dest_words, word, bits, c.ctl);
+  }
+  if (launch_rec_finish(c.rec) && threadIdx.x == 0) {
+    if (c.once_pending) *c.once_pending = 1;
+    prof_add(c.ctl, kPCopy, 8 * n);
+  }
+}
+
+// RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT).  The
+// destination bitmap is cleared by a k_bm_clear launched just before.
+__global__ void __launch_bounds__(256) k_acopy_bm(const u32 *src_bm, u64 words, Sel2 sel,
+                                                  u32 *dest_bm, int dk, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < words;
+       w += (u64)gridDim.x * blockDim.x) {
+    u32 x = src_bm[w];
+    while (x) {
+      const int b = __ffs(x) - 1;
+      x &= x - 1;
+      bm_set(dest_bm, words, dense_vkey(gen_join(sel, dense_key((w << 5) + b, dk), 0), dk), ctl);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, words * 4);
+}
+
+}  // namespace gdl

@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "control.cuh"
+#include "dense.cuh"
 #include "index.cuh"
 #include "join.cuh"
 #include "merge.cuh"
@@ -97,6 +98,9 @@ struct LieHost {
   unsigned long long cond_handle = 0;
   bool graph_dirty = true;
   Counts per_iter;  // launches of one enqueued iteration
+  // Dense form of the running fixpoint (dense.cuh): bits per column, or 0.
+  bool dense = false;
+  int dk = 0;
 };
 
 struct RelHost {
@@ -110,6 +114,7 @@ struct RelHost {
   u64 raw_n = 0;
   bool raw_is_full = true;
   bool delta_sorted = true;
+  u64 bm_words = 0;  // size of this relation's bitmaps (dense form), words
 };
 
 }  // namespace
@@ -139,6 +144,17 @@ struct gdl_engine {
   u64 crow_cap = 0;
   Lb lb_cnt{}, lb_nz{}, lb_merge{};
   u64 *merge_parts = nullptr;  // [lb_merge_tiles + 1]
+  // Dense scans: tile prefixes, look-back state, the scan record.
+  u64 *bm_prefix = nullptr;
+  u64 bm_tiles = 0;
+  Lb lb_bm{};
+  u64 lb_bm_tiles = 0;
+  BmScanRec *bm_rec = nullptr;
+  // Largest 2*bits domain kept as bitmaps (GDLOG_DENSE_MAX_BITS), and the
+  // dedup path: 0 chosen by domain size, 1 always sort/merge, 2 always
+  // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
+  int dense_max_bits = kDenseMaxDomainBits;
+  int dedup_mode = 0;
   u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
   LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
@@ -383,6 +399,39 @@ gdl_status ensure_scratch(gdl_engine *e) {
   return GDL_OK;
 }
 
+// Bitmaps of one relation in dense form: NEWT always, FULL and its next
+// version for update relations.
+gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
+  RelHost &rh = e->rels[r];
+  RelDev &h = e->h[r];
+  if (rh.bm_words != words) {
+    for (u32 **p : {&h.bmF, &h.bmF_next, &h.bmG}) {
+      dfree(e, *p);
+      *p = nullptr;
+    }
+    rh.bm_words = words;
+  }
+  if (!h.bmG) TRY(dalloc(e, (void **)&h.bmG, words * 4));
+  if (with_full && !h.bmF) TRY(dalloc(e, (void **)&h.bmF, words * 4));
+  if (with_full && !h.bmF_next) TRY(dalloc(e, (void **)&h.bmF_next, words * 4));
+  return GDL_OK;
+}
+
+gdl_status ensure_dense_scratch(gdl_engine *e, u64 words) {
+  const u64 tiles = words / kBmTileWords + 2;
+  if (e->bm_tiles < tiles) {
+    dfree(e, e->bm_prefix);
+    TRY(dalloc(e, (void **)&e->bm_prefix, tiles * sizeof(u64)));
+    e->bm_tiles = tiles;
+  }
+  TRY(ensure_lb(e, e->lb_bm, e->lb_bm_tiles, tiles));
+  if (!e->bm_rec) {
+    TRY(dalloc(e, (void **)&e->bm_rec, sizeof(BmScanRec)));
+    CK(e, cudaMemsetAsync(e->bm_rec, 0, sizeof(BmScanRec), e->s));
+  }
+  return GDL_OK;
+}
+
 // Put the device control block in a runnable state (no stop flags, no
 // graph condition) keeping the build generation.
 gdl_status reset_ctl(gdl_engine *e) {
@@ -493,25 +542,78 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
 // ---------------------------------------------------------------------------
 struct Plan {
   std::vector<char> full_idx, delta_idx;  // per relation: index needed
+  std::vector<char> full_list;            // FULL read as a list by some op
+  std::vector<char> newt_list;            // NEWT read as a join outer
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
   Plan p;
-  p.full_idx.assign(e->rels.size(), 0);
-  p.delta_idx.assign(e->rels.size(), 0);
-  for (const OpHost &op : L.ops)
-    if (op.kind == 0) (op.inner_ver == GDL_DELTA ? p.delta_idx : p.full_idx)[op.inner] = 1;
+  const size_t n = e->rels.size();
+  p.full_idx.assign(n, 0);
+  p.delta_idx.assign(n, 0);
+  p.full_list.assign(n, 0);
+  p.newt_list.assign(n, 0);
+  for (const OpHost &op : L.ops) {
+    if (op.kind == 0) {
+      (op.inner_ver == GDL_DELTA ? p.delta_idx : p.full_idx)[op.inner] = 1;
+      if (op.inner_ver != GDL_DELTA) p.full_list[op.inner] = 1;
+      if (op.outer_ver == GDL_FULL) p.full_list[op.outer] = 1;
+      if (op.outer_ver == GDL_NEWT) p.newt_list[op.outer] = 1;
+    } else if (op.kind == 1 && op.inner_ver == GDL_FULL) {
+      p.full_list[op.inner] = 1;
+    }
+  }
   return p;
+}
+
+// Bitmap size, in 32-bit words, of one relation version in dense form.
+u64 dense_words(int dk) { return 1ull << (2 * dk - 5); }
+
+// One bitmap scan (dense.cuh): count pass, then write pass.
+void launch_scan(gdl_engine *e, BmScanArgs a, Counts *kc) {
+  a.tile_prefix = e->bm_prefix;
+  a.tiles_cap = e->bm_tiles;
+  a.rec = e->bm_rec;
+  a.lb = e->lb_bm;
+  a.ctl = e->d_ctl;
+  const u64 tiles = (a.words + kBmTileWords - 1) / kBmTileWords;
+  a.lrec = &e->recs[4];
+  PLAUNCH(kc, kPBitmap, k_bm_count<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
+  a.lrec = &e->recs[5];
+  PLAUNCH(kc, kPBitmap, k_bm_write<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
+}
+
+BmScanArgs scan_none(int dk) {
+  BmScanArgs a;
+  memset(&a, 0, sizeof a);
+  a.words = dense_words(dk);
+  a.dk = dk;
+  a.ex_a = a.ex_b = kBmNone;
+  a.need_a = a.need_b = -1;
+  return a;
 }
 
 void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
+  const bool dense = L.dense;
+  const int dk = L.dk;
+  const u64 words = dense ? dense_words(dk) : 0;
   PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
+  if (dense) {
+    // NEWT of every update and tmp relation starts empty.
+    for (int r : L.update)
+      PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+                                e->h[r].bmG, words, nullptr, nullptr, e->d_ctl));
+    for (int r : L.tmps)
+      PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+                                e->h[r].bmG, words, nullptr, nullptr, e->d_ctl));
+  }
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (op.kind == 0) {
       JoinArgs a;
+      memset(&a, 0, sizeof a);
       const RelDev &oh = e->h[op.outer];
       if (op.outer_ver == GDL_DELTA) {
         a.outer = &R[op.outer].delta;
@@ -522,6 +624,17 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       } else {
         a.outer = &R[op.outer].newt;
         a.outer_vis = nullptr;
+        if (dense && oh.bmG) {
+          // NEWT as a join outer: the sorted list of its bitmap.
+          BmScanArgs c = scan_none(dk);
+          c.g = oh.bmG;
+          c.ex_a = kBmUnion;
+          c.list_a = &R[op.outer].newt;
+          c.need_a = need_index(op.outer, kNeedNewt);
+          launch_scan(e, c, kc);
+          a.outer_bm = oh.bmG;
+          a.outer_bm_words = words;
+        }
       }
       if (op.inner_ver == GDL_DELTA) {
         a.inner = &R[op.inner].delta;
@@ -546,6 +659,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       a.crow_cap = e->crow_cap;
       a.ctl = e->d_ctl;
       a.out_rel = op.out;
+      a.dense = dense;
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
       PLAUNCH(kc, kPJoinCount,
@@ -553,7 +667,10 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       JoinArgs b = a;
       b.rec = &e->recs[1];
       const u64 out_cap = e->h[op.out].newt.cap;
-      if (op.pred.kind)
+      if (dense)
+        PLAUNCH(kc, kPJoinMat,
+                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, e->h[op.out].bmG, words, dk));
+      else if (op.pred.kind)
         PLAUNCH(kc, kPJoinMat,
                 k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b));
       else
@@ -561,6 +678,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
                 k_join_mat<<<grid_for(e, out_cap, kMatTile, 8), kMatBlock, 0, s>>>(b));
     } else {
       CopyArgs c;
+      memset(&c, 0, sizeof c);
       const RelDev &sh = e->h[op.inner];
       if (op.kind == 2) {
         c.src = &R[op.inner].newt;
@@ -582,35 +700,69 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       c.dest_rel = op.out;
       c.replace = op.kind == 2;
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
-      PLAUNCH(kc, kPCopy, k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c));
+      if (dense && op.kind == 2) {
+        // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
+        u32 *dbm = e->h[op.out].bmG;
+        PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+                                  dbm, words, nullptr, nullptr, e->d_ctl));
+        if (sh.bmG)  // a source without a NEWT bitmap (static) has an empty NEWT
+          PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, words, 256, 8), 256, 0, s>>>(
+                                  sh.bmG, words, op.sel, dbm, dk, e->d_ctl));
+      } else if (dense) {
+        PLAUNCH(kc, kPCopy, k_copy_bm<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
+                                c, e->h[op.out].bmG, words, dk));
+      } else {
+        PLAUNCH(kc, kPCopy,
+                k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c));
+      }
     }
   }
   for (int r : L.update) {
     const RelDev &rh = e->h[r];
-    launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
-    MergeArgs m;
-    m.newt = &R[r].newt;
-    m.a = sorted_location(e, rh.newt.ptr);
-    m.full = &R[r].full;
-    m.full_next = &R[r].full_next;
-    m.delta_next = &R[r].delta_next;
-    m.c_newt_n = &R[r].c_newt_n;
-    m.rec = &e->recs[2];
-    m.lb = e->lb_merge;
-    m.parts = e->merge_parts;
-    m.parts_cap = e->lb_merge_tiles + 1;
-    m.ctl = e->d_ctl;
-    m.rel = r;
-    u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
-    PLAUNCH(kc, kPMerge,
-            k_merge_partition<<<grid_for(e, mcap / kMergeTile + 2, 256, 8), 256, 0, s>>>(m));
-    PLAUNCH(kc, kPMerge,
-            k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m));
-    if (plan.full_idx[r]) {
-      u64 c = std::max(rh.full.cap, rh.full_next.cap);
-      PLAUNCH(kc, kPIndex,
-              k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
-                  &R[r].full_next, &R[r].full_idx_next, &R[r].delta_next, e->d_ctl));
+    if (dense) {
+      // DELTA = NEWT \ FULL, FULL' = FULL | NEWT, both sorted; FULL's list
+      // and index only when some op reads them during the loop.
+      BmScanArgs a = scan_none(dk);
+      a.rd = &R[r];  // bitmaps as the device sees them (k_commit swaps F)
+      a.ex_a = kBmDelta;
+      a.list_a = &R[r].delta_next;
+      a.need_a = need_index(r, kNeedDelta);
+      a.ex_b = kBmUnion;
+      if (plan.full_list[r]) {
+        a.list_b = &R[r].full_next;
+        a.need_b = need_index(r, kNeedFull);
+        if (plan.full_idx[r]) a.idx_b = &R[r].full_idx_next;
+      } else {
+        a.count_b = &R[r].f_count;
+      }
+      a.pop_g_out = &R[r].c_newt_n;
+      launch_scan(e, a, kc);
+    } else {
+      launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
+      MergeArgs m;
+      m.newt = &R[r].newt;
+      m.a = sorted_location(e, rh.newt.ptr);
+      m.full = &R[r].full;
+      m.full_next = &R[r].full_next;
+      m.delta_next = &R[r].delta_next;
+      m.c_newt_n = &R[r].c_newt_n;
+      m.rec = &e->recs[2];
+      m.lb = e->lb_merge;
+      m.parts = e->merge_parts;
+      m.parts_cap = e->lb_merge_tiles + 1;
+      m.ctl = e->d_ctl;
+      m.rel = r;
+      u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
+      PLAUNCH(kc, kPMerge,
+              k_merge_partition<<<grid_for(e, mcap / kMergeTile + 2, 256, 8), 256, 0, s>>>(m));
+      PLAUNCH(kc, kPMerge,
+              k_merge_diff<<<grid_for(e, mcap, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m));
+      if (plan.full_idx[r]) {
+        u64 c = std::max(rh.full.cap, rh.full_next.cap);
+        PLAUNCH(kc, kPIndex,
+                k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
+                    &R[r].full_next, &R[r].full_idx_next, &R[r].delta_next, e->d_ctl));
+      }
     }
     if (plan.delta_idx[r]) {
       u64 c = std::max(rh.delta.cap, rh.delta_next.cap);
@@ -776,8 +928,42 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, kMinCap), false));
     h.newt.n = 0;
   }
+  // Dense form (dense.cuh) when the key domain is small enough.
+  {
+    const int dk = std::max(e->kbits, 5);
+    L.dense = e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits;
+    L.dk = L.dense ? dk : 0;
+  }
+  for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+  if (L.dense) {
+    const u64 words = dense_words(L.dk);
+    for (int r : L.update) {
+      TRY(ensure_bitmaps(e, r, words, true));
+      e->h[r].dense = 1;
+      e->h[r].full_lazy = !plan.full_list[r];
+    }
+    for (int r : L.tmps) {
+      TRY(ensure_bitmaps(e, r, words, false));
+      e->h[r].dense = 1;
+    }
+    TRY(ensure_dense_scratch(e, words));
+  }
   TRY(ensure_scratch(e));
   TRY(push(e));
+  if (L.dense) {
+    // FULL's bitmap from its list; NEWT bitmaps empty.
+    const u64 words = dense_words(L.dk);
+    for (int r : L.update) {
+      const RelDev &h = e->h[r];
+      CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
+      CK(e, cudaMemsetAsync(h.bmG, 0, words * 4, e->s));
+      if (h.full.n)
+        k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
+            &e->d_rels[r].full, h.bmF, words, L.dk, e->d_ctl);
+    }
+    for (int r : L.tmps) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+    CK(e, cudaGetLastError());
+  }
   // An unsorted DELTA (raw load order) used as a join inner is sorted and
   // deduplicated first (the reference's index walk is undefined there).
   for (int r : L.update) {
@@ -909,6 +1095,36 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (c.done) break;
     batch = std::min<u64>(batch * 2, 64);
   }
+  if (L.dense) {
+    // FULL lists that were not kept during the loop are written from the
+    // FULL bitmaps, sorted (bit order is tuple order).
+    const u64 kept_iteration = c.iteration;
+    TRY(reset_ctl(e));  // clear done/pause so that the scans below run
+    TRY(pull(e));
+    bool any = false;
+    for (int r : L.update)
+      if (e->h[r].full_lazy) {
+        TRY(ensure_arr(e, e->h[r].full, e->h[r].full.n, false));
+        any = true;
+      }
+    if (any) {
+      TRY(push(e));
+      Counts kc;
+      for (int r : L.update) {
+        if (!e->h[r].full_lazy) continue;
+        BmScanArgs a = scan_none(L.dk);
+        a.f = e->h[r].bmF;
+        a.ex_b = kBmUnion;
+        a.list_b = &e->d_rels[r].full;
+        launch_scan(e, a, &kc);
+      }
+      CK(e, cudaGetLastError());
+      TRY(pull(e));
+    }
+    for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+    TRY(push(e));
+    c.iteration = kept_iteration;
+  }
   CK(e, cudaEventRecord(e->ev1, e->s));
   CK(e, cudaEventSynchronize(e->ev1));
   float ms = 0;
@@ -987,6 +1203,12 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
     e->err = cudaGetErrorString(r);
     return true;
   };
+  if (const char *m = getenv("GDLOG_DEDUP")) {
+    if (!strcmp(m, "sort")) e->dedup_mode = 1;
+    if (!strcmp(m, "dense")) e->dedup_mode = 2;
+  }
+  if (const char *b = getenv("GDLOG_DENSE_MAX_BITS"))
+    e->dense_max_bits = std::min(atoi(b), kDenseMaxDomainBits);
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
     u64 thr = ~0ull;
@@ -1024,6 +1246,8 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
+    for (u32 *bm : {r.bmF, r.bmF_next, r.bmG})
+      if (bm) cudaFreeAsync(bm, e->s);
     if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
   }
   for (LieHost &L : e->lies) {
@@ -1066,6 +1290,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->lb_cnt.agg, (void *)e->lb_cnt.inc, (void *)e->lb_nz.flag,
                   (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
                   (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->merge_parts,
+                  (void *)e->bm_prefix, (void *)e->lb_bm.flag, (void *)e->lb_bm.agg,
+                  (void *)e->lb_bm.inc, (void *)e->bm_rec,
                   (void *)e->recs,
                   (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
                   (void *)e->d_ctl})
@@ -1417,14 +1643,23 @@ gdl_status gdl_lie_trace(gdl_engine *e, int32_t lie, uint64_t *rec, uint64_t cap
   return GDL_OK;
 }
 
-static const char *const kProfNames[kPKinds] = {"sort_hist", "sort_pass",  "merge_diff",
-                                                 "index_build", "join_count", "join_mat",
-                                                 "copy",      "control"};
+static const char *const kProfNames[kPKinds] = {
+    "sort_hist", "sort_pass", "merge_diff", "index_build", "join_count",
+    "join_mat",  "copy",      "control",    "bitmap_scan"};
 
 int32_t gdl_profile_kinds(void) { return kPKinds; }
 
 const char *gdl_profile_kind_name(int32_t kind) {
   return kind >= 0 && kind < kPKinds ? kProfNames[kind] : "";
+}
+
+gdl_status gdl_engine_set_dedup(gdl_engine *e, int32_t mode, int32_t dense_max_bits) {
+  if (!e || mode < GDL_DEDUP_AUTO || mode > GDL_DEDUP_DENSE) return GDL_E_INVALID;
+  if (dense_max_bits < 0 || dense_max_bits > kDenseMaxDomainBits)
+    return fail(e, GDL_E_INVALID, "dense_max_bits must be in [0, %d]", kDenseMaxDomainBits);
+  e->dedup_mode = mode;
+  if (dense_max_bits) e->dense_max_bits = dense_max_bits;
+  return GDL_OK;
 }
 
 gdl_status gdl_engine_set_profile(gdl_engine *e, int32_t flag) {

@@ -60,6 +60,13 @@ struct JoinArgs {
   u64 crow_cap;
   Ctl *ctl;
   int out_rel;
+  // Dense output (dense.cuh): count every candidate (the predicate is
+  // applied when bits are set) and skip the NEWT capacity check.  A NEWT
+  // outer emptied by an empty inner (src/join.cu:38-45) also has its bitmap
+  // cleared.
+  int dense;
+  u32 *outer_bm;
+  u64 outer_bm_words;
 };
 
 __device__ __forceinline__ u64 eff_count(const DArr *a, const u32 *vis) {
@@ -92,6 +99,12 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
           ((DArr *)a.outer)->n = 0;
       }
     }
+    if (n_outer != 0 && !a.outer_vis && a.outer_bm) {
+      uint4 *p = reinterpret_cast<uint4 *>(a.outer_bm);
+      for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.outer_bm_words / 4;
+           i += (u64)gridDim.x * blockDim.x)
+        p[i] = make_uint4(0, 0, 0, 0);
+    }
     return;
   }
   const u64 tiles = (n_outer + kJoinTile - 1) / kJoinTile;
@@ -121,7 +134,7 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
         u32 l = index_probe(ix, key_c0(row), &s);
         start[k] = s;
         len[k] = l;
-        if (a.pred.kind == 0) {
+        if (a.pred.kind == 0 || a.dense) {
           cnt[k] = l;
         } else {
           u64 c = 0;
@@ -183,8 +196,8 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
       // ctl flags must not change while blocks of this launch may still
       // test them on entry.
       const u64 need = a.out_newt->n + ((total + 1) & ~1ull);
-      a.op->overflow = need > a.out_newt->cap;
-      if (need > a.out_newt->cap) atomicMax(&a.ctl->need[need_index(a.out_rel, kNeedNewt)], need);
+      a.op->overflow = !a.dense && need > a.out_newt->cap;
+      if (a.op->overflow) atomicMax(&a.ctl->need[need_index(a.out_rel, kNeedNewt)], need);
     }
   }
   launch_rec_finish(a.rec);

@@ -111,6 +111,8 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_engine_sync.restype = _I
         lib.gdl_relation_load_device.argtypes = [_P, _I, _P, _U64]
         lib.gdl_relation_load_device.restype = _I
+        lib.gdl_engine_set_dedup.argtypes = [_P, _I, _I]
+        lib.gdl_engine_set_dedup.restype = _I
         lib.gdl_engine_clear.argtypes = [_P]
         lib.gdl_engine_clear.restype = _I
         lib.gdl_profile_kinds.argtypes = []
@@ -266,8 +268,10 @@ class Lie:
 class Engine:
     """One engine (GPU: one CUDA stream on one device; oracle: CPU threads)."""
 
+    DEDUP = {"auto": 0, "sort": 1, "dense": 2}
+
     def __init__(self, kind: str = "gpu", device: int = 0, threads: int = 0,
-                 max_arity: int = 2, stream: int | None = None):
+                 max_arity: int = 2, stream: int | None = None, dedup: str | None = None):
         if kind not in ("gpu", "oracle"):
             raise ValueError(kind)
         self.kind = kind
@@ -284,6 +288,8 @@ class Engine:
                 raise GdlError(code, "orc_engine_create failed")
         self.h = h
         self.relations: list[Relation] = []
+        if kind == "gpu" and dedup is not None:
+            self._check(self.lib.gdl_engine_set_dedup(self.h, self.DEDUP[dedup], 0))
 
     def close(self) -> None:
         if self.h:

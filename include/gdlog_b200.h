@@ -86,6 +86,21 @@ gdl_status gdl_engine_destroy(gdl_engine *e);
  * no counterpart (its drivers leak relations at exit, test/tc.cu:80-149). */
 gdl_status gdl_engine_clear(gdl_engine *e);
 
+/* How a fixpoint deduplicates NEWT and merges it into FULL.  SORT: radix
+ * sort of NEWT, then one merge-path pass giving NEWT \ FULL and FULL ∪ NEWT
+ * (the reference's sort/unique/set_difference/merge, src/lie.cu:122-185).
+ * DENSE: when 2 * bits(largest column value) <= dense_max_bits (at most 30,
+ * the default), relations are kept as bitmaps over the key domain during the
+ * loop and NEWT is deduplicated by setting bits.  AUTO (default): DENSE
+ * where the domain allows, else SORT.  Results are identical in all modes.
+ * dense_max_bits == 0 keeps the current bound.  The environment variables
+ * GDLOG_DEDUP=auto|sort|dense and GDLOG_DENSE_MAX_BITS set the defaults.
+ * No reference counterpart. */
+#define GDL_DEDUP_AUTO 0
+#define GDL_DEDUP_SORT 1
+#define GDL_DEDUP_DENSE 2
+gdl_status gdl_engine_set_dedup(gdl_engine *e, int32_t mode, int32_t dense_max_bits);
+
 /* Declare a relation.  Replaces `new Relation()` plus the field writes the
  * drivers make before loading (include/relation.cuh:257-300; index_flag as
  * set at test/tc.cu:108, tmp_flag as in load_relation's last argument,

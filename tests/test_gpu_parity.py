@@ -21,6 +21,11 @@ from test_oracle import GOLDEN, SMALL, build_workload
 
 pytestmark = pytest.mark.gpu
 
+# Both deduplication paths of the engine: radix sort + merge-path merge, and
+# bitmaps over the key domain (every workload here has a small domain, so
+# "dense" is what the engine picks by itself).
+MODES = ["sort", "dense"]
+
 
 def summarize(r):
     return {
@@ -31,18 +36,19 @@ def summarize(r):
     }
 
 
-def run_both(prog, *args):
-    with Engine("gpu") as g:
+def run_both(prog, *args, mode="dense"):
+    with Engine("gpu", dedup=mode) as g:
         got = summarize(prog(g, *args, sync=g.sync))
     with Engine("oracle") as o:
         want = summarize(prog(o, *args))
     return got, want
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", SMALL)
-def test_small_workloads_match_golden(name):
+def test_small_workloads_match_golden(name, mode):
     prog, args = build_workload(name)
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         got = summarize(prog(g, *args, sync=g.sync))
     want = GOLDEN["workloads"][name]
     assert got["sizes"] == want["sizes"]
@@ -51,9 +57,10 @@ def test_small_workloads_match_golden(name):
     assert got["traces"] == want["traces"]
 
 
-def test_grid_tc_64x64():
+@pytest.mark.parametrize("mode", MODES)
+def test_grid_tc_64x64(mode):
     want = GOLDEN["workloads"]["tc_grid_64x64"]
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         r = P.tc(g, W.grid_edges(64, 64), sync=g.sync)
         assert r.output.size() == 4322304
         assert r.iterations["tc"] == 126
@@ -61,9 +68,10 @@ def test_grid_tc_64x64():
         assert r.lies["tc"].trace().tolist() == want["traces"]["tc"]
 
 
-def test_sg_rmat_scale14_full_size():
+@pytest.mark.parametrize("mode", MODES)
+def test_sg_rmat_scale14_full_size(mode):
     want = GOLDEN["workloads"]["sg_rmat_s14_40000_s14"]
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         r = P.sg(g, W.rmat_edges(14, 40000, seed=14), sync=g.sync)
         assert r.output.size() == want["sizes"]["sg"]
         assert r.iterations == want["iterations"]
@@ -74,29 +82,32 @@ def test_sg_rmat_scale14_full_size():
         assert rows.max() < 2**14
 
 
-def test_graph_and_stream_paths_agree():
+@pytest.mark.parametrize("mode", MODES)
+def test_graph_and_stream_paths_agree(mode):
     e = W.layered_dag(20, 12, 7)
     os.environ["GDLOG_NO_GRAPH"] = "1"
     try:
-        with Engine("gpu") as g:
+        with Engine("gpu", dedup=mode) as g:
             a = summarize(P.tc(g, e, sync=g.sync))
     finally:
         del os.environ["GDLOG_NO_GRAPH"]
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         b = summarize(P.tc(g, e, sync=g.sync))
     assert a == b
 
 
-def test_duplicate_and_unsorted_input():
+@pytest.mark.parametrize("mode", MODES)
+def test_duplicate_and_unsorted_input(mode):
     e = W.layered_dag(10, 9, 3)
     noisy = np.concatenate([e[::-1], e[: len(e) // 2]])
-    got, want = run_both(P.tc, noisy)
+    got, want = run_both(P.tc, noisy, mode=mode)
     assert got == want
 
 
-def test_empty_relation():
+@pytest.mark.parametrize("mode", MODES)
+def test_empty_relation(mode):
     e = np.zeros((0, 2), dtype=np.uint64)
-    got, want = run_both(P.tc, e)
+    got, want = run_both(P.tc, e, mode=mode)
     assert got == want
     assert got["sizes"]["path"] == 0
 
@@ -115,12 +126,13 @@ def test_values_above_32_bits_rejected():
             g.load(r, np.array([[1 << 33, 1]], dtype=np.uint64))
 
 
-def test_max_iteration_cap():
+@pytest.mark.parametrize("mode", MODES)
+def test_max_iteration_cap(mode):
     e = W.grid_edges(12, 12)
     for cap in (0, 1, 5):
         res = []
         for kind in ("gpu", "oracle"):
-            with Engine(kind) as eng:
+            with Engine(kind, dedup=mode if kind == "gpu" else None) as eng:
                 path = eng.relation("path", index_flag=False)
                 edge = eng.relation("edge")
                 eng.load(path, e)
@@ -157,16 +169,18 @@ def empty_inner_program(eng):
     return it, a.size(), c.size(), c.digest(), lie.trace().tolist()
 
 
-def test_empty_inner_quirk():
-    with Engine("gpu") as g:
+@pytest.mark.parametrize("mode", MODES)
+def test_empty_inner_quirk(mode):
+    with Engine("gpu", dedup=mode) as g:
         got = empty_inner_program(g)
     with Engine("oracle") as o:
         want = empty_inner_program(o)
     assert got == want
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("kind", [PRED_NE, PRED_LT, PRED_GT])
-def test_predicates(kind):
+def test_predicates(kind, mode):
     e = W.rmat_edges(7, 300, seed=9)
 
     def prog(eng, sync=None):
@@ -181,7 +195,7 @@ def test_predicates(kind):
         it = lie.fixpoint()
         return it, out.size(), out.digest()
 
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         got = prog(g)
     with Engine("oracle") as o:
         want = prog(o)
@@ -197,10 +211,11 @@ def test_relation_export_roundtrip():
         assert r.rows().tolist() == [[0, 9], [7, 0], [7, 1]]
 
 
-def test_repeated_fixpoints_on_one_engine():
+@pytest.mark.parametrize("mode", MODES)
+def test_repeated_fixpoints_on_one_engine(mode):
     """Engine state (scratch buffers, index epochs, look-back generations)
     carries over correctly from one program to the next."""
-    with Engine("gpu") as g:
+    with Engine("gpu", dedup=mode) as g:
         outs = []
         for seed in (1, 2, 3):
             prog, args = build_workload(f"sg_rmat_s8_600_s{seed}")
@@ -208,3 +223,18 @@ def test_repeated_fixpoints_on_one_engine():
     for seed, got in zip((1, 2, 3), outs):
         want = GOLDEN["workloads"][f"sg_rmat_s8_600_s{seed}"]
         assert got["sizes"] == want["sizes"] and got["digests"] == want["digests"]
+
+
+def test_modes_agree_on_cspa_with_clear():
+    """Sort and dense paths give identical CSPA results on one engine that
+    is cleared between programs (scratch and bitmaps are reused)."""
+    assign, deref = W.cspa_facts(200, 400, 150, seed=8)
+    out = []
+    with Engine("gpu") as g:
+        for mode in ("sort", "dense", "sort"):
+            g.clear()
+            g.lib.gdl_engine_set_dedup(g.h, Engine.DEDUP[mode], 0)
+            out.append(summarize(P.cspa(g, assign, deref, sync=g.sync)))
+    with Engine("oracle") as o:
+        want = summarize(P.cspa(o, assign, deref))
+    assert out[0] == out[1] == out[2] == want
