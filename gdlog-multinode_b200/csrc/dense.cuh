@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
       const u64 vbase = (w0 + i) << 5;
       if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
       ob += __popc(eb[i]);
-      u32 x = ea[i];
+      u32 x = la ? ea[i] : 0u;
       while (x) {
         const int b = __ffs(x) - 1;
         x &= x - 1;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
           atomicOr(&a.ctl->oob, 2048u);
         pa++;
       }
-      x = eb[i];
+      x = lb ? eb[i] : 0u;
       while (x) {
         const int b = __ffs(x) - 1;
         x &= x - 1;
