@@ -38,6 +38,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 using namespace gdl;
@@ -1177,7 +1178,13 @@ const char *gdl_status_string(gdl_status s) {
   return "unknown status";
 }
 
-const char *gdl_last_error(const gdl_engine *e) { return e ? e->err.c_str() : "null engine"; }
+// Message of the last failing call that has no engine (the allocation-free
+// entry point below), per host thread.
+static thread_local std::string g_engineless_error = "null engine";
+
+const char *gdl_last_error(const gdl_engine *e) {
+  return e ? e->err.c_str() : g_engineless_error.c_str();
+}
 
 gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
   if (!out) return GDL_E_INVALID;
@@ -1699,3 +1706,195 @@ gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out, int32_t n_out)
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free sort + deduplicate (gdl_sort_unique_rows_noalloc)
+// ===========================================================================
+// Some callers cannot allocate device memory: code running inside another
+// library's memory arena, or a process that has handed all of HBM to a
+// fixed-size pool before it starts.  For them this entry point sorts and
+// deduplicates rows with the same kernels load_relation uses (pack, onesweep
+// radix sort, merge-path dedup, unpack) but takes every byte of scratch from
+// one file-scope device array of fixed size, which each GPU that loads the
+// library holds until the process exits.
+namespace {
+
+constexpr u64 kNoAllocMaxRows = 1ull << 17;  // 131,072 rows per call
+constexpr u64 kNoAllocSortTiles = kNoAllocMaxRows / kSortTile + 2;
+constexpr u64 kNoAllocMergeTiles = (2 * kNoAllocMaxRows) / kMergeTile + 2;
+
+// Byte layout of the scratch array.  The four key buffers come first; every
+// byte after kNaCtrl is control state that must start at zero on each call.
+constexpr u64 kNaKeys = 0;                                    // packed input
+constexpr u64 kNaPing = kNaKeys + 8 * kNoAllocMaxRows;        // sort ping-pong
+constexpr u64 kNaUniq = kNaPing + 8 * kNoAllocMaxRows;        // FULL' of the merge
+constexpr u64 kNaDelta = kNaUniq + 8 * kNoAllocMaxRows;       // DELTA of the merge
+constexpr u64 kNaStatus = kNaDelta + 8 * kNoAllocMaxRows;     // sort look-back words
+constexpr u64 kNaCtrl = kNaStatus + 4 * kMaxPasses * kNoAllocSortTiles * kRadix;
+constexpr u64 kNaOffsets = kNaCtrl;                                   // u32 [8][256]
+constexpr u64 kNaCounters = kNaOffsets + 4 * kMaxPasses * kRadix;     // u32 [9] (+pad)
+constexpr u64 kNaLbFlag = kNaCounters + 64;                           // u32 [tiles]
+constexpr u64 kNaLbAgg = kNaLbFlag + 4 * kNoAllocMergeTiles + 256;    // u64 [tiles]
+constexpr u64 kNaLbInc = kNaLbAgg + 8 * kNoAllocMergeTiles;           // u64 [tiles]
+constexpr u64 kNaParts = kNaLbInc + 8 * kNoAllocMergeTiles;           // u64 [tiles + 1]
+constexpr u64 kNaCtl = ((kNaParts + 8 * (kNoAllocMergeTiles + 1)) + 255) / 256 * 256;
+constexpr u64 kNaRecs = kNaCtl + (sizeof(Ctl) + 255) / 256 * 256;     // LaunchRec [4]
+constexpr u64 kNaDarr = kNaRecs + 256;                                // DArr [4]
+constexpr u64 kNaScalars = kNaDarr + 256;                             // u64 [4]
+constexpr u64 kNaBytes = kNaScalars + 256;
+
+}  // namespace
+
+// The scratch.  In host code this name is only a host-side stand-in for the
+// device array: its device address comes from cudaGetSymbolAddress, once per
+// device, and only that address is passed to kernels.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+void *g_noalloc_addr[64] = {nullptr};  // device address of the scratch, per device
+
+__global__ void k_noalloc_init(unsigned char *base, u64 rows) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  DArr *d = reinterpret_cast<DArr *>(base + kNaDarr);
+  d[0] = DArr{reinterpret_cast<u64 *>(base + kNaKeys), rows, kNoAllocMaxRows};   // NEWT
+  d[1] = DArr{reinterpret_cast<u64 *>(base + kNaDelta), 0, 0};                   // empty FULL
+  d[2] = DArr{reinterpret_cast<u64 *>(base + kNaUniq), 0, kNoAllocMaxRows};      // FULL'
+  d[3] = DArr{reinterpret_cast<u64 *>(base + kNaDelta), 0, kNoAllocMaxRows};     // DELTA
+}
+
+__global__ void k_noalloc_unpack(const DArr *keys, u64 *rows) {
+  const u64 n = keys->n;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 k = keys->ptr[i];
+    rows[2 * i] = key_c0(k);
+    rows[2 * i + 1] = key_c1(k);
+  }
+}
+
+gdl_status noalloc_fail(gdl_status code, const char *msg) {
+  g_engineless_error = msg;
+  return code;
+}
+
+#define NA_CK(call)                                                              \
+  do {                                                                           \
+    cudaError_t _r = (call);                                                     \
+    if (_r != cudaSuccess) {                                                     \
+      g_engineless_error = std::string(#call) + ": " + cudaGetErrorString(_r);   \
+      return GDL_E_CUDA;                                                         \
+    }                                                                            \
+  } while (0)
+
+}  // namespace
+
+extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, uint64_t rows,
+                                                   uint64_t *device_out_rows, uint64_t *out_rows,
+                                                   void *stream) {
+  if (!out_rows || (rows && (!device_rows || !device_out_rows)))
+    return noalloc_fail(GDL_E_INVALID, "gdl_sort_unique_rows_noalloc: null argument");
+  *out_rows = 0;
+  if (rows > kNoAllocMaxRows) {
+    char msg[160];
+    snprintf(msg, sizeof msg,
+             "gdl_sort_unique_rows_noalloc: %llu rows exceed the fixed scratch limit of %llu rows",
+             (unsigned long long)rows, (unsigned long long)kNoAllocMaxRows);
+    return noalloc_fail(GDL_E_CAPACITY, msg);
+  }
+  if (rows == 0) return GDL_OK;
+  int dev = 0;
+  NA_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return noalloc_fail(GDL_E_UNSUPPORTED, "device ordinal above 63");
+  unsigned char *base = nullptr;
+  {
+    // Set-up, once per device, with that device current.
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+      void *p = nullptr;
+      NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_addr[dev] = p;
+    }
+    base = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int sms = 148;
+  NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  static bool smem_set[64] = {false};
+  if (!smem_set[dev]) {
+    NA_CK(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSortSmemBytes));
+    NA_CK(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSortSmemBytes));
+    NA_CK(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kMergeSmemBytes));
+    smem_set[dev] = true;
+  }
+  // The array keeps the previous call's contents: zero the control state.
+  NA_CK(cudaMemsetAsync(base + kNaCtrl, 0, kNaBytes - kNaCtrl, s));
+  k_noalloc_init<<<1, 32, 0, s>>>(base, rows);
+  u64 *keys = reinterpret_cast<u64 *>(base + kNaKeys);
+  u64 *scal = reinterpret_cast<u64 *>(base + kNaScalars);  // [0] max value, [1] bad flag
+  auto blocks = [&](u64 work, u64 per, int per_sm) {
+    u64 g = (work + per - 1) / per, lim = (u64)sms * per_sm;
+    return (int)std::max<u64>(1, std::min(g, lim));
+  };
+  k_pack_rows<<<blocks(rows, 256, 8), 256, 0, s>>>(reinterpret_cast<const u64 *>(device_rows),
+                                                    rows, keys, scal,
+                                                    reinterpret_cast<u32 *>(scal + 1));
+  NA_CK(cudaGetLastError());
+  u64 host_scal[2] = {0, 0};
+  NA_CK(cudaMemcpyAsync(host_scal, scal, sizeof host_scal, cudaMemcpyDeviceToHost, s));
+  NA_CK(cudaStreamSynchronize(s));
+  if (host_scal[1])
+    return noalloc_fail(GDL_E_UNSUPPORTED, "gdl_sort_unique_rows_noalloc: values must be below 2^32");
+  int kbits = 1;
+  while (kbits < 64 && (host_scal[0] >> kbits)) kbits++;
+  Ctl *ctl = reinterpret_cast<Ctl *>(base + kNaCtl);
+  DArr *d = reinterpret_cast<DArr *>(base + kNaDarr);
+  LaunchRec *recs = reinterpret_cast<LaunchRec *>(base + kNaRecs);
+  SortArgs a;
+  a.keys = &d[0];
+  a.buf0 = keys;
+  a.buf1 = reinterpret_cast<u64 *>(base + kNaPing);
+  a.cap = kNoAllocMaxRows;
+  a.kbits = kbits;
+  a.passes = std::max(1, (2 * kbits + 7) / 8);
+  a.offsets = reinterpret_cast<u32 *>(base + kNaOffsets);
+  a.status = reinterpret_cast<u32 *>(base + kNaStatus);
+  a.max_tiles = kNoAllocSortTiles;
+  a.counters = reinterpret_cast<u32 *>(base + kNaCounters);
+  a.ctl = ctl;
+  k_sort_hist<<<blocks(rows, (u64)kSortTile * 4, 2), kSortBlock, kSortSmemBytes, s>>>(a);
+  for (int p = 0; p < a.passes; p++)
+    k_sort_pass<<<blocks(rows, kSortTile, 4), kSortBlock, kSortSmemBytes, s>>>(a, p);
+  MergeArgs m;
+  m.newt = &d[0];
+  m.a = (a.passes & 1) ? a.buf1 : a.buf0;
+  m.full = &d[1];
+  m.full_next = &d[2];
+  m.delta_next = &d[3];
+  m.c_newt_n = scal + 2;
+  m.rec = &recs[0];
+  m.lb = Lb{reinterpret_cast<u32 *>(base + kNaLbFlag), reinterpret_cast<u64 *>(base + kNaLbAgg),
+            reinterpret_cast<u64 *>(base + kNaLbInc)};
+  m.parts = reinterpret_cast<u64 *>(base + kNaParts);
+  m.parts_cap = kNoAllocMergeTiles + 1;
+  m.ctl = ctl;
+  m.rel = 0;
+  k_merge_partition<<<blocks(rows / kMergeTile + 2, 256, 8), 256, 0, s>>>(m);
+  k_merge_diff<<<blocks(rows, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, s>>>(m);
+  k_noalloc_unpack<<<blocks(rows, 256, 8), 256, 0, s>>>(&d[2],
+                                                         reinterpret_cast<u64 *>(device_out_rows));
+  NA_CK(cudaGetLastError());
+  DArr uniq;
+  Ctl c;
+  NA_CK(cudaMemcpyAsync(&uniq, &d[2], sizeof uniq, cudaMemcpyDeviceToHost, s));
+  NA_CK(cudaMemcpyAsync(&c, ctl, sizeof c, cudaMemcpyDeviceToHost, s));
+  NA_CK(cudaStreamSynchronize(s));
+  if (c.timeout || c.oob || c.overflow)
+    return noalloc_fail(GDL_E_TIMEOUT, "gdl_sort_unique_rows_noalloc: device-side check failed");
+  *out_rows = uniq.n;
+  return GDL_OK;
+}

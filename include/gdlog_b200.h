@@ -226,6 +226,32 @@ gdl_status gdl_engine_set_profile(gdl_engine *e, int32_t flag);
 gdl_status gdl_engine_profile(gdl_engine *e, double *out, int32_t n_out);
 gdl_status gdl_engine_profile_reset(gdl_engine *e);
 
+/* Allocation-free sort + deduplicate.  No counterpart in the reference; it
+ * is an extra entry point for callers that cannot allocate device memory
+ * (code running inside another library's memory arena, or a process that
+ * gave all of HBM to a fixed pool before starting): it makes no cudaMalloc
+ * or cudaFree call and no call into any allocating library.
+ *
+ * Sorts `rows` rows of two uint64 columns (device memory, row-major, values
+ * below 2^32) lexicographically, removes duplicates, writes the unique rows
+ * to `device_out_rows` (caller-provided, room for `rows` rows) and their
+ * count to *out_rows (host).  Same result as gdl_relation_load_device
+ * followed by gdl_relation_export of FULL.  At most 131,072 rows per call;
+ * larger inputs are refused with GDL_E_CAPACITY.  Runs on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) on the current device
+ * and returns after that stream has finished the work.
+ *
+ * Scratch is one fixed array of about 4.3 MB inside the library, present on
+ * every GPU that loads the library until the process exits.  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls on a device
+ * share the array: calls that can overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  On failure,
+ * gdl_last_error(NULL) holds the message. */
+gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, uint64_t rows,
+                                        uint64_t *device_out_rows, uint64_t *out_rows,
+                                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif
