@@ -81,6 +81,8 @@ struct Ctl {
   u32 timeout;   // a bounded wait gave up
   u32 oob;       // a write was dropped by a bounds check (must stay 0)
   u32 cond_set;  // graph conditional handle is valid
+  u32 overflow_stage;  // 1: the overflow came from a dense update scan
+  u32 pad_ctl;
   u64 iteration;     // iteration_counter of the reference loop
   u64 stop_at;       // pause when iteration reaches this
   u64 max_iteration; // LIE::max_iteration

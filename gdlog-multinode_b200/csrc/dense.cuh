@@ -79,6 +79,7 @@ struct BmScanArgs {
   u64 *count_b;    // if set: receives total_b (FULL count without a list)
   u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
+  int update_stage;    // an update-step scan: its overflow can be resumed
   u64 *tile_prefix;    // [tiles] packed exclusive prefix (a << 32 | b)
   u64 tiles_cap;
   BmScanRec *rec;
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   if (a.rec->overflow) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.rec->pop_g = 0;
+      if (a.update_stage) a.ctl->overflow_stage = 1;
       atomicExch(&a.ctl->overflow, 1u);
     }
     return;
@@ -319,9 +321,13 @@ __device__ __forceinline__ void bm_set_warp(u32 *bm, u64 words, u64 word, u32 bi
 }
 
 // RelationalJoin materialisation into the output's NEWT bitmap.  Balanced
-// over candidate positions exactly as k_join_mat; consecutive lanes take
-// consecutive positions, so the outputs of one outer row (one c0, ascending
-// c1) fall into few bitmap words and are set with few atomics.
+// over candidate positions as k_join_mat: a block owns kMatTile consecutive
+// positions, each thread kMatPer consecutive ones, found with one binary
+// search over the tile's records and then walked forward.  A candidate is one
+// inner read, the column move, the predicate and one atomicOr (outputs of
+// different outer rows rarely share a bitmap word, so no warp aggregation).
+constexpr int kMatPer = kMatTile / kMatBlock;  // positions per thread
+
 __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_bm, u64 out_words,
                                                            int dk) {
   __shared__ MatSmem sm;
@@ -358,20 +364,25 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_
       }
     }
     __syncthreads();
-    for (u64 q = 0; q < (u64)kMatTile; q += blockDim.x) {
-      const u64 p = p0 + q + threadIdx.x;
-      u64 word = ~0ull;
-      u32 bits = 0;
-      if (p < p1) {
-        const u32 r = find_rec(sm.off, m, p);
+    u64 p = p0 + (u64)threadIdx.x * kMatPer;
+    if (p < p1) {
+      u32 r = find_rec(sm.off, m, p);
+      u64 next = sm.off[r + 1];
+      const u64 pe = min(p + kMatPer, p1);
+      for (; p < pe; p++) {
+        while (p >= next) {
+          r++;
+          next = sm.off[r + 1];
+        }
         const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
         if (pred_ok(a.pred, t)) {
           const u64 v = dense_vkey(t, dk);
-          word = v >> 5;
-          bits = 1u << (v & 31);
+          if ((v >> 5) < out_words)
+            atomicOr(out_bm + (v >> 5), 1u << (v & 31));
+          else
+            atomicOr(&a.ctl->oob, 8192u);
         }
       }
-      bm_set_warp(out_bm, out_words, word, bits, a.ctl);
     }
   }
   if (launch_rec_finish(a.rec) && threadIdx.x == 0)

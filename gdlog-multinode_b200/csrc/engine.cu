@@ -594,6 +594,8 @@ BmScanArgs scan_none(int dk) {
   return a;
 }
 
+void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc);
+
 void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
@@ -718,6 +720,17 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       }
     }
   }
+  enqueue_update_step(e, L, plan, kc);
+}
+
+// The per-relation update step (DELTA, FULL', indexes) and the commit of
+// one iteration.  After a capacity overflow in a dense scan it is enqueued
+// again on its own: the NEWT bitmaps still hold the iteration's joins.
+void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
+  cudaStream_t s = e->s;
+  RelDev *R = e->d_rels;
+  const bool dense = L.dense;
+  const int dk = L.dk;
   for (int r : L.update) {
     const RelDev &rh = e->h[r];
     if (dense) {
@@ -737,6 +750,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
         a.count_b = &R[r].f_count;
       }
       a.pop_g_out = &R[r].c_newt_n;
+      a.update_stage = 1;
       launch_scan(e, a, kc);
     } else {
       launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
@@ -948,6 +962,36 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       e->h[r].dense = 1;
     }
     TRY(ensure_dense_scratch(e, words));
+    // Every list of the loop is bounded by the key domain: size them for
+    // it up front (within a quarter of free HBM shared among the lists), so
+    // that the loop does not stop to grow buffers.  Untouched capacity
+    // costs nothing but address space in the stream-ordered pool.
+    size_t free_b = 0, total_b = 0;
+    CK(e, cudaMemGetInfo(&free_b, &total_b));
+    u64 lists = 0;
+    for (int r : L.update) lists += 2 + (plan.newt_list[r] ? 1 : 0) + (plan.full_list[r] ? 2 : 0);
+    lists += L.tmps.size();
+    const u64 domain = words * 32;
+    const u64 cap = std::min<u64>(domain, (u64)(free_b / 4) / std::max<u64>(lists, 1) / 8);
+    for (int r : L.update) {
+      RelDev &h = e->h[r];
+      TRY(ensure_arr(e, h.delta, cap, true));
+      TRY(ensure_arr(e, h.delta_next, cap, false));
+      if (plan.newt_list[r]) TRY(ensure_arr(e, h.newt, cap, false));
+      if (plan.full_list[r]) {
+        TRY(ensure_arr(e, h.full, cap, true));
+        TRY(ensure_arr(e, h.full_next, cap, false));
+        if (plan.full_idx[r]) {
+          TRY(ensure_index(e, h.full_idx, h.full.cap));
+          TRY(ensure_index(e, h.full_idx_next, h.full_next.cap));
+        }
+      }
+      if (plan.delta_idx[r]) {
+        TRY(ensure_index(e, h.delta_idx, h.delta.cap));
+        TRY(ensure_index(e, h.delta_idx_next, h.delta_next.cap));
+      }
+    }
+    for (int r : L.tmps) TRY(ensure_arr(e, e->h[r].newt, cap, false));
   }
   TRY(ensure_scratch(e));
   TRY(push(e));
@@ -1087,10 +1131,62 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       const auto tg = std::chrono::steady_clock::now();
       TRY(grow_after_overflow(e, c));
       L.grow_ms += host_ms_since(tg);
+      const bool resume = L.dense && c.overflow_stage == 1;
       c.overflow = 0;
+      c.overflow_stage = 0;
       memset(c.need, 0, sizeof c.need);
       L.retries++;
       L.graph_dirty = true;
+      if (resume) {
+        // Re-run only the update step and the commit of the iteration that
+        // overflowed, launch by launch, until its lists fit.
+        while (true) {
+          c.pause = 0;
+          c.stop_at = ~0ull;
+          c.trace_base = c.iteration;
+          c.cond_set = 0;
+          CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
+          const u64 it1 = c.iteration;
+          Counts kc;
+          enqueue_update_step(e, L, plan, &kc);
+          CK(e, cudaGetLastError());
+          CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+          CK(e, cudaStreamSynchronize(e->s));
+          prof_collect(e);
+          c = *e->h_ctl;
+          L.kernels += kc.total;
+          for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += kc.kind[k];
+          if (c.timeout || c.oob) {
+            e->broken = true;
+            return fail(e, GDL_E_TIMEOUT,
+                        "device-side check failed in iteration %llu (timeout=%u, dropped "
+                        "writes=%u)",
+                        (unsigned long long)c.iteration, c.timeout, c.oob);
+          }
+          if (c.overflow) {
+            const auto tg2 = std::chrono::steady_clock::now();
+            TRY(grow_after_overflow(e, c));
+            L.grow_ms += host_ms_since(tg2);
+            c.overflow = 0;
+            c.overflow_stage = 0;
+            memset(c.need, 0, sizeof c.need);
+            L.retries++;
+            continue;
+          }
+          if (L.trace_on && c.iteration > it1) {
+            std::vector<u64> rows(L.update.size() * 3);
+            CK(e, cudaMemcpyAsync(rows.data(), ld.trace, rows.size() * sizeof(u64),
+                                  cudaMemcpyDeviceToHost, e->s));
+            CK(e, cudaStreamSynchronize(e->s));
+            for (size_t i = 0; i < L.update.size(); i++) {
+              const u64 *x = &rows[i * 3];
+              L.trace.insert(L.trace.end(), {it1, (u64)L.update[i], x[0], x[1], x[2]});
+            }
+          }
+          break;
+        }
+        if (c.done) break;
+      }
       continue;
     }
     if (c.done) break;
