@@ -50,6 +50,14 @@ struct Index {
   u32 hash_mode;  // 0: identity (c0 & mask), 1: 64-bit mixer
 };
 
+// One instance of a batched LIE in the dense (bitmap) form: its rows start at
+// word base_word, each 2^row_shift words long, n rows (= n local ids).
+struct SegInfo {
+  u64 base_word;
+  u32 row_shift;
+  u32 n;
+};
+
 // Device state of one relation.  `x` is committed state, `x_next` is what
 // the running iteration builds; the commit kernel swaps them.
 struct RelDev {

@@ -2,17 +2,15 @@
 //
 // When every column value is below 2^dk with 2*dk <= 30, the whole key
 // domain of an arity-2 relation is 2^(2dk) bits (at most 128 MB), and a
-// version of the relation can be held as a bitmap whose bit v is the tuple
-// (v >> dk, v & (2^dk - 1)).  Bit order is the reference's tuple order
-// (include/tuple.cuh:106-126), so compacting a bitmap gives the sorted,
-// deduplicated tuple list directly.  This replaces, for such domains, the
-// sort -> unique -> set_difference -> merge sequence of the reference's
-// update step (src/lie.cu:122-185, src/relation.cu:405-521, src/join.cu:
-// 160-225):
+// version of the relation can be held as a bitmap whose bit (c0, c1) sits in
+// row c0.  Bit order is the reference's tuple order (include/tuple.cuh:
+// 106-126), so compacting a bitmap gives the sorted, deduplicated tuple list
+// directly.  This replaces, for such domains, the sort -> unique ->
+// set_difference -> merge sequence of the reference's update step
+// (src/lie.cu:122-185, src/relation.cu:405-521, src/join.cu:160-225):
 //   * joins and copies test-and-set bits of the output relation's NEWT
-//     bitmap G (atomicOr, aggregated per warp), so the raw join output --
-//     often tens of times larger than its distinct tuples -- is never
-//     written to memory;
+//     bitmap G (atomicOr), so the raw join output -- often tens of times
+//     larger than its distinct tuples -- is never written to memory;
 //   * one streaming pass over (G, F) per relation then yields DELTA =
 //     G & ~F and FULL' = F | G as sorted lists, the next FULL bitmap, and
 //     the run index of FULL' from per-row popcounts.
@@ -20,6 +18,13 @@
 // exclusive prefixes (decoupled look-back) and checks the output
 // capacities; k_bm_write writes.  Nothing but idempotent bit-sets happens
 // before a capacity check, so an iteration that overflows can be re-run.
+//
+// Batched form.  Many independent instances of one program can share one
+// LIE: instance i owns the ids (i << S) | local, local < n_i, and its
+// tuples keep both columns inside its own range.  The bitmap is then block
+// diagonal: instance i has n_i rows of 2^row_shift words (the power of two
+// at or above n_i / 32), starting at a tile-aligned word.  A DenseMap
+// describes either layout; the square domain is the one-instance case.
 #pragma once
 
 #include "common.cuh"
@@ -32,18 +37,52 @@ constexpr int kBmBlock = 256;
 constexpr int kBmWordsPerThread = 8;
 constexpr int kBmTileWords = kBmBlock * kBmWordsPerThread;  // 2048 words = 65536 keys
 constexpr int kDenseMaxDomainBits = 30;
+constexpr int kMaxInstanceNodes = 1 << 16;  // a row is at most one scan tile
 
-__device__ __forceinline__ u64 dense_vkey(u64 key, int dk) {
-  return ((u64)key_c0(key) << dk) | (u64)key_c1(key);
+// Where a key lives in the bitmap: the tuple (c0, c1) of instance
+// i = c0 >> seg_shift is bit (c1 & 31) of word
+//   seg[i].base_word + (local(c0) << seg[i].row_shift) + (local(c1) >> 5).
+struct DenseMap {
+  const SegInfo *seg;     // one entry per instance
+  const u32 *tile_inst;   // instance of each scan tile (null: all instance 0)
+  u32 n_inst;
+  int seg_shift;          // 31 for the square domain (every id is local)
+  u64 words;              // total bitmap words
+};
+
+__device__ __forceinline__ bool dm_locate(const DenseMap &m, u64 key, u64 *word, u32 *bit) {
+  const u32 c0 = key_c0(key), c1 = key_c1(key);
+  const u32 i = c0 >> m.seg_shift;
+  if (i >= m.n_inst || (c1 >> m.seg_shift) != i) return false;
+  const u32 mask = (1u << m.seg_shift) - 1u;
+  const u32 lx = c0 & mask, lz = c1 & mask;
+  const SegInfo s = m.seg[i];
+  if (lx >= s.n || lz >= s.n) return false;
+  *word = s.base_word + ((u64)lx << s.row_shift) + (lz >> 5);
+  *bit = lz & 31u;
+  return true;
 }
-__device__ __forceinline__ u64 dense_key(u64 vkey, int dk) {
-  return make_key((u32)(vkey >> dk), (u32)(vkey & ((1ull << dk) - 1)));
+
+__device__ __forceinline__ u32 dm_tile_inst(const DenseMap &m, u64 tile) {
+  return m.tile_inst ? m.tile_inst[tile] : 0u;
 }
-// Bit sets are bounds-checked against the bitmap size: a key outside the
-// domain is dropped and recorded in Ctl::oob instead of being written.
-__device__ __forceinline__ void bm_set(u32 *bm, u64 words, u64 vkey, Ctl *ctl) {
-  if ((vkey >> 5) < words)
-    atomicOr(bm + (vkey >> 5), 1u << (vkey & 31));
+
+// The key of bit b of word w, w inside instance inst.
+__device__ __forceinline__ u64 dm_key(const DenseMap &m, u32 inst, const SegInfo &s, u64 w, int b) {
+  const u64 wl = w - s.base_word;
+  const u32 lx = (u32)(wl >> s.row_shift);
+  const u32 lz = (u32)(((wl & ((1ull << s.row_shift) - 1)) << 5) + (u64)b);
+  const u32 hi = m.seg_shift >= 31 ? 0u : (inst << m.seg_shift);
+  return make_key(hi | lx, hi | lz);
+}
+
+// Set the bit of one key; keys outside their instance's range are dropped
+// and recorded in Ctl::oob instead of being written.
+__device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u64 key, Ctl *ctl) {
+  u64 w;
+  u32 b;
+  if (dm_locate(m, key, &w, &b) && w < m.words)
+    atomicOr(bm + w, 1u << b);
   else
     atomicOr(&ctl->oob, 8192u);
 }
@@ -70,14 +109,14 @@ struct BmScanArgs {
   // and bmF_next on the device, so pointers captured in a graph would go
   // stale.
   const RelDev *rd;
-  u64 words;       // bitmap words (multiple of kBmTileWords or smaller)
-  int dk;          // bits per column
+  DenseMap map;
   int ex_a, ex_b;  // expressions for list a and list b
-  DArr *list_a;    // output lists (sorted keys); null when ex is kBmNone
+  DArr *list_a;    // output lists (sorted keys); null when not wanted
   DArr *list_b;
-  Index *idx_b;    // if set: run index of list b (identity addressing)
+  Index *idx_b;    // if set: run index of list b
   u64 *count_b;    // if set: receives total_b (FULL count without a list)
   u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
+  u64 *inst_delta; // if set: per-instance count of list a is added here
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
   int update_stage;    // an update-step scan: its overflow can be resumed
   u64 *tile_prefix;    // [tiles] packed exclusive prefix (a << 32 | b)
@@ -98,7 +137,8 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_count(BmScanArgs a) {
   __shared__ u64 s_scan[kBmBlock / 32];
   __shared__ long long s_tile;
   if (ctl_stop(a.ctl)) return;
-  const u64 tiles = bm_tiles(a.words);
+  const u64 words = a.map.words;
+  const u64 tiles = bm_tiles(words);
   if (tiles > a.tiles_cap) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->oob, 1024u);
     return;
@@ -118,7 +158,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_count(BmScanArgs a) {
 #pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
       const u64 w = w0 + i;
-      if (w < a.words) {
+      if (w < words) {
         const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
         ca += __popc(bm_eval(a.ex_a, g, f));
         cb += __popc(bm_eval(a.ex_b, g, f));
@@ -179,14 +219,14 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     }
     return;
   }
-  const u64 tiles = bm_tiles(a.words);
+  const u64 words = a.map.words;
+  const u64 tiles = bm_tiles(words);
   if (tiles > a.tiles_cap) return;
   if (a.rd) {
     a.g = a.rd->bmG;
     a.f = a.rd->bmF;
     a.f_next = a.rd->bmF_next;
   }
-  const int row_shift = a.dk - 5;  // words per row = 2^row_shift (dk >= 5)
   const u32 epoch = (u32)(a.ctl->generation + 1);
   const Index ix = a.idx_b ? *a.idx_b : Index{};
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.idx_b) a.idx_b->epoch = epoch;
@@ -196,6 +236,8 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const u64 prefix = a.tile_prefix[tile];
     const u64 wt = tile * kBmTileWords;
+    const u32 inst = dm_tile_inst(a.map, tile);
+    const SegInfo seg = a.map.seg[inst];
     const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
     u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
     u32 ca = 0, cb = 0;
@@ -203,7 +245,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     for (int i = 0; i < kBmWordsPerThread; i++) {
       const u64 w = w0 + i;
       u32 g = 0, f = 0;
-      if (w < a.words) {
+      if (w < words) {
         g = a.g ? a.g[w] : 0u;
         f = a.f ? a.f[w] : 0u;
         if (a.f_next) a.f_next[w] = f | g;
@@ -215,12 +257,12 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     }
     u64 tot;
     const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
+    if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
     u64 pa = (prefix >> 32) + (ex >> 32);
     u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
     u32 ob = (u32)(ex & 0xFFFFFFFFull);
 #pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u64 vbase = (w0 + i) << 5;
       if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
       ob += __popc(eb[i]);
       u32 x = la ? ea[i] : 0u;
@@ -228,7 +270,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
         const int b = __ffs(x) - 1;
         x &= x - 1;
         if (pa < cap_a)
-          la[pa] = dense_key(vbase + b, a.dk);
+          la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
         else
           atomicOr(&a.ctl->oob, 2048u);
         pa++;
@@ -238,7 +280,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
         const int b = __ffs(x) - 1;
         x &= x - 1;
         if (pb < cap_b)
-          lb[pb] = dense_key(vbase + b, a.dk);
+          lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
         else
           atomicOr(&a.ctl->oob, 4096u);
         pb++;
@@ -248,16 +290,20 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
       if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
       __syncthreads();
       // One slot per non-empty row of the tile: {c0, epoch, start, len}.
-      const u64 row_words = 1ull << row_shift;
-      const u64 rows = kBmTileWords >> row_shift;
+      // Rows are 2^row_shift words, at most one tile, aligned in the tile.
+      const u32 rs = seg.row_shift;
+      const u64 row_words = 1ull << rs;
+      const u64 rows = kBmTileWords >> rs;
+      const u32 hi = a.map.seg_shift >= 31 ? 0u : (inst << a.map.seg_shift);
       for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
-        const u64 lw = r << row_shift;  // first word of the row in the tile
-        if (wt + lw >= a.words) break;
+        const u64 lw = r << rs;  // first word of the row in the tile
+        if (wt + lw >= words || wt + lw < seg.base_word) break;
+        const u64 row = (wt + lw - seg.base_word) >> rs;
+        if (row >= seg.n) break;
         const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
         if (len) {
-          const u32 c0 = (u32)((wt + lw) >> row_shift);
           const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
-          index_insert(ix, epoch, c0, start, len, a.ctl);
+          index_insert(ix, epoch, hi | (u32)row, start, len, a.ctl);
         }
       }
     }
@@ -270,17 +316,14 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
     a.rec->pop_g = 0;
     prof_add(a.ctl, kPBitmap,
-             a.words * 4 * ((a.g ? 2 : 0) + (a.f ? 2 : 0) + (a.f_next ? 1 : 0)) +
+             words * 4 * ((a.g ? 2 : 0) + (a.f ? 2 : 0) + (a.f_next ? 1 : 0)) +
                  8 * (a.rec->total_a + a.rec->total_b));
   }
 }
 
-// Zero a bitmap.  With `only_if_empty`, only when *only_if_empty == 0 (the
-// copy of an empty source empties its destination NEWT, src/copy.cu:24-27).
-__global__ void __launch_bounds__(256) k_bm_clear(u32 *bm, u64 words, const DArr *only_if_empty,
-                                                  const u32 *vis, Ctl *ctl) {
+// Zero a bitmap (words a multiple of 4).
+__global__ void __launch_bounds__(256) k_bm_clear(u32 *bm, u64 words, Ctl *ctl) {
   if (ctl_stop(ctl)) return;
-  if (only_if_empty && eff_count(only_if_empty, vis) != 0) return;
   uint4 *p = reinterpret_cast<uint4 *>(bm);
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < words / 4;
        i += (u64)gridDim.x * blockDim.x)
@@ -289,35 +332,14 @@ __global__ void __launch_bounds__(256) k_bm_clear(u32 *bm, u64 words, const DArr
 }
 
 // Set the bits of a key list (FULL at the start of a LIE).
-__global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm, u64 words, int dk,
+__global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm, DenseMap map,
                                                       Ctl *ctl) {
   if (ctl_stop(ctl)) return;
   const u64 n = list->n;
   const u64 *k = list->ptr;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-    bm_set(bm, words, dense_vkey(k[i], dk), ctl);
+    dm_set(map, bm, k[i], ctl);
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
-}
-
-// Warp-aggregated bit set: lanes whose words are equal and adjacent OR their
-// bits together and the last lane of each run issues one atomicOr.  Lanes
-// with word == ~0 set nothing.
-__device__ __forceinline__ void bm_set_warp(u32 *bm, u64 words, u64 word, u32 bits, Ctl *ctl) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const u32 ob = __shfl_up_sync(0xffffffffu, bits, o);
-    const u64 ow = __shfl_up_sync(0xffffffffu, word, o);
-    if (lane >= o && ow == word) bits |= ob;
-  }
-  const u64 nw = __shfl_down_sync(0xffffffffu, word, 1);
-  const bool last = lane == 31 || nw != word;
-  if (last && word != ~0ull && bits) {
-    if (word < words)
-      atomicOr(bm + word, bits);
-    else
-      atomicOr(&ctl->oob, 8192u);
-  }
 }
 
 // RelationalJoin materialisation into the output's NEWT bitmap.  Balanced
@@ -328,8 +350,7 @@ __device__ __forceinline__ void bm_set_warp(u32 *bm, u64 words, u64 word, u32 bi
 // different outer rows rarely share a bitmap word, so no warp aggregation).
 constexpr int kMatPer = kMatTile / kMatBlock;  // positions per thread
 
-__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_bm, u64 out_words,
-                                                           int dk) {
+__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_bm, DenseMap map) {
   __shared__ MatSmem sm;
   if (ctl_stop(a.ctl)) return;
   const u64 total = a.op->total;
@@ -375,13 +396,7 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_
           next = sm.off[r + 1];
         }
         const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
-        if (pred_ok(a.pred, t)) {
-          const u64 v = dense_vkey(t, dk);
-          if ((v >> 5) < out_words)
-            atomicOr(out_bm + (v >> 5), 1u << (v & 31));
-          else
-            atomicOr(&a.ctl->oob, 8192u);
-        }
+        if (pred_ok(a.pred, t)) dm_set(map, out_bm, t, a.ctl);
       }
     }
   }
@@ -391,31 +406,21 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_
 
 // RelationalCopy into the destination's NEWT bitmap (src/copy.cu:12-95).
 // An empty source empties the destination NEWT (src/copy.cu:24-27).
-__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, u32 *dest_bm, u64 dest_words,
-                                                 int dk) {
+__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, u32 *dest_bm, DenseMap map) {
   if (ctl_stop(c.ctl)) return;
   if (c.once && *c.once) return;
   const u64 n = eff_count(c.src, c.src_vis);
   if (n == 0) {
     uint4 *p = reinterpret_cast<uint4 *>(dest_bm);
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < dest_words / 4;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < map.words / 4;
          i += (u64)gridDim.x * blockDim.x)
       p[i] = make_uint4(0, 0, 0, 0);
     if (blockIdx.x == 0 && threadIdx.x == 0 && c.once_pending) *c.once_pending = 1;
     return;
   }
   const u64 *src = c.src->ptr;
-  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
-    const u64 i = i0 + threadIdx.x;
-    u64 word = ~0ull;
-    u32 bits = 0;
-    if (i < n) {
-      const u64 v = dense_vkey(gen_join(c.sel, src[i], 0), dk);
-      word = v >> 5;
-      bits = 1u << (v & 31);
-    }
-    bm_set_warp(dest_bm, dest_words, word, bits, c.ctl);
-  }
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    dm_set(map, dest_bm, gen_join(c.sel, src[i], 0), c.ctl);
   if (launch_rec_finish(c.rec) && threadIdx.x == 0) {
     if (c.once_pending) *c.once_pending = 1;
     prof_add(c.ctl, kPCopy, 8 * n);
@@ -424,19 +429,105 @@ __global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, u32 *dest_bm, u64 d
 
 // RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT).  The
 // destination bitmap is cleared by a k_bm_clear launched just before.
-__global__ void __launch_bounds__(256) k_acopy_bm(const u32 *src_bm, u64 words, Sel2 sel,
-                                                  u32 *dest_bm, int dk, Ctl *ctl) {
+__global__ void __launch_bounds__(256) k_acopy_bm(const u32 *src_bm, Sel2 sel, u32 *dest_bm,
+                                                  DenseMap map, Ctl *ctl) {
   if (ctl_stop(ctl)) return;
-  for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < words;
+  for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < map.words;
        w += (u64)gridDim.x * blockDim.x) {
     u32 x = src_bm[w];
+    if (!x) continue;
+    const u32 inst = dm_tile_inst(map, w / kBmTileWords);
+    const SegInfo seg = map.seg[inst];
     while (x) {
       const int b = __ffs(x) - 1;
       x &= x - 1;
-      bm_set(dest_bm, words, dense_vkey(gen_join(sel, dense_key((w << 5) + b, dk), 0), dk), ctl);
+      dm_set(map, dest_bm, gen_join(sel, dm_key(map, inst, seg, w, b), 0), ctl);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, words * 4);
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, map.words * 4);
+}
+
+// Batched form: an instance whose update relations produced new tuples in
+// this iteration records it (inst_last = iteration + 1), so that its own
+// loop-pass count is known when the shared loop ends.
+__global__ void k_inst_track(u64 *inst_delta, u64 *inst_last, u32 n_inst, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u64 it = ctl->iteration;
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n_inst; i += gridDim.x * blockDim.x) {
+    if (inst_delta[i]) {
+      inst_last[i] = it + 1;
+      inst_delta[i] = 0;
+    }
+  }
+}
+
+// Per-instance size and digest of a FULL bitmap, in each instance's local
+// ids (the digest gdl_relation_digest gives for the instance run alone).
+// Pass 1: popcount per tile.
+__global__ void __launch_bounds__(256) k_inst_tile_pop(const u32 *bm, DenseMap map, u32 *tile_pop) {
+  __shared__ u32 s_sum;
+  const u64 tiles = bm_tiles(map.words);
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+    u32 c = 0;
+    for (u64 w = t * kBmTileWords + threadIdx.x; w < min((t + 1) * kBmTileWords, map.words);
+         w += blockDim.x)
+      c += __popc(bm[w]);
+    atomicAdd(&s_sum, c);
+    __syncthreads();
+    if (threadIdx.x == 0) tile_pop[t] = s_sum;
+    __syncthreads();
+  }
+}
+
+// Pass 2 (after a per-instance exclusive scan of tile_pop into tile_rank):
+// digest terms of every tuple, summed per instance.
+__global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map,
+                                                     const u64 *tile_rank, u64 *acc) {
+  __shared__ u32 s_off[257];
+  const u64 tiles = bm_tiles(map.words);
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const u32 inst = dm_tile_inst(map, t);
+    const SegInfo seg = map.seg[inst];
+    const u64 w0 = t * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 cnt = 0;
+    for (int i = 0; i < kBmWordsPerThread; i++)
+      if (w0 + i < map.words) cnt += __popc(bm[w0 + i]);
+    // exclusive scan of cnt over the block (small, via shared memory)
+    s_off[threadIdx.x] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u32 run = 0;
+      for (int k = 0; k < 256; k++) {
+        const u32 v = s_off[k];
+        s_off[k] = run;
+        run += v;
+      }
+    }
+    __syncthreads();
+    u64 rank = tile_rank[t] + s_off[threadIdx.x];
+    u64 h_sum = 0;
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u64 w = w0 + i;
+      if (w >= map.words) break;
+      u32 x = bm[w];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        const u64 wl = w - seg.base_word;
+        const u64 lx = wl >> seg.row_shift;
+        const u64 lz = ((wl & ((1ull << seg.row_shift) - 1)) << 5) + (u64)b;
+        u64 h = mix64(rank);
+        h = mix64(h ^ lx);
+        h = mix64(h ^ lz);
+        h_sum += h;
+        rank++;
+      }
+    }
+    if (h_sum) atomicAdd(&acc[inst], h_sum);
+    __syncthreads();
+  }
 }
 
 }  // namespace gdl

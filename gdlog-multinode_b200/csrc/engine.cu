@@ -99,9 +99,15 @@ struct LieHost {
   unsigned long long cond_handle = 0;
   bool graph_dirty = true;
   Counts per_iter;  // launches of one enqueued iteration
-  // Dense form of the running fixpoint (dense.cuh): bits per column, or 0.
+  // Dense form of the running fixpoint (dense.cuh): bits per column (square
+  // domain) and the bitmap layout.
   bool dense = false;
   int dk = 0;
+  DenseMap map{};
+  // Batched form: per-instance new-tuple counts of the running iteration and
+  // the last iteration (+1) in which each instance produced new tuples.
+  u64 *d_inst_delta = nullptr, *d_inst_last = nullptr;
+  u32 n_inst = 0;
 };
 
 struct RelHost {
@@ -116,6 +122,8 @@ struct RelHost {
   bool raw_is_full = true;
   bool delta_sorted = true;
   u64 bm_words = 0;  // size of this relation's bitmaps (dense form), words
+  bool bm_valid = false;       // bmF holds FULL (set by a dense LIE)
+  bool full_resident = false;  // FULL exists only as bmF (batched form)
 };
 
 }  // namespace
@@ -156,6 +164,14 @@ struct gdl_engine {
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
   int dense_max_bits = kDenseMaxDomainBits;
   int dedup_mode = 0;
+  // Batched form (gdl_engine_set_instances): the block-diagonal layout.
+  bool instances = false;
+  std::vector<SegInfo> segs;
+  int seg_shift = 31;
+  u64 seg_words = 0;
+  SegInfo *d_segs = nullptr;
+  u32 *d_tile_inst = nullptr;
+  SegInfo *d_square_seg = nullptr;  // the one segment of the square domain
   u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
   LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
@@ -478,6 +494,8 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   RelHost &rh = e->rels[rel];
   TRY(pull(e));
   RelDev &r = e->h[rel];
+  rh.bm_valid = false;
+  rh.full_resident = false;
   // raw := keys in load order
   if (rh.raw && !rh.raw_is_full) dfree(e, rh.raw);
   rh.raw = nullptr;
@@ -567,7 +585,8 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   return p;
 }
 
-// Bitmap size, in 32-bit words, of one relation version in dense form.
+// Bitmap size, in 32-bit words, of one relation version over the square
+// domain of dk-bit columns.
 u64 dense_words(int dk) { return 1ull << (2 * dk - 5); }
 
 // One bitmap scan (dense.cuh): count pass, then write pass.
@@ -577,18 +596,17 @@ void launch_scan(gdl_engine *e, BmScanArgs a, Counts *kc) {
   a.rec = e->bm_rec;
   a.lb = e->lb_bm;
   a.ctl = e->d_ctl;
-  const u64 tiles = (a.words + kBmTileWords - 1) / kBmTileWords;
+  const u64 tiles = (a.map.words + kBmTileWords - 1) / kBmTileWords;
   a.lrec = &e->recs[4];
   PLAUNCH(kc, kPBitmap, k_bm_count<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
   a.lrec = &e->recs[5];
   PLAUNCH(kc, kPBitmap, k_bm_write<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
 }
 
-BmScanArgs scan_none(int dk) {
+BmScanArgs scan_none(const DenseMap &map) {
   BmScanArgs a;
   memset(&a, 0, sizeof a);
-  a.words = dense_words(dk);
-  a.dk = dk;
+  a.map = map;
   a.ex_a = a.ex_b = kBmNone;
   a.need_a = a.need_b = -1;
   return a;
@@ -600,17 +618,17 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
-  const int dk = L.dk;
-  const u64 words = dense ? dense_words(dk) : 0;
+  const DenseMap &map = L.map;
+  const u64 words = dense ? map.words : 0;
   PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
   if (dense) {
     // NEWT of every update and tmp relation starts empty.
     for (int r : L.update)
       PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                e->h[r].bmG, words, nullptr, nullptr, e->d_ctl));
+                                e->h[r].bmG, words, e->d_ctl));
     for (int r : L.tmps)
       PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                e->h[r].bmG, words, nullptr, nullptr, e->d_ctl));
+                                e->h[r].bmG, words, e->d_ctl));
   }
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
@@ -629,7 +647,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
         a.outer_vis = nullptr;
         if (dense && oh.bmG) {
           // NEWT as a join outer: the sorted list of its bitmap.
-          BmScanArgs c = scan_none(dk);
+          BmScanArgs c = scan_none(map);
           c.g = oh.bmG;
           c.ex_a = kBmUnion;
           c.list_a = &R[op.outer].newt;
@@ -672,7 +690,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       const u64 out_cap = e->h[op.out].newt.cap;
       if (dense)
         PLAUNCH(kc, kPJoinMat,
-                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, e->h[op.out].bmG, words, dk));
+                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, e->h[op.out].bmG, map));
       else if (op.pred.kind)
         PLAUNCH(kc, kPJoinMat,
                 k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b));
@@ -707,13 +725,13 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
         // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
         u32 *dbm = e->h[op.out].bmG;
         PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                  dbm, words, nullptr, nullptr, e->d_ctl));
+                                  dbm, words, e->d_ctl));
         if (sh.bmG)  // a source without a NEWT bitmap (static) has an empty NEWT
           PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, words, 256, 8), 256, 0, s>>>(
-                                  sh.bmG, words, op.sel, dbm, dk, e->d_ctl));
+                                  sh.bmG, op.sel, dbm, map, e->d_ctl));
       } else if (dense) {
         PLAUNCH(kc, kPCopy, k_copy_bm<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
-                                c, e->h[op.out].bmG, words, dk));
+                                c, e->h[op.out].bmG, map));
       } else {
         PLAUNCH(kc, kPCopy,
                 k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c));
@@ -730,13 +748,13 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
-  const int dk = L.dk;
   for (int r : L.update) {
     const RelDev &rh = e->h[r];
     if (dense) {
       // DELTA = NEWT \ FULL, FULL' = FULL | NEWT, both sorted; FULL's list
       // and index only when some op reads them during the loop.
-      BmScanArgs a = scan_none(dk);
+      BmScanArgs a = scan_none(L.map);
+      a.inst_delta = L.d_inst_delta;
       a.rd = &R[r];  // bitmaps as the device sees them (k_commit swaps F)
       a.ex_a = kBmDelta;
       a.list_a = &R[r].delta_next;
@@ -786,6 +804,9 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
                   &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl));
     }
   }
+  if (L.d_inst_delta)
+    PLAUNCH(kc, kPControl, k_inst_track<<<grid_for(e, L.n_inst, 256, 1), 256, 0, s>>>(
+                               L.d_inst_delta, L.d_inst_last, L.n_inst, e->d_ctl));
   PLAUNCH(kc, kPControl, k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
 }
 
@@ -943,15 +964,39 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, kMinCap), false));
     h.newt.n = 0;
   }
-  // Dense form (dense.cuh) when the key domain is small enough.
+  // Dense form (dense.cuh) when the key domain is small enough; always in
+  // the batched form, whose block-diagonal bitmap is the only layout.
+  for (int r : L.update)
+    if (e->rels[r].full_resident)
+      return fail(e, GDL_E_UNSUPPORTED,
+                  "FULL of %s is kept as a bitmap only (batched form, too large for a list)",
+                  e->rels[r].name.c_str());
   {
     const int dk = std::max(e->kbits, 5);
-    L.dense = e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits;
-    L.dk = L.dense ? dk : 0;
+    L.dense = e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits);
+    L.dk = L.dense && !e->instances ? dk : 0;
   }
   for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
   if (L.dense) {
-    const u64 words = dense_words(L.dk);
+    if (e->instances) {
+      L.map = DenseMap{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
+      const u32 n = (u32)e->segs.size();
+      if (L.n_inst != n) {
+        dfree(e, L.d_inst_delta);
+        dfree(e, L.d_inst_last);
+        TRY(dalloc(e, (void **)&L.d_inst_delta, n * sizeof(u64)));
+        TRY(dalloc(e, (void **)&L.d_inst_last, n * sizeof(u64)));
+        L.n_inst = n;
+      }
+      CK(e, cudaMemsetAsync(L.d_inst_delta, 0, n * sizeof(u64), e->s));
+      CK(e, cudaMemsetAsync(L.d_inst_last, 0, n * sizeof(u64), e->s));
+    } else {
+      if (!e->d_square_seg) TRY(dalloc(e, (void **)&e->d_square_seg, sizeof(SegInfo)));
+      const SegInfo sq{0, (u32)(L.dk - 5), 1u << L.dk};
+      CK(e, cudaMemcpyAsync(e->d_square_seg, &sq, sizeof sq, cudaMemcpyHostToDevice, e->s));
+      L.map = DenseMap{e->d_square_seg, nullptr, 1, 31, dense_words(L.dk)};
+    }
+    const u64 words = L.map.words;
     for (int r : L.update) {
       TRY(ensure_bitmaps(e, r, words, true));
       e->h[r].dense = 1;
@@ -972,7 +1017,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     for (int r : L.update) lists += 2 + (plan.newt_list[r] ? 1 : 0) + (plan.full_list[r] ? 2 : 0);
     lists += L.tmps.size();
     const u64 domain = words * 32;
-    const u64 cap = std::min<u64>(domain, (u64)(free_b / 4) / std::max<u64>(lists, 1) / 8);
+    const u64 cap = std::min<u64>(
+        {domain, (u64)(free_b / 4) / std::max<u64>(lists, 1) / 8, kMaxRows});
     for (int r : L.update) {
       RelDev &h = e->h[r];
       TRY(ensure_arr(e, h.delta, cap, true));
@@ -997,14 +1043,15 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   TRY(push(e));
   if (L.dense) {
     // FULL's bitmap from its list; NEWT bitmaps empty.
-    const u64 words = dense_words(L.dk);
+    const u64 words = L.map.words;
     for (int r : L.update) {
       const RelDev &h = e->h[r];
       CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(h.bmG, 0, words * 4, e->s));
       if (h.full.n)
         k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
-            &e->d_rels[r].full, h.bmF, words, L.dk, e->d_ctl);
+            &e->d_rels[r].full, h.bmF, L.map, e->d_ctl);
+      e->rels[r].bm_valid = true;
     }
     for (int r : L.tmps) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
     CK(e, cudaGetLastError());
@@ -1199,9 +1246,19 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(reset_ctl(e));  // clear done/pause so that the scans below run
     TRY(pull(e));
     bool any = false;
+    size_t free_b = 0, total_b = 0;
+    CK(e, cudaMemGetInfo(&free_b, &total_b));
     for (int r : L.update)
       if (e->h[r].full_lazy) {
-        TRY(ensure_arr(e, e->h[r].full, e->h[r].full.n, false));
+        // The batched form may keep a FULL too large for a list as its
+        // bitmap only (per-instance sizes, digests and exports read it).
+        const u64 n = e->h[r].full.n;
+        if (e->instances && (n > kMaxRows || n * 8 > free_b / 2)) {
+          e->rels[r].full_resident = true;
+          e->h[r].full_lazy = 0;
+          continue;
+        }
+        TRY(ensure_arr(e, e->h[r].full, n, false));
         any = true;
       }
     if (any) {
@@ -1209,7 +1266,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       Counts kc;
       for (int r : L.update) {
         if (!e->h[r].full_lazy) continue;
-        BmScanArgs a = scan_none(L.dk);
+        BmScanArgs a = scan_none(L.map);
         a.f = e->h[r].bmF;
         a.ex_b = kBmUnion;
         a.list_b = &e->d_rels[r].full;
@@ -1362,6 +1419,8 @@ static void release_program(gdl_engine *e) {
       cudaFree(L.d_lie);
     }
     cudaFree(L.d_joinrec);
+    if (L.d_inst_delta) cudaFreeAsync(L.d_inst_delta, e->s);
+    if (L.d_inst_last) cudaFreeAsync(L.d_inst_last, e->s);
   }
   cudaStreamSynchronize(e->s);
   e->rels.clear();
@@ -1394,7 +1453,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
                   (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->merge_parts,
                   (void *)e->bm_prefix, (void *)e->lb_bm.flag, (void *)e->lb_bm.agg,
-                  (void *)e->lb_bm.inc, (void *)e->bm_rec,
+                  (void *)e->lb_bm.inc, (void *)e->bm_rec, (void *)e->d_segs,
+                  (void *)e->d_tile_inst, (void *)e->d_square_seg,
                   (void *)e->recs,
                   (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
                   (void *)e->d_ctl})
@@ -1504,11 +1564,15 @@ gdl_status gdl_relation_load_device(gdl_engine *e, int32_t rel, const uint64_t *
 }
 
 static gdl_status version_view(gdl_engine *e, int rel, int ver, const u64 **ptr, u64 *n,
-                               bool *sorted) {
+                               bool *sorted, bool need_rows = true) {
   TRY(pull(e));
   const RelDev &r = e->h[rel];
   *sorted = true;
   if (ver == GDL_FULL) {
+    if (e->rels[rel].full_resident && need_rows)
+      return fail(e, GDL_E_UNSUPPORTED,
+                  "FULL of %s is kept as a bitmap only (batched form): read it per instance",
+                  e->rels[rel].name.c_str());
     *ptr = r.full.ptr;
     *n = r.full_vis ? r.full.n : 0;
   } else if (ver == GDL_DELTA) {
@@ -1552,7 +1616,7 @@ gdl_status gdl_relation_size(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *
   const u64 *p = nullptr;
   u64 n = 0;
   bool sorted;
-  TRY(version_view(e, rel, ver, &p, &n, &sorted));
+  TRY(version_view(e, rel, ver, &p, &n, &sorted, false));
   *out = n;
   return GDL_OK;
 }
@@ -1787,6 +1851,128 @@ gdl_status gdl_engine_profile_reset(gdl_engine *e) {
     e->prof_ms[k] = 0;
     e->prof_launches[k] = 0;
     e->prof_bytes[k] = 0;
+  }
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_set_instances(gdl_engine *e, const uint32_t *node_counts,
+                                    int32_t n_instances) {
+  if (!e || n_instances < 0 || (n_instances && !node_counts)) return GDL_E_INVALID;
+  cudaSetDevice(e->device);
+  CK(e, cudaStreamSynchronize(e->s));
+  dfree(e, e->d_segs);
+  dfree(e, e->d_tile_inst);
+  e->d_segs = nullptr;
+  e->d_tile_inst = nullptr;
+  e->segs.clear();
+  e->instances = false;
+  e->seg_words = 0;
+  if (n_instances == 0) return GDL_OK;
+  u32 maxn = 1;
+  for (int i = 0; i < n_instances; i++) {
+    if (node_counts[i] < 1 || node_counts[i] > (u32)kMaxInstanceNodes)
+      return fail(e, GDL_E_INVALID, "instance %d: node count must be in [1, %d]", i,
+                  kMaxInstanceNodes);
+    maxn = std::max(maxn, node_counts[i]);
+  }
+  int S = 1;
+  while ((1u << S) < maxn) S++;
+  if ((u64)n_instances << S > (1ull << 32))
+    return fail(e, GDL_E_UNSUPPORTED, "%d instances of up to %u nodes exceed 32-bit ids",
+                n_instances, maxn);
+  u64 base = 0;
+  std::vector<u32> tile_inst;
+  for (int i = 0; i < n_instances; i++) {
+    const u32 n = node_counts[i];
+    u32 rs = 0;
+    while ((1ull << rs) * 32 < n) rs++;
+    SegInfo sg{base, rs, n};
+    e->segs.push_back(sg);
+    const u64 region = round_up((u64)n << rs, kBmTileWords);
+    for (u64 t = 0; t < region / kBmTileWords; t++) tile_inst.push_back((u32)i);
+    base += region;
+  }
+  e->seg_shift = S;
+  e->seg_words = base;
+  TRY(dalloc(e, (void **)&e->d_segs, e->segs.size() * sizeof(SegInfo)));
+  TRY(dalloc(e, (void **)&e->d_tile_inst, tile_inst.size() * sizeof(u32)));
+  CK(e, cudaMemcpyAsync(e->d_segs, e->segs.data(), e->segs.size() * sizeof(SegInfo),
+                        cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaMemcpyAsync(e->d_tile_inst, tile_inst.data(), tile_inst.size() * sizeof(u32),
+                        cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  e->instances = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_instance_shift(gdl_engine *e, int32_t *out_shift) {
+  if (!e || !out_shift) return GDL_E_INVALID;
+  if (!e->instances) return fail(e, GDL_E_INVALID, "no instances declared");
+  *out_shift = e->seg_shift;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_instance_iterations(gdl_engine *e, int32_t lie, uint64_t *out, int32_t n) {
+  CHECK_LIE(e, lie);
+  const LieHost &L = e->lies[lie];
+  if (!out || n < 0) return GDL_E_INVALID;
+  if (!L.d_inst_last || (u32)n > L.n_inst)
+    return fail(e, GDL_E_INVALID, "the LIE did not run in the batched form with %d instances", n);
+  std::vector<u64> last(L.n_inst);
+  CK(e, cudaMemcpyAsync(last.data(), L.d_inst_last, L.n_inst * sizeof(u64),
+                        cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  // An instance's own loop would stop after the first pass without new
+  // tuples: passes = last productive iteration + 2, or 1 (src/lie.cu:208-215).
+  for (int i = 0; i < n; i++) out[i] = last[i] ? last[i] + 1 : 1;
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *sizes,
+                                       uint64_t *digests, int32_t n) {
+  CHECK_REL(e, rel);
+  if (!e->instances) return fail(e, GDL_E_INVALID, "no instances declared");
+  if (n < 0 || (u32)n > e->segs.size() || (n && (!sizes || !digests))) return GDL_E_INVALID;
+  const RelHost &rh = e->rels[rel];
+  if (!rh.bm_valid || rh.bm_words != e->seg_words)
+    return fail(e, GDL_E_INVALID, "relation %s has no FULL bitmap of the batched form",
+                rh.name.c_str());
+  TRY(pull(e));
+  const u32 *bm = e->h[rel].bmF;
+  const DenseMap map{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
+  const u64 tiles = e->seg_words / kBmTileWords;
+  u32 *d_pop = nullptr;
+  u64 *d_rank = nullptr, *d_acc = nullptr;
+  TRY(dalloc(e, (void **)&d_pop, tiles * sizeof(u32)));
+  TRY(dalloc(e, (void **)&d_rank, tiles * sizeof(u64)));
+  TRY(dalloc(e, (void **)&d_acc, e->segs.size() * sizeof(u64)));
+  k_inst_tile_pop<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_pop);
+  std::vector<u32> pop(tiles);
+  CK(e, cudaMemcpyAsync(pop.data(), d_pop, tiles * sizeof(u32), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  std::vector<u64> rank(tiles), size(e->segs.size(), 0);
+  for (size_t i = 0, t = 0; i < e->segs.size(); i++) {
+    const u64 region = round_up((u64)e->segs[i].n << e->segs[i].row_shift, kBmTileWords);
+    u64 run = 0;
+    for (u64 k = 0; k < region / kBmTileWords; k++, t++) {
+      rank[t] = run;
+      run += pop[t];
+    }
+    size[i] = run;
+  }
+  CK(e, cudaMemcpyAsync(d_rank, rank.data(), tiles * sizeof(u64), cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaMemsetAsync(d_acc, 0, e->segs.size() * sizeof(u64), e->s));
+  k_inst_digest<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_rank, d_acc);
+  std::vector<u64> acc(e->segs.size());
+  CK(e, cudaMemcpyAsync(acc.data(), d_acc, acc.size() * sizeof(u64), cudaMemcpyDeviceToHost,
+                        e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  dfree(e, d_pop);
+  dfree(e, d_rank);
+  dfree(e, d_acc);
+  for (int i = 0; i < n; i++) {
+    sizes[i] = size[i];
+    digests[i] = mix64(acc[i] ^ size[i]);
   }
   return GDL_OK;
 }

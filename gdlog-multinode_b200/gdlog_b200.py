@@ -111,6 +111,14 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_engine_sync.restype = _I
         lib.gdl_relation_load_device.argtypes = [_P, _I, _P, _U64]
         lib.gdl_relation_load_device.restype = _I
+        lib.gdl_engine_set_instances.argtypes = [_P, C.POINTER(C.c_uint32), _I]
+        lib.gdl_engine_set_instances.restype = _I
+        lib.gdl_engine_instance_shift.argtypes = [_P, _PI]
+        lib.gdl_engine_instance_shift.restype = _I
+        lib.gdl_lie_instance_iterations.argtypes = [_P, _I, _PU64, _I]
+        lib.gdl_lie_instance_iterations.restype = _I
+        lib.gdl_relation_instance_stats.argtypes = [_P, _I, _PU64, _PU64, _I]
+        lib.gdl_relation_instance_stats.restype = _I
         lib.gdl_engine_set_dedup.argtypes = [_P, _I, _I]
         lib.gdl_engine_set_dedup.restype = _I
         lib.gdl_engine_clear.argtypes = [_P]
@@ -188,6 +196,14 @@ class Relation:
     def digest(self, version: int = FULL) -> int:
         return self.eng.digest(self, version)
 
+    def instance_stats(self, n: int):
+        """Batched form: per-instance (sizes, digests) of FULL, local ids."""
+        sizes = np.zeros(n, dtype=np.uint64)
+        digests = np.zeros(n, dtype=np.uint64)
+        self.eng._check(self.eng.lib.gdl_relation_instance_stats(
+            self.eng.h, self.id, sizes.ctypes.data_as(_PU64), digests.ctypes.data_as(_PU64), n))
+        return sizes, digests
+
     def __repr__(self):
         return f"Relation({self.name!r}, id={self.id})"
 
@@ -245,6 +261,13 @@ class Lie:
         self._call("lie_fixpoint", self.id, C.byref(out))
         self.iterations = int(out.value)
         return self.iterations
+
+    def instance_iterations(self, n: int) -> np.ndarray:
+        """Batched form: loop passes each instance would have taken alone."""
+        out = np.zeros(n, dtype=np.uint64)
+        self.eng._check(self.eng.lib.gdl_lie_instance_iterations(
+            self.eng.h, self.id, out.ctypes.data_as(_PU64), n))
+        return out
 
     def trace(self) -> np.ndarray:
         n = C.c_uint64(0)
@@ -377,6 +400,18 @@ class Engine:
     def sync(self) -> None:
         if self.kind == "gpu":
             self._check(self.lib.gdl_engine_sync(self.h))
+
+    def set_instances(self, node_counts) -> int:
+        """Batched form: declare the instances' node counts; returns S, the
+        shift of global ids (instance << S) | local."""
+        counts = np.ascontiguousarray(np.asarray(node_counts, dtype=np.uint32))
+        self._check(self.lib.gdl_engine_set_instances(
+            self.h, counts.ctypes.data_as(C.POINTER(C.c_uint32)), len(counts)))
+        if len(counts) == 0:
+            return 0
+        sh = C.c_int32(0)
+        self._check(self.lib.gdl_engine_instance_shift(self.h, C.byref(sh)))
+        return int(sh.value)
 
     def clear(self) -> None:
         """Drop every relation and LIE; keep buffers and the memory pool."""

@@ -226,6 +226,34 @@ gdl_status gdl_engine_set_profile(gdl_engine *e, int32_t flag);
 gdl_status gdl_engine_profile(gdl_engine *e, double *out, int32_t n_out);
 gdl_status gdl_engine_profile_reset(gdl_engine *e);
 
+/* Batched form: many independent instances of one program in one LIE.  No
+ * reference counterpart (the reference runs one fixpoint at a time).
+ * Declare node_counts[i] local node ids for instance i before loading; the
+ * instance's tuples then use the global ids (i << S) | local, where S is
+ * given by gdl_engine_instance_shift, and both columns of every tuple must
+ * belong to the same instance.  The fixpoint over the disjoint union equals
+ * the union of the per-instance fixpoints (every rule joins on shared
+ * values); the engine keeps the relations as one block-diagonal bitmap, so
+ * all instances advance together in the same kernels and an instance that
+ * has converged costs nothing but its scan.  Passing 0 instances returns to
+ * the plain form.  Node counts are limited to 65,536 per instance. */
+gdl_status gdl_engine_set_instances(gdl_engine *e, const uint32_t *node_counts,
+                                    int32_t n_instances);
+gdl_status gdl_engine_instance_shift(gdl_engine *e, int32_t *out_shift);
+
+/* Loop passes each instance would have taken alone (the reference's
+ * iteration_counter for that instance, src/lie.cu:208-215), for the last
+ * fixpoint of `lie` in the batched form. */
+gdl_status gdl_lie_instance_iterations(gdl_engine *e, int32_t lie, uint64_t *out,
+                                       int32_t n_instances);
+
+/* Per-instance size and digest of FULL of a relation updated by a batched
+ * fixpoint, in the instance's local ids: the values gdl_relation_size and
+ * gdl_relation_digest give when the instance runs alone.  Works also when
+ * FULL is too large for a list and is kept only as its bitmap. */
+gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *sizes,
+                                       uint64_t *digests, int32_t n_instances);
+
 /* Allocation-free sort + deduplicate.  No counterpart in the reference; it
  * is an extra entry point for callers that cannot allocate device memory
  * (code running inside another library's memory arena, or a process that
