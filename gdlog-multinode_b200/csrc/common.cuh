@@ -79,7 +79,14 @@ struct RelDev {
   u64 f_count;     // |FULL'| when the FULL list is not rebuilt every iteration
   u32 dense;       // the running LIE keeps this relation as bitmaps
   u32 full_lazy;   // FULL's list is materialised only when the LIE ends
+  // Emission (dense.cuh): 0 = the update step scans the bitmaps;
+  // kEmitDelta = ops append new keys (not in FULL) to delta_next as they
+  // set them; kEmitNewt = ops append every first-set key to the NEWT list.
+  u32 emit;
+  u32 pad2;
+  u64 gen_count;   // tuples generated this iteration (kEmitDelta: NEWT non-empty?)
 };
+enum EmitMode { kEmitNone = 0, kEmitDelta = 1, kEmitNewt = 2 };
 
 // Loop control of a running fixpoint (one per engine, device memory).
 struct Ctl {

@@ -342,20 +342,99 @@ __global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm,
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
 }
 
+// Emission.  A relation whose FULL list is not read during the loop
+// (kEmitDelta) or whose NEWT is read as a list (kEmitNewt, tmp relations)
+// gets its new keys listed by the ops themselves: the first thread to set a
+// key's NEWT bit appends the key, so the update step works on the list and
+// never scans the bitmap.  kEmitDelta skips keys already in FULL, so its
+// list is DELTA itself.  A full list raises Ctl::overflow; the host then
+// clears the NEWT bitmaps and runs the iteration again with larger lists.
+struct EmitTarget {
+  u32 *g;          // NEWT bitmap
+  const u32 *f;    // FULL bitmap for kEmitDelta (keys in FULL are skipped)
+  DArr *list;      // delta_next or newt; null: bits only (scan path)
+  u64 *ptr;        // list storage and capacity, read once
+  u64 cap;
+  u64 *gen;        // tuples generated (kEmitDelta: is NEWT empty?)
+  int need_slot;
+};
+
+__device__ __forceinline__ EmitTarget emit_target(RelDev *rd, int rel) {
+  EmitTarget t;
+  t.g = rd->bmG;
+  t.f = rd->emit == kEmitDelta ? rd->bmF : nullptr;
+  t.list = rd->emit == kEmitDelta ? &rd->delta_next : rd->emit == kEmitNewt ? &rd->newt : nullptr;
+  t.ptr = t.list ? t.list->ptr : nullptr;
+  t.cap = t.list ? t.list->cap : 0;
+  t.gen = &rd->gen_count;
+  t.need_slot = need_index(rel, rd->emit == kEmitDelta ? kNeedDelta : kNeedNewt);
+  return t;
+}
+
+// Append `key` at position pos of the target list (bounds-checked).
+__device__ __forceinline__ void emit_store(const EmitTarget &T, u64 pos, u64 key, Ctl *ctl) {
+  if (pos < T.cap) {
+    T.ptr[pos] = key;
+  } else {
+    atomicMax(&ctl->need[T.need_slot], pos + 1);
+    atomicExch(&ctl->overflow, 1u);
+  }
+}
+
+// Set one key's NEWT bit; true if this thread set it first (and it is not
+// in FULL when the target checks FULL).
+__device__ __forceinline__ bool emit_set(const DenseMap &m, const EmitTarget &T, u64 key, Ctl *ctl) {
+  u64 w;
+  u32 b;
+  if (!dm_locate(m, key, &w, &b) || w >= m.words) {
+    atomicOr(&ctl->oob, 8192u);
+    return false;
+  }
+  if (T.f && ((T.f[w] >> b) & 1u)) return false;
+  const u32 old = atomicOr(T.g + w, 1u << b);
+  return !(old & (1u << b));
+}
+
+// Warp-synchronous emission of one candidate per lane (all 32 lanes call).
+__device__ __forceinline__ void emit_warp(const DenseMap &m, const EmitTarget &T, bool valid,
+                                          u64 key, Ctl *ctl) {
+  const int lane = threadIdx.x & 31;
+  const unsigned vm = __ballot_sync(0xffffffffu, valid);
+  if (T.list && lane == 0 && vm) atomicAdd(T.gen, (u64)__popc(vm));
+  const bool first = valid && emit_set(m, T, key, ctl);
+  if (!T.list) return;
+  const unsigned fm = __ballot_sync(0xffffffffu, first);
+  if (!fm) return;
+  const int leader = __ffs(fm) - 1;
+  u64 base = 0;
+  if (lane == leader) base = atomicAdd(&T.list->n, (u64)__popc(fm));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (first) emit_store(T, base + __popc(fm & ((1u << lane) - 1u)), key, ctl);
+}
+
+// The same for one thread alone.
+__device__ __forceinline__ void emit_one(const DenseMap &m, const EmitTarget &T, u64 key, Ctl *ctl) {
+  if (T.list) atomicAdd(T.gen, 1ull);
+  if (emit_set(m, T, key, ctl) && T.list) emit_store(T, atomicAdd(&T.list->n, 1ull), key, ctl);
+}
+
 // RelationalJoin materialisation into the output's NEWT bitmap.  Balanced
 // over candidate positions as k_join_mat: a block owns kMatTile consecutive
 // positions, each thread kMatPer consecutive ones, found with one binary
 // search over the tile's records and then walked forward.  A candidate is one
 // inner read, the column move, the predicate and one atomicOr (outputs of
-// different outer rows rarely share a bitmap word, so no warp aggregation).
+// different outer rows rarely share a bitmap word, so no warp aggregation of
+// the bits; only list appends are aggregated).
 constexpr int kMatPer = kMatTile / kMatBlock;  // positions per thread
 
-__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_bm, DenseMap map) {
+__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, RelDev *out_rd,
+                                                           DenseMap map) {
   __shared__ MatSmem sm;
   if (ctl_stop(a.ctl)) return;
   const u64 total = a.op->total;
   const u64 nc = a.op->nc;
   if (total == 0) return;
+  const EmitTarget T = emit_target(out_rd, a.out_rel);
   const u64 *inner = a.inner->ptr;
   const u64 tiles = (total + kMatTile - 1) / kMatTile;
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -386,52 +465,98 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, u32 *out_
     }
     __syncthreads();
     u64 p = p0 + (u64)threadIdx.x * kMatPer;
+    u32 r = 0;
+    u64 next = 0;
     if (p < p1) {
-      u32 r = find_rec(sm.off, m, p);
-      u64 next = sm.off[r + 1];
-      const u64 pe = min(p + kMatPer, p1);
-      for (; p < pe; p++) {
+      r = find_rec(sm.off, m, p);
+      next = sm.off[r + 1];
+    }
+#pragma unroll
+    for (int j = 0; j < kMatPer; j++, p++) {
+      bool valid = p < p1;
+      u64 t = 0;
+      if (valid) {
         while (p >= next) {
           r++;
           next = sm.off[r + 1];
         }
-        const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
-        if (pred_ok(a.pred, t)) dm_set(map, out_bm, t, a.ctl);
+        t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+        valid = pred_ok(a.pred, t);
       }
+      emit_warp(map, T, valid, t, a.ctl);
     }
   }
   if (launch_rec_finish(a.rec) && threadIdx.x == 0)
     prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
 }
 
-// RelationalCopy into the destination's NEWT bitmap (src/copy.cu:12-95).
-// An empty source empties the destination NEWT (src/copy.cu:24-27).
-__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, u32 *dest_bm, DenseMap map) {
+// Clear one relation's NEWT: bitmap and emission list (ACopy replaces the
+// destination's NEWT, src/acopy.cu:37-43).
+__global__ void __launch_bounds__(256) k_newt_reset(RelDev *rd, DenseMap map, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  uint4 *p = reinterpret_cast<uint4 *>(rd->bmG);
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < map.words / 4;
+       i += (u64)gridDim.x * blockDim.x)
+    p[i] = make_uint4(0, 0, 0, 0);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (rd->emit == kEmitDelta) rd->delta_next.n = 0;
+    if (rd->emit == kEmitNewt) rd->newt.n = 0;
+    rd->gen_count = 0;
+    prof_add(ctl, kPBitmap, map.words * 4);
+  }
+}
+
+// RelationalCopy into the destination's NEWT (src/copy.cu:12-95).  An empty
+// source empties the destination NEWT (src/copy.cu:24-27).
+__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, RelDev *dest_rd, DenseMap map) {
   if (ctl_stop(c.ctl)) return;
   if (c.once && *c.once) return;
   const u64 n = eff_count(c.src, c.src_vis);
   if (n == 0) {
-    uint4 *p = reinterpret_cast<uint4 *>(dest_bm);
+    uint4 *p = reinterpret_cast<uint4 *>(dest_rd->bmG);
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < map.words / 4;
          i += (u64)gridDim.x * blockDim.x)
       p[i] = make_uint4(0, 0, 0, 0);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && c.once_pending) *c.once_pending = 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (c.once_pending) *c.once_pending = 1;
+      if (dest_rd->emit == kEmitDelta) dest_rd->delta_next.n = 0;
+      if (dest_rd->emit == kEmitNewt) dest_rd->newt.n = 0;
+      dest_rd->gen_count = 0;
+    }
     return;
   }
+  const EmitTarget T = emit_target(dest_rd, c.dest_rel);
   const u64 *src = c.src->ptr;
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-    dm_set(map, dest_bm, gen_join(c.sel, src[i], 0), c.ctl);
+  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+    const u64 i = i0 + threadIdx.x;
+    const bool valid = i < n;
+    emit_warp(map, T, valid, valid ? gen_join(c.sel, src[i], 0) : 0, c.ctl);
+  }
   if (launch_rec_finish(c.rec) && threadIdx.x == 0) {
     if (c.once_pending) *c.once_pending = 1;
     prof_add(c.ctl, kPCopy, 8 * n);
   }
 }
 
-// RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT).  The
-// destination bitmap is cleared by a k_bm_clear launched just before.
-__global__ void __launch_bounds__(256) k_acopy_bm(const u32 *src_bm, Sel2 sel, u32 *dest_bm,
-                                                  DenseMap map, Ctl *ctl) {
+// RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT); the
+// destination was reset by k_newt_reset just before.  The source NEWT is
+// its list when it has one, else its bitmap.
+__global__ void __launch_bounds__(256) k_acopy_bm(const RelDev *src_rd, Sel2 sel, RelDev *dest_rd,
+                                                  int dest_rel, DenseMap map, Ctl *ctl) {
   if (ctl_stop(ctl)) return;
+  const EmitTarget T = emit_target(dest_rd, dest_rel);
+  if (src_rd->emit == kEmitNewt) {
+    const u64 n = src_rd->newt.n;
+    const u64 *src = src_rd->newt.ptr;
+    for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+      const u64 i = i0 + threadIdx.x;
+      const bool valid = i < n;
+      emit_warp(map, T, valid, valid ? gen_join(sel, src[i], 0) : 0, ctl);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, 8 * n);
+    return;
+  }
+  const u32 *src_bm = src_rd->bmG;
   for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < map.words;
        w += (u64)gridDim.x * blockDim.x) {
     u32 x = src_bm[w];
@@ -441,10 +566,81 @@ __global__ void __launch_bounds__(256) k_acopy_bm(const u32 *src_bm, Sel2 sel, u
     while (x) {
       const int b = __ffs(x) - 1;
       x &= x - 1;
-      dm_set(map, dest_bm, gen_join(sel, dm_key(map, inst, seg, w, b), 0), ctl);
+      emit_one(map, T, gen_join(sel, dm_key(map, inst, seg, w, b), 0), ctl);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, map.words * 4);
+}
+
+// Update step of an emitting relation.  kEmitDelta: delta_next already is
+// DELTA; kEmitNewt: DELTA = the NEWT keys not in FULL.  Then FULL |= DELTA
+// in place and the NEWT bitmap is cleared word by word from the list (its
+// bits are exactly the listed keys).  With inst_delta set, each instance
+// that gained a key is flagged.
+__global__ void __launch_bounds__(256) k_emit_update(RelDev *rd, int rel, DenseMap map,
+                                                     u64 *inst_delta, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const bool from_newt = rd->emit == kEmitNewt;
+  const DArr &L = from_newt ? rd->newt : rd->delta_next;
+  const u64 n = L.n;
+  const u64 *keys = L.ptr;
+  u32 *F = rd->bmF, *G = rd->bmG;
+  DArr *D = &rd->delta_next;
+  u64 *dptr = D->ptr;
+  const u64 dcap = D->cap;
+  const int lane = threadIdx.x & 31;
+  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+    const u64 i = i0 + threadIdx.x;
+    bool add = false;
+    u64 key = 0, w = 0;
+    u32 b = 0;
+    if (i < n) {
+      key = keys[i];
+      if (dm_locate(map, key, &w, &b) && w < map.words) {
+        G[w] = 0;
+        add = !from_newt || !((F[w] >> b) & 1u);
+      } else {
+        atomicOr(&ctl->oob, 8192u);
+      }
+    }
+    if (add) {
+      atomicOr(F + w, 1u << b);
+      if (inst_delta) inst_delta[key_c0(key) >> map.seg_shift] = 1;
+    }
+    if (from_newt) {
+      const unsigned am = __ballot_sync(0xffffffffu, add);
+      if (am) {
+        const int leader = __ffs(am) - 1;
+        u64 base = 0;
+        if (lane == leader) base = atomicAdd(&D->n, (u64)__popc(am));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (add) {
+          const u64 pos = base + __popc(am & ((1u << lane) - 1u));
+          if (pos < dcap) {
+            dptr[pos] = key;
+          } else {
+            atomicMax(&ctl->need[need_index(rel, kNeedDelta)], pos + 1);
+            atomicOr(&ctl->oob, 16384u);  // cannot happen: delta_next >= newt
+          }
+        }
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 16 * n);
+}
+
+// Clear a NEWT bitmap word by word from its list (tmp relations at the end
+// of an iteration).
+__global__ void __launch_bounds__(256) k_newt_unset(RelDev *rd, DenseMap map, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u64 n = rd->newt.n;
+  const u64 *keys = rd->newt.ptr;
+  u32 *G = rd->bmG;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    u64 w;
+    u32 b;
+    if (dm_locate(map, keys[i], &w, &b) && w < map.words) G[w] = 0;
+  }
 }
 
 // Batched form: an instance whose update relations produced new tuples in

@@ -563,6 +563,7 @@ struct Plan {
   std::vector<char> full_idx, delta_idx;  // per relation: index needed
   std::vector<char> full_list;            // FULL read as a list by some op
   std::vector<char> newt_list;            // NEWT read as a join outer
+  std::vector<char> acopy_src;            // NEWT read by an ACopy
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -572,7 +573,9 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.delta_idx.assign(n, 0);
   p.full_list.assign(n, 0);
   p.newt_list.assign(n, 0);
+  p.acopy_src.assign(n, 0);
   for (const OpHost &op : L.ops) {
+    if (op.kind == 2) p.acopy_src[op.inner] = 1;
     if (op.kind == 0) {
       (op.inner_ver == GDL_DELTA ? p.delta_idx : p.full_idx)[op.inner] = 1;
       if (op.inner_ver != GDL_DELTA) p.full_list[op.inner] = 1;
@@ -622,13 +625,12 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
   const u64 words = dense ? map.words : 0;
   PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
   if (dense) {
-    // NEWT of every update and tmp relation starts empty.
+    // NEWT of every scan-path relation starts empty (emitting relations
+    // clear their NEWT bitmap from their list in the update step).
     for (int r : L.update)
-      PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                e->h[r].bmG, words, e->d_ctl));
-    for (int r : L.tmps)
-      PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                e->h[r].bmG, words, e->d_ctl));
+      if (e->h[r].emit == kEmitNone)
+        PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+                                  e->h[r].bmG, words, e->d_ctl));
   }
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
@@ -645,7 +647,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       } else {
         a.outer = &R[op.outer].newt;
         a.outer_vis = nullptr;
-        if (dense && oh.bmG) {
+        if (dense && oh.bmG && oh.emit != kEmitNewt) {
           // NEWT as a join outer: the sorted list of its bitmap.
           BmScanArgs c = scan_none(map);
           c.g = oh.bmG;
@@ -690,7 +692,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       const u64 out_cap = e->h[op.out].newt.cap;
       if (dense)
         PLAUNCH(kc, kPJoinMat,
-                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, e->h[op.out].bmG, map));
+                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, &R[op.out], map));
       else if (op.pred.kind)
         PLAUNCH(kc, kPJoinMat,
                 k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b));
@@ -723,15 +725,15 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
       if (dense && op.kind == 2) {
         // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
-        u32 *dbm = e->h[op.out].bmG;
-        PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                  dbm, words, e->d_ctl));
+        PLAUNCH(kc, kPBitmap, k_newt_reset<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+                                  &R[op.out], map, e->d_ctl));
         if (sh.bmG)  // a source without a NEWT bitmap (static) has an empty NEWT
-          PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, words, 256, 8), 256, 0, s>>>(
-                                  sh.bmG, op.sel, dbm, map, e->d_ctl));
+          PLAUNCH(kc, kPCopy,
+                  k_acopy_bm<<<grid_for(e, std::max(words, sh.newt.cap), 256, 8), 256, 0, s>>>(
+                      &R[op.inner], op.sel, &R[op.out], op.out, map, e->d_ctl));
       } else if (dense) {
         PLAUNCH(kc, kPCopy, k_copy_bm<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
-                                c, e->h[op.out].bmG, map));
+                                c, &R[op.out], map));
       } else {
         PLAUNCH(kc, kPCopy,
                 k_copy<<<grid_for(e, cap / 2 + 1, kMatBlock, 8), kMatBlock, 0, s>>>(c));
@@ -748,8 +750,12 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
+  // Scan-path and sort-path relations first: a capacity overflow there is
+  // resumed by running this step again, which is only correct while no
+  // emitting relation has updated its FULL bitmap in place yet.
   for (int r : L.update) {
     const RelDev &rh = e->h[r];
+    if (dense && rh.emit != kEmitNone) continue;
     if (dense) {
       // DELTA = NEWT \ FULL, FULL' = FULL | NEWT, both sorted; FULL's list
       // and index only when some op reads them during the loop.
@@ -803,6 +809,20 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
               k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
                   &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl));
     }
+  }
+  if (dense) {
+    // Emitting relations: FULL |= DELTA in place, NEWT bitmap cleared from
+    // the list; tmp relations' NEWT bitmaps likewise.
+    for (int r : L.update) {
+      const RelDev &rh = e->h[r];
+      if (rh.emit == kEmitNone) continue;
+      const u64 cap = rh.emit == kEmitNewt ? rh.newt.cap : rh.delta_next.cap;
+      PLAUNCH(kc, kPBitmap, k_emit_update<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
+                                &R[r], r, L.map, L.d_inst_delta, e->d_ctl));
+    }
+    for (int r : L.tmps)
+      PLAUNCH(kc, kPBitmap, k_newt_unset<<<grid_for(e, e->h[r].newt.cap, 256, 8), 256, 0, s>>>(
+                                &R[r], L.map, e->d_ctl));
   }
   if (L.d_inst_delta)
     PLAUNCH(kc, kPControl, k_inst_track<<<grid_for(e, L.n_inst, 256, 1), 256, 0, s>>>(
@@ -976,7 +996,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     L.dense = e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits);
     L.dk = L.dense && !e->instances ? dk : 0;
   }
-  for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+  for (RelDev &h : e->h) h.dense = h.full_lazy = h.emit = 0;
   if (L.dense) {
     if (e->instances) {
       L.map = DenseMap{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
@@ -999,12 +1019,19 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     const u64 words = L.map.words;
     for (int r : L.update) {
       TRY(ensure_bitmaps(e, r, words, true));
-      e->h[r].dense = 1;
-      e->h[r].full_lazy = !plan.full_list[r];
+      RelDev &h = e->h[r];
+      h.dense = 1;
+      h.full_lazy = !plan.full_list[r];
+      // FULL not read as a list and DELTA not probed: the ops list DELTA
+      // (or NEWT, when an op reads NEWT) themselves.
+      h.emit = (plan.full_list[r] || plan.delta_idx[r])
+                   ? kEmitNone
+                   : (plan.newt_list[r] || plan.acopy_src[r]) ? kEmitNewt : kEmitDelta;
     }
     for (int r : L.tmps) {
       TRY(ensure_bitmaps(e, r, words, false));
       e->h[r].dense = 1;
+      e->h[r].emit = kEmitNewt;
     }
     TRY(ensure_dense_scratch(e, words));
     // Every list of the loop is bounded by the key domain: size them for
@@ -1014,7 +1041,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     size_t free_b = 0, total_b = 0;
     CK(e, cudaMemGetInfo(&free_b, &total_b));
     u64 lists = 0;
-    for (int r : L.update) lists += 2 + (plan.newt_list[r] ? 1 : 0) + (plan.full_list[r] ? 2 : 0);
+    for (int r : L.update)
+      lists += 2 + ((plan.newt_list[r] || plan.acopy_src[r]) ? 1 : 0) +
+               (plan.full_list[r] ? 2 : 0);
     lists += L.tmps.size();
     const u64 domain = words * 32;
     const u64 cap = std::min<u64>(
@@ -1023,7 +1052,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       RelDev &h = e->h[r];
       TRY(ensure_arr(e, h.delta, cap, true));
       TRY(ensure_arr(e, h.delta_next, cap, false));
-      if (plan.newt_list[r]) TRY(ensure_arr(e, h.newt, cap, false));
+      if (plan.newt_list[r] || plan.acopy_src[r]) TRY(ensure_arr(e, h.newt, cap, false));
       if (plan.full_list[r]) {
         TRY(ensure_arr(e, h.full, cap, true));
         TRY(ensure_arr(e, h.full_next, cap, false));
@@ -1184,6 +1213,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       memset(c.need, 0, sizeof c.need);
       L.retries++;
       L.graph_dirty = true;
+      if (L.dense && !resume) {
+        // The iteration runs again from its start: its NEWT bitmaps must
+        // be empty again (emitting relations clear them only on success).
+        const u64 words = L.map.words;
+        for (int r : L.update) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+        for (int r : L.tmps) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+      }
       if (resume) {
         // Re-run only the update step and the commit of the iteration that
         // overflowed, launch by launch, until its lists fit.
@@ -1275,7 +1311,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       CK(e, cudaGetLastError());
       TRY(pull(e));
     }
-    for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+    for (RelDev &h : e->h) h.dense = h.full_lazy = h.emit = 0;
     TRY(push(e));
     c.iteration = kept_iteration;
   }
