@@ -50,6 +50,14 @@ struct Index {
   u32 hash_mode;  // 0: identity (c0 & mask), 1: 64-bit mixer
 };
 
+// Totals of one bitmap scan (dense.cuh).
+struct BmScanRec {
+  u64 total_a, total_b;  // list sizes
+  u64 pop_g;             // popcount of NEWT (accumulated, reset by the write pass)
+  u32 overflow;          // a list is too small
+  u32 pad;
+};
+
 // One instance of a batched LIE in the dense (bitmap) form: its rows start at
 // word base_word, each 2^row_shift words long, n rows (= n local ids).
 struct SegInfo {
@@ -74,19 +82,16 @@ struct RelDev {
   u64 c_newt_n;  // NEWT count seen by the last merge step (0: empty branch)
   u32 sorted_in_scratch;
   u32 pad;
-  // Dense form (dense.cuh): FULL bitmap, its next version, NEWT bitmap.
-  u32 *bmF, *bmF_next, *bmG;
+  // Dense form (dense.cuh): FULL bitmap, NEWT bitmap and the dirty map of
+  // NEWT (one bit per 64-word chunk), the tile counts / prefixes of this
+  // relation's update scan and its record.
+  u32 *bmF, *bmG, *bmD;
+  u64 *tile_prefix;
+  BmScanRec scan;
   u64 f_count;     // |FULL'| when the FULL list is not rebuilt every iteration
   u32 dense;       // the running LIE keeps this relation as bitmaps
   u32 full_lazy;   // FULL's list is materialised only when the LIE ends
-  // Emission (dense.cuh): 0 = the update step scans the bitmaps;
-  // kEmitDelta = ops append new keys (not in FULL) to delta_next as they
-  // set them; kEmitNewt = ops append every first-set key to the NEWT list.
-  u32 emit;
-  u32 pad2;
-  u64 gen_count;   // tuples generated this iteration (kEmitDelta: NEWT non-empty?)
 };
-enum EmitMode { kEmitNone = 0, kEmitDelta = 1, kEmitNewt = 2 };
 
 // Loop control of a running fixpoint (one per engine, device memory).
 struct Ctl {

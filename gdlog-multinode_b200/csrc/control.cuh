@@ -32,8 +32,6 @@ __global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
     r.w_full_vis = r.full_vis;
     r.w_delta_vis = r.delta_vis;
     r.newt.n = 0;
-    r.gen_count = 0;
-    if (r.emit == kEmitDelta) r.delta_next.n = 0;  // the ops list DELTA here
   }
   for (int i = 0; i < L->n_static; i++) {
     RelDev &r = rels[L->statics[i]];
@@ -66,12 +64,8 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
     for (int i = 0; i < L->n_update; i++) {
       RelDev &r = rels[L->update[i]];
       u64 *tr = (L->trace && row < ctl->trace_rows) ? L->trace + (row * L->n_update + i) * 3 : 0;
-      // Dense form: the scan wrote FULL | NEWT into bmF_next (dense.cuh);
-      // emitting relations updated bmF in place and know NEWT's size from
-      // their own counters.
-      if (r.dense && r.emit == kEmitNone) dswap(r.bmF, r.bmF_next);
-      if (r.dense && r.emit == kEmitDelta) r.c_newt_n = r.gen_count;
-      if (r.dense && r.emit == kEmitNewt) r.c_newt_n = r.newt.n;
+      // (Dense form: the update scan has already merged NEWT into the FULL
+      // bitmap in place, dense.cuh.)
       if (r.c_newt_n == 0) {
         // src/lie.cu:114-121: no new tuple -> a fresh, empty DELTA.
         r.delta.n = 0;
@@ -88,10 +82,8 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
         r.delta_vis = 1;
         if (r.delta.n) {
           // flush_delta (src/relation.cu:405-521): FULL := FULL ∪ DELTA.
-          if (r.dense && r.emit != kEmitNone) {
+          if (r.dense && r.full_lazy) {
             r.full.n += r.delta.n;  // the list is written when the LIE ends
-          } else if (r.dense && r.full_lazy) {
-            r.full.n = r.f_count;  // the list is written when the LIE ends
           } else {
             dswap(r.full, r.full_next);
             dswap(r.full_idx, r.full_idx_next);

@@ -8,16 +8,19 @@
 // directly.  This replaces, for such domains, the sort -> unique ->
 // set_difference -> merge sequence of the reference's update step
 // (src/lie.cu:122-185, src/relation.cu:405-521, src/join.cu:160-225):
-//   * joins and copies test-and-set bits of the output relation's NEWT
-//     bitmap G (atomicOr), so the raw join output -- often tens of times
-//     larger than its distinct tuples -- is never written to memory;
-//   * one streaming pass over (G, F) per relation then yields DELTA =
-//     G & ~F and FULL' = F | G as sorted lists, the next FULL bitmap, and
-//     the run index of FULL' from per-row popcounts.
-// Each scan is two kernels: k_bm_count computes per-tile counts and their
-// exclusive prefixes (decoupled look-back) and checks the output
-// capacities; k_bm_write writes.  Nothing but idempotent bit-sets happens
-// before a capacity check, so an iteration that overflows can be re-run.
+//   * joins and copies set bits of the output relation's NEWT bitmap G with
+//     fire-and-forget atomicOr (no return value, so no round trip), plus a
+//     bit in a small dirty map (one bit per 64-word chunk of G);
+//   * the update step reads only the dirty chunks of G: DELTA = G & ~F as a
+//     sorted list, FULL |= G in place, G cleared.  A relation whose FULL
+//     list is read during the loop also gets FULL' = F | G as a sorted list
+//     and its run index from per-row popcounts (a full pass over F).
+// A scan is three kernels: k_bm_tilecount (per 2048-word tile, clean tiles
+// skipped by their dirty word), k_bm_scan (exclusive prefix of the tile
+// counts, totals, capacity check) and k_bm_write.  All update relations are
+// counted and checked before any of them is written (k_scan_gate), so a
+// capacity overflow leaves every bitmap untouched and the update step can
+// simply run again after the lists grow.
 //
 // Batched form.  Many independent instances of one program can share one
 // LIE: instance i owns the ids (i << S) | local, local < n_i, and its
@@ -36,6 +39,7 @@ namespace gdl {
 constexpr int kBmBlock = 256;
 constexpr int kBmWordsPerThread = 8;
 constexpr int kBmTileWords = kBmBlock * kBmWordsPerThread;  // 2048 words = 65536 keys
+constexpr int kBmChunkWords = 64;                          // dirty granularity (256 B)
 constexpr int kDenseMaxDomainBits = 30;
 constexpr int kMaxInstanceNodes = 1 << 16;  // a row is at most one scan tile
 
@@ -47,7 +51,7 @@ struct DenseMap {
   const u32 *tile_inst;   // instance of each scan tile (null: all instance 0)
   u32 n_inst;
   int seg_shift;          // 31 for the square domain (every id is local)
-  u64 words;              // total bitmap words
+  u64 words;              // total bitmap words (a multiple of kBmTileWords)
 };
 
 __device__ __forceinline__ bool dm_locate(const DenseMap &m, u64 key, u64 *word, u32 *bit) {
@@ -76,13 +80,19 @@ __device__ __forceinline__ u64 dm_key(const DenseMap &m, u32 inst, const SegInfo
   return make_key(hi | lx, hi | lz);
 }
 
+// The dirty map has one u32 per scan tile, one bit per 64-word chunk.
+__device__ __forceinline__ void bm_mark(u32 *bm, u32 *dirty, u64 w, u32 b) {
+  atomicOr(bm + w, 1u << b);
+  if (dirty) atomicOr(dirty + w / kBmTileWords, 1u << ((w / kBmChunkWords) & 31u));
+}
+
 // Set the bit of one key; keys outside their instance's range are dropped
 // and recorded in Ctl::oob instead of being written.
-__device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u64 key, Ctl *ctl) {
+__device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u32 *dirty, u64 key, Ctl *ctl) {
   u64 w;
   u32 b;
   if (dm_locate(m, key, &w, &b) && w < m.words)
-    atomicOr(bm + w, 1u << b);
+    bm_mark(bm, dirty, w, b);
   else
     atomicOr(&ctl->oob, 8192u);
 }
@@ -93,34 +103,26 @@ __device__ __forceinline__ u32 bm_eval(int ex, u32 g, u32 f) {
   return ex == kBmDelta ? (g & ~f) : ex == kBmUnion ? (f | g) : 0u;
 }
 
-struct BmScanRec {
-  u64 total_a, total_b;  // list sizes
-  u64 pop_g;             // popcount of g (accumulated, reset by k_bm_write)
-  u32 overflow;
-  u32 pad;
-};
-
 struct BmScanArgs {
   const u32 *g;    // NEWT bitmap (may be null: all zero)
-  const u32 *f;    // FULL bitmap (may be null: all zero)
-  u32 *f_next;     // if set: receives f | g
-  // If set, g / f / f_next are this relation's bmG / bmF / bmF_next, read
-  // from the device descriptor when the kernel starts: k_commit swaps bmF
-  // and bmF_next on the device, so pointers captured in a graph would go
-  // stale.
+  u32 *f;          // FULL bitmap (may be null: all zero)
+  // If set, g / f / dirty are this relation's bmG / bmF / bmD, read from the
+  // device descriptor when the kernel starts.
   const RelDev *rd;
+  u32 *dirty;      // dirty map of g
+  int skip_clean;  // read only dirty chunks (every expression is 0 where g is)
+  int inplace;     // write pass: f |= g, g := 0 and dirty := 0 in dirty chunks
   DenseMap map;
   int ex_a, ex_b;  // expressions for list a and list b
   DArr *list_a;    // output lists (sorted keys); null when not wanted
   DArr *list_b;
   Index *idx_b;    // if set: run index of list b
-  u64 *count_b;    // if set: receives total_b (FULL count without a list)
+  u64 *count_b;    // if set: receives total_b (a count without a list)
   u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
   u64 *inst_delta; // if set: per-instance count of list a is added here
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
-  int update_stage;    // an update-step scan: its overflow can be resumed
-  u64 *tile_prefix;    // [tiles] packed exclusive prefix (a << 32 | b)
-  u64 tiles_cap;
+  int gated;           // the overflow is raised by k_scan_gate, not by k_bm_write
+  u64 *tile_prefix;    // [tiles] tile counts, then their exclusive prefix (a << 32 | b)
   BmScanRec *rec;
   LaunchRec *lrec;
   Lb lb;
@@ -131,54 +133,116 @@ __device__ __forceinline__ u64 bm_tiles(u64 words) {
   return (words + kBmTileWords - 1) / kBmTileWords;
 }
 
-// Pass 1: per-tile counts, exclusive prefixes by decoupled look-back, and
-// the capacity check (recorded in rec->overflow for k_bm_write to raise).
-__global__ void __launch_bounds__(kBmBlock) k_bm_count(BmScanArgs a) {
-  __shared__ u64 s_scan[kBmBlock / 32];
-  __shared__ long long s_tile;
-  if (ctl_stop(a.ctl)) return;
-  const u64 words = a.map.words;
-  const u64 tiles = bm_tiles(words);
-  if (tiles > a.tiles_cap) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->oob, 1024u);
-    return;
-  }
+__device__ __forceinline__ void scan_bind(BmScanArgs &a) {
   if (a.rd) {
     a.g = a.rd->bmG;
     a.f = a.rd->bmF;
-    a.f_next = a.rd->bmF_next;
+    a.dirty = a.rd->bmD;
   }
-  const u32 gen = a.lrec->gen;
+}
+
+// Pass 1: packed (a, b) counts of every tile.  A block takes 32 tiles (one
+// warp reads their 32 dirty words); clean tiles are skipped when allowed.
+__global__ void __launch_bounds__(kBmBlock) k_bm_tilecount(BmScanArgs a) {
+  __shared__ u32 s_dirty[32];
+  __shared__ u32 s_red[2][kBmBlock / 32];
+  if (ctl_stop(a.ctl)) return;
+  scan_bind(a);
+  const u64 words = a.map.words;
+  const u64 tiles = bm_tiles(words);
+  const u64 groups = (tiles + 31) / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 my_g = 0;
-  while (true) {
-    const long long tile = grab_tile(a.lrec, &s_tile);
-    if (tile >= (long long)tiles) break;
-    const u64 w0 = (u64)tile * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
-    u32 ca = 0, cb = 0;
-#pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u64 w = w0 + i;
-      if (w < words) {
-        const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
-        ca += __popc(bm_eval(a.ex_a, g, f));
-        cb += __popc(bm_eval(a.ex_b, g, f));
-        my_g += __popc(g);
+  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+    __syncthreads();
+    if (warp == 0) {
+      const u64 t = grp * 32 + lane;
+      s_dirty[lane] = t < tiles ? ((a.skip_clean && a.dirty) ? a.dirty[t] : 0xFFFFFFFFu) : 0u;
+    }
+    __syncthreads();
+    for (int k = 0; k < 32; k++) {
+      const u64 tile = grp * 32 + k;
+      if (tile >= tiles) break;
+      const u32 d = s_dirty[k];
+      if (!d) {
+        if (threadIdx.x == 0) a.tile_prefix[tile] = 0;
+        continue;
       }
+      const u64 w0 = tile * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+      u32 ca = 0, cb = 0;
+      if ((d >> (threadIdx.x / (kBmChunkWords / kBmWordsPerThread))) & 1u) {
+#pragma unroll
+        for (int i = 0; i < kBmWordsPerThread; i++) {
+          const u64 w = w0 + i;
+          const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
+          ca += __popc(bm_eval(a.ex_a, g, f));
+          cb += __popc(bm_eval(a.ex_b, g, f));
+          my_g += __popc(g);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ca += __shfl_xor_sync(0xffffffffu, ca, o);
+        cb += __shfl_xor_sync(0xffffffffu, cb, o);
+      }
+      if (lane == 0) {
+        s_red[0][warp] = ca;
+        s_red[1][warp] = cb;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        u64 ta = 0, tb = 0;
+        for (int w = 0; w < kBmBlock / 32; w++) {
+          ta += s_red[0][w];
+          tb += s_red[1][w];
+        }
+        a.tile_prefix[tile] = (ta << 32) | tb;
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_g += __shfl_xor_sync(0xffffffffu, my_g, o);
+  if (lane == 0 && my_g) atomicAdd(&a.rec->pop_g, my_g);
+}
+
+// Pass 2: exclusive prefix of the tile counts in place (decoupled
+// look-back over chunks of 2048 tiles), totals and the capacity check.
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kBmBlock * kScanItems;
+
+__global__ void __launch_bounds__(kBmBlock) k_bm_scan(BmScanArgs a) {
+  __shared__ u64 s_scan[kBmBlock / 32];
+  __shared__ long long s_tile;
+  __shared__ u64 s_base;
+  if (ctl_stop(a.ctl)) return;
+  const u64 tiles = bm_tiles(a.map.words);
+  const u64 chunks = (tiles + kScanChunk - 1) / kScanChunk;
+  const u32 gen = a.lrec->gen;
+  while (true) {
+    const long long c = grab_tile(a.lrec, &s_tile);
+    if (c >= (long long)chunks) break;
+    const u64 t0 = (u64)c * kScanChunk + (u64)threadIdx.x * kScanItems;
+    u64 v[kScanItems], sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+      v[i] = t0 + i < tiles ? a.tile_prefix[t0 + i] : 0;
+      sum += v[i];
     }
     u64 tot;
-    block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, s_scan, &tot);
+    const u64 ex = block_excl_scan<kBmBlock>(sum, s_scan, &tot);
     if (threadIdx.x < 32) {
       u64 prefix = 0;
-      if (tile == 0) {
-        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, true, tot);
+      if (c == 0) {
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, true, tot);
       } else {
-        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, false, tot);
-        prefix = lb_warp_prefix(a.lb, tile, gen, a.ctl);
-        if (threadIdx.x == 0) lb_publish(a.lb, tile, gen, true, prefix + tot);
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, false, tot);
+        prefix = lb_warp_prefix(a.lb, c, gen, a.ctl);
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, true, prefix + tot);
       }
       if (threadIdx.x == 0) {
-        a.tile_prefix[tile] = prefix;
-        if ((u64)tile == tiles - 1) {
+        s_base = prefix;
+        if ((u64)c == chunks - 1) {
           const u64 ta = (prefix + tot) >> 32, tb = (prefix + tot) & 0xFFFFFFFFull;
           a.rec->total_a = ta;
           a.rec->total_b = tb;
@@ -195,17 +259,37 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_count(BmScanArgs a) {
         }
       }
     }
-  }
+    __syncthreads();
+    u64 run = s_base + ex;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) my_g += __shfl_xor_sync(0xffffffffu, my_g, o);
-  if ((threadIdx.x & 31) == 0 && my_g) atomicAdd(&a.rec->pop_g, my_g);
+    for (int i = 0; i < kScanItems; i++) {
+      if (t0 + i < tiles) a.tile_prefix[t0 + i] = run;
+      run += v[i];
+    }
+  }
   launch_rec_finish(a.lrec);
 }
 
-// Pass 2: write list a, list b (+ its index) and f_next.
+// After the count and scan passes of every update relation: raise an
+// overflow before any relation's bitmaps are written.
+__global__ void k_scan_gate(RelDev *rels, const int *update, int n_update, Ctl *ctl) {
+  if (threadIdx.x != 0 || ctl_stop(ctl)) return;
+  for (int i = 0; i < n_update; i++) {
+    RelDev &r = rels[update[i]];
+    if (r.dense && r.scan.overflow) {
+      ctl->overflow_stage = 1;
+      atomicExch(&ctl->overflow, 1u);
+    }
+  }
+}
+
+// Pass 3: write list a, list b (+ its index), update f in place and clear g
+// in the dirty chunks.  Tiles are visited 32 at a time as in pass 1.
 struct BmWriteSmem {
   u32 off_b[kBmTileWords + 1];  // exclusive offsets of list b per word
   u64 scan_tmp[kBmBlock / 32];
+  u32 dirty[32];   // chunks to read per tile of the group
+  u32 dclear[32];  // dirty chunks per tile (g is non-zero only there)
 };
 
 __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
@@ -214,100 +298,118 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   if (a.rec->overflow) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.rec->pop_g = 0;
-      if (a.update_stage) a.ctl->overflow_stage = 1;
-      atomicExch(&a.ctl->overflow, 1u);
+      if (!a.gated) atomicExch(&a.ctl->overflow, 1u);
     }
     return;
   }
+  scan_bind(a);
   const u64 words = a.map.words;
   const u64 tiles = bm_tiles(words);
-  if (tiles > a.tiles_cap) return;
-  if (a.rd) {
-    a.g = a.rd->bmG;
-    a.f = a.rd->bmF;
-    a.f_next = a.rd->bmF_next;
-  }
+  const u64 groups = (tiles + 31) / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const u32 epoch = (u32)(a.ctl->generation + 1);
   const Index ix = a.idx_b ? *a.idx_b : Index{};
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.idx_b) a.idx_b->epoch = epoch;
   u64 *la = a.list_a ? a.list_a->ptr : nullptr;
   u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
   const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
-  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const u64 prefix = a.tile_prefix[tile];
-    const u64 wt = tile * kBmTileWords;
-    const u32 inst = dm_tile_inst(a.map, tile);
-    const SegInfo seg = a.map.seg[inst];
-    const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
-    u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
-    u32 ca = 0, cb = 0;
-#pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u64 w = w0 + i;
-      u32 g = 0, f = 0;
-      if (w < words) {
-        g = a.g ? a.g[w] : 0u;
-        f = a.f ? a.f[w] : 0u;
-        if (a.f_next) a.f_next[w] = f | g;
-      }
-      ea[i] = bm_eval(a.ex_a, g, f);
-      eb[i] = bm_eval(a.ex_b, g, f);
-      ca += __popc(ea[i]);
-      cb += __popc(eb[i]);
-    }
-    u64 tot;
-    const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
-    if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
-    u64 pa = (prefix >> 32) + (ex >> 32);
-    u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
-    u32 ob = (u32)(ex & 0xFFFFFFFFull);
-#pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) {
-      if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
-      ob += __popc(eb[i]);
-      u32 x = la ? ea[i] : 0u;
-      while (x) {
-        const int b = __ffs(x) - 1;
-        x &= x - 1;
-        if (pa < cap_a)
-          la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
-        else
-          atomicOr(&a.ctl->oob, 2048u);
-        pa++;
-      }
-      x = lb ? eb[i] : 0u;
-      while (x) {
-        const int b = __ffs(x) - 1;
-        x &= x - 1;
-        if (pb < cap_b)
-          lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
-        else
-          atomicOr(&a.ctl->oob, 4096u);
-        pb++;
-      }
-    }
-    if (a.idx_b) {
-      if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
-      __syncthreads();
-      // One slot per non-empty row of the tile: {c0, epoch, start, len}.
-      // Rows are 2^row_shift words, at most one tile, aligned in the tile.
-      const u32 rs = seg.row_shift;
-      const u64 row_words = 1ull << rs;
-      const u64 rows = kBmTileWords >> rs;
-      const u32 hi = a.map.seg_shift >= 31 ? 0u : (inst << a.map.seg_shift);
-      for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
-        const u64 lw = r << rs;  // first word of the row in the tile
-        if (wt + lw >= words || wt + lw < seg.base_word) break;
-        const u64 row = (wt + lw - seg.base_word) >> rs;
-        if (row >= seg.n) break;
-        const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
-        if (len) {
-          const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
-          index_insert(ix, epoch, hi | (u32)row, start, len, a.ctl);
-        }
-      }
+  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+    __syncthreads();
+    if (warp == 0) {
+      const u64 t = grp * 32 + lane;
+      const u32 d = (t < tiles && a.dirty) ? a.dirty[t] : 0u;
+      sm.dirty[lane] = t < tiles ? (a.skip_clean ? d : 0xFFFFFFFFu) : 0u;
+      sm.dclear[lane] = d;
+      if (a.inplace && d) a.dirty[t] = 0;
     }
     __syncthreads();
+    for (int k = 0; k < 32; k++) {
+      const u64 tile = grp * 32 + k;
+      if (tile >= tiles) break;
+      const u32 d = sm.dirty[k];
+      if (!d) continue;
+      const u32 dclr = sm.dclear[k];
+      const u64 prefix = a.tile_prefix[tile];
+      const u64 wt = tile * kBmTileWords;
+      const u32 inst = dm_tile_inst(a.map, tile);
+      const SegInfo seg = a.map.seg[inst];
+      const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
+      const int chunk = threadIdx.x / (kBmChunkWords / kBmWordsPerThread);
+      const bool read = (d >> chunk) & 1u;
+      const bool clr = a.inplace && ((dclr >> chunk) & 1u);
+      u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
+      u32 ca = 0, cb = 0;
+#pragma unroll
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        const u64 w = w0 + i;
+        u32 g = 0, f = 0;
+        if (read) {
+          g = a.g ? a.g[w] : 0u;
+          f = a.f ? a.f[w] : 0u;
+          if (clr) {
+            if (g) a.f[w] = f | g;
+            const_cast<u32 *>(a.g)[w] = 0u;
+          }
+        }
+        ea[i] = bm_eval(a.ex_a, g, f);
+        eb[i] = bm_eval(a.ex_b, g, f);
+        ca += __popc(ea[i]);
+        cb += __popc(eb[i]);
+      }
+      u64 tot;
+      const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
+      if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
+      u64 pa = (prefix >> 32) + (ex >> 32);
+      u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
+      u32 ob = (u32)(ex & 0xFFFFFFFFull);
+#pragma unroll
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
+        ob += __popc(eb[i]);
+        u32 x = la ? ea[i] : 0u;
+        while (x) {
+          const int b = __ffs(x) - 1;
+          x &= x - 1;
+          if (pa < cap_a)
+            la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
+          else
+            atomicOr(&a.ctl->oob, 2048u);
+          pa++;
+        }
+        x = lb ? eb[i] : 0u;
+        while (x) {
+          const int b = __ffs(x) - 1;
+          x &= x - 1;
+          if (pb < cap_b)
+            lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
+          else
+            atomicOr(&a.ctl->oob, 4096u);
+          pb++;
+        }
+      }
+      if (a.idx_b) {
+        if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
+        __syncthreads();
+        // One slot per non-empty row of the tile: {c0, epoch, start, len}.
+        // Rows are 2^row_shift words, at most one tile, aligned in the tile.
+        const u32 rs = seg.row_shift;
+        const u64 row_words = 1ull << rs;
+        const u64 rows = kBmTileWords >> rs;
+        const u32 hi = a.map.seg_shift >= 31 ? 0u : (inst << a.map.seg_shift);
+        for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
+          const u64 lw = r << rs;  // first word of the row in the tile
+          if (wt + lw >= words || wt + lw < seg.base_word) break;
+          const u64 row = (wt + lw - seg.base_word) >> rs;
+          if (row >= seg.n) break;
+          const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
+          if (len) {
+            const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
+            index_insert(ix, epoch, hi | (u32)row, start, len, a.ctl);
+          }
+        }
+      }
+      __syncthreads();
+    }
   }
   if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
     if (a.list_a) a.list_a->n = a.rec->total_a;
@@ -315,126 +417,68 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     if (a.count_b) *a.count_b = a.rec->total_b;
     if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
     a.rec->pop_g = 0;
-    prof_add(a.ctl, kPBitmap,
-             words * 4 * ((a.g ? 2 : 0) + (a.f ? 2 : 0) + (a.f_next ? 1 : 0)) +
-                 8 * (a.rec->total_a + a.rec->total_b));
+    prof_add(a.ctl, kPBitmap, 8 * (a.rec->total_a + a.rec->total_b));
   }
 }
 
-// Zero a bitmap (words a multiple of 4).
-__global__ void __launch_bounds__(256) k_bm_clear(u32 *bm, u64 words, Ctl *ctl) {
+// Zero a NEWT bitmap in its dirty chunks and clear the dirty map (one block
+// per 32 tiles).  With only_if_empty, only when that source is empty (a
+// Copy from an empty source empties its destination, src/copy.cu:24-27).
+__global__ void __launch_bounds__(256) k_bm_clear_dirty(const RelDev *rd, DenseMap map, Ctl *ctl) {
+  __shared__ u32 s_d[32];
   if (ctl_stop(ctl)) return;
-  uint4 *p = reinterpret_cast<uint4 *>(bm);
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < words / 4;
-       i += (u64)gridDim.x * blockDim.x)
-    p[i] = make_uint4(0, 0, 0, 0);
-  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, words * 4);
+  u32 *G = rd->bmG, *D = rd->bmD;
+  const u64 tiles = bm_tiles(map.words);
+  const u64 groups = (tiles + 31) / 32;
+  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const u64 t = grp * 32 + threadIdx.x;
+      s_d[threadIdx.x] = t < tiles ? D[t] : 0u;
+      if (t < tiles && s_d[threadIdx.x]) D[t] = 0;
+    }
+    __syncthreads();
+    for (int k = 0; k < 32; k++) {
+      const u32 d = s_d[k];
+      if (!d) continue;
+      const u64 wt = (grp * 32 + k) * kBmTileWords;
+      // 256 threads x 8 words; thread t holds chunk t / 8
+      if ((d >> (threadIdx.x / 8)) & 1u) {
+        uint4 *p = reinterpret_cast<uint4 *>(G + wt + threadIdx.x * 8);
+        p[0] = make_uint4(0, 0, 0, 0);
+        p[1] = make_uint4(0, 0, 0, 0);
+      }
+    }
+  }
 }
 
-// Set the bits of a key list (FULL at the start of a LIE).
+// Set the bits of a key list (FULL at the start of a LIE; no dirty map).
 __global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm, DenseMap map,
                                                       Ctl *ctl) {
   if (ctl_stop(ctl)) return;
   const u64 n = list->n;
   const u64 *k = list->ptr;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-    dm_set(map, bm, k[i], ctl);
+    dm_set(map, bm, nullptr, k[i], ctl);
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
-}
-
-// Emission.  A relation whose FULL list is not read during the loop
-// (kEmitDelta) or whose NEWT is read as a list (kEmitNewt, tmp relations)
-// gets its new keys listed by the ops themselves: the first thread to set a
-// key's NEWT bit appends the key, so the update step works on the list and
-// never scans the bitmap.  kEmitDelta skips keys already in FULL, so its
-// list is DELTA itself.  A full list raises Ctl::overflow; the host then
-// clears the NEWT bitmaps and runs the iteration again with larger lists.
-struct EmitTarget {
-  u32 *g;          // NEWT bitmap
-  const u32 *f;    // FULL bitmap for kEmitDelta (keys in FULL are skipped)
-  DArr *list;      // delta_next or newt; null: bits only (scan path)
-  u64 *ptr;        // list storage and capacity, read once
-  u64 cap;
-  u64 *gen;        // tuples generated (kEmitDelta: is NEWT empty?)
-  int need_slot;
-};
-
-__device__ __forceinline__ EmitTarget emit_target(RelDev *rd, int rel) {
-  EmitTarget t;
-  t.g = rd->bmG;
-  t.f = rd->emit == kEmitDelta ? rd->bmF : nullptr;
-  t.list = rd->emit == kEmitDelta ? &rd->delta_next : rd->emit == kEmitNewt ? &rd->newt : nullptr;
-  t.ptr = t.list ? t.list->ptr : nullptr;
-  t.cap = t.list ? t.list->cap : 0;
-  t.gen = &rd->gen_count;
-  t.need_slot = need_index(rel, rd->emit == kEmitDelta ? kNeedDelta : kNeedNewt);
-  return t;
-}
-
-// Append `key` at position pos of the target list (bounds-checked).
-__device__ __forceinline__ void emit_store(const EmitTarget &T, u64 pos, u64 key, Ctl *ctl) {
-  if (pos < T.cap) {
-    T.ptr[pos] = key;
-  } else {
-    atomicMax(&ctl->need[T.need_slot], pos + 1);
-    atomicExch(&ctl->overflow, 1u);
-  }
-}
-
-// Set one key's NEWT bit; true if this thread set it first (and it is not
-// in FULL when the target checks FULL).
-__device__ __forceinline__ bool emit_set(const DenseMap &m, const EmitTarget &T, u64 key, Ctl *ctl) {
-  u64 w;
-  u32 b;
-  if (!dm_locate(m, key, &w, &b) || w >= m.words) {
-    atomicOr(&ctl->oob, 8192u);
-    return false;
-  }
-  if (T.f && ((T.f[w] >> b) & 1u)) return false;
-  const u32 old = atomicOr(T.g + w, 1u << b);
-  return !(old & (1u << b));
-}
-
-// Warp-synchronous emission of one candidate per lane (all 32 lanes call).
-__device__ __forceinline__ void emit_warp(const DenseMap &m, const EmitTarget &T, bool valid,
-                                          u64 key, Ctl *ctl) {
-  const int lane = threadIdx.x & 31;
-  const unsigned vm = __ballot_sync(0xffffffffu, valid);
-  if (T.list && lane == 0 && vm) atomicAdd(T.gen, (u64)__popc(vm));
-  const bool first = valid && emit_set(m, T, key, ctl);
-  if (!T.list) return;
-  const unsigned fm = __ballot_sync(0xffffffffu, first);
-  if (!fm) return;
-  const int leader = __ffs(fm) - 1;
-  u64 base = 0;
-  if (lane == leader) base = atomicAdd(&T.list->n, (u64)__popc(fm));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (first) emit_store(T, base + __popc(fm & ((1u << lane) - 1u)), key, ctl);
-}
-
-// The same for one thread alone.
-__device__ __forceinline__ void emit_one(const DenseMap &m, const EmitTarget &T, u64 key, Ctl *ctl) {
-  if (T.list) atomicAdd(T.gen, 1ull);
-  if (emit_set(m, T, key, ctl) && T.list) emit_store(T, atomicAdd(&T.list->n, 1ull), key, ctl);
 }
 
 // RelationalJoin materialisation into the output's NEWT bitmap.  Balanced
 // over candidate positions as k_join_mat: a block owns kMatTile consecutive
 // positions, each thread kMatPer consecutive ones, found with one binary
 // search over the tile's records and then walked forward.  A candidate is one
-// inner read, the column move, the predicate and one atomicOr (outputs of
-// different outer rows rarely share a bitmap word, so no warp aggregation of
-// the bits; only list appends are aggregated).
+// inner read, the column move, the predicate and two fire-and-forget
+// atomicOr (the bit and its chunk's dirty bit).
 constexpr int kMatPer = kMatTile / kMatBlock;  // positions per thread
 
-__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, RelDev *out_rd,
+__global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, const RelDev *out_rd,
                                                            DenseMap map) {
   __shared__ MatSmem sm;
   if (ctl_stop(a.ctl)) return;
   const u64 total = a.op->total;
   const u64 nc = a.op->nc;
   if (total == 0) return;
-  const EmitTarget T = emit_target(out_rd, a.out_rel);
+  u32 *G = out_rd->bmG, *D = out_rd->bmD;
   const u64 *inner = a.inner->ptr;
   const u64 tiles = (total + kMatTile - 1) / kMatTile;
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -465,181 +509,112 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, RelDev *o
     }
     __syncthreads();
     u64 p = p0 + (u64)threadIdx.x * kMatPer;
-    u32 r = 0;
-    u64 next = 0;
     if (p < p1) {
-      r = find_rec(sm.off, m, p);
-      next = sm.off[r + 1];
-    }
-#pragma unroll
-    for (int j = 0; j < kMatPer; j++, p++) {
-      bool valid = p < p1;
-      u64 t = 0;
-      if (valid) {
+      u32 r = find_rec(sm.off, m, p);
+      u64 next = sm.off[r + 1];
+      const u64 pe = min(p + kMatPer, p1);
+      for (; p < pe; p++) {
         while (p >= next) {
           r++;
           next = sm.off[r + 1];
         }
-        t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
-        valid = pred_ok(a.pred, t);
+        const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+        if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
       }
-      emit_warp(map, T, valid, t, a.ctl);
     }
   }
   if (launch_rec_finish(a.rec) && threadIdx.x == 0)
     prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
 }
 
-// Clear one relation's NEWT: bitmap and emission list (ACopy replaces the
-// destination's NEWT, src/acopy.cu:37-43).
-__global__ void __launch_bounds__(256) k_newt_reset(RelDev *rd, DenseMap map, Ctl *ctl) {
-  if (ctl_stop(ctl)) return;
-  uint4 *p = reinterpret_cast<uint4 *>(rd->bmG);
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < map.words / 4;
-       i += (u64)gridDim.x * blockDim.x)
-    p[i] = make_uint4(0, 0, 0, 0);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (rd->emit == kEmitDelta) rd->delta_next.n = 0;
-    if (rd->emit == kEmitNewt) rd->newt.n = 0;
-    rd->gen_count = 0;
-    prof_add(ctl, kPBitmap, map.words * 4);
-  }
-}
-
-// RelationalCopy into the destination's NEWT (src/copy.cu:12-95).  An empty
-// source empties the destination NEWT (src/copy.cu:24-27).
-__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, RelDev *dest_rd, DenseMap map) {
+// RelationalCopy into the destination's NEWT bitmap (src/copy.cu:12-95).  An
+// empty source empties the destination NEWT (src/copy.cu:24-27): that case
+// is handled by a k_bm_clear_dirty launched conditionally before.
+__global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, const RelDev *dest_rd, DenseMap map) {
   if (ctl_stop(c.ctl)) return;
   if (c.once && *c.once) return;
   const u64 n = eff_count(c.src, c.src_vis);
   if (n == 0) {
-    uint4 *p = reinterpret_cast<uint4 *>(dest_rd->bmG);
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < map.words / 4;
-         i += (u64)gridDim.x * blockDim.x)
-      p[i] = make_uint4(0, 0, 0, 0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      if (c.once_pending) *c.once_pending = 1;
-      if (dest_rd->emit == kEmitDelta) dest_rd->delta_next.n = 0;
-      if (dest_rd->emit == kEmitNewt) dest_rd->newt.n = 0;
-      dest_rd->gen_count = 0;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c.once_pending) *c.once_pending = 1;
     return;
   }
-  const EmitTarget T = emit_target(dest_rd, c.dest_rel);
+  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
   const u64 *src = c.src->ptr;
-  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
-    const u64 i = i0 + threadIdx.x;
-    const bool valid = i < n;
-    emit_warp(map, T, valid, valid ? gen_join(c.sel, src[i], 0) : 0, c.ctl);
-  }
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    dm_set(map, G, D, gen_join(c.sel, src[i], 0), c.ctl);
   if (launch_rec_finish(c.rec) && threadIdx.x == 0) {
     if (c.once_pending) *c.once_pending = 1;
     prof_add(c.ctl, kPCopy, 8 * n);
   }
 }
 
-// RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT); the
-// destination was reset by k_newt_reset just before.  The source NEWT is
-// its list when it has one, else its bitmap.
-__global__ void __launch_bounds__(256) k_acopy_bm(const RelDev *src_rd, Sel2 sel, RelDev *dest_rd,
-                                                  int dest_rel, DenseMap map, Ctl *ctl) {
-  if (ctl_stop(ctl)) return;
-  const EmitTarget T = emit_target(dest_rd, dest_rel);
-  if (src_rd->emit == kEmitNewt) {
-    const u64 n = src_rd->newt.n;
-    const u64 *src = src_rd->newt.ptr;
-    for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
-      const u64 i = i0 + threadIdx.x;
-      const bool valid = i < n;
-      emit_warp(map, T, valid, valid ? gen_join(sel, src[i], 0) : 0, ctl);
+// Empties the destination NEWT of a Copy whose source is empty (launched
+// just before k_copy_bm; a no-op otherwise or for a FULL source already
+// copied).
+__global__ void __launch_bounds__(256) k_copy_empty_clear(CopyArgs c, const RelDev *dest_rd,
+                                                          DenseMap map) {
+  __shared__ u32 s_d[32];
+  if (ctl_stop(c.ctl)) return;
+  if (c.once && *c.once) return;
+  if (eff_count(c.src, c.src_vis) != 0) return;
+  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
+  const u64 tiles = bm_tiles(map.words);
+  const u64 groups = (tiles + 31) / 32;
+  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const u64 t = grp * 32 + threadIdx.x;
+      s_d[threadIdx.x] = t < tiles ? D[t] : 0u;
+      if (t < tiles && s_d[threadIdx.x]) D[t] = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, 8 * n);
-    return;
-  }
-  const u32 *src_bm = src_rd->bmG;
-  for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < map.words;
-       w += (u64)gridDim.x * blockDim.x) {
-    u32 x = src_bm[w];
-    if (!x) continue;
-    const u32 inst = dm_tile_inst(map, w / kBmTileWords);
-    const SegInfo seg = map.seg[inst];
-    while (x) {
-      const int b = __ffs(x) - 1;
-      x &= x - 1;
-      emit_one(map, T, gen_join(sel, dm_key(map, inst, seg, w, b), 0), ctl);
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPCopy, map.words * 4);
-}
-
-// Update step of an emitting relation.  kEmitDelta: delta_next already is
-// DELTA; kEmitNewt: DELTA = the NEWT keys not in FULL.  Then FULL |= DELTA
-// in place and the NEWT bitmap is cleared word by word from the list (its
-// bits are exactly the listed keys).  With inst_delta set, each instance
-// that gained a key is flagged.
-__global__ void __launch_bounds__(256) k_emit_update(RelDev *rd, int rel, DenseMap map,
-                                                     u64 *inst_delta, Ctl *ctl) {
-  if (ctl_stop(ctl)) return;
-  const bool from_newt = rd->emit == kEmitNewt;
-  const DArr &L = from_newt ? rd->newt : rd->delta_next;
-  const u64 n = L.n;
-  const u64 *keys = L.ptr;
-  u32 *F = rd->bmF, *G = rd->bmG;
-  DArr *D = &rd->delta_next;
-  u64 *dptr = D->ptr;
-  const u64 dcap = D->cap;
-  const int lane = threadIdx.x & 31;
-  for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
-    const u64 i = i0 + threadIdx.x;
-    bool add = false;
-    u64 key = 0, w = 0;
-    u32 b = 0;
-    if (i < n) {
-      key = keys[i];
-      if (dm_locate(map, key, &w, &b) && w < map.words) {
-        G[w] = 0;
-        add = !from_newt || !((F[w] >> b) & 1u);
-      } else {
-        atomicOr(&ctl->oob, 8192u);
+    __syncthreads();
+    for (int k = 0; k < 32; k++) {
+      const u32 d = s_d[k];
+      if (!d) continue;
+      const u64 wt = (grp * 32 + k) * kBmTileWords;
+      if ((d >> (threadIdx.x / 8)) & 1u) {
+        uint4 *p = reinterpret_cast<uint4 *>(G + wt + threadIdx.x * 8);
+        p[0] = make_uint4(0, 0, 0, 0);
+        p[1] = make_uint4(0, 0, 0, 0);
       }
     }
-    if (add) {
-      atomicOr(F + w, 1u << b);
-      if (inst_delta) inst_delta[key_c0(key) >> map.seg_shift] = 1;
+  }
+}
+
+// RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT).  The
+// destination NEWT was cleared by k_bm_clear_dirty just before; the source
+// NEWT bitmap is read in its dirty chunks only.
+__global__ void __launch_bounds__(256) k_acopy_bm(const RelDev *src_rd, Sel2 sel,
+                                                  const RelDev *dest_rd, DenseMap map, Ctl *ctl) {
+  __shared__ u32 s_d[32];
+  if (ctl_stop(ctl)) return;
+  const u32 *S = src_rd->bmG, *SD = src_rd->bmD;
+  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
+  const u64 tiles = bm_tiles(map.words);
+  const u64 groups = (tiles + 31) / 32;
+  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const u64 t = grp * 32 + threadIdx.x;
+      s_d[threadIdx.x] = t < tiles ? SD[t] : 0u;
     }
-    if (from_newt) {
-      const unsigned am = __ballot_sync(0xffffffffu, add);
-      if (am) {
-        const int leader = __ffs(am) - 1;
-        u64 base = 0;
-        if (lane == leader) base = atomicAdd(&D->n, (u64)__popc(am));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (add) {
-          const u64 pos = base + __popc(am & ((1u << lane) - 1u));
-          if (pos < dcap) {
-            dptr[pos] = key;
-          } else {
-            atomicMax(&ctl->need[need_index(rel, kNeedDelta)], pos + 1);
-            atomicOr(&ctl->oob, 16384u);  // cannot happen: delta_next >= newt
-          }
+    __syncthreads();
+    for (int k = 0; k < 32; k++) {
+      const u32 d = s_d[k];
+      if (!d || !((d >> (threadIdx.x / 8)) & 1u)) continue;
+      const u64 tile = grp * 32 + k;
+      const u32 inst = dm_tile_inst(map, tile);
+      const SegInfo seg = map.seg[inst];
+      const u64 w0 = tile * kBmTileWords + threadIdx.x * 8;
+      for (int i = 0; i < 8; i++) {
+        u32 x = S[w0 + i];
+        while (x) {
+          const int b = __ffs(x) - 1;
+          x &= x - 1;
+          dm_set(map, G, D, gen_join(sel, dm_key(map, inst, seg, w0 + i, b), 0), ctl);
         }
       }
     }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 16 * n);
-}
-
-// Clear a NEWT bitmap word by word from its list (tmp relations at the end
-// of an iteration).
-__global__ void __launch_bounds__(256) k_newt_unset(RelDev *rd, DenseMap map, Ctl *ctl) {
-  if (ctl_stop(ctl)) return;
-  const u64 n = rd->newt.n;
-  const u64 *keys = rd->newt.ptr;
-  u32 *G = rd->bmG;
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-    u64 w;
-    u32 b;
-    if (dm_locate(map, keys[i], &w, &b) && w < map.words) G[w] = 0;
   }
 }
 

@@ -153,12 +153,9 @@ struct gdl_engine {
   u64 crow_cap = 0;
   Lb lb_cnt{}, lb_nz{}, lb_merge{};
   u64 *merge_parts = nullptr;  // [lb_merge_tiles + 1]
-  // Dense scans: tile prefixes, look-back state, the scan record.
-  u64 *bm_prefix = nullptr;
-  u64 bm_tiles = 0;
+  // Dense scans: look-back state of the tile-count scan.
   Lb lb_bm{};
   u64 lb_bm_tiles = 0;
-  BmScanRec *bm_rec = nullptr;
   // Largest 2*bits domain kept as bitmaps (GDLOG_DENSE_MAX_BITS), and the
   // dedup path: 0 chosen by domain size, 1 always sort/merge, 2 always
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
@@ -422,30 +419,26 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   RelHost &rh = e->rels[r];
   RelDev &h = e->h[r];
   if (rh.bm_words != words) {
-    for (u32 **p : {&h.bmF, &h.bmF_next, &h.bmG}) {
+    for (u32 **p : {&h.bmF, &h.bmG, &h.bmD}) {
       dfree(e, *p);
       *p = nullptr;
     }
+    dfree(e, h.tile_prefix);
+    h.tile_prefix = nullptr;
     rh.bm_words = words;
   }
+  const u64 tiles = words / kBmTileWords;
   if (!h.bmG) TRY(dalloc(e, (void **)&h.bmG, words * 4));
+  if (!h.bmD) TRY(dalloc(e, (void **)&h.bmD, tiles * 4));
+  if (!h.tile_prefix) TRY(dalloc(e, (void **)&h.tile_prefix, tiles * sizeof(u64)));
   if (with_full && !h.bmF) TRY(dalloc(e, (void **)&h.bmF, words * 4));
-  if (with_full && !h.bmF_next) TRY(dalloc(e, (void **)&h.bmF_next, words * 4));
+  memset(&h.scan, 0, sizeof h.scan);
   return GDL_OK;
 }
 
 gdl_status ensure_dense_scratch(gdl_engine *e, u64 words) {
-  const u64 tiles = words / kBmTileWords + 2;
-  if (e->bm_tiles < tiles) {
-    dfree(e, e->bm_prefix);
-    TRY(dalloc(e, (void **)&e->bm_prefix, tiles * sizeof(u64)));
-    e->bm_tiles = tiles;
-  }
-  TRY(ensure_lb(e, e->lb_bm, e->lb_bm_tiles, tiles));
-  if (!e->bm_rec) {
-    TRY(dalloc(e, (void **)&e->bm_rec, sizeof(BmScanRec)));
-    CK(e, cudaMemsetAsync(e->bm_rec, 0, sizeof(BmScanRec), e->s));
-  }
+  const u64 chunks = words / kBmTileWords / kScanChunk + 2;
+  TRY(ensure_lb(e, e->lb_bm, e->lb_bm_tiles, chunks));
   return GDL_OK;
 }
 
@@ -592,18 +585,29 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
 // domain of dk-bit columns.
 u64 dense_words(int dk) { return 1ull << (2 * dk - 5); }
 
-// One bitmap scan (dense.cuh): count pass, then write pass.
-void launch_scan(gdl_engine *e, BmScanArgs a, Counts *kc) {
-  a.tile_prefix = e->bm_prefix;
-  a.tiles_cap = e->bm_tiles;
-  a.rec = e->bm_rec;
+// One bitmap scan (dense.cuh) of relation `rel`: tile counts and their
+// prefix, then (unless the caller gates it) the write pass.
+void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
+  a.tile_prefix = e->h[rel].tile_prefix;
+  a.rec = &e->d_rels[rel].scan;
   a.lb = e->lb_bm;
   a.ctl = e->d_ctl;
-  const u64 tiles = (a.map.words + kBmTileWords - 1) / kBmTileWords;
+  const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[4];
-  PLAUNCH(kc, kPBitmap, k_bm_count<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
+  PLAUNCH(kc, kPBitmap,
+          k_bm_tilecount<<<grid_for(e, (tiles + 31) / 32, 1, 8), kBmBlock, 0, e->s>>>(a));
+  PLAUNCH(kc, kPBitmap,
+          k_bm_scan<<<grid_for(e, tiles / kScanChunk + 1, 1, 4), kBmBlock, 0, e->s>>>(a));
+}
+void launch_scan_write(gdl_engine *e, BmScanArgs a, Counts *kc) {
+  const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[5];
-  PLAUNCH(kc, kPBitmap, k_bm_write<<<grid_for(e, tiles, 1, 4), kBmBlock, 0, e->s>>>(a));
+  PLAUNCH(kc, kPBitmap,
+          k_bm_write<<<grid_for(e, (tiles + 31) / 32, 1, 8), kBmBlock, 0, e->s>>>(a));
+}
+void launch_scan(gdl_engine *e, BmScanArgs a, int rel, Counts *kc) {
+  launch_scan_count(e, a, rel, kc);
+  launch_scan_write(e, a, kc);
 }
 
 BmScanArgs scan_none(const DenseMap &map) {
@@ -624,14 +628,6 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
   const DenseMap &map = L.map;
   const u64 words = dense ? map.words : 0;
   PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
-  if (dense) {
-    // NEWT of every scan-path relation starts empty (emitting relations
-    // clear their NEWT bitmap from their list in the update step).
-    for (int r : L.update)
-      if (e->h[r].emit == kEmitNone)
-        PLAUNCH(kc, kPBitmap, k_bm_clear<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
-                                  e->h[r].bmG, words, e->d_ctl));
-  }
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (op.kind == 0) {
@@ -647,14 +643,17 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       } else {
         a.outer = &R[op.outer].newt;
         a.outer_vis = nullptr;
-        if (dense && oh.bmG && oh.emit != kEmitNewt) {
-          // NEWT as a join outer: the sorted list of its bitmap.
+        if (dense && oh.bmG) {
+          // NEWT as a join outer: the sorted list of its bitmap (dirty
+          // chunks only).
           BmScanArgs c = scan_none(map);
           c.g = oh.bmG;
+          c.dirty = oh.bmD;
+          c.skip_clean = 1;
           c.ex_a = kBmUnion;
           c.list_a = &R[op.outer].newt;
           c.need_a = need_index(op.outer, kNeedNewt);
-          launch_scan(e, c, kc);
+          launch_scan(e, c, op.outer, kc);
           a.outer_bm = oh.bmG;
           a.outer_bm_words = words;
         }
@@ -725,13 +724,16 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
       if (dense && op.kind == 2) {
         // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
-        PLAUNCH(kc, kPBitmap, k_newt_reset<<<grid_for(e, words / 4, 256, 8), 256, 0, s>>>(
+        const u64 groups = words / kBmTileWords / 32 + 1;
+        PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
                                   &R[op.out], map, e->d_ctl));
         if (sh.bmG)  // a source without a NEWT bitmap (static) has an empty NEWT
-          PLAUNCH(kc, kPCopy,
-                  k_acopy_bm<<<grid_for(e, std::max(words, sh.newt.cap), 256, 8), 256, 0, s>>>(
-                      &R[op.inner], op.sel, &R[op.out], op.out, map, e->d_ctl));
+          PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+                                  &R[op.inner], op.sel, &R[op.out], map, e->d_ctl));
       } else if (dense) {
+        const u64 groups = words / kBmTileWords / 32 + 1;
+        PLAUNCH(kc, kPBitmap, k_copy_empty_clear<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+                                  c, &R[op.out], map));
         PLAUNCH(kc, kPCopy, k_copy_bm<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
                                 c, &R[op.out], map));
       } else {
@@ -750,33 +752,44 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
-  // Scan-path and sort-path relations first: a capacity overflow there is
-  // resumed by running this step again, which is only correct while no
-  // emitting relation has updated its FULL bitmap in place yet.
-  for (int r : L.update) {
-    const RelDev &rh = e->h[r];
-    if (dense && rh.emit != kEmitNone) continue;
-    if (dense) {
-      // DELTA = NEWT \ FULL, FULL' = FULL | NEWT, both sorted; FULL's list
-      // and index only when some op reads them during the loop.
+  if (dense) {
+    // DELTA = NEWT \ FULL (sorted), FULL |= NEWT in place, NEWT cleared; a
+    // relation whose FULL list is read during the loop also gets FULL' and
+    // its index.  All relations are counted and checked (gate) before any
+    // bitmap is written.
+    std::vector<BmScanArgs> scans;
+    for (int r : L.update) {
       BmScanArgs a = scan_none(L.map);
+      a.rd = &R[r];
+      a.inplace = 1;
+      a.skip_clean = !plan.full_list[r];
+      a.gated = 1;
       a.inst_delta = L.d_inst_delta;
-      a.rd = &R[r];  // bitmaps as the device sees them (k_commit swaps F)
       a.ex_a = kBmDelta;
       a.list_a = &R[r].delta_next;
       a.need_a = need_index(r, kNeedDelta);
-      a.ex_b = kBmUnion;
       if (plan.full_list[r]) {
+        a.ex_b = kBmUnion;
         a.list_b = &R[r].full_next;
         a.need_b = need_index(r, kNeedFull);
         if (plan.full_idx[r]) a.idx_b = &R[r].full_idx_next;
-      } else {
-        a.count_b = &R[r].f_count;
       }
       a.pop_g_out = &R[r].c_newt_n;
-      a.update_stage = 1;
-      launch_scan(e, a, kc);
-    } else {
+      launch_scan_count(e, a, r, kc);
+      scans.push_back(a);
+    }
+    PLAUNCH(kc, kPControl, k_scan_gate<<<1, 32, 0, s>>>(R, &L.d_lie->update[0],
+                                                         (int)L.update.size(), e->d_ctl));
+    for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
+    // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
+    const u64 groups = L.map.words / kBmTileWords / 32 + 1;
+    for (int r : L.tmps)
+      PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+                                &R[r], L.map, e->d_ctl));
+  }
+  for (int r : L.update) {
+    const RelDev &rh = e->h[r];
+    if (!dense) {
       launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
       MergeArgs m;
       m.newt = &R[r].newt;
@@ -809,20 +822,6 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
               k_index_build<<<grid_for(e, c, kIndexBlock, 8), kIndexBlock, 0, s>>>(
                   &R[r].delta_next, &R[r].delta_idx_next, nullptr, e->d_ctl));
     }
-  }
-  if (dense) {
-    // Emitting relations: FULL |= DELTA in place, NEWT bitmap cleared from
-    // the list; tmp relations' NEWT bitmaps likewise.
-    for (int r : L.update) {
-      const RelDev &rh = e->h[r];
-      if (rh.emit == kEmitNone) continue;
-      const u64 cap = rh.emit == kEmitNewt ? rh.newt.cap : rh.delta_next.cap;
-      PLAUNCH(kc, kPBitmap, k_emit_update<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
-                                &R[r], r, L.map, L.d_inst_delta, e->d_ctl));
-    }
-    for (int r : L.tmps)
-      PLAUNCH(kc, kPBitmap, k_newt_unset<<<grid_for(e, e->h[r].newt.cap, 256, 8), 256, 0, s>>>(
-                                &R[r], L.map, e->d_ctl));
   }
   if (L.d_inst_delta)
     PLAUNCH(kc, kPControl, k_inst_track<<<grid_for(e, L.n_inst, 256, 1), 256, 0, s>>>(
@@ -996,7 +995,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     L.dense = e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits);
     L.dk = L.dense && !e->instances ? dk : 0;
   }
-  for (RelDev &h : e->h) h.dense = h.full_lazy = h.emit = 0;
+  for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
   if (L.dense) {
     if (e->instances) {
       L.map = DenseMap{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
@@ -1022,16 +1021,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       RelDev &h = e->h[r];
       h.dense = 1;
       h.full_lazy = !plan.full_list[r];
-      // FULL not read as a list and DELTA not probed: the ops list DELTA
-      // (or NEWT, when an op reads NEWT) themselves.
-      h.emit = (plan.full_list[r] || plan.delta_idx[r])
-                   ? kEmitNone
-                   : (plan.newt_list[r] || plan.acopy_src[r]) ? kEmitNewt : kEmitDelta;
     }
     for (int r : L.tmps) {
       TRY(ensure_bitmaps(e, r, words, false));
       e->h[r].dense = 1;
-      e->h[r].emit = kEmitNewt;
     }
     TRY(ensure_dense_scratch(e, words));
     // Every list of the loop is bounded by the key domain: size them for
@@ -1077,12 +1070,16 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       const RelDev &h = e->h[r];
       CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(h.bmG, 0, words * 4, e->s));
+      CK(e, cudaMemsetAsync(h.bmD, 0, words / kBmTileWords * 4, e->s));
       if (h.full.n)
         k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
             &e->d_rels[r].full, h.bmF, L.map, e->d_ctl);
       e->rels[r].bm_valid = true;
     }
-    for (int r : L.tmps) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+    for (int r : L.tmps) {
+      CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+      CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmTileWords * 4, e->s));
+    }
     CK(e, cudaGetLastError());
   }
   // An unsorted DELTA (raw load order) used as a join inner is sorted and
@@ -1217,8 +1214,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         // The iteration runs again from its start: its NEWT bitmaps must
         // be empty again (emitting relations clear them only on success).
         const u64 words = L.map.words;
-        for (int r : L.update) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
-        for (int r : L.tmps) CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+        for (auto *v : {&L.update, &L.tmps})
+          for (int r : *v) {
+            CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
+            CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmTileWords * 4, e->s));
+          }
       }
       if (resume) {
         // Re-run only the update step and the commit of the iteration that
@@ -1306,12 +1306,12 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         a.f = e->h[r].bmF;
         a.ex_b = kBmUnion;
         a.list_b = &e->d_rels[r].full;
-        launch_scan(e, a, &kc);
+        launch_scan(e, a, r, &kc);
       }
       CK(e, cudaGetLastError());
       TRY(pull(e));
     }
-    for (RelDev &h : e->h) h.dense = h.full_lazy = h.emit = 0;
+    for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
     TRY(push(e));
     c.iteration = kept_iteration;
   }
@@ -1442,8 +1442,9 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
-    for (u32 *bm : {r.bmF, r.bmF_next, r.bmG})
+    for (u32 *bm : {r.bmF, r.bmG, r.bmD})
       if (bm) cudaFreeAsync(bm, e->s);
+    if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);
     if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
   }
   for (LieHost &L : e->lies) {
@@ -1488,8 +1489,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->lb_cnt.agg, (void *)e->lb_cnt.inc, (void *)e->lb_nz.flag,
                   (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
                   (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->merge_parts,
-                  (void *)e->bm_prefix, (void *)e->lb_bm.flag, (void *)e->lb_bm.agg,
-                  (void *)e->lb_bm.inc, (void *)e->bm_rec, (void *)e->d_segs,
+                  (void *)e->lb_bm.flag, (void *)e->lb_bm.agg, (void *)e->lb_bm.inc,
+                  (void *)e->d_segs,
                   (void *)e->d_tile_inst, (void *)e->d_square_seg,
                   (void *)e->recs,
                   (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
