@@ -1,0 +1,105 @@
+"""Autotuner for the fixpoint engine's launch and layout parameters.
+
+The reference fixes its launch shape per driver (grid = 32 x SMs, block 512,
+test/tc.cu:223-225) and its index load factor (0.8, src/relation.cu:836).
+Here the engine exposes, through gdl_tuning, the choices whose best value
+depends on the instance: the dedup path (bitmaps or radix sort + merge), the
+largest domain kept as bitmaps, the CTAs per SM of the join's count and
+materialisation passes, and the slots per key of the hashed index.  The
+radix sort's digit width is fixed at 8 bits; its number of passes already
+follows the key width.
+
+The tuner buckets a workload by program and by log2 of its node and tuple
+counts, times each candidate configuration on the workload (device time of
+the fixpoints, best of `reps`), keeps the fastest, and remembers it per
+(GPU, bucket) in a JSON cache.  Results never depend on the choice: every
+configuration gives the same tuples, sizes and loop-pass counts.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_CACHE = os.path.join(HERE, "tuning_cache.json")
+
+# Candidate values per parameter (0 keeps the engine's default).
+SPACE = {
+    "dedup": ["dense", "sort"],
+    "join_ctas_per_sm": [4, 8, 16],
+    "count_ctas_per_sm": [2, 4, 8],
+    "index_slots_per_key": [2, 4],
+}
+
+
+def bucket(program: str, inputs) -> str:
+    """Size class of a workload: program, log2(nodes), log2(tuples)."""
+    n_rows = sum(len(x) for x in inputs)
+    nodes = 1
+    for x in inputs:
+        if len(x):
+            nodes = max(nodes, int(np.asarray(x).max()) + 1)
+    return f"{program}:n{int(math.log2(max(nodes, 1)))}:t{int(math.log2(max(n_rows, 1)))}"
+
+
+def candidates(space=SPACE, limit=None):
+    keys = list(space)
+    out = [dict(zip(keys, vals)) for vals in itertools.product(*(space[k] for k in keys))]
+    # the sort path does not use the hashed-index choice differently; keep
+    # the grid the same size for both paths (small, so tuning stays cheap)
+    return out[:limit] if limit else out
+
+
+def measure(eng, prog, inputs, cfg, reps=2) -> float:
+    """Best device milliseconds of the program's fixpoints under cfg."""
+    eng.set_tuning(**cfg)
+    best = float("inf")
+    for _ in range(reps):
+        eng.clear()
+        r = prog(eng, *inputs, sync=eng.sync)
+        best = min(best, sum(lie.stats()["ms"] for lie in r.lies.values()))
+    return best
+
+
+class Tuner:
+    def __init__(self, cache_path: str = DEFAULT_CACHE, gpu_name: str = "B200"):
+        self.path = cache_path
+        self.gpu = gpu_name
+        self.cache = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.cache = json.load(f)
+
+    def key(self, program: str, inputs) -> str:
+        return f"{self.gpu}|{bucket(program, inputs)}"
+
+    def lookup(self, program: str, inputs):
+        return self.cache.get(self.key(program, inputs))
+
+    def tune(self, eng, prog, inputs, space=SPACE, reps=2, save=True) -> dict:
+        """Time every candidate on this workload; remember and return the best."""
+        results = []
+        for cfg in candidates(space):
+            results.append((measure(eng, prog, inputs, cfg, reps), cfg))
+        results.sort(key=lambda x: x[0])
+        best_ms, best = results[0]
+        default_ms = next((ms for ms, c in results if c == candidates(space)[0]), None)
+        rec = {"config": best, "ms": best_ms, "default_ms": default_ms,
+               "tried": len(results)}
+        self.cache[self.key(prog.__name__, inputs)] = rec
+        if save:
+            with open(self.path, "w") as f:
+                json.dump(self.cache, f, indent=1, sort_keys=True)
+        eng.set_tuning(**best)
+        return rec
+
+    def apply(self, eng, prog, inputs) -> dict | None:
+        """Set the cached best configuration for this workload, if any."""
+        rec = self.lookup(prog.__name__, inputs)
+        if rec:
+            eng.set_tuning(**rec["config"])
+        return rec

@@ -161,6 +161,9 @@ struct gdl_engine {
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
   int dense_max_bits = kDenseMaxDomainBits;
   int dedup_mode = 0;
+  int join_ctas_per_sm = 8;   // gdl_tuning
+  int count_ctas_per_sm = 4;
+  int index_slots_per_key = 2;
   // Batched form (gdl_engine_set_instances): the block-diagonal layout.
   bool instances = false;
   std::vector<SegInfo> segs;
@@ -258,7 +261,7 @@ gdl_status ensure_index(gdl_engine *e, Index &ix, u64 cap) {
   } else {
     mode = 1;
     u64 distinct = std::min<u64>(cap, 1ull << std::min(e->kbits, 40));
-    slots = next_pow2(std::max<u64>(2 * distinct, 1024));
+    slots = next_pow2(std::max<u64>((u64)e->index_slots_per_key * distinct, 1024));
   }
   if (ix.slots && ix.hash_mode == mode && ix.mask + 1 >= slots) return GDL_OK;
   dfree(e, ix.slots);
@@ -582,8 +585,9 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
 }
 
 // Bitmap size, in 32-bit words, of one relation version over the square
-// domain of dk-bit columns.
-u64 dense_words(int dk) { return 1ull << (2 * dk - 5); }
+// domain of dk-bit columns, padded to whole scan tiles (the scan kernels
+// work on whole tiles; padding bits are never set).
+u64 dense_words(int dk) { return round_up(1ull << (2 * dk - 5), kBmTileWords); }
 
 // One bitmap scan (dense.cuh) of relation `rel`: tile counts and their
 // prefix, then (unless the caller gates it) the write pass.
@@ -685,19 +689,22 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
       PLAUNCH(kc, kPJoinCount,
-              k_join_count<<<grid_for(e, outer_cap, kJoinTile, 4), kJoinBlock, 0, s>>>(a));
+              k_join_count<<<grid_for(e, outer_cap, kJoinTile, e->count_ctas_per_sm), kJoinBlock,
+                             0, s>>>(a));
       JoinArgs b = a;
       b.rec = &e->recs[1];
       const u64 out_cap = e->h[op.out].newt.cap;
       if (dense)
         PLAUNCH(kc, kPJoinMat,
-                k_join_mat_bm<<<(int)e->sms * 8, kMatBlock, 0, s>>>(b, &R[op.out], map));
+                k_join_mat_bm<<<(int)e->sms * e->join_ctas_per_sm, kMatBlock, 0, s>>>(
+                    b, &R[op.out], map));
       else if (op.pred.kind)
         PLAUNCH(kc, kPJoinMat,
                 k_join_mat_pred<<<grid_for(e, outer_cap, 8 * 16, 8), kMatBlock, 0, s>>>(b));
       else
         PLAUNCH(kc, kPJoinMat,
-                k_join_mat<<<grid_for(e, out_cap, kMatTile, 8), kMatBlock, 0, s>>>(b));
+                k_join_mat<<<grid_for(e, out_cap, kMatTile, e->join_ctas_per_sm), kMatBlock, 0,
+                             s>>>(b));
     } else {
       CopyArgs c;
       memset(&c, 0, sizeof c);
@@ -1863,6 +1870,34 @@ gdl_status gdl_engine_set_dedup(gdl_engine *e, int32_t mode, int32_t dense_max_b
     return fail(e, GDL_E_INVALID, "dense_max_bits must be in [0, %d]", kDenseMaxDomainBits);
   e->dedup_mode = mode;
   if (dense_max_bits) e->dense_max_bits = dense_max_bits;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
+  if (!e || !t) return GDL_E_INVALID;
+  if (t->dedup < 0 || t->dedup > GDL_DEDUP_DENSE || t->dense_max_bits < 0 ||
+      t->dense_max_bits > kDenseMaxDomainBits || t->join_ctas_per_sm < 0 ||
+      t->join_ctas_per_sm > 32 || t->count_ctas_per_sm < 0 || t->count_ctas_per_sm > 32 ||
+      t->index_slots_per_key < 0 || t->index_slots_per_key > 64 ||
+      (t->index_slots_per_key && (t->index_slots_per_key < 2 ||
+                                  (t->index_slots_per_key & (t->index_slots_per_key - 1)))))
+    return fail(e, GDL_E_INVALID, "tuning value out of range");
+  e->dedup_mode = t->dedup;
+  if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
+  if (t->join_ctas_per_sm) e->join_ctas_per_sm = t->join_ctas_per_sm;
+  if (t->count_ctas_per_sm) e->count_ctas_per_sm = t->count_ctas_per_sm;
+  if (t->index_slots_per_key) e->index_slots_per_key = t->index_slots_per_key;
+  for (LieHost &L : e->lies) L.graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
+  if (!e || !t) return GDL_E_INVALID;
+  t->dedup = e->dedup_mode;
+  t->dense_max_bits = e->dense_max_bits;
+  t->join_ctas_per_sm = e->join_ctas_per_sm;
+  t->count_ctas_per_sm = e->count_ctas_per_sm;
+  t->index_slots_per_key = e->index_slots_per_key;
   return GDL_OK;
 }
 

@@ -48,6 +48,16 @@ def SRC(c: int) -> int:
     return c
 
 
+class Tuning(C.Structure):
+    """gdl_tuning (include/gdlog_b200.h); a zero field keeps the default."""
+    _fields_ = [("dedup", C.c_int32), ("dense_max_bits", C.c_int32),
+                ("join_ctas_per_sm", C.c_int32), ("count_ctas_per_sm", C.c_int32),
+                ("index_slots_per_key", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
 class GdlError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS.get(code, code)}: {msg}")
@@ -119,6 +129,10 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_lie_instance_iterations.restype = _I
         lib.gdl_relation_instance_stats.argtypes = [_P, _I, _PU64, _PU64, _I]
         lib.gdl_relation_instance_stats.restype = _I
+        lib.gdl_engine_set_tuning.argtypes = [_P, C.POINTER(Tuning)]
+        lib.gdl_engine_set_tuning.restype = _I
+        lib.gdl_engine_get_tuning.argtypes = [_P, C.POINTER(Tuning)]
+        lib.gdl_engine_get_tuning.restype = _I
         lib.gdl_engine_set_dedup.argtypes = [_P, _I, _I]
         lib.gdl_engine_set_dedup.restype = _I
         lib.gdl_engine_clear.argtypes = [_P]
@@ -400,6 +414,20 @@ class Engine:
     def sync(self) -> None:
         if self.kind == "gpu":
             self._check(self.lib.gdl_engine_sync(self.h))
+
+    def set_tuning(self, **kw) -> None:
+        """Set gdl_tuning fields by name (dedup may be "auto"/"sort"/"dense")."""
+        t = self.get_tuning()
+        for k, v in kw.items():
+            if k == "dedup" and isinstance(v, str):
+                v = self.DEDUP[v]
+            setattr(t, k, int(v))
+        self._check(self.lib.gdl_engine_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self._check(self.lib.gdl_engine_get_tuning(self.h, C.byref(t)))
+        return t
 
     def set_instances(self, node_counts) -> int:
         """Batched form: declare the instances' node counts; returns S, the

@@ -101,6 +101,20 @@ gdl_status gdl_engine_clear(gdl_engine *e);
 #define GDL_DEDUP_DENSE 2
 gdl_status gdl_engine_set_dedup(gdl_engine *e, int32_t mode, int32_t dense_max_bits);
 
+/* Launch and layout parameters an autotuner may set (no reference
+ * counterpart; the reference takes grid/block sizes per call, e.g.
+ * LIE(grid, block), include/lie.cuh:26-34, and fixes the index load factor
+ * at 0.8, src/relation.cu:836).  A zero field keeps the engine's default. */
+typedef struct gdl_tuning {
+  int32_t dedup;               /* GDL_DEDUP_* */
+  int32_t dense_max_bits;      /* largest 2*bits domain kept as bitmaps (<= 30) */
+  int32_t join_ctas_per_sm;    /* materialisation grid, CTAs per SM (default 8) */
+  int32_t count_ctas_per_sm;   /* count-pass grid, CTAs per SM (default 4) */
+  int32_t index_slots_per_key; /* hashed index: slots per distinct key, power of two >= 2 (default 2) */
+} gdl_tuning;
+gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
+gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);
+
 /* Declare a relation.  Replaces `new Relation()` plus the field writes the
  * drivers make before loading (include/relation.cuh:257-300; index_flag as
  * set at test/tc.cu:108, tmp_flag as in load_relation's last argument,
