@@ -23,6 +23,7 @@ namespace gdl {
 
 typedef unsigned long long u64;
 typedef unsigned int u32;
+typedef unsigned char u8;
 
 constexpr int kWarp = 32;
 constexpr int kMaxRels = 64;  // relations per engine (device table size)
@@ -85,7 +86,9 @@ struct RelDev {
   // Dense form (dense.cuh): FULL bitmap, NEWT bitmap and the dirty map of
   // NEWT (one bit per 64-word chunk), the tile counts / prefixes of this
   // relation's update scan and its record.
-  u32 *bmF, *bmG, *bmD;
+  u32 *bmF, *bmG;
+  u8 *bmD;         // dirty map storage (one byte per 64-word chunk of bmG)
+  u8 *dirty;       // bmD while the running LIE keeps a dirty map, else null
   u64 *tile_prefix;
   BmScanRec scan;
   u64 f_count;     // |FULL'| when the FULL list is not rebuilt every iteration

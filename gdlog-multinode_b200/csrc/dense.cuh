@@ -80,21 +80,30 @@ __device__ __forceinline__ u64 dm_key(const DenseMap &m, u32 inst, const SegInfo
   return make_key(hi | lx, hi | lz);
 }
 
-// The dirty map has one u32 per scan tile, one bit per 64-word chunk.
-__device__ __forceinline__ void bm_mark(u32 *bm, u32 *dirty, u64 w, u32 b) {
+// The dirty map has one byte per 64-word chunk of NEWT, set with a plain
+// store (no read-modify-write, so no contention between the many threads
+// that touch one chunk).  It is only kept for large bitmaps; without it
+// (null) every chunk counts as dirty.
+__device__ __forceinline__ void bm_mark(u32 *bm, u8 *dirty, u64 w, u32 b) {
   atomicOr(bm + w, 1u << b);
-  if (dirty) atomicOr(dirty + w / kBmTileWords, 1u << ((w / kBmChunkWords) & 31u));
+  if (dirty) dirty[w / kBmChunkWords] = 1;
 }
 
 // Set the bit of one key; keys outside their instance's range are dropped
 // and recorded in Ctl::oob instead of being written.
-__device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u32 *dirty, u64 key, Ctl *ctl) {
+__device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u8 *dirty, u64 key, Ctl *ctl) {
   u64 w;
   u32 b;
   if (dm_locate(m, key, &w, &b) && w < m.words)
     bm_mark(bm, dirty, w, b);
   else
     atomicOr(&ctl->oob, 8192u);
+}
+
+// Dirty byte of the chunk thread `tid` reads in scan tile `tile` (8 words
+// per thread, 8 threads per chunk); 1 when no map is kept.
+__device__ __forceinline__ u8 chunk_dirty(const u8 *dirty, u64 tile, int tid) {
+  return dirty ? dirty[tile * (kBmTileWords / kBmChunkWords) + tid / (kBmChunkWords / 8)] : 1;
 }
 
 // Expressions a scan can compact, over the word pair (g, f).
@@ -106,10 +115,10 @@ __device__ __forceinline__ u32 bm_eval(int ex, u32 g, u32 f) {
 struct BmScanArgs {
   const u32 *g;    // NEWT bitmap (may be null: all zero)
   u32 *f;          // FULL bitmap (may be null: all zero)
-  // If set, g / f / dirty are this relation's bmG / bmF / bmD, read from the
-  // device descriptor when the kernel starts.
+  // If set, g / f / dirty are this relation's bmG / bmF / dirty map, read
+  // from the device descriptor when the kernel starts.
   const RelDev *rd;
-  u32 *dirty;      // dirty map of g
+  u8 *dirty;       // dirty map of g (null: every chunk may hold bits)
   int skip_clean;  // read only dirty chunks (every expression is 0 where g is)
   int inplace;     // write pass: f |= g, g := 0 and dirty := 0 in dirty chunks
   DenseMap map;
@@ -137,68 +146,54 @@ __device__ __forceinline__ void scan_bind(BmScanArgs &a) {
   if (a.rd) {
     a.g = a.rd->bmG;
     a.f = a.rd->bmF;
-    a.dirty = a.rd->bmD;
+    a.dirty = a.rd->dirty;
   }
 }
 
-// Pass 1: packed (a, b) counts of every tile.  A block takes 32 tiles (one
-// warp reads their 32 dirty words); clean tiles are skipped when allowed.
+// Pass 1: packed (a, b) counts of every tile, one block per tile; a tile
+// whose chunks are all clean is skipped when allowed.
 __global__ void __launch_bounds__(kBmBlock) k_bm_tilecount(BmScanArgs a) {
-  __shared__ u32 s_dirty[32];
   __shared__ u32 s_red[2][kBmBlock / 32];
   if (ctl_stop(a.ctl)) return;
   scan_bind(a);
-  const u64 words = a.map.words;
-  const u64 tiles = bm_tiles(words);
-  const u64 groups = (tiles + 31) / 32;
+  const u64 tiles = bm_tiles(a.map.words);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 my_g = 0;
-  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
-    __syncthreads();
-    if (warp == 0) {
-      const u64 t = grp * 32 + lane;
-      s_dirty[lane] = t < tiles ? ((a.skip_clean && a.dirty) ? a.dirty[t] : 0xFFFFFFFFu) : 0u;
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const bool read = !a.skip_clean || chunk_dirty(a.dirty, tile, threadIdx.x);
+    if (!__syncthreads_or(read)) {
+      if (threadIdx.x == 0) a.tile_prefix[tile] = 0;
+      continue;
+    }
+    const u64 w0 = tile * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 ca = 0, cb = 0;
+    if (read) {
+#pragma unroll
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        const u64 w = w0 + i;
+        const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
+        ca += __popc(bm_eval(a.ex_a, g, f));
+        cb += __popc(bm_eval(a.ex_b, g, f));
+        my_g += __popc(g);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ca += __shfl_xor_sync(0xffffffffu, ca, o);
+      cb += __shfl_xor_sync(0xffffffffu, cb, o);
+    }
+    if (lane == 0) {
+      s_red[0][warp] = ca;
+      s_red[1][warp] = cb;
     }
     __syncthreads();
-    for (int k = 0; k < 32; k++) {
-      const u64 tile = grp * 32 + k;
-      if (tile >= tiles) break;
-      const u32 d = s_dirty[k];
-      if (!d) {
-        if (threadIdx.x == 0) a.tile_prefix[tile] = 0;
-        continue;
+    if (threadIdx.x == 0) {
+      u64 ta = 0, tb = 0;
+      for (int w = 0; w < kBmBlock / 32; w++) {
+        ta += s_red[0][w];
+        tb += s_red[1][w];
       }
-      const u64 w0 = tile * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
-      u32 ca = 0, cb = 0;
-      if ((d >> (threadIdx.x / (kBmChunkWords / kBmWordsPerThread))) & 1u) {
-#pragma unroll
-        for (int i = 0; i < kBmWordsPerThread; i++) {
-          const u64 w = w0 + i;
-          const u32 g = a.g ? a.g[w] : 0u, f = a.f ? a.f[w] : 0u;
-          ca += __popc(bm_eval(a.ex_a, g, f));
-          cb += __popc(bm_eval(a.ex_b, g, f));
-          my_g += __popc(g);
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        ca += __shfl_xor_sync(0xffffffffu, ca, o);
-        cb += __shfl_xor_sync(0xffffffffu, cb, o);
-      }
-      if (lane == 0) {
-        s_red[0][warp] = ca;
-        s_red[1][warp] = cb;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        u64 ta = 0, tb = 0;
-        for (int w = 0; w < kBmBlock / 32; w++) {
-          ta += s_red[0][w];
-          tb += s_red[1][w];
-        }
-        a.tile_prefix[tile] = (ta << 32) | tb;
-      }
-      __syncthreads();
+      a.tile_prefix[tile] = (ta << 32) | tb;
     }
   }
 #pragma unroll
@@ -284,12 +279,10 @@ __global__ void k_scan_gate(RelDev *rels, const int *update, int n_update, Ctl *
 }
 
 // Pass 3: write list a, list b (+ its index), update f in place and clear g
-// in the dirty chunks.  Tiles are visited 32 at a time as in pass 1.
+// in the dirty chunks (every chunk without a dirty map).  One block per tile.
 struct BmWriteSmem {
   u32 off_b[kBmTileWords + 1];  // exclusive offsets of list b per word
   u64 scan_tmp[kBmBlock / 32];
-  u32 dirty[32];   // chunks to read per tile of the group
-  u32 dclear[32];  // dirty chunks per tile (g is non-zero only there)
 };
 
 __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
@@ -305,107 +298,92 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   scan_bind(a);
   const u64 words = a.map.words;
   const u64 tiles = bm_tiles(words);
-  const u64 groups = (tiles + 31) / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const u32 epoch = (u32)(a.ctl->generation + 1);
   const Index ix = a.idx_b ? *a.idx_b : Index{};
   if (blockIdx.x == 0 && threadIdx.x == 0 && a.idx_b) a.idx_b->epoch = epoch;
   u64 *la = a.list_a ? a.list_a->ptr : nullptr;
   u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
   const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
-  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
-    __syncthreads();
-    if (warp == 0) {
-      const u64 t = grp * 32 + lane;
-      const u32 d = (t < tiles && a.dirty) ? a.dirty[t] : 0u;
-      sm.dirty[lane] = t < tiles ? (a.skip_clean ? d : 0xFFFFFFFFu) : 0u;
-      sm.dclear[lane] = d;
-      if (a.inplace && d) a.dirty[t] = 0;
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const u8 db = chunk_dirty(a.dirty, tile, threadIdx.x);
+    const bool read = !a.skip_clean || db;
+    if (!__syncthreads_or(read)) continue;
+    const bool clr = a.inplace && db;
+    const u64 prefix = a.tile_prefix[tile];
+    const u64 wt = tile * kBmTileWords;
+    const u32 inst = dm_tile_inst(a.map, tile);
+    const SegInfo seg = a.map.seg[inst];
+    const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
+    u32 ca = 0, cb = 0;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u64 w = w0 + i;
+      u32 g = 0, f = 0;
+      if (read) {
+        g = a.g ? a.g[w] : 0u;
+        f = a.f ? a.f[w] : 0u;
+        if (clr && g) {
+          a.f[w] = f | g;
+          const_cast<u32 *>(a.g)[w] = 0u;
+        }
+      }
+      ea[i] = bm_eval(a.ex_a, g, f);
+      eb[i] = bm_eval(a.ex_b, g, f);
+      ca += __popc(ea[i]);
+      cb += __popc(eb[i]);
     }
-    __syncthreads();
-    for (int k = 0; k < 32; k++) {
-      const u64 tile = grp * 32 + k;
-      if (tile >= tiles) break;
-      const u32 d = sm.dirty[k];
-      if (!d) continue;
-      const u32 dclr = sm.dclear[k];
-      const u64 prefix = a.tile_prefix[tile];
-      const u64 wt = tile * kBmTileWords;
-      const u32 inst = dm_tile_inst(a.map, tile);
-      const SegInfo seg = a.map.seg[inst];
-      const u64 w0 = wt + (u64)threadIdx.x * kBmWordsPerThread;
-      const int chunk = threadIdx.x / (kBmChunkWords / kBmWordsPerThread);
-      const bool read = (d >> chunk) & 1u;
-      const bool clr = a.inplace && ((dclr >> chunk) & 1u);
-      u32 ea[kBmWordsPerThread], eb[kBmWordsPerThread];
-      u32 ca = 0, cb = 0;
+    if (clr && a.dirty && (threadIdx.x % (kBmChunkWords / 8)) == 0)
+      a.dirty[tile * (kBmTileWords / kBmChunkWords) + threadIdx.x / (kBmChunkWords / 8)] = 0;
+    u64 tot;
+    const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
+    if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
+    u64 pa = (prefix >> 32) + (ex >> 32);
+    u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
+    u32 ob = (u32)(ex & 0xFFFFFFFFull);
 #pragma unroll
-      for (int i = 0; i < kBmWordsPerThread; i++) {
-        const u64 w = w0 + i;
-        u32 g = 0, f = 0;
-        if (read) {
-          g = a.g ? a.g[w] : 0u;
-          f = a.f ? a.f[w] : 0u;
-          if (clr) {
-            if (g) a.f[w] = f | g;
-            const_cast<u32 *>(a.g)[w] = 0u;
-          }
-        }
-        ea[i] = bm_eval(a.ex_a, g, f);
-        eb[i] = bm_eval(a.ex_b, g, f);
-        ca += __popc(ea[i]);
-        cb += __popc(eb[i]);
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
+      ob += __popc(eb[i]);
+      u32 x = la ? ea[i] : 0u;
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        if (pa < cap_a)
+          la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
+        else
+          atomicOr(&a.ctl->oob, 2048u);
+        pa++;
       }
-      u64 tot;
-      const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
-      if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
-      u64 pa = (prefix >> 32) + (ex >> 32);
-      u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
-      u32 ob = (u32)(ex & 0xFFFFFFFFull);
-#pragma unroll
-      for (int i = 0; i < kBmWordsPerThread; i++) {
-        if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
-        ob += __popc(eb[i]);
-        u32 x = la ? ea[i] : 0u;
-        while (x) {
-          const int b = __ffs(x) - 1;
-          x &= x - 1;
-          if (pa < cap_a)
-            la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
-          else
-            atomicOr(&a.ctl->oob, 2048u);
-          pa++;
-        }
-        x = lb ? eb[i] : 0u;
-        while (x) {
-          const int b = __ffs(x) - 1;
-          x &= x - 1;
-          if (pb < cap_b)
-            lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
-          else
-            atomicOr(&a.ctl->oob, 4096u);
-          pb++;
-        }
+      x = lb ? eb[i] : 0u;
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        if (pb < cap_b)
+          lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
+        else
+          atomicOr(&a.ctl->oob, 4096u);
+        pb++;
       }
-      if (a.idx_b) {
-        if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
-        __syncthreads();
-        // One slot per non-empty row of the tile: {c0, epoch, start, len}.
-        // Rows are 2^row_shift words, at most one tile, aligned in the tile.
-        const u32 rs = seg.row_shift;
-        const u64 row_words = 1ull << rs;
-        const u64 rows = kBmTileWords >> rs;
-        const u32 hi = a.map.seg_shift >= 31 ? 0u : (inst << a.map.seg_shift);
-        for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
-          const u64 lw = r << rs;  // first word of the row in the tile
-          if (wt + lw >= words || wt + lw < seg.base_word) break;
-          const u64 row = (wt + lw - seg.base_word) >> rs;
-          if (row >= seg.n) break;
-          const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
-          if (len) {
-            const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
-            index_insert(ix, epoch, hi | (u32)row, start, len, a.ctl);
-          }
+    }
+    if (a.idx_b) {
+      if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
+      __syncthreads();
+      // One slot per non-empty row of the tile: {c0, epoch, start, len}.
+      // Rows are 2^row_shift words, at most one tile, aligned in the tile.
+      const u32 rs = seg.row_shift;
+      const u64 row_words = 1ull << rs;
+      const u64 rows = kBmTileWords >> rs;
+      const u32 hi = a.map.seg_shift >= 31 ? 0u : (inst << a.map.seg_shift);
+      for (u64 r = threadIdx.x; r < rows; r += blockDim.x) {
+        const u64 lw = r << rs;  // first word of the row in the tile
+        if (wt + lw >= words || wt + lw < seg.base_word) break;
+        const u64 row = (wt + lw - seg.base_word) >> rs;
+        if (row >= seg.n) break;
+        const u32 len = sm.off_b[lw + row_words] - sm.off_b[lw];
+        if (len) {
+          const u32 start = (u32)((prefix & 0xFFFFFFFFull) + sm.off_b[lw]);
+          index_insert(ix, epoch, hi | (u32)row, start, len, a.ctl);
         }
       }
       __syncthreads();
@@ -421,35 +399,23 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   }
 }
 
-// Zero a NEWT bitmap in its dirty chunks and clear the dirty map (one block
-// per 32 tiles).  With only_if_empty, only when that source is empty (a
-// Copy from an empty source empties its destination, src/copy.cu:24-27).
-__global__ void __launch_bounds__(256) k_bm_clear_dirty(const RelDev *rd, DenseMap map, Ctl *ctl) {
-  __shared__ u32 s_d[32];
-  if (ctl_stop(ctl)) return;
-  u32 *G = rd->bmG, *D = rd->bmD;
-  const u64 tiles = bm_tiles(map.words);
-  const u64 groups = (tiles + 31) / 32;
-  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const u64 t = grp * 32 + threadIdx.x;
-      s_d[threadIdx.x] = t < tiles ? D[t] : 0u;
-      if (t < tiles && s_d[threadIdx.x]) D[t] = 0;
-    }
-    __syncthreads();
-    for (int k = 0; k < 32; k++) {
-      const u32 d = s_d[k];
-      if (!d) continue;
-      const u64 wt = (grp * 32 + k) * kBmTileWords;
-      // 256 threads x 8 words; thread t holds chunk t / 8
-      if ((d >> (threadIdx.x / 8)) & 1u) {
-        uint4 *p = reinterpret_cast<uint4 *>(G + wt + threadIdx.x * 8);
-        p[0] = make_uint4(0, 0, 0, 0);
-        p[1] = make_uint4(0, 0, 0, 0);
-      }
-    }
+// Zero a NEWT bitmap in its dirty chunks (all of it without a dirty map)
+// and clear the dirty map.  One block per tile.
+__device__ __forceinline__ void clear_newt_tiles(u32 *G, u8 *D, u64 words) {
+  const u64 tiles = bm_tiles(words);
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    if (!chunk_dirty(D, tile, threadIdx.x)) continue;
+    uint4 *p = reinterpret_cast<uint4 *>(G + tile * kBmTileWords + threadIdx.x * 8);
+    p[0] = make_uint4(0, 0, 0, 0);
+    p[1] = make_uint4(0, 0, 0, 0);
+    if (D && (threadIdx.x % (kBmChunkWords / 8)) == 0)
+      D[tile * (kBmTileWords / kBmChunkWords) + threadIdx.x / (kBmChunkWords / 8)] = 0;
   }
+}
+
+__global__ void __launch_bounds__(256) k_bm_clear_dirty(const RelDev *rd, DenseMap map, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  clear_newt_tiles(rd->bmG, rd->dirty, map.words);
 }
 
 // Set the bits of a key list (FULL at the start of a LIE; no dirty map).
@@ -478,7 +444,8 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, const Rel
   const u64 total = a.op->total;
   const u64 nc = a.op->nc;
   if (total == 0) return;
-  u32 *G = out_rd->bmG, *D = out_rd->bmD;
+  u32 *G = out_rd->bmG;
+  u8 *D = out_rd->dirty;
   const u64 *inner = a.inner->ptr;
   const u64 tiles = (total + kMatTile - 1) / kMatTile;
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -538,7 +505,8 @@ __global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, const RelDev *dest_
     if (blockIdx.x == 0 && threadIdx.x == 0 && c.once_pending) *c.once_pending = 1;
     return;
   }
-  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
+  u32 *G = dest_rd->bmG;
+  u8 *D = dest_rd->dirty;
   const u64 *src = c.src->ptr;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
     dm_set(map, G, D, gen_join(c.sel, src[i], 0), c.ctl);
@@ -553,66 +521,34 @@ __global__ void __launch_bounds__(256) k_copy_bm(CopyArgs c, const RelDev *dest_
 // copied).
 __global__ void __launch_bounds__(256) k_copy_empty_clear(CopyArgs c, const RelDev *dest_rd,
                                                           DenseMap map) {
-  __shared__ u32 s_d[32];
   if (ctl_stop(c.ctl)) return;
   if (c.once && *c.once) return;
   if (eff_count(c.src, c.src_vis) != 0) return;
-  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
-  const u64 tiles = bm_tiles(map.words);
-  const u64 groups = (tiles + 31) / 32;
-  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const u64 t = grp * 32 + threadIdx.x;
-      s_d[threadIdx.x] = t < tiles ? D[t] : 0u;
-      if (t < tiles && s_d[threadIdx.x]) D[t] = 0;
-    }
-    __syncthreads();
-    for (int k = 0; k < 32; k++) {
-      const u32 d = s_d[k];
-      if (!d) continue;
-      const u64 wt = (grp * 32 + k) * kBmTileWords;
-      if ((d >> (threadIdx.x / 8)) & 1u) {
-        uint4 *p = reinterpret_cast<uint4 *>(G + wt + threadIdx.x * 8);
-        p[0] = make_uint4(0, 0, 0, 0);
-        p[1] = make_uint4(0, 0, 0, 0);
-      }
-    }
-  }
+  clear_newt_tiles(dest_rd->bmG, dest_rd->dirty, map.words);
 }
 
 // RelationalACopy (src/acopy.cu:12-50): dest NEWT := sel(src NEWT).  The
 // destination NEWT was cleared by k_bm_clear_dirty just before; the source
-// NEWT bitmap is read in its dirty chunks only.
+// NEWT bitmap is read in its dirty chunks only.  One block per tile.
 __global__ void __launch_bounds__(256) k_acopy_bm(const RelDev *src_rd, Sel2 sel,
                                                   const RelDev *dest_rd, DenseMap map, Ctl *ctl) {
-  __shared__ u32 s_d[32];
   if (ctl_stop(ctl)) return;
-  const u32 *S = src_rd->bmG, *SD = src_rd->bmD;
-  u32 *G = dest_rd->bmG, *D = dest_rd->bmD;
+  const u32 *S = src_rd->bmG;
+  const u8 *SD = src_rd->dirty;
+  u32 *G = dest_rd->bmG;
+  u8 *D = dest_rd->dirty;
   const u64 tiles = bm_tiles(map.words);
-  const u64 groups = (tiles + 31) / 32;
-  for (u64 grp = blockIdx.x; grp < groups; grp += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const u64 t = grp * 32 + threadIdx.x;
-      s_d[threadIdx.x] = t < tiles ? SD[t] : 0u;
-    }
-    __syncthreads();
-    for (int k = 0; k < 32; k++) {
-      const u32 d = s_d[k];
-      if (!d || !((d >> (threadIdx.x / 8)) & 1u)) continue;
-      const u64 tile = grp * 32 + k;
-      const u32 inst = dm_tile_inst(map, tile);
-      const SegInfo seg = map.seg[inst];
-      const u64 w0 = tile * kBmTileWords + threadIdx.x * 8;
-      for (int i = 0; i < 8; i++) {
-        u32 x = S[w0 + i];
-        while (x) {
-          const int b = __ffs(x) - 1;
-          x &= x - 1;
-          dm_set(map, G, D, gen_join(sel, dm_key(map, inst, seg, w0 + i, b), 0), ctl);
-        }
+  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    if (!chunk_dirty(SD, tile, threadIdx.x)) continue;
+    const u32 inst = dm_tile_inst(map, tile);
+    const SegInfo seg = map.seg[inst];
+    const u64 w0 = tile * kBmTileWords + threadIdx.x * 8;
+    for (int i = 0; i < 8; i++) {
+      u32 x = S[w0 + i];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        dm_set(map, G, D, gen_join(sel, dm_key(map, inst, seg, w0 + i, b), 0), ctl);
       }
     }
   }

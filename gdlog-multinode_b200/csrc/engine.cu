@@ -164,6 +164,7 @@ struct gdl_engine {
   int join_ctas_per_sm = 8;   // gdl_tuning
   int count_ctas_per_sm = 4;
   int index_slots_per_key = 2;
+  int dirty_min_log2_words = 24;
   // Batched form (gdl_engine_set_instances): the block-diagonal layout.
   bool instances = false;
   std::vector<SegInfo> segs;
@@ -422,17 +423,19 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   RelHost &rh = e->rels[r];
   RelDev &h = e->h[r];
   if (rh.bm_words != words) {
-    for (u32 **p : {&h.bmF, &h.bmG, &h.bmD}) {
+    for (u32 **p : {&h.bmF, &h.bmG}) {
       dfree(e, *p);
       *p = nullptr;
     }
+    dfree(e, h.bmD);
+    h.bmD = nullptr;
     dfree(e, h.tile_prefix);
     h.tile_prefix = nullptr;
     rh.bm_words = words;
   }
   const u64 tiles = words / kBmTileWords;
   if (!h.bmG) TRY(dalloc(e, (void **)&h.bmG, words * 4));
-  if (!h.bmD) TRY(dalloc(e, (void **)&h.bmD, tiles * 4));
+  if (!h.bmD) TRY(dalloc(e, (void **)&h.bmD, words / kBmChunkWords));
   if (!h.tile_prefix) TRY(dalloc(e, (void **)&h.tile_prefix, tiles * sizeof(u64)));
   if (with_full && !h.bmF) TRY(dalloc(e, (void **)&h.bmF, words * 4));
   memset(&h.scan, 0, sizeof h.scan);
@@ -598,16 +601,14 @@ void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
   a.ctl = e->d_ctl;
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[4];
-  PLAUNCH(kc, kPBitmap,
-          k_bm_tilecount<<<grid_for(e, (tiles + 31) / 32, 1, 8), kBmBlock, 0, e->s>>>(a));
+  PLAUNCH(kc, kPBitmap, k_bm_tilecount<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(a));
   PLAUNCH(kc, kPBitmap,
           k_bm_scan<<<grid_for(e, tiles / kScanChunk + 1, 1, 4), kBmBlock, 0, e->s>>>(a));
 }
 void launch_scan_write(gdl_engine *e, BmScanArgs a, Counts *kc) {
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[5];
-  PLAUNCH(kc, kPBitmap,
-          k_bm_write<<<grid_for(e, (tiles + 31) / 32, 1, 8), kBmBlock, 0, e->s>>>(a));
+  PLAUNCH(kc, kPBitmap, k_bm_write<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(a));
 }
 void launch_scan(gdl_engine *e, BmScanArgs a, int rel, Counts *kc) {
   launch_scan_count(e, a, rel, kc);
@@ -652,8 +653,8 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
           // chunks only).
           BmScanArgs c = scan_none(map);
           c.g = oh.bmG;
-          c.dirty = oh.bmD;
-          c.skip_clean = 1;
+          c.dirty = oh.dirty;
+          c.skip_clean = oh.dirty != nullptr;
           c.ex_a = kBmUnion;
           c.list_a = &R[op.outer].newt;
           c.need_a = need_index(op.outer, kNeedNewt);
@@ -731,15 +732,15 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
       if (dense && op.kind == 2) {
         // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
-        const u64 groups = words / kBmTileWords / 32 + 1;
-        PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+        const u64 tiles = words / kBmTileWords;
+        PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
                                   &R[op.out], map, e->d_ctl));
         if (sh.bmG)  // a source without a NEWT bitmap (static) has an empty NEWT
-          PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+          PLAUNCH(kc, kPCopy, k_acopy_bm<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
                                   &R[op.inner], op.sel, &R[op.out], map, e->d_ctl));
       } else if (dense) {
-        const u64 groups = words / kBmTileWords / 32 + 1;
-        PLAUNCH(kc, kPBitmap, k_copy_empty_clear<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+        const u64 tiles = words / kBmTileWords;
+        PLAUNCH(kc, kPBitmap, k_copy_empty_clear<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
                                   c, &R[op.out], map));
         PLAUNCH(kc, kPCopy, k_copy_bm<<<grid_for(e, cap, 256, 8), 256, 0, s>>>(
                                 c, &R[op.out], map));
@@ -769,7 +770,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       BmScanArgs a = scan_none(L.map);
       a.rd = &R[r];
       a.inplace = 1;
-      a.skip_clean = !plan.full_list[r];
+      a.skip_clean = !plan.full_list[r] && e->h[r].dirty != nullptr;
       a.gated = 1;
       a.inst_delta = L.d_inst_delta;
       a.ex_a = kBmDelta;
@@ -789,9 +790,9 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
                                                          (int)L.update.size(), e->d_ctl));
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
-    const u64 groups = L.map.words / kBmTileWords / 32 + 1;
+    const u64 tiles = L.map.words / kBmTileWords;
     for (int r : L.tmps)
-      PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, groups, 1, 8), 256, 0, s>>>(
+      PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
                                 &R[r], L.map, e->d_ctl));
   }
   for (int r : L.update) {
@@ -1002,7 +1003,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     L.dense = e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits);
     L.dk = L.dense && !e->instances ? dk : 0;
   }
-  for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+  for (RelDev &h : e->h) {
+    h.dense = h.full_lazy = 0;
+    h.dirty = nullptr;
+  }
   if (L.dense) {
     if (e->instances) {
       L.map = DenseMap{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
@@ -1033,6 +1037,12 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       TRY(ensure_bitmaps(e, r, words, false));
       e->h[r].dense = 1;
     }
+    // A dirty map pays when a NEWT bitmap is too large to scan whole every
+    // iteration; for small ones the scans read everything and the joins
+    // skip the extra store.
+    const bool use_dirty = words >= (1ull << e->dirty_min_log2_words);
+    for (auto *v : {&L.update, &L.tmps})
+      for (int r : *v) e->h[r].dirty = use_dirty ? e->h[r].bmD : nullptr;
     TRY(ensure_dense_scratch(e, words));
     // Every list of the loop is bounded by the key domain: size them for
     // it up front (within a quarter of free HBM shared among the lists), so
@@ -1077,7 +1087,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       const RelDev &h = e->h[r];
       CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(h.bmG, 0, words * 4, e->s));
-      CK(e, cudaMemsetAsync(h.bmD, 0, words / kBmTileWords * 4, e->s));
+      CK(e, cudaMemsetAsync(h.bmD, 0, words / kBmChunkWords, e->s));
       if (h.full.n)
         k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
             &e->d_rels[r].full, h.bmF, L.map, e->d_ctl);
@@ -1085,7 +1095,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     }
     for (int r : L.tmps) {
       CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
-      CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmTileWords * 4, e->s));
+      CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmChunkWords, e->s));
     }
     CK(e, cudaGetLastError());
   }
@@ -1224,7 +1234,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         for (auto *v : {&L.update, &L.tmps})
           for (int r : *v) {
             CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
-            CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmTileWords * 4, e->s));
+            CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmChunkWords, e->s));
           }
       }
       if (resume) {
@@ -1318,7 +1328,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       CK(e, cudaGetLastError());
       TRY(pull(e));
     }
-    for (RelDev &h : e->h) h.dense = h.full_lazy = 0;
+    for (RelDev &h : e->h) {
+      h.dense = h.full_lazy = 0;
+      h.dirty = nullptr;
+    }
     TRY(push(e));
     c.iteration = kept_iteration;
   }
@@ -1449,8 +1462,9 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
-    for (u32 *bm : {r.bmF, r.bmG, r.bmD})
+    for (u32 *bm : {r.bmF, r.bmG})
       if (bm) cudaFreeAsync(bm, e->s);
+    if (r.bmD) cudaFreeAsync(r.bmD, e->s);
     if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);
     if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
   }
@@ -1880,13 +1894,15 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       t->join_ctas_per_sm > 32 || t->count_ctas_per_sm < 0 || t->count_ctas_per_sm > 32 ||
       t->index_slots_per_key < 0 || t->index_slots_per_key > 64 ||
       (t->index_slots_per_key && (t->index_slots_per_key < 2 ||
-                                  (t->index_slots_per_key & (t->index_slots_per_key - 1)))))
+                                  (t->index_slots_per_key & (t->index_slots_per_key - 1)))) ||
+      (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)))
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
   if (t->join_ctas_per_sm) e->join_ctas_per_sm = t->join_ctas_per_sm;
   if (t->count_ctas_per_sm) e->count_ctas_per_sm = t->count_ctas_per_sm;
   if (t->index_slots_per_key) e->index_slots_per_key = t->index_slots_per_key;
+  if (t->dirty_min_log2_words) e->dirty_min_log2_words = t->dirty_min_log2_words;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -1898,6 +1914,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->join_ctas_per_sm = e->join_ctas_per_sm;
   t->count_ctas_per_sm = e->count_ctas_per_sm;
   t->index_slots_per_key = e->index_slots_per_key;
+  t->dirty_min_log2_words = e->dirty_min_log2_words;
   return GDL_OK;
 }
 

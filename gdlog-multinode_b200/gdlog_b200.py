@@ -52,7 +52,7 @@ class Tuning(C.Structure):
     """gdl_tuning (include/gdlog_b200.h); a zero field keeps the default."""
     _fields_ = [("dedup", C.c_int32), ("dense_max_bits", C.c_int32),
                 ("join_ctas_per_sm", C.c_int32), ("count_ctas_per_sm", C.c_int32),
-                ("index_slots_per_key", C.c_int32)]
+                ("index_slots_per_key", C.c_int32), ("dirty_min_log2_words", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -326,7 +326,10 @@ class Engine:
         self.h = h
         self.relations: list[Relation] = []
         if kind == "gpu" and dedup is not None:
-            self._check(self.lib.gdl_engine_set_dedup(self.h, self.DEDUP[dedup], 0))
+            if dedup == "dense_dirty":  # bitmaps, with dirty maps at every size
+                self.set_tuning(dedup="dense", dirty_min_log2_words=11)
+            else:
+                self._check(self.lib.gdl_engine_set_dedup(self.h, self.DEDUP[dedup], 0))
 
     def close(self) -> None:
         if self.h:

@@ -57,11 +57,12 @@ def test_batched_oracle_loop_matches_itself():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("seed", [1, 2])
-def test_batched_tc_matches_plain_and_oracle(seed):
+@pytest.mark.parametrize("seed,dirty", [(1, 24), (2, 11)])
+def test_batched_tc_matches_plain_and_oracle(seed, dirty):
     inst = dag_instances(12, seed)
     inst.append((np.zeros((0, 2), dtype=np.uint64),))  # an instance without edges
     with Engine("gpu") as g:
+        g.set_tuning(dirty_min_log2_words=dirty)
         batched = B.run_batched(g, P.tc, inst)
         plain = B.run_plain_loop(g, P.tc, inst)
     with Engine("oracle") as o:
@@ -73,6 +74,7 @@ def test_batched_tc_matches_plain_and_oracle(seed):
 def test_batched_sg_matches_oracle():
     inst = sg_instances(8, 3)
     with Engine("gpu") as g:
+        g.set_tuning(dirty_min_log2_words=11)
         batched = B.run_batched(g, P.sg, inst)
     with Engine("oracle") as o:
         oracle = B.run_plain_loop(o, P.sg, inst)
@@ -83,6 +85,7 @@ def test_batched_sg_matches_oracle():
 def test_batched_cspa_matches_oracle():
     inst = cspa_instances(6, 4)
     with Engine("gpu") as g:
+        g.set_tuning(dirty_min_log2_words=11)
         batched = B.run_batched(g, P.cspa, inst)
     with Engine("oracle") as o:
         oracle = B.run_plain_loop(o, P.cspa, inst)

@@ -24,7 +24,7 @@ pytestmark = pytest.mark.gpu
 # Both deduplication paths of the engine: radix sort + merge-path merge, and
 # bitmaps over the key domain (every workload here has a small domain, so
 # "dense" is what the engine picks by itself).
-MODES = ["sort", "dense"]
+MODES = ["sort", "dense", "dense_dirty"]
 
 
 def summarize(r):
@@ -231,10 +231,10 @@ def test_modes_agree_on_cspa_with_clear():
     assign, deref = W.cspa_facts(200, 400, 150, seed=8)
     out = []
     with Engine("gpu") as g:
-        for mode in ("sort", "dense", "sort"):
+        for mode, dirty in (("sort", 24), ("dense", 24), ("dense", 11), ("sort", 24)):
             g.clear()
-            g.lib.gdl_engine_set_dedup(g.h, Engine.DEDUP[mode], 0)
+            g.set_tuning(dedup=mode, dirty_min_log2_words=dirty)
             out.append(summarize(P.cspa(g, assign, deref, sync=g.sync)))
     with Engine("oracle") as o:
         want = summarize(P.cspa(o, assign, deref))
-    assert out[0] == out[1] == out[2] == want
+    assert out[0] == out[1] == out[2] == out[3] == want
