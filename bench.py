@@ -365,6 +365,11 @@ def run_dag_batch(a) -> None:
     inst = [(e,) for (_, _, e) in dags]
     counts = [L * Wd for (L, Wd, _) in dags]
     eng = Engine("gpu")
+    if a.single:
+        rb = B.run_batched(eng, P.tc, inst, node_counts=counts)
+        print(json.dumps({"single_step_ms": rb.device_ms, "launches": rb.kernels}), flush=True)
+        eng.close()
+        return
     for _ in range(a.warmup):
         B.run_batched(eng, P.tc, inst, node_counts=counts)
     ms_b, wall_b = [], []
