@@ -62,6 +62,19 @@ def globalize(instances, shift: int):
     return out
 
 
+def shard_instances(costs, world: int, rank: int) -> list:
+    """Instances of `rank` when `world` GPUs share a batch: largest cost
+    first, each to the currently least-loaded rank (LPT).  Deterministic, so
+    every rank computes the same partition without communicating."""
+    load = [0.0] * world
+    owner = [0] * len(costs)
+    for i in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += costs[i]
+    return [i for i in range(len(costs)) if owner[i] == rank]
+
+
 def run_batched(eng, prog, instances, node_counts=None) -> BatchRun:
     """Run `prog` (a programs.* builder) once over all instances."""
     n = len(instances)

@@ -102,3 +102,47 @@ def test_batched_large_instances_keep_full_as_bitmap():
         batched = B.run_batched(g, P.tc, inst)
         plain = B.run_plain_loop(g, P.tc, inst)
     assert as_tuples(batched) == as_tuples(plain)
+
+
+def test_shard_instances_partitions_and_balances():
+    costs = [float(c) for c in np.random.default_rng(5).integers(1, 1000, size=97)]
+    for world in (1, 2, 3, 8):
+        parts = [B.shard_instances(costs, world, r) for r in range(world)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+
+
+def _shard_worker(rank, world, port, costs, q):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    mine = B.shard_instances(costs, world, rank)
+    out = [None] * world
+    dist.all_gather_object(out, mine)
+    if rank == 0:
+        q.put(out)
+    dist.destroy_process_group()
+
+
+def test_shard_instances_agree_across_gloo_ranks():
+    """Every rank computes the same partition without exchanging work."""
+    import multiprocessing as mp
+    import socket
+
+    costs = [float(c) for c in np.random.default_rng(9).integers(1, 500, size=40)]
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, costs, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    parts = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+    assert sorted(parts[0] + parts[1]) == list(range(40))
+    assert not set(parts[0]) & set(parts[1])
+    assert parts == [B.shard_instances(costs, 2, r) for r in range(2)]
