@@ -448,45 +448,30 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, const Rel
   u8 *D = out_rd->dirty;
   const u64 *inner = a.inner->ptr;
   const u64 tiles = (total + kMatTile - 1) / kMatTile;
-  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const u64 p0 = tile * kMatTile;
-    const u64 p1 = min(p0 + kMatTile, total);
+  for (u64 batch = blockIdx.x; batch < tiles; batch += (u64)gridDim.x * kMatBlock) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      u64 lo = 0, hi = nc;
-      while (hi - lo > 1) {
-        u64 mid = (lo + hi) >> 1;
-        if (a.crow_off[mid] <= p0)
-          lo = mid;
-        else
-          hi = mid;
-      }
-      sm.k0 = lo;
-      sm.nrec = (u32)min((u64)kMatTile, nc - lo);
-    }
-    __syncthreads();
-    const u64 k0 = sm.k0;
-    const u32 m = sm.nrec;
-    for (u32 i = threadIdx.x; i <= m; i += blockDim.x) {
-      sm.off[i] = a.crow_off[k0 + i];
-      if (i < m) {
-        sm.start[i] = a.crow_start[k0 + i];
-        sm.key[i] = a.crow_key[k0 + i];
-      }
-    }
-    __syncthreads();
-    u64 p = p0 + (u64)threadIdx.x * kMatPer;
-    if (p < p1) {
-      u32 r = find_rec(sm.off, m, p);
-      u64 next = sm.off[r + 1];
-      const u64 pe = min(p + kMatPer, p1);
-      for (; p < pe; p++) {
-        while (p >= next) {
-          r++;
-          next = sm.off[r + 1];
+    mat_batch_starts(a.crow_off, nc, tiles, batch, sm.tile_k0);
+    for (u32 j = 0; j < kMatBlock; j++) {
+      const u64 tile = batch + (u64)j * gridDim.x;
+      if (tile >= tiles) break;
+      const u64 p0 = tile * kMatTile;
+      const u64 p1 = min(p0 + kMatTile, total);
+      __syncthreads();
+      const u32 m = mat_stage_tile(a, nc, sm.tile_k0[j], sm);
+      __syncthreads();
+      u64 p = p0 + (u64)threadIdx.x * kMatPer;
+      if (p < p1) {
+        u32 r = find_rec(sm.off, m, p);
+        u64 next = sm.off[r + 1];
+        const u64 pe = min(p + kMatPer, p1);
+        for (; p < pe; p++) {
+          while (p >= next) {
+            r++;
+            next = sm.off[r + 1];
+          }
+          const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+          if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
         }
-        const u64 t = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
-        if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
       }
     }
   }
@@ -592,7 +577,7 @@ __global__ void __launch_bounds__(256) k_inst_tile_pop(const u32 *bm, DenseMap m
 // digest terms of every tuple, summed per instance.
 __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map,
                                                      const u64 *tile_rank, u64 *acc) {
-  __shared__ u32 s_off[257];
+  __shared__ u64 s_warp[kBmBlock / 32];
   const u64 tiles = bm_tiles(map.words);
   for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
     const u32 inst = dm_tile_inst(map, t);
@@ -601,19 +586,10 @@ __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map
     u32 cnt = 0;
     for (int i = 0; i < kBmWordsPerThread; i++)
       if (w0 + i < map.words) cnt += __popc(bm[w0 + i]);
-    // exclusive scan of cnt over the block (small, via shared memory)
-    s_off[threadIdx.x] = cnt;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      u32 run = 0;
-      for (int k = 0; k < 256; k++) {
-        const u32 v = s_off[k];
-        s_off[k] = run;
-        run += v;
-      }
-    }
-    __syncthreads();
-    u64 rank = tile_rank[t] + s_off[threadIdx.x];
+    u64 tile_n;
+    const u64 ex = block_excl_scan<kBmBlock>(cnt, s_warp, &tile_n);
+    if (tile_n == 0) continue;  // uniform: every thread saw the same total
+    u64 rank = tile_rank[t] + ex;
     u64 h_sum = 0;
     for (int i = 0; i < kBmWordsPerThread; i++) {
       const u64 w = w0 + i;
@@ -632,8 +608,10 @@ __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map
         rank++;
       }
     }
-    if (h_sum) atomicAdd(&acc[inst], h_sum);
-    __syncthreads();
+    // one atomic per tile: the tile's terms summed over the block
+    u64 dummy;
+    const u64 ex_h = block_excl_scan<kBmBlock>(h_sum, s_warp, &dummy);
+    if (threadIdx.x == kBmBlock - 1 && (ex_h + h_sum)) atomicAdd(&acc[inst], ex_h + h_sum);
   }
 }
 

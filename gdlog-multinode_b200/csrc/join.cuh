@@ -220,9 +220,43 @@ struct MatSmem {
   u64 off[kMatTile + 1];
   u32 start[kMatTile];
   u64 key[kMatTile];
-  u64 k0;
-  u32 nrec;
+  u64 tile_k0[kMatBlock];  // first record of each tile of the current batch
 };
+
+// Materialisation tiles are handed out round-robin (tile = blockIdx.x +
+// j * gridDim.x).  A block finds the first records of its next kMatBlock
+// tiles at once, one binary search over crow_off per thread, so the
+// dependent global loads of the searches overlap instead of stalling the
+// block before every tile.
+__device__ __forceinline__ void mat_batch_starts(const u64 *crow_off, u64 nc, u64 tiles,
+                                                 u64 batch, u64 *tile_k0) {
+  const u64 t = batch + (u64)threadIdx.x * gridDim.x;
+  if (t >= tiles) return;
+  const u64 p0 = t * kMatTile;
+  u64 lo = 0, hi = nc;  // largest k with crow_off[k] <= p0
+  while (hi - lo > 1) {
+    const u64 mid = (lo + hi) >> 1;
+    if (crow_off[mid] <= p0)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  tile_k0[threadIdx.x] = lo;
+}
+
+// Stage the records of one tile (k0 .. k0+m-1 cover its positions; each
+// record holds >= 1 output) in shared memory.
+__device__ __forceinline__ u32 mat_stage_tile(const JoinArgs &a, u64 nc, u64 k0, MatSmem &sm) {
+  const u32 m = (u32)min((u64)kMatTile, nc - k0);
+  for (u32 i = threadIdx.x; i <= m; i += blockDim.x) {
+    sm.off[i] = a.crow_off[k0 + i];
+    if (i < m) {
+      sm.start[i] = a.crow_start[k0 + i];
+      sm.key[i] = a.crow_key[k0 + i];
+    }
+  }
+  return m;
+}
 
 __global__ void __launch_bounds__(kMatBlock) k_join_mat(JoinArgs a) {
   __shared__ MatSmem sm;
@@ -239,51 +273,33 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat(JoinArgs a) {
   u64 *out = a.out_newt->ptr + base;
   const u64 cap_left = a.out_newt->cap - base;
   const u64 tiles = (total + kMatTile - 1) / kMatTile;
-  for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const u64 p0 = tile * kMatTile;
-    const u64 p1 = min(p0 + kMatTile, total);
+  for (u64 batch = blockIdx.x; batch < tiles; batch += (u64)gridDim.x * kMatBlock) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      // largest k with crow_off[k] <= p0
-      u64 lo = 0, hi = nc;
-      while (hi - lo > 1) {
-        u64 mid = (lo + hi) >> 1;
-        if (a.crow_off[mid] <= p0)
-          lo = mid;
+    mat_batch_starts(a.crow_off, nc, tiles, batch, sm.tile_k0);
+    for (u32 j = 0; j < kMatBlock; j++) {
+      const u64 tile = batch + (u64)j * gridDim.x;
+      if (tile >= tiles) break;
+      const u64 p0 = tile * kMatTile;
+      const u64 p1 = min(p0 + kMatTile, total);
+      __syncthreads();
+      const u32 m = mat_stage_tile(a, nc, sm.tile_k0[j], sm);
+      __syncthreads();
+      // Two rounds of one 16-byte store (two tuples) per thread.
+      for (u64 q = threadIdx.x; q < (u64)kMatTile / 2; q += blockDim.x) {
+        const u64 p = p0 + 2 * q;
+        if (p >= p1) break;
+        u32 r = find_rec(sm.off, m, p);
+        u64 o0 = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+        u64 o1 = o0;
+        if (p + 1 < total) {
+          if (p + 1 >= sm.off[r + 1]) r++;
+          o1 = gen_join(a.sel, inner[sm.start[r] + (p + 1 - sm.off[r])], sm.key[r]);
+        }
+        if (p + 1 < cap_left)
+          reinterpret_cast<ulonglong2 *>(out)[p >> 1] = make_ulonglong2(o0, o1);
         else
-          hi = mid;
+          atomicOr(&a.ctl->oob, 128u);
       }
-      sm.k0 = lo;
-      // records k0 .. k0+m-1 cover [p0, p1); each holds >= 1 output
-      u64 m = min((u64)kMatTile, nc - lo);
-      sm.nrec = (u32)m;
-    }
-    __syncthreads();
-    const u64 k0 = sm.k0;
-    const u32 m = sm.nrec;
-    for (u32 i = threadIdx.x; i <= m; i += blockDim.x) {
-      sm.off[i] = a.crow_off[k0 + i];
-      if (i < m) {
-        sm.start[i] = a.crow_start[k0 + i];
-        sm.key[i] = a.crow_key[k0 + i];
-      }
-    }
-    __syncthreads();
-    // Two rounds of one 16-byte store (two tuples) per thread.
-    for (u64 q = threadIdx.x; q < (u64)kMatTile / 2; q += blockDim.x) {
-      const u64 p = p0 + 2 * q;
-      if (p >= p1) break;
-      u32 r = find_rec(sm.off, m, p);
-      u64 o0 = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
-      u64 o1 = o0;
-      if (p + 1 < total) {
-        if (p + 1 >= sm.off[r + 1]) r++;
-        o1 = gen_join(a.sel, inner[sm.start[r] + (p + 1 - sm.off[r])], sm.key[r]);
-      }
-      if (p + 1 < cap_left)
-        reinterpret_cast<ulonglong2 *>(out)[p >> 1] = make_ulonglong2(o0, o1);
-      else
-        atomicOr(&a.ctl->oob, 128u);
     }
   }
   // The last block to finish publishes the new NEWT count.
