@@ -151,6 +151,11 @@ def oracle_run(wl: dict, inputs, threads: int = 0):
         return secs, derived(r), eng.threads
 
 
+def single_families(prof):
+    return {kd: {"launches": v["launches"], "alg_bytes": v["bytes"]}
+            for kd, v in prof.items() if v["launches"]}
+
+
 def traffic_for(kind: str, alg_bytes_per_launch: float):
     """DRAM bytes per launch from the committed ncu summary of this kernel
     family, scaled by algorithmic bytes (capture of a smaller case)."""
@@ -228,8 +233,15 @@ def run_ours(a) -> None:
             dist.barrier()
 
     if a.single:
+        # one step with an event pair around every launch; the algorithmic
+        # bytes per kernel family are what an ncu capture of this same
+        # command is compared against
+        eng.profile_reset()
+        eng.set_profile(True)
         ms, t, k = device_step()
-        print(json.dumps({"single_step_ms": ms, "tuples": t, "launches": k}), flush=True)
+        eng.set_profile(False)
+        print(json.dumps({"single_step_ms": ms, "tuples": t, "launches": k,
+                          "families": single_families(eng.profile())}), flush=True)
         eng.close()
         return
     for _ in range(a.warmup):
@@ -378,8 +390,12 @@ def run_dag_batch(a) -> None:
     counts = [L * Wd for (L, Wd, _) in dags]
     eng = Engine("gpu", device=local)
     if a.single:
+        eng.profile_reset()
+        eng.set_profile(True)
         rb = B.run_batched(eng, P.tc, inst, node_counts=counts)
-        print(json.dumps({"single_step_ms": rb.device_ms, "launches": rb.kernels}), flush=True)
+        eng.set_profile(False)
+        print(json.dumps({"single_step_ms": rb.device_ms, "launches": rb.kernels,
+                          "families": single_families(eng.profile())}), flush=True)
         eng.close()
         return
     for _ in range(a.warmup):

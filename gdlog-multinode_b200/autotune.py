@@ -4,8 +4,10 @@ The reference fixes its launch shape per driver (grid = 32 x SMs, block 512,
 test/tc.cu:223-225) and its index load factor (0.8, src/relation.cu:836).
 Here the engine exposes, through gdl_tuning, the choices whose best value
 depends on the instance: the dedup path (bitmaps or radix sort + merge), the
-largest domain kept as bitmaps, the CTAs per SM of the join's count and
-materialisation passes, and the slots per key of the hashed index.  The
+largest domain kept as bitmaps, the form of a join into bitmaps (one
+probe-and-expand pass, or count + materialise passes), the CTAs per SM of
+the join's count and materialisation passes, and the slots per key of the
+hashed index.  The
 radix sort's digit width is fixed at 8 bits; its number of passes already
 follows the key width.
 
@@ -30,10 +32,22 @@ DEFAULT_CACHE = os.path.join(HERE, "tuning_cache.json")
 # Candidate values per parameter (0 keeps the engine's default).
 SPACE = {
     "dedup": ["dense", "sort"],
+    "dense_join_passes": [1, 2],
     "join_ctas_per_sm": [4, 8, 16],
     "count_ctas_per_sm": [2, 4, 8],
     "index_slots_per_key": [2, 4],
 }
+
+
+def _redundant(cfg: dict) -> bool:
+    """Configurations that differ from an earlier one only in a parameter
+    their path does not read: the join form of the sort path, and the grids
+    of the count / materialise passes of the one-pass dense join."""
+    if cfg.get("dedup") == "sort" and cfg.get("dense_join_passes", 1) != 1:
+        return True
+    if cfg.get("dedup") == "dense" and cfg.get("dense_join_passes", 1) == 1:
+        return (cfg.get("count_ctas_per_sm", 2) != 2 or cfg.get("join_ctas_per_sm", 4) != 4)
+    return False
 
 
 def bucket(program: str, inputs) -> str:
@@ -49,8 +63,7 @@ def bucket(program: str, inputs) -> str:
 def candidates(space=SPACE, limit=None):
     keys = list(space)
     out = [dict(zip(keys, vals)) for vals in itertools.product(*(space[k] for k in keys))]
-    # the sort path does not use the hashed-index choice differently; keep
-    # the grid the same size for both paths (small, so tuning stays cheap)
+    out = [c for c in out if not _redundant(c)]
     return out[:limit] if limit else out
 
 

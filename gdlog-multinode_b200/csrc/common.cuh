@@ -56,7 +56,7 @@ struct BmScanRec {
   u64 total_a, total_b;  // list sizes
   u64 pop_g;             // popcount of NEWT (accumulated, reset by the write pass)
   u32 overflow;          // a list is too small
-  u32 pad;
+  u32 n_listed;          // dirty chunks listed by k_bm_dirty_chunks
 };
 
 // One instance of a batched LIE in the dense (bitmap) form: its rows start at

@@ -132,6 +132,10 @@ struct BmScanArgs {
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
   int gated;           // the overflow is raised by k_scan_gate, not by k_bm_write
   u64 *tile_prefix;    // [tiles] tile counts, then their exclusive prefix (a << 32 | b)
+  // Listed mode (dirty map, skip_clean, no index): [chunks] the dirty
+  // 64-word chunks in order; tile_prefix then holds one entry per group of
+  // kGroupChunks listed chunks.  Null: whole tiles.
+  u32 *chunk_list;
   BmScanRec *rec;
   LaunchRec *lrec;
   Lb lb;
@@ -148,6 +152,137 @@ __device__ __forceinline__ void scan_bind(BmScanArgs &a) {
     a.f = a.rd->bmF;
     a.dirty = a.rd->dirty;
   }
+}
+
+// Listed mode.  A large NEWT bitmap touched in few places (the batched form:
+// a fraction of every active instance's rows each iteration) is scanned by
+// its dirty chunks only.  Pass 0 lists the dirty chunks in order; the count
+// and write passes then give each warp a group of kGroupChunks listed chunks
+// (8 words per lane), with warp shuffles instead of block barriers, and the
+// scan pass (k_bm_scan) runs over the group counts.
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kBmBlock * kScanItems;
+constexpr int kGroupChunks = 32 * 8 / kBmChunkWords;  // 4
+constexpr int kDirtyItems = 16;                       // dirty bytes per thread (one uint4)
+constexpr int kDirtyUnit = kBmBlock * kDirtyItems;    // chunks per look-back unit
+
+__device__ __forceinline__ u64 scan_items(const BmScanArgs &a) {
+  return a.chunk_list ? (a.rec->n_listed + kGroupChunks - 1) / kGroupChunks
+                      : bm_tiles(a.map.words);
+}
+
+// Pass 0 (listed mode): the ordered list of dirty chunks (decoupled
+// look-back over units of kDirtyUnit chunks).
+__global__ void __launch_bounds__(kBmBlock) k_bm_dirty_chunks(BmScanArgs a) {
+  __shared__ u64 s_scan[kBmBlock / 32];
+  __shared__ long long s_unit;
+  __shared__ u64 s_base;
+  if (ctl_stop(a.ctl)) return;
+  scan_bind(a);
+  const u64 chunks = a.map.words / kBmChunkWords;  // words: whole tiles, so a multiple of 32
+  const u64 units = (chunks + kDirtyUnit - 1) / kDirtyUnit;
+  const u32 gen = a.lrec->gen;
+  while (true) {
+    const long long c = grab_tile(a.lrec, &s_unit);
+    if (c >= (long long)units) break;
+    const u64 c0 = (u64)c * kDirtyUnit + (u64)threadIdx.x * kDirtyItems;
+    u32 bits = 0;
+    if (c0 < chunks) {
+      if (a.dirty) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(a.dirty + c0);
+        const u32 q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < kDirtyItems; i++)
+          if ((q[i >> 2] >> (8 * (i & 3))) & 0xFFu) bits |= 1u << i;
+      } else {
+        bits = (1u << kDirtyItems) - 1u;
+      }
+    }
+    u64 tot;
+    const u64 ex = block_excl_scan<kBmBlock>((u64)__popc(bits), s_scan, &tot);
+    if (threadIdx.x < 32) {
+      u64 prefix = 0;
+      if (c == 0) {
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, true, tot);
+      } else {
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, false, tot);
+        prefix = lb_warp_prefix(a.lb, c, gen, a.ctl);
+        if (threadIdx.x == 0) lb_publish(a.lb, c, gen, true, prefix + tot);
+      }
+      if (threadIdx.x == 0) {
+        s_base = prefix;
+        if ((u64)c == units - 1) a.rec->n_listed = (u32)(prefix + tot);
+      }
+    }
+    __syncthreads();
+    u64 pos = s_base + ex;
+    while (bits) {
+      const int i = __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (pos < chunks) a.chunk_list[pos] = (u32)(c0 + i);
+      pos++;
+    }
+  }
+  launch_rec_finish(a.lrec);
+}
+
+// The listed chunk and the 8 words a lane covers in group gi (false past the list).
+__device__ __forceinline__ bool group_words(const BmScanArgs &a, u64 n_listed, u64 gi, int lane,
+                                            u64 *chunk, u64 *w0) {
+  const u64 li = gi * kGroupChunks + (u64)(lane >> 3);
+  if (li >= n_listed) return false;
+  *chunk = a.chunk_list[li];
+  *w0 = *chunk * kBmChunkWords + (u64)(lane & 7) * 8;
+  return true;
+}
+
+__device__ __forceinline__ void load8(const u32 *p, u32 *v) {
+  const uint4 x = reinterpret_cast<const uint4 *>(p)[0], y = reinterpret_cast<const uint4 *>(p)[1];
+  v[0] = x.x;
+  v[1] = x.y;
+  v[2] = x.z;
+  v[3] = x.w;
+  v[4] = y.x;
+  v[5] = y.y;
+  v[6] = y.z;
+  v[7] = y.w;
+}
+
+// Pass 1 (listed mode): packed (a, b) counts of every group, a warp per group.
+__global__ void __launch_bounds__(kBmBlock) k_bm_groupcount(BmScanArgs a) {
+  if (ctl_stop(a.ctl)) return;
+  scan_bind(a);
+  const u64 n_listed = a.rec->n_listed;
+  const u64 groups = (n_listed + kGroupChunks - 1) / kGroupChunks;
+  const int lane = threadIdx.x & 31;
+  const u64 nw = (u64)gridDim.x * (kBmBlock / 32);
+  u64 my_g = 0;
+  for (u64 gi = ((u64)blockIdx.x * kBmBlock + threadIdx.x) >> 5; gi < groups; gi += nw) {
+    u64 ch, w0;
+    u32 ca = 0, cb = 0;
+    if (group_words(a, n_listed, gi, lane, &ch, &w0)) {
+      u32 g[8] = {0, 0, 0, 0, 0, 0, 0, 0}, f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (a.g) load8(a.g + w0, g);
+      const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
+      // f matters where g has bits (delta), or everywhere for a union
+      if (a.f && (any_g || a.ex_a == kBmUnion || a.ex_b == kBmUnion)) load8(a.f + w0, f);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        ca += __popc(bm_eval(a.ex_a, g[i], f[i]));
+        cb += __popc(bm_eval(a.ex_b, g[i], f[i]));
+        my_g += __popc(g[i]);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ca += __shfl_xor_sync(0xffffffffu, ca, o);
+      cb += __shfl_xor_sync(0xffffffffu, cb, o);
+    }
+    if (lane == 0) a.tile_prefix[gi] = ((u64)ca << 32) | cb;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_g += __shfl_xor_sync(0xffffffffu, my_g, o);
+  if (lane == 0 && my_g) atomicAdd(&a.rec->pop_g, my_g);
 }
 
 // Pass 1: packed (a, b) counts of every tile, one block per tile; a tile
@@ -201,18 +336,17 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_tilecount(BmScanArgs a) {
   if (lane == 0 && my_g) atomicAdd(&a.rec->pop_g, my_g);
 }
 
-// Pass 2: exclusive prefix of the tile counts in place (decoupled
-// look-back over chunks of 2048 tiles), totals and the capacity check.
-constexpr int kScanItems = 8;
-constexpr int kScanChunk = kBmBlock * kScanItems;
-
+// Pass 2: exclusive prefix of the tile (listed mode: group) counts in place
+// (decoupled look-back over chunks of 2048 entries), totals and the
+// capacity check.
 __global__ void __launch_bounds__(kBmBlock) k_bm_scan(BmScanArgs a) {
   __shared__ u64 s_scan[kBmBlock / 32];
   __shared__ long long s_tile;
   __shared__ u64 s_base;
   if (ctl_stop(a.ctl)) return;
-  const u64 tiles = bm_tiles(a.map.words);
-  const u64 chunks = (tiles + kScanChunk - 1) / kScanChunk;
+  const u64 tiles = scan_items(a);
+  // at least one chunk, so that the totals are written when nothing is listed
+  const u64 chunks = max((tiles + kScanChunk - 1) / kScanChunk, (u64)1);
   const u32 gen = a.lrec->gen;
   while (true) {
     const long long c = grab_tile(a.lrec, &s_tile);
@@ -278,11 +412,72 @@ __global__ void k_scan_gate(RelDev *rels, const int *update, int n_update, Ctl *
   }
 }
 
+// The block that finishes a write pass last publishes the list sizes.
+__device__ __forceinline__ void write_finish(const BmScanArgs &a) {
+  if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
+    if (a.list_a) a.list_a->n = a.rec->total_a;
+    if (a.list_b) a.list_b->n = a.rec->total_b;
+    if (a.count_b) *a.count_b = a.rec->total_b;
+    if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
+    a.rec->pop_g = 0;
+    prof_add(a.ctl, kPBitmap, 8 * (a.rec->total_a + a.rec->total_b));
+  }
+}
+
 // Pass 3: write list a, list b (+ its index), update f in place and clear g
 // in the dirty chunks (every chunk without a dirty map).  One block per tile.
+// Listing the set bits of the 256 words a warp holds (8 consecutive words
+// per lane, lane-major) in bit order: key r goes to lane r % 32, so keys are
+// stored in coalesced runs and no lane waits on another lane's denser words.
+// Each lane finds its word by an 8-step search over the words' exclusive
+// bit offsets and its bit by a 5-step popcount search.
+struct WarpBits {
+  u32 w[256];  // the warp's words
+  u32 p[256];  // exclusive bit offsets of the words within the warp
+};
+
+__device__ __forceinline__ u32 nth_set_bit(u32 x, u32 n) {
+  u32 pos = 0;
+#pragma unroll
+  for (int h = 16; h > 0; h >>= 1) {
+    const u32 low = __popc(x & ((1u << h) - 1u));
+    if (n >= low) {
+      n -= low;
+      x >>= h;
+      pos += h;
+    }
+  }
+  return pos;
+}
+
+// emit(r, k, b): key r of the warp is bit b of the warp's word k.
+// lane_excl: bits held by lower lanes; total: bits of the whole warp.
+template <class Emit>
+__device__ __forceinline__ void warp_list_bits(const u32 *e, u32 lane_excl, u32 total,
+                                               WarpBits &s, Emit emit) {
+  const int lane = threadIdx.x & 31;
+  u32 run = lane_excl;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s.w[lane * 8 + i] = e[i];
+    s.p[lane * 8 + i] = run;
+    run += __popc(e[i]);
+  }
+  __syncwarp();
+  for (u32 r = lane; r < total; r += 32) {
+    u32 k = 0;
+#pragma unroll
+    for (u32 h = 128; h > 0; h >>= 1)
+      if (s.p[k + h] <= r) k += h;
+    emit(r, k, nth_set_bit(s.w[k], r - s.p[k]));
+  }
+  __syncwarp();
+}
+
 struct BmWriteSmem {
   u32 off_b[kBmTileWords + 1];  // exclusive offsets of list b per word
   u64 scan_tmp[kBmBlock / 32];
+  WarpBits bits[kBmBlock / 32];
 };
 
 __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
@@ -338,33 +533,44 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
     u64 tot;
     const u64 ex = block_excl_scan<kBmBlock>(((u64)ca << 32) | cb, sm.scan_tmp, &tot);
     if (threadIdx.x == 0 && a.inst_delta && (tot >> 32)) atomicAdd(&a.inst_delta[inst], tot >> 32);
-    u64 pa = (prefix >> 32) + (ex >> 32);
-    u64 pb = (prefix & 0xFFFFFFFFull) + (ex & 0xFFFFFFFFull);
-    u32 ob = (u32)(ex & 0xFFFFFFFFull);
+    if (a.idx_b) {
+      u32 ob = (u32)(ex & 0xFFFFFFFFull);
 #pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) {
-      if (a.idx_b) sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
-      ob += __popc(eb[i]);
-      u32 x = la ? ea[i] : 0u;
-      while (x) {
-        const int b = __ffs(x) - 1;
-        x &= x - 1;
-        if (pa < cap_a)
-          la[pa] = dm_key(a.map, inst, seg, w0 + i, b);
-        else
-          atomicOr(&a.ctl->oob, 2048u);
-        pa++;
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        sm.off_b[threadIdx.x * kBmWordsPerThread + i] = ob;
+        ob += __popc(eb[i]);
       }
-      x = lb ? eb[i] : 0u;
-      while (x) {
-        const int b = __ffs(x) - 1;
-        x &= x - 1;
-        if (pb < cap_b)
-          lb[pb] = dm_key(a.map, inst, seg, w0 + i, b);
-        else
-          atomicOr(&a.ctl->oob, 4096u);
-        pb++;
+    }
+    // the keys, warp by warp (warp wid holds words wt + 256 wid ...)
+    {
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      const u64 ex0 = __shfl_sync(0xffffffffu, ex, 0);
+      const u64 end = __shfl_sync(0xffffffffu, ex + (((u64)ca << 32) | cb), 31);
+      const u64 ww = wt + (u64)wid * 256;
+      if (la) {
+        const u64 base = (prefix >> 32) + (ex0 >> 32);
+        warp_list_bits(ea, (u32)((ex >> 32) - (ex0 >> 32)), (u32)((end >> 32) - (ex0 >> 32)),
+                       sm.bits[wid], [&](u32 r, u32 k, u32 b) {
+                         const u64 pos = base + r;
+                         if (pos < cap_a)
+                           la[pos] = dm_key(a.map, inst, seg, ww + k, (int)b);
+                         else
+                           atomicOr(&a.ctl->oob, 2048u);
+                       });
       }
+      if (lb) {
+        const u64 lo0 = ex0 & 0xFFFFFFFFull;
+        const u64 base = (prefix & 0xFFFFFFFFull) + lo0;
+        warp_list_bits(eb, (u32)((ex & 0xFFFFFFFFull) - lo0), (u32)((end & 0xFFFFFFFFull) - lo0),
+                       sm.bits[wid], [&](u32 r, u32 k, u32 b) {
+                         const u64 pos = base + r;
+                         if (pos < cap_b)
+                           lb[pos] = dm_key(a.map, inst, seg, ww + k, (int)b);
+                         else
+                           atomicOr(&a.ctl->oob, 4096u);
+                       });
+      }
+      (void)lane;
     }
     if (a.idx_b) {
       if (threadIdx.x == 0) sm.off_b[kBmTileWords] = (u32)(tot & 0xFFFFFFFFull);
@@ -389,14 +595,111 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
       __syncthreads();
     }
   }
-  if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
-    if (a.list_a) a.list_a->n = a.rec->total_a;
-    if (a.list_b) a.list_b->n = a.rec->total_b;
-    if (a.count_b) *a.count_b = a.rec->total_b;
-    if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
-    a.rec->pop_g = 0;
-    prof_add(a.ctl, kPBitmap, 8 * (a.rec->total_a + a.rec->total_b));
+  write_finish(a);
+}
+
+// Pass 3 (listed mode): as k_bm_write, a warp per group of listed chunks.
+// No index is built in this mode (it needs whole rows).
+struct GroupWriteSmem {
+  WarpBits bits[kBmBlock / 32];
+  u64 w0[kBmBlock / 32][32];   // first word of each lane
+  u32 inst[kBmBlock / 32][32]; // instance of each lane's chunk
+};
+
+__global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
+  __shared__ GroupWriteSmem sm;
+  if (ctl_stop(a.ctl)) return;
+  if (a.rec->overflow) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.rec->pop_g = 0;
+      if (!a.gated) atomicExch(&a.ctl->overflow, 1u);
+    }
+    return;
   }
+  scan_bind(a);
+  const u64 n_listed = a.rec->n_listed;
+  const u64 groups = (n_listed + kGroupChunks - 1) / kGroupChunks;
+  const int lane = threadIdx.x & 31;
+  const u64 nw = (u64)gridDim.x * (kBmBlock / 32);
+  u64 *la = a.list_a ? a.list_a->ptr : nullptr;
+  u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
+  const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
+  for (u64 gi = ((u64)blockIdx.x * kBmBlock + threadIdx.x) >> 5; gi < groups; gi += nw) {
+    u64 ch = 0, w0 = 0;
+    u32 ea[8], eb[8];
+    u32 ca = 0, cb = 0;
+    const bool on = group_words(a, n_listed, gi, lane, &ch, &w0);
+    u32 g[8] = {0, 0, 0, 0, 0, 0, 0, 0}, f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (on) {
+      if (a.g) load8(a.g + w0, g);
+      const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
+      if (a.f && (any_g || a.ex_a == kBmUnion || a.ex_b == kBmUnion)) load8(a.f + w0, f);
+      if (a.inplace && any_g) {
+        uint4 *pf = reinterpret_cast<uint4 *>(a.f + w0);
+        pf[0] = make_uint4(f[0] | g[0], f[1] | g[1], f[2] | g[2], f[3] | g[3]);
+        pf[1] = make_uint4(f[4] | g[4], f[5] | g[5], f[6] | g[6], f[7] | g[7]);
+        uint4 *pg = reinterpret_cast<uint4 *>(const_cast<u32 *>(a.g) + w0);
+        pg[0] = make_uint4(0, 0, 0, 0);
+        pg[1] = make_uint4(0, 0, 0, 0);
+      }
+      if (a.inplace && a.dirty && (lane & 7) == 0) a.dirty[ch] = 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      ea[i] = bm_eval(a.ex_a, g[i], f[i]);
+      eb[i] = bm_eval(a.ex_b, g[i], f[i]);
+      ca += __popc(ea[i]);
+      cb += __popc(eb[i]);
+    }
+    // warp exclusive scan of the packed counts
+    const u64 mine = ((u64)ca << 32) | cb;
+    u64 inc = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const u64 prefix = a.tile_prefix[gi];
+    // per-instance count of list a: one atomic per chunk (its 8 lanes summed)
+    u32 c8 = ca;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) c8 += __shfl_xor_sync(0xffffffffu, c8, o);
+    const int wid = threadIdx.x >> 5;
+    const u32 inst = on ? dm_tile_inst(a.map, w0 / kBmTileWords) : 0u;
+    if (on && a.inst_delta && (lane & 7) == 0 && c8) atomicAdd(&a.inst_delta[inst], (u64)c8);
+    sm.w0[wid][lane] = w0;
+    sm.inst[wid][lane] = inst;
+    const u64 end = __shfl_sync(0xffffffffu, inc, 31);
+    // the keys of the group, key r by lane r % 32 (lanes past the list hold
+    // no bits)
+    if (la) {
+      const u64 base = prefix >> 32;
+      warp_list_bits(ea, (u32)((inc - mine) >> 32), (u32)(end >> 32), sm.bits[wid],
+                     [&](u32 r, u32 k, u32 b) {
+                       const u32 in = sm.inst[wid][k >> 3];
+                       const SegInfo sg = a.map.seg[in];
+                       const u64 pos = base + r;
+                       if (pos < cap_a)
+                         la[pos] = dm_key(a.map, in, sg, sm.w0[wid][k >> 3] + (k & 7), (int)b);
+                       else
+                         atomicOr(&a.ctl->oob, 2048u);
+                     });
+    }
+    if (lb) {
+      const u64 base = prefix & 0xFFFFFFFFull;
+      warp_list_bits(eb, (u32)((inc - mine) & 0xFFFFFFFFull), (u32)(end & 0xFFFFFFFFull),
+                     sm.bits[wid], [&](u32 r, u32 k, u32 b) {
+                       const u32 in = sm.inst[wid][k >> 3];
+                       const SegInfo sg = a.map.seg[in];
+                       const u64 pos = base + r;
+                       if (pos < cap_b)
+                         lb[pos] = dm_key(a.map, in, sg, sm.w0[wid][k >> 3] + (k & 7), (int)b);
+                       else
+                         atomicOr(&a.ctl->oob, 4096u);
+                     });
+    }
+  }
+  write_finish(a);
 }
 
 // Zero a NEWT bitmap in its dirty chunks (all of it without a dirty map)
@@ -477,6 +780,129 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_bm(JoinArgs a, const Rel
   }
   if (launch_rec_finish(a.rec) && threadIdx.x == 0)
     prof_add(a.ctl, kPJoinMat, 16 * total + 24 * nc);
+}
+
+// Dense joins in one pass (src/join.cu:12-158 with a bitmap output).  No
+// output position is needed when results are bits, so the count pass of
+// the list form (k_join_count's counts and record compaction, then
+// k_join_mat_bm balanced by output position) is replaced by probe and
+// expand: a warp takes 32 outer rows, probes the inner index for each and
+// expands their runs together, 32 candidates per step (lane p takes
+// candidate base + p of the warp's concatenated runs, found by a 5-step
+// search over the runs' offsets).  A run longer than kHeavyRun is cut into
+// pieces of kHeavyPiece candidates, appended to the record buffer
+// (crow_key / crow_start / crow_len, count in op->nc), and expanded by
+// k_join_heavy_bm, a block per piece, so no key can hold one warp long.
+constexpr int kFuseBlock = 256;
+constexpr int kFuseCtasPerSm = 6;
+constexpr u32 kHeavyRun = 128;
+constexpr u32 kHeavyPiece = 2048;
+
+struct FuseSmem {
+  u64 row[kFuseBlock / 32][32];
+  u64 excl[kFuseBlock / 32][32];
+  u32 start[kFuseBlock / 32][32];
+};
+
+__global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
+    k_join_bm(JoinArgs a, const RelDev *out_rd, DenseMap map) {
+  __shared__ FuseSmem sm;
+  if (ctl_stop(a.ctl)) return;
+  const u64 n_outer = eff_count(a.outer, a.outer_vis);
+  const u64 n_inner = eff_count(a.inner, a.inner_vis);
+  if (n_outer == 0 || n_inner == 0) {
+    join_empty_side(a, n_outer);
+    return;
+  }
+  u32 *G = out_rd->bmG;
+  u8 *D = out_rd->dirty;
+  const Index ix = *a.inner_idx;
+  const u64 *inner = a.inner->ptr;
+  const u64 *outer = a.outer->ptr;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const u64 chunks = (n_outer + 31) / 32;
+  const u64 nw = (u64)gridDim.x * (kFuseBlock / 32);
+  u64 cand = 0;  // candidates expanded by this warp
+  for (u64 c = (u64)blockIdx.x * (kFuseBlock / 32) + wid; c < chunks; c += nw) {
+    const u64 i = c * 32 + lane;
+    u64 row = 0;
+    u32 s = 0, l = 0;
+    if (i < n_outer) {
+      row = outer[i];
+      l = index_probe(ix, key_c0(row), &s);
+    }
+    if (l > kHeavyRun) {
+      const u32 np = (l + kHeavyPiece - 1) / kHeavyPiece;
+      const u64 pos = atomicAdd(reinterpret_cast<unsigned long long *>(&a.op->nc), (u64)np);
+      if (pos + np <= a.crow_cap) {
+        for (u32 k = 0; k < np; k++) {
+          a.crow_key[pos + k] = row;
+          a.crow_start[pos + k] = s + k * kHeavyPiece;
+          a.crow_len[pos + k] = min(kHeavyPiece, l - k * kHeavyPiece);
+        }
+        l = 0;
+      }  // else: no room, the warp expands the run itself
+    }
+    u64 inc = l;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const u64 total = __shfl_sync(0xffffffffu, inc, 31);
+    sm.row[wid][lane] = row;
+    sm.start[wid][lane] = s;
+    sm.excl[wid][lane] = inc - l;
+    __syncwarp();
+    for (u64 base = 0; base < total; base += 32) {
+      const u64 p = base + lane;
+      if (p < total) {
+        // the last run starting at or before p (an empty run shares its
+        // offset with the next one, so it is never the last)
+        int r = 0;
+#pragma unroll
+        for (int h = 16; h > 0; h >>= 1)
+          if (sm.excl[wid][r + h] <= p) r += h;
+        const u64 t = gen_join(a.sel, inner[sm.start[wid][r] + (p - sm.excl[wid][r])],
+                               sm.row[wid][r]);
+        if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
+      }
+    }
+    __syncwarp();
+    cand += total;
+  }
+  if (lane == 0) prof_add(a.ctl, kPJoinMat, cand * 12);
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, n_outer * 16);
+}
+
+// The pieces of long runs appended by k_join_bm, a block per piece; the
+// last block empties the piece list for the next launch (so does block 0
+// of a stopped launch, which expands nothing).
+__global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const RelDev *out_rd,
+                                                             DenseMap map) {
+  if (ctl_stop(a.ctl)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.op->nc = 0;
+    return;
+  }
+  const u64 np = min(a.op->nc, a.crow_cap);
+  u32 *G = out_rd->bmG;
+  u8 *D = out_rd->dirty;
+  const u64 *inner = a.inner->ptr;
+  u64 cand = 0;
+  for (u64 k = blockIdx.x; k < np; k += gridDim.x) {
+    const u64 row = a.crow_key[k];
+    const u32 s = a.crow_start[k], l = a.crow_len[k];
+    for (u32 j = threadIdx.x; j < l; j += blockDim.x) {
+      const u64 t = gen_join(a.sel, inner[s + j], row);
+      if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
+    }
+    cand += l;
+  }
+  if (threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, cand * 12);
+  if (launch_rec_finish(a.rec) && threadIdx.x == 0) {
+    a.op->nc = 0;
+    prof_add(a.ctl, kPJoinMat, np * 24);
+  }
 }
 
 // RelationalCopy into the destination's NEWT bitmap (src/copy.cu:12-95).  An
@@ -578,36 +1004,39 @@ __global__ void __launch_bounds__(256) k_inst_tile_pop(const u32 *bm, DenseMap m
 __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map,
                                                      const u64 *tile_rank, u64 *acc) {
   __shared__ u64 s_warp[kBmBlock / 32];
+  __shared__ WarpBits s_bits[kBmBlock / 32];
   const u64 tiles = bm_tiles(map.words);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
     const u32 inst = dm_tile_inst(map, t);
     const SegInfo seg = map.seg[inst];
     const u64 w0 = t * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 x[kBmWordsPerThread];
     u32 cnt = 0;
-    for (int i = 0; i < kBmWordsPerThread; i++)
-      if (w0 + i < map.words) cnt += __popc(bm[w0 + i]);
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      x[i] = w0 + i < map.words ? bm[w0 + i] : 0u;
+      cnt += __popc(x[i]);
+    }
     u64 tile_n;
     const u64 ex = block_excl_scan<kBmBlock>(cnt, s_warp, &tile_n);
     if (tile_n == 0) continue;  // uniform: every thread saw the same total
-    u64 rank = tile_rank[t] + ex;
+    // the warp's tuples, rank r of the warp by lane r % 32
+    const u64 ex0 = __shfl_sync(0xffffffffu, ex, 0);
+    const u64 end = __shfl_sync(0xffffffffu, ex + cnt, 31);
+    const u64 rank0 = tile_rank[t] + ex0;
+    const u64 ww = t * kBmTileWords + (u64)wid * 256;
     u64 h_sum = 0;
-    for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u64 w = w0 + i;
-      if (w >= map.words) break;
-      u32 x = bm[w];
-      while (x) {
-        const int b = __ffs(x) - 1;
-        x &= x - 1;
-        const u64 wl = w - seg.base_word;
-        const u64 lx = wl >> seg.row_shift;
-        const u64 lz = ((wl & ((1ull << seg.row_shift) - 1)) << 5) + (u64)b;
-        u64 h = mix64(rank);
-        h = mix64(h ^ lx);
-        h = mix64(h ^ lz);
-        h_sum += h;
-        rank++;
-      }
-    }
+    warp_list_bits(x, (u32)(ex - ex0), (u32)(end - ex0), s_bits[wid], [&](u32 r, u32 k, u32 b) {
+      const u64 wl = ww + k - seg.base_word;
+      const u64 lx = wl >> seg.row_shift;
+      const u64 lz = ((wl & ((1ull << seg.row_shift) - 1)) << 5) + (u64)b;
+      u64 h = mix64(rank0 + r);
+      h = mix64(h ^ lx);
+      h = mix64(h ^ lz);
+      h_sum += h;
+    });
+    (void)lane;
     // one atomic per tile: the tile's terms summed over the block
     u64 dummy;
     const u64 ex_h = block_excl_scan<kBmBlock>(h_sum, s_warp, &dummy);

@@ -165,6 +165,7 @@ struct gdl_engine {
   int count_ctas_per_sm = 4;
   int index_slots_per_key = 2;
   int dirty_min_log2_words = 24;
+  int dense_join_passes = 1;
   // Batched form (gdl_engine_set_instances): the block-diagonal layout.
   bool instances = false;
   std::vector<SegInfo> segs;
@@ -417,6 +418,14 @@ gdl_status ensure_scratch(gdl_engine *e) {
   return GDL_OK;
 }
 
+// Scan scratch of a relation kept as bitmaps of `words` words: one u64 per
+// tile or per group of kGroupChunks chunks (more of the latter), then the
+// dirty-chunk list (u32 per chunk).
+u64 scan_scratch_bytes(u64 words) {
+  const u64 chunks = words / kBmChunkWords;
+  return chunks / kGroupChunks * sizeof(u64) + chunks * sizeof(u32);
+}
+
 // Bitmaps of one relation in dense form: NEWT always, FULL and its next
 // version for update relations.
 gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
@@ -433,18 +442,22 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
     h.tile_prefix = nullptr;
     rh.bm_words = words;
   }
-  const u64 tiles = words / kBmTileWords;
   if (!h.bmG) TRY(dalloc(e, (void **)&h.bmG, words * 4));
   if (!h.bmD) TRY(dalloc(e, (void **)&h.bmD, words / kBmChunkWords));
-  if (!h.tile_prefix) TRY(dalloc(e, (void **)&h.tile_prefix, tiles * sizeof(u64)));
+  // tile (or chunk-group) counts / prefixes, then the dirty-chunk list
+  if (!h.tile_prefix) TRY(dalloc(e, (void **)&h.tile_prefix, scan_scratch_bytes(words)));
   if (with_full && !h.bmF) TRY(dalloc(e, (void **)&h.bmF, words * 4));
   memset(&h.scan, 0, sizeof h.scan);
   return GDL_OK;
 }
 
 gdl_status ensure_dense_scratch(gdl_engine *e, u64 words) {
-  const u64 chunks = words / kBmTileWords / kScanChunk + 2;
-  TRY(ensure_lb(e, e->lb_bm, e->lb_bm_tiles, chunks));
+  // look-back units: tiles / kScanChunk, or in listed mode dirty chunks /
+  // kDirtyUnit and chunk groups / kScanChunk (the largest of the three)
+  const u64 chunks = words / kBmChunkWords;
+  const u64 units = std::max({words / kBmTileWords / kScanChunk, chunks / kDirtyUnit,
+                              chunks / kGroupChunks / kScanChunk}) + 2;
+  TRY(ensure_lb(e, e->lb_bm, e->lb_bm_tiles, units));
   return GDL_OK;
 }
 
@@ -601,6 +614,20 @@ void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
   a.ctl = e->d_ctl;
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[4];
+  if (a.skip_clean && e->h[rel].dirty && !a.idx_b) {
+    // listed mode: dirty chunks only, a warp per group of them
+    const u64 chunks = a.map.words / kBmChunkWords;
+    const u64 groups = chunks / kGroupChunks;
+    a.chunk_list = reinterpret_cast<u32 *>(a.tile_prefix + groups);
+    PLAUNCH(kc, kPBitmap,
+            k_bm_dirty_chunks<<<grid_for(e, chunks / kDirtyUnit + 1, 1, 4), kBmBlock, 0, e->s>>>(
+                a));
+    PLAUNCH(kc, kPBitmap,
+            k_bm_groupcount<<<grid_for(e, groups * 32, kBmBlock, 8), kBmBlock, 0, e->s>>>(a));
+    PLAUNCH(kc, kPBitmap,
+            k_bm_scan<<<grid_for(e, groups / kScanChunk + 1, 1, 4), kBmBlock, 0, e->s>>>(a));
+    return;
+  }
   PLAUNCH(kc, kPBitmap, k_bm_tilecount<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(a));
   PLAUNCH(kc, kPBitmap,
           k_bm_scan<<<grid_for(e, tiles / kScanChunk + 1, 1, 4), kBmBlock, 0, e->s>>>(a));
@@ -608,6 +635,12 @@ void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
 void launch_scan_write(gdl_engine *e, BmScanArgs a, Counts *kc) {
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[5];
+  if (a.chunk_list) {
+    const u64 groups = a.map.words / kBmChunkWords / kGroupChunks;
+    PLAUNCH(kc, kPBitmap,
+            k_bm_groupwrite<<<grid_for(e, groups * 32, kBmBlock, 8), kBmBlock, 0, e->s>>>(a));
+    return;
+  }
   PLAUNCH(kc, kPBitmap, k_bm_write<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(a));
 }
 void launch_scan(gdl_engine *e, BmScanArgs a, int rel, Counts *kc) {
@@ -689,11 +722,19 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       a.dense = dense;
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
+      JoinArgs b = a;
+      b.rec = &e->recs[1];
+      if (dense && e->dense_join_passes == 1) {
+        PLAUNCH(kc, kPJoinMat,
+                k_join_bm<<<grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm), kFuseBlock, 0,
+                            s>>>(a, &R[op.out], map));
+        PLAUNCH(kc, kPJoinMat,
+                k_join_heavy_bm<<<(int)e->sms * 4, kFuseBlock, 0, s>>>(b, &R[op.out], map));
+        continue;
+      }
       PLAUNCH(kc, kPJoinCount,
               k_join_count<<<grid_for(e, outer_cap, kJoinTile, e->count_ctas_per_sm), kJoinBlock,
                              0, s>>>(a));
-      JoinArgs b = a;
-      b.rec = &e->recs[1];
       const u64 out_cap = e->h[op.out].newt.cap;
       if (dense)
         PLAUNCH(kc, kPJoinMat,
@@ -1895,7 +1936,8 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       t->index_slots_per_key < 0 || t->index_slots_per_key > 64 ||
       (t->index_slots_per_key && (t->index_slots_per_key < 2 ||
                                   (t->index_slots_per_key & (t->index_slots_per_key - 1)))) ||
-      (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)))
+      (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
+      t->dense_join_passes < 0 || t->dense_join_passes > 2)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -1903,6 +1945,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->count_ctas_per_sm) e->count_ctas_per_sm = t->count_ctas_per_sm;
   if (t->index_slots_per_key) e->index_slots_per_key = t->index_slots_per_key;
   if (t->dirty_min_log2_words) e->dirty_min_log2_words = t->dirty_min_log2_words;
+  if (t->dense_join_passes) e->dense_join_passes = t->dense_join_passes;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -1915,6 +1958,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->count_ctas_per_sm = e->count_ctas_per_sm;
   t->index_slots_per_key = e->index_slots_per_key;
   t->dirty_min_log2_words = e->dirty_min_log2_words;
+  t->dense_join_passes = e->dense_join_passes;
   return GDL_OK;
 }
 

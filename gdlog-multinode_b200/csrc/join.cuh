@@ -73,6 +73,29 @@ __device__ __forceinline__ u64 eff_count(const DArr *a, const u32 *vis) {
   return (vis && *vis == 0) ? 0 : a->n;
 }
 
+// src/join.cu:38-45: either side empty -> no output, and the OUTER's
+// tuple_counts is set to 0 (a real change only when the inner is empty).
+// Every block of the launch calls this.
+__device__ __forceinline__ void join_empty_side(const JoinArgs &a, u64 n_outer) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.op->total = 0;
+    a.op->nc = 0;
+    a.op->overflow = 0;
+    if (n_outer != 0) {
+      if (a.outer_vis)
+        *a.outer_vis = 0;
+      else
+        ((DArr *)a.outer)->n = 0;
+    }
+  }
+  if (n_outer != 0 && !a.outer_vis && a.outer_bm) {
+    uint4 *p = reinterpret_cast<uint4 *>(a.outer_bm);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.outer_bm_words / 4;
+         i += (u64)gridDim.x * blockDim.x)
+      p[i] = make_uint4(0, 0, 0, 0);
+  }
+}
+
 struct JoinSmem {
   u64 keys[kJoinTile];
   u64 scan_tmp[kJoinBlock / 32];
@@ -86,25 +109,7 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
   const u64 n_outer = eff_count(a.outer, a.outer_vis);
   const u64 n_inner = eff_count(a.inner, a.inner_vis);
   if (n_outer == 0 || n_inner == 0) {
-    // src/join.cu:38-45: either side empty -> no output, and the OUTER's
-    // tuple_counts is set to 0 (a real change only when the inner is empty).
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      a.op->total = 0;
-      a.op->nc = 0;
-      a.op->overflow = 0;
-      if (n_outer != 0) {
-        if (a.outer_vis)
-          *a.outer_vis = 0;
-        else
-          ((DArr *)a.outer)->n = 0;
-      }
-    }
-    if (n_outer != 0 && !a.outer_vis && a.outer_bm) {
-      uint4 *p = reinterpret_cast<uint4 *>(a.outer_bm);
-      for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.outer_bm_words / 4;
-           i += (u64)gridDim.x * blockDim.x)
-        p[i] = make_uint4(0, 0, 0, 0);
-    }
+    join_empty_side(a, n_outer);
     return;
   }
   const u64 tiles = (n_outer + kJoinTile - 1) / kJoinTile;

@@ -113,6 +113,9 @@ typedef struct gdl_tuning {
   int32_t index_slots_per_key; /* hashed index: slots per distinct key, power of two >= 2 (default 2) */
   int32_t dirty_min_log2_words;/* keep a dirty map for NEWT bitmaps of at least 2^this
                                   words (default 24 = 64 MB; 11..40) */
+  int32_t dense_join_passes;   /* joins into bitmaps: 1 = probe and expand in one
+                                  pass (default), 2 = count pass, then a pass
+                                  balanced by output position */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

@@ -14,8 +14,11 @@ def test_bucket_and_candidates():
     e = W.grid_edges(16, 16)
     assert A.bucket("tc", (e,)) == "tc:n8:t8"
     cands = A.candidates()
-    assert len(cands) == 2 * 3 * 3 * 2
+    # sort: 3 x 3 x 2 grids; dense with 2 passes: the same; dense with one
+    # pass: only the index choice matters
+    assert len(cands) == 18 + 18 + 2
     assert {c["dedup"] for c in cands} == {"dense", "sort"}
+    assert {c["dense_join_passes"] for c in cands} == {1, 2}
 
 
 @pytest.mark.gpu
