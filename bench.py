@@ -94,10 +94,16 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up (NVML initialisation) takes the driver for
+            # a while; let it finish before the timed region opens, so that
+            # only the periodic queries overlap the measured steps
+            t_end = time.time() + 5.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
@@ -151,18 +157,38 @@ def oracle_run(wl: dict, inputs, threads: int = 0):
         return secs, derived(r), eng.threads
 
 
+def roofline_of(prof: dict, workload: str, peaks: dict) -> dict:
+    """Roofline object of the dominant kernel family (most device time) of
+    one profiled step: its algorithmic bytes per launch over its mean
+    launch time (CUDA events on the engine stream), against the measured
+    HBM copy bandwidth."""
+    kind, rec = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    per_launch_ms = rec["ms"] / max(rec["launches"], 1)
+    per_launch_bytes = rec["bytes"] / max(rec["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else 0.0
+    return {"bound": "hbm", "kernel": kind, "achieved": achieved,
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+            "traffic": traffic_for(workload, kind, per_launch_bytes),
+            "alg_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
+            "launches": rec["launches"],
+            "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)"}
+
+
 def single_families(prof):
     return {kd: {"launches": v["launches"], "alg_bytes": v["bytes"]}
             for kd, v in prof.items() if v["launches"]}
 
 
-def traffic_for(kind: str, alg_bytes_per_launch: float):
-    """DRAM bytes per launch from the committed ncu summary of this kernel
-    family, scaled by algorithmic bytes (capture of a smaller case)."""
+def traffic_for(workload: str, kind: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch of a kernel family: the family's DRAM bytes
+    (dram__bytes_read.sum + dram__bytes_write.sum over all its launches in
+    one ncu capture of `bench.py --single --workload <workload>`, committed
+    in profiles/traffic.json) per algorithmic byte of that same step, times
+    this launch's algorithmic bytes."""
     p = os.path.join(REPO, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    rec = json.load(open(p)).get(kind)
+    rec = json.load(open(p)).get(workload, {}).get(kind)
     if not rec or not rec.get("alg_bytes"):
         return None
     return rec["dram_bytes"] / rec["alg_bytes"] * alg_bytes_per_launch
@@ -202,6 +228,17 @@ def run_ours(a) -> None:
     inputs = wl["make"]()
     stream = torch.cuda.Stream(device=dev)
     eng = Engine("gpu", device=local, stream=stream.cuda_stream)
+    from autotune import Tuner
+    tuner = Tuner()
+    if a.tune:
+        # time every candidate configuration on this workload and cache the best
+        rec = tuner.tune(eng, wl["prog"], inputs)
+        print(json.dumps({"tuned": a.workload, "bucket": tuner.key(wl["prog"].__name__, inputs),
+                          **rec}), flush=True)
+        eng.close()
+        return
+    rec = tuner.apply(eng, wl["prog"], inputs)
+    tuning = rec["config"] if rec else "engine defaults (no cached tuning for this size bucket)"
     dev_inputs = [DeviceRows(torch.from_numpy(x.astype(np.int64)).to(dev)) for x in inputs]
     pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in inputs]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -289,11 +326,6 @@ def run_ours(a) -> None:
     if rank != 0:
         return
     peaks = measured_peaks()
-    kind, rec = max(prof.items(), key=lambda kv: kv[1]["ms"])
-    per_launch_ms = rec["ms"] / max(rec["launches"], 1)
-    per_launch_bytes = rec["bytes"] / max(rec["launches"], 1)
-    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else 0.0
-    tr = traffic_for(kind, per_launch_bytes)
     line = {
         "metric": "derived tuples/s (SG fixpoint)" if a.workload == "sg_rmat_s14"
         else "derived tuples/s", "value": tuples / (ms_total / 1e3), "unit": "tuples/s",
@@ -303,17 +335,13 @@ def run_ours(a) -> None:
         "config": {"workload": wl["desc"], "program": wl["prog"].__name__,
                    "tuples_per_step": tuples / a.steps / world,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "tuning": tuning,
                    "l2": "flushed between steps (256 MB write); relations exceed L2"},
         "e2e": {"value": e2e_tuples / (e2e_ms / 1e3), "unit": "tuples/s",
                 "h2d_bytes_per_step": int(sum(x.nbytes for x in pinned)),
                 "d2h_bytes_per_step": 16 * n_out[0]},
         "gpu_launches": int(kernels),
-        "roofline": {"bound": "hbm", "kernel": kind, "achieved": achieved,
-                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": tr,
-                     "alg_bytes_per_launch": per_launch_bytes,
-                     "ms_per_launch": per_launch_ms, "launches": rec["launches"],
-                     "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "roofline": roofline_of(prof, a.workload, peaks),
         "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4),
                         "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] else None}
                     for k, v in prof.items() if v["launches"]},
@@ -409,6 +437,12 @@ def run_dag_batch(a) -> None:
     rp = B.run_plain_loop(eng, P.tc, inst)
     same = sum((x.sizes, x.digests, x.iterations) == (y.sizes, y.digests, y.iterations)
                for x, y in zip(rb.results, rp.results))
+    # profiled batched step: an event pair around every launch
+    eng.profile_reset()
+    eng.set_profile(True)
+    B.run_batched(eng, P.tc, inst, node_counts=counts)
+    eng.set_profile(False)
+    prof = eng.profile()
     eng.close()
     ms = statistics.median(ms_b)
     wall = statistics.median(wall_b)
@@ -441,7 +475,18 @@ def run_dag_batch(a) -> None:
         "batched_over_plain": plain_ms / ms,
         "bit_exact_instances": f"{same}/384",
         "gpu_launches": rb.kernels, "clocks": clocks.summary(),
+        "roofline": roofline_of(prof, "dag_batch384", measured_peaks()),
     }
+    if world == 1 and not a.no_cpu_baseline:
+        # bounded sample: the first 24 DAGs, one after another on the oracle
+        from gdlog_b200 import Engine as _E
+        with _E("oracle") as o:
+            ro = B.run_plain_loop(o, P.tc, inst[:24])
+            cores = o.threads
+        line["cpu_baseline"] = {"value": 24 / ro.seconds, "unit": "instances/s",
+                                "cores": cores, "kind": "port",
+                                "sample": "the first 24 of the 384 DAGs, one plain fixpoint "
+                                          "each on the CPU oracle (wall time)"}
     print(json.dumps(line), flush=True)
 
 
@@ -455,6 +500,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--single", action="store_true",
                     help="run one device step and exit (for profiler captures)")
+    ap.add_argument("--tune", action="store_true",
+                    help="autotune this workload's size bucket, save the cache, and exit")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":
         a.warmup = 3

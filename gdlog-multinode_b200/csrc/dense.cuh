@@ -85,7 +85,9 @@ __device__ __forceinline__ u64 dm_key(const DenseMap &m, u32 inst, const SegInfo
 // that touch one chunk).  It is only kept for large bitmaps; without it
 // (null) every chunk counts as dirty.
 __device__ __forceinline__ void bm_mark(u32 *bm, u8 *dirty, u64 w, u32 b) {
-  atomicOr(bm + w, 1u << b);
+  // A reduction (red), not an atomic: the old value is never needed, so
+  // the L2 does the OR without sending anything back.
+  asm volatile("red.global.or.b32 [%0], %1;" ::"l"(bm + w), "r"(1u << b) : "memory");
   if (dirty) dirty[w / kBmChunkWords] = 1;
 }
 
@@ -132,9 +134,11 @@ struct BmScanArgs {
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
   int gated;           // the overflow is raised by k_scan_gate, not by k_bm_write
   u64 *tile_prefix;    // [tiles] tile counts, then their exclusive prefix (a << 32 | b)
-  // Listed mode (dirty map, skip_clean, no index): [chunks] the dirty
-  // 64-word chunks in order; tile_prefix then holds one entry per group of
-  // kGroupChunks listed chunks.  Null: whole tiles.
+  // Group mode (no index built): a warp per group of kGroupChunks 64-word
+  // chunks, tile_prefix holding one entry per group.  chunk_list: [chunks]
+  // the dirty chunks in order (listed mode, with a dirty map); null: every
+  // chunk, group g = words 256 g .. 256 g + 255.
+  int grouped;
   u32 *chunk_list;
   BmScanRec *rec;
   LaunchRec *lrec;
@@ -166,9 +170,13 @@ constexpr int kGroupChunks = 32 * 8 / kBmChunkWords;  // 4
 constexpr int kDirtyItems = 16;                       // dirty bytes per thread (one uint4)
 constexpr int kDirtyUnit = kBmBlock * kDirtyItems;    // chunks per look-back unit
 
+// Chunks a group-mode pass covers: the listed ones, or all of them.
+__device__ __forceinline__ u64 group_chunks(const BmScanArgs &a) {
+  return a.chunk_list ? (u64)a.rec->n_listed : a.map.words / kBmChunkWords;
+}
+
 __device__ __forceinline__ u64 scan_items(const BmScanArgs &a) {
-  return a.chunk_list ? (a.rec->n_listed + kGroupChunks - 1) / kGroupChunks
-                      : bm_tiles(a.map.words);
+  return a.grouped ? (group_chunks(a) + kGroupChunks - 1) / kGroupChunks : bm_tiles(a.map.words);
 }
 
 // Pass 0 (listed mode): the ordered list of dirty chunks (decoupled
@@ -231,7 +239,7 @@ __device__ __forceinline__ bool group_words(const BmScanArgs &a, u64 n_listed, u
                                             u64 *chunk, u64 *w0) {
   const u64 li = gi * kGroupChunks + (u64)(lane >> 3);
   if (li >= n_listed) return false;
-  *chunk = a.chunk_list[li];
+  *chunk = a.chunk_list ? a.chunk_list[li] : li;
   *w0 = *chunk * kBmChunkWords + (u64)(lane & 7) * 8;
   return true;
 }
@@ -248,11 +256,11 @@ __device__ __forceinline__ void load8(const u32 *p, u32 *v) {
   v[7] = y.w;
 }
 
-// Pass 1 (listed mode): packed (a, b) counts of every group, a warp per group.
+// Pass 1 (group mode): packed (a, b) counts of every group, a warp per group.
 __global__ void __launch_bounds__(kBmBlock) k_bm_groupcount(BmScanArgs a) {
   if (ctl_stop(a.ctl)) return;
   scan_bind(a);
-  const u64 n_listed = a.rec->n_listed;
+  const u64 n_listed = group_chunks(a);
   const u64 groups = (n_listed + kGroupChunks - 1) / kGroupChunks;
   const int lane = threadIdx.x & 31;
   const u64 nw = (u64)gridDim.x * (kBmBlock / 32);
@@ -413,7 +421,18 @@ __global__ void k_scan_gate(RelDev *rels, const int *update, int n_update, Ctl *
 }
 
 // The block that finishes a write pass last publishes the list sizes.
-__device__ __forceinline__ void write_finish(const BmScanArgs &a) {
+// `bytes`: this thread's bitmap traffic (words of G and F examined, F
+// words updated and G words cleared), added to the scan family's
+// algorithmic bytes with one global atomic per block.
+__device__ __forceinline__ void write_finish(const BmScanArgs &a, u64 bytes) {
+  __shared__ unsigned long long s_bytes;
+  if (threadIdx.x == 0) s_bytes = 0;
+  __syncthreads();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+  if ((threadIdx.x & 31) == 0 && bytes) atomicAdd(&s_bytes, (unsigned long long)bytes);
+  __syncthreads();
+  if (threadIdx.x == 0) prof_add(a.ctl, kPBitmap, s_bytes);
   if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
     if (a.list_a) a.list_a->n = a.rec->total_a;
     if (a.list_b) a.list_b->n = a.rec->total_b;
@@ -480,7 +499,7 @@ struct BmWriteSmem {
   WarpBits bits[kBmBlock / 32];
 };
 
-__global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
+__global__ void __launch_bounds__(kBmBlock, 3) k_bm_write(BmScanArgs a) {
   __shared__ BmWriteSmem sm;
   if (ctl_stop(a.ctl)) return;
   if (a.rec->overflow) {
@@ -499,11 +518,13 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
   u64 *la = a.list_a ? a.list_a->ptr : nullptr;
   u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
   const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
+  u64 moved = 0;  // bitmap bytes examined / updated by this thread
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const u8 db = chunk_dirty(a.dirty, tile, threadIdx.x);
     const bool read = !a.skip_clean || db;
     if (!__syncthreads_or(read)) continue;
     const bool clr = a.inplace && db;
+    if (read) moved += kBmWordsPerThread * ((a.g ? 4 : 0) + (a.f ? 4 : 0));
     const u64 prefix = a.tile_prefix[tile];
     const u64 wt = tile * kBmTileWords;
     const u32 inst = dm_tile_inst(a.map, tile);
@@ -521,6 +542,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
         if (clr && g) {
           a.f[w] = f | g;
           const_cast<u32 *>(a.g)[w] = 0u;
+          moved += 8;
         }
       }
       ea[i] = bm_eval(a.ex_a, g, f);
@@ -595,11 +617,11 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_write(BmScanArgs a) {
       __syncthreads();
     }
   }
-  write_finish(a);
+  write_finish(a, moved);
 }
 
-// Pass 3 (listed mode): as k_bm_write, a warp per group of listed chunks.
-// No index is built in this mode (it needs whole rows).
+// Pass 3 (group mode): as k_bm_write, a warp per group of chunks.  No
+// index is built in this mode (it needs whole rows).
 struct GroupWriteSmem {
   WarpBits bits[kBmBlock / 32];
   u64 w0[kBmBlock / 32][32];   // first word of each lane
@@ -617,13 +639,14 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
     return;
   }
   scan_bind(a);
-  const u64 n_listed = a.rec->n_listed;
+  const u64 n_listed = group_chunks(a);
   const u64 groups = (n_listed + kGroupChunks - 1) / kGroupChunks;
   const int lane = threadIdx.x & 31;
   const u64 nw = (u64)gridDim.x * (kBmBlock / 32);
   u64 *la = a.list_a ? a.list_a->ptr : nullptr;
   u64 *lb = a.list_b ? a.list_b->ptr : nullptr;
   const u64 cap_a = a.list_a ? a.list_a->cap : 0, cap_b = a.list_b ? a.list_b->cap : 0;
+  u64 moved = 0;  // bitmap bytes examined / updated by this lane
   for (u64 gi = ((u64)blockIdx.x * kBmBlock + threadIdx.x) >> 5; gi < groups; gi += nw) {
     u64 ch = 0, w0 = 0;
     u32 ea[8], eb[8];
@@ -634,6 +657,9 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
       if (a.g) load8(a.g + w0, g);
       const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
       if (a.f && (any_g || a.ex_a == kBmUnion || a.ex_b == kBmUnion)) load8(a.f + w0, f);
+      moved += a.g ? 32 : 0;
+      if (a.f && (any_g || a.ex_a == kBmUnion || a.ex_b == kBmUnion)) moved += 32;
+      if (a.inplace && any_g) moved += 64;
       if (a.inplace && any_g) {
         uint4 *pf = reinterpret_cast<uint4 *>(a.f + w0);
         pf[0] = make_uint4(f[0] | g[0], f[1] | g[1], f[2] | g[2], f[3] | g[3]);
@@ -699,7 +725,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
                      });
     }
   }
-  write_finish(a);
+  write_finish(a, moved);
 }
 
 // Zero a NEWT bitmap in its dirty chunks (all of it without a dirty map)

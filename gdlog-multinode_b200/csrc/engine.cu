@@ -614,14 +614,18 @@ void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
   a.ctl = e->d_ctl;
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[4];
-  if (a.skip_clean && e->h[rel].dirty && !a.idx_b) {
-    // listed mode: dirty chunks only, a warp per group of them
+  if (!a.idx_b) {
+    // group mode: a warp per group of 4 chunks; with a dirty map (listed
+    // mode) only the dirty chunks, listed first
     const u64 chunks = a.map.words / kBmChunkWords;
     const u64 groups = chunks / kGroupChunks;
-    a.chunk_list = reinterpret_cast<u32 *>(a.tile_prefix + groups);
-    PLAUNCH(kc, kPBitmap,
-            k_bm_dirty_chunks<<<grid_for(e, chunks / kDirtyUnit + 1, 1, 4), kBmBlock, 0, e->s>>>(
-                a));
+    a.grouped = 1;
+    if (a.skip_clean && e->h[rel].dirty) {
+      a.chunk_list = reinterpret_cast<u32 *>(a.tile_prefix + groups);
+      PLAUNCH(kc, kPBitmap,
+              k_bm_dirty_chunks<<<grid_for(e, chunks / kDirtyUnit + 1, 1, 4), kBmBlock, 0,
+                                  e->s>>>(a));
+    }
     PLAUNCH(kc, kPBitmap,
             k_bm_groupcount<<<grid_for(e, groups * 32, kBmBlock, 8), kBmBlock, 0, e->s>>>(a));
     PLAUNCH(kc, kPBitmap,
@@ -635,7 +639,7 @@ void launch_scan_count(gdl_engine *e, BmScanArgs &a, int rel, Counts *kc) {
 void launch_scan_write(gdl_engine *e, BmScanArgs a, Counts *kc) {
   const u64 tiles = a.map.words / kBmTileWords;
   a.lrec = &e->recs[5];
-  if (a.chunk_list) {
+  if (a.grouped) {
     const u64 groups = a.map.words / kBmChunkWords / kGroupChunks;
     PLAUNCH(kc, kPBitmap,
             k_bm_groupwrite<<<grid_for(e, groups * 32, kBmBlock, 8), kBmBlock, 0, e->s>>>(a));
@@ -1013,7 +1017,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     RelHost &rh = e->rels[r];
     if (!h.full_vis) h.full.n = 0;  // tuple_full gets tuple_counts rows
     const u64 take = rh.raw_is_full ? h.full.n : std::min(h.full.n, rh.raw_n);
-    const u64 base = std::max<u64>(2 * h.full.n, kMinCap);
+    // room to double, within the list limit (a FULL at the limit keeps it)
+    const u64 base = std::max<u64>(std::min<u64>(2 * h.full.n, std::max<u64>(h.full.n, kMaxRows)),
+                                   kMinCap);
     TRY(ensure_arr(e, h.full, base, true));
     TRY(ensure_arr(e, h.full_next, h.full.cap, false));
     TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, base), false));

@@ -15,7 +15,13 @@ Admission uses an HBM estimate per query: the bitmaps of its relations
 (n^2 / 8 bytes each, three per updated relation plus NEWT of the tmp
 relation) plus 16 bytes per candidate of its first join, which is the
 sum k_join_count forms (per outer row, the length of the inner run it
-probes) taken here from the graph's degrees.
+probes) taken here from the graph's degrees.  The same candidate count
+bounds the largest list the batch's first fixpoint hands to the next one,
+so a batch is also capped at half of the engine's list limit (2^30 rows)
+in summed candidates.  Later iterations can still outgrow a list (a batch of
+same-generation queries grows fast); a batch the engine refuses for size
+(GDL_E_UNSUPPORTED list limit, GDL_E_NOMEM) is split in halves and each half
+run again, down to single queries.
 
 The plain baseline serves the same stream one query at a time through the
 plain (unbatched) engine.  Both report p50 / p99 latency (finish - arrival)
@@ -36,7 +42,10 @@ import numpy as np
 import batch as B
 import programs as P
 import workloads as W
-from gdlog_b200 import Engine
+from gdlog_b200 import Engine, GdlError
+
+# gdl_status codes of a batch too large for the engine (include/gdlog_b200.h)
+_TOO_LARGE = (3, 4)  # GDL_E_NOMEM, GDL_E_UNSUPPORTED
 
 PROGRAMS = {"tc": P.tc, "sg": P.sg}
 
@@ -49,6 +58,7 @@ class Request:
     nodes: int
     arrival: float
     est_bytes: int = 0
+    est_tuples: int = 0
     start: float = -1.0
     finish: float = -1.0
     result: object = None
@@ -74,12 +84,13 @@ def make_stream(n=20000, rate=200.0, tc_frac=0.7, seed=7, max_scale=14, min_scal
             e = W.rmat_edges(scale, 4 * nodes, seed=seed * 1_000_003 + i)
             reqs.append(Request(i, "sg", (e,), nodes, float(t[i])))
     for r in reqs:
-        r.est_bytes = hbm_estimate(r)
+        r.est_bytes, r.est_tuples = hbm_estimate(r)
     return reqs
 
 
-def hbm_estimate(r: Request) -> int:
-    """Bytes a query needs on the device (see the module docstring)."""
+def hbm_estimate(r: Request) -> tuple[int, int]:
+    """(bytes a query needs on the device, candidates of its first join);
+    see the module docstring."""
     n = r.nodes
     e = r.inputs[0]
     bitmap = (n * max(32, 1 << int(np.ceil(np.log2(max(n, 32) / 32)) + 5))) // 8
@@ -93,7 +104,7 @@ def hbm_estimate(r: Request) -> int:
         # init join: edge x edge on the shared source
         cands = int((outdeg.astype(np.int64) ** 2).sum())
         bitmaps = 4
-    return bitmaps * bitmap + 16 * (cands + len(e))
+    return bitmaps * bitmap + 16 * (cands + len(e)), cands + len(e)
 
 
 def percentiles(lat):
@@ -105,9 +116,11 @@ def percentiles(lat):
 
 
 class Server:
-    def __init__(self, slots=2, budget_bytes=24 << 30, max_batch=256, batched=True, device=0):
+    def __init__(self, slots=2, budget_bytes=24 << 30, max_batch=256, batched=True, device=0,
+                 tuple_cap=1 << 29):
         self.slots = slots
         self.budget = budget_bytes
+        self.tuple_cap = tuple_cap
         self.max_batch = max_batch
         self.batched = batched
         self.device = device
@@ -115,6 +128,7 @@ class Server:
         self.cv = threading.Condition()
         self.done = False
         self.batches = []  # (kind, size, seconds)
+        self.splits = 0    # batches split after the engine refused their size
         self.error = None
 
     def _take(self):
@@ -125,13 +139,15 @@ class Server:
         kind = self.queue[0].kind
         if not self.batched:
             return [self.queue.popleft()]
-        take, used, keep = [], 0, collections.deque()
+        take, used, tuples, keep = [], 0, 0, collections.deque()
         while self.queue:
             r = self.queue.popleft()
             if (r.kind == kind and len(take) < self.max_batch
-                    and (not take or used + r.est_bytes <= self.budget)):
+                    and (not take or (used + r.est_bytes <= self.budget
+                                      and tuples + r.est_tuples <= self.tuple_cap))):
                 take.append(r)
                 used += r.est_bytes
+                tuples += r.est_tuples
             else:
                 keep.append(r)
         self.queue = keep
@@ -162,18 +178,29 @@ class Server:
                     r.start = now
                 prog = PROGRAMS[reqs[0].kind]
                 ts = time.perf_counter()
-                if self.batched:
-                    run = B.run_batched(eng, prog, [r.inputs for r in reqs],
-                                        node_counts=[r.nodes for r in reqs])
-                else:
-                    run = B.run_plain_loop(eng, prog, [r.inputs for r in reqs])
+                results = self._run(eng, prog, reqs)
                 end = time.perf_counter() - t0
                 self.batches.append((reqs[0].kind, len(reqs), time.perf_counter() - ts))
-                for r, res in zip(reqs, run.results):
+                for r, res in zip(reqs, results):
                     r.result = res
                     r.finish = end
         finally:
             eng.close()
+
+    def _run(self, eng, prog, reqs) -> list:
+        """Results of one batch (or, unbatched, of each query in turn); a
+        batch refused for its size is split in halves."""
+        if not self.batched:
+            return B.run_plain_loop(eng, prog, [r.inputs for r in reqs]).results
+        try:
+            return B.run_batched(eng, prog, [r.inputs for r in reqs],
+                                 node_counts=[r.nodes for r in reqs]).results
+        except GdlError as exc:
+            if exc.code not in _TOO_LARGE or len(reqs) == 1:
+                raise
+            self.splits += 1  # run_batched clears the engine before each half
+            h = len(reqs) // 2
+            return self._run(eng, prog, reqs[:h]) + self._run(eng, prog, reqs[h:])
 
     def serve(self, requests, time_scale=1.0):
         """Release requests at their arrival times (scaled) and serve them."""
@@ -202,7 +229,8 @@ class Server:
         lat = [r.finish - r.arrival for r in requests]
         out = {"requests": len(requests), "makespan_s": makespan,
                "throughput_rps": len(requests) / makespan, "batches": len(self.batches),
-               "mean_batch": float(np.mean([b[1] for b in self.batches])) if self.batches else 0}
+               "mean_batch": float(np.mean([b[1] for b in self.batches])) if self.batches else 0,
+               "splits": self.splits}
         out.update(percentiles(lat))
         for kind in ("tc", "sg"):
             sub = [r.finish - r.arrival for r in requests if r.kind == kind]

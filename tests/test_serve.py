@@ -23,7 +23,19 @@ def test_stream_shape_and_estimates():
     assert 0.55 < kinds.count("tc") / len(kinds) < 0.85
     arr = [r.arrival for r in reqs]
     assert arr == sorted(arr) and 0.5 < arr[-1] < 2.0  # ~200 requests at 200/s
-    assert all(r.est_bytes > 0 for r in reqs)
+    assert all(r.est_bytes > 0 and r.est_tuples > 0 for r in reqs)
+
+
+def test_take_respects_the_tuple_cap():
+    """A batch's summed first-join candidates stay within the cap (its first
+    request is always admitted, so one query can still run alone)."""
+    reqs = small_stream(30)
+    cap = max(r.est_tuples for r in reqs) * 2
+    srv = S.Server(slots=1, budget_bytes=1 << 40, max_batch=64, tuple_cap=cap)
+    srv.queue.extend(reqs)
+    while srv.queue:
+        batch = srv._take()
+        assert batch and (len(batch) == 1 or sum(r.est_tuples for r in batch) <= cap)
 
 
 def test_take_batches_one_kind_within_budget():
@@ -56,3 +68,32 @@ def test_plain_server_serves_everything():
     stats = S.Server(slots=1, batched=False).serve(reqs)
     assert stats["requests"] == 12 and stats["batches"] == 12
     assert all(r.result is not None for r in reqs)
+
+
+@pytest.mark.gpu
+def test_refused_batch_is_split_and_served(monkeypatch):
+    """A batch the engine refuses for its size is run again in halves; every
+    query still gets the result it gets alone."""
+    import gdlog_b200 as G
+    reqs = small_stream(10, seed=9)
+    real = B.run_batched
+    calls = []
+
+    def picky(eng, prog, instances, node_counts=None):
+        calls.append(len(instances))
+        if len(instances) > 2:  # stand-in for the engine's list limit
+            raise G.GdlError(4, "relation exceeds the tuple limit")
+        return real(eng, prog, instances, node_counts=node_counts)
+
+    monkeypatch.setattr(S.B, "run_batched", picky)
+    srv = S.Server(slots=1, budget_bytes=1 << 40, max_batch=8)
+    srv.queue.extend(reqs)
+    srv.done = True
+    srv._work(0.0)
+    assert srv.splits > 0 and all(r.result is not None for r in reqs)
+    monkeypatch.setattr(S.B, "run_batched", real)
+    with Engine("gpu") as g:
+        for r in reqs:
+            alone = B.run_plain_loop(g, S.PROGRAMS[r.kind], [r.inputs]).results[0]
+            assert (r.result.sizes, r.result.digests, r.result.iterations) == \
+                (alone.sizes, alone.digests, alone.iterations), r.id
