@@ -25,8 +25,9 @@ struct LieDev {
   u64 *trace;                 // [trace rows][n_update][3]
 };
 
-__global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
-  if (ctl_stop(ctl) || threadIdx.x != 0) return;
+// Open an iteration: working visibilities from the committed ones, NEWT
+// emptied, this iteration's Copy-once flags cleared.
+__device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L) {
   for (int i = 0; i < L->n_update; i++) {
     RelDev &r = rels[L->update[i]];
     r.w_full_vis = r.full_vis;
@@ -47,6 +48,11 @@ __global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
   for (int i = 0; i < L->n_ops; i++) L->once_pending[i] = 0;
 }
 
+__global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
+  if (ctl_stop(ctl) || threadIdx.x != 0) return;
+  begin_iteration(rels, L);
+}
+
 template <class T>
 __device__ __forceinline__ void dswap(T &a, T &b) {
   T t = a;
@@ -54,7 +60,10 @@ __device__ __forceinline__ void dswap(T &a, T &b) {
   b = t;
 }
 
-__global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
+// begin_next: when the loop goes on, also open the next iteration (the
+// graph body then needs no k_begin of its own; the host launches one
+// before each graph launch).
+__global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
   if (threadIdx.x != 0) return;
   bool stop = ctl->done | ctl->pause | ctl->overflow | ctl->timeout;
   if (!stop) {
@@ -119,8 +128,9 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl) {
       ctl->done = 1;
     else if (next >= ctl->stop_at)
       ctl->pause = 1;
-    __threadfence();
     stop = ctl->done | ctl->pause;
+    if (begin_next && !stop) begin_iteration(rels, L);
+    __threadfence();
   }
   if (ctl->cond_set) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
 }

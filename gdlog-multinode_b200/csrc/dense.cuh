@@ -18,7 +18,8 @@
 // A scan is three kernels: k_bm_tilecount (per 2048-word tile, clean tiles
 // skipped by their dirty word), k_bm_scan (exclusive prefix of the tile
 // counts, totals, capacity check) and k_bm_write.  All update relations are
-// counted and checked before any of them is written (k_scan_gate), so a
+// counted and checked before any of them is written (the write passes'
+// capacity gate), so a
 // capacity overflow leaves every bitmap untouched and the update step can
 // simply run again after the lists grow.
 //
@@ -132,7 +133,13 @@ struct BmScanArgs {
   u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
   u64 *inst_delta; // if set: per-instance count of list a is added here
   int need_a, need_b;  // need slots to raise on overflow (-1: none)
-  int gated;           // the overflow is raised by k_scan_gate, not by k_bm_write
+  // Gated write pass: before writing anything, every update relation's
+  // count pass is checked (gate_rels[gate_update[0 .. gate_n)]); one list
+  // too small anywhere raises the overflow and no bitmap is touched.
+  int gated;
+  const RelDev *gate_rels;
+  const int *gate_update;
+  int gate_n;
   u64 *tile_prefix;    // [tiles] tile counts, then their exclusive prefix (a << 32 | b)
   // Group mode (no index built): a warp per group of kGroupChunks 64-word
   // chunks, tile_prefix holding one entry per group.  chunk_list: [chunks]
@@ -407,17 +414,24 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_scan(BmScanArgs a) {
   launch_rec_finish(a.lrec);
 }
 
-// After the count and scan passes of every update relation: raise an
-// overflow before any relation's bitmaps are written.
-__global__ void k_scan_gate(RelDev *rels, const int *update, int n_update, Ctl *ctl) {
-  if (threadIdx.x != 0 || ctl_stop(ctl)) return;
-  for (int i = 0; i < n_update; i++) {
-    RelDev &r = rels[update[i]];
-    if (r.dense && r.scan.overflow) {
-      ctl->overflow_stage = 1;
-      atomicExch(&ctl->overflow, 1u);
-    }
+// The capacity gate of a write pass (after the count and scan passes of
+// every update relation): true when some relation's list is too small.
+// The block that sees it closed first raises the overflow (stage 1: the
+// joins' bits are kept, only the update step reruns); every block returns
+// without writing.
+__device__ __forceinline__ bool write_gate_closed(const BmScanArgs &a) {
+  if (!a.gated) return a.rec->overflow != 0;
+  bool closed = false;
+  for (int i = 0; i < a.gate_n; i++) {
+    const RelDev &r = a.gate_rels[a.gate_update[i]];
+    closed |= r.dense && r.scan.overflow;
   }
+  if (closed && blockIdx.x == 0 && threadIdx.x == 0) {
+    a.rec->pop_g = 0;
+    a.ctl->overflow_stage = 1;
+    atomicExch(&a.ctl->overflow, 1u);
+  }
+  return closed;
 }
 
 // The block that finishes a write pass last publishes the list sizes.
@@ -502,10 +516,10 @@ struct BmWriteSmem {
 __global__ void __launch_bounds__(kBmBlock, 3) k_bm_write(BmScanArgs a) {
   __shared__ BmWriteSmem sm;
   if (ctl_stop(a.ctl)) return;
-  if (a.rec->overflow) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (write_gate_closed(a)) {
+    if (!a.gated && blockIdx.x == 0 && threadIdx.x == 0) {
       a.rec->pop_g = 0;
-      if (!a.gated) atomicExch(&a.ctl->overflow, 1u);
+      atomicExch(&a.ctl->overflow, 1u);
     }
     return;
   }
@@ -631,10 +645,10 @@ struct GroupWriteSmem {
 __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
   __shared__ GroupWriteSmem sm;
   if (ctl_stop(a.ctl)) return;
-  if (a.rec->overflow) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (write_gate_closed(a)) {
+    if (!a.gated && blockIdx.x == 0 && threadIdx.x == 0) {
       a.rec->pop_g = 0;
-      if (!a.gated) atomicExch(&a.ctl->overflow, 1u);
+      atomicExch(&a.ctl->overflow, 1u);
     }
     return;
   }

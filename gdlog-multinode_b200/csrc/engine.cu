@@ -14,7 +14,11 @@
 //            k_sort_hist + k_sort_pass x P      (onesweep radix sort NEWT)
 //            k_merge_diff                       (dedup, NEWT \ FULL, FULL ∪ Δ)
 //            k_index_build (FULL, DELTA)        (only indexes some op probes)
-//   k_commit                     swap in, log, decide termination
+//   k_commit                     swap in, log, decide termination (and,
+//                                in the graph, open the next iteration)
+//
+// (In the dense form the per-relation dedup is a bitmap scan instead, and
+// joins set bits: dense.cuh.)
 //
 // That sequence is captured once into a CUDA graph as the body of a
 // conditional while-node; k_commit sets the node's condition, so a whole
@@ -661,15 +665,19 @@ BmScanArgs scan_none(const DenseMap &map) {
   return a;
 }
 
-void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc);
+void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc,
+                         bool begin_next);
 
-void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
+// One iteration.  in_graph: the body of the graph's while-node, which the
+// host opens with a k_begin before each launch and whose k_commit opens
+// the next iteration; otherwise the iteration opens itself.
+void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, bool in_graph) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
   const DenseMap &map = L.map;
   const u64 words = dense ? map.words : 0;
-  PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
+  if (!in_graph) PLAUNCH(kc, kPControl, k_begin<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (op.kind == 0) {
@@ -795,13 +803,14 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) 
       }
     }
   }
-  enqueue_update_step(e, L, plan, kc);
+  enqueue_update_step(e, L, plan, kc, in_graph);
 }
 
 // The per-relation update step (DELTA, FULL', indexes) and the commit of
 // one iteration.  After a capacity overflow in a dense scan it is enqueued
 // again on its own: the NEWT bitmaps still hold the iteration's joins.
-void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc) {
+void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc,
+                         bool begin_next) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
   const bool dense = L.dense;
@@ -828,11 +837,12 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
         if (plan.full_idx[r]) a.idx_b = &R[r].full_idx_next;
       }
       a.pop_g_out = &R[r].c_newt_n;
+      a.gate_rels = R;
+      a.gate_update = &L.d_lie->update[0];
+      a.gate_n = (int)L.update.size();
       launch_scan_count(e, a, r, kc);
       scans.push_back(a);
     }
-    PLAUNCH(kc, kPControl, k_scan_gate<<<1, 32, 0, s>>>(R, &L.d_lie->update[0],
-                                                         (int)L.update.size(), e->d_ctl));
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
     const u64 tiles = L.map.words / kBmTileWords;
@@ -879,7 +889,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
   if (L.d_inst_delta)
     PLAUNCH(kc, kPControl, k_inst_track<<<grid_for(e, L.n_inst, 256, 1), 256, 0, s>>>(
                                L.d_inst_delta, L.d_inst_last, L.n_inst, e->d_ctl));
-  PLAUNCH(kc, kPControl, k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl));
+  PLAUNCH(kc, kPControl, k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl, begin_next ? 1 : 0));
 }
 
 gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
@@ -910,7 +920,7 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   CK(e, cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal));
   Counts kc;
-  enqueue_iteration(e, L, plan, &kc);
+  enqueue_iteration(e, L, plan, &kc, true);
   cudaGraph_t captured = nullptr;
   r = cudaStreamEndCapture(e->s, &captured);
   if (r != cudaSuccess) {
@@ -1222,6 +1232,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     const u64 it0 = c.iteration;
     u64 enqueued = 0;
     if (use_graph) {
+      // the body's first iteration is opened here, later ones by k_commit
+      k_begin<<<1, 32, 0, e->s>>>(e->d_rels, L.d_lie, e->d_ctl);
+      L.kernels++;
+      e->prof_launches[kPControl]++;
       CK(e, cudaGraphLaunch(L.gexec, e->s));
       L.graph_launches++;
     } else {
@@ -1230,7 +1244,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       const u64 nb = e->profile ? 1 : std::min<u64>(batch, trace_rows);
       for (u64 k = 0; k < nb; k++) {
         Counts kc;
-        enqueue_iteration(e, L, plan, &kc);
+        enqueue_iteration(e, L, plan, &kc, false);
         L.per_iter = kc;
         enqueued++;
       }
@@ -1295,7 +1309,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
           const u64 it1 = c.iteration;
           Counts kc;
-          enqueue_update_step(e, L, plan, &kc);
+          enqueue_update_step(e, L, plan, &kc, false);
           CK(e, cudaGetLastError());
           CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
           CK(e, cudaStreamSynchronize(e->s));

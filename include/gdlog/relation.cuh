@@ -8,6 +8,8 @@
 // after each load and each LIE::fixpoint_loop.
 #pragma once
 
+#include <climits>
+
 #include <string>
 #include <vector>
 
@@ -17,12 +19,23 @@
 enum RelationVersion { DELTA, FULL, NEWT };  // include/relation.cuh:13
 enum JoinDirection { LEFT, RIGHT };          // include/relation.cuh:75 (unused)
 
+// The reference's empty-slot marker of its hash index (include/relation.cuh:
+// 27); drivers print it.  This engine's index slots carry a build epoch
+// instead, so the value marks nothing here.
+#ifndef EMPTY_HASH_ENTRY
+#define EMPTY_HASH_ENTRY ULONG_MAX
+#endif
+
 struct GHashRelContainer {
   tuple_size_t index_column_size = 1;
   int dependent_column_size = 0;
   tuple_size_t tuple_counts = 0;
   int arity = 2;
   bool tmp_flag = false;
+  // which engine relation and version this container stands for (set by
+  // load_relation; used by the printers of print.cuh)
+  int32_t rel_id = -1;
+  int32_t version = -1;
   GHashRelContainer(int arity, int indexed_column_size, int dependent_column_size,
                     bool tmp_flag = false)
       : index_column_size(indexed_column_size), dependent_column_size(dependent_column_size),
@@ -104,6 +117,10 @@ inline void load_relation(Relation *target, std::string name, int arity, column_
                                             dependent_column_size, target->index_flag ? 1 : 0,
                                             tmp_flag ? 1 : 0, &target->id),
                         "gdl_relation_create");
+  target->full->rel_id = target->delta->rel_id = target->newt->rel_id = target->id;
+  target->full->version = GDL_FULL;
+  target->delta->version = GDL_DELTA;
+  target->newt->version = GDL_NEWT;
   gdlog_compat::check(
       gdl_relation_load(e, target->id, (const uint64_t *)data, data ? data_row_size : 0),
       "gdl_relation_load");

@@ -23,12 +23,36 @@ def test_headers_compile_standalone(tmp_path):
     """Every drop-in header compiles on its own (nvcc, no device needed)."""
     inc = os.path.join(REPO, "include")
     for h in ("tuple.cuh", "relation.cuh", "relational_algebra.cuh", "lie.cuh", "exception.cuh",
-              "timer.cuh"):
+              "timer.cuh", "print.cuh"):
         src = tmp_path / f"t_{h}.cu"
         src.write_text(f'#include "gdlog/{h}"\nint main() {{ return 0; }}\n')
         r = subprocess.run(["nvcc", "-std=c++17", "-rdc=true", "-I", inc, "-c", str(src), "-o",
                             str(tmp_path / "t.o")], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-2000:]
+
+
+REF_TEST = "/root/reference/test"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_TEST), reason="reference sources not present")
+@pytest.mark.parametrize("driver", ["tc", "sg", "cspa"])
+def test_reference_drivers_build_unchanged(tmp_path, driver):
+    """The reference's own drivers (test/tc.cu, sg.cu, cspa.cu), unchanged
+    except that their `../include/*.cuh` lines name this repository's
+    drop-in headers, compile and link against the engine's library (nvcc,
+    no device needed; a copy in a temporary directory, nothing kept)."""
+    import re
+    src = open(os.path.join(REF_TEST, f"{driver}.cu")).read()
+    src = re.sub(r'"\.\./include/([a-z_]+\.cuh)"', r'"gdlog/\1"', src)
+    f = tmp_path / f"{driver}.cu"
+    f.write_text(src)
+    lib = os.path.join(REPO, "gdlog-multinode_b200", "lib")
+    r = subprocess.run(["nvcc", "-std=c++17", "-rdc=true", "-gencode",
+                        "arch=compute_100a,code=sm_100a", "-I", os.path.join(REPO, "include"),
+                        "-o", str(tmp_path / driver), str(f), "-L", lib, "-lgdlog_b200"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert (tmp_path / driver).exists()
 
 
 @pytest.mark.gpu
