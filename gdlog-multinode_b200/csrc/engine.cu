@@ -170,6 +170,10 @@ struct gdl_engine {
   int index_slots_per_key = 2;
   int dirty_min_log2_words = 24;
   int dense_join_passes = 1;
+  // Device memory in bytes, read once at creation: cudaMemGetInfo can take
+  // tens of milliseconds on a busy host, so the fixpoint sizes its lists
+  // from this and asks for free memory only after an allocation failed.
+  u64 total_mem = 0;
   // Batched form (gdl_engine_set_instances): the block-diagonal layout.
   bool instances = false;
   std::vector<SegInfo> segs;
@@ -995,6 +999,31 @@ gdl_status build_index_now(gdl_engine *e, int r, bool delta) {
   return GDL_OK;
 }
 
+// The lists of a dense LIE at capacity `cap` rows each (and the indexes
+// some op probes on them).
+gdl_status presize_lists(gdl_engine *e, LieHost &L, const Plan &plan, u64 cap) {
+  for (int r : L.update) {
+    RelDev &h = e->h[r];
+    TRY(ensure_arr(e, h.delta, cap, true));
+    TRY(ensure_arr(e, h.delta_next, cap, false));
+    if (plan.newt_list[r] || plan.acopy_src[r]) TRY(ensure_arr(e, h.newt, cap, false));
+    if (plan.full_list[r]) {
+      TRY(ensure_arr(e, h.full, cap, true));
+      TRY(ensure_arr(e, h.full_next, cap, false));
+      if (plan.full_idx[r]) {
+        TRY(ensure_index(e, h.full_idx, h.full.cap));
+        TRY(ensure_index(e, h.full_idx_next, h.full_next.cap));
+      }
+    }
+    if (plan.delta_idx[r]) {
+      TRY(ensure_index(e, h.delta_idx, h.delta.cap));
+      TRY(ensure_index(e, h.delta_idx_next, h.delta_next.cap));
+    }
+  }
+  for (int r : L.tmps) TRY(ensure_arr(e, e->h[r].newt, cap, false));
+  return GDL_OK;
+}
+
 gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
   if ((int)L.ops.size() > kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops in one LIE");
@@ -1018,8 +1047,20 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   // whole fixpoint_loop (test/tc.cu:120-140): setup, loop and finish.
   CK(e, cudaEventRecord(e->ev0, e->s));
   const auto t_setup = std::chrono::steady_clock::now();
+  // GDLOG_TRACE_SETUP=1: host time of each setup phase on stderr
+  static const bool trace_setup = getenv("GDLOG_TRACE_SETUP") != nullptr;
+  std::vector<std::pair<const char *, double>> phases;
+  auto t_phase = t_setup;
+  auto mark = [&](const char *name) {
+    if (!trace_setup) return;
+    const auto now = std::chrono::steady_clock::now();
+    phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - t_phase).count());
+    t_phase = now;
+  };
   TRY(reset_ctl(e));
+  mark("reset_ctl");
   TRY(pull(e));
+  mark("pull");
   // Setup (src/lie.cu:49-59): DELTA := the first |FULL| rows of FULL's raw
   // buffer; capacities for the loop.
   for (int r : L.update) {
@@ -1048,6 +1089,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(ensure_arr(e, h.newt, std::max<u64>(h.newt.cap, kMinCap), false));
     h.newt.n = 0;
   }
+  mark("arrays");
   // Dense form (dense.cuh) when the key domain is small enough; always in
   // the batched form, whose block-diagonal bitmap is the only layout.
   for (int r : L.update)
@@ -1094,6 +1136,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       TRY(ensure_bitmaps(e, r, words, false));
       e->h[r].dense = 1;
     }
+    mark("bitmap_alloc");
     // A dirty map pays when a NEWT bitmap is too large to scan whole every
     // iteration; for small ones the scans read everything and the joins
     // skip the extra store.
@@ -1101,12 +1144,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     for (auto *v : {&L.update, &L.tmps})
       for (int r : *v) e->h[r].dirty = use_dirty ? e->h[r].bmD : nullptr;
     TRY(ensure_dense_scratch(e, words));
+    mark("dense_scratch");
     // Every list of the loop is bounded by the key domain: size them for
-    // it up front (within a quarter of free HBM shared among the lists), so
-    // that the loop does not stop to grow buffers.  Untouched capacity
-    // costs nothing but address space in the stream-ordered pool.
-    size_t free_b = 0, total_b = 0;
-    CK(e, cudaMemGetInfo(&free_b, &total_b));
+    // it up front (within a quarter of the device's memory shared among
+    // the lists), so that the loop does not stop to grow buffers.  If that
+    // does not fit, retry within a quarter of the memory actually free.
     u64 lists = 0;
     for (int r : L.update)
       lists += 2 + ((plan.newt_list[r] || plan.acopy_src[r]) ? 1 : 0) +
@@ -1114,29 +1156,22 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     lists += L.tmps.size();
     const u64 domain = words * 32;
     const u64 cap = std::min<u64>(
-        {domain, (u64)(free_b / 4) / std::max<u64>(lists, 1) / 8, kMaxRows});
-    for (int r : L.update) {
-      RelDev &h = e->h[r];
-      TRY(ensure_arr(e, h.delta, cap, true));
-      TRY(ensure_arr(e, h.delta_next, cap, false));
-      if (plan.newt_list[r] || plan.acopy_src[r]) TRY(ensure_arr(e, h.newt, cap, false));
-      if (plan.full_list[r]) {
-        TRY(ensure_arr(e, h.full, cap, true));
-        TRY(ensure_arr(e, h.full_next, cap, false));
-        if (plan.full_idx[r]) {
-          TRY(ensure_index(e, h.full_idx, h.full.cap));
-          TRY(ensure_index(e, h.full_idx_next, h.full_next.cap));
-        }
-      }
-      if (plan.delta_idx[r]) {
-        TRY(ensure_index(e, h.delta_idx, h.delta.cap));
-        TRY(ensure_index(e, h.delta_idx_next, h.delta_next.cap));
-      }
+        {domain, e->total_mem / 4 / std::max<u64>(lists, 1) / 8, kMaxRows});
+    gdl_status ps = presize_lists(e, L, plan, cap);
+    if (ps == GDL_E_NOMEM) {
+      cudaGetLastError();
+      size_t free_b = 0, total_b = 0;
+      CK(e, cudaMemGetInfo(&free_b, &total_b));
+      ps = presize_lists(e, L, plan,
+                         std::min<u64>(cap, (u64)(free_b / 4) / std::max<u64>(lists, 1) / 8));
     }
-    for (int r : L.tmps) TRY(ensure_arr(e, e->h[r].newt, cap, false));
+    TRY(ps);
   }
+  mark("dense_alloc");
   TRY(ensure_scratch(e));
+  mark("scratch");
   TRY(push(e));
+  mark("push");
   if (L.dense) {
     // FULL's bitmap from its list; NEWT bitmaps empty.
     const u64 words = L.map.words;
@@ -1156,6 +1191,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     }
     CK(e, cudaGetLastError());
   }
+  mark("bitmaps");
   // An unsorted DELTA (raw load order) used as a join inner is sorted and
   // deduplicated first (the reference's index walk is undefined there).
   for (int r : L.update) {
@@ -1179,11 +1215,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       TRY(push(e));
     }
   }
+  mark("delta_sort");
   // Indexes every join of this LIE probes.
   for (size_t r = 0; r < e->rels.size(); r++) {
     if (plan.full_idx[r]) TRY(build_index_now(e, (int)r, false));
     if (plan.delta_idx[r]) TRY(build_index_now(e, (int)r, true));
   }
+  mark("indexes");
   // Device LIE description.
   LieDev ld;
   CK(e, cudaMemcpyAsync(&ld, L.d_lie, sizeof(LieDev), cudaMemcpyDeviceToHost, e->s));
@@ -1211,7 +1249,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   L.trace.clear();
   L.retries = 0;
   L.grow_ms = L.graph_ms = 0;
+  mark("lie_ctl");
   L.setup_ms = host_ms_since(t_setup);
+  if (trace_setup) {
+    fprintf(stderr, "gdlog setup %.3f ms:", L.setup_ms);
+    for (auto &ph : phases) fprintf(stderr, " %s %.3f", ph.first, ph.second);
+    fprintf(stderr, "\n");
+  }
   L.graph_launches = 0;
   L.kernels = 0;
   L.graph_dirty = true;
@@ -1360,19 +1404,21 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(reset_ctl(e));  // clear done/pause so that the scans below run
     TRY(pull(e));
     bool any = false;
-    size_t free_b = 0, total_b = 0;
-    CK(e, cudaMemGetInfo(&free_b, &total_b));
     for (int r : L.update)
       if (e->h[r].full_lazy) {
         // The batched form may keep a FULL too large for a list as its
         // bitmap only (per-instance sizes, digests and exports read it).
         const u64 n = e->h[r].full.n;
-        if (e->instances && (n > kMaxRows || n * 8 > free_b / 2)) {
+        gdl_status as = GDL_E_NOMEM;
+        if (!e->instances || (n <= kMaxRows && n * 8 <= e->total_mem / 4))
+          as = ensure_arr(e, e->h[r].full, n, false);
+        if (as == GDL_E_NOMEM && e->instances) {
+          cudaGetLastError();
           e->rels[r].full_resident = true;
           e->h[r].full_lazy = 0;
           continue;
         }
-        TRY(ensure_arr(e, e->h[r].full, n, false));
+        TRY(as);
         any = true;
       }
     if (any) {
@@ -1466,6 +1512,10 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
   gdl_engine *e = new gdl_engine;
   e->device = device;
   cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device);
+  {
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) == cudaSuccess) e->total_mem = t;
+  }
   if (stream) {
     e->s = (cudaStream_t)stream;
   } else {
