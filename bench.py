@@ -417,6 +417,21 @@ def run_dag_batch(a) -> None:
     inst = [(e,) for (_, _, e) in dags]
     counts = [L * Wd for (L, Wd, _) in dags]
     eng = Engine("gpu", device=local)
+    import autotune as A
+    tuner = A.Tuner()
+    tkey = f"{tuner.gpu}|{A.batch_bucket('tc', inst)}"
+    if a.tune:
+        # the batched fixpoint's device time under every candidate (the
+        # sort path does not take the batched form: dense candidates only)
+        space = dict(A.SPACE, dedup=["dense"])
+        rec = tuner.tune_runner(
+            eng, tkey, lambda e: B.run_batched(e, P.tc, inst, node_counts=counts).device_ms,
+            space=space, reps=1)
+        print(json.dumps({"tuned": "dag_batch384", "bucket": tkey, **rec}), flush=True)
+        eng.close()
+        return
+    rec = tuner.apply_key(eng, tkey)
+    tuning = rec["config"] if rec else "engine defaults (no cached tuning for this size bucket)"
     if a.single:
         eng.profile_reset()
         eng.set_profile(True)
@@ -465,7 +480,7 @@ def run_dag_batch(a) -> None:
         "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic",
         "config": {"workload": "384 layered DAGs, L in [8,128], W in [16,256] log-uniform",
-                   "program": "tc", "tuples_per_step": tuples,
+                   "program": "tc", "tuples_per_step": tuples, "tuning": tuning,
                    "parallelism": f"instances sharded over {world} ranks (LPT, no exchange)"
                    if world > 1 else "single"},
         "e2e": {"value": 384 / wall, "unit": "instances/s",

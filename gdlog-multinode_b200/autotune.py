@@ -33,6 +33,7 @@ DEFAULT_CACHE = os.path.join(HERE, "tuning_cache.json")
 SPACE = {
     "dedup": ["dense", "sort"],
     "dense_join_passes": [1, 2],
+    "join_aggregate": [1, 2],
     "join_ctas_per_sm": [4, 8, 16],
     "count_ctas_per_sm": [2, 4, 8],
     "index_slots_per_key": [2, 4],
@@ -41,12 +42,16 @@ SPACE = {
 
 def _redundant(cfg: dict) -> bool:
     """Configurations that differ from an earlier one only in a parameter
-    their path does not read: the join form of the sort path, and the grids
-    of the count / materialise passes of the one-pass dense join."""
-    if cfg.get("dedup") == "sort" and cfg.get("dense_join_passes", 1) != 1:
+    their path does not read: the join form and bit aggregation of the sort
+    path, the aggregation of the two-pass dense join, and the grids of the
+    count / materialise passes of the one-pass dense join."""
+    one_pass = cfg.get("dense_join_passes", 1) == 1
+    if cfg.get("dedup") == "sort" and (not one_pass or cfg.get("join_aggregate", 1) != 1):
         return True
-    if cfg.get("dedup") == "dense" and cfg.get("dense_join_passes", 1) == 1:
+    if cfg.get("dedup") == "dense" and one_pass:
         return (cfg.get("count_ctas_per_sm", 2) != 2 or cfg.get("join_ctas_per_sm", 4) != 4)
+    if cfg.get("dedup") == "dense" and cfg.get("join_aggregate", 1) != 1:
+        return True
     return False
 
 
@@ -69,13 +74,30 @@ def candidates(space=SPACE, limit=None):
 
 def measure(eng, prog, inputs, cfg, reps=2) -> float:
     """Best device milliseconds of the program's fixpoints under cfg."""
+    def run(e):
+        e.clear()
+        r = prog(e, *inputs, sync=e.sync)
+        return sum(lie.stats()["ms"] for lie in r.lies.values())
+    return measure_runner(eng, run, cfg, reps)
+
+
+def measure_runner(eng, run, cfg, reps=2) -> float:
+    """Best of `reps` calls of run(eng) -> device milliseconds under cfg."""
     eng.set_tuning(**cfg)
-    best = float("inf")
-    for _ in range(reps):
-        eng.clear()
-        r = prog(eng, *inputs, sync=eng.sync)
-        best = min(best, sum(lie.stats()["ms"] for lie in r.lies.values()))
-    return best
+    return min(run(eng) for _ in range(reps))
+
+
+def batch_bucket(program: str, instances) -> str:
+    """Size class of a batch of instances: program, instance count (log2),
+    largest instance (log2 nodes), total tuples (log2)."""
+    n_rows = sum(len(x) for inp in instances for x in inp)
+    nodes = 1
+    for inp in instances:
+        for x in inp:
+            if len(x):
+                nodes = max(nodes, int(np.asarray(x).max()) + 1)
+    return (f"{program}-batch:i{int(math.log2(max(len(instances), 1)))}"
+            f":n{int(math.log2(nodes))}:t{int(math.log2(max(n_rows, 1)))}")
 
 
 class Tuner:
@@ -95,19 +117,35 @@ class Tuner:
 
     def tune(self, eng, prog, inputs, space=SPACE, reps=2, save=True) -> dict:
         """Time every candidate on this workload; remember and return the best."""
+        def run(e):
+            e.clear()
+            r = prog(e, *inputs, sync=e.sync)
+            return sum(lie.stats()["ms"] for lie in r.lies.values())
+        return self.tune_runner(eng, self.key(prog.__name__, inputs), run, space, reps, save)
+
+    def tune_runner(self, eng, key: str, run, space=SPACE, reps=2, save=True) -> dict:
+        """tune() for any run(eng) -> device milliseconds (e.g. a batched
+        fixpoint over many instances), cached under `key`."""
         results = []
         for cfg in candidates(space):
-            results.append((measure(eng, prog, inputs, cfg, reps), cfg))
+            results.append((measure_runner(eng, run, cfg, reps), cfg))
         results.sort(key=lambda x: x[0])
         best_ms, best = results[0]
         default_ms = next((ms for ms, c in results if c == candidates(space)[0]), None)
         rec = {"config": best, "ms": best_ms, "default_ms": default_ms,
                "tried": len(results)}
-        self.cache[self.key(prog.__name__, inputs)] = rec
+        self.cache[key] = rec
         if save:
             with open(self.path, "w") as f:
                 json.dump(self.cache, f, indent=1, sort_keys=True)
         eng.set_tuning(**best)
+        return rec
+
+    def apply_key(self, eng, key: str) -> dict | None:
+        """Set the cached best configuration stored under `key`, if any."""
+        rec = self.cache.get(key)
+        if rec:
+            eng.set_tuning(**rec["config"])
         return rec
 
     def apply(self, eng, prog, inputs) -> dict | None:

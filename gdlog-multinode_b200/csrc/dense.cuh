@@ -103,6 +103,40 @@ __device__ __forceinline__ void dm_set(const DenseMap &m, u32 *bm, u8 *dirty, u6
     atomicOr(&ctl->oob, 8192u);
 }
 
+// Warp-aggregated bit-sets: every lane of the warp holds at most one
+// candidate (w = ~0: none); lanes whose bits fall in the same word OR them
+// in shared memory first (s: this warp's 32 slots), and one lane per
+// distinct word sends the reduction.  All 32 lanes must call it.  Pays when
+// a warp's candidates share words (the batched DAG closures: one row, one
+// layer); costs a match and two warp barriers per 32 candidates otherwise.
+__device__ __forceinline__ void warp_set_bits(u32 *bm, u8 *dirty, u64 w, u32 bit, u32 *s) {
+  const int lane = threadIdx.x & 31;
+  const unsigned same = __match_any_sync(0xffffffffu, w);
+  const int leader = __ffs(same) - 1;
+  s[lane] = 0u;
+  __syncwarp();
+  if (bit) atomicOr(&s[leader], bit);
+  __syncwarp();
+  if (lane == leader && w != ~0ull) {
+    asm volatile("red.global.or.b32 [%0], %1;" ::"l"(bm + w), "r"(s[lane]) : "memory");
+    if (dirty) dirty[w / kBmChunkWords] = 1;
+  }
+  __syncwarp();
+}
+
+// The word and bit of one candidate for warp_set_bits (w = ~0 when it fails
+// the predicate, or lies outside its instance: then recorded in Ctl::oob).
+__device__ __forceinline__ void dm_word(const DenseMap &m, u64 key, Ctl *ctl, u64 *w, u32 *bit) {
+  u32 b;
+  if (dm_locate(m, key, w, &b) && *w < m.words) {
+    *bit = 1u << b;
+  } else {
+    atomicOr(&ctl->oob, 8192u);
+    *w = ~0ull;
+    *bit = 0u;
+  }
+}
+
 // Dirty byte of the chunk thread `tid` reads in scan tile `tile` (8 words
 // per thread, 8 threads per chunk); 1 when no map is kept.
 __device__ __forceinline__ u8 chunk_dirty(const u8 *dirty, u64 tile, int tid) {
@@ -842,8 +876,10 @@ struct FuseSmem {
   u64 row[kFuseBlock / 32][32];
   u64 excl[kFuseBlock / 32][32];
   u32 start[kFuseBlock / 32][32];
+  u32 agg[kFuseBlock / 32][32];  // warp_set_bits slots
 };
 
+template <bool AGG>
 __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
     k_join_bm(JoinArgs a, const RelDev *out_rd, DenseMap map) {
   __shared__ FuseSmem sm;
@@ -896,6 +932,8 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
     __syncwarp();
     for (u64 base = 0; base < total; base += 32) {
       const u64 p = base + lane;
+      u64 w = ~0ull;
+      u32 bit = 0u;
       if (p < total) {
         // the last run starting at or before p (an empty run shares its
         // offset with the next one, so it is never the last)
@@ -905,8 +943,14 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
           if (sm.excl[wid][r + h] <= p) r += h;
         const u64 t = gen_join(a.sel, inner[sm.start[wid][r] + (p - sm.excl[wid][r])],
                                sm.row[wid][r]);
-        if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
+        if (pred_ok(a.pred, t)) {
+          if (AGG)
+            dm_word(map, t, a.ctl, &w, &bit);
+          else
+            dm_set(map, G, D, t, a.ctl);
+        }
       }
+      if (AGG) warp_set_bits(G, D, w, bit, sm.agg[wid]);
     }
     __syncwarp();
     cand += total;
@@ -918,8 +962,10 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
 // The pieces of long runs appended by k_join_bm, a block per piece; the
 // last block empties the piece list for the next launch (so does block 0
 // of a stopped launch, which expands nothing).
+template <bool AGG>
 __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const RelDev *out_rd,
                                                              DenseMap map) {
+  __shared__ u32 s_agg[kFuseBlock / 32][32];
   if (ctl_stop(a.ctl)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.op->nc = 0;
     return;
@@ -932,9 +978,20 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
   for (u64 k = blockIdx.x; k < np; k += gridDim.x) {
     const u64 row = a.crow_key[k];
     const u32 s = a.crow_start[k], l = a.crow_len[k];
-    for (u32 j = threadIdx.x; j < l; j += blockDim.x) {
-      const u64 t = gen_join(a.sel, inner[s + j], row);
-      if (pred_ok(a.pred, t)) dm_set(map, G, D, t, a.ctl);
+    for (u32 j0 = 0; j0 < l; j0 += blockDim.x) {  // rounds uniform over the block
+      const u32 j = j0 + threadIdx.x;
+      u64 w = ~0ull;
+      u32 bit = 0u;
+      if (j < l) {
+        const u64 t = gen_join(a.sel, inner[s + j], row);
+        if (pred_ok(a.pred, t)) {
+          if (AGG)
+            dm_word(map, t, a.ctl, &w, &bit);
+          else
+            dm_set(map, G, D, t, a.ctl);
+        }
+      }
+      if (AGG) warp_set_bits(G, D, w, bit, s_agg[threadIdx.x >> 5]);
     }
     cand += l;
   }

@@ -170,6 +170,7 @@ struct gdl_engine {
   int index_slots_per_key = 2;
   int dirty_min_log2_words = 24;
   int dense_join_passes = 1;
+  int join_aggregate = 1;  // 1: one reduction per candidate, 2: warp-aggregated by word
   // Device memory in bytes, read once at creation: cudaMemGetInfo can take
   // tens of milliseconds on a busy host, so the fixpoint sizes its lists
   // from this and asks for free memory only after an allocation failed.
@@ -741,11 +742,16 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       JoinArgs b = a;
       b.rec = &e->recs[1];
       if (dense && e->dense_join_passes == 1) {
-        PLAUNCH(kc, kPJoinMat,
-                k_join_bm<<<grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm), kFuseBlock, 0,
-                            s>>>(a, &R[op.out], map));
-        PLAUNCH(kc, kPJoinMat,
-                k_join_heavy_bm<<<(int)e->sms * 4, kFuseBlock, 0, s>>>(b, &R[op.out], map));
+        const int jg = grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm);
+        if (e->join_aggregate == 2) {
+          PLAUNCH(kc, kPJoinMat, k_join_bm<true><<<jg, kFuseBlock, 0, s>>>(a, &R[op.out], map));
+          PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<true><<<(int)e->sms * 4, kFuseBlock, 0, s>>>(
+                                     b, &R[op.out], map));
+        } else {
+          PLAUNCH(kc, kPJoinMat, k_join_bm<false><<<jg, kFuseBlock, 0, s>>>(a, &R[op.out], map));
+          PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<false><<<(int)e->sms * 4, kFuseBlock, 0, s>>>(
+                                     b, &R[op.out], map));
+        }
         continue;
       }
       PLAUNCH(kc, kPJoinCount,
@@ -2007,7 +2013,8 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       (t->index_slots_per_key && (t->index_slots_per_key < 2 ||
                                   (t->index_slots_per_key & (t->index_slots_per_key - 1)))) ||
       (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
-      t->dense_join_passes < 0 || t->dense_join_passes > 2)
+      t->dense_join_passes < 0 || t->dense_join_passes > 2 || t->join_aggregate < 0 ||
+      t->join_aggregate > 2)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -2016,6 +2023,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->index_slots_per_key) e->index_slots_per_key = t->index_slots_per_key;
   if (t->dirty_min_log2_words) e->dirty_min_log2_words = t->dirty_min_log2_words;
   if (t->dense_join_passes) e->dense_join_passes = t->dense_join_passes;
+  if (t->join_aggregate) e->join_aggregate = t->join_aggregate;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -2029,6 +2037,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->index_slots_per_key = e->index_slots_per_key;
   t->dirty_min_log2_words = e->dirty_min_log2_words;
   t->dense_join_passes = e->dense_join_passes;
+  t->join_aggregate = e->join_aggregate;
   return GDL_OK;
 }
 

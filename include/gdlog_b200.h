@@ -116,6 +116,9 @@ typedef struct gdl_tuning {
   int32_t dense_join_passes;   /* joins into bitmaps: 1 = probe and expand in one
                                   pass (default), 2 = count pass, then a pass
                                   balanced by output position */
+  int32_t join_aggregate;      /* one-pass joins into bitmaps: 1 = one reduction
+                                  per candidate (default), 2 = lanes of a warp
+                                  that hit the same word combine their bits */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

@@ -15,8 +15,8 @@ def test_bucket_and_candidates():
     assert A.bucket("tc", (e,)) == "tc:n8:t8"
     cands = A.candidates()
     # sort: 3 x 3 x 2 grids; dense with 2 passes: the same; dense with one
-    # pass: only the index choice matters
-    assert len(cands) == 18 + 18 + 2
+    # pass: the index choice and the bit aggregation
+    assert len(cands) == 18 + 18 + 4
     assert {c["dedup"] for c in cands} == {"dense", "sort"}
     assert {c["dense_join_passes"] for c in cands} == {1, 2}
 

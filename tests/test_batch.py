@@ -57,12 +57,12 @@ def test_batched_oracle_loop_matches_itself():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("seed,dirty", [(1, 24), (2, 11)])
-def test_batched_tc_matches_plain_and_oracle(seed, dirty):
+@pytest.mark.parametrize("seed,dirty,agg", [(1, 24, 1), (2, 11, 1), (3, 11, 2)])
+def test_batched_tc_matches_plain_and_oracle(seed, dirty, agg):
     inst = dag_instances(12, seed)
     inst.append((np.zeros((0, 2), dtype=np.uint64),))  # an instance without edges
     with Engine("gpu") as g:
-        g.set_tuning(dirty_min_log2_words=dirty)
+        g.set_tuning(dirty_min_log2_words=dirty, join_aggregate=agg)
         batched = B.run_batched(g, P.tc, inst)
         plain = B.run_plain_loop(g, P.tc, inst)
     with Engine("oracle") as o:

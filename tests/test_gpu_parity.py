@@ -24,9 +24,10 @@ pytestmark = pytest.mark.gpu
 # Both deduplication paths of the engine: radix sort + merge-path merge, and
 # bitmaps over the key domain (every workload here has a small domain, so
 # "dense" is what the engine picks by itself); bitmaps with dirty maps at
-# every size (scans of listed dirty chunks), and bitmaps with joins as count
-# + materialise passes instead of one probe-and-expand pass.
-MODES = ["sort", "dense", "dense_dirty", "dense_2pass"]
+# every size (scans of listed dirty chunks), bitmaps with joins as count +
+# materialise passes instead of one probe-and-expand pass, and bitmaps whose
+# joins combine a warp's bits per word before the reduction.
+MODES = ["sort", "dense", "dense_dirty", "dense_2pass", "dense_agg"]
 
 
 def summarize(r):
