@@ -1812,6 +1812,100 @@ gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t ver, uint64_t
   return GDL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Files (get_row_size + get_relation_from_file, test/tc.cu:17-57)
+// ---------------------------------------------------------------------------
+namespace {
+bool tsv_space(char c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f';
+}
+
+// Parse one "%lld" at *p (leading white space skipped); false at the end
+// of the data or on a character that starts no number.
+bool tsv_value(const char *&p, const char *end, u64 *v) {
+  while (p < end && tsv_space(*p)) p++;
+  if (p >= end) return false;
+  bool neg = false;
+  if (*p == '+' || *p == '-') {
+    neg = *p == '-';
+    p++;
+  }
+  if (p >= end || *p < '0' || *p > '9') return false;
+  u64 x = 0;
+  while (p < end && *p >= '0' && *p <= '9') x = x * 10 + (u64)(*p++ - '0');
+  *v = neg ? (u64)(0 - x) : x;
+  return true;
+}
+}  // namespace
+
+gdl_status gdl_read_tsv(const char *path, int32_t arity, uint64_t *host_rows, uint64_t cap_rows,
+                        uint64_t *out_rows) {
+  auto bad = [](gdl_status s, const std::string &m) {
+    g_engineless_error = m;
+    return s;
+  };
+  if (!path || !out_rows || arity < 1) return bad(GDL_E_INVALID, "gdl_read_tsv: bad argument");
+  *out_rows = 0;
+  FILE *f = fopen(path, "rb");
+  if (!f) return bad(GDL_E_INVALID, std::string("cannot open ") + path);
+  std::string buf;
+  char chunk[1 << 16];
+  size_t got;
+  while ((got = fread(chunk, 1, sizeof chunk, f)) > 0) buf.append(chunk, got);
+  fclose(f);
+  u64 rows = 0;
+  for (char c : buf) rows += c == '\n';
+  *out_rows = rows;
+  if (rows > cap_rows || (rows && !host_rows))
+    return bad(GDL_E_CAPACITY, "gdl_read_tsv: the file has " + std::to_string(rows) + " rows");
+  const char *p = buf.data(), *end = buf.data() + buf.size();
+  for (u64 i = 0; i < rows; i++)
+    for (int j = 0; j < arity; j++) {
+      u64 v = 0;
+      if (!tsv_value(p, end, &v))
+        return bad(GDL_E_INVALID, std::string(path) + ": no value for row " + std::to_string(i) +
+                                      " column " + std::to_string(j));
+      host_rows[i * arity + j] = (uint64_t)v;
+      if (j != arity - 1 && p < end) p++;  // the separator character ("%lld%c")
+    }
+  return GDL_OK;
+}
+
+gdl_status gdl_relation_load_tsv(gdl_engine *e, int32_t rel, const char *path) {
+  CHECK_REL(e, rel);
+  const int arity = e->rels[rel].arity;
+  uint64_t n = 0;
+  gdl_status s = gdl_read_tsv(path, arity, nullptr, 0, &n);
+  if (s != GDL_OK && s != GDL_E_CAPACITY) return fail(e, s, "%s", g_engineless_error.c_str());
+  std::vector<uint64_t> rows(n * arity);
+  s = gdl_read_tsv(path, arity, rows.data(), n, &n);
+  if (s != GDL_OK) return fail(e, s, "%s", g_engineless_error.c_str());
+  return gdl_relation_load(e, rel, n ? rows.data() : nullptr, n);
+}
+
+gdl_status gdl_relation_dump_tsv(gdl_engine *e, int32_t rel, int32_t ver, const char *path,
+                                 uint64_t *out_rows) {
+  CHECK_REL(e, rel);
+  if (!path) return fail(e, GDL_E_INVALID, "null path");
+  std::vector<u64> k;
+  TRY(host_rows(e, rel, ver, k));
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(e, GDL_E_INVALID, "cannot write %s", path);
+  std::string out;
+  out.reserve(k.size() * 16);
+  char line[48];
+  for (u64 key : k) {
+    const int m = snprintf(line, sizeof line, "%llu\t%llu\n", (unsigned long long)key_c0(key),
+                           (unsigned long long)key_c1(key));
+    out.append(line, (size_t)m);
+  }
+  const bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
+  fclose(f);
+  if (!ok) return fail(e, GDL_E_INVALID, "short write to %s", path);
+  if (out_rows) *out_rows = k.size();
+  return GDL_OK;
+}
+
 gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *out) {
   CHECK_REL(e, rel);
   if (!out) return GDL_E_INVALID;

@@ -148,6 +148,12 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_engine_profile.restype = _I
         lib.gdl_engine_profile_reset.argtypes = [_P]
         lib.gdl_engine_profile_reset.restype = _I
+        lib.gdl_read_tsv.argtypes = [C.c_char_p, _I, _PU64, _U64, _PU64]
+        lib.gdl_read_tsv.restype = _I
+        lib.gdl_relation_load_tsv.argtypes = [_P, _I, C.c_char_p]
+        lib.gdl_relation_load_tsv.restype = _I
+        lib.gdl_relation_dump_tsv.argtypes = [_P, _I, _I, C.c_char_p, _PU64]
+        lib.gdl_relation_dump_tsv.restype = _I
     else:
         lib.orc_engine_create.argtypes = [_I, _I, C.POINTER(_P)]
         lib.orc_engine_create.restype = _I
@@ -163,6 +169,30 @@ def load_library(kind: str) -> C.CDLL:
         lib.orc_lie_seconds.restype = _I
     _libs[kind] = lib
     return lib
+
+
+def read_tsv(path: str, arity: int = 2) -> np.ndarray:
+    """The reference drivers' file read (test/tc.cu:17-57) through
+    gdl_read_tsv: rows = number of newlines, "%lld" values, one separator
+    character after every column but the last.  Needs no GPU."""
+    lib = load_library("gpu")
+    n = C.c_uint64(0)
+    code = lib.gdl_read_tsv(path.encode(), arity, None, 0, C.byref(n))
+    if code not in (0, 6):  # GDL_OK, GDL_E_CAPACITY (sizing call)
+        raise GdlError(code, lib.gdl_last_error(None).decode())
+    out = np.zeros((max(int(n.value), 1), arity), dtype=np.uint64)
+    code = lib.gdl_read_tsv(path.encode(), arity, out.ctypes.data_as(_PU64), n.value, C.byref(n))
+    if code:
+        raise GdlError(code, lib.gdl_last_error(None).decode())
+    return out[: int(n.value)]
+
+
+def write_tsv(path: str, rows: np.ndarray) -> None:
+    """Sorted-relation dump layout of gdl_relation_dump_tsv: decimal
+    columns separated by a tab, one row per line."""
+    with open(path, "w") as f:
+        for r in np.asarray(rows, dtype=np.uint64).tolist():
+            f.write("\t".join(str(c) for c in r) + "\n")
 
 
 class DeviceRows:
@@ -210,6 +240,10 @@ class Relation:
 
     def digest(self, version: int = FULL) -> int:
         return self.eng.digest(self, version)
+
+    def dump_tsv(self, path: str, version: int = FULL) -> int:
+        """Write this version's sorted tuples as TSV; returns the rows."""
+        return self.eng.dump_tsv(self, path, version)
 
     def instance_stats(self, n: int):
         """Batched form: per-instance (sizes, digests) of FULL, local ids."""
@@ -395,6 +429,23 @@ class Engine:
         if a.ndim != 2 or a.shape[1] != rel.arity:
             raise ValueError(f"rows must be (n, {rel.arity})")
         self._call("relation_load", rel.id, a.ctypes.data_as(_PU64), a.shape[0])
+
+    def load_tsv(self, rel: Relation, path: str) -> None:
+        """load_relation from a file read as the reference's drivers read it."""
+        if self.kind == "gpu":
+            self._check(self.lib.gdl_relation_load_tsv(self.h, rel.id, path.encode()))
+        else:
+            self.load(rel, read_tsv(path, rel.arity))
+
+    def dump_tsv(self, rel: Relation, path: str, version: int = FULL) -> int:
+        if self.kind == "gpu":
+            out = C.c_uint64(0)
+            self._check(self.lib.gdl_relation_dump_tsv(self.h, rel.id, version, path.encode(),
+                                                       C.byref(out)))
+            return int(out.value)
+        rows = self.export(rel, version)
+        write_tsv(path, rows)
+        return len(rows)
 
     def size(self, rel: Relation, version: int = FULL) -> int:
         out = C.c_uint64(0)

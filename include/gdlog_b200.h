@@ -165,6 +165,35 @@ gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t version,
 gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t version,
                                uint64_t *out_digest);
 
+/* Input and output files.
+ *
+ * gdl_read_tsv replaces the drivers' get_row_size + get_relation_from_file
+ * (test/tc.cu:17-57) with the same reading rules: the row count is the
+ * number of '\n' characters in the file (a last line without one is not
+ * read), each value is a signed decimal integer read after any white space
+ * (fscanf "%lld"), and after every column but the last exactly one
+ * character (the separator) is consumed.  Values are stored as uint64_t
+ * (a negative value wraps, as the reference's stores do).  Host only: no
+ * engine and no GPU needed.  Writes at most cap_rows rows of `arity`
+ * columns to host_rows and the file's row count to *out_rows; with too
+ * small a cap_rows (or host_rows NULL) it returns GDL_E_CAPACITY after
+ * setting *out_rows, so a first call can size the buffer.  GDL_E_INVALID
+ * if the file cannot be read or runs out of values. */
+gdl_status gdl_read_tsv(const char *path, int32_t arity, uint64_t *host_rows, uint64_t cap_rows,
+                        uint64_t *out_rows);
+
+/* gdl_read_tsv + gdl_relation_load: the driver's file read followed by
+ * load_relation (test/tc.cu:101-111). */
+gdl_status gdl_relation_load_tsv(gdl_engine *e, int32_t rel, const char *path);
+
+/* Write one version's tuples, sorted (gdl_relation_export), one row per
+ * line, columns separated by a tab, in decimal: the layout of Souffle's
+ * .output files, for diffs against them (no reference counterpart; the
+ * reference only prints, src/print.cu).  *out_rows (may be NULL) receives
+ * the rows written. */
+gdl_status gdl_relation_dump_tsv(gdl_engine *e, int32_t rel, int32_t version, const char *path,
+                                 uint64_t *out_rows);
+
 /* LIE(grid, block) (include/lie.cuh:11-65, src/lie.cu:13-24). */
 gdl_status gdl_lie_create(gdl_engine *e, int32_t *out_lie);
 /* LIE::add_relations (src/lie.cu:15-22). */
