@@ -871,6 +871,14 @@ constexpr int kFuseBlock = 256;
 constexpr int kFuseCtasPerSm = 6;
 constexpr u32 kHeavyRun = 128;
 constexpr u32 kHeavyPiece = 2048;
+// Row-OR pieces: a run at least as long as its row has words (one reduction
+// per word then replaces one per candidate, and the row is 4 bytes a word
+// instead of 8 per candidate) is ORed from the inner's FULL bitmap in
+// pieces of kRowPiece words.  A row piece's record: crow_key = first output
+// word, crow_off = first inner word, crow_start = 0, crow_len = kRowFlag |
+// words.
+constexpr u32 kRowPiece = 256;
+constexpr u32 kRowFlag = 0x80000000u;
 
 struct FuseSmem {
   u64 row[kFuseBlock / 32][32];
@@ -908,13 +916,37 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
       l = index_probe(ix, key_c0(row), &s);
     }
     if (l > kHeavyRun) {
-      const u32 np = (l + kHeavyPiece - 1) / kHeavyPiece;
+      // output row x (from the outer row) and inner row z (the join key)
+      u64 xw = 0, zw = 0;
+      u32 rw = 0;
+      if (a.row_or) {
+        // ids of instance i are (i << seg_shift) | local; the square
+        // domain is one instance of every id
+        const bool square = map.seg_shift >= 31;
+        const u32 x = pick4(a.sel.s0, 0, row), z = key_c0(row);
+        const u32 xi = square ? 0u : x >> map.seg_shift, zi = square ? 0u : z >> map.seg_shift;
+        const u32 base = square ? 0u : xi << map.seg_shift;
+        u32 bx, bz;
+        if (xi == zi && dm_locate(map, make_key(x, base), &xw, &bx) &&
+            dm_locate(map, make_key(z, base), &zw, &bz)) {
+          rw = 1u << map.seg[xi].row_shift;
+          if (l < rw) rw = 0;  // shorter than its row: expand it
+        }
+      }
+      const u32 np = rw ? (rw + kRowPiece - 1) / kRowPiece : (l + kHeavyPiece - 1) / kHeavyPiece;
       const u64 pos = atomicAdd(reinterpret_cast<unsigned long long *>(&a.op->nc), (u64)np);
       if (pos + np <= a.crow_cap) {
         for (u32 k = 0; k < np; k++) {
-          a.crow_key[pos + k] = row;
-          a.crow_start[pos + k] = s + k * kHeavyPiece;
-          a.crow_len[pos + k] = min(kHeavyPiece, l - k * kHeavyPiece);
+          if (rw) {
+            a.crow_key[pos + k] = xw + (u64)k * kRowPiece;
+            a.crow_off[pos + k] = zw + (u64)k * kRowPiece;
+            a.crow_start[pos + k] = 0;
+            a.crow_len[pos + k] = kRowFlag | min(kRowPiece, rw - k * kRowPiece);
+          } else {
+            a.crow_key[pos + k] = row;
+            a.crow_start[pos + k] = s + k * kHeavyPiece;
+            a.crow_len[pos + k] = min(kHeavyPiece, l - k * kHeavyPiece);
+          }
         }
         l = 0;
       }  // else: no room, the warp expands the run itself
@@ -975,9 +1007,25 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
   u8 *D = out_rd->dirty;
   const u64 *inner = a.inner->ptr;
   u64 cand = 0;
+  const u32 *F = a.row_or ? a.inner_rd->bmF : nullptr;
+  u64 row_bytes = 0;
   for (u64 k = blockIdx.x; k < np; k += gridDim.x) {
     const u64 row = a.crow_key[k];
     const u32 s = a.crow_start[k], l = a.crow_len[k];
+    if (l & kRowFlag) {
+      // a row piece: OR the inner row's words into the output row
+      const u32 nw = l & ~kRowFlag;
+      const u64 zw = a.crow_off[k];
+      for (u32 j = threadIdx.x; j < nw; j += blockDim.x) {
+        const u32 v = F[zw + j];
+        if (v) {
+          asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + row + j), "r"(v) : "memory");
+          if (D) D[(row + j) / kBmChunkWords] = 1;
+        }
+      }
+      row_bytes += 8 * (u64)nw;  // a word read and a word reduced
+      continue;
+    }
     for (u32 j0 = 0; j0 < l; j0 += blockDim.x) {  // rounds uniform over the block
       const u32 j = j0 + threadIdx.x;
       u64 w = ~0ull;
@@ -995,7 +1043,7 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
     }
     cand += l;
   }
-  if (threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, cand * 12);
+  if (threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, cand * 12 + row_bytes);
   if (launch_rec_finish(a.rec) && threadIdx.x == 0) {
     a.op->nc = 0;
     prof_add(a.ctl, kPJoinMat, np * 24);

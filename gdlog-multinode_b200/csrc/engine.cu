@@ -171,6 +171,7 @@ struct gdl_engine {
   int dirty_min_log2_words = 24;
   int dense_join_passes = 1;
   int join_aggregate = 1;  // 1: one reduction per candidate, 2: warp-aggregated by word
+  bool row_or_joins = true;  // GDLOG_ROW_OR=0 turns row-OR joins off
   // Device memory in bytes, read once at creation: cudaMemGetInfo can take
   // tens of milliseconds on a busy host, so the fixpoint sizes its lists
   // from this and asks for free memory only after an allocation failed.
@@ -737,6 +738,12 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       a.ctl = e->d_ctl;
       a.out_rel = op.out;
       a.dense = dense;
+      // Row-OR: inner FULL kept as a bitmap, output (outer column, inner
+      // column 1), no predicate (dense.cuh, k_join_bm).
+      a.inner_rd = &R[op.inner];
+      a.row_or = dense && e->row_or_joins && op.inner_ver != GDL_DELTA &&
+                 e->h[op.inner].dense && e->h[op.inner].bmF && op.pred.kind == 0 &&
+                 (op.sel.s0 == 2 || op.sel.s0 == 3) && op.sel.s1 == 1;
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
       JoinArgs b = a;
@@ -1540,6 +1547,7 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
     if (!strcmp(m, "sort")) e->dedup_mode = 1;
     if (!strcmp(m, "dense")) e->dedup_mode = 2;
   }
+  if (const char *ro = getenv("GDLOG_ROW_OR")) e->row_or_joins = strcmp(ro, "0") != 0;
   if (const char *b = getenv("GDLOG_DENSE_MAX_BITS"))
     e->dense_max_bits = std::min(atoi(b), kDenseMaxDomainBits);
   cudaMemPool_t pool;

@@ -67,6 +67,11 @@ struct JoinArgs {
   int dense;
   u32 *outer_bm;
   u64 outer_bm_words;
+  // Row-OR joins (dense.cuh, k_join_bm): the inner is a FULL kept as a
+  // bitmap (inner_rd->bmF) and the output is (an outer column, inner
+  // column 1), so a long run is its bitmap row, ORed into the output row.
+  const RelDev *inner_rd;
+  int row_or;
 };
 
 __device__ __forceinline__ u64 eff_count(const DArr *a, const u32 *vis) {

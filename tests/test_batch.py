@@ -146,3 +146,16 @@ def test_shard_instances_agree_across_gloo_ranks():
     assert sorted(parts[0] + parts[1]) == list(range(40))
     assert not set(parts[0]) & set(parts[1])
     assert parts == [B.shard_instances(costs, 2, r) for r in range(2)]
+
+
+@pytest.mark.gpu
+def test_batched_cspa_long_runs_match_oracle():
+    """CSPA instances large enough for runs longer than a bitmap row, so the
+    joins OR whole rows of the inner's FULL bitmap in the block-diagonal
+    layout; every instance still matches the oracle."""
+    inst = [W.cspa_facts(v, 2 * v, 3 * v // 4, seed=40 + v) for v in (260, 300, 200)]
+    with Engine("gpu") as g:
+        batched = B.run_batched(g, P.cspa, inst)
+    with Engine("oracle") as o:
+        oracle = B.run_plain_loop(o, P.cspa, inst)
+    assert as_tuples(batched) == as_tuples(oracle)

@@ -100,5 +100,6 @@ def test_load_from_file_and_dump_sorted(tmp_path):
     with Engine("oracle") as o:
         ro = P.sg(o, read_tsv(str(f)))
         o.dump_tsv(ro.output, str(tmp_path / "sg_oracle.tsv"))
-    assert n == ro.output.size()
+        n_oracle = ro.output.size()
+    assert n == n_oracle
     assert (tmp_path / "sg.tsv").read_text() == (tmp_path / "sg_oracle.tsv").read_text()
