@@ -170,6 +170,56 @@ __device__ __forceinline__ u64 gen_join(Sel2 g, u64 inner, u64 outer) {
   return make_key(pick4(g.s0, inner, outer), pick4(g.s1, inner, outer));
 }
 
+// Arity 3 (a third, dependent column such as a path length; the reference's
+// test/path_length.cu).  A tuple (c0, c1, c2) is the key
+// c0 << 32 | c1 << k2 | c2: column 0 keeps the high half, so index builds
+// and join probes read it as for arity 2, and keys still sort in the
+// lexicographic order of the tuples (include/tuple.cuh:106-126) when
+// c1 < 2^(32-k2) and c2 < 2^k2.
+__host__ __device__ __forceinline__ u32 key_col(u64 k, int arity, int j, int k2) {
+  if (j == 0) return (u32)(k >> 32);
+  const u32 lo = (u32)k;
+  if (arity == 2) return lo;
+  return j == 1 ? (lo >> k2) : (lo & ((1u << k2) - 1u));
+}
+
+// General tuple generator: output column j is column src[j] of the inner /
+// source tuple (0..2) or of the outer tuple (16..18), plus add[j] (hooks
+// such as path_length's outer[2] + 1, recognised as a column plus a
+// constant).
+struct GenSpec {
+  int src[3];
+  u32 add[3];
+  int out_arity, in_arity, outer_arity;
+  int k2;  // bits of column 2 in arity-3 keys
+};
+
+// The key of the generated tuple; a value that does not fit its column
+// sets Ctl::oob bit 32768 (the fixpoint then fails) and yields key 0.
+__device__ __forceinline__ u64 gen_spec(const GenSpec &g, u64 inner, u64 outer, u32 *oob) {
+  u64 v[3] = {0, 0, 0};
+  for (int j = 0; j < g.out_arity; j++) {
+    const int s = g.src[j];
+    const u64 x = s < 16 ? key_col(inner, g.in_arity, s, g.k2)
+                         : key_col(outer, g.outer_arity, s - 16, g.k2);
+    v[j] = x + g.add[j];
+  }
+  bool fits;
+  u64 k;
+  if (g.out_arity == 2) {
+    fits = ((v[0] | v[1]) >> 32) == 0;
+    k = (v[0] << 32) | v[1];
+  } else {
+    fits = (v[0] >> 32) == 0 && (v[1] >> (32 - g.k2)) == 0 && (v[2] >> g.k2) == 0;
+    k = (v[0] << 32) | (v[1] << g.k2) | v[2];
+  }
+  if (!fits) {
+    atomicOr(oob, 32768u);
+    return 0;
+  }
+  return k;
+}
+
 // Predicate on the generated tuple (tuple_predicate): t[a] op t[b].
 struct Pred {
   int kind, a, b;

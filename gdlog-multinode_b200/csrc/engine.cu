@@ -83,6 +83,8 @@ struct OpHost {
   int inner = -1, inner_ver = GDL_FULL, outer = -1, outer_ver = GDL_DELTA, out = -1;
   Sel2 sel{0, 1};
   Pred pred{0, 0, 0};
+  bool generic = false;  // arity 3 or a computed column: tuples from gen
+  GenSpec gen{};
 };
 
 struct LieHost {
@@ -144,6 +146,11 @@ struct gdl_engine {
   Ctl *d_ctl = nullptr;
   Ctl *h_ctl = nullptr;  // pinned
   int kbits = 1;         // bits of the largest column value loaded
+  // Arity 3 (common.cuh, key_col): once a relation of arity 3 exists every
+  // sort covers the whole low half of the keys; k2 = bits of column 2, fixed
+  // by the first arity-3 load (32 - bits of the ids loaded until then).
+  bool wide = false;
+  int k2 = 0;
   u64 max_value = 0;
   std::vector<LieHost> lies;
   // scratch
@@ -308,7 +315,18 @@ int grid_for(gdl_engine *e, u64 work, u64 per_block, int per_sm) {
   return (int)g;
 }
 
-int sort_passes(const gdl_engine *e) { return std::max(1, (2 * e->kbits + 7) / 8); }
+// Sorts radix the significant bits only: column 0's kbits and the low half's
+// kbits (arity 2) or all 32 (once arity-3 keys exist).
+int sort_lo_bits(const gdl_engine *e) { return e->wide ? 32 : e->kbits; }
+int sort_passes(const gdl_engine *e) { return std::max(1, (e->kbits + sort_lo_bits(e) + 7) / 8); }
+
+// The key bits of a relation's dependent columns (cleared to compare the
+// set difference's prefix, merge.cuh k_dep_mask); 0 without any.
+u64 dep_low_mask(const gdl_engine *e, const RelHost &h) {
+  if (h.dep == 0) return 0;
+  if (h.arity == 3 && h.dep == 1) return (1ull << e->k2) - 1;
+  return 0xFFFFFFFFull;  // columns 1.. of the low half
+}
 
 cudaEvent_t take_event(gdl_engine *e) {
   cudaEvent_t ev = nullptr;
@@ -495,7 +513,7 @@ void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *
   a.buf0 = buf0;
   a.buf1 = e->sort_buf;
   a.cap = std::min(cap, e->sort_cap);
-  a.kbits = e->kbits;
+  a.kbits = sort_lo_bits(e);
   a.passes = sort_passes(e);
   a.offsets = e->sort_offsets;
   a.status = e->sort_status;
@@ -725,6 +743,9 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       }
       a.out_newt = &R[op.out].newt;
       a.sel = op.sel;
+      a.generic = op.generic;
+      a.gen = op.gen;
+      a.gen.k2 = e->k2;
       a.pred = op.pred;
       a.op = L.d_joinrec + oi;
       a.rec = &e->recs[0];
@@ -792,6 +813,9 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       }
       c.dest = &R[op.out].newt;
       c.sel = op.sel;
+      c.generic = op.generic;
+      c.gen = op.gen;
+      c.gen.k2 = e->k2;
       bool once = op.kind == 1 && op.inner_ver == GDL_FULL;
       c.once = once ? &L.d_lie->once[oi] : nullptr;
       c.once_pending = once ? &L.d_lie->once_pending[oi] : nullptr;
@@ -885,6 +909,9 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       m.ctl = e->d_ctl;
       m.rel = r;
       u64 mcap = std::max(rh.full.cap, rh.full_next.cap) + rh.newt.cap;
+      if (const u64 lm = dep_low_mask(e, e->rels[r]))
+        PLAUNCH(kc, kPMerge, k_dep_mask<<<grid_for(e, rh.newt.cap, 256, 8), 256, 0, s>>>(
+                                 const_cast<u64 *>(m.a), &R[r].newt, &R[r].full, lm, e->d_ctl));
       PLAUNCH(kc, kPMerge,
               k_merge_partition<<<grid_for(e, mcap / kMergeTile + 2, 256, 8), 256, 0, s>>>(m));
       PLAUNCH(kc, kPMerge,
@@ -988,13 +1015,13 @@ gdl_status grow_after_overflow(gdl_engine *e, const Ctl &c) {
 
 gdl_status validate_rel(gdl_engine *e, int r) {
   const RelHost &h = e->rels[r];
-  if (h.arity != 2 || h.icols != 1 || h.dep != 0)
+  if ((h.arity != 2 && h.arity != 3) || h.icols != 1 || h.dep >= h.arity)
     return fail(e, GDL_E_UNSUPPORTED,
-                "relation %s: only arity 2, index_column_size 1, dependent_column_size 0 "
-                "are supported",
+                "relation %s: only arity 2 or 3 with index_column_size 1 is supported",
                 h.name.c_str());
   return GDL_OK;
 }
+
 
 gdl_status build_index_now(gdl_engine *e, int r, bool delta) {
   RelDev &h = e->h[r];
@@ -1046,6 +1073,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   for (int r : L.update) TRY(validate_rel(e, r));
   for (int r : L.statics) TRY(validate_rel(e, r));
   for (int r : L.tmps) TRY(validate_rel(e, r));
+  if (e->wide && !e->k2) e->k2 = 32 - std::max(bits_for(e->max_value), 1);
   for (const OpHost &op : L.ops) {
     TRY(validate_rel(e, op.inner));
     if (op.outer >= 0) TRY(validate_rel(e, op.outer));
@@ -1112,7 +1140,12 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
                   e->rels[r].name.c_str());
   {
     const int dk = std::max(e->kbits, 5);
-    L.dense = e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits);
+    // Bitmaps hold arity-2 tuples without dependent columns only.
+    bool plain = !e->wide;
+    for (auto *v : {&L.update, &L.statics, &L.tmps})
+      for (int r : *v) plain = plain && e->rels[r].dep == 0;
+    for (const OpHost &op : L.ops) plain = plain && !op.generic;
+    L.dense = plain && (e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits));
     L.dk = L.dense && !e->instances ? dk : 0;
   }
   for (RelDev &h : e->h) {
@@ -1328,6 +1361,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           const u64 *x = &rows[(t * L.update.size() + i) * 3];
           L.trace.insert(L.trace.end(), {it0 + t, (u64)L.update[i], x[0], x[1], x[2]});
         }
+    }
+    if (c.oob & 32768u) {
+      e->broken = true;
+      return fail(e, GDL_E_UNSUPPORTED,
+                  "iteration %llu generated a value too large for its column (arity-3 keys "
+                  "hold column 1 below 2^%d and column 2 below 2^%d)",
+                  (unsigned long long)c.iteration, 32 - e->k2, e->k2);
     }
     if (c.timeout || c.oob) {
       e->broken = true;
@@ -1664,7 +1704,10 @@ gdl_status gdl_relation_create(gdl_engine *e, const char *name, int32_t arity, i
   if ((int)e->rels.size() >= kMaxRels) return fail(e, GDL_E_UNSUPPORTED, "too many relations");
   if (arity < 1 || icols < 1 || icols > arity || dep < 0 || dep >= arity)
     return fail(e, GDL_E_INVALID, "bad arity/index/dependent column sizes");
-  if (arity != 2) return fail(e, GDL_E_UNSUPPORTED, "arity %d not supported (arity 2 only)", arity);
+  if (arity != 2 && arity != 3)
+    return fail(e, GDL_E_UNSUPPORTED, "arity %d not supported (arity 2 and 3 only)", arity);
+  if (icols != 1) return fail(e, GDL_E_UNSUPPORTED, "index_column_size must be 1");
+  if (arity == 3) e->wide = true;
   cudaSetDevice(e->device);
   RelHost rh;
   rh.name = name ? name : "";
@@ -1705,6 +1748,34 @@ static gdl_status load_common(gdl_engine *e, int32_t rel, const uint64_t *rows, 
   if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
   if (n > kMaxRows) return fail(e, GDL_E_UNSUPPORTED, "too many rows");
   if (n == 0) return load_keys(e, rel, nullptr, 0);
+  if (e->rels[rel].arity == 3) {
+    // arity 3: packed on the host (key_col layout), column 2 width fixed by
+    // the first such load
+    if (on_device) return fail(e, GDL_E_UNSUPPORTED, "arity-3 rows load from host memory");
+    u64 m01 = 0, m2 = 0;
+    for (u64 i = 0; i < n; i++) {
+      m01 = std::max<u64>({m01, (u64)rows[3 * i], (u64)rows[3 * i + 1]});
+      m2 = std::max<u64>(m2, (u64)rows[3 * i + 2]);
+    }
+    if (m01 >> 32) return fail(e, GDL_E_UNSUPPORTED, "column values must be below 2^32");
+    if (!e->k2) e->k2 = 32 - std::max(bits_for(std::max(e->max_value, m01)), 1);
+    if (bits_for(m01) > 32 - e->k2 || (m2 >> e->k2))
+      return fail(e, GDL_E_UNSUPPORTED,
+                  "arity-3 keys hold column 1 below 2^%d and column 2 below 2^%d",
+                  32 - e->k2, e->k2);
+    std::vector<u64> keys(n);
+    for (u64 i = 0; i < n; i++)
+      keys[i] = (rows[3 * i] << 32) | (rows[3 * i + 1] << e->k2) | rows[3 * i + 2];
+    u64 *dk = nullptr;
+    TRY(dalloc(e, (void **)&dk, n * sizeof(u64)));
+    CK(e, cudaMemcpyAsync(dk, keys.data(), n * sizeof(u64), cudaMemcpyHostToDevice, e->s));
+    e->max_value = std::max(e->max_value, m01);
+    e->kbits = std::max(e->kbits, bits_for(e->max_value));
+    gdl_status s = load_keys(e, rel, dk, n);
+    CK(e, cudaStreamSynchronize(e->s));
+    dfree(e, dk);
+    return s;
+  }
   u64 *d_rows = nullptr, *d_keys = nullptr;
   if (on_device) {
     d_rows = (u64 *)rows;
@@ -1726,6 +1797,11 @@ static gdl_status load_common(gdl_engine *e, int32_t rel, const uint64_t *rows, 
   if (badv) {
     dfree(e, d_keys);
     return fail(e, GDL_E_UNSUPPORTED, "column values must be below 2^32");
+  }
+  if (e->k2 && bits_for(maxv) > 32 - e->k2) {
+    dfree(e, d_keys);
+    return fail(e, GDL_E_UNSUPPORTED,
+                "ids must stay below 2^%d once arity-3 relations are loaded", 32 - e->k2);
   }
   e->max_value = std::max(e->max_value, maxv);
   e->kbits = std::max(e->kbits, bits_for(e->max_value));
@@ -1813,10 +1889,9 @@ gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t ver, uint64_t
   *out_n = k.size();
   if (k.size() > cap) return fail(e, GDL_E_CAPACITY, "export needs %zu rows", k.size());
   if (k.size() && !rows) return GDL_E_INVALID;
-  for (size_t i = 0; i < k.size(); i++) {
-    rows[2 * i] = key_c0(k[i]);
-    rows[2 * i + 1] = key_c1(k[i]);
-  }
+  const int ar = e->rels[rel].arity;
+  for (size_t i = 0; i < k.size(); i++)
+    for (int j = 0; j < ar; j++) rows[ar * i + j] = key_col(k[i], ar, j, e->k2);
   return GDL_OK;
 }
 
@@ -1902,10 +1977,13 @@ gdl_status gdl_relation_dump_tsv(gdl_engine *e, int32_t rel, int32_t ver, const 
   std::string out;
   out.reserve(k.size() * 16);
   char line[48];
+  const int ar = e->rels[rel].arity;
   for (u64 key : k) {
-    const int m = snprintf(line, sizeof line, "%llu\t%llu\n", (unsigned long long)key_c0(key),
-                           (unsigned long long)key_c1(key));
-    out.append(line, (size_t)m);
+    for (int j = 0; j < ar; j++) {
+      const int m = snprintf(line, sizeof line, j + 1 < ar ? "%u\t" : "%u\n",
+                             key_col(key, ar, j, e->k2));
+      out.append(line, (size_t)m);
+    }
   }
   const bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
   fclose(f);
@@ -1922,13 +2000,13 @@ gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t ver, uint64_t
   bool sorted;
   TRY(version_view(e, rel, ver, &p, &n, &sorted));
   u64 acc = 0;
-  if (!sorted) {
+  const int ar = e->rels[rel].arity;
+  if (!sorted || ar != 2) {
     std::vector<u64> k;
     TRY(host_rows(e, rel, ver, k));
     for (size_t i = 0; i < k.size(); i++) {
       u64 h = mix64(i);
-      h = mix64(h ^ (u64)key_c0(k[i]));
-      h = mix64(h ^ (u64)key_c1(k[i]));
+      for (int j = 0; j < ar; j++) h = mix64(h ^ (u64)key_col(k[i], ar, j, e->k2));
       acc += h;
     }
     *out = mix64(acc ^ (u64)k.size());
@@ -1973,6 +2051,34 @@ gdl_status gdl_lie_add_tmp_relation(gdl_engine *e, int32_t lie, int32_t rel) {
   return GDL_OK;
 }
 
+// A hook given as gen entries GDL_INNER(c) / GDL_OUTER(c) / GDL_SRC(c), each
+// possibly GDL_PLUS(entry, k): column moves only, between arity-2
+// relations, become a Sel2; anything else (arity 3, a constant added) a
+// GenSpec the kernels evaluate per tuple.
+static gdl_status decode_gen(gdl_engine *e, const int32_t *gen, int32_t len, bool join, int a_in,
+                             int a_outer, int a_out, OpHost *op) {
+  if (!gen || len != a_out)
+    return fail(e, GDL_E_INVALID, "gen must have one entry per output column (%d)", a_out);
+  bool plain = a_in == 2 && a_out == 2 && (!join || a_outer == 2);
+  for (int j = 0; j < len; j++) {
+    const int g = gen[j] & 0xFF;
+    const u32 add = (u32)gen[j] >> 8;
+    const bool in_ok = g >= 0 && g < a_in;
+    const bool out_ok = join && g >= 16 && g - 16 < a_outer;
+    if (!in_ok && !out_ok) return fail(e, GDL_E_INVALID, "gen entry %d out of range", gen[j]);
+    op->gen.src[j] = g;
+    op->gen.add[j] = add;
+    plain = plain && add == 0;
+  }
+  op->gen.out_arity = a_out;
+  op->gen.in_arity = a_in;
+  op->gen.outer_arity = join ? a_outer : 0;
+  op->generic = !plain;
+  if (plain) return GDL_OK;
+  for (int j = len; j < 3; j++) op->gen.src[j] = 0, op->gen.add[j] = 0;
+  return GDL_OK;
+}
+
 static gdl_status decode_sel(gdl_engine *e, const int32_t *gen, int32_t len, bool join, Sel2 *s) {
   if (!gen || len != 2) return fail(e, GDL_E_INVALID, "gen must have 2 entries (arity 2)");
   int v[2];
@@ -2011,7 +2117,11 @@ gdl_status gdl_lie_add_join(gdl_engine *e, int32_t lie, int32_t inner, int32_t i
   op.outer = outer;
   op.outer_ver = outer_ver;
   op.out = output;
-  TRY(decode_sel(e, gen, gen_len, true, &op.sel));
+  TRY(decode_gen(e, gen, gen_len, true, e->rels[inner].arity, e->rels[outer].arity,
+                 e->rels[output].arity, &op));
+  if (!op.generic) TRY(decode_sel(e, gen, gen_len, true, &op.sel));
+  if (op.generic && pred_kind)
+    return fail(e, GDL_E_UNSUPPORTED, "predicates with arity 3 or computed columns");
   op.pred = Pred{pred_kind, pa, pb};
   e->lies[lie].ops.push_back(op);
   e->lies[lie].graph_dirty = true;
@@ -2031,7 +2141,8 @@ gdl_status gdl_lie_add_copy(gdl_engine *e, int32_t lie, int32_t src, int32_t src
   op.inner = src;
   op.inner_ver = src_ver;
   op.out = dest;
-  TRY(decode_sel(e, gen, gen_len, false, &op.sel));
+  TRY(decode_gen(e, gen, gen_len, false, e->rels[src].arity, 0, e->rels[dest].arity, &op));
+  if (!op.generic) TRY(decode_sel(e, gen, gen_len, false, &op.sel));
   e->lies[lie].ops.push_back(op);
   e->lies[lie].graph_dirty = true;
   return GDL_OK;
@@ -2048,7 +2159,8 @@ gdl_status gdl_lie_add_acopy(gdl_engine *e, int32_t lie, int32_t src, int32_t de
   op.inner = src;
   op.inner_ver = GDL_NEWT;
   op.out = dest;
-  TRY(decode_sel(e, gen, gen_len, false, &op.sel));
+  TRY(decode_gen(e, gen, gen_len, false, e->rels[src].arity, 0, e->rels[dest].arity, &op));
+  if (!op.generic) TRY(decode_sel(e, gen, gen_len, false, &op.sel));
   e->lies[lie].ops.push_back(op);
   e->lies[lie].graph_dirty = true;
   return GDL_OK;

@@ -72,7 +72,14 @@ struct JoinArgs {
   // column 1), so a long run is its bitmap row, ORed into the output row.
   const RelDev *inner_rd;
   int row_or;
+  // arity 3 or computed columns: tuples come from gen (list form only)
+  int generic;
+  GenSpec gen;
 };
+
+__device__ __forceinline__ u64 join_out(const JoinArgs &a, u64 inner, u64 outer) {
+  return a.generic ? gen_spec(a.gen, inner, outer, &a.ctl->oob) : gen_join(a.sel, inner, outer);
+}
 
 __device__ __forceinline__ u64 eff_count(const DArr *a, const u32 *vis) {
   return (vis && *vis == 0) ? 0 : a->n;
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(kJoinBlock) k_join_count(JoinArgs a) {
           cnt[k] = l;
         } else {
           u64 c = 0;
-          for (u32 j = 0; j < l; j++) c += pred_ok(a.pred, gen_join(a.sel, inner[s + j], row));
+          for (u32 j = 0; j < l; j++) c += pred_ok(a.pred, join_out(a, inner[s + j], row));
           cnt[k] = c;
         }
         my_cnt += cnt[k];
@@ -299,11 +306,11 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat(JoinArgs a) {
         const u64 p = p0 + 2 * q;
         if (p >= p1) break;
         u32 r = find_rec(sm.off, m, p);
-        u64 o0 = gen_join(a.sel, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
+        u64 o0 = join_out(a, inner[sm.start[r] + (p - sm.off[r])], sm.key[r]);
         u64 o1 = o0;
         if (p + 1 < total) {
           if (p + 1 >= sm.off[r + 1]) r++;
-          o1 = gen_join(a.sel, inner[sm.start[r] + (p + 1 - sm.off[r])], sm.key[r]);
+          o1 = join_out(a, inner[sm.start[r] + (p + 1 - sm.off[r])], sm.key[r]);
         }
         if (p + 1 < cap_left)
           reinterpret_cast<ulonglong2 *>(out)[p >> 1] = make_ulonglong2(o0, o1);
@@ -346,7 +353,7 @@ __global__ void __launch_bounds__(kMatBlock) k_join_mat_pred(JoinArgs a) {
       u64 t = 0;
       bool ok = false;
       if (j < l) {
-        t = gen_join(a.sel, inner[s + j], row);
+        t = join_out(a, inner[s + j], row);
         ok = pred_ok(a.pred, t);
       }
       unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -386,7 +393,13 @@ struct CopyArgs {
   Ctl *ctl;
   int dest_rel;
   int replace;  // ACopy: dest := sel(src) instead of appending
+  int generic;  // arity 3 or computed columns: tuples come from gen
+  GenSpec gen;
 };
+
+__device__ __forceinline__ u64 copy_out(const CopyArgs &c, u64 src) {
+  return c.generic ? gen_spec(c.gen, src, 0, &c.ctl->oob) : gen_join(c.sel, src, 0);
+}
 
 __global__ void __launch_bounds__(kMatBlock) k_copy(CopyArgs c) {
   if (ctl_stop(c.ctl)) return;
@@ -415,8 +428,8 @@ __global__ void __launch_bounds__(kMatBlock) k_copy(CopyArgs c) {
   for (u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x; q < pairs;
        q += (u64)gridDim.x * blockDim.x) {
     const u64 p = 2 * q;
-    u64 o0 = gen_join(c.sel, src[p], 0);
-    u64 o1 = p + 1 < n ? gen_join(c.sel, src[p + 1], 0) : o0;
+    u64 o0 = copy_out(c, src[p]);
+    u64 o1 = p + 1 < n ? copy_out(c, src[p + 1]) : o0;
     reinterpret_cast<ulonglong2 *>(out)[q] = make_ulonglong2(o0, o1);
   }
   if (launch_rec_finish(c.rec) && threadIdx.x == 0) {

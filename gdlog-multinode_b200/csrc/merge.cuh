@@ -53,6 +53,33 @@ __device__ __forceinline__ u64 merge_path(const u64 *A, u64 na, const u64 *B, u6
   return lo;
 }
 
+// Dependent columns (Relation::dependent_column_size): the set difference
+// NEWT \ FULL of the update step compares only the first arity - dep
+// columns (src/lie.cu:131-138), while unique and merge compare whole
+// tuples.  Before the merge, every sorted NEWT key whose prefix (the key
+// with its dependent bits, low_mask, cleared) is already in FULL is replaced
+// by the first FULL key with that prefix.  NEWT stays sorted, the merge sees
+// those keys tie with FULL (not new, nothing added), and DELTA and FULL'
+// come out as set_difference then merge give them.
+__global__ void k_dep_mask(u64 *a, const DArr *newt, const DArr *full, u64 low_mask, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u64 na = newt->n, nb = full->n;
+  const u64 *B = full->ptr;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < na;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 p = a[i] & ~low_mask;
+    u64 lo = 0, hi = nb;  // first FULL key >= p
+    while (lo < hi) {
+      const u64 mid = (lo + hi) >> 1;
+      if (B[mid] < p)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < nb && (B[lo] & ~low_mask) == p) a[i] = B[lo];
+  }
+}
+
 __device__ __forceinline__ bool merge_fits(const MergeArgs &m, u64 na, u64 nb) {
   return na + nb <= m.full_next->cap && na <= m.delta_next->cap;
 }

@@ -48,6 +48,11 @@ def SRC(c: int) -> int:
     return c
 
 
+def PLUS(sel: int, k: int) -> int:
+    """GDL_PLUS: a hook column plus a constant, e.g. PLUS(OUTER(2), 1)."""
+    return sel | (k << 8)
+
+
 class Tuning(C.Structure):
     """gdl_tuning (include/gdlog_b200.h); a zero field keeps the default."""
     _fields_ = [("dedup", C.c_int32), ("dense_max_bits", C.c_int32),

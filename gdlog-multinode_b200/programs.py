@@ -10,6 +10,9 @@ order, as the reference's hand-compiled driver, and runs them on an Engine
                                    relation)
 * ``cspa`` – test/cspa.cu:100-379 (init SCC of 7 copies + analysis SCC of
                                    11 joins and 2 ACopies, 3 tmp relations)
+* ``path_length`` – test/path_length.cu:59-140 (path(a, y, l + 1) :-
+                                   edge(a, x), path(x, y, l); arity 3 with a
+                                   dependent length column)
 
 The hooks of the drivers are pure column selections; they are written here
 in the C-ABI encoding (INNER(c) / OUTER(c) / SRC(c)):
@@ -21,6 +24,8 @@ in the C-ABI encoding (INNER(c) / OUTER(c) / SRC(c)):
   cp_2_1__1            (src[0], src[0])       test/cspa.cu:62-65
   cp_2_1__2            (src[1], src[1])       test/cspa.cu:67-70
   tuple_pred_eq_11     t[0] != t[1]           test/sg.cu:88
+and path_length's computing hook in the PLUS encoding:
+  reorder_path  newt = (inner[1], outer[1], outer[2] + 1)   test/path_length.cu:52-57
 """
 from __future__ import annotations
 
@@ -30,7 +35,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from gdlog_b200 import (DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, SRC, Engine,
-                        Relation)
+                        Relation, PLUS)
 from workloads import reverse
 
 REORDER_PATH = (INNER(1), OUTER(1))
@@ -193,4 +198,33 @@ def cspa(eng: Engine, assign: np.ndarray, deref: np.ndarray, sync=None) -> Resul
     r.relations.update(value_flow=vf12, memory_alias=ma12, value_alias=va12)
     r.iterations.update(init=it0, analysis=it1)
     r.lies.update(init=init, analysis=lie)
+    return r
+
+
+def path_length(eng: Engine, edges: np.ndarray, sync=None) -> Result:
+    """test/path_length.cu:59-140: path(x, y, 1) for every edge, then
+    path(a, y, l + 1) :- edge(a, x), path(x, y, l), where a (x, y) pair is
+    new only if no path(x, y, _) exists yet (dependent_column_size 1), so
+    the lengths are the shortest in edges."""
+    e = np.asarray(edges, dtype=np.uint64)
+    rows = np.concatenate([e, np.ones((len(e), 1), dtype=np.uint64)], axis=1) if len(e) else \
+        np.zeros((0, 3), dtype=np.uint64)
+    edge_2__2_1 = eng.relation("edge_2__2_1")
+    path_3__1_2_3 = eng.relation("path_3__1_2_3", arity=3, dependent_column_size=1,
+                                 index_flag=False)
+    eng.load(path_3__1_2_3, rows)
+    eng.load(edge_2__2_1, reverse(e))
+    t0 = time.perf_counter()
+    lie = eng.lie()
+    lie.add_relations(edge_2__2_1, True)
+    lie.add_relations(path_3__1_2_3, False)
+    lie.add_join(edge_2__2_1, FULL, path_3__1_2_3, DELTA, path_3__1_2_3,
+                 (INNER(1), OUTER(1), PLUS(OUTER(2), 1)))
+    it = lie.fixpoint()
+    if sync:
+        sync()
+    r = Result(seconds=time.perf_counter() - t0)
+    r.relations["path"] = path_3__1_2_3
+    r.iterations["plen"] = it
+    r.lies["plen"] = lie
     return r

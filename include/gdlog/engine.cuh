@@ -56,19 +56,26 @@ inline gdl_engine *engine() {
 // ---------------------------------------------------------------------------
 // Hook probes.  A hook that only moves columns is recognised by running it
 // on two sets of distinct sentinel values: output column j is input column
-// k exactly when it shows the k-th sentinel of both sets.
+// k exactly when it shows the k-th sentinel of both sets.  A join hook may
+// also add a constant to a column (path_length's outer[2] + 1): output j is
+// input k plus c when it shows sentinel k + c in both sets.
 // ---------------------------------------------------------------------------
 constexpr column_type kProbeA[4] = {1000003ul, 2000029ul, 3000017ul, 4000037ul};
 constexpr column_type kProbeB[4] = {5000011ul, 6000007ul, 7000003ul, 8000009ul};
 constexpr column_type kUnset = 0xFFFFFFFFFFFFFFFFul;
 
 __global__ void probe_generator(tuple_generator_hook h, column_type *buf) {
-  // buf: [0..1] inner, [2..3] outer, [4..5] out  (set A), [6..11] set B
+  // buf: [0..2] inner, [3..5] outer, [6..8] out (set A), [9..17] set B
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    h(buf + 0, buf + 2, buf + 4);
-    h(buf + 6, buf + 8, buf + 10);
+    h(buf + 0, buf + 3, buf + 6);
+    h(buf + 9, buf + 12, buf + 15);
   }
 }
+
+constexpr column_type kProbe3A[6] = {1000003ul, 2000029ul, 3000017ul,
+                                     4000037ul, 5000011ul, 6000007ul};
+constexpr column_type kProbe3B[6] = {7000003ul, 8000009ul, 9000011ul,
+                                     10000019ul, 11000027ul, 12000017ul};
 
 __global__ void probe_copy(tuple_copy_hook h, column_type *buf) {
   // buf: [0..1] src, [2..3] dst (set A), [4..5] src, [6..7] dst (set B)
@@ -83,11 +90,16 @@ __global__ void probe_predicate(tuple_predicate p, const column_type *rows, int 
     for (int i = 0; i < n; i++) out[i] = p(const_cast<column_type *>(rows) + 2 * i) ? 1 : 0;
 }
 
-// Returns false when the hook computes values instead of moving columns.
-inline bool decode_generator(tuple_generator_hook h, int32_t gen[2]) {
-  column_type host[12];
-  for (int i = 0; i < 4; i++) host[i] = kProbeA[i], host[6 + i] = kProbeB[i];
-  host[4] = host[5] = host[10] = host[11] = kUnset;
+// gen[0..out_arity) for a join hook over tuples of in_arity (inner) and
+// outer_arity columns.  Returns false when the hook computes anything but a
+// column, or a column plus a small constant.
+inline bool decode_generator(tuple_generator_hook h, int in_arity, int outer_arity, int out_arity,
+                             int32_t *gen) {
+  column_type host[18];
+  for (int i = 0; i < 3; i++) {
+    host[i] = kProbe3A[i], host[3 + i] = kProbe3A[3 + i], host[6 + i] = kUnset;
+    host[9 + i] = kProbe3B[i], host[12 + i] = kProbe3B[3 + i], host[15 + i] = kUnset;
+  }
   column_type *d = nullptr;
   if (cudaMalloc(&d, sizeof host) != cudaSuccess) return false;
   cudaMemcpy(d, host, sizeof host, cudaMemcpyHostToDevice);
@@ -95,11 +107,16 @@ inline bool decode_generator(tuple_generator_hook h, int32_t gen[2]) {
   cudaError_t r = cudaMemcpy(host, d, sizeof host, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (r != cudaSuccess) return false;
-  for (int j = 0; j < 2; j++) {
+  for (int j = 0; j < out_arity; j++) {
     gen[j] = -1;
-    for (int k = 0; k < 4; k++)
-      if (host[4 + j] == kProbeA[k] && host[10 + j] == kProbeB[k])
-        gen[j] = k < 2 ? GDL_INNER(k) : GDL_OUTER(k - 2);
+    for (int k = 0; k < 6; k++) {
+      if ((k < 3 && k >= in_arity) || (k >= 3 && k - 3 >= outer_arity)) continue;
+      const column_type a = host[6 + j], b = host[15 + j];
+      if (a < kProbe3A[k] || b < kProbe3B[k]) continue;
+      const column_type c = a - kProbe3A[k];
+      if (c != b - kProbe3B[k] || c >= 500000ul) continue;
+      gen[j] = GDL_PLUS(k < 3 ? GDL_INNER(k) : GDL_OUTER(k - 3), (int32_t)c);
+    }
     if (gen[j] < 0) return false;
   }
   return true;

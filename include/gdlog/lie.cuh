@@ -75,14 +75,17 @@ struct LIE {
  private:
   static void add_op(gdl_engine *e, int32_t lie, RelationalJoin &j) {
     using namespace gdlog_compat;
-    int32_t gen[2];
-    if (!j.tuple_generator || !decode_generator(j.tuple_generator, gen))
-      check(GDL_E_UNSUPPORTED, "RelationalJoin: the generator hook must move columns only");
+    int32_t gen[3];
+    const int out_arity = j.output_rel->arity;
+    if (!j.tuple_generator ||
+        !decode_generator(j.tuple_generator, j.inner_rel->arity, j.outer_rel->arity, out_arity, gen))
+      check(GDL_E_UNSUPPORTED,
+            "RelationalJoin: the generator hook must move columns (plus constants) only");
     int32_t kind = GDL_PRED_NONE;
     if (j.tuple_pred && !decode_predicate(j.tuple_pred, &kind))
       check(GDL_E_UNSUPPORTED, "RelationalJoin: the predicate must compare t[0] with t[1]");
     check(gdl_lie_add_join(e, lie, j.inner_rel->id, (int32_t)j.inner_ver, j.outer_rel->id,
-                           (int32_t)j.outer_ver, j.output_rel->id, gen, 2, kind, 0, 1),
+                           (int32_t)j.outer_ver, j.output_rel->id, gen, out_arity, kind, 0, 1),
           "gdl_lie_add_join");
   }
   static void add_op(gdl_engine *e, int32_t lie, RelationalCopy &c) {

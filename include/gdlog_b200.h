@@ -19,11 +19,17 @@
  *    function says "device".  The engine stores arity-2 relations packed as
  *    one 64-bit key (c0 << 32 | c1), which is order-preserving for column
  *    values below 2^32; larger values are rejected with GDL_E_UNSUPPORTED.
+ *    Arity 3 (with dependent_column_size 0 or 1, as test/path_length.cu
+ *    uses it) packs c0 << 32 | c1 << k2 | c2, k2 fixed by the first arity-3
+ *    load to 32 minus the bits of the ids loaded so far: ids then stay below
+ *    2^(32-k2) and column 2 below 2^k2.  Relations of arity 3, dependent
+ *    columns and computed hooks run on the sorted-list path.
  *  - Hooks.  The reference passes __device__ function pointers
  *    (tuple_generator_hook / tuple_copy_hook / tuple_predicate,
  *    include/tuple.cuh:23-25).  Across a C-ABI they are described instead
  *    as column selections: gen[j] names the source of output column j,
- *    GDL_INNER(c) or GDL_OUTER(c) for a join, GDL_SRC(c) for a copy.
+ *    GDL_INNER(c) or GDL_OUTER(c) for a join, GDL_SRC(c) for a copy,
+ *    optionally plus a constant (GDL_PLUS).
  *    A predicate compares two columns of the generated tuple.
  *  - One engine owns one CUDA stream; calls on one engine are not
  *    thread-safe.  Device memory is owned by the engine.
@@ -55,6 +61,9 @@ typedef int32_t gdl_status;
 #define GDL_INNER(c) (c)
 #define GDL_OUTER(c) (16 + (c))
 #define GDL_SRC(c) (c)
+/* A hook column plus a constant k (0 <= k < 2^23), e.g. path_length's
+ * outer[2] + 1 (test/path_length.cu:52-57): GDL_PLUS(GDL_OUTER(2), 1). */
+#define GDL_PLUS(sel, k) ((sel) | ((k) << 8))
 
 /* Predicate on the generated tuple t: t[a] <op> t[b]. */
 #define GDL_PRED_NONE 0

@@ -235,12 +235,15 @@ struct Engine final : EngineBase {
   // tuple_generator_hook / tuple_copy_hook restated as a column selection.
   static inline Row gen_join(const std::vector<int32_t> &g, const Row &in, const Row &outr) {
     Row t{};
-    for (size_t j = 0; j < g.size(); j++) t[j] = g[j] < 16 ? in[g[j]] : outr[g[j] - 16];
+    for (size_t j = 0; j < g.size(); j++) {
+      const int s = g[j] & 0xFF;  // GDL_PLUS: constant in bits 8..
+      t[j] = (s < 16 ? in[s] : outr[s - 16]) + (uint64_t)((uint32_t)g[j] >> 8);
+    }
     return t;
   }
   static inline Row gen_copy(const std::vector<int32_t> &g, const Row &s) {
     Row t{};
-    for (size_t j = 0; j < g.size(); j++) t[j] = s[g[j]];
+    for (size_t j = 0; j < g.size(); j++) t[j] = s[g[j] & 0xFF] + (uint64_t)((uint32_t)g[j] >> 8);
     return t;
   }
   static inline bool pred_ok(int kind, int a, int b, const Row &t) {
@@ -576,7 +579,7 @@ static int32_t check_gen(orc_engine *e, const int32_t *gen, int32_t n, int out_a
                          int a_in, int a_out) {
   if (!gen || n != out_arity) return e->impl->fail(E_INVALID, "gen length != output arity");
   for (int j = 0; j < n; j++) {
-    int g = gen[j];
+    int g = gen[j] & 0xFF;
     if (join) {
       if (!((g >= 0 && g < a_in) || (g >= 16 && g - 16 < a_out)))
         return e->impl->fail(E_INVALID, "gen column out of range");

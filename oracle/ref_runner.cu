@@ -53,6 +53,13 @@ __device__ void c_second_twice(tuple_type src, tuple_type dst) {
   dst[1] = src[1];
 }
 __device__ bool p_not_equal(tuple_type t) { return t[0] != t[1]; }
+// path_length's step: path(a, y, l + 1) from edge (x, a) reversed, path (x, y, l)
+__device__ void h_path_step(tuple_type inner, tuple_type outer, tuple_type out) {
+  out[0] = inner[1];
+  out[1] = outer[1];
+  out[2] = outer[2] + 1;
+}
+__device__ tuple_generator_hook d_path_step = h_path_step;
 
 __device__ tuple_generator_hook d_inner1_outer1 = h_inner1_outer1;
 __device__ tuple_generator_hook d_outer1_inner1 = h_outer1_inner1;
@@ -94,12 +101,11 @@ static std::vector<column_type> swapped(const std::vector<column_type> &v) {
 }
 
 // -- result digest ----------------------------------------------------------
-__global__ void k_gather_rows(tuple_type *tuples, unsigned long long n, unsigned long long *out) {
+__global__ void k_gather_rows(tuple_type *tuples, unsigned long long n, int arity,
+                              unsigned long long *out) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    out[2 * i] = tuples[i][0];
-    out[2 * i + 1] = tuples[i][1];
-  }
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    for (int c = 0; c < arity; c++) out[arity * i + c] = tuples[i][c];
 }
 static unsigned long long mix64(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -107,25 +113,32 @@ static unsigned long long mix64(unsigned long long x) {
   x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
   return x ^ (x >> 31);
 }
+// Digest of FULL's tuples in the container's order (mix64 over the row
+// index and every column); *sorted reports whether that order is strictly
+// increasing.
 static std::string digest_full(Relation *r, bool *sorted) {
+  const int ar = r->arity;
   unsigned long long n = r->full->tuple_counts;
-  std::vector<unsigned long long> h(2 * n);
+  std::vector<unsigned long long> h((size_t)ar * n);
   if (n) {
     unsigned long long *d;
-    checkCuda(cudaMalloc(&d, 2 * n * sizeof(unsigned long long)));
-    k_gather_rows<<<1024, 256>>>(r->full->tuples, n, d);
+    checkCuda(cudaMalloc(&d, (size_t)ar * n * sizeof(unsigned long long)));
+    k_gather_rows<<<1024, 256>>>(r->full->tuples, n, ar, d);
     checkCuda(cudaGetLastError());
-    checkCuda(cudaMemcpy(h.data(), d, 2 * n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    checkCuda(cudaMemcpy(h.data(), d, (size_t)ar * n * sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost));
     checkCuda(cudaFree(d));
   }
   unsigned long long acc = 0;
   *sorted = true;
   for (unsigned long long i = 0; i < n; i++) {
-    if (i && (h[2 * i - 2] > h[2 * i] || (h[2 * i - 2] == h[2 * i] && h[2 * i - 1] >= h[2 * i + 1])))
-      *sorted = false;
+    if (i) {
+      int c = 0;
+      while (c < ar && h[ar * (i - 1) + c] == h[ar * i + c]) c++;
+      if (c == ar || h[ar * (i - 1) + c] > h[ar * i + c]) *sorted = false;
+    }
     unsigned long long x = mix64(i);
-    x = mix64(x ^ h[2 * i]);
-    x = mix64(x ^ h[2 * i + 1]);
+    for (int c = 0; c < ar; c++) x = mix64(x ^ h[ar * i + c]);
     acc += x;
   }
   char buf[32];
@@ -304,6 +317,30 @@ int main(int argc, char **argv) {
     out["value_flow"] = vf12;
     out["memory_alias"] = ma12;
     out["value_alias"] = va12;
+  } else if (prog == "plen") {
+    // test/path_length.cu:59-140: path (x, y, 1) per edge, arity 3 with one
+    // dependent column, joined with the reversed edges
+    auto e = read_tsv(argv[2]);
+    auto re = swapped(e);
+    std::vector<column_type> p3;
+    for (size_t i = 0; i + 1 < e.size(); i += 2) {
+      p3.push_back(e[i]);
+      p3.push_back(e[i + 1]);
+      p3.push_back(1);
+    }
+    std::cout.rdbuf(sink.rdbuf());
+    Relation *edge = rel("edge_2__2_1", &re, true, false, grid, block);
+    Relation *path = new Relation();
+    path->index_flag = false;
+    load_relation(path, "path_3__1_2_3", 3, p3.data(), p3.size() / 3, 1, 1, grid, block);
+    std::cout.rdbuf(old);
+    LIE lie(grid, block);
+    lie.add_relations(edge, true);
+    lie.add_relations(path, false);
+    lie.add_ra(RelationalJoin(edge, FULL, path, DELTA, path, sym(d_path_step), nullptr, LEFT, grid,
+                              block, detail));
+    iters["plen"] = run_lie(lie);
+    out["path"] = path;
   } else {
     fprintf(stderr, "unknown program %s\n", prog.c_str());
     return 2;

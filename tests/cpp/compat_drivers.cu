@@ -7,6 +7,8 @@
 //   compat_drivers tc   <edges.tsv>
 //   compat_drivers sg   <edges.tsv>
 //   compat_drivers cspa <assign.tsv> <dereference.tsv>
+//   compat_drivers path_length <edges.tsv>   (arity 3, dependent column,
+//                                             a hook that adds 1)
 //
 // Prints one line: RESULT {"sizes": ..., "digests": ..., "iterations": ...}
 #include <cstdio>
@@ -39,6 +41,13 @@ __device__ void copy_c1c1(tuple_type src, tuple_type dst) {
   dst[1] = src[1];
 }
 __device__ bool not_equal(tuple_type t) { return t[0] != t[1]; }
+// path(a, y, l + 1) from edge (x, a) reversed and path (x, y, l)
+__device__ void path_step(tuple_type inner, tuple_type outer, tuple_type out) {
+  out[0] = inner[1];
+  out[1] = outer[1];
+  out[2] = outer[2] + 1;
+}
+__device__ tuple_generator_hook path_step_d = path_step;
 
 __device__ tuple_generator_hook join_i1_o1_d = join_i1_o1;
 __device__ tuple_generator_hook join_o1_i1_d = join_o1_i1;
@@ -137,6 +146,27 @@ int main(int argc, char **argv) {
     iters["init"] = init.iteration_counter;
     iters["sg"] = lie.iteration_counter;
     out["sg"] = sg;
+  } else if (prog == "path_length") {
+    auto e = read_tsv(argv[2]);
+    auto re = swap_cols(e);
+    std::vector<column_type> p3;
+    for (size_t i = 0; i + 1 < e.size(); i += 2) {
+      p3.push_back(e[i]);
+      p3.push_back(e[i + 1]);
+      p3.push_back(1);
+    }
+    Relation *edge = new Relation(), *path = new Relation();
+    path->index_flag = false;
+    load_relation(path, "path_3__1_2_3", 3, p3.data(), p3.size() / 3, 1, 1, 0, 0);
+    load(edge, "edge_2__2_1", &re);
+    LIE plen(grid, block);
+    plen.add_relations(edge, true);
+    plen.add_relations(path, false);
+    plen.add_ra(RelationalJoin(edge, FULL, path, DELTA, path, fetch(path_step_d), nullptr, LEFT,
+                               grid, block, detail));
+    plen.fixpoint_loop();
+    iters["plen"] = plen.iteration_counter;
+    out["path"] = path;
   } else if (prog == "cspa" && argc >= 4) {
     auto as = read_tsv(argv[2]), de = read_tsv(argv[3]);
     auto ras = swap_cols(as), rde = swap_cols(de);

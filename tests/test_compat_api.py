@@ -35,7 +35,7 @@ REF_TEST = "/root/reference/test"
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_TEST), reason="reference sources not present")
-@pytest.mark.parametrize("driver", ["tc", "sg", "cspa"])
+@pytest.mark.parametrize("driver", ["tc", "sg", "cspa", "path_length"])
 def test_reference_drivers_build_unchanged(tmp_path, driver):
     """The reference's own drivers (test/tc.cu, sg.cu, cspa.cu), unchanged
     except that their `../include/*.cuh` lines name this repository's
@@ -74,3 +74,24 @@ def test_compat_drivers_match_golden(tmp_path, name):
     assert got["sizes"] == want["sizes"]
     assert got["iterations"] == want["iterations"]
     assert got["digests"] == want["digests"]
+
+
+@pytest.mark.gpu
+def test_compat_path_length_matches_oracle(tmp_path):
+    """The arity-3 program through the drop-in API: a __device__ hook that
+    adds 1 to a column, fetched with cudaMemcpyFromSymbol, recognised as
+    GDL_PLUS; same sizes, digest and passes as the oracle."""
+    import programs as P
+    from gdlog_b200 import Engine
+    e = W.rmat_edges(8, 600, seed=3)
+    p = tmp_path / "e.tsv"
+    W.write_tsv(str(p), e)
+    r = subprocess.run([DRIVERS, "path_length", str(p)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("RESULT ")][-1][7:])
+    with Engine("oracle", max_arity=3) as o:
+        ro = P.path_length(o, e)
+        want = (ro.relations["path"].size(), hex(ro.relations["path"].digest()),
+                ro.iterations["plen"])
+    assert (got["sizes"]["path"], got["digests"]["path"], got["iterations"]["plen"]) == want
