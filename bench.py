@@ -63,6 +63,10 @@ WORKLOADS = {
     "cspa_v300": dict(
         prog=P.cspa, make=lambda: W.cspa_facts(300, 600, 225, seed=3),
         desc="CSPA, 300 variables, 600 assign, 225 dereference, Zipf(1.1) sources, seed 3"),
+    # arity 3 rows load from the host (the fixpoint's device time excludes loads)
+    "plen_grid_64": dict(
+        prog=P.path_length, make=lambda: (W.grid_edges(64, 64),), host_inputs=True, max_arity=3,
+        desc="path_length (arity 3, dependent length column), 64x64 directed grid, 8,064 edges"),
 }
 
 
@@ -151,7 +155,7 @@ def dist_env():
 def oracle_run(wl: dict, inputs, threads: int = 0):
     """One run of the workload on the CPU oracle: (fixpoint seconds, tuples)."""
     from gdlog_b200 import Engine
-    with Engine("oracle", threads=threads) as eng:
+    with Engine("oracle", threads=threads, max_arity=wl.get("max_arity", 2)) as eng:
         r = wl["prog"](eng, *inputs)
         secs = sum(lie.stats()["ms"] for lie in r.lies.values()) / 1e3
         return secs, derived(r), eng.threads
@@ -198,7 +202,7 @@ def reference_gpu(workload: str):
     """Fixpoint seconds of the reference CUDA engine on this workload, as
     recorded by tests/golden/make_ref_gpu.py on a B200."""
     key = {"sg_rmat_s14": "sg_rmat_s14_40000_s14", "tc_grid_64": "tc_grid_64x64",
-           "cspa_v300": "cspa_v300_s3"}.get(workload)
+           "cspa_v300": "cspa_v300_s3", "plen_grid_64": "plen_grid_64x64"}.get(workload)
     p = os.path.join(REPO, "tests", "golden", "ref_gpu.json")
     if not os.path.exists(p):
         return None
@@ -239,7 +243,8 @@ def run_ours(a) -> None:
         return
     rec = tuner.apply(eng, wl["prog"], inputs)
     tuning = rec["config"] if rec else "engine defaults (no cached tuning for this size bucket)"
-    dev_inputs = [DeviceRows(torch.from_numpy(x.astype(np.int64)).to(dev)) for x in inputs]
+    dev_inputs = inputs if wl.get("host_inputs") else \
+        [DeviceRows(torch.from_numpy(x.astype(np.int64)).to(dev)) for x in inputs]
     pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in inputs]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 

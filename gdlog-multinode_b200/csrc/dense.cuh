@@ -1,7 +1,7 @@
 // dense.cuh — bitmap form of relation versions over a small key domain.
 //
-// When every column value is below 2^dk with 2*dk <= 30, the whole key
-// domain of an arity-2 relation is 2^(2dk) bits (at most 128 MB), and a
+// When every column value is below 2^dk with 2*dk <= 32, the whole key
+// domain of an arity-2 relation is 2^(2dk) bits (at most 512 MB), and a
 // version of the relation can be held as a bitmap whose bit (c0, c1) sits in
 // row c0.  Bit order is the reference's tuple order (include/tuple.cuh:
 // 106-126), so compacting a bitmap gives the sorted, deduplicated tuple list
@@ -41,7 +41,7 @@ constexpr int kBmBlock = 256;
 constexpr int kBmWordsPerThread = 8;
 constexpr int kBmTileWords = kBmBlock * kBmWordsPerThread;  // 2048 words = 65536 keys
 constexpr int kBmChunkWords = 64;                          // dirty granularity (256 B)
-constexpr int kDenseMaxDomainBits = 30;
+constexpr int kDenseMaxDomainBits = 32;  // ids below 2^16: a row is one scan tile
 constexpr int kMaxInstanceNodes = 1 << 16;  // a row is at most one scan tile
 
 // Where a key lives in the bitmap: the tuple (c0, c1) of instance

@@ -129,7 +129,8 @@ struct RelHost {
   bool delta_sorted = true;
   u64 bm_words = 0;  // size of this relation's bitmaps (dense form), words
   bool bm_valid = false;       // bmF holds FULL (set by a dense LIE)
-  bool full_resident = false;  // FULL exists only as bmF (batched form)
+  bool full_resident = false;  // FULL exists only as bmF (batched form, or too large)
+  int bm_dk = 0;               // square domain bits of that bitmap (plain form)
 };
 
 }  // namespace
@@ -1461,13 +1462,16 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       if (e->h[r].full_lazy) {
         // The batched form may keep a FULL too large for a list as its
         // bitmap only (per-instance sizes, digests and exports read it).
+        // So does the plain form when FULL is beyond the list limit: its
+        // size and digest are then read from the bitmap.
         const u64 n = e->h[r].full.n;
         gdl_status as = GDL_E_NOMEM;
-        if (!e->instances || (n <= kMaxRows && n * 8 <= e->total_mem / 4))
+        if (n <= kMaxRows && (!e->instances || n * 8 <= e->total_mem / 4))
           as = ensure_arr(e, e->h[r].full, n, false);
-        if (as == GDL_E_NOMEM && e->instances) {
+        if (as == GDL_E_NOMEM && (e->instances || n > kMaxRows)) {
           cudaGetLastError();
           e->rels[r].full_resident = true;
+          e->rels[r].bm_dk = L.dk;
           e->h[r].full_lazy = 0;
           continue;
         }
@@ -1830,8 +1834,9 @@ static gdl_status version_view(gdl_engine *e, int rel, int ver, const u64 **ptr,
   if (ver == GDL_FULL) {
     if (e->rels[rel].full_resident && need_rows)
       return fail(e, GDL_E_UNSUPPORTED,
-                  "FULL of %s is kept as a bitmap only (batched form): read it per instance",
-                  e->rels[rel].name.c_str());
+                  "FULL of %s is kept as a bitmap only (more than %llu tuples, or the batched "
+                  "form): read its size and digest, or per instance",
+                  e->rels[rel].name.c_str(), (unsigned long long)kMaxRows);
     *ptr = r.full.ptr;
     *n = r.full_vis ? r.full.n : 0;
   } else if (ver == GDL_DELTA) {
@@ -1992,9 +1997,26 @@ gdl_status gdl_relation_dump_tsv(gdl_engine *e, int32_t rel, int32_t ver, const 
   return GDL_OK;
 }
 
+static gdl_status bitmap_stats(gdl_engine *e, const u32 *bm, const DenseMap &map,
+                               const std::vector<SegInfo> &segs, std::vector<u64> &size,
+                               std::vector<u64> &digest);
+
 gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *out) {
   CHECK_REL(e, rel);
   if (!out) return GDL_E_INVALID;
+  const RelHost &rr = e->rels[rel];
+  if (ver == GDL_FULL && rr.full_resident && !e->instances && rr.bm_valid && rr.bm_dk) {
+    // FULL beyond the list limit, kept as its square-domain bitmap
+    TRY(pull(e));
+    if (!e->d_square_seg) TRY(dalloc(e, (void **)&e->d_square_seg, sizeof(SegInfo)));
+    const SegInfo sq{0, (u32)(rr.bm_dk - 5), 1u << rr.bm_dk};
+    CK(e, cudaMemcpyAsync(e->d_square_seg, &sq, sizeof sq, cudaMemcpyHostToDevice, e->s));
+    const DenseMap map{e->d_square_seg, nullptr, 1, 31, rr.bm_words};
+    std::vector<u64> size, dig;
+    TRY(bitmap_stats(e, e->h[rel].bmF, map, {sq}, size, dig));
+    *out = dig[0];
+    return GDL_OK;
+  }
   const u64 *p = nullptr;
   u64 n = 0;
   bool sorted;
@@ -2354,6 +2376,47 @@ gdl_status gdl_lie_instance_iterations(gdl_engine *e, int32_t lie, uint64_t *out
   return GDL_OK;
 }
 
+// Size and digest of every instance's tuples in a FULL bitmap (local ids),
+// from per-tile popcounts, their per-instance prefix, and k_inst_digest.
+static gdl_status bitmap_stats(gdl_engine *e, const u32 *bm, const DenseMap &map,
+                               const std::vector<SegInfo> &segs, std::vector<u64> &size,
+                               std::vector<u64> &digest) {
+  const u64 tiles = map.words / kBmTileWords;
+  u32 *d_pop = nullptr;
+  u64 *d_rank = nullptr, *d_acc = nullptr;
+  TRY(dalloc(e, (void **)&d_pop, tiles * sizeof(u32)));
+  TRY(dalloc(e, (void **)&d_rank, tiles * sizeof(u64)));
+  TRY(dalloc(e, (void **)&d_acc, segs.size() * sizeof(u64)));
+  k_inst_tile_pop<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_pop);
+  std::vector<u32> pop(tiles);
+  CK(e, cudaMemcpyAsync(pop.data(), d_pop, tiles * sizeof(u32), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  std::vector<u64> rank(tiles);
+  size.assign(segs.size(), 0);
+  for (size_t i = 0, t = 0; i < segs.size(); i++) {
+    const u64 region = round_up((u64)segs[i].n << segs[i].row_shift, kBmTileWords);
+    u64 run = 0;
+    for (u64 k = 0; k < region / kBmTileWords; k++, t++) {
+      rank[t] = run;
+      run += pop[t];
+    }
+    size[i] = run;
+  }
+  CK(e, cudaMemcpyAsync(d_rank, rank.data(), tiles * sizeof(u64), cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaMemsetAsync(d_acc, 0, segs.size() * sizeof(u64), e->s));
+  k_inst_digest<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_rank, d_acc);
+  std::vector<u64> acc(segs.size());
+  CK(e, cudaMemcpyAsync(acc.data(), d_acc, acc.size() * sizeof(u64), cudaMemcpyDeviceToHost,
+                        e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  dfree(e, d_pop);
+  dfree(e, d_rank);
+  dfree(e, d_acc);
+  digest.resize(segs.size());
+  for (size_t i = 0; i < segs.size(); i++) digest[i] = mix64(acc[i] ^ size[i]);
+  return GDL_OK;
+}
+
 gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *sizes,
                                        uint64_t *digests, int32_t n) {
   CHECK_REL(e, rel);
@@ -2364,41 +2427,12 @@ gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *siz
     return fail(e, GDL_E_INVALID, "relation %s has no FULL bitmap of the batched form",
                 rh.name.c_str());
   TRY(pull(e));
-  const u32 *bm = e->h[rel].bmF;
   const DenseMap map{e->d_segs, e->d_tile_inst, (u32)e->segs.size(), e->seg_shift, e->seg_words};
-  const u64 tiles = e->seg_words / kBmTileWords;
-  u32 *d_pop = nullptr;
-  u64 *d_rank = nullptr, *d_acc = nullptr;
-  TRY(dalloc(e, (void **)&d_pop, tiles * sizeof(u32)));
-  TRY(dalloc(e, (void **)&d_rank, tiles * sizeof(u64)));
-  TRY(dalloc(e, (void **)&d_acc, e->segs.size() * sizeof(u64)));
-  k_inst_tile_pop<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_pop);
-  std::vector<u32> pop(tiles);
-  CK(e, cudaMemcpyAsync(pop.data(), d_pop, tiles * sizeof(u32), cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
-  std::vector<u64> rank(tiles), size(e->segs.size(), 0);
-  for (size_t i = 0, t = 0; i < e->segs.size(); i++) {
-    const u64 region = round_up((u64)e->segs[i].n << e->segs[i].row_shift, kBmTileWords);
-    u64 run = 0;
-    for (u64 k = 0; k < region / kBmTileWords; k++, t++) {
-      rank[t] = run;
-      run += pop[t];
-    }
-    size[i] = run;
-  }
-  CK(e, cudaMemcpyAsync(d_rank, rank.data(), tiles * sizeof(u64), cudaMemcpyHostToDevice, e->s));
-  CK(e, cudaMemsetAsync(d_acc, 0, e->segs.size() * sizeof(u64), e->s));
-  k_inst_digest<<<grid_for(e, tiles, 1, 8), 256, 0, e->s>>>(bm, map, d_rank, d_acc);
-  std::vector<u64> acc(e->segs.size());
-  CK(e, cudaMemcpyAsync(acc.data(), d_acc, acc.size() * sizeof(u64), cudaMemcpyDeviceToHost,
-                        e->s));
-  CK(e, cudaStreamSynchronize(e->s));
-  dfree(e, d_pop);
-  dfree(e, d_rank);
-  dfree(e, d_acc);
+  std::vector<u64> size, dig;
+  TRY(bitmap_stats(e, e->h[rel].bmF, map, e->segs, size, dig));
   for (int i = 0; i < n; i++) {
     sizes[i] = size[i];
-    digests[i] = mix64(acc[i] ^ size[i]);
+    digests[i] = dig[i];
   }
   return GDL_OK;
 }

@@ -98,7 +98,7 @@ gdl_status gdl_engine_clear(gdl_engine *e);
 /* How a fixpoint deduplicates NEWT and merges it into FULL.  SORT: radix
  * sort of NEWT, then one merge-path pass giving NEWT \ FULL and FULL ∪ NEWT
  * (the reference's sort/unique/set_difference/merge, src/lie.cu:122-185).
- * DENSE: when 2 * bits(largest column value) <= dense_max_bits (at most 30,
+ * DENSE: when 2 * bits(largest column value) <= dense_max_bits (at most 32,
  * the default), relations are kept as bitmaps over the key domain during the
  * loop and NEWT is deduplicated by setting bits.  AUTO (default): DENSE
  * where the domain allows, else SORT.  Results are identical in all modes.
@@ -116,7 +116,7 @@ gdl_status gdl_engine_set_dedup(gdl_engine *e, int32_t mode, int32_t dense_max_b
  * at 0.8, src/relation.cu:836).  A zero field keeps the engine's default. */
 typedef struct gdl_tuning {
   int32_t dedup;               /* GDL_DEDUP_* */
-  int32_t dense_max_bits;      /* largest 2*bits domain kept as bitmaps (<= 30) */
+  int32_t dense_max_bits;      /* largest 2*bits domain kept as bitmaps (<= 32) */
   int32_t join_ctas_per_sm;    /* materialisation grid, CTAs per SM (default 8) */
   int32_t count_ctas_per_sm;   /* count-pass grid, CTAs per SM (default 4) */
   int32_t index_slots_per_key; /* hashed index: slots per distinct key, power of two >= 2 (default 2) */

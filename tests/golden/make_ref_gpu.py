@@ -39,6 +39,7 @@ WORKLOADS = {
     "cspa_v120_s1": ("cspa", lambda: W.cspa_facts(120, 240, 90, seed=1)),
     "cspa_v300_s3": ("cspa", lambda: W.cspa_facts(300, 600, 225, seed=3)),
     "plen_grid_16x16": ("plen", lambda: (W.grid_edges(16, 16),)),
+    "plen_grid_64x64": ("plen", lambda: (W.grid_edges(64, 64),)),
     "plen_dag_L12_W10_s1": ("plen", lambda: (W.layered_dag(12, 10, 1),)),
     "plen_rmat_s8_600_s1": ("plen", lambda: (W.rmat_edges(8, 600, seed=1),)),
 }

@@ -241,3 +241,51 @@ def test_modes_agree_on_cspa_with_clear():
     with Engine("oracle") as o:
         want = summarize(P.cspa(o, assign, deref))
     assert out[0] == out[1] == out[2] == out[3] == want
+
+
+@pytest.mark.parametrize("mode", ["dense", "sort"])
+def test_ids_up_to_2_16_match_oracle(mode):
+    """Ids above 2^15 (a 2^32-bit key domain: 512 MB bitmaps, rows of one
+    scan tile): both paths still match the oracle."""
+    e = W.rmat_edges(16, 3000, seed=21)
+    assert int(e.max()) >= 1 << 15
+    with Engine("gpu", dedup=mode) as g:
+        got = summarize(P.sg(g, e, sync=g.sync))
+    with Engine("oracle") as o:
+        want = summarize(P.sg(o, e))
+    assert got == want
+
+
+def dag_closure_size(L, Wd, seed):
+    """|TC| of a layered DAG from reachability bitsets, layer by layer from
+    the last one (independent of both engines)."""
+    e = W.layered_dag(L, Wd, seed).astype(np.int64)
+    n = L * Wd
+    words = (n + 63) // 64
+    reach = np.zeros((n, words), dtype=np.uint64)
+    succ = [[] for _ in range(n)]
+    for a, b in e.tolist():
+        succ[a].append(b)
+    for x in range(n - 1, -1, -1):
+        for y in succ[x]:
+            reach[x] |= reach[y]
+            reach[x, y // 64] |= np.uint64(1) << np.uint64(y % 64)
+    return int(np.bitwise_count(reach).sum())
+
+
+def test_closure_beyond_the_list_limit_stays_a_bitmap():
+    """A closure of more than 2^30 pairs (60,000 nodes) cannot be a list:
+    FULL stays the bitmap, whose size and digest are still readable and
+    whose rows are refused with a status."""
+    L, Wd, seed = 200, 300, 5
+    e = W.layered_dag(L, Wd, seed)
+    with Engine("gpu") as g:
+        r = P.tc(g, e, sync=g.sync)
+        path = r.output
+        n = path.size()
+        d1 = path.digest()
+        assert n > (1 << 30)
+        with pytest.raises(GdlError):
+            path.rows()
+        assert path.digest() == d1
+    assert n == dag_closure_size(L, Wd, seed)

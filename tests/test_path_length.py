@@ -96,6 +96,8 @@ def test_gpu_64x64_grid_lengths():
     assert (l == np.abs(y // 64 - a // 64) + np.abs(y % 64 - a % 64)).all()
     _, dig_o, it_o = run("oracle", W.grid_edges(64, 64))
     assert dig == dig_o and it == it_o
+    ref = REF_GPU["plen_grid_64x64"]  # the reference engine's own answer
+    assert hex(dig) == ref["digests"]["path"] and it["plen"] == ref["iterations"]["plen"]
 
 
 @pytest.mark.gpu
