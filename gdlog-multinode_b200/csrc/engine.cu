@@ -982,6 +982,14 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
 }
 
 // Grow the buffers an overflow asked for.
+// Capacity after an overflow: half again the need, and at least four times
+// the old capacity (within the list limit), so that a relation growing by
+// orders of magnitude reruns few iterations (each rerun also rebuilds the
+// graph).
+u64 grown(u64 need, u64 cap) {
+  return std::max<u64>(need, std::min<u64>(std::max<u64>(need + need / 2, 4 * cap), kMaxRows));
+}
+
 gdl_status grow_after_overflow(gdl_engine *e, const Ctl &c) {
   TRY(pull(e));
   for (size_t i = 0; i < e->rels.size(); i++) {
@@ -990,21 +998,21 @@ gdl_status grow_after_overflow(gdl_engine *e, const Ctl &c) {
     u64 nf = c.need[need_index((int)i, kNeedFull)];
     u64 nd = c.need[need_index((int)i, kNeedDelta)];
     if (nn) {
-      TRY(ensure_arr(e, r.newt, nn + nn / 2, false));
+      TRY(ensure_arr(e, r.newt, grown(nn, r.newt.cap), false));
       if (r.delta_next.cap < r.newt.cap) {
         TRY(ensure_arr(e, r.delta, r.newt.cap, true));
         TRY(ensure_arr(e, r.delta_next, r.newt.cap, false));
       }
     }
     if (nf) {
-      TRY(ensure_arr(e, r.full, nf + nf / 2, true));
-      TRY(ensure_arr(e, r.full_next, nf + nf / 2, false));
+      TRY(ensure_arr(e, r.full, grown(nf, r.full.cap), true));
+      TRY(ensure_arr(e, r.full_next, r.full.cap, false));
       TRY(ensure_index(e, r.full_idx, r.full.cap));
       TRY(ensure_index(e, r.full_idx_next, r.full_next.cap));
     }
     if (nd) {
-      TRY(ensure_arr(e, r.delta, nd + nd / 2, true));
-      TRY(ensure_arr(e, r.delta_next, nd + nd / 2, false));
+      TRY(ensure_arr(e, r.delta, grown(nd, r.delta.cap), true));
+      TRY(ensure_arr(e, r.delta_next, r.delta.cap, false));
       TRY(ensure_index(e, r.delta_idx, r.delta.cap));
       TRY(ensure_index(e, r.delta_idx_next, r.delta_next.cap));
     }
