@@ -63,6 +63,16 @@ WORKLOADS = {
     "cspa_v300": dict(
         prog=P.cspa, make=lambda: W.cspa_facts(300, 600, 225, seed=3),
         desc="CSPA, 300 variables, 600 assign, 225 dereference, Zipf(1.1) sources, seed 3"),
+    # ids above 2^15: bitmaps over a 2^32-bit domain (the sorted-list path
+    # cannot hold this program's candidates); no CPU baseline (the oracle
+    # would take many minutes)
+    "sg_rmat_s16": dict(
+        prog=P.sg, make=lambda: (W.rmat_edges(16, 120000, seed=16),), no_cpu=True,
+        desc="same generation, R-MAT scale 16 (65,536 nodes), 120,000 edges, seed 16"),
+    # C3: the full CSPA configuration, about a minute per step on one B200
+    "cspa_c3": dict(
+        prog=P.cspa, make=lambda: W.cspa_facts(), no_cpu=True,
+        desc="CSPA, 20,000 variables, 40,000 assign, 15,000 dereference, Zipf(1.1), seed 3"),
     # arity 3 rows load from the host (the fixpoint's device time excludes loads)
     "plen_grid_64": dict(
         prog=P.path_length, make=lambda: (W.grid_edges(64, 64),), host_inputs=True, max_arity=3,
@@ -356,11 +366,15 @@ def run_ours(a) -> None:
     ref = reference_gpu(a.workload)
     if ref:
         line["reference_gpu"] = ref
-    if world == 1 and not a.no_cpu_baseline:
+    if world == 1 and not a.no_cpu_baseline and not wl.get("no_cpu"):
         secs, t, threads = oracle_run(wl, inputs)
         line["cpu_baseline"] = {"value": t / secs, "unit": "tuples/s", "cores": threads,
                                 "kind": "port",
                                 "sample": "one full run of the same workload on the CPU oracle"}
+    elif wl.get("no_cpu"):
+        line["cpu_baseline"] = {"value": None, "unavailable":
+                                "the CPU oracle would need many minutes (or more host memory) "
+                                "for this workload"}
     print(json.dumps(line), flush=True)
 
 
@@ -368,7 +382,15 @@ def run_reference(a) -> None:
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    if a.workload == "dag_batch384":
+        run_reference_dag(a, world)
+        return
     wl = WORKLOADS[a.workload]
+    if wl.get("no_cpu"):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the CPU implementation would need many minutes (or more host "
+                          "memory) for this workload"}), flush=True)
+        return
     inputs = wl["make"]()
     secs0, _, _ = oracle_run(wl, inputs)  # one warm-up run (CPU caches, page faults)
     budget = 240.0
@@ -391,6 +413,32 @@ def run_reference(a) -> None:
         "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
                          "sample": f"{steps} full run(s) of the workload, after one warm-up run"},
         "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_reference_dag(a, world) -> None:
+    """The reference arm of the batched workload: one plain fixpoint per DAG
+    (the reference has no batched form) on the CPU, over a bounded sample."""
+    import batch as B
+    from gdlog_b200 import Engine
+    dags = W.dag_batch(384)
+    inst = [(e,) for (_, _, e) in dags[:4]]
+    with Engine("oracle") as o:
+        B.run_plain_loop(o, P.tc, inst[:1])  # warm-up
+        r = B.run_plain_loop(o, P.tc, inst)
+        threads = o.threads
+    v = len(inst) / r.seconds
+    print(json.dumps({
+        "impl": "reference", "metric": "batched TC instances/s (384 layered DAGs)", "value": v,
+        "unit": "instances/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 384 / v * 1e3, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "384 layered DAGs, L in [8,128], W in [16,256] log-uniform",
+                   "program": "tc", "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "instances/s", "cores": threads, "kind": "port",
+                         "sample": "the first 4 of the 384 DAGs, one plain fixpoint each"},
+        "e2e": {"value": v, "unit": "instances/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
 
