@@ -37,6 +37,7 @@ SPACE = {
     "join_ctas_per_sm": [4, 8, 16],
     "count_ctas_per_sm": [2, 4, 8],
     "index_slots_per_key": [2, 4],
+    "pull_joins": [2, 1],
 }
 
 
@@ -44,9 +45,11 @@ def _redundant(cfg: dict) -> bool:
     """Configurations that differ from an earlier one only in a parameter
     their path does not read: the join form and bit aggregation of the sort
     path, the aggregation of the two-pass dense join, and the grids of the
-    count / materialise passes of the one-pass dense join."""
+    count / materialise passes of the one-pass dense join, and the pull
+    form's switch on the sort path."""
     one_pass = cfg.get("dense_join_passes", 1) == 1
-    if cfg.get("dedup") == "sort" and (not one_pass or cfg.get("join_aggregate", 1) != 1):
+    if cfg.get("dedup") == "sort" and (not one_pass or cfg.get("join_aggregate", 1) != 1 or
+                                       cfg.get("pull_joins", 2) != 2):
         return True
     if cfg.get("dedup") == "dense" and one_pass:
         return (cfg.get("count_ctas_per_sm", 2) != 2 or cfg.get("join_ctas_per_sm", 4) != 4)

@@ -163,6 +163,7 @@ struct BmScanArgs {
   DArr *list_a;    // output lists (sorted keys); null when not wanted
   DArr *list_b;
   Index *idx_b;    // if set: run index of list b
+  u64 *count_a;    // if set: receives total_a (a count without a list)
   u64 *count_b;    // if set: receives total_b (a count without a list)
   u64 *pop_g_out;  // if set: receives popcount(g) (NEWT size)
   u64 *inst_delta; // if set: per-instance count of list a is added here
@@ -484,6 +485,7 @@ __device__ __forceinline__ void write_finish(const BmScanArgs &a, u64 bytes) {
   if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
     if (a.list_a) a.list_a->n = a.rec->total_a;
     if (a.list_b) a.list_b->n = a.rec->total_b;
+    if (a.count_a) *a.count_a = a.rec->total_a;
     if (a.count_b) *a.count_b = a.rec->total_b;
     if (a.pop_g_out) *a.pop_g_out = a.rec->pop_g;
     a.rec->pop_g = 0;

@@ -34,6 +34,7 @@
 #include "index.cuh"
 #include "join.cuh"
 #include "merge.cuh"
+#include "pull.cuh"
 #include "sort.cuh"
 
 #include <algorithm>
@@ -180,6 +181,10 @@ struct gdl_engine {
   int dense_join_passes = 1;
   int join_aggregate = 1;  // 1: one reduction per candidate, 2: warp-aggregated by word
   bool row_or_joins = true;  // GDLOG_ROW_OR=0 turns row-OR joins off
+  // 1: push form only, 2: pull form where eligible from 2^kPullAutoBits ids,
+  // 3: pull form where eligible (pull.cuh)
+  int pull_joins = 2;
+  u64 *d_pull_count = nullptr;  // bit count of a transposed NEWT (zero between launches)
   // Device memory in bytes, read once at creation: cudaMemGetInfo can take
   // tens of milliseconds on a busy host, so the fixpoint sizes its lists
   // from this and asks for free memory only after an allocation failed.
@@ -193,7 +198,8 @@ struct gdl_engine {
   u32 *d_tile_inst = nullptr;
   SegInfo *d_square_seg = nullptr;  // the one segment of the square domain
   u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
-  LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy
+  LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy,
+                              // [4] [5] bitmap scans, [6] pull join, [7] transpose
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
   u64 *d_u64 = nullptr;       // [4] small device scalars
   u32 *d_u32 = nullptr;       // [4]
@@ -461,7 +467,7 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   RelHost &rh = e->rels[r];
   RelDev &h = e->h[r];
   if (rh.bm_words != words) {
-    for (u32 **p : {&h.bmF, &h.bmG}) {
+    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT}) {
       dfree(e, *p);
       *p = nullptr;
     }
@@ -605,6 +611,9 @@ struct Plan {
   std::vector<char> full_list;            // FULL read as a list by some op
   std::vector<char> newt_list;            // NEWT read as a join outer
   std::vector<char> acopy_src;            // NEWT read by an ACopy
+  std::vector<char> pull;                 // per op: pull form (pull.cuh)
+  std::vector<char> delta_t, newt_t;      // per relation: transposed DELTA / NEWT read
+  std::vector<char> delta_list;           // per relation: DELTA read as a list by some op
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -615,7 +624,13 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.full_list.assign(n, 0);
   p.newt_list.assign(n, 0);
   p.acopy_src.assign(n, 0);
+  p.pull.assign(L.ops.size(), 0);
+  p.delta_t.assign(n, 0);
+  p.newt_t.assign(n, 0);
+  p.delta_list.assign(n, 0);
   for (const OpHost &op : L.ops) {
+    if (op.kind == 0 && op.outer_ver == GDL_DELTA) p.delta_list[op.outer] = 1;
+    if (op.kind != 2 && op.inner_ver == GDL_DELTA) p.delta_list[op.inner] = 1;
     if (op.kind == 2) p.acopy_src[op.inner] = 1;
     if (op.kind == 0) {
       (op.inner_ver == GDL_DELTA ? p.delta_idx : p.full_idx)[op.inner] = 1;
@@ -627,6 +642,48 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
     }
   }
   return p;
+}
+
+// Pull-form joins (pull.cuh), decided once the LIE's dense form is known: a
+// join into bitmaps over the square domain whose output is (outer column 1,
+// inner column 1), without predicate, over the DELTA of an update relation
+// or the NEWT of a tmp relation.  A NEWT read only by such joins needs no
+// list.
+void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
+  if (e->pull_joins < 2 || !L.dense || e->instances ||
+      L.dk < (e->pull_joins == 3 ? kPullMinBits : kPullAutoBits))
+    return;
+  std::vector<char> is_update(e->rels.size(), 0), is_tmp(e->rels.size(), 0);
+  for (int r : L.update) is_update[r] = 1;
+  for (int r : L.tmps) is_tmp[r] = 1;
+  std::fill(p.newt_list.begin(), p.newt_list.end(), 0);
+  std::fill(p.delta_list.begin(), p.delta_list.end(), 0);
+  for (size_t oi = 0; oi < L.ops.size(); oi++) {
+    const OpHost &op = L.ops[oi];
+    if (op.kind != 0) continue;
+    const bool shape = !op.generic && op.pred.kind == 0 && op.sel.s0 == 3 && op.sel.s1 == 1;
+    const bool outer_ok = (op.outer_ver == GDL_DELTA && is_update[op.outer]) ||
+                          (op.outer_ver == GDL_NEWT && is_tmp[op.outer]);
+    if (shape && outer_ok) {
+      p.pull[oi] = 1;
+      (op.outer_ver == GDL_DELTA ? p.delta_t : p.newt_t)[op.outer] = 1;
+    } else if (op.outer_ver == GDL_NEWT) {
+      p.newt_list[op.outer] = 1;
+    } else if (op.outer_ver == GDL_DELTA) {
+      p.delta_list[op.outer] = 1;
+    }
+    if (op.inner_ver == GDL_DELTA) p.delta_list[op.inner] = 1;
+  }
+  for (size_t oi = 0; oi < L.ops.size(); oi++)
+    if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
+}
+
+// Transposed bitmaps of the relations pull-form joins read.
+gdl_status ensure_tbitmaps(gdl_engine *e, const Plan &p, int r, u64 words) {
+  RelDev &h = e->h[r];
+  if (p.delta_t[r] && !h.bmDT) TRY(dalloc(e, (void **)&h.bmDT, words * 4));
+  if (p.newt_t[r] && !h.bmGT) TRY(dalloc(e, (void **)&h.bmGT, words * 4));
+  return GDL_OK;
 }
 
 // Bitmap size, in 32-bit words, of one relation version over the square
@@ -718,7 +775,11 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       } else {
         a.outer = &R[op.outer].newt;
         a.outer_vis = nullptr;
-        if (dense && oh.bmG) {
+        if (dense && oh.bmG && plan.pull[oi]) {
+          // pull form: NEWT's bitmap transposed, its size counted (no list)
+          a.outer_bm = oh.bmG;
+          a.outer_bm_words = words;
+        } else if (dense && oh.bmG) {
           // NEWT as a join outer: the sorted list of its bitmap (dirty
           // chunks only).
           BmScanArgs c = scan_none(map);
@@ -766,6 +827,23 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       a.row_or = dense && e->row_or_joins && op.inner_ver != GDL_DELTA &&
                  e->h[op.inner].dense && e->h[op.inner].bmF && op.pred.kind == 0 &&
                  (op.sel.s0 == 2 || op.sel.s0 == 3) && op.sel.s1 == 1;
+      if (plan.pull[oi]) {
+        const u32 *OT = oh.bmDT;
+        const u64 side = 1ull << (L.dk - kPullMinBits);
+        if (op.outer_ver == GDL_NEWT) {
+          TransposeArgs t{oh.bmG, nullptr, oh.bmGT, L.dk, &R[op.outer].newt, e->d_pull_count,
+                          &e->recs[7], e->d_ctl};
+          PLAUNCH(kc, kPBitmap,
+                  k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(t));
+          OT = oh.bmGT;
+        }
+        a.rec = &e->recs[6];
+        PLAUNCH(kc, kPJoinMat,
+                k_join_pull_bm<<<(int)e->sms * 8, kPullBlock,
+                                 pull_acc_words(L.dk) * 4, s>>>(
+                    a, &R[op.out], OT, L.dk));
+        continue;
+      }
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
       JoinArgs b = a;
@@ -870,8 +948,15 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       a.gated = 1;
       a.inst_delta = L.d_inst_delta;
       a.ex_a = kBmDelta;
-      a.list_a = &R[r].delta_next;
-      a.need_a = need_index(r, kNeedDelta);
+      if (plan.delta_list[r] || !plan.delta_t[r]) {
+        a.list_a = &R[r].delta_next;
+        a.need_a = need_index(r, kNeedDelta);
+      } else {
+        // no op reads DELTA as a list (pull-form joins read its transposed
+        // bitmap): only its size; the list is written from the transposed
+        // bitmap if the loop ends with a DELTA left
+        a.count_a = &R[r].delta_next.n;
+      }
       if (plan.full_list[r]) {
         a.ex_b = kBmUnion;
         a.list_b = &R[r].full_next;
@@ -885,6 +970,15 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       launch_scan_count(e, a, r, kc);
       scans.push_back(a);
     }
+    // the next DELTA transposed, for the pull-form joins that read it
+    // (before the write passes change FULL and clear NEWT)
+    for (int r : L.update)
+      if (plan.delta_t[r]) {
+        const u64 side = 1ull << (L.dk - kPullMinBits);
+        TransposeArgs t{e->h[r].bmG, e->h[r].bmF, e->h[r].bmDT, L.dk, nullptr, nullptr,
+                        &e->recs[7], e->d_ctl};
+        PLAUNCH(kc, kPBitmap, k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(t));
+      }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
     const u64 tiles = L.map.words / kBmTileWords;
@@ -1092,7 +1186,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
                   "op output %s is neither an update nor a tmp relation of the LIE",
                   e->rels[op.out].name.c_str());
   }
-  const Plan plan = make_plan(e, L);
+  Plan plan = make_plan(e, L);
   // The timed span is the whole call, as the reference's drivers time the
   // whole fixpoint_loop (test/tc.cu:120-140): setup, loop and finish.
   CK(e, cudaEventRecord(e->ev0, e->s));
@@ -1156,6 +1250,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     for (const OpHost &op : L.ops) plain = plain && !op.generic;
     L.dense = plain && (e->instances || (e->dedup_mode != 1 && 2 * dk <= e->dense_max_bits));
     L.dk = L.dense && !e->instances ? dk : 0;
+    plan_pull(e, L, plan);
   }
   for (RelDev &h : e->h) {
     h.dense = h.full_lazy = 0;
@@ -1191,6 +1286,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       TRY(ensure_bitmaps(e, r, words, false));
       e->h[r].dense = 1;
     }
+    for (auto *v : {&L.update, &L.tmps})
+      for (int r : *v) TRY(ensure_tbitmaps(e, plan, r, words));
     mark("bitmap_alloc");
     // A dirty map pays when a NEWT bitmap is too large to scan whole every
     // iteration; for small ones the scans read everything and the joins
@@ -1238,6 +1335,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       if (h.full.n)
         k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
             &e->d_rels[r].full, h.bmF, L.map, e->d_ctl);
+      if (plan.delta_t[r]) {
+        // the first DELTA, transposed, for the pull-form joins that read it
+        CK(e, cudaMemsetAsync(h.bmDT, 0, words * 4, e->s));
+        if (h.delta.n)
+          k_bm_from_list_t<<<grid_for(e, h.delta.n, 256, 8), 256, 0, e->s>>>(
+              &e->d_rels[r].delta, h.bmDT, L.dk, e->d_ctl);
+      }
       e->rels[r].bm_valid = true;
     }
     for (int r : L.tmps) {
@@ -1500,6 +1604,35 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       CK(e, cudaGetLastError());
       TRY(pull(e));
     }
+    // DELTA lists that were not kept (read only transposed by pull-form
+    // joins) and are not empty (max_iteration ended the loop): transposed
+    // back into the (empty) NEWT bitmap and listed from it.
+    bool any_delta = false;
+    for (int r : L.update)
+      if (plan.delta_t[r] && !plan.delta_list[r] && e->h[r].delta.n) {
+        RelDev &h = e->h[r];
+        TRY(ensure_arr(e, h.delta, h.delta.n, false));
+        any_delta = true;
+      }
+    if (any_delta) {
+      TRY(push(e));
+      Counts kc;
+      const u64 side = 1ull << (L.dk - kPullMinBits);
+      for (int r : L.update) {
+        const RelDev &h = e->h[r];
+        if (!(plan.delta_t[r] && !plan.delta_list[r] && h.delta.n)) continue;
+        TransposeArgs t{h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr, &e->recs[7], e->d_ctl};
+        k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
+        BmScanArgs a = scan_none(L.map);
+        a.g = h.bmG;
+        a.ex_b = kBmUnion;
+        a.list_b = &e->d_rels[r].delta;
+        launch_scan(e, a, r, &kc);
+        CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
+      }
+      CK(e, cudaGetLastError());
+      TRY(pull(e));
+    }
     for (RelDev &h : e->h) {
       h.dense = h.full_lazy = 0;
       h.dirty = nullptr;
@@ -1600,6 +1733,7 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
     if (!strcmp(m, "dense")) e->dedup_mode = 2;
   }
   if (const char *ro = getenv("GDLOG_ROW_OR")) e->row_or_joins = strcmp(ro, "0") != 0;
+  if (const char *pj = getenv("GDLOG_PULL")) e->pull_joins = strcmp(pj, "0") != 0 ? 3 : 1;
   if (const char *b = getenv("GDLOG_DENSE_MAX_BITS"))
     e->dense_max_bits = std::min(atoi(b), kDenseMaxDomainBits);
   cudaMemPool_t pool;
@@ -1613,15 +1747,19 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
                                (int)kSortSmemBytes)) ||
       bad(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kMergeSmemBytes)) ||
+      bad(cudaFuncSetAttribute(k_join_pull_bm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(pull_acc_words(16) * 4))) ||
       bad(cudaMalloc(&e->d_rels, kMaxRels * sizeof(RelDev))) ||
       bad(cudaMalloc(&e->d_ctl, sizeof(Ctl))) || bad(cudaMallocHost(&e->h_ctl, sizeof(Ctl))) ||
       bad(cudaMalloc(&e->recs, 8 * sizeof(LaunchRec))) ||
       bad(cudaMalloc(&e->d_tmp, 4 * sizeof(DArr))) || bad(cudaMalloc(&e->d_u64, 4 * sizeof(u64))) ||
-      bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) || bad(cudaEventCreate(&e->ev0)) ||
+      bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) ||
+      bad(cudaMalloc(&e->d_pull_count, sizeof(u64))) || bad(cudaEventCreate(&e->ev0)) ||
       bad(cudaEventCreate(&e->ev1)) ||
       bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
       bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
       bad(cudaMemsetAsync(e->recs, 0, 8 * sizeof(LaunchRec), e->s)) ||
+      bad(cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s)) ||
       bad(cudaStreamSynchronize(e->s))) {
     gdl_engine_destroy(e);
     return GDL_E_CUDA;
@@ -1639,7 +1777,7 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
-    for (u32 *bm : {r.bmF, r.bmG})
+    for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT})
       if (bm) cudaFreeAsync(bm, e->s);
     if (r.bmD) cudaFreeAsync(r.bmD, e->s);
     if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);
@@ -1691,7 +1829,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->d_segs,
                   (void *)e->d_tile_inst, (void *)e->d_square_seg,
                   (void *)e->recs,
-                  (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_rels,
+                  (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_pull_count,
+                  (void *)e->d_rels,
                   (void *)e->d_ctl})
     if (p) cudaFree(p);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -2258,7 +2397,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
                                   (t->index_slots_per_key & (t->index_slots_per_key - 1)))) ||
       (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
       t->dense_join_passes < 0 || t->dense_join_passes > 2 || t->join_aggregate < 0 ||
-      t->join_aggregate > 2)
+      t->join_aggregate > 2 || t->pull_joins < 0 || t->pull_joins > 3)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -2268,6 +2407,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->dirty_min_log2_words) e->dirty_min_log2_words = t->dirty_min_log2_words;
   if (t->dense_join_passes) e->dense_join_passes = t->dense_join_passes;
   if (t->join_aggregate) e->join_aggregate = t->join_aggregate;
+  if (t->pull_joins) e->pull_joins = t->pull_joins;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -2282,6 +2422,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->dirty_min_log2_words = e->dirty_min_log2_words;
   t->dense_join_passes = e->dense_join_passes;
   t->join_aggregate = e->join_aggregate;
+  t->pull_joins = e->pull_joins;
   return GDL_OK;
 }
 

@@ -1,0 +1,269 @@
+// pull.cuh — joins into bitmaps gathered by output row ("pull" form).
+//
+// A join whose output tuple is (outer column 1, inner column 1), joined on
+// column 0 of both sides, makes output row r the union of the inner runs
+// I[k] over the keys k with (k, r) in the outer.  Same generation's two
+// recursive rules have this shape (test/sg.cu:158-170):
+//   tmp(b, x) :- sg(a, b), edge(a, x)       sg(x, y) :- tmp(b, x), edge(b, y)
+// and so do the value-flow rules of CSPA (test/cspa.cu).  The push form
+// (k_join_bm, dense.cuh) walks the outer in key order and sends one L2
+// reduction per candidate tuple, and the candidates of one output row
+// repeat each other many times over: on R-MAT graphs 35-49 candidates fall
+// on each distinct output word.  Here the outer is read transposed — bit
+// (r, k) of OT is outer tuple (k, r) — so that one block sees a run of a
+// row's keys together, gathers the row in shared memory and sends one
+// reduction per nonzero word.
+//
+//   k_bm_transpose  OT := transpose(g) or transpose(g & ~f) (the DELTA that
+//                   the next update step lists), in 256 x 256-bit tiles:
+//                   each 32 x 32 block is transposed in registers with five
+//                   shuffle rounds and written out through shared memory
+//                   as whole 32-byte sectors.  Optionally counts the bits
+//                   (the size of a NEWT outer, whose list is not built).
+//   k_join_pull_bm  a block per unit of 256 OT words (part of one row, or
+//                   several short rows), taken from a work counter: lists
+//                   the unit's keys 256 at a time, probes the inner index
+//                   (one 16-byte slot per key), expands the runs balanced
+//                   over the block into the shared row (candidate p of the
+//                   round by thread p mod 256, so a run is read coalesced),
+//                   then ORs the row's nonzero words into the output.
+//
+// The square domain only (ids below 2^dk, 8 <= dk <= 16; one instance).
+#pragma once
+
+#include "common.cuh"
+#include "dense.cuh"
+#include "index.cuh"
+#include "join.cuh"
+
+namespace gdl {
+
+constexpr int kTrBlock = 256;
+constexpr int kPullBlock = 256;
+constexpr int kPullUnit = 256;   // OT words per unit of work (a word per thread): 8192 keys
+constexpr int kPullMinBits = 8;  // a transposed tile is 256 ids square
+constexpr int kPullAutoBits = 12;  // the pull form by default from 2^12 ids on
+
+// Lane l holds row l of a 32 x 32 bit block (bit j = column j); afterwards
+// lane j holds column j (bit l = row l).  Each round swaps the off-diagonal
+// quarters of the blocks of side 2s between lane pairs l, l ^ s.
+__device__ __forceinline__ u32 transpose32(u32 x, int lane) {
+  const u32 masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    const int s = 16 >> i;
+    const u32 m = masks[i];
+    const u32 y = __shfl_xor_sync(0xffffffffu, x, s);
+    x = (lane & s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
+  }
+  return x;
+}
+
+struct TransposeArgs {
+  const u32 *g;   // source bitmap
+  const u32 *f;   // if set: the source is g & ~f
+  u32 *dst;       // transposed bitmap (every word written)
+  int dk;         // 2^dk ids, rows of 2^(dk-5) words
+  DArr *count_to; // if set: receives the number of bits as its n
+  u64 *count_acc; // zero between launches
+  LaunchRec *lrec;
+  Ctl *ctl;
+};
+
+__global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
+  __shared__ u32 s_t[256][9];  // the transposed tile; row pitch 9 avoids bank conflicts
+  __shared__ unsigned long long s_bits;
+  if (ctl_stop(a.ctl)) return;
+  const int rs = a.dk - 5;
+  const u64 per = 1ull << (a.dk - 8);  // tiles per side
+  const u64 tiles = per * per;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u64 bits = 0, moved = 0;
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const u64 tr = t / per, tc = t % per;
+    // this thread's input row: tile row tr, row threadIdx.x of the tile
+    // (warp wid holds rows 32 wid .. 32 wid + 31), words 8 tc .. 8 tc + 7
+    const u64 src = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
+    u32 v[8];
+    load8(a.g + src, v);
+    bool any = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
+    moved += 32;
+    if (a.f && any) {
+      u32 w[8];
+      load8(a.f + src, w);
+      moved += 32;
+#pragma unroll
+      for (int i = 0; i < 8; i++) v[i] &= ~w[i];
+      any = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) bits += __popc(v[i]);
+    const bool tile_any = __syncthreads_or(any);
+    if (tile_any) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        // lane j: input column 32 (8 tc + i) + j = output row, its bits
+        // the input rows 256 tr + 32 wid + l = output word 8 tr + wid
+        s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+      }
+    }
+    __syncthreads();
+    uint4 *d = reinterpret_cast<uint4 *>(a.dst + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
+    if (tile_any) {
+      const u32 *q = s_t[threadIdx.x];
+      d[0] = make_uint4(q[0], q[1], q[2], q[3]);
+      d[1] = make_uint4(q[4], q[5], q[6], q[7]);
+    } else {
+      d[0] = make_uint4(0, 0, 0, 0);
+      d[1] = make_uint4(0, 0, 0, 0);
+    }
+    moved += 32;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    bits += __shfl_xor_sync(0xffffffffu, bits, o);
+    moved += __shfl_xor_sync(0xffffffffu, moved, o);
+  }
+  if (lane == 0) prof_add(a.ctl, kPBitmap, moved);
+  if (!a.count_to) return;
+  if (threadIdx.x == 0) s_bits = 0;
+  __syncthreads();
+  if (lane == 0 && bits) atomicAdd(&s_bits, (unsigned long long)bits);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_bits) atomicAdd(reinterpret_cast<unsigned long long *>(a.count_acc), s_bits);
+  if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
+    a.count_to->n = *a.count_acc;
+    *a.count_acc = 0;
+  }
+}
+
+// Shared state of k_join_pull_bm.  The row accumulator is the dynamic
+// shared memory: pull_acc_words(dk) words.
+struct PullSmem {
+  u32 w[kPullUnit];         // the unit's OT words
+  u32 wpre[kPullUnit];      // exclusive bit offsets of the words
+  u32 off[kPullBlock];      // exclusive candidate offsets of the round's keys
+  u32 start[kPullBlock];    // inner run start of each key
+  u32 arow[kPullBlock];     // accumulator offset of each key's output row
+  u64 scan_tmp[kPullBlock / 32];
+  long long unit;
+};
+
+// The accumulator holds the unit's rows, and at least one whole row (the
+// output columns of a key can be anywhere in its row): max(256, 2^(dk-5)).
+__host__ __device__ __forceinline__ u32 pull_acc_words(int dk) {
+  return 1u << (dk - 5 > 8 ? dk - 5 : 8);
+}
+
+__global__ void __launch_bounds__(kPullBlock) k_join_pull_bm(JoinArgs a, const RelDev *out_rd,
+                                                            const u32 *OT, int dk) {
+  __shared__ PullSmem sm;
+  extern __shared__ u32 acc[];
+  if (ctl_stop(a.ctl)) return;
+  const u64 n_outer = eff_count(a.outer, a.outer_vis);
+  const u64 n_inner = eff_count(a.inner, a.inner_vis);
+  if (n_outer == 0 || n_inner == 0) {
+    join_empty_side(a, n_outer);
+    return;
+  }
+  u32 *G = out_rd->bmG;
+  u8 *D = out_rd->dirty;
+  const Index ix = *a.inner_idx;
+  const u64 *inner = a.inner->ptr;
+  const int tid = threadIdx.x;
+  const int rs = dk - 5;
+  const u32 row_mask = (1u << rs) - 1;
+  const u32 acc_words = pull_acc_words(dk);
+  const u32 units = (u32)((1ull << (2 * dk - 5)) / kPullUnit);
+  const u32 n_ids = 1u << dk;
+  for (u32 i = tid; i < acc_words; i += kPullBlock) acc[i] = 0;
+  u64 cand = 0, keys = 0, flushed = 0;
+  while (true) {
+    const long long u = grab_tile(a.rec, &sm.unit);
+    if (u >= (long long)units) break;
+    const u32 w0 = (u32)u * kPullUnit;  // below 2^27
+    const u32 wv = OT[w0 + tid];
+    sm.w[tid] = wv;
+    u64 tot64;
+    sm.wpre[tid] = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
+    const u32 tot = (u32)tot64;
+    if (tot == 0) continue;  // block-uniform
+    __syncthreads();
+    keys += tot;
+    const u32 r0 = w0 >> rs;  // first output row of the unit
+    for (u32 q0 = 0; q0 < tot; q0 += kPullBlock) {
+      const u32 q = q0 + tid;
+      u32 len = 0, st = 0, arow = 0;
+      if (q < tot) {
+        // the word holding key q: the last word whose offset is <= q
+        u32 k = 0;
+#pragma unroll
+        for (u32 h = kPullUnit / 2; h > 0; h >>= 1)
+          if (sm.wpre[k + h] <= q) k += h;
+        const u32 b = nth_set_bit(sm.w[k], q - sm.wpre[k]);
+        const u32 ow = w0 + k;  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
+        arow = ((ow >> rs) - r0) << rs;
+        len = index_probe(ix, ((ow & row_mask) << 5) + b, &st);
+      }
+      u64 ctot64;
+      sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
+      const u32 ctot = (u32)ctot64;  // at most 256 runs of at most 2^16
+      sm.start[tid] = st;
+      sm.arow[tid] = arow;
+      __syncthreads();
+      for (u32 p = tid; p < ctot; p += kPullBlock) {
+        // the last key whose offset is <= p (an empty run shares its offset
+        // with the next key, so it is never the last)
+        u32 j = 0;
+#pragma unroll
+        for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
+          if (sm.off[j + h] <= p) j += h;
+        const u32 col = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
+        if (col < n_ids)
+          atomicOr(&acc[sm.arow[j] + (col >> 5)], 1u << (col & 31));
+        else
+          atomicOr(&a.ctl->oob, 8192u);
+      }
+      cand += ctot;
+      __syncthreads();
+    }
+    // flush the unit's rows: one reduction per nonzero word
+    for (u32 i = tid; i < acc_words; i += kPullBlock) {
+      const u32 v = acc[i];
+      if (v) {
+        const u64 gw = ((u64)r0 << rs) + i;
+        asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + gw), "r"(v) : "memory");
+        if (D) D[gw / kBmChunkWords] = 1;
+        acc[i] = 0;
+        flushed++;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) flushed += __shfl_xor_sync(0xffffffffu, flushed, o);
+  // algorithmic bytes: 4 per OT word, 16 per key (its index slot), 8 per
+  // candidate (the inner tuple), 4 per word reduced into the output
+  if ((tid & 31) == 0) prof_add(a.ctl, kPJoinMat, 4 * flushed);
+  if (tid == 0) prof_add(a.ctl, kPJoinMat, 16 * keys + 8 * cand);
+  if (launch_rec_finish(a.rec) && tid == 0) prof_add(a.ctl, kPJoinMat, 4ull * units * kPullUnit);
+}
+
+// Set the transposed bits (c1, c0) of a key list (DELTA at the start of a
+// LIE), square domain of 2^dk ids.
+__global__ void __launch_bounds__(256) k_bm_from_list_t(const DArr *list, u32 *bm, int dk, Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u64 n = list->n;
+  const u64 *k = list->ptr;
+  const u32 lim = 1u << dk;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u32 c0 = key_c0(k[i]), c1 = key_c1(k[i]);
+    if (c0 < lim && c1 < lim)
+      atomicOr(bm + (((u64)c1 << (dk - 5)) + (c0 >> 5)), 1u << (c0 & 31));
+    else
+      atomicOr(&ctl->oob, 8192u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
+}
+
+}  // namespace gdl

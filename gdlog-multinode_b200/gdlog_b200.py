@@ -58,7 +58,8 @@ class Tuning(C.Structure):
     _fields_ = [("dedup", C.c_int32), ("dense_max_bits", C.c_int32),
                 ("join_ctas_per_sm", C.c_int32), ("count_ctas_per_sm", C.c_int32),
                 ("index_slots_per_key", C.c_int32), ("dirty_min_log2_words", C.c_int32),
-                ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32)]
+                ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32),
+                ("pull_joins", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -368,10 +369,14 @@ class Engine:
         if kind == "gpu" and dedup is not None:
             if dedup == "dense_dirty":  # bitmaps, with dirty maps at every size
                 self.set_tuning(dedup="dense", dirty_min_log2_words=11)
-            elif dedup == "dense_2pass":  # bitmaps, joins as count + materialise passes
-                self.set_tuning(dedup="dense", dense_join_passes=2)
-            elif dedup == "dense_agg":  # bitmaps, warp-aggregated bit-sets in the joins
-                self.set_tuning(dedup="dense", join_aggregate=2)
+            elif dedup == "dense_push":  # bitmaps, every join in the push form
+                self.set_tuning(dedup="dense", pull_joins=1)
+            elif dedup == "dense_pull":  # bitmaps, pull form wherever it applies
+                self.set_tuning(dedup="dense", pull_joins=3)
+            elif dedup == "dense_2pass":  # bitmaps, push joins as count + materialise passes
+                self.set_tuning(dedup="dense", dense_join_passes=2, pull_joins=1)
+            elif dedup == "dense_agg":  # bitmaps, push joins with warp-aggregated bit-sets
+                self.set_tuning(dedup="dense", join_aggregate=2, pull_joins=1)
             else:
                 self._check(self.lib.gdl_engine_set_dedup(self.h, self.DEDUP[dedup], 0))
 

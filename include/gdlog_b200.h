@@ -128,6 +128,13 @@ typedef struct gdl_tuning {
   int32_t join_aggregate;      /* one-pass joins into bitmaps: 1 = one reduction
                                   per candidate (default), 2 = lanes of a warp
                                   that hit the same word combine their bits */
+  int32_t pull_joins;          /* joins into bitmaps whose output is (outer
+                                  column 1, inner column 1) over a DELTA or
+                                  tmp NEWT outer: 1 = push form (outer in key
+                                  order), 2 = pull form (gathered by output
+                                  row from the transposed outer) when ids
+                                  reach 2^12 (default), 3 = pull form from
+                                  2^8 ids */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

@@ -14,11 +14,13 @@ def test_bucket_and_candidates():
     e = W.grid_edges(16, 16)
     assert A.bucket("tc", (e,)) == "tc:n8:t8"
     cands = A.candidates()
-    # sort: 3 x 3 x 2 grids; dense with 2 passes: the same; dense with one
-    # pass: the index choice and the bit aggregation
-    assert len(cands) == 18 + 18 + 4
+    # sort: 3 x 3 x 2 grids; dense with 2 passes: the same, push or pull
+    # form; dense with one pass: the index choice and the bit aggregation,
+    # push or pull form
+    assert len(cands) == 18 + 2 * 18 + 2 * 4
     assert {c["dedup"] for c in cands} == {"dense", "sort"}
     assert {c["dense_join_passes"] for c in cands} == {1, 2}
+    assert {c["pull_joins"] for c in cands} == {1, 2}
 
 
 @pytest.mark.gpu

@@ -23,11 +23,13 @@ pytestmark = pytest.mark.gpu
 
 # Both deduplication paths of the engine: radix sort + merge-path merge, and
 # bitmaps over the key domain (every workload here has a small domain, so
-# "dense" is what the engine picks by itself); bitmaps with dirty maps at
-# every size (scans of listed dirty chunks), bitmaps with joins as count +
-# materialise passes instead of one probe-and-expand pass, and bitmaps whose
-# joins combine a warp's bits per word before the reduction.
-MODES = ["sort", "dense", "dense_dirty", "dense_2pass", "dense_agg"]
+# "dense" is what the engine picks by itself); bitmaps with every eligible
+# join in the pull form (gathered by output row) or every join in the push
+# form; bitmaps with dirty maps at every size (scans of listed dirty
+# chunks), bitmaps with push joins as count + materialise passes instead of
+# one probe-and-expand pass, and bitmaps whose push joins combine a warp's
+# bits per word before the reduction.
+MODES = ["sort", "dense", "dense_pull", "dense_push", "dense_dirty", "dense_2pass", "dense_agg"]
 
 
 def summarize(r):
