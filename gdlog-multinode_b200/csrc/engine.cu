@@ -678,6 +678,12 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
 }
 
+// The update step of relation r is one fused pass (pull.cuh, k_bm_update_t):
+// its DELTA is read only transposed and its FULL not as a list.
+bool fused_update(const Plan &p, int r) {
+  return p.delta_t[r] && !p.delta_list[r] && !p.full_list[r];
+}
+
 // Transposed bitmaps of the relations pull-form joins read.
 gdl_status ensure_tbitmaps(gdl_engine *e, const Plan &p, int r, u64 words) {
   RelDev &h = e->h[r];
@@ -939,7 +945,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
     // relation whose FULL list is read during the loop also gets FULL' and
     // its index.  All relations are counted and checked (gate) before any
     // bitmap is written.
-    std::vector<BmScanArgs> scans;
+    std::vector<BmScanArgs> scans, fused;
     for (int r : L.update) {
       BmScanArgs a = scan_none(L.map);
       a.rd = &R[r];
@@ -967,18 +973,35 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       a.gate_rels = R;
       a.gate_update = &L.d_lie->update[0];
       a.gate_n = (int)L.update.size();
+      if (fused_update(plan, r)) {
+        // DELTA read only transposed, FULL not as a list: one fused pass
+        // (pull.cuh, k_bm_update_t) after every count pass
+        a.rec = &R[r].scan;
+        a.lrec = &e->recs[5];
+        a.ctl = e->d_ctl;
+        fused.push_back(a);
+        continue;
+      }
       launch_scan_count(e, a, r, kc);
       scans.push_back(a);
     }
     // the next DELTA transposed, for the pull-form joins that read it
     // (before the write passes change FULL and clear NEWT)
-    for (int r : L.update)
+    for (const BmScanArgs &a : scans) {
+      const int r = (int)(a.rd - R);
       if (plan.delta_t[r]) {
         const u64 side = 1ull << (L.dk - kPullMinBits);
         TransposeArgs t{e->h[r].bmG, e->h[r].bmF, e->h[r].bmDT, L.dk, nullptr, nullptr,
                         &e->recs[7], e->d_ctl};
         PLAUNCH(kc, kPBitmap, k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(t));
       }
+    }
+    for (const BmScanArgs &a : fused) {
+      const int r = (int)(a.rd - R);
+      const u64 side = 1ull << (L.dk - kPullMinBits);
+      PLAUNCH(kc, kPBitmap, k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
+                                a, e->h[r].bmDT, L.dk));
+    }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
     const u64 tiles = L.map.words / kBmTileWords;
@@ -1293,8 +1316,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     // iteration; for small ones the scans read everything and the joins
     // skip the extra store.
     const bool use_dirty = words >= (1ull << e->dirty_min_log2_words);
+    // (a fused update pass reads all of NEWT: no dirty map)
     for (auto *v : {&L.update, &L.tmps})
-      for (int r : *v) e->h[r].dirty = use_dirty ? e->h[r].bmD : nullptr;
+      for (int r : *v)
+        e->h[r].dirty = use_dirty && !fused_update(plan, r) ? e->h[r].bmD : nullptr;
     TRY(ensure_dense_scratch(e, words));
     mark("dense_scratch");
     // Every list of the loop is bounded by the key domain: size them for

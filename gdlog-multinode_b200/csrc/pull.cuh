@@ -24,9 +24,10 @@
 //                   several short rows), taken from a work counter: lists
 //                   the unit's keys 256 at a time, probes the inner index
 //                   (one 16-byte slot per key), expands the runs balanced
-//                   over the block into the shared row (candidate p of the
-//                   round by thread p mod 256, so a run is read coalesced),
-//                   then ORs the row's nonzero words into the output.
+//                   over the block into the shared row (4 consecutive
+//                   candidates per thread, so a run is read in 32-byte
+//                   pieces), then ORs the row's nonzero words into the
+//                   output.
 //
 // The square domain only (ids below 2^dk, 8 <= dk <= 16; one instance).
 #pragma once
@@ -41,6 +42,7 @@ namespace gdl {
 constexpr int kTrBlock = 256;
 constexpr int kPullBlock = 256;
 constexpr int kPullUnit = 256;   // OT words per unit of work (a word per thread): 8192 keys
+constexpr int kPullPer = 4;      // consecutive candidates per thread and step
 constexpr int kPullMinBits = 8;  // a transposed tile is 256 ids square
 constexpr int kPullAutoBits = 12;  // the pull form by default from 2^12 ids on
 
@@ -138,6 +140,97 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
   }
 }
 
+// The update step of a relation whose DELTA only pull-form joins read and
+// whose FULL is not read as a list during the loop, in one pass over the
+// 256 x 256-bit tiles (instead of count, scan, write and transpose passes):
+// DELTA = G & ~F counted and written transposed into dt, F |= G and G
+// cleared where G has bits, NEWT's size counted.  Behind the write passes'
+// capacity gate: when another relation's list is too small nothing is
+// written and the update step runs again after the lists grow.
+__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk) {
+  __shared__ u32 s_t[256][9];
+  __shared__ unsigned long long s_cnt[2];
+  if (ctl_stop(a.ctl)) return;
+  if (write_gate_closed(a)) return;
+  scan_bind(a);
+  u32 *G = const_cast<u32 *>(a.g);
+  u32 *F = a.f;
+  const int rs = dk - 5;
+  const u64 per = 1ull << (dk - 8);
+  const u64 tiles = per * per;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+  u64 n_delta = 0, n_newt = 0, moved = 0;
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const u64 tr = t / per, tc = t % per;
+    const u64 src = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
+    u32 g[8], d[8];
+    load8(G + src, g);
+    const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
+    moved += 32;
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < 8; i++) d[i] = 0;
+    if (any_g) {
+      u32 f[8];
+      load8(F + src, f);
+      uint4 *pf = reinterpret_cast<uint4 *>(F + src);
+      pf[0] = make_uint4(f[0] | g[0], f[1] | g[1], f[2] | g[2], f[3] | g[3]);
+      pf[1] = make_uint4(f[4] | g[4], f[5] | g[5], f[6] | g[6], f[7] | g[7]);
+      uint4 *pg = reinterpret_cast<uint4 *>(G + src);
+      pg[0] = make_uint4(0, 0, 0, 0);
+      pg[1] = make_uint4(0, 0, 0, 0);
+      moved += 96;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        d[i] = g[i] & ~f[i];
+        n_delta += __popc(d[i]);
+        n_newt += __popc(g[i]);
+        any |= d[i] != 0u;
+      }
+    }
+    const bool tile_any = __syncthreads_or(any);
+    if (tile_any) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(d[i], lane);
+    }
+    __syncthreads();
+    uint4 *o = reinterpret_cast<uint4 *>(dt + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
+    if (tile_any) {
+      const u32 *q = s_t[threadIdx.x];
+      o[0] = make_uint4(q[0], q[1], q[2], q[3]);
+      o[1] = make_uint4(q[4], q[5], q[6], q[7]);
+    } else {
+      o[0] = make_uint4(0, 0, 0, 0);
+      o[1] = make_uint4(0, 0, 0, 0);
+    }
+    moved += 32;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_delta += __shfl_xor_sync(0xffffffffu, n_delta, o);
+    n_newt += __shfl_xor_sync(0xffffffffu, n_newt, o);
+    moved += __shfl_xor_sync(0xffffffffu, moved, o);
+  }
+  if (lane == 0) {
+    if (n_delta) atomicAdd(&s_cnt[0], (unsigned long long)n_delta);
+    if (n_newt) atomicAdd(&s_cnt[1], (unsigned long long)n_newt);
+    prof_add(a.ctl, kPBitmap, moved);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_cnt[0]) atomicAdd(reinterpret_cast<unsigned long long *>(&a.rec->total_a), s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(reinterpret_cast<unsigned long long *>(&a.rec->pop_g), s_cnt[1]);
+  }
+  if (launch_rec_finish(a.lrec) && threadIdx.x == 0) {
+    *a.count_a = a.rec->total_a;
+    *a.pop_g_out = a.rec->pop_g;
+    a.rec->total_a = 0;
+    a.rec->pop_g = 0;
+  }
+}
+
 // Shared state of k_join_pull_bm.  The row accumulator is the dynamic
 // shared memory: pull_acc_words(dk) words.
 struct PullSmem {
@@ -212,18 +305,38 @@ __global__ void __launch_bounds__(kPullBlock) k_join_pull_bm(JoinArgs a, const R
       sm.start[tid] = st;
       sm.arow[tid] = arow;
       __syncthreads();
-      for (u32 p = tid; p < ctot; p += kPullBlock) {
-        // the last key whose offset is <= p (an empty run shares its offset
-        // with the next key, so it is never the last)
+      // kPullPer consecutive candidates per thread: one search for the
+      // first (the last key whose offset is <= p; an empty run shares its
+      // offset with the next key, so it is never the last), then walked
+      // forward; the loads are issued before the ORs
+      for (u32 p0 = tid * kPullPer; p0 < ctot; p0 += kPullBlock * kPullPer) {
         u32 j = 0;
 #pragma unroll
         for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
-          if (sm.off[j + h] <= p) j += h;
-        const u32 col = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
-        if (col < n_ids)
-          atomicOr(&acc[sm.arow[j] + (col >> 5)], 1u << (col & 31));
-        else
-          atomicOr(&a.ctl->oob, 8192u);
+          if (sm.off[j + h] <= p0) j += h;
+        u32 jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+        u32 col[kPullPer], ar[kPullPer];
+#pragma unroll
+        for (int i = 0; i < kPullPer; i++) {
+          const u32 p = p0 + i;
+          col[i] = ~0u;
+          if (p < ctot) {
+            while (p >= jend) {  // next non-empty run
+              j++;
+              jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+            }
+            col[i] = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
+            ar[i] = sm.arow[j];
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < kPullPer; i++) {
+          if (col[i] == ~0u) continue;
+          if (col[i] < n_ids)
+            atomicOr(&acc[ar[i] + (col[i] >> 5)], 1u << (col[i] & 31));
+          else
+            atomicOr(&a.ctl->oob, 8192u);
+        }
       }
       cand += ctot;
       __syncthreads();
