@@ -135,6 +135,14 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
   if (ctl->cond_set) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
 }
 
+// Point the control block at a graph's while-node condition: the loop's
+// first iteration ran on the stream, the graph runs the ones after it.
+__global__ void k_arm_graph(Ctl *ctl, unsigned long long handle) {
+  if (threadIdx.x != 0) return;
+  ctl->cond_handle = handle;
+  ctl->cond_set = 1;
+}
+
 // Pack host-layout rows (two u64 columns) into keys; raise bit 0 of *bad if
 // a column does not fit 32 bits.  *maxv receives the largest column value.
 __global__ void k_pack_rows(const u64 *rows, u64 n, u64 *keys, u64 *maxv, u32 *bad) {

@@ -204,6 +204,10 @@ struct gdl_engine {
   u64 *d_u64 = nullptr;       // [4] small device scalars
   u32 *d_u32 = nullptr;       // [4]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Graph capture runs on its own stream, so that the engine stream can run
+  // a loop's first iteration meanwhile; ev_first marks that iteration's end.
+  cudaStream_t cap_s = nullptr;
+  cudaEvent_t ev_first = nullptr;
   u64 kernels_launched = 0;
   bool broken = false;  // a bounded wait gave up or a bounds check fired
   // Per-kernel accounting of fixpoint loops (gdl_engine_profile).  With
@@ -1079,6 +1083,14 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
     return fail(e, GDL_E_CUDA, "cudaGraphAddNode(conditional): %s", cudaGetErrorString(r));
   }
   cudaGraph_t body = p.conditional.phGraph_out[0];
+  // captured on the capture stream (the engine stream may be running the
+  // loop's first iteration)
+  struct Swap {
+    gdl_engine *e;
+    cudaStream_t keep;
+    ~Swap() { e->s = keep; }
+  } swap{e, e->s};
+  e->s = e->cap_s;
   CK(e, cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal));
   Counts kc;
@@ -1445,28 +1457,67 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   L.graph_dirty = true;
   const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr && !e->profile;
   u64 batch = 4;
+  bool first_batch = true;
   while (true) {
     c.pause = 0;
     c.stop_at = c.iteration + (use_graph ? std::min<u64>(trace_rows, 1u << 20) : batch);
     c.trace_base = c.iteration;
+    const u64 it0 = c.iteration;
+    // The loop's first iteration runs on the stream while the host captures
+    // and instantiates the graph for the iterations after it; when that
+    // iteration already ended the loop (and the host sees it), no graph
+    // launch follows.
+    const bool pre = use_graph && L.graph_dirty && first_batch;
+    first_batch = false;
+    Counts pre_kc;
+    if (pre) {
+      c.cond_set = 0;
+      c.cond_handle = 0;
+      CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
+      enqueue_iteration(e, L, plan, &pre_kc, false);
+      CK(e, cudaGetLastError());
+      CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+      CK(e, cudaEventRecord(e->ev_first, e->s));
+    }
     if (use_graph && L.graph_dirty) {
       const auto tg = std::chrono::steady_clock::now();
       TRY(build_graph(e, L, plan));
       L.graph_ms += host_ms_since(tg);
     }
-    c.cond_set = use_graph ? 1 : 0;
-    c.cond_handle = use_graph ? L.cond_handle : 0;
-    CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
-    const u64 it0 = c.iteration;
+    bool run_graph = use_graph;
+    if (pre) {
+      const cudaError_t q = cudaEventQuery(e->ev_first);
+      if (q == cudaSuccess) {
+        const Ctl &h = *e->h_ctl;
+        if (h.done || h.pause || h.overflow || h.timeout || h.oob) run_graph = false;
+      } else if (q != cudaErrorNotReady) {
+        CK(e, q);
+      }
+      cudaGetLastError();
+      L.kernels += pre_kc.total;
+      for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += pre_kc.kind[k];
+    }
     u64 enqueued = 0;
-    if (use_graph) {
+    if (run_graph) {
+      if (pre) {
+        k_arm_graph<<<1, 32, 0, e->s>>>(e->d_ctl, L.cond_handle);
+        L.kernels++;
+        e->prof_launches[kPControl]++;
+      } else {
+        c.cond_set = 1;
+        c.cond_handle = L.cond_handle;
+        CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
+      }
       // the body's first iteration is opened here, later ones by k_commit
       k_begin<<<1, 32, 0, e->s>>>(e->d_rels, L.d_lie, e->d_ctl);
       L.kernels++;
       e->prof_launches[kPControl]++;
       CK(e, cudaGraphLaunch(L.gexec, e->s));
       L.graph_launches++;
-    } else {
+    } else if (!use_graph) {
+      c.cond_set = 0;
+      c.cond_handle = 0;
+      CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
       // Profiling enqueues one iteration at a time, so that no launch of an
       // iteration past the fixpoint enters the per-kernel times.
       const u64 nb = e->profile ? 1 : std::min<u64>(batch, trace_rows);
@@ -1484,9 +1535,16 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     c = *e->h_ctl;
     const u64 ran = c.iteration - it0;
     // In a graph, the body runs once per committed iteration plus once for
-    // an iteration that overflowed; on the stream, every enqueued
-    // iteration launches (those past the fixpoint return at once).
-    const u64 bodies = use_graph ? ran + (c.overflow ? 1 : 0) : enqueued;
+    // an iteration that overflowed (after a first iteration on the stream,
+    // at least once); on the stream, every enqueued iteration launches
+    // (those past the fixpoint return at once).
+    u64 bodies = enqueued;
+    if (run_graph) {
+      bodies = ran + (c.overflow ? 1 : 0);
+      if (pre) bodies = std::max<u64>(bodies, 2) - 1;
+    } else if (use_graph) {
+      bodies = 0;
+    }
     L.kernels += bodies * (u64)L.per_iter.total;
     for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += bodies * (u64)L.per_iter.kind[k];
     if (L.trace_on && ran) {
@@ -1781,6 +1839,8 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
       bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) ||
       bad(cudaMalloc(&e->d_pull_count, sizeof(u64))) || bad(cudaEventCreate(&e->ev0)) ||
       bad(cudaEventCreate(&e->ev1)) ||
+      bad(cudaEventCreateWithFlags(&e->ev_first, cudaEventDisableTiming)) ||
+      bad(cudaStreamCreateWithFlags(&e->cap_s, cudaStreamNonBlocking)) ||
       bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
       bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
       bad(cudaMemsetAsync(e->recs, 0, 8 * sizeof(LaunchRec), e->s)) ||
@@ -1861,6 +1921,8 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->ev_first) cudaEventDestroy(e->ev_first);
+  if (e->cap_s) cudaStreamDestroy(e->cap_s);
   prof_collect(e);
   for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
   if (e->own_stream && e->s) cudaStreamDestroy(e->s);
