@@ -653,10 +653,16 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
 // inner column 1), without predicate, over the DELTA of an update relation
 // or the NEWT of a tmp relation.  A NEWT read only by such joins needs no
 // list.
+// An update relation whose DELTA no op reads as a list then gets the
+// transposed DELTA too: its update step is the fused pass when FULL is not
+// read as a list either, and the transposed DELTA restores the list if the
+// loop ends with a DELTA left.
 void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
-  if (e->pull_joins < 2 || !L.dense || e->instances ||
-      L.dk < (e->pull_joins == 3 ? kPullMinBits : kPullAutoBits))
-    return;
+  if (!L.dense || e->instances || L.dk < kPullMinBits) return;
+  const bool pull_on = e->pull_joins == 3 || (e->pull_joins == 2 && L.dk >= kPullAutoBits);
+  for (int r : L.update)
+    if (!p.delta_list[r]) p.delta_t[r] = 1;
+  if (!pull_on) return;
   std::vector<char> is_update(e->rels.size(), 0), is_tmp(e->rels.size(), 0);
   for (int r : L.update) is_update[r] = 1;
   for (int r : L.tmps) is_tmp[r] = 1;
@@ -680,6 +686,8 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   }
   for (size_t oi = 0; oi < L.ops.size(); oi++)
     if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
+  for (int r : L.update)
+    if (!p.delta_list[r]) p.delta_t[r] = 1;
 }
 
 // The update step of relation r is one fused pass (pull.cuh, k_bm_update_t):

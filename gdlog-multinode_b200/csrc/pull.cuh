@@ -21,11 +21,12 @@
 //                   as whole 32-byte sectors.  Optionally counts the bits
 //                   (the size of a NEWT outer, whose list is not built).
 //   k_join_pull_bm  a block per unit of 256 OT words (part of one row, or
-//                   several short rows), taken from a work counter: lists
+//                   several short rows), taken from a work counter (an
+//                   empty unit costs one barrier after the grab): lists
 //                   the unit's keys 256 at a time, probes the inner index
 //                   (one 16-byte slot per key), expands the runs balanced
-//                   over the block into the shared row (4 consecutive
-//                   candidates per thread, so a run is read in 32-byte
+//                   over the block into the shared row (2 consecutive
+//                   candidates per thread, so a run is read in 16-byte
 //                   pieces), then ORs the row's nonzero words into the
 //                   output.
 //
@@ -42,7 +43,8 @@ namespace gdl {
 constexpr int kTrBlock = 256;
 constexpr int kPullBlock = 256;
 constexpr int kPullUnit = 256;   // OT words per unit of work (a word per thread): 8192 keys
-constexpr int kPullPer = 4;      // consecutive candidates per thread and step
+constexpr int kPullPer = 2;      // consecutive candidates per thread and step
+constexpr int kPullGrab = 1;     // units taken from the work counter at a time
 constexpr int kPullMinBits = 8;  // a transposed tile is 256 ids square
 constexpr int kPullAutoBits = 12;  // the pull form by default from 2^12 ids on
 
@@ -249,7 +251,7 @@ __host__ __device__ __forceinline__ u32 pull_acc_words(int dk) {
   return 1u << (dk - 5 > 8 ? dk - 5 : 8);
 }
 
-__global__ void __launch_bounds__(kPullBlock) k_join_pull_bm(JoinArgs a, const RelDev *out_rd,
+__global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, const RelDev *out_rd,
                                                             const u32 *OT, int dk) {
   __shared__ PullSmem sm;
   extern __shared__ u32 acc[];
@@ -273,83 +275,86 @@ __global__ void __launch_bounds__(kPullBlock) k_join_pull_bm(JoinArgs a, const R
   for (u32 i = tid; i < acc_words; i += kPullBlock) acc[i] = 0;
   u64 cand = 0, keys = 0, flushed = 0;
   while (true) {
-    const long long u = grab_tile(a.rec, &sm.unit);
-    if (u >= (long long)units) break;
-    const u32 w0 = (u32)u * kPullUnit;  // below 2^27
-    const u32 wv = OT[w0 + tid];
-    sm.w[tid] = wv;
-    u64 tot64;
-    sm.wpre[tid] = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
-    const u32 tot = (u32)tot64;
-    if (tot == 0) continue;  // block-uniform
-    __syncthreads();
-    keys += tot;
-    const u32 r0 = w0 >> rs;  // first output row of the unit
-    for (u32 q0 = 0; q0 < tot; q0 += kPullBlock) {
-      const u32 q = q0 + tid;
-      u32 len = 0, st = 0, arow = 0;
-      if (q < tot) {
-        // the word holding key q: the last word whose offset is <= q
-        u32 k = 0;
-#pragma unroll
-        for (u32 h = kPullUnit / 2; h > 0; h >>= 1)
-          if (sm.wpre[k + h] <= q) k += h;
-        const u32 b = nth_set_bit(sm.w[k], q - sm.wpre[k]);
-        const u32 ow = w0 + k;  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
-        arow = ((ow >> rs) - r0) << rs;
-        len = index_probe(ix, ((ow & row_mask) << 5) + b, &st);
-      }
-      u64 ctot64;
-      sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
-      const u32 ctot = (u32)ctot64;  // at most 256 runs of at most 2^16
-      sm.start[tid] = st;
-      sm.arow[tid] = arow;
+    const long long g = grab_tile(a.rec, &sm.unit);
+    if (g * kPullGrab >= (long long)units) break;
+    for (u32 u = (u32)g * kPullGrab; u < min(units, (u32)(g + 1) * kPullGrab); u++) {
+      const u32 w0 = u * kPullUnit;  // below 2^27
+      const u32 wv = OT[w0 + tid];
+      if (!__syncthreads_or(wv != 0u)) continue;  // an empty unit: one barrier
+      sm.w[tid] = wv;
+      u64 tot64;
+      sm.wpre[tid] = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
+      const u32 tot = (u32)tot64;
+      if (tot == 0) continue;  // block-uniform
       __syncthreads();
-      // kPullPer consecutive candidates per thread: one search for the
-      // first (the last key whose offset is <= p; an empty run shares its
-      // offset with the next key, so it is never the last), then walked
-      // forward; the loads are issued before the ORs
-      for (u32 p0 = tid * kPullPer; p0 < ctot; p0 += kPullBlock * kPullPer) {
-        u32 j = 0;
+      keys += tot;
+      const u32 r0 = w0 >> rs;  // first output row of the unit
+      for (u32 q0 = 0; q0 < tot; q0 += kPullBlock) {
+        const u32 q = q0 + tid;
+        u32 len = 0, st = 0, arow = 0;
+        if (q < tot) {
+          // the word holding key q: the last word whose offset is <= q
+          u32 k = 0;
 #pragma unroll
-        for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
-          if (sm.off[j + h] <= p0) j += h;
-        u32 jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
-        u32 col[kPullPer], ar[kPullPer];
+          for (u32 h = kPullUnit / 2; h > 0; h >>= 1)
+            if (sm.wpre[k + h] <= q) k += h;
+          const u32 b = nth_set_bit(sm.w[k], q - sm.wpre[k]);
+          const u32 ow = w0 + k;  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
+          arow = ((ow >> rs) - r0) << rs;
+          len = index_probe(ix, ((ow & row_mask) << 5) + b, &st);
+        }
+        u64 ctot64;
+        sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
+        const u32 ctot = (u32)ctot64;  // at most 256 runs of at most 2^16
+        sm.start[tid] = st;
+        sm.arow[tid] = arow;
+        __syncthreads();
+        // kPullPer consecutive candidates per thread: one search for the
+        // first (the last key whose offset is <= p; an empty run shares its
+        // offset with the next key, so it is never the last), then walked
+        // forward; the loads are issued before the ORs
+        for (u32 p0 = tid * kPullPer; p0 < ctot; p0 += kPullBlock * kPullPer) {
+          u32 j = 0;
 #pragma unroll
-        for (int i = 0; i < kPullPer; i++) {
-          const u32 p = p0 + i;
-          col[i] = ~0u;
-          if (p < ctot) {
-            while (p >= jend) {  // next non-empty run
-              j++;
-              jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+          for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
+            if (sm.off[j + h] <= p0) j += h;
+          u32 jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+          u32 col[kPullPer], ar[kPullPer];
+#pragma unroll
+          for (int i = 0; i < kPullPer; i++) {
+            const u32 p = p0 + i;
+            col[i] = ~0u;
+            if (p < ctot) {
+              while (p >= jend) {  // next non-empty run
+                j++;
+                jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+              }
+              col[i] = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
+              ar[i] = sm.arow[j];
             }
-            col[i] = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
-            ar[i] = sm.arow[j];
+          }
+#pragma unroll
+          for (int i = 0; i < kPullPer; i++) {
+            if (col[i] == ~0u) continue;
+            if (col[i] < n_ids)
+              atomicOr(&acc[ar[i] + (col[i] >> 5)], 1u << (col[i] & 31));
+            else
+              atomicOr(&a.ctl->oob, 8192u);
           }
         }
-#pragma unroll
-        for (int i = 0; i < kPullPer; i++) {
-          if (col[i] == ~0u) continue;
-          if (col[i] < n_ids)
-            atomicOr(&acc[ar[i] + (col[i] >> 5)], 1u << (col[i] & 31));
-          else
-            atomicOr(&a.ctl->oob, 8192u);
-        }
+        cand += ctot;
+        __syncthreads();
       }
-      cand += ctot;
-      __syncthreads();
-    }
-    // flush the unit's rows: one reduction per nonzero word
-    for (u32 i = tid; i < acc_words; i += kPullBlock) {
-      const u32 v = acc[i];
-      if (v) {
-        const u64 gw = ((u64)r0 << rs) + i;
-        asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + gw), "r"(v) : "memory");
-        if (D) D[gw / kBmChunkWords] = 1;
-        acc[i] = 0;
-        flushed++;
+      // flush the unit's rows: one reduction per nonzero word
+      for (u32 i = tid; i < acc_words; i += kPullBlock) {
+        const u32 v = acc[i];
+        if (v) {
+          const u64 gw = ((u64)r0 << rs) + i;
+          asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + gw), "r"(v) : "memory");
+          if (D) D[gw / kBmChunkWords] = 1;
+          acc[i] = 0;
+          flushed++;
+        }
       }
     }
   }
