@@ -23,12 +23,13 @@
 //   k_join_pull_bm  a block per unit of 256 OT words (part of one row, or
 //                   several short rows), taken from a work counter (an
 //                   empty unit costs one barrier after the grab): lists
-//                   the unit's keys 256 at a time, probes the inner index
-//                   (one 16-byte slot per key), expands the runs balanced
-//                   over the block into the shared row (2 consecutive
-//                   candidates per thread, so a run is read in 16-byte
-//                   pieces), then ORs the row's nonzero words into the
-//                   output.
+//                   the unit's keys into shared memory (each thread those
+//                   of its word), takes them 256 at a time, probes the
+//                   inner index (one 16-byte slot per key), expands the
+//                   runs balanced over the block into the shared row (2
+//                   consecutive candidates per thread, so a run is read in
+//                   16-byte pieces), then ORs the row's nonzero words into
+//                   the output.
 //
 // The square domain only (ids below 2^dk, 8 <= dk <= 16; one instance).
 #pragma once
@@ -236,8 +237,7 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
 // Shared state of k_join_pull_bm.  The row accumulator is the dynamic
 // shared memory: pull_acc_words(dk) words.
 struct PullSmem {
-  u32 w[kPullUnit];         // the unit's OT words
-  u32 wpre[kPullUnit];      // exclusive bit offsets of the words
+  unsigned short keys[kPullUnit * 32];  // the unit's keys in order: word << 5 | bit
   u32 off[kPullBlock];      // exclusive candidate offsets of the round's keys
   u32 start[kPullBlock];    // inner run start of each key
   u32 arow[kPullBlock];     // accumulator offset of each key's output row
@@ -281,11 +281,13 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
       const u32 w0 = u * kPullUnit;  // below 2^27
       const u32 wv = OT[w0 + tid];
       if (!__syncthreads_or(wv != 0u)) continue;  // an empty unit: one barrier
-      sm.w[tid] = wv;
       u64 tot64;
-      sm.wpre[tid] = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
+      u32 pos = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
       const u32 tot = (u32)tot64;
       if (tot == 0) continue;  // block-uniform
+      // each thread lists its own word's keys in place (the unit's keys in
+      // order: word-major, then bit)
+      for (u32 x = wv; x; x &= x - 1) sm.keys[pos++] = (unsigned short)((tid << 5) | (__ffs(x) - 1));
       __syncthreads();
       keys += tot;
       const u32 r0 = w0 >> rs;  // first output row of the unit
@@ -293,13 +295,9 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
         const u32 q = q0 + tid;
         u32 len = 0, st = 0, arow = 0;
         if (q < tot) {
-          // the word holding key q: the last word whose offset is <= q
-          u32 k = 0;
-#pragma unroll
-          for (u32 h = kPullUnit / 2; h > 0; h >>= 1)
-            if (sm.wpre[k + h] <= q) k += h;
-          const u32 b = nth_set_bit(sm.w[k], q - sm.wpre[k]);
-          const u32 ow = w0 + k;  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
+          const u32 kb = sm.keys[q];
+          const u32 b = kb & 31u;
+          const u32 ow = w0 + (kb >> 5);  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
           arow = ((ow >> rs) - r0) << rs;
           len = index_probe(ix, ((ow & row_mask) << 5) + b, &st);
         }
