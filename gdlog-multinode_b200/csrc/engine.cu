@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -95,6 +96,8 @@ struct LieHost {
   bool reload_full = true;                 // include/lie.cuh:29
   bool trace_on = true;
   LieDev *d_lie = nullptr;
+  LieDev hdr{};                  // host copy of the header fields (not the copy-once flags)
+  u64 *d_trace = nullptr;        // the device trace rows
   JoinRec *d_joinrec = nullptr;  // [kMaxOps]
   std::vector<uint64_t> trace;   // 5 words per record
   double ms = 0;
@@ -210,6 +213,10 @@ struct gdl_engine {
   cudaEvent_t ev_first = nullptr;
   u64 kernels_launched = 0;
   bool broken = false;  // a bounded wait gave up or a bounds check fired
+  // The control block's build generation (index epochs), tracked on the
+  // host: set by reset_ctl and by every read of the control block after a
+  // loop ran, so setting up a loop needs no read-back.
+  u64 generation = 0;
   // Per-kernel accounting of fixpoint loops (gdl_engine_profile).  With
   // `profile` set, loops run launch by launch with an event pair around
   // every kernel instead of from the captured graph.
@@ -310,11 +317,12 @@ gdl_status pull(gdl_engine *e) {
   CK(e, cudaStreamSynchronize(e->s));
   return GDL_OK;
 }
+// The host mirror to the device, stream-ordered: a copy from pageable
+// memory is staged when the call returns, so the mirror may change at once.
 gdl_status push(gdl_engine *e) {
   if (e->rels.empty()) return GDL_OK;
   CK(e, cudaMemcpyAsync(e->d_rels, e->h.data(), e->rels.size() * sizeof(RelDev),
                         cudaMemcpyHostToDevice, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
   return GDL_OK;
 }
 
@@ -504,11 +512,8 @@ gdl_status ensure_dense_scratch(gdl_engine *e, u64 words) {
 // graph condition) keeping the build generation.
 gdl_status reset_ctl(gdl_engine *e) {
   Ctl c;
-  CK(e, cudaMemcpyAsync(&c, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
-  const u64 g = c.generation;
   memset(&c, 0, sizeof c);
-  c.generation = g + 1;
+  c.generation = ++e->generation;
   c.max_iteration = ~0ull;
   c.stop_at = ~0ull;
   CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
@@ -1169,22 +1174,6 @@ gdl_status validate_rel(gdl_engine *e, int r) {
 }
 
 
-gdl_status build_index_now(gdl_engine *e, int r, bool delta) {
-  RelDev &h = e->h[r];
-  DArr &a = delta ? h.delta : h.full;
-  Index &ix = delta ? h.delta_idx : h.full_idx;
-  Index &ixn = delta ? h.delta_idx_next : h.full_idx_next;
-  TRY(ensure_index(e, ix, a.cap));
-  TRY(ensure_index(e, ixn, delta ? h.delta_next.cap : h.full_next.cap));
-  TRY(push(e));
-  k_index_build<<<grid_for(e, a.n, kIndexBlock, 8), kIndexBlock, 0, e->s>>>(
-      delta ? &e->d_rels[r].delta : &e->d_rels[r].full,
-      delta ? &e->d_rels[r].delta_idx : &e->d_rels[r].full_idx, nullptr, e->d_ctl);
-  CK(e, cudaGetLastError());
-  TRY(pull(e));
-  return GDL_OK;
-}
-
 // The lists of a dense LIE at capacity `cap` rows each (and the indexes
 // some op probes on them).
 gdl_status presize_lists(gdl_engine *e, LieHost &L, const Plan &plan, u64 cap) {
@@ -1420,16 +1409,40 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     }
   }
   mark("delta_sort");
-  // Indexes every join of this LIE probes.
-  for (size_t r = 0; r < e->rels.size(); r++) {
-    if (plan.full_idx[r]) TRY(build_index_now(e, (int)r, false));
-    if (plan.delta_idx[r]) TRY(build_index_now(e, (int)r, true));
+  // Indexes every join of this LIE probes: sized, then built with one
+  // upload of the relation table (the builds take the epoch generation + 1,
+  // written into the host mirror here).
+  {
+    bool any = false;
+    const u32 epoch = (u32)(e->generation + 1);
+    for (size_t r = 0; r < e->rels.size(); r++)
+      for (int dv = 0; dv < 2; dv++) {
+        if (!(dv ? plan.delta_idx[r] : plan.full_idx[r])) continue;
+        RelDev &h = e->h[r];
+        TRY(ensure_index(e, dv ? h.delta_idx : h.full_idx, dv ? h.delta.cap : h.full.cap));
+        TRY(ensure_index(e, dv ? h.delta_idx_next : h.full_idx_next,
+                         dv ? h.delta_next.cap : h.full_next.cap));
+        (dv ? h.delta_idx : h.full_idx).epoch = epoch;
+        any = true;
+      }
+    if (any) {
+      TRY(push(e));
+      for (size_t r = 0; r < e->rels.size(); r++)
+        for (int dv = 0; dv < 2; dv++) {
+          if (!(dv ? plan.delta_idx[r] : plan.full_idx[r])) continue;
+          const RelDev &h = e->h[r];
+          k_index_build<<<grid_for(e, (dv ? h.delta : h.full).n, kIndexBlock, 8), kIndexBlock, 0,
+                          e->s>>>(dv ? &e->d_rels[r].delta : &e->d_rels[r].full,
+                                  dv ? &e->d_rels[r].delta_idx : &e->d_rels[r].full_idx, nullptr,
+                                  e->d_ctl);
+        }
+      CK(e, cudaGetLastError());
+    }
   }
   mark("indexes");
-  // Device LIE description.
-  LieDev ld;
-  CK(e, cudaMemcpyAsync(&ld, L.d_lie, sizeof(LieDev), cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
+  // Device LIE description: the header and the trace buffer (the copy-once
+  // flags stay as the device has them).
+  LieDev &ld = L.hdr;
   ld.n_update = (int)L.update.size();
   ld.n_static = (int)L.statics.size();
   ld.n_tmp = (int)L.tmps.size();
@@ -1439,15 +1452,14 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   for (size_t i = 0; i < L.tmps.size(); i++) ld.tmps[i] = L.tmps[i];
   // trace buffer: rows for one batch
   const u64 trace_rows = 256;
-  if (!ld.trace) TRY(dalloc(e, (void **)&ld.trace, trace_rows * kMaxRels * 3 * sizeof(u64)));
-  CK(e, cudaMemcpyAsync(L.d_lie, &ld, sizeof(LieDev), cudaMemcpyHostToDevice, e->s));
+  if (!L.d_trace) TRY(dalloc(e, (void **)&L.d_trace, trace_rows * kMaxRels * 3 * sizeof(u64)));
+  ld.trace = L.d_trace;
+  CK(e, cudaMemcpyAsync(L.d_lie, &ld, offsetof(LieDev, once), cudaMemcpyHostToDevice, e->s));
+  CK(e, cudaMemcpyAsync(&L.d_lie->trace, &ld.trace, sizeof(u64 *), cudaMemcpyHostToDevice, e->s));
   // Control block.
   Ctl c;
-  CK(e, cudaMemcpyAsync(&c, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
-  const u64 generation = c.generation;
   memset(&c, 0, sizeof c);
-  c.generation = generation + 1;
+  c.generation = ++e->generation;
   c.max_iteration = L.max_iteration < 0 ? 0 : (u64)L.max_iteration;
   c.trace_rows = trace_rows;
   L.trace.clear();
@@ -1541,6 +1553,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     CK(e, cudaStreamSynchronize(e->s));
     prof_collect(e);
     c = *e->h_ctl;
+    e->generation = c.generation;
     const u64 ran = c.iteration - it0;
     // In a graph, the body runs once per committed iteration plus once for
     // an iteration that overflowed (after a first iteration on the stream,
@@ -1616,6 +1629,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           CK(e, cudaStreamSynchronize(e->s));
           prof_collect(e);
           c = *e->h_ctl;
+          e->generation = c.generation;
           L.kernels += kc.total;
           for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += kc.kind[k];
           if (c.timeout || c.oob) {
