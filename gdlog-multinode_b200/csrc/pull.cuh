@@ -241,6 +241,9 @@ struct PullSmem {
   u32 off[kPullBlock];      // exclusive candidate offsets of the round's keys
   u32 start[kPullBlock];    // inner run start of each key
   u32 arow[kPullBlock];     // accumulator offset of each key's output row
+  u32 row_key[kPullBlock];  // the round's keys ORed as inner bitmap rows
+  u32 row_arow[kPullBlock];
+  u32 n_rows;
   u64 scan_tmp[kPullBlock / 32];
   long long unit;
 };
@@ -272,8 +275,15 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
   const u32 acc_words = pull_acc_words(dk);
   const u32 units = (u32)((1ull << (2 * dk - 5)) / kPullUnit);
   const u32 n_ids = 1u << dk;
+  // Row-OR (the inner is a FULL kept as a bitmap): a run of at least a
+  // quarter of a row is ORed from the inner's bitmap row instead of being
+  // expanded, 4 bytes a word read coalesced instead of a search, 8 bytes
+  // and a shared atomic per candidate.
+  const u32 *F = a.row_or ? a.inner_rd->bmF : nullptr;
+  const u32 row_min = max(64u, (1u << rs) >> 2);
   for (u32 i = tid; i < acc_words; i += kPullBlock) acc[i] = 0;
-  u64 cand = 0, keys = 0, flushed = 0;
+  if (tid == 0) sm.n_rows = 0;
+  u64 cand = 0, keys = 0, flushed = 0, row_words = 0;
   while (true) {
     const long long g = grab_tile(a.rec, &sm.unit);
     if (g * kPullGrab >= (long long)units) break;
@@ -299,7 +309,14 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
           const u32 b = kb & 31u;
           const u32 ow = w0 + (kb >> 5);  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
           arow = ((ow >> rs) - r0) << rs;
-          len = index_probe(ix, ((ow & row_mask) << 5) + b, &st);
+          const u32 key = ((ow & row_mask) << 5) + b;
+          len = index_probe(ix, key, &st);
+          if (F && len >= row_min) {
+            const u32 slot = atomicAdd(&sm.n_rows, 1u);
+            sm.row_key[slot] = key;
+            sm.row_arow[slot] = arow;
+            len = 0;
+          }
         }
         u64 ctot64;
         sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
@@ -342,6 +359,23 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
         }
         cand += ctot;
         __syncthreads();
+        if (F) {
+          // the round's row keys, after its candidates (plain ORs: each
+          // word of the shared row belongs to one thread)
+          const u32 nr = sm.n_rows;
+          __syncthreads();  // every thread has read the count
+          for (u32 i = 0; i < nr; i++) {
+            const u32 *src = F + ((u64)sm.row_key[i] << rs);
+            u32 *dst = acc + sm.row_arow[i];
+            for (u32 w = tid; w < (1u << rs); w += kPullBlock) {
+              const u32 v = src[w];
+              if (v) dst[w] |= v;
+            }
+          }
+          row_words += (u64)nr << rs;
+          if (tid == 0) sm.n_rows = 0;
+          __syncthreads();  // rows ORed, count reset before the next round's probes
+        }
       }
       // flush the unit's rows: one reduction per nonzero word
       for (u32 i = tid; i < acc_words; i += kPullBlock) {
@@ -359,9 +393,10 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) flushed += __shfl_xor_sync(0xffffffffu, flushed, o);
   // algorithmic bytes: 4 per OT word, 16 per key (its index slot), 8 per
-  // candidate (the inner tuple), 4 per word reduced into the output
+  // candidate (the inner tuple), 4 per inner bitmap word of a row-OR key,
+  // 4 per word reduced into the output
   if ((tid & 31) == 0) prof_add(a.ctl, kPJoinMat, 4 * flushed);
-  if (tid == 0) prof_add(a.ctl, kPJoinMat, 16 * keys + 8 * cand);
+  if (tid == 0) prof_add(a.ctl, kPJoinMat, 16 * keys + 8 * cand + 4 * row_words);
   if (launch_rec_finish(a.rec) && tid == 0) prof_add(a.ctl, kPJoinMat, 4ull * units * kPullUnit);
 }
 
