@@ -94,9 +94,11 @@ struct RelDev {
   u64 f_count;     // |FULL'| when the FULL list is not rebuilt every iteration
   u32 dense;       // the running LIE keeps this relation as bitmaps
   u32 full_lazy;   // FULL's list is materialised only when the LIE ends
-  // Transposed bitmaps read by pull-form joins (pull.cuh): DELTA (written
-  // by the update step) and NEWT (written before the join that reads it).
-  u32 *bmDT, *bmGT;
+  // Transposed bitmaps of pull-form joins (pull.cuh): DELTA (written by the
+  // update step) and NEWT (written before the join that reads it), read as
+  // outers; and NEWT's transposed twin that joins with a transposed output
+  // write (folded into NEWT after each such join, zero between them).
+  u32 *bmDT, *bmGT, *bmOT;
 };
 
 // Loop control of a running fixpoint (one per engine, device memory).

@@ -479,7 +479,7 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   RelHost &rh = e->rels[r];
   RelDev &h = e->h[r];
   if (rh.bm_words != words) {
-    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT}) {
+    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT, &h.bmOT}) {
       dfree(e, *p);
       *p = nullptr;
     }
@@ -621,6 +621,8 @@ struct Plan {
   std::vector<char> newt_list;            // NEWT read as a join outer
   std::vector<char> acopy_src;            // NEWT read by an ACopy
   std::vector<char> pull;                 // per op: pull form (pull.cuh)
+  std::vector<char> pull_t;               // per op: pull form with a transposed output
+  std::vector<char> out_t;                // per relation: written by such an op
   std::vector<char> delta_t, newt_t;      // per relation: transposed DELTA / NEWT read
   std::vector<char> delta_list;           // per relation: DELTA read as a list by some op
 };
@@ -634,6 +636,8 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.newt_list.assign(n, 0);
   p.acopy_src.assign(n, 0);
   p.pull.assign(L.ops.size(), 0);
+  p.pull_t.assign(L.ops.size(), 0);
+  p.out_t.assign(n, 0);
   p.delta_t.assign(n, 0);
   p.newt_t.assign(n, 0);
   p.delta_list.assign(n, 0);
@@ -676,11 +680,19 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (op.kind != 0) continue;
-    const bool shape = !op.generic && op.pred.kind == 0 && op.sel.s0 == 3 && op.sel.s1 == 1;
+    // (outer column 1, inner column 1), or its transpose (inner column 1,
+    // outer column 1): gathered into a transposed twin of the output
+    const bool plain = !op.generic && op.pred.kind == 0;
+    const bool fwd = plain && op.sel.s0 == 3 && op.sel.s1 == 1;
+    const bool rev = plain && op.sel.s0 == 1 && op.sel.s1 == 3;
     const bool outer_ok = (op.outer_ver == GDL_DELTA && is_update[op.outer]) ||
                           (op.outer_ver == GDL_NEWT && is_tmp[op.outer]);
-    if (shape && outer_ok) {
+    if ((fwd || rev) && outer_ok) {
       p.pull[oi] = 1;
+      if (rev) {
+        p.pull_t[oi] = 1;
+        p.out_t[op.out] = 1;
+      }
       (op.outer_ver == GDL_DELTA ? p.delta_t : p.newt_t)[op.outer] = 1;
     } else if (op.outer_ver == GDL_NEWT) {
       p.newt_list[op.outer] = 1;
@@ -706,6 +718,7 @@ gdl_status ensure_tbitmaps(gdl_engine *e, const Plan &p, int r, u64 words) {
   RelDev &h = e->h[r];
   if (p.delta_t[r] && !h.bmDT) TRY(dalloc(e, (void **)&h.bmDT, words * 4));
   if (p.newt_t[r] && !h.bmGT) TRY(dalloc(e, (void **)&h.bmGT, words * 4));
+  if (p.out_t[r] && !h.bmOT) TRY(dalloc(e, (void **)&h.bmOT, words * 4));
   return GDL_OK;
 }
 
@@ -861,10 +874,18 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
           OT = oh.bmGT;
         }
         a.rec = &e->recs[6];
+        // row-OR: the gathered row is the inner's column 1 in both
+        // orientations
+        a.row_or = e->row_or_joins && op.inner_ver != GDL_DELTA && e->h[op.inner].dense &&
+                   e->h[op.inner].bmF;
+        const RelDev &out = e->h[op.out];
         PLAUNCH(kc, kPJoinMat,
-                k_join_pull_bm<<<(int)e->sms * 8, kPullBlock,
-                                 pull_acc_words(L.dk) * 4, s>>>(
-                    a, &R[op.out], OT, L.dk));
+                k_join_pull_bm<<<(int)e->sms * 8, kPullBlock, pull_acc_words(L.dk) * 4, s>>>(
+                    a, plan.pull_t[oi] ? out.bmOT : out.bmG,
+                    plan.pull_t[oi] ? nullptr : out.dirty, OT, L.dk));
+        if (plan.pull_t[oi])
+          PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
+                                    out.bmOT, out.bmG, out.dirty, L.dk, e->d_ctl));
         continue;
       }
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
@@ -1382,6 +1403,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmChunkWords, e->s));
     }
+    for (auto *v : {&L.update, &L.tmps})
+      for (int r : *v)
+        if (plan.out_t[r]) CK(e, cudaMemsetAsync(e->h[r].bmOT, 0, words * 4, e->s));
     CK(e, cudaGetLastError());
   }
   mark("bitmaps");
@@ -1884,7 +1908,7 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
-    for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT})
+    for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT, r.bmOT})
       if (bm) cudaFreeAsync(bm, e->s);
     if (r.bmD) cudaFreeAsync(r.bmD, e->s);
     if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);

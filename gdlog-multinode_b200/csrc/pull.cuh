@@ -31,6 +31,11 @@
 //                   16-byte pieces), then ORs the row's nonzero words into
 //                   the output.
 //
+//   k_bm_fold_t     for a join whose output is (inner column 1, outer
+//                   column 1): the same kernel gathers by the outer's
+//                   column 1 into a transposed twin of the output NEWT,
+//                   which this pass ORs into NEWT transposed and clears.
+//
 // The square domain only (ids below 2^dk, 8 <= dk <= 16; one instance).
 #pragma once
 
@@ -254,8 +259,11 @@ __host__ __device__ __forceinline__ u32 pull_acc_words(int dk) {
   return 1u << (dk - 5 > 8 ? dk - 5 : 8);
 }
 
-__global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, const RelDev *out_rd,
-                                                            const u32 *OT, int dk) {
+// G / D: the output bitmap and its dirty map (or null): the output
+// relation's NEWT, or its transposed twin for a join whose output is
+// (inner column 1, outer column 1).
+__global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, u32 *G, u8 *D,
+                                                               const u32 *OT, int dk) {
   __shared__ PullSmem sm;
   extern __shared__ u32 acc[];
   if (ctl_stop(a.ctl)) return;
@@ -265,8 +273,6 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
     join_empty_side(a, n_outer);
     return;
   }
-  u32 *G = out_rd->bmG;
-  u8 *D = out_rd->dirty;
   const Index ix = *a.inner_idx;
   const u64 *inner = a.inner->ptr;
   const int tid = threadIdx.x;
@@ -398,6 +404,54 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, cons
   if ((tid & 31) == 0) prof_add(a.ctl, kPJoinMat, 4 * flushed);
   if (tid == 0) prof_add(a.ctl, kPJoinMat, 16 * keys + 8 * cand + 4 * row_words);
   if (launch_rec_finish(a.rec) && tid == 0) prof_add(a.ctl, kPJoinMat, 4ull * units * kPullUnit);
+}
+
+// dst |= transpose(src), src cleared: the transposed output of the joins
+// whose output is (inner column 1, outer column 1), folded into the output
+// relation's NEWT (and its dirty map) after each such join.  Every word of
+// dst comes from one tile of src, so the ORs need no atomics.
+__global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *dirty, int dk,
+                                                        Ctl *ctl) {
+  __shared__ u32 s_t[256][9];
+  if (ctl_stop(ctl)) return;
+  const int rs = dk - 5;
+  const u64 per = 1ull << (dk - 8);
+  const u64 tiles = per * per;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u64 moved = 0;
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const u64 tr = t / per, tc = t % per;
+    const u64 at = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
+    u32 v[8];
+    load8(src + at, v);
+    const bool any = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
+    moved += 4 * 8;
+    if (any) {
+      uint4 *ps = reinterpret_cast<uint4 *>(src + at);
+      ps[0] = make_uint4(0, 0, 0, 0);
+      ps[1] = make_uint4(0, 0, 0, 0);
+      moved += 4 * 8;
+    }
+    if (!__syncthreads_or(any)) continue;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+    __syncthreads();
+    const u32 *q = s_t[threadIdx.x];
+    if ((q[0] | q[1] | q[2] | q[3] | q[4] | q[5] | q[6] | q[7]) != 0u) {
+      const u64 dw = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
+      u32 d[8];
+      load8(dst + dw, d);
+      uint4 *pd = reinterpret_cast<uint4 *>(dst + dw);
+      pd[0] = make_uint4(d[0] | q[0], d[1] | q[1], d[2] | q[2], d[3] | q[3]);
+      pd[1] = make_uint4(d[4] | q[4], d[5] | q[5], d[6] | q[6], d[7] | q[7]);
+      if (dirty) dirty[dw / kBmChunkWords] = 1;
+      moved += 8 * 8;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(0xffffffffu, moved, o);
+  if (lane == 0) prof_add(ctl, kPBitmap, moved);
 }
 
 // Set the transposed bits (c1, c0) of a key list (DELTA at the start of a

@@ -13,7 +13,7 @@ import pytest
 
 import programs as P
 import workloads as W
-from gdlog_b200 import DELTA, FULL, INNER, NEWT, OUTER, Engine
+from gdlog_b200 import DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, Engine
 
 pytestmark = pytest.mark.gpu
 
@@ -42,6 +42,18 @@ def test_sg_pull_matches_push_and_oracle(scale, edges):
     e = W.rmat_edges(scale, edges, seed=scale)
     assert int(e.max()) >= 1 << (scale - 1)
     pull, push, want = three_ways(P.sg, e)
+    assert pull == want
+    assert push == want
+
+
+@pytest.mark.parametrize("case", ["grid_24", "dag_L30_W40", "rmat_s11"])
+def test_tc_transposed_output_matches_push_and_oracle(case):
+    """TC's join (edge FULL, path DELTA, output (inner 1, outer 1)) in the
+    pull form with a transposed output folded into NEWT."""
+    e = {"grid_24": lambda: W.grid_edges(24, 24),
+         "dag_L30_W40": lambda: W.layered_dag(30, 40, 2),
+         "rmat_s11": lambda: W.rmat_edges(11, 3000, seed=5)}[case]()
+    pull, push, want = three_ways(P.tc, e)
     assert pull == want
     assert push == want
 
@@ -80,8 +92,8 @@ def test_cspa_1000_pull_equals_push():
 def pull_quirks(eng, sync=None):
     """Pull-shaped joins at the reference's edges: an empty inner zeroes the
     outer's count (src/join.cu:38-45), for a DELTA and for a tmp NEWT outer;
-    one tmp NEWT read by two pull joins and by a push join; ids >= 256 so
-    the dense form runs over 2^9 ids."""
+    one tmp NEWT read by pull joins of both orientations and by a push join;
+    ids >= 256 so the dense form runs over 2^9 ids."""
     rng = np.random.default_rng(5)
     base = rng.integers(0, 400, size=(300, 2)).astype(np.uint64)
     a = eng.relation("a")
@@ -104,8 +116,13 @@ def pull_quirks(eng, sync=None):
     lie.add_join(e, FULL, a, DELTA, t, (OUTER(1), INNER(1)))
     # a(y, z) :- t(x, y), e(x, z)         (pull: tmp NEWT outer)
     lie.add_join(e, FULL, t, NEWT, a, (OUTER(1), INNER(1)))
-    # c(z, y) :- t(x, y), e(x, z)         (push: same tmp NEWT outer)
+    # c(z, y) :- t(x, y), e(x, z)         (pull, transposed output: same tmp NEWT)
     lie.add_join(e, FULL, t, NEWT, c, (INNER(1), OUTER(1)))
+    # c(z, y) :- t(x, y), e(x, z), z != y  (push: a predicate)
+    lie.add_join(e, FULL, t, NEWT, c, (INNER(1), OUTER(1)), pred=(PRED_NE, 0, 1))
+    # a(z, y) :- a(x, y), a(x, z)         (pull, transposed output; FULL inner
+    #                                      of an update relation: row-OR)
+    lie.add_join(a, FULL, a, DELTA, a, (INNER(1), OUTER(1)))
     # c(y, z) :- t(x, y), b(x, z)         (pull, empty inner: t's count zeroed)
     lie.add_join(b, FULL, t, NEWT, c, (OUTER(1), INNER(1)))
     # c(y, z) :- t(x, y), e(x, z)         (pull: sees t emptied)
