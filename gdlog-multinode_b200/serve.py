@@ -23,6 +23,12 @@ same-generation queries grows fast); a batch the engine refuses for size
 (GDL_E_UNSUPPORTED list limit, GDL_E_NOMEM) is split in halves and each half
 run again, down to single queries.
 
+A same-generation query on 2^12 or more nodes is served alone through the
+plain engine instead (`plain_min_nodes`): there its joins run gathered by
+output row (pull form, csrc/pull.cuh), which the block-diagonal batched
+layout does not have, and a large query no longer sets the pace of a batch
+of small ones.
+
 The plain baseline serves the same stream one query at a time through the
 plain (unbatched) engine.  Both report p50 / p99 latency (finish - arrival)
 and throughput, and every query's result (size, digest of its sorted tuples
@@ -117,8 +123,9 @@ def percentiles(lat):
 
 class Server:
     def __init__(self, slots=2, budget_bytes=24 << 30, max_batch=256, batched=True, device=0,
-                 tuple_cap=1 << 29):
+                 tuple_cap=1 << 29, plain_min_nodes=1 << 12):
         self.slots = slots
+        self.plain_min_nodes = plain_min_nodes
         self.budget = budget_bytes
         self.tuple_cap = tuple_cap
         self.max_batch = max_batch
@@ -137,12 +144,12 @@ class Server:
         if not self.queue:
             return []
         kind = self.queue[0].kind
-        if not self.batched:
+        if not self.batched or self._alone(self.queue[0]):
             return [self.queue.popleft()]
         take, used, tuples, keep = [], 0, 0, collections.deque()
         while self.queue:
             r = self.queue.popleft()
-            if (r.kind == kind and len(take) < self.max_batch
+            if (r.kind == kind and not self._alone(r) and len(take) < self.max_batch
                     and (not take or (used + r.est_bytes <= self.budget
                                       and tuples + r.est_tuples <= self.tuple_cap))):
                 take.append(r)
@@ -152,6 +159,10 @@ class Server:
                 keep.append(r)
         self.queue = keep
         return take
+
+    def _alone(self, r) -> bool:
+        """Served alone through the plain engine (see the module docstring)."""
+        return r.kind == "sg" and self.plain_min_nodes and r.nodes >= self.plain_min_nodes
 
     def _worker(self, t0):
         try:
@@ -190,7 +201,7 @@ class Server:
     def _run(self, eng, prog, reqs) -> list:
         """Results of one batch (or, unbatched, of each query in turn); a
         batch refused for its size is split in halves."""
-        if not self.batched:
+        if not self.batched or (len(reqs) == 1 and self._alone(reqs[0])):
             return B.run_plain_loop(eng, prog, [r.inputs for r in reqs]).results
         try:
             return B.run_batched(eng, prog, [r.inputs for r in reqs],
@@ -248,10 +259,13 @@ def main():
     ap.add_argument("--max-scale", type=int, default=14)
     ap.add_argument("--plain", action="store_true", help="serve one query at a time, unbatched")
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--plain-min-scale", type=int, default=12,
+                    help="SG queries on 2^this nodes or more run alone, unbatched (0: never)")
     a = ap.parse_args()
     reqs = make_stream(a.requests, a.rate, seed=a.seed, max_scale=a.max_scale)
     srv = Server(slots=1 if a.plain else a.slots, budget_bytes=int(a.budget_gb * (1 << 30)),
-                 batched=not a.plain)
+                 batched=not a.plain,
+                 plain_min_nodes=(1 << a.plain_min_scale) if a.plain_min_scale else 0)
     stats = srv.serve(reqs)
     stats.update({"mode": "plain" if a.plain else "batched", "rate": a.rate,
                   "slots": srv.slots})

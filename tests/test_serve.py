@@ -48,11 +48,30 @@ def test_take_batches_one_kind_within_budget():
     assert len(srv.queue) == len(reqs) - len(first)
 
 
+def test_large_sg_queries_are_taken_alone():
+    """A same-generation query on plain_min_nodes nodes or more is served
+    alone (plain engine); no batch holds one with other queries."""
+    reqs = S.make_stream(60, rate=2000.0, seed=4, min_scale=10, max_scale=13, l_range=(3, 9),
+                         w_range=(3, 9))
+    assert any(r.kind == "sg" and r.nodes >= 1 << 12 for r in reqs)
+    srv = S.Server(slots=1, budget_bytes=1 << 40, max_batch=64, plain_min_nodes=1 << 12)
+    srv.queue.extend(reqs)
+    sizes = []
+    while srv.queue:
+        batch = srv._take()
+        big = [r for r in batch if r.kind == "sg" and r.nodes >= 1 << 12]
+        assert not big or len(batch) == 1
+        sizes.append(len(batch))
+    assert max(sizes) > 1
+
+
 @pytest.mark.gpu
-def test_results_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("plain_min_nodes", [0, 1 << 6])
+def test_results_same_alone_and_in_the_mix(plain_min_nodes):
     reqs = small_stream()
     mixed = copy.deepcopy(reqs)
-    stats = S.Server(slots=2, budget_bytes=1 << 30, max_batch=16).serve(mixed)
+    stats = S.Server(slots=2, budget_bytes=1 << 30, max_batch=16,
+                     plain_min_nodes=plain_min_nodes).serve(mixed)
     assert stats["requests"] == len(reqs)
     assert stats["mean_batch"] > 1.0  # arrivals overlap, so queries were batched
     with Engine("gpu") as g:
