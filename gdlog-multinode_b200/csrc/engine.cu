@@ -623,6 +623,7 @@ struct Plan {
   std::vector<char> pull;                 // per op: pull form (pull.cuh)
   std::vector<char> pull_t;               // per op: pull form with a transposed output
   std::vector<char> out_t;                // per relation: written by such an op
+  std::vector<char> fold_late;            // per relation: its transposed twin is its NEWT
   std::vector<char> delta_t, newt_t;      // per relation: transposed DELTA / NEWT read
   std::vector<char> delta_list;           // per relation: DELTA read as a list by some op
 };
@@ -638,6 +639,7 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.pull.assign(L.ops.size(), 0);
   p.pull_t.assign(L.ops.size(), 0);
   p.out_t.assign(n, 0);
+  p.fold_late.assign(n, 0);
   p.delta_t.assign(n, 0);
   p.newt_t.assign(n, 0);
   p.delta_list.assign(n, 0);
@@ -655,6 +657,12 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
     }
   }
   return p;
+}
+
+// The update step of relation r is one fused pass (pull.cuh, k_bm_update_t):
+// its DELTA is read only transposed and its FULL not as a list.
+bool fused_update(const Plan &p, int r) {
+  return p.delta_t[r] && !p.delta_list[r] && !p.full_list[r];
 }
 
 // Pull-form joins (pull.cuh), decided once the LIE's dense form is known: a
@@ -705,12 +713,17 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
   for (int r : L.update)
     if (!p.delta_list[r]) p.delta_t[r] = 1;
-}
-
-// The update step of relation r is one fused pass (pull.cuh, k_bm_update_t):
-// its DELTA is read only transposed and its FULL not as a list.
-bool fused_update(const Plan &p, int r) {
-  return p.delta_t[r] && !p.delta_list[r] && !p.full_list[r];
+  // A relation written only by transposed-output joins, whose NEWT no op
+  // reads and whose update step is the fused pass, keeps NEWT as the
+  // transposed twin: no fold after each join, the update reads it.
+  for (int r : L.update) {
+    if (!p.out_t[r] || !fused_update(p, r) || p.newt_list[r] || p.newt_t[r] || p.acopy_src[r])
+      continue;
+    bool only_t = true;
+    for (size_t oi = 0; oi < L.ops.size(); oi++)
+      if (L.ops[oi].out == r && !p.pull_t[oi]) only_t = false;
+    p.fold_late[r] = only_t;
+  }
 }
 
 // Transposed bitmaps of the relations pull-form joins read.
@@ -883,7 +896,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
                 k_join_pull_bm<<<(int)e->sms * 8, kPullBlock, pull_acc_words(L.dk) * 4, s>>>(
                     a, plan.pull_t[oi] ? out.bmOT : out.bmG,
                     plan.pull_t[oi] ? nullptr : out.dirty, OT, L.dk));
-        if (plan.pull_t[oi])
+        if (plan.pull_t[oi] && !plan.fold_late[op.out])
           PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
                                     out.bmOT, out.bmG, out.dirty, L.dk, e->d_ctl));
         continue;
@@ -1038,7 +1051,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       const int r = (int)(a.rd - R);
       const u64 side = 1ull << (L.dk - kPullMinBits);
       PLAUNCH(kc, kPBitmap, k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                a, e->h[r].bmDT, L.dk));
+                                a, e->h[r].bmDT, L.dk, plan.fold_late[r] ? e->h[r].bmOT : nullptr));
     }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)

@@ -154,8 +154,11 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
 // DELTA = G & ~F counted and written transposed into dt, F |= G and G
 // cleared where G has bits, NEWT's size counted.  Behind the write passes'
 // capacity gate: when another relation's list is too small nothing is
-// written and the update step runs again after the lists grow.
-__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk) {
+// written and the update step runs again after the lists grow.  gt: when
+// every join that writes the relation has a transposed output and nothing
+// reads its NEWT during the iteration, NEWT is only that transposed twin
+// (never folded): it is read transposed, tile by tile, and cleared.
+__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk, u32 *gt) {
   __shared__ u32 s_t[256][9];
   __shared__ unsigned long long s_cnt[2];
   if (ctl_stop(a.ctl)) return;
@@ -173,9 +176,35 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
     const u64 tr = t / per, tc = t % per;
     const u64 src = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
     u32 g[8], d[8];
-    load8(G + src, g);
+    if (gt) {
+      // NEWT's tile (tr, tc) is the transpose of gt's tile (tc, tr)
+      const u64 tsrc = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
+      u32 v[8];
+      load8(gt + tsrc, v);
+      const bool any_v = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
+      moved += 32;
+      if (any_v) {
+        uint4 *pv = reinterpret_cast<uint4 *>(gt + tsrc);
+        pv[0] = make_uint4(0, 0, 0, 0);
+        pv[1] = make_uint4(0, 0, 0, 0);
+        moved += 32;
+      }
+      if (__syncthreads_or(any_v)) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 8; i++) g[i] = s_t[threadIdx.x][i];
+        __syncthreads();
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) g[i] = 0;
+      }
+    } else {
+      load8(G + src, g);
+      moved += 32;
+    }
     const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
-    moved += 32;
     bool any = false;
 #pragma unroll
     for (int i = 0; i < 8; i++) d[i] = 0;
@@ -185,10 +214,12 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
       uint4 *pf = reinterpret_cast<uint4 *>(F + src);
       pf[0] = make_uint4(f[0] | g[0], f[1] | g[1], f[2] | g[2], f[3] | g[3]);
       pf[1] = make_uint4(f[4] | g[4], f[5] | g[5], f[6] | g[6], f[7] | g[7]);
-      uint4 *pg = reinterpret_cast<uint4 *>(G + src);
-      pg[0] = make_uint4(0, 0, 0, 0);
-      pg[1] = make_uint4(0, 0, 0, 0);
-      moved += 96;
+      if (!gt) {
+        uint4 *pg = reinterpret_cast<uint4 *>(G + src);
+        pg[0] = make_uint4(0, 0, 0, 0);
+        pg[1] = make_uint4(0, 0, 0, 0);
+      }
+      moved += gt ? 64 : 96;
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         d[i] = g[i] & ~f[i];
