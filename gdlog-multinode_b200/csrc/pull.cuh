@@ -50,7 +50,6 @@ constexpr int kTrBlock = 256;
 constexpr int kPullBlock = 256;
 constexpr int kPullUnit = 256;   // OT words per unit of work (a word per thread): 8192 keys
 constexpr int kPullPer = 2;      // consecutive candidates per thread and step
-constexpr int kPullGrab = 1;     // units taken from the work counter at a time
 constexpr int kPullMinBits = 8;  // a transposed tile is 256 ids square
 constexpr int kPullAutoBits = 12;  // the pull form by default from 2^12 ids on
 
@@ -323,107 +322,106 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, u32 
   u64 cand = 0, keys = 0, flushed = 0, row_words = 0;
   while (true) {
     const long long g = grab_tile(a.rec, &sm.unit);
-    if (g * kPullGrab >= (long long)units) break;
-    for (u32 u = (u32)g * kPullGrab; u < min(units, (u32)(g + 1) * kPullGrab); u++) {
-      const u32 w0 = u * kPullUnit;  // below 2^27
-      const u32 wv = OT[w0 + tid];
-      if (!__syncthreads_or(wv != 0u)) continue;  // an empty unit: one barrier
-      u64 tot64;
-      u32 pos = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
-      const u32 tot = (u32)tot64;
-      if (tot == 0) continue;  // block-uniform
-      // each thread lists its own word's keys in place (the unit's keys in
-      // order: word-major, then bit)
-      for (u32 x = wv; x; x &= x - 1) sm.keys[pos++] = (unsigned short)((tid << 5) | (__ffs(x) - 1));
-      __syncthreads();
-      keys += tot;
-      const u32 r0 = w0 >> rs;  // first output row of the unit
-      for (u32 q0 = 0; q0 < tot; q0 += kPullBlock) {
-        const u32 q = q0 + tid;
-        u32 len = 0, st = 0, arow = 0;
-        if (q < tot) {
-          const u32 kb = sm.keys[q];
-          const u32 b = kb & 31u;
-          const u32 ow = w0 + (kb >> 5);  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
-          arow = ((ow >> rs) - r0) << rs;
-          const u32 key = ((ow & row_mask) << 5) + b;
-          len = index_probe(ix, key, &st);
-          if (F && len >= row_min) {
-            const u32 slot = atomicAdd(&sm.n_rows, 1u);
-            sm.row_key[slot] = key;
-            sm.row_arow[slot] = arow;
-            len = 0;
-          }
-        }
-        u64 ctot64;
-        sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
-        const u32 ctot = (u32)ctot64;  // at most 256 runs of at most 2^16
-        sm.start[tid] = st;
-        sm.arow[tid] = arow;
-        __syncthreads();
-        // kPullPer consecutive candidates per thread: one search for the
-        // first (the last key whose offset is <= p; an empty run shares its
-        // offset with the next key, so it is never the last), then walked
-        // forward; the loads are issued before the ORs
-        for (u32 p0 = tid * kPullPer; p0 < ctot; p0 += kPullBlock * kPullPer) {
-          u32 j = 0;
-#pragma unroll
-          for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
-            if (sm.off[j + h] <= p0) j += h;
-          u32 jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
-          u32 col[kPullPer], ar[kPullPer];
-#pragma unroll
-          for (int i = 0; i < kPullPer; i++) {
-            const u32 p = p0 + i;
-            col[i] = ~0u;
-            if (p < ctot) {
-              while (p >= jend) {  // next non-empty run
-                j++;
-                jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
-              }
-              col[i] = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
-              ar[i] = sm.arow[j];
-            }
-          }
-#pragma unroll
-          for (int i = 0; i < kPullPer; i++) {
-            if (col[i] == ~0u) continue;
-            if (col[i] < n_ids)
-              atomicOr(&acc[ar[i] + (col[i] >> 5)], 1u << (col[i] & 31));
-            else
-              atomicOr(&a.ctl->oob, 8192u);
-          }
-        }
-        cand += ctot;
-        __syncthreads();
-        if (F) {
-          // the round's row keys, after its candidates (plain ORs: each
-          // word of the shared row belongs to one thread)
-          const u32 nr = sm.n_rows;
-          __syncthreads();  // every thread has read the count
-          for (u32 i = 0; i < nr; i++) {
-            const u32 *src = F + ((u64)sm.row_key[i] << rs);
-            u32 *dst = acc + sm.row_arow[i];
-            for (u32 w = tid; w < (1u << rs); w += kPullBlock) {
-              const u32 v = src[w];
-              if (v) dst[w] |= v;
-            }
-          }
-          row_words += (u64)nr << rs;
-          if (tid == 0) sm.n_rows = 0;
-          __syncthreads();  // rows ORed, count reset before the next round's probes
+    if (g >= (long long)units) break;
+    const u32 u = (u32)g;
+    const u32 w0 = u * kPullUnit;  // below 2^27
+    const u32 wv = OT[w0 + tid];
+    if (!__syncthreads_or(wv != 0u)) continue;  // an empty unit: one barrier
+    u64 tot64;
+    u32 pos = (u32)block_excl_scan<kPullBlock>((u64)__popc(wv), sm.scan_tmp, &tot64);
+    const u32 tot = (u32)tot64;
+    if (tot == 0) continue;  // block-uniform
+    // each thread lists its own word's keys in place (the unit's keys in
+    // order: word-major, then bit)
+    for (u32 x = wv; x; x &= x - 1) sm.keys[pos++] = (unsigned short)((tid << 5) | (__ffs(x) - 1));
+    __syncthreads();
+    keys += tot;
+    const u32 r0 = w0 >> rs;  // first output row of the unit
+    for (u32 q0 = 0; q0 < tot; q0 += kPullBlock) {
+      const u32 q = q0 + tid;
+      u32 len = 0, st = 0, arow = 0;
+      if (q < tot) {
+        const u32 kb = sm.keys[q];
+        const u32 b = kb & 31u;
+        const u32 ow = w0 + (kb >> 5);  // OT word: row ow >> rs, keys 32 (ow & row_mask) ..
+        arow = ((ow >> rs) - r0) << rs;
+        const u32 key = ((ow & row_mask) << 5) + b;
+        len = index_probe(ix, key, &st);
+        if (F && len >= row_min) {
+          const u32 slot = atomicAdd(&sm.n_rows, 1u);
+          sm.row_key[slot] = key;
+          sm.row_arow[slot] = arow;
+          len = 0;
         }
       }
-      // flush the unit's rows: one reduction per nonzero word
-      for (u32 i = tid; i < acc_words; i += kPullBlock) {
-        const u32 v = acc[i];
-        if (v) {
-          const u64 gw = ((u64)r0 << rs) + i;
-          asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + gw), "r"(v) : "memory");
-          if (D) D[gw / kBmChunkWords] = 1;
-          acc[i] = 0;
-          flushed++;
+      u64 ctot64;
+      sm.off[tid] = (u32)block_excl_scan<kPullBlock>((u64)len, sm.scan_tmp, &ctot64);
+      const u32 ctot = (u32)ctot64;  // at most 256 runs of at most 2^16
+      sm.start[tid] = st;
+      sm.arow[tid] = arow;
+      __syncthreads();
+      // kPullPer consecutive candidates per thread: one search for the
+      // first (the last key whose offset is <= p; an empty run shares its
+      // offset with the next key, so it is never the last), then walked
+      // forward; the loads are issued before the ORs
+      for (u32 p0 = tid * kPullPer; p0 < ctot; p0 += kPullBlock * kPullPer) {
+        u32 j = 0;
+#pragma unroll
+        for (u32 h = kPullBlock / 2; h > 0; h >>= 1)
+          if (sm.off[j + h] <= p0) j += h;
+        u32 jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+        u32 col[kPullPer], ar[kPullPer];
+#pragma unroll
+        for (int i = 0; i < kPullPer; i++) {
+          const u32 p = p0 + i;
+          col[i] = ~0u;
+          if (p < ctot) {
+            while (p >= jend) {  // next non-empty run
+              j++;
+              jend = j + 1 < kPullBlock ? sm.off[j + 1] : ctot;
+            }
+            col[i] = key_c1(inner[sm.start[j] + (p - sm.off[j])]);
+            ar[i] = sm.arow[j];
+          }
         }
+#pragma unroll
+        for (int i = 0; i < kPullPer; i++) {
+          if (col[i] == ~0u) continue;
+          if (col[i] < n_ids)
+            atomicOr(&acc[ar[i] + (col[i] >> 5)], 1u << (col[i] & 31));
+          else
+            atomicOr(&a.ctl->oob, 8192u);
+        }
+      }
+      cand += ctot;
+      __syncthreads();
+      if (F) {
+        // the round's row keys, after its candidates (plain ORs: each
+        // word of the shared row belongs to one thread)
+        const u32 nr = sm.n_rows;
+        __syncthreads();  // every thread has read the count
+        for (u32 i = 0; i < nr; i++) {
+          const u32 *src = F + ((u64)sm.row_key[i] << rs);
+          u32 *dst = acc + sm.row_arow[i];
+          for (u32 w = tid; w < (1u << rs); w += kPullBlock) {
+            const u32 v = src[w];
+            if (v) dst[w] |= v;
+          }
+        }
+        row_words += (u64)nr << rs;
+        if (tid == 0) sm.n_rows = 0;
+        __syncthreads();  // rows ORed, count reset before the next round's probes
+      }
+    }
+    // flush the unit's rows: one reduction per nonzero word
+    for (u32 i = tid; i < acc_words; i += kPullBlock) {
+      const u32 v = acc[i];
+      if (v) {
+        const u64 gw = ((u64)r0 << rs) + i;
+        asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + gw), "r"(v) : "memory");
+        if (D) D[gw / kBmChunkWords] = 1;
+        acc[i] = 0;
+        flushed++;
       }
     }
   }
