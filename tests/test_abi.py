@@ -80,3 +80,22 @@ def test_null_arguments_rejected():
     assert lib.gdl_lie_fixpoint(None, 0, None) == 1
     msg = lib.gdl_last_error(None)
     assert msg
+
+
+def test_tuning_struct_matches_the_header(tmp_path):
+    """gdl_tuning as the C compiler lays it out (include/gdlog_b200.h) and
+    the ctypes mirror the binding passes to gdl_engine_set_tuning agree
+    field by field."""
+    fields = [f for f, _ in G.Tuning._fields_]
+    src = tmp_path / "t.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"gdlog_b200.h\"\n"
+                   "int main(void) {\n  printf(\"%zu\\n\", sizeof(gdl_tuning));\n"
+                   + "".join(f"  printf(\"%zu\\n\", offsetof(gdl_tuning, {f}));\n" for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "t"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(REPO, "include"), str(src), "-o",
+                    str(exe)], check=True)
+    vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                           check=True).stdout.split()]
+    assert vals[0] == C.sizeof(G.Tuning)
+    assert vals[1:] == [getattr(G.Tuning, f).offset for f in fields]
