@@ -217,6 +217,10 @@ struct gdl_engine {
   // host: set by reset_ctl and by every read of the control block after a
   // loop ran, so setting up a loop needs no read-back.
   u64 generation = 0;
+  // The host mirror `h` equals the device relation table: set by a pull and
+  // by the last push of a load or a fixpoint, cleared before the kernels
+  // that change the table run, so reads need no round trip when it is set.
+  bool mirror_fresh = false;
   // Per-kernel accounting of fixpoint loops (gdl_engine_profile).  With
   // `profile` set, loops run launch by launch with an event pair around
   // every kernel instead of from the captured graph.
@@ -315,8 +319,11 @@ gdl_status pull(gdl_engine *e) {
   CK(e, cudaMemcpyAsync(e->h.data(), e->d_rels, e->rels.size() * sizeof(RelDev),
                         cudaMemcpyDeviceToHost, e->s));
   CK(e, cudaStreamSynchronize(e->s));
+  e->mirror_fresh = true;
   return GDL_OK;
 }
+// pull() unless the mirror is known to equal the device table.
+gdl_status refresh(gdl_engine *e) { return e->mirror_fresh ? GDL_OK : pull(e); }
 // The host mirror to the device, stream-ordered: a copy from pageable
 // memory is staged when the call returns, so the mirror may change at once.
 gdl_status push(gdl_engine *e) {
@@ -548,7 +555,7 @@ u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e
 // FULL := unique(sort(keys[0..n))) for a load; DELTA/NEWT cleared.
 gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   RelHost &rh = e->rels[rel];
-  TRY(pull(e));
+  TRY(refresh(e));
   RelDev &r = e->h[rel];
   rh.bm_valid = false;
   rh.full_resident = false;
@@ -577,6 +584,7 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     r.newt.n = n;
     TRY(push(e));
     TRY(reset_ctl(e));
+    e->mirror_fresh = false;
     Counts kc;
     launch_sort(e, &e->d_rels[rel].newt, r.newt.ptr, r.newt.cap, &kc);
     MergeArgs m;
@@ -596,10 +604,13 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     k_merge_partition<<<grid_for(e, n / kMergeTile + 2, 256, 8), 256, 0, e->s>>>(m);
     k_merge_diff<<<grid_for(e, n, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, e->s>>>(m);
     CK(e, cudaGetLastError());
-    TRY(pull(e));
+    // the table and the control block in one round trip
     Ctl c2;
+    CK(e, cudaMemcpyAsync(e->h.data(), e->d_rels, e->rels.size() * sizeof(RelDev),
+                          cudaMemcpyDeviceToHost, e->s));
     CK(e, cudaMemcpyAsync(&c2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
     CK(e, cudaStreamSynchronize(e->s));
+    e->mirror_fresh = true;
     if (c2.timeout || c2.oob || c2.overflow)
       return fail(e, GDL_E_TIMEOUT, "load of %s: device check failed (timeout=%u oob=%u overflow=%u)",
                   rh.name.c_str(), c2.timeout, c2.oob, c2.overflow);
@@ -1269,7 +1280,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   };
   TRY(reset_ctl(e));
   mark("reset_ctl");
-  TRY(pull(e));
+  TRY(refresh(e));
   mark("pull");
   // Setup (src/lie.cu:49-59): DELTA := the first |FULL| rows of FULL's raw
   // buffer; capacities for the loop.
@@ -1515,6 +1526,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr && !e->profile;
   u64 batch = 4;
   bool first_batch = true;
+  e->mirror_fresh = false;
   while (true) {
     c.pause = 0;
     c.stop_at = c.iteration + (use_graph ? std::min<u64>(trace_rows, 1u << 20) : batch);
@@ -1705,6 +1717,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (c.done) break;
     batch = std::min<u64>(batch * 2, 64);
   }
+  e->mirror_fresh = false;  // (a pull while growing buffers preceded more launches)
   if (L.dense) {
     // FULL lists that were not kept during the loop are written from the
     // FULL bitmaps, sorted (bit order is tuple order).
@@ -1791,7 +1804,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   e->kernels_launched += L.kernels;
   for (int k = 0; k < kPKinds; k++) e->prof_bytes[k] += c.prof[k];
   // Finish (src/lie.cu:217-260).
-  TRY(pull(e));
+  TRY(refresh(e));
   for (int r : L.update) {
     RelDev &h = e->h[r];
     RelHost &rh = e->rels[r];
@@ -2019,7 +2032,7 @@ gdl_status gdl_relation_create(gdl_engine *e, const char *name, int32_t arity, i
   d.full_vis = d.delta_vis = d.w_full_vis = d.w_delta_vis = 1;
   e->h.push_back(d);
   *out = (int32_t)e->rels.size() - 1;
-  TRY(pull(e));  // keep the mirror coherent, then write the new entry
+  TRY(refresh(e));  // keep the mirror coherent, then write the new entry
   e->h.back() = d;
   TRY(push(e));
   return GDL_OK;
@@ -2121,7 +2134,7 @@ gdl_status gdl_relation_load_device(gdl_engine *e, int32_t rel, const uint64_t *
 
 static gdl_status version_view(gdl_engine *e, int rel, int ver, const u64 **ptr, u64 *n,
                                bool *sorted, bool need_rows = true) {
-  TRY(pull(e));
+  TRY(refresh(e));
   const RelDev &r = e->h[rel];
   *sorted = true;
   if (ver == GDL_FULL) {
