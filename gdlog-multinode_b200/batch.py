@@ -1,7 +1,7 @@
 """Batched fixpoints: many independent instances of one program at once.
 
 The reference runs one fixpoint per driver invocation; a workload of many
-small, uneven instances (BASELINE's 384 layered DAGs, or a stream of
+small, uneven instances (384 layered DAGs of mixed sizes, or a stream of
 queries) is then a loop of single-instance runs, each paying the engine's
 per-fixpoint overheads.  Here every instance's ids are moved into their own
 range, (instance << S) | local, and ONE program runs over the disjoint
