@@ -1942,13 +1942,9 @@ static void release_program(gdl_engine *e) {
   }
   for (LieHost &L : e->lies) {
     if (L.gexec) cudaGraphExecDestroy(L.gexec);
-    if (L.d_lie) {
-      LieDev ld;
-      if (cudaMemcpy(&ld, L.d_lie, sizeof ld, cudaMemcpyDeviceToHost) == cudaSuccess)
-        cudaFree(ld.trace);
-      cudaFree(L.d_lie);
-    }
-    cudaFree(L.d_joinrec);
+    // stream-ordered frees (a cudaFree would wait for the whole device)
+    for (void *p : {(void *)L.d_trace, (void *)L.d_lie, (void *)L.d_joinrec})
+      if (p) cudaFreeAsync(p, e->s);
     if (L.d_inst_delta) cudaFreeAsync(L.d_inst_delta, e->s);
     if (L.d_inst_last) cudaFreeAsync(L.d_inst_last, e->s);
   }
@@ -2353,10 +2349,10 @@ gdl_status gdl_lie_create(gdl_engine *e, int32_t *out) {
   if (!e || !out) return GDL_E_INVALID;
   cudaSetDevice(e->device);
   LieHost L;
-  CK(e, cudaMalloc(&L.d_lie, sizeof(LieDev)));
-  CK(e, cudaMemset(L.d_lie, 0, sizeof(LieDev)));
-  CK(e, cudaMalloc(&L.d_joinrec, kMaxOps * sizeof(JoinRec)));
-  CK(e, cudaMemset(L.d_joinrec, 0, kMaxOps * sizeof(JoinRec)));
+  TRY(dalloc(e, (void **)&L.d_lie, sizeof(LieDev)));
+  CK(e, cudaMemsetAsync(L.d_lie, 0, sizeof(LieDev), e->s));
+  TRY(dalloc(e, (void **)&L.d_joinrec, kMaxOps * sizeof(JoinRec)));
+  CK(e, cudaMemsetAsync(L.d_joinrec, 0, kMaxOps * sizeof(JoinRec), e->s));
   e->lies.push_back(L);
   *out = (int32_t)e->lies.size() - 1;
   return GDL_OK;
