@@ -51,7 +51,7 @@ constexpr int kPullBlock = 256;
 constexpr int kPullUnit = 256;   // OT words per unit of work (a word per thread): 8192 keys
 constexpr int kPullPer = 2;      // consecutive candidates per thread and step
 constexpr int kPullMinBits = 8;  // a transposed tile is 256 ids square
-constexpr int kPullAutoBits = 12;  // the pull form by default from 2^12 ids on
+constexpr int kPullAutoBits = 10;  // the pull form by default from 2^10 ids on
 
 // Lane l holds row l of a 32 x 32 bit block (bit j = column j); afterwards
 // lane j holds column j (bit l = row l).  Each round swaps the off-diagonal

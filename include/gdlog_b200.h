@@ -133,7 +133,7 @@ typedef struct gdl_tuning {
                                   tmp NEWT outer: 1 = push form (outer in key
                                   order), 2 = pull form (gathered by output
                                   row from the transposed outer) when ids
-                                  reach 2^12 (default), 3 = pull form from
+                                  reach 2^10 (default), 3 = pull form from
                                   2^8 ids */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
