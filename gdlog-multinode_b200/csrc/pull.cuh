@@ -3,9 +3,9 @@
 // A join whose output tuple is (outer column 1, inner column 1), joined on
 // column 0 of both sides, makes output row r the union of the inner runs
 // I[k] over the keys k with (k, r) in the outer.  Same generation's two
-// recursive rules have this shape (test/sg.cu:158-170):
+// recursive rules have this shape (test/sg.cu:165-175):
 //   tmp(b, x) :- sg(a, b), edge(a, x)       sg(x, y) :- tmp(b, x), edge(b, y)
-// and so do the value-flow rules of CSPA (test/cspa.cu).  The push form
+// and so do CSPA's joins (test/cspa.cu:279-352).  The push form
 // (k_join_bm, dense.cuh) walks the outer in key order and sends one L2
 // reduction per candidate tuple, and the candidates of one output row
 // repeat each other many times over: on R-MAT graphs 35-49 candidates fall
@@ -29,8 +29,11 @@
 //                   runs balanced over the block into the shared row (2
 //                   consecutive candidates per thread, so a run is read in
 //                   16-byte pieces), then ORs the row's nonzero words into
-//                   the output.
-//
+//                   the output.  A long run whose inner is a FULL kept as
+//                   a bitmap is ORed from that bitmap's row instead.
+//   k_bm_update_t   the update step of a relation whose DELTA only these
+//                   joins read, in one pass that also writes DELTA
+//                   transposed.
 //   k_bm_fold_t     for a join whose output is (inner column 1, outer
 //                   column 1): the same kernel gathers by the outer's
 //                   column 1 into a transposed twin of the output NEWT,
