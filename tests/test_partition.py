@@ -1,0 +1,88 @@
+"""Partitioned fixpoint (partition.py): transitive closure with path
+hash-partitioned over ranks and one all-to-all of new tuples per pass.
+On CPU: 2 and 3 gloo ranks, each with the oracle as its engine, against one
+oracle run (the same closure and the same loop-pass count).  On a GPU: one
+rank over the CUDA engine."""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import partition as PT
+import programs as P
+import workloads as W
+from gdlog_b200 import Engine
+
+CASES = {
+    "grid_10": lambda: W.grid_edges(10, 10),
+    "dag_L12_W10": lambda: W.layered_dag(12, 10, 1),
+    "rmat_s7": lambda: W.rmat_edges(7, 300, seed=3),
+}
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, case, out_dir):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                           world_size=world)
+    try:
+        with Engine("oracle") as eng:
+            res = PT.partitioned_tc(eng, CASES[case](), rank, world)
+        rows = PT.gather_rows(res.full, world)
+        with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+            json.dump({"passes": res.passes, "n": len(res.full), "rows": rows.tolist(),
+                       "per_pass": res.per_pass_new}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def single(case):
+    with Engine("oracle") as o:
+        r = P.tc(o, CASES[case]())
+        rows = r.output.rows()
+        return r.iterations["tc"], rows[np.lexsort((rows[:, 1], rows[:, 0]))].tolist()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_partitioned_tc_equals_single(case, world, tmp_path):
+    mp.spawn(_rank, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
+    outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
+    iters, rows = single(case)
+    for o in outs:
+        assert o["passes"] == iters
+        assert o["rows"] == rows
+    assert sum(o["n"] for o in outs) == len(rows)  # disjoint partitions
+
+
+def test_owner_and_route_shapes():
+    ids = np.array([0, 1, 2, 3, 7, 10])
+    assert PT.owner(ids, 3).tolist() == [0, 1, 2, 0, 1, 1]
+    rows = np.array([[5, 1], [2, 3], [1 << 20, 7]], dtype=np.uint64)
+    assert (PT._unpack(PT._pack(rows)) == rows).all()
+
+
+@pytest.mark.gpu
+def test_partitioned_tc_one_rank_on_the_gpu():
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{free_port()}", rank=0,
+                            world_size=1)
+    try:
+        e = W.grid_edges(24, 24)
+        with Engine("gpu") as g:
+            res = PT.partitioned_tc(g, e, 0, 1)
+            full = res.full[np.lexsort((res.full[:, 1], res.full[:, 0]))]
+        with Engine("gpu") as g:
+            r = P.tc(g, e, sync=g.sync)
+            want = r.output.rows()
+            assert res.passes == r.iterations["tc"]
+        assert full.tolist() == want[np.lexsort((want[:, 1], want[:, 0]))].tolist()
+    finally:
+        dist.destroy_process_group()
