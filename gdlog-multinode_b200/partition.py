@@ -23,6 +23,13 @@ One pass on rank r:
 Each pass extends the paths by one edge, as the single-GPU loop does, so the
 pass count equals its loop-pass count and the union of the FULL partitions
 is its closure.  The engine on each rank is any gdlog_b200.Engine.
+
+Same generation (test/sg.cu:93-191) partitions the same way: edge and sg
+on their first column (sg(a, b) with a owned), so both joins of a pass —
+tmp(b, x) :- edge(a, x), sg(a, b) and sg(x, y) :- edge(b, y), tmp(b, x) —
+read only owned keys; a pass routes tmp candidates to owner(b), then sg
+candidates to owner(x).  Its non-recursive rule sg(x, y) :- edge(p, x),
+edge(p, y), x != y runs as its own loop, as the driver's first LIE does.
 """
 from __future__ import annotations
 
@@ -32,7 +39,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-from gdlog_b200 import DELTA, FULL, INNER, OUTER, SRC, Engine
+from gdlog_b200 import DELTA, FULL, INNER, OUTER, PRED_NE, SRC, Engine
 
 
 def owner(ids: np.ndarray, world: int) -> np.ndarray:
@@ -132,6 +139,122 @@ def partitioned_tc(eng: Engine, edges: np.ndarray, rank: int, world: int,
         if n.item() == 0:
             break
     res.full = P.rows() if P.size() else np.zeros((0, 2), dtype=np.uint64)
+    return res
+
+
+class _Owned:
+    """A relation partition that grows by deduplicated merges: received rows
+    are copied into it by a one-pass LIE whose update step keeps the new
+    ones (its DELTA)."""
+
+    def __init__(self, eng: Engine, name: str, rows):
+        self.eng = eng
+        self.full = eng.relation(name, index_flag=False)
+        eng.load(self.full, rows if rows is not None and len(rows) else None)
+        self.recv = eng.relation(name + "_recv", index_flag=False)
+        # a Copy from the received relation's DELTA (its rows at every LIE
+        # start, src/lie.cu:49-59; a Copy from FULL would run once per LIE)
+        self.lie = eng.lie()
+        self.lie.set_reload_full(False)
+        self.lie.add_relations(self.recv, False)
+        self.lie.add_relations(self.full, False)
+        self.lie.add_copy(self.recv, DELTA, self.full, (SRC(0), SRC(1)))
+        self.lie.max_iteration = 0
+
+    def merge(self, rows: np.ndarray) -> np.ndarray:
+        """Add rows; return those that were not there yet.  Rows are
+        deduplicated first: a relation's DELTA at LIE start is the first
+        |FULL| of its rows in load order, so a repeat would hide a tuple."""
+        if len(rows):
+            rows = np.unique(rows, axis=0)
+        self.eng.load(self.recv, rows if len(rows) else None)
+        self.lie.fixpoint()
+        return self.full.rows(DELTA) if self.full.size(DELTA) else np.zeros((0, 2), np.uint64)
+
+    def rows(self) -> np.ndarray:
+        return self.full.rows() if self.full.size() else np.zeros((0, 2), np.uint64)
+
+
+class _Join:
+    """One join of the partitioned program as a one-pass LIE: the inner's
+    FULL joined with the outer's FULL into a candidates relation."""
+
+    def __init__(self, eng: Engine, inner, outer, sel, pred=None, name="cand"):
+        self.eng = eng
+        self.out = eng.relation(name, index_flag=False)
+        self.lie = eng.lie()
+        self.lie.add_relations(inner, True)
+        if outer is not inner:
+            self.lie.add_relations(outer, True)
+        self.lie.add_relations(self.out, False)
+        if pred is None:
+            self.lie.add_join(inner, FULL, outer, FULL, self.out, sel)
+        else:
+            self.lie.add_join(inner, FULL, outer, FULL, self.out, sel, pred=pred)
+        self.lie.max_iteration = 0
+
+    def run(self) -> np.ndarray:
+        self.eng.load(self.out, None)
+        self.lie.fixpoint()
+        return self.out.rows() if self.out.size() else np.zeros((0, 2), np.uint64)
+
+
+def _to_owners(rows: np.ndarray, col: int, world: int, device) -> np.ndarray:
+    dest = owner(rows[:, col], world) if len(rows) else np.zeros(0, np.int64)
+    return route(rows, dest, world, device)
+
+
+def _any(n: int, device) -> int:
+    t = torch.tensor([n], dtype=torch.int64, device=device if device is not None else "cpu")
+    dist.all_reduce(t)
+    return int(t.item())
+
+
+@dataclass
+class PartSG:
+    init_passes: int = 0
+    passes: int = 0
+    full: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), dtype=np.uint64))
+
+
+def partitioned_sg(eng: Engine, edges: np.ndarray, rank: int, world: int,
+                   device=None) -> PartSG:
+    """Same generation of `edges` (every rank passes the same edges) with sg
+    partitioned over the ranks; returns this rank's sg partition and the
+    loop-pass counts of the two LIEs (equal on every rank)."""
+    e = np.asarray(edges, dtype=np.uint64).reshape(-1, 2)
+    E = eng.relation("edge_2__1_2")
+    mine = e[owner(e[:, 0], world) == rank]
+    eng.load(E, mine if len(mine) else None)
+    sg = _Owned(eng, "sg", None)
+    D = eng.relation("sg_delta")
+    T = eng.relation("tmp")
+    res = PartSG()
+    # sg(x, y) :- edge(p, x), edge(p, y), x != y: its own loop (the second
+    # pass finds nothing new, as the driver's first LIE does)
+    init = _Join(eng, E, E, (INNER(1), OUTER(1)), pred=(PRED_NE, 0, 1), name="cand_init")
+    while True:
+        res.init_passes += 1
+        new = sg.merge(_to_owners(init.run(), 0, world, device))
+        if _any(len(new), device) == 0:
+            break
+    # the recursive rules, from DELTA = FULL (src/lie.cu:49-59)
+    delta = sg.rows()
+    tmp_join = _Join(eng, E, D, (OUTER(1), INNER(1)), name="cand_tmp")
+    sg_join = _Join(eng, E, T, (OUTER(1), INNER(1)), name="cand_sg")
+    while True:
+        res.passes += 1
+        eng.load(D, delta if len(delta) else None)
+        # tmp(b, x) :- edge(a, x), sg(a, b): to owner(b)
+        tmp = _to_owners(tmp_join.run(), 0, world, device)
+        if len(tmp):
+            tmp = np.unique(tmp, axis=0)
+        eng.load(T, tmp if len(tmp) else None)
+        # sg(x, y) :- edge(b, y), tmp(b, x): to owner(x), deduplicated there
+        delta = sg.merge(_to_owners(sg_join.run(), 0, world, device))
+        if _any(len(delta), device) == 0:
+            break
+    res.full = sg.rows()
     return res
 
 

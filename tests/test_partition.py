@@ -1,8 +1,8 @@
-"""Partitioned fixpoint (partition.py): transitive closure with path
-hash-partitioned over ranks and one all-to-all of new tuples per pass.
-On CPU: 2 and 3 gloo ranks, each with the oracle as its engine, against one
-oracle run (the same closure and the same loop-pass count).  On a GPU: one
-rank over the CUDA engine."""
+"""Partitioned fixpoint (partition.py): transitive closure and same
+generation with their relations hash-partitioned over ranks and
+all-to-all exchanges of new tuples per pass.  On CPU: 2 and 3 gloo ranks,
+each with the oracle as its engine, against one oracle run (the same result
+and the same loop-pass counts).  On a GPU: one rank over the CUDA engine."""
 import json
 import os
 import socket
@@ -51,8 +51,7 @@ def single(case):
         return r.iterations["tc"], rows[np.lexsort((rows[:, 1], rows[:, 0]))].tolist()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case,world", [(c, 2) for c in sorted(CASES)] + [("grid_10", 3)])
 def test_partitioned_tc_equals_single(case, world, tmp_path):
     mp.spawn(_rank, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
     outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
@@ -61,6 +60,42 @@ def test_partitioned_tc_equals_single(case, world, tmp_path):
         assert o["passes"] == iters
         assert o["rows"] == rows
     assert sum(o["n"] for o in outs) == len(rows)  # disjoint partitions
+
+
+SG_CASES = {
+    "rmat_s7": lambda: W.rmat_edges(7, 300, seed=3),
+    "rmat_s8": lambda: W.rmat_edges(8, 600, seed=1),
+    "dag_L8_W6": lambda: W.layered_dag(8, 6, 2),
+}
+
+
+def _rank_sg(rank, world, port, case, out_dir):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        with Engine("oracle") as eng:
+            res = PT.partitioned_sg(eng, SG_CASES[case](), rank, world)
+        rows = PT.gather_rows(res.full, world)
+        with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+            json.dump({"init": res.init_passes, "sg": res.passes, "n": len(res.full),
+                       "rows": rows.tolist()}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case,world", [(c, 2) for c in sorted(SG_CASES)] + [("rmat_s8", 3)])
+def test_partitioned_sg_equals_single(case, world, tmp_path):
+    mp.spawn(_rank_sg, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
+    outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
+    with Engine("oracle") as o:
+        r = P.sg(o, SG_CASES[case]())
+        want = r.output.rows()
+        want = want[np.lexsort((want[:, 1], want[:, 0]))].tolist()
+        iters = r.iterations
+    for o in outs:
+        assert (o["init"], o["sg"]) == (iters["init"], iters["sg"])
+        assert o["rows"] == want
+    assert sum(o["n"] for o in outs) == len(want)
 
 
 def test_owner_and_route_shapes():
