@@ -1,0 +1,330 @@
+"""Datalog rules over binary relations compiled to the engine's operator
+program.
+
+The reference's users write the semi-naive program by hand (test/tc.cu,
+test/sg.cu, test/cspa.cu): relations in each column order a join needs
+(edge_2__1_2, edge_2__2_1), one LIE per recursive component, a
+RelationalJoin per rule and per recursive body atom (that atom's DELTA
+against the other atoms' FULL), tmp relations for three-atom rules, and an
+ACopy that keeps each swapped copy of a recursive relation current.  This
+module derives that program from the rules:
+
+    path(x, y) :- edge(x, y).
+    path(x, z) :- path(x, y), edge(y, z).
+
+Supported: binary predicates; rule bodies of one atom (a Copy, its head any
+selection of the atom's columns, e.g. vf(x, x) :- assign(x, y)), two atoms
+sharing one variable (a join on it), or three atoms in a chain a-b-c (a and
+b share one variable, b and c another; compiled through a tmp relation
+keyed for the last join, and, for a DELTA on the third atom, through one
+keyed for the first); one optional `X != Y` on the two head variables.
+Predicates without rules are inputs (EDB).  Components of mutually
+recursive predicates run as LIEs in dependency order; rules whose body has
+no predicate of the component join FULL with FULL (a Copy from a FULL runs
+once per LIE, src/copy.cu).
+"""
+from __future__ import annotations
+
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from gdlog_b200 import (DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, SRC, Engine)
+
+_ATOM = re.compile(r"\s*([A-Za-z_]\w*)\s*\(\s*([A-Za-z_]\w*)\s*,\s*([A-Za-z_]\w*)\s*\)\s*")
+_NE = re.compile(r"\s*([A-Za-z_]\w*)\s*!=\s*([A-Za-z_]\w*)\s*")
+
+
+@dataclass(frozen=True)
+class Atom:
+    pred: str
+    args: tuple  # two variable names
+
+
+@dataclass
+class Rule:
+    head: Atom
+    body: list
+    ne: tuple | None = None  # (X, Y): X != Y over head variables
+    text: str = ""
+
+
+def parse(text: str) -> list:
+    """Rules of a program ('%' and '//' start comments; a rule ends with '.')."""
+    lines = [re.split(r"%|//", ln)[0] for ln in text.splitlines()]
+    rules = []
+    for stmt in " ".join(lines).split("."):
+        stmt = stmt.strip()
+        if not stmt:
+            continue
+        if ":-" not in stmt:
+            raise ValueError(f"not a rule: {stmt!r}")
+        head_s, body_s = stmt.split(":-", 1)
+        m = _ATOM.fullmatch(head_s)
+        if not m:
+            raise ValueError(f"bad head: {head_s!r}")
+        head = Atom(m.group(1), (m.group(2), m.group(3)))
+        body, ne = [], None
+        for part in re.split(r",(?![^(]*\))", body_s):
+            ma, mn = _ATOM.fullmatch(part), _NE.fullmatch(part)
+            if ma:
+                body.append(Atom(ma.group(1), (ma.group(2), ma.group(3))))
+            elif mn and ne is None:
+                ne = (mn.group(1), mn.group(2))
+            else:
+                raise ValueError(f"bad body literal: {part!r}")
+        bvars = {v for a in body for v in a.args}
+        if not body or not set(head.args) <= bvars:
+            raise ValueError(f"head variables must appear in the body: {stmt!r}")
+        if ne and set(ne) != set(head.args):
+            raise ValueError(f"'!=' must relate the two head variables: {stmt!r}")
+        if len(body) > 3:
+            raise ValueError(f"at most three body atoms: {stmt!r}")
+        if ne and len(body) == 1:
+            # a Copy ignores predicates (src/copy.cu)
+            raise ValueError(f"'!=' needs a join (two or three body atoms): {stmt!r}")
+        rules.append(Rule(head, body, ne, stmt))
+    return rules
+
+
+def _components(rules: list) -> list:
+    """Strongly connected components of the head predicates, dependencies
+    first (Tarjan)."""
+    idb = sorted({r.head.pred for r in rules})
+    deps = {p: sorted({a.pred for r in rules if r.head.pred == p for a in r.body if a.pred in idb})
+            for p in idb}
+    index, low, stack, on, out, n = {}, {}, [], set(), [], [0]
+
+    def visit(v):
+        index[v] = low[v] = n[0]
+        n[0] += 1
+        stack.append(v)
+        on.add(v)
+        for w in deps[v]:
+            if w not in index:
+                visit(w)
+                low[v] = min(low[v], low[w])
+            elif w in on:
+                low[v] = min(low[v], index[w])
+        if low[v] == index[v]:
+            comp = []
+            while True:
+                w = stack.pop()
+                on.discard(w)
+                comp.append(w)
+                if w == v:
+                    break
+            out.append(sorted(comp))
+
+    for v in idb:
+        if v not in index:
+            visit(v)
+    return out
+
+
+def _shared(a: Atom, b: Atom) -> list:
+    return [v for v in a.args if v in b.args]
+
+
+def _other(a: Atom, v: str) -> str:
+    return a.args[1] if a.args[0] == v else a.args[0]
+
+
+def _order(a: Atom, key: str) -> int:
+    """12: the atom's relation as stored; 21: swapped (key first)."""
+    if a.args[0] == key:
+        return 12
+    if a.args[1] == key:
+        return 21
+    raise ValueError(f"{a} does not hold {key}")
+
+
+@dataclass
+class Compiled:
+    relations: dict = field(default_factory=dict)   # head predicate -> Relation (order 12)
+    iterations: dict = field(default_factory=dict)  # component name -> loop passes
+    lies: dict = field(default_factory=dict)
+
+    @property
+    def output(self):
+        return next(iter(self.relations.values()))
+
+
+def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
+    """Compile `text` and run it on `eng` over the input relations
+    (predicate -> rows); returns the head predicates' relations."""
+    rules = parse(text)
+    idb = {r.head.pred for r in rules}
+    for r in rules:
+        for a in r.body:
+            if a.pred not in idb and a.pred not in inputs:
+                raise ValueError(f"no rule and no input for {a.pred!r}")
+    rels = {}  # (pred, order) -> Relation
+
+    def rows_of(pred, order):
+        if pred in inputs:
+            rows = np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, 2)
+        else:
+            rel = rels[(pred, 12)]
+            rows = rel.rows() if rel.size() else np.zeros((0, 2), np.uint64)
+        return rows if order == 12 else rows[:, ::-1].copy()
+
+    def static(pred, order):
+        if (pred, order) not in rels:
+            rel = eng.relation(f"{pred}_2__{'1_2' if order == 12 else '2_1'}")
+            rows = rows_of(pred, order)
+            eng.load(rel, rows if len(rows) else None)
+            rels[(pred, order)] = rel
+        return rels[(pred, order)]
+
+    out = Compiled()
+    tmp_n = [0]
+    for comp in _components(rules):
+        comp_set = set(comp)
+        comp_rules = [r for r in rules if r.head.pred in comp_set]
+        # relations of the component: every predicate in order 12, a swapped
+        # mirror where a join needs one (kept by an ACopy)
+        mirrors = set()
+
+        def need(a: Atom, key: str):
+            o = _order(a, key)
+            if a.pred in comp_set and o == 21:
+                mirrors.add(a.pred)
+            return o
+
+        plan = []  # ("copy", ...) / ("join", ...) in rule order
+        tmps = []
+        for r in comp_rules:
+            rec = [a.pred in comp_set for a in r.body]
+            h0, h1 = r.head.args
+            pred = (PRED_NE, 0, 1) if r.ne else None
+            if len(r.body) == 1:
+                a = r.body[0]
+                sel = tuple(SRC(a.args.index(h)) for h in (h0, h1))
+                plan.append(("copy", a.pred, DELTA if rec[0] else FULL, r.head.pred, sel, pred))
+                continue
+            if len(r.body) == 2:
+                a, b = r.body
+                sv = _shared(a, b)
+                if len(sv) != 1:
+                    raise ValueError(f"two atoms must share one variable: {r.text!r}")
+                v = sv[0]
+                variants = [i for i in (0, 1) if rec[i]] or [None]
+                for d in variants:
+                    outer, inner = (r.body[d], r.body[1 - d]) if d is not None else (b, a)
+                    oo, io = need(outer, v), need(inner, v)
+                    sel = tuple(_sel(h, v, inner, outer) for h in (h0, h1))
+                    plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
+                                 DELTA if d is not None else FULL, r.head.pred, sel, pred))
+                continue
+            a, b, c = r.body
+            s_ab, s_bc, s_ac = _shared(a, b), _shared(b, c), _shared(a, c)
+            if len(s_ab) != 1 or len(s_bc) != 1 or s_ac or s_ab == s_bc:
+                raise ValueError(f"three atoms must form a chain a-b-c: {r.text!r}")
+            v1, v2 = s_ab[0], s_bc[0]
+            ax, cy = _other(a, v1), _other(c, v2)
+            if {h0, h1} != {ax, cy}:
+                raise ValueError(f"the head must hold the chain's two ends: {r.text!r}")
+            if rec[0] or rec[1] or not any(rec):
+                # tmp(v2, ax) from a and b (a DELTA on a or on b), then c
+                t = f"tmp_{tmp_n[0]}"
+                tmp_n[0] += 1
+                tmps.append(t)
+                for d in ([i for i in (0, 1) if rec[i]] or [None]):
+                    outer, inner = ((a, b) if d == 0 else (b, a)) if d is not None else (b, a)
+                    oo, io = need(outer, v1), need(inner, v1)
+                    tsel = tuple(_sel(h, v1, inner, outer) for h in (v2, ax))
+                    plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
+                                 DELTA if d is not None else FULL, t, tsel, None))
+                tmp_atom = Atom(t, (v2, ax))
+                co = need(c, v2)
+                sel = tuple(_sel(h, v2, c, tmp_atom) for h in (h0, h1))
+                plan.append(("join", c.pred, co, FULL, t, 12, NEWT, r.head.pred, sel, pred))
+            if rec[2]:
+                # a DELTA on c: tmp(v1, cy) from b and c, then a
+                t = f"tmp_{tmp_n[0]}"
+                tmp_n[0] += 1
+                tmps.append(t)
+                oo, io = need(c, v2), need(b, v2)
+                tsel = tuple(_sel(h, v2, b, c) for h in (v1, cy))
+                plan.append(("join", b.pred, io, FULL, c.pred, oo, DELTA, t, tsel, None))
+                tmp_atom = Atom(t, (v1, cy))
+                ao = need(a, v1)
+                sel = tuple(_sel(h, v1, a, tmp_atom) for h in (h0, h1))
+                plan.append(("join", a.pred, ao, FULL, t, 12, NEWT, r.head.pred, sel, pred))
+        # relations of this component
+        for p in comp:
+            if (p, 12) not in rels:
+                rel = eng.relation(f"{p}_2__1_2")
+                rows = rows_of(p, 12) if p in inputs else np.zeros((0, 2), np.uint64)
+                eng.load(rel, rows if len(rows) else None)
+                rels[(p, 12)] = rel
+            if p in mirrors and (p, 21) not in rels:
+                rel = eng.relation(f"{p}_2__2_1")
+                rows = rels[(p, 12)].rows() if rels[(p, 12)].size() else np.zeros((0, 2), np.uint64)
+                eng.load(rel, rows[:, ::-1].copy() if len(rows) else None)
+                rels[(p, 21)] = rel
+        tmp_rels = {}
+        for t in tmps:
+            tmp_rels[t] = eng.relation(t, index_flag=False)
+            eng.load(tmp_rels[t], None)
+        lie = eng.lie()
+        statics = set()
+
+        def rel_of(pred, order):
+            if pred in tmp_rels:
+                return tmp_rels[pred]
+            if pred in comp_set:
+                return rels[(pred, order)]
+            r_ = static(pred, order)
+            if r_ not in statics:
+                statics.add(r_)
+                lie.add_relations(r_, True)
+            return r_
+
+        # resolve the static relations first (their LIE role), then add
+        # the component's relations and ops
+        for step in plan:
+            if step[0] == "copy":
+                rel_of(step[1], 12)
+            else:
+                rel_of(step[1], step[2])
+                rel_of(step[4], step[5])
+        for p in comp:
+            lie.add_relations(rels[(p, 12)], False)
+            if p in mirrors:
+                lie.add_relations(rels[(p, 21)], False)
+        for t in tmps:
+            lie.add_tmp_relation(tmp_rels[t])
+        for step in plan:
+            if step[0] == "copy":
+                _, src, ver, head, sel, pred = step
+                lie.add_copy(rel_of(src, 12), ver, rels[(head, 12)], sel)
+            else:
+                _, ip, io, iv, op_, oo, ov, head, sel, pred = step
+                dest = tmp_rels[head] if head in tmp_rels else rels[(head, 12)]
+                kw = {"pred": pred} if pred else {}
+                lie.add_join(rel_of(ip, io), iv, rel_of(op_, oo), ov, dest, sel, **kw)
+        for p in sorted(mirrors):
+            lie.add_acopy(rels[(p, 12)], rels[(p, 21)], (SRC(1), SRC(0)))
+        name = "+".join(comp)
+        out.iterations[name] = lie.fixpoint()
+        out.lies[name] = lie
+        for p in comp:
+            out.relations[p] = rels[(p, 12)]
+    if sync:
+        sync()
+    return out
+
+
+def _sel(h: str, key: str, inner: Atom, outer: Atom) -> int:
+    """The column selection of head variable h in a join of inner and outer
+    on `key` (each stored with the key first)."""
+    if h == key:
+        return INNER(0)
+    if h == _other(inner, key):
+        return INNER(1)
+    if h == _other(outer, key):
+        return OUTER(1)
+    raise ValueError(f"variable {h} is not in the join")

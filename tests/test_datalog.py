@@ -1,0 +1,93 @@
+"""Datalog front end (datalog.py): rules compiled to the engine's operator
+program give the same relations as the hand-written drivers (programs.py,
+which follow test/tc.cu, test/sg.cu and test/cspa.cu).  CPU: the oracle
+engine."""
+import numpy as np
+import pytest
+
+import datalog as D
+import programs as P
+import workloads as W
+from gdlog_b200 import Engine
+
+TC = """
+path(x, y) :- edge(x, y).
+path(x, z) :- path(x, y), edge(y, z).
+"""
+
+SG = """
+sg(x, y) :- edge(p, x), edge(p, y), x != y.
+sg(x, y) :- edge(a, x), sg(a, b), edge(b, y).
+"""
+
+# The rules of the CSPA driver (programs.cspa): the copies of its first LIE
+# and the joins of its analysis LIE.
+CSPA = """
+vf(y, y) :- assign(x, y).
+vf(x, x) :- assign(x, y).
+vf(x, y) :- assign(x, y).
+ma(y, y) :- assign(x, y).
+ma(x, x) :- assign(x, y).
+vf(x, y) :- vf(x, z), vf(z, y).
+va(x, y) :- vf(z, x), vf(z, y).
+vf(x, y) :- assign(x, z), ma(z, y).
+ma(x, w) :- deref(y, x), va(y, z), deref(z, w).   % three atoms, a chain
+va(x, y) :- vf(z, x), ma(z, w), vf(w, y).
+"""
+
+
+def sorted_rows(rel):
+    r = rel.rows()
+    return r[np.lexsort((r[:, 1], r[:, 0]))].tolist()
+
+
+@pytest.mark.parametrize("edges", [lambda: W.grid_edges(10, 10), lambda: W.layered_dag(10, 8, 3),
+                                   lambda: W.rmat_edges(7, 300, seed=5)])
+def test_tc_rules_equal_the_driver(edges):
+    e = edges()
+    with Engine("oracle") as o:
+        got = sorted_rows(D.run(o, TC, {"edge": e}).relations["path"])
+    with Engine("oracle") as o:
+        want = sorted_rows(P.tc(o, e).output)
+    assert got == want
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_sg_rules_equal_the_driver(seed):
+    e = W.rmat_edges(8, 600, seed=seed)
+    with Engine("oracle") as o:
+        got = sorted_rows(D.run(o, SG, {"edge": e}).relations["sg"])
+    with Engine("oracle") as o:
+        want = sorted_rows(P.sg(o, e).output)
+    assert got == want
+
+
+def test_cspa_rules_equal_the_driver():
+    assign, deref = W.cspa_facts(120, 240, 90, seed=1)
+    with Engine("oracle") as o:
+        r = D.run(o, CSPA, {"assign": assign, "deref": deref})
+        got = {k: sorted_rows(r.relations[k]) for k in ("vf", "ma", "va")}
+    with Engine("oracle") as o:
+        w = P.cspa(o, assign, deref)
+        want = {"vf": sorted_rows(w.relations["value_flow"]),
+                "ma": sorted_rows(w.relations["memory_alias"]),
+                "va": sorted_rows(w.relations["value_alias"])}
+    assert got == want
+
+
+def test_components_in_dependency_order():
+    rules = D.parse("a(x, y) :- e(x, y).  b(x, y) :- a(x, y).  b(x, z) :- b(x, y), a(y, z).")
+    assert D._components(rules) == [["a"], ["b"]]
+
+
+@pytest.mark.parametrize("bad", [
+    "p(x, y) :- q(x, z).",                          # head variable not in the body
+    "p(x, y) :- q(x, y), x != y.",                  # a Copy ignores predicates
+    "p(x, y) :- q(x, a), r(b, y).",                 # no shared variable
+    "p(x, y) :- q(x, a), r(a, b), s(b, c), t(c, y).",  # four atoms
+    "p(x) :- q(x, y).",                             # not binary
+])
+def test_unsupported_rules_are_refused(bad):
+    inputs = {k: np.zeros((0, 2), dtype=np.uint64) for k in "qrst"}
+    with Engine("oracle") as o, pytest.raises(ValueError):
+        D.run(o, bad, inputs)
