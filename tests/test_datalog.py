@@ -91,3 +91,19 @@ def test_unsupported_rules_are_refused(bad):
     inputs = {k: np.zeros((0, 2), dtype=np.uint64) for k in "qrst"}
     with Engine("oracle") as o, pytest.raises(ValueError):
         D.run(o, bad, inputs)
+
+
+@pytest.mark.gpu
+def test_rules_on_the_gpu_engine():
+    e = W.rmat_edges(8, 600, seed=2)
+    g_edges = W.grid_edges(16, 16)
+    with Engine("gpu") as g:
+        sg_got = sorted_rows(D.run(g, SG, {"edge": e}, sync=g.sync).relations["sg"])
+        g.clear()
+        tc_got = sorted_rows(D.run(g, TC, {"edge": g_edges}, sync=g.sync).relations["path"])
+    with Engine("oracle") as o:
+        sg_want = sorted_rows(P.sg(o, e).output)
+    with Engine("oracle") as o:
+        tc_want = sorted_rows(P.tc(o, g_edges).output)
+    assert sg_got == sg_want
+    assert tc_got == tc_want
