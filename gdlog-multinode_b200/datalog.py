@@ -22,6 +22,14 @@ Predicates without rules are inputs (EDB).  Components of mutually
 recursive predicates run as LIEs in dependency order; rules whose body has
 no predicate of the component join FULL with FULL (a Copy from a FULL runs
 once per LIE, src/copy.cu).
+
+Souffle's directives, as the reference's test/souffle/*.dl programs use
+them, are read too: `.decl p(a: number, b: number)` (binary, numbers),
+`.input p(...)` (tab-separated facts: the caller's rows, else
+<facts_dir>/p.facts, else the `filename` given, relative to the program),
+`.output p` (<out_dir>/p.csv, sorted, tab-separated), `.printsize p`;
+`_` is a fresh variable.  `python datalog.py prog.dl --facts DIR --out DIR`
+runs a program file.
 """
 from __future__ import annotations
 
@@ -50,10 +58,53 @@ class Rule:
     text: str = ""
 
 
+@dataclass
+class Directives:
+    decl: dict = field(default_factory=dict)      # predicate -> arity
+    inputs: dict = field(default_factory=dict)    # predicate -> filename or None
+    outputs: list = field(default_factory=list)
+    printsize: list = field(default_factory=list)
+
+
+_DIRECTIVE = re.compile(r"^\s*\.(decl|input|output|printsize)\s+([A-Za-z_]\w*)\s*(\((.*)\))?")
+
+
+def _strip(text: str) -> str:
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    return "\n".join(re.split(r"%|//", ln)[0] for ln in text.splitlines())
+
+
+def directives(text: str) -> Directives:
+    """The Souffle directives of a program."""
+    d = Directives()
+    for ln in _strip(text).splitlines():
+        m = _DIRECTIVE.match(ln)
+        if not m:
+            continue
+        kind, name, args = m.group(1), m.group(2), m.group(4) or ""
+        if kind == "decl":
+            d.decl[name] = len([a for a in args.split(",") if a.strip()])
+        elif kind == "input":
+            fm = re.search(r'filename\s*=\s*"([^"]*)"', args)
+            d.inputs[name] = fm.group(1) if fm else None
+        elif kind == "output":
+            d.outputs.append(name)
+        else:
+            d.printsize.append(name)
+    return d
+
+
 def parse(text: str) -> list:
-    """Rules of a program ('%' and '//' start comments; a rule ends with '.')."""
-    lines = [re.split(r"%|//", ln)[0] for ln in text.splitlines()]
+    """Rules of a program ('%', '//' and '/* */' are comments, lines that
+    start with '.' are directives, a rule ends with '.')."""
+    lines = [ln for ln in _strip(text).splitlines() if not ln.lstrip().startswith(".")]
     rules = []
+    fresh = [0]
+
+    def anon(m):
+        fresh[0] += 1
+        return f"_{fresh[0]}"
+
     for stmt in " ".join(lines).split("."):
         stmt = stmt.strip()
         if not stmt:
@@ -61,6 +112,7 @@ def parse(text: str) -> list:
         if ":-" not in stmt:
             raise ValueError(f"not a rule: {stmt!r}")
         head_s, body_s = stmt.split(":-", 1)
+        body_s = re.sub(r"(?<![\w])_(?![\w])", anon, body_s)
         m = _ATOM.fullmatch(head_s)
         if not m:
             raise ValueError(f"bad head: {head_s!r}")
@@ -328,3 +380,64 @@ def _sel(h: str, key: str, inner: Atom, outer: Atom) -> int:
     if h == _other(outer, key):
         return OUTER(1)
     raise ValueError(f"variable {h} is not in the join")
+
+
+def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str | None = None,
+             inputs: dict | None = None, sync=None) -> tuple:
+    """Run a Souffle-style program file: its `.input` relations from
+    `inputs`, else <facts_dir>/<name>.facts, else the file name the
+    directive gives (relative to the program); `.output` relations written
+    to <out_dir>/<name>.csv.  Returns (Compiled, {name: size} for the
+    `.printsize` relations)."""
+    import os
+    from gdlog_b200 import read_tsv
+    text = open(path).read()
+    d = directives(text)
+    for name, arity in d.decl.items():
+        if arity != 2:
+            raise ValueError(f"{name}: only binary relations are supported (arity {arity})")
+    given = dict(inputs or {})
+    for name, fname in d.inputs.items():
+        if name in given:
+            continue
+        cands = []
+        if facts_dir:
+            cands.append(os.path.join(facts_dir, name + ".facts"))
+        if fname:
+            cands.append(os.path.join(os.path.dirname(os.path.abspath(path)), fname))
+        found = next((c for c in cands if os.path.exists(c)), None)
+        if found is None:
+            raise FileNotFoundError(f"no facts for {name}: tried {cands}")
+        given[name] = read_tsv(found, 2)
+    res = run(eng, text, given, sync=sync)
+    if out_dir:
+        os.makedirs(out_dir, exist_ok=True)
+        for name in d.outputs:
+            res.relations[name].dump_tsv(os.path.join(out_dir, name + ".csv"))
+    def size(name):
+        if name in res.relations:
+            return res.relations[name].size()
+        if name in given and len(given[name]):
+            return len(np.unique(np.asarray(given[name]).reshape(-1, 2), axis=0))
+        return 0  # declared, with neither rules nor facts
+
+    sizes = {name: size(name) for name in d.printsize}
+    return res, sizes
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="Run a Datalog program file on the engine.")
+    ap.add_argument("program")
+    ap.add_argument("--facts", default=None, help="directory of <name>.facts inputs")
+    ap.add_argument("--out", default=None, help="directory for <name>.csv outputs")
+    ap.add_argument("--engine", default="gpu", choices=["gpu", "oracle"])
+    a = ap.parse_args()
+    with Engine(a.engine) as eng:
+        res, sizes = run_file(eng, a.program, a.facts, a.out, sync=getattr(eng, "sync", None))
+        print(json.dumps({"sizes": sizes, "iterations": res.iterations}))
+
+
+if __name__ == "__main__":
+    main()

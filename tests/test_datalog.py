@@ -2,6 +2,8 @@
 program give the same relations as the hand-written drivers (programs.py,
 which follow test/tc.cu, test/sg.cu and test/cspa.cu).  CPU: the oracle
 engine."""
+import os
+
 import numpy as np
 import pytest
 
@@ -107,3 +109,65 @@ def test_rules_on_the_gpu_engine():
         tc_want = sorted_rows(P.tc(o, g_edges).output)
     assert sg_got == sg_want
     assert tc_got == tc_want
+
+
+REF_SOUFFLE = os.path.join("/root/reference", "test", "souffle")
+
+
+def write_facts(path, rows):
+    with open(path, "w") as f:
+        for a, b in np.asarray(rows).reshape(-1, 2).tolist():
+            f.write(f"{a}\t{b}\n")
+
+
+def test_program_file_with_directives(tmp_path):
+    prog = tmp_path / "tc.dl"
+    prog.write_text(""".decl edge(x: number, y: number)
+.input edge
+.decl path(x: number, y: number)
+.output path
+.printsize path
+/* transitive closure */
+path(x, y) :- edge(x, y).
+path(x, z) :- path(x, y), edge(y, z).   // one step further
+.decl hub(x: number, y: number)
+.printsize hub
+hub(x, x) :- edge(x, _).
+""")
+    e = W.layered_dag(6, 5, 2)
+    write_facts(tmp_path / "edge.facts", e)
+    with Engine("oracle") as o:
+        res, sizes = D.run_file(o, str(prog), facts_dir=str(tmp_path), out_dir=str(tmp_path / "out"))
+        got = sorted_rows(res.relations["path"])
+    with Engine("oracle") as o:
+        want = sorted_rows(P.tc(o, e).output)
+    assert got == want and sizes["path"] == len(want)
+    assert sizes["hub"] == len(np.unique(e[:, 0]))
+    lines = open(tmp_path / "out" / "path.csv").read().split()
+    assert len(lines) == 2 * len(want)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SOUFFLE), reason="reference programs not present")
+def test_reference_souffle_programs_run(tmp_path):
+    """The reference's own sg.dl and cspa.dl (test/souffle), their inputs
+    from facts files, against the hand-written drivers."""
+    e = W.rmat_edges(8, 600, seed=3)
+    write_facts(tmp_path / "edge.facts", e)
+    assign, deref = W.cspa_facts(120, 240, 90, seed=2)
+    write_facts(tmp_path / "assign.facts", assign)
+    write_facts(tmp_path / "dereference.facts", deref)
+    with Engine("oracle") as o:
+        res, sizes = D.run_file(o, os.path.join(REF_SOUFFLE, "sg.dl"), facts_dir=str(tmp_path))
+        sg_got = sorted_rows(res.relations["sg"])
+    with Engine("oracle") as o:
+        assert sg_got == sorted_rows(P.sg(o, e).output)
+    with Engine("oracle") as o:
+        res, sizes = D.run_file(o, os.path.join(REF_SOUFFLE, "cspa.dl"), facts_dir=str(tmp_path))
+        got = {k: sorted_rows(res.relations[k]) for k in ("ValueFlow", "MemoryAlias", "ValueAlias")}
+    with Engine("oracle") as o:
+        w = P.cspa(o, assign, deref)
+        want = {"ValueFlow": sorted_rows(w.relations["value_flow"]),
+                "MemoryAlias": sorted_rows(w.relations["memory_alias"]),
+                "ValueAlias": sorted_rows(w.relations["value_alias"])}
+    assert got == want
+    assert sizes["ValueFlow"] == len(want["ValueFlow"])
