@@ -171,3 +171,29 @@ def test_reference_souffle_programs_run(tmp_path):
                 "ValueAlias": sorted_rows(w.relations["value_alias"])}
     assert got == want
     assert sizes["ValueFlow"] == len(want["ValueFlow"])
+
+
+def test_command_line(tmp_path):
+    import json
+    import subprocess
+    import sys
+    prog = tmp_path / "sg.dl"
+    prog.write_text(""".decl edge(x: number, y: number)
+.input edge
+.decl sg(x: number, y: number)
+.output sg
+.printsize sg
+sg(x, y) :- edge(p, x), edge(p, y), x != y.
+sg(x, y) :- edge(a, x), sg(a, b), edge(b, y).
+""")
+    e = W.rmat_edges(6, 120, seed=4)
+    write_facts(tmp_path / "edge.facts", e)
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(here, "gdlog-multinode_b200", "datalog.py"),
+                          str(prog), "--facts", str(tmp_path), "--out", str(tmp_path / "o"),
+                          "--engine", "oracle"], capture_output=True, text=True, check=True)
+    sizes = json.loads(out.stdout.strip().splitlines()[-1])["sizes"]
+    with Engine("oracle") as o:
+        want = P.sg(o, e).output.size()
+    assert sizes["sg"] == want
+    assert os.path.exists(tmp_path / "o" / "sg.csv")
