@@ -1,5 +1,4 @@
-"""Datalog rules over binary relations compiled to the engine's operator
-program.
+"""Datalog rules compiled to the engine's operator program.
 
 The reference's users write the semi-naive program by hand (test/tc.cu,
 test/sg.cu, test/cspa.cu): relations in each column order a join needs
@@ -7,24 +6,31 @@ test/sg.cu, test/cspa.cu): relations in each column order a join needs
 RelationalJoin per rule and per recursive body atom (that atom's DELTA
 against the other atoms' FULL), tmp relations for three-atom rules, and an
 ACopy that keeps each swapped copy of a recursive relation current.  This
-module derives that program from the rules:
+module derives that program from the rules (test/path_length.cu's too):
 
     path(x, y) :- edge(x, y).
     path(x, z) :- path(x, y), edge(y, z).
 
-Supported: binary predicates; rule bodies of one atom (a Copy, its head any
+Supported: predicates of two columns; rule bodies of one atom (a Copy, its head any
 selection of the atom's columns, e.g. vf(x, x) :- assign(x, y)), two atoms
 sharing one variable (a join on it), or three atoms in a chain a-b-c (a and
 b share one variable, b and c another; compiled through a tmp relation
 keyed for the last join, and, for a DELTA on the third atom, through one
-keyed for the first); one optional `X != Y` on the two head variables.
+keyed for the first); one optional `X != Y` on the first two head
+variables.
 Predicates without rules are inputs (EDB).  Components of mutually
 recursive predicates run as LIEs in dependency order; rules whose body has
 no predicate of the component join FULL with FULL (a Copy from a FULL runs
 once per LIE, src/copy.cu).
 
+Relations of three columns join on their first (as test/path_length.cu
+keys path); a head term may add a constant to a variable (l+1: GDL_PLUS) or
+be a number (rows computed on the host, from a rule over one input atom).
+
 Souffle's directives, as the reference's test/souffle/*.dl programs use
-them, are read too: `.decl p(a: number, b: number)` (binary, numbers),
+them, are read too: `.decl p(a: number, b: number)` (2 or 3 columns,
+numbers; `choice-domain` over all columns but the last makes that column
+dependent, as path_length's dependent_column_size 1),
 `.input p(...)` (tab-separated facts: the caller's rows, else
 <facts_dir>/p.facts, else the `filename` given, relative to the program),
 `.output p` (<out_dir>/p.csv, sorted, tab-separated), `.printsize p`;
@@ -38,35 +44,49 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from gdlog_b200 import (DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, SRC, Engine)
+from gdlog_b200 import DELTA, FULL, INNER, NEWT, OUTER, PLUS, PRED_NE, SRC, Engine
 
-_ATOM = re.compile(r"\s*([A-Za-z_]\w*)\s*\(\s*([A-Za-z_]\w*)\s*,\s*([A-Za-z_]\w*)\s*\)\s*")
+_TERM = r"[A-Za-z_]\w*(?:\s*\+\s*\d+)?|\d+"
+_ATOM = re.compile(r"\s*([A-Za-z_]\w*)\s*\(\s*(" + _TERM + r")\s*,\s*(" + _TERM + r")\s*"
+                   r"(?:,\s*(" + _TERM + r")\s*)?\)\s*")
 _NE = re.compile(r"\s*([A-Za-z_]\w*)\s*!=\s*([A-Za-z_]\w*)\s*")
 
 
 @dataclass(frozen=True)
 class Atom:
     pred: str
-    args: tuple  # two variable names
+    args: tuple  # terms: a variable; in a head also var+k or a number
 
 
 @dataclass
 class Rule:
     head: Atom
     body: list
-    ne: tuple | None = None  # (X, Y): X != Y over head variables
+    ne: tuple | None = None  # (X, Y): X != Y over the first two head terms
     text: str = ""
+
+
+def _term(t: str):
+    """(variable or None, added constant, number or None) of a term."""
+    t = t.replace(" ", "")
+    if t.isdigit():
+        return None, 0, int(t)
+    if "+" in t:
+        v, k = t.split("+")
+        return v, int(k), None
+    return t, 0, None
 
 
 @dataclass
 class Directives:
     decl: dict = field(default_factory=dict)      # predicate -> arity
+    dep: dict = field(default_factory=dict)       # predicate -> dependent columns (choice-domain)
     inputs: dict = field(default_factory=dict)    # predicate -> filename or None
     outputs: list = field(default_factory=list)
     printsize: list = field(default_factory=list)
 
 
-_DIRECTIVE = re.compile(r"^\s*\.(decl|input|output|printsize)\s+([A-Za-z_]\w*)\s*(\((.*)\))?")
+_DIRECTIVE = re.compile(r"^\s*\.(decl|input|output|printsize)\s+([A-Za-z_]\w*)\s*(\(([^)]*)\))?(.*)$")
 
 
 def _strip(text: str) -> str:
@@ -81,9 +101,16 @@ def directives(text: str) -> Directives:
         m = _DIRECTIVE.match(ln)
         if not m:
             continue
-        kind, name, args = m.group(1), m.group(2), m.group(4) or ""
+        kind, name, args, rest = m.group(1), m.group(2), m.group(4) or "", m.group(5) or ""
         if kind == "decl":
-            d.decl[name] = len([a for a in args.split(",") if a.strip()])
+            cols = [a.split(":")[0].strip() for a in args.split(",") if a.strip()]
+            d.decl[name] = len(cols)
+            cm = re.search(r"choice-domain\s*\(?\s*([^)]*)\)?", rest)
+            if cm:
+                dom = [c.strip() for c in cm.group(1).split(",") if c.strip()]
+                if dom != cols[:len(dom)] or len(dom) != len(cols) - 1:
+                    raise ValueError(f"{name}: choice-domain must be all columns but the last")
+                d.dep[name] = 1
         elif kind == "input":
             fm = re.search(r'filename\s*=\s*"([^"]*)"', args)
             d.inputs[name] = fm.group(1) if fm else None
@@ -105,7 +132,8 @@ def parse(text: str) -> list:
         fresh[0] += 1
         return f"_{fresh[0]}"
 
-    for stmt in " ".join(lines).split("."):
+    # a rule ends at a '.' that is not inside a number
+    for stmt in re.split(r"\.(?!\d)", " ".join(lines)):
         stmt = stmt.strip()
         if not stmt:
             continue
@@ -116,21 +144,25 @@ def parse(text: str) -> list:
         m = _ATOM.fullmatch(head_s)
         if not m:
             raise ValueError(f"bad head: {head_s!r}")
-        head = Atom(m.group(1), (m.group(2), m.group(3)))
+        head = Atom(m.group(1), tuple(g.replace(" ", "") for g in m.groups()[1:] if g))
         body, ne = [], None
         for part in re.split(r",(?![^(]*\))", body_s):
             ma, mn = _ATOM.fullmatch(part), _NE.fullmatch(part)
             if ma:
-                body.append(Atom(ma.group(1), (ma.group(2), ma.group(3))))
+                args = tuple(g.replace(" ", "") for g in ma.groups()[1:] if g)
+                if any(_term(t)[0] is None or _term(t)[1] for t in args):
+                    raise ValueError(f"body atoms take variables only: {part!r}")
+                body.append(Atom(ma.group(1), args))
             elif mn and ne is None:
                 ne = (mn.group(1), mn.group(2))
             else:
                 raise ValueError(f"bad body literal: {part!r}")
         bvars = {v for a in body for v in a.args}
-        if not body or not set(head.args) <= bvars:
+        hvars = {_term(t)[0] for t in head.args} - {None}
+        if not body or not hvars <= bvars:
             raise ValueError(f"head variables must appear in the body: {stmt!r}")
-        if ne and set(ne) != set(head.args):
-            raise ValueError(f"'!=' must relate the two head variables: {stmt!r}")
+        if ne and set(ne) != {_term(t)[0] for t in head.args[:2]}:
+            raise ValueError(f"'!=' must relate the first two head variables: {stmt!r}")
         if len(body) > 3:
             raise ValueError(f"at most three body atoms: {stmt!r}")
         if ne and len(body) == 1:
@@ -184,7 +216,13 @@ def _other(a: Atom, v: str) -> str:
 
 
 def _order(a: Atom, key: str) -> int:
-    """12: the atom's relation as stored; 21: swapped (key first)."""
+    """How the atom's relation is stored for a join on `key`: 12 as written,
+    21 swapped (key first), 123 a ternary relation keyed on its first
+    column."""
+    if len(a.args) == 3:
+        if a.args[0] != key:
+            raise ValueError(f"{a.pred}: a ternary relation joins on its first column")
+        return 123
     if a.args[0] == key:
         return 12
     if a.args[1] == key:
@@ -192,9 +230,14 @@ def _order(a: Atom, key: str) -> int:
     raise ValueError(f"{a} does not hold {key}")
 
 
+def _stored(a: Atom, order: int) -> tuple:
+    """The atom's variables in the stored column order."""
+    return (a.args[1], a.args[0]) if order == 21 else a.args
+
+
 @dataclass
 class Compiled:
-    relations: dict = field(default_factory=dict)   # head predicate -> Relation (order 12)
+    relations: dict = field(default_factory=dict)   # head predicate -> Relation (as written)
     iterations: dict = field(default_factory=dict)  # component name -> loop passes
     lies: dict = field(default_factory=dict)
 
@@ -203,40 +246,85 @@ class Compiled:
         return next(iter(self.relations.values()))
 
 
-def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
+def _rel_name(pred: str, order: int) -> str:
+    return {12: f"{pred}_2__1_2", 21: f"{pred}_2__2_1", 123: f"{pred}_3__1_2_3"}[order]
+
+
+def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = None) -> Compiled:
     """Compile `text` and run it on `eng` over the input relations
-    (predicate -> rows); returns the head predicates' relations."""
+    (predicate -> rows); returns the head predicates' relations.  deps:
+    dependent columns of a ternary predicate (1: its last column, as
+    Souffle's choice-domain over the others)."""
     rules = parse(text)
+    deps = deps or {}
     idb = {r.head.pred for r in rules}
+    arity = {}
     for r in rules:
+        for a in [r.head] + r.body:
+            if arity.setdefault(a.pred, len(a.args)) != len(a.args):
+                raise ValueError(f"{a.pred} is used with {arity[a.pred]} and {len(a.args)} columns")
         for a in r.body:
             if a.pred not in idb and a.pred not in inputs:
                 raise ValueError(f"no rule and no input for {a.pred!r}")
+    main = {p: (123 if arity[p] == 3 else 12) for p in arity}
     rels = {}  # (pred, order) -> Relation
 
     def rows_of(pred, order):
         if pred in inputs:
-            rows = np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, 2)
+            rows = np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, arity[pred])
         else:
-            rel = rels[(pred, 12)]
-            rows = rel.rows() if rel.size() else np.zeros((0, 2), np.uint64)
-        return rows if order == 12 else rows[:, ::-1].copy()
+            rel = rels[(pred, main[pred])]
+            rows = rel.rows() if rel.size() else np.zeros((0, arity[pred]), np.uint64)
+        return rows[:, ::-1].copy() if order == 21 else rows
+
+    def new_rel(pred, order):
+        if order == 123:
+            return eng.relation(_rel_name(pred, order), arity=3,
+                                dependent_column_size=deps.get(pred, 0))
+        return eng.relation(_rel_name(pred, order))
 
     def static(pred, order):
         if (pred, order) not in rels:
-            rel = eng.relation(f"{pred}_2__{'1_2' if order == 12 else '2_1'}")
+            rel = new_rel(pred, order)
             rows = rows_of(pred, order)
             eng.load(rel, rows if len(rows) else None)
             rels[(pred, order)] = rel
         return rels[(pred, order)]
 
+    # rules with a number in the head: rows computed here from an input
+    seeds = {}
+    for r in rules:
+        if any(_term(t)[2] is not None for t in r.head.args):
+            if len(r.body) != 1 or r.body[0].pred not in inputs:
+                raise ValueError(f"a number in the head needs one input atom: {r.text!r}")
+            a = r.body[0]
+            src = np.asarray(inputs[a.pred], dtype=np.uint64).reshape(-1, arity[a.pred])
+            cols = []
+            for t in r.head.args:
+                v, k, c = _term(t)
+                cols.append(np.full(len(src), c, np.uint64) if c is not None
+                            else src[:, a.args.index(v)] + np.uint64(k))
+            seeds.setdefault(r.head.pred, []).append(np.stack(cols, axis=1))
+    rules = [r for r in rules if not any(_term(t)[2] is not None for t in r.head.args)]
+
+    def sel_of(t, key, inner, io, outer, oo):
+        """The column selection of head term t in a join of inner and outer
+        on `key`."""
+        v, k, _ = _term(t)
+        si, so = _stored(inner, io), _stored(outer, oo)
+        base = INNER(si.index(v)) if v in si else OUTER(so.index(v)) if v in so else None
+        if base is None:
+            raise ValueError(f"variable {v} is not in the join")
+        return PLUS(base, k) if k else base
+
     out = Compiled()
     tmp_n = [0]
-    for comp in _components(rules):
+    # predicates defined by number-headed rules only come first (their rows
+    # are all seeds)
+    heads = {r.head.pred for r in rules}
+    for comp in [[p] for p in sorted(seeds) if p not in heads] + _components(rules):
         comp_set = set(comp)
         comp_rules = [r for r in rules if r.head.pred in comp_set]
-        # relations of the component: every predicate in order 12, a swapped
-        # mirror where a join needs one (kept by an ACopy)
         mirrors = set()
 
         def need(a: Atom, key: str):
@@ -249,12 +337,17 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
         tmps = []
         for r in comp_rules:
             rec = [a.pred in comp_set for a in r.body]
-            h0, h1 = r.head.args
+            hterms = r.head.args
             pred = (PRED_NE, 0, 1) if r.ne else None
             if len(r.body) == 1:
                 a = r.body[0]
-                sel = tuple(SRC(a.args.index(h)) for h in (h0, h1))
-                plan.append(("copy", a.pred, DELTA if rec[0] else FULL, r.head.pred, sel, pred))
+                sel = []
+                for t in hterms:
+                    v, k, _ = _term(t)
+                    s_ = SRC(a.args.index(v))
+                    sel.append(PLUS(s_, k) if k else s_)
+                plan.append(("copy", a.pred, main[a.pred], DELTA if rec[0] else FULL,
+                             r.head.pred, tuple(sel)))
                 continue
             if len(r.body) == 2:
                 a, b = r.body
@@ -266,11 +359,15 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
                 for d in variants:
                     outer, inner = (r.body[d], r.body[1 - d]) if d is not None else (b, a)
                     oo, io = need(outer, v), need(inner, v)
-                    sel = tuple(_sel(h, v, inner, outer) for h in (h0, h1))
+                    sel = tuple(sel_of(t, v, inner, io, outer, oo) for t in hterms)
                     plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
                                  DELTA if d is not None else FULL, r.head.pred, sel, pred))
                 continue
             a, b, c = r.body
+            if any(len(x.args) != 2 for x in (a, b, c)) or len(hterms) != 2 or \
+                    any(_term(t)[1] for t in hterms):
+                raise ValueError(f"three-atom rules are over binary relations: {r.text!r}")
+            h0, h1 = hterms
             s_ab, s_bc, s_ac = _shared(a, b), _shared(b, c), _shared(a, c)
             if len(s_ab) != 1 or len(s_bc) != 1 or s_ac or s_ab == s_bc:
                 raise ValueError(f"three atoms must form a chain a-b-c: {r.text!r}")
@@ -286,12 +383,12 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
                 for d in ([i for i in (0, 1) if rec[i]] or [None]):
                     outer, inner = ((a, b) if d == 0 else (b, a)) if d is not None else (b, a)
                     oo, io = need(outer, v1), need(inner, v1)
-                    tsel = tuple(_sel(h, v1, inner, outer) for h in (v2, ax))
+                    tsel = tuple(sel_of(x, v1, inner, io, outer, oo) for x in (v2, ax))
                     plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
                                  DELTA if d is not None else FULL, t, tsel, None))
                 tmp_atom = Atom(t, (v2, ax))
                 co = need(c, v2)
-                sel = tuple(_sel(h, v2, c, tmp_atom) for h in (h0, h1))
+                sel = tuple(sel_of(x, v2, c, co, tmp_atom, 12) for x in (h0, h1))
                 plan.append(("join", c.pred, co, FULL, t, 12, NEWT, r.head.pred, sel, pred))
             if rec[2]:
                 # a DELTA on c: tmp(v1, cy) from b and c, then a
@@ -299,28 +396,34 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
                 tmp_n[0] += 1
                 tmps.append(t)
                 oo, io = need(c, v2), need(b, v2)
-                tsel = tuple(_sel(h, v2, b, c) for h in (v1, cy))
+                tsel = tuple(sel_of(x, v2, b, io, c, oo) for x in (v1, cy))
                 plan.append(("join", b.pred, io, FULL, c.pred, oo, DELTA, t, tsel, None))
                 tmp_atom = Atom(t, (v1, cy))
                 ao = need(a, v1)
-                sel = tuple(_sel(h, v1, a, tmp_atom) for h in (h0, h1))
+                sel = tuple(sel_of(x, v1, a, ao, tmp_atom, 12) for x in (h0, h1))
                 plan.append(("join", a.pred, ao, FULL, t, 12, NEWT, r.head.pred, sel, pred))
-        # relations of this component
+        # relations of this component (their input rows and seeds first)
         for p in comp:
-            if (p, 12) not in rels:
-                rel = eng.relation(f"{p}_2__1_2")
-                rows = rows_of(p, 12) if p in inputs else np.zeros((0, 2), np.uint64)
+            if (p, main[p]) not in rels:
+                rel = new_rel(p, main[p])
+                parts = ([rows_of(p, main[p])] if p in inputs else []) + seeds.get(p, [])
+                rows = np.concatenate(parts) if parts else np.zeros((0, arity[p]), np.uint64)
                 eng.load(rel, rows if len(rows) else None)
-                rels[(p, 12)] = rel
+                rels[(p, main[p])] = rel
             if p in mirrors and (p, 21) not in rels:
-                rel = eng.relation(f"{p}_2__2_1")
-                rows = rels[(p, 12)].rows() if rels[(p, 12)].size() else np.zeros((0, 2), np.uint64)
+                rel = new_rel(p, 21)
+                base = rels[(p, 12)]
+                rows = base.rows() if base.size() else np.zeros((0, 2), np.uint64)
                 eng.load(rel, rows[:, ::-1].copy() if len(rows) else None)
                 rels[(p, 21)] = rel
         tmp_rels = {}
         for t in tmps:
             tmp_rels[t] = eng.relation(t, index_flag=False)
             eng.load(tmp_rels[t], None)
+        if not comp_rules:
+            for p in comp:
+                out.relations[p] = rels[(p, main[p])]
+            continue
         lie = eng.lie()
         statics = set()
 
@@ -335,27 +438,27 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
                 lie.add_relations(r_, True)
             return r_
 
-        # resolve the static relations first (their LIE role), then add
-        # the component's relations and ops
+        # the static relations first (their LIE role), then the
+        # component's relations and ops
         for step in plan:
             if step[0] == "copy":
-                rel_of(step[1], 12)
+                rel_of(step[1], step[2])
             else:
                 rel_of(step[1], step[2])
                 rel_of(step[4], step[5])
         for p in comp:
-            lie.add_relations(rels[(p, 12)], False)
+            lie.add_relations(rels[(p, main[p])], False)
             if p in mirrors:
                 lie.add_relations(rels[(p, 21)], False)
         for t in tmps:
             lie.add_tmp_relation(tmp_rels[t])
         for step in plan:
             if step[0] == "copy":
-                _, src, ver, head, sel, pred = step
-                lie.add_copy(rel_of(src, 12), ver, rels[(head, 12)], sel)
+                _, src, so, ver, head, sel = step
+                lie.add_copy(rel_of(src, so), ver, rels[(head, main[head])], sel)
             else:
                 _, ip, io, iv, op_, oo, ov, head, sel, pred = step
-                dest = tmp_rels[head] if head in tmp_rels else rels[(head, 12)]
+                dest = tmp_rels[head] if head in tmp_rels else rels[(head, main[head])]
                 kw = {"pred": pred} if pred else {}
                 lie.add_join(rel_of(ip, io), iv, rel_of(op_, oo), ov, dest, sel, **kw)
         for p in sorted(mirrors):
@@ -364,22 +467,10 @@ def run(eng: Engine, text: str, inputs: dict, sync=None) -> Compiled:
         out.iterations[name] = lie.fixpoint()
         out.lies[name] = lie
         for p in comp:
-            out.relations[p] = rels[(p, 12)]
+            out.relations[p] = rels[(p, main[p])]
     if sync:
         sync()
     return out
-
-
-def _sel(h: str, key: str, inner: Atom, outer: Atom) -> int:
-    """The column selection of head variable h in a join of inner and outer
-    on `key` (each stored with the key first)."""
-    if h == key:
-        return INNER(0)
-    if h == _other(inner, key):
-        return INNER(1)
-    if h == _other(outer, key):
-        return OUTER(1)
-    raise ValueError(f"variable {h} is not in the join")
 
 
 def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str | None = None,
@@ -394,8 +485,8 @@ def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str 
     text = open(path).read()
     d = directives(text)
     for name, arity in d.decl.items():
-        if arity != 2:
-            raise ValueError(f"{name}: only binary relations are supported (arity {arity})")
+        if arity not in (2, 3):
+            raise ValueError(f"{name}: relations of 2 or 3 columns only (arity {arity})")
     given = dict(inputs or {})
     for name, fname in d.inputs.items():
         if name in given:
@@ -408,8 +499,8 @@ def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str 
         found = next((c for c in cands if os.path.exists(c)), None)
         if found is None:
             raise FileNotFoundError(f"no facts for {name}: tried {cands}")
-        given[name] = read_tsv(found, 2)
-    res = run(eng, text, given, sync=sync)
+        given[name] = read_tsv(found, d.decl.get(name, 2))
+    res = run(eng, text, given, sync=sync, deps=d.dep)
     if out_dir:
         os.makedirs(out_dir, exist_ok=True)
         for name in d.outputs:
@@ -418,7 +509,8 @@ def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str 
         if name in res.relations:
             return res.relations[name].size()
         if name in given and len(given[name]):
-            return len(np.unique(np.asarray(given[name]).reshape(-1, 2), axis=0))
+            rows = np.asarray(given[name]).reshape(len(given[name]), -1)
+            return len(np.unique(rows, axis=0))
         return 0  # declared, with neither rules nor facts
 
     sizes = {name: size(name) for name in d.printsize}

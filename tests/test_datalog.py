@@ -197,3 +197,35 @@ sg(x, y) :- edge(a, x), sg(a, b), edge(b, y).
         want = P.sg(o, e).output.size()
     assert sizes["sg"] == want
     assert os.path.exists(tmp_path / "o" / "sg.csv")
+
+
+PLEN = """
+path(x, y, 1) :- edge(x, y).
+path(x, y, l+1) :- edge(x, m), path(m, y, l).
+"""
+
+
+def test_path_length_rules_equal_the_driver():
+    """Ternary path with a dependent length column (the shortest length of
+    each pair), the length computed by l+1, the first lengths from a number
+    in the head."""
+    e = W.rmat_edges(7, 300, seed=6)
+    with Engine("oracle", max_arity=3) as o:
+        r = D.run(o, PLEN, {"edge": e}, deps={"path": 1})
+        got = sorted(map(tuple, r.relations["path"].rows().tolist()))
+    with Engine("oracle", max_arity=3) as o:
+        want = sorted(map(tuple, P.path_length(o, e).output.rows().tolist()))
+    assert got == want
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SOUFFLE), reason="reference programs not present")
+def test_reference_path_length_program_runs(tmp_path):
+    e = W.layered_dag(8, 6, 4)
+    write_facts(tmp_path / "edge.facts", e)
+    with Engine("oracle", max_arity=3) as o:
+        res, sizes = D.run_file(o, os.path.join(REF_SOUFFLE, "path_length.dl"),
+                                facts_dir=str(tmp_path))
+        got = sorted(map(tuple, res.relations["path"].rows().tolist()))
+    with Engine("oracle", max_arity=3) as o:
+        want = sorted(map(tuple, P.path_length(o, e).output.rows().tolist()))
+    assert got == want and sizes["path"] == len(want)
