@@ -229,3 +229,32 @@ def test_reference_path_length_program_runs(tmp_path):
     with Engine("oracle", max_arity=3) as o:
         want = sorted(map(tuple, P.path_length(o, e).output.rows().tolist()))
     assert got == want and sizes["path"] == len(want)
+
+
+def test_strata_and_mirrors():
+    """A non-recursive component (sym) feeding a recursive one (reach) that
+    joins on its second column (a swapped mirror kept by an ACopy), checked
+    against a closure computed here."""
+    prog = """
+    sym(x, y) :- e(x, y).
+    sym(x, y) :- e(y, x).
+    reach(x, y) :- sym(x, y).
+    reach(x, z) :- reach(x, y), sym(y, z).
+    """
+    e = W.rmat_edges(6, 60, seed=8)
+    with Engine("oracle") as o:
+        r = D.run(o, prog, {"e": e})
+        got = set(map(tuple, r.relations["reach"].rows().tolist()))
+        assert [k for k in r.iterations] == ["sym", "reach"]
+    n = int(e.max()) + 1
+    adj = np.zeros((n, n), dtype=bool)
+    adj[e[:, 0].astype(int), e[:, 1].astype(int)] = True
+    adj |= adj.T
+    reach = adj.copy()
+    while True:
+        nxt = reach | ((reach.astype(np.int64) @ adj.astype(np.int64)) > 0)
+        if (nxt == reach).all():
+            break
+        reach = nxt
+    want = {(int(a), int(b)) for a, b in zip(*np.nonzero(reach))}
+    assert got == want
