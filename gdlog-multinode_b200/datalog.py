@@ -250,13 +250,47 @@ def _rel_name(pred: str, order: int) -> str:
     return {12: f"{pred}_2__1_2", 21: f"{pred}_2__2_1", 123: f"{pred}_3__1_2_3"}[order]
 
 
-def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = None) -> Compiled:
-    """Compile `text` and run it on `eng` over the input relations
-    (predicate -> rows); returns the head predicates' relations.  deps:
-    dependent columns of a ternary predicate (1: its last column, as
-    Souffle's choice-domain over the others)."""
+# A relation of the program is (predicate, order): order 12 as written, 21
+# swapped, 123 a ternary relation; a tmp relation is (name, 12).
+
+
+@dataclass
+class OpSpec:
+    kind: str                 # "join", "copy" or "acopy"
+    src: tuple                # inner of a join, source of a copy
+    src_ver: int
+    outer: tuple | None       # outer of a join
+    outer_ver: int | None
+    out: tuple
+    sel: tuple
+    pred: tuple | None = None
+
+
+@dataclass
+class Component:
+    name: str
+    preds: list
+    update: list = field(default_factory=list)   # relations the LIE updates
+    statics: list = field(default_factory=list)  # relations it reads from outside
+    tmps: list = field(default_factory=list)
+    ops: list = field(default_factory=list)      # in the LIE's order
+
+
+@dataclass
+class Program:
+    arity: dict
+    deps: dict
+    main: dict        # predicate -> its order as written (12 or 123)
+    seed_rules: list  # number-headed rules over one input atom
+    inputs: set
+    comps: list       # in dependency order
+
+
+def compile(text: str, input_names, deps: dict | None = None) -> Program:
+    """The operator program of `text`, inputs being the predicates named."""
     rules = parse(text)
-    deps = deps or {}
+    deps = dict(deps or {})
+    input_names = set(input_names)
     idb = {r.head.pred for r in rules}
     arity = {}
     for r in rules:
@@ -264,52 +298,18 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
             if arity.setdefault(a.pred, len(a.args)) != len(a.args):
                 raise ValueError(f"{a.pred} is used with {arity[a.pred]} and {len(a.args)} columns")
         for a in r.body:
-            if a.pred not in idb and a.pred not in inputs:
+            if a.pred not in idb and a.pred not in input_names:
                 raise ValueError(f"no rule and no input for {a.pred!r}")
     main = {p: (123 if arity[p] == 3 else 12) for p in arity}
-    rels = {}  # (pred, order) -> Relation
-
-    def rows_of(pred, order):
-        if pred in inputs:
-            rows = np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, arity[pred])
-        else:
-            rel = rels[(pred, main[pred])]
-            rows = rel.rows() if rel.size() else np.zeros((0, arity[pred]), np.uint64)
-        return rows[:, ::-1].copy() if order == 21 else rows
-
-    def new_rel(pred, order):
-        if order == 123:
-            return eng.relation(_rel_name(pred, order), arity=3,
-                                dependent_column_size=deps.get(pred, 0))
-        return eng.relation(_rel_name(pred, order))
-
-    def static(pred, order):
-        if (pred, order) not in rels:
-            rel = new_rel(pred, order)
-            rows = rows_of(pred, order)
-            eng.load(rel, rows if len(rows) else None)
-            rels[(pred, order)] = rel
-        return rels[(pred, order)]
-
-    # rules with a number in the head: rows computed here from an input
-    seeds = {}
+    seed_rules = []
     for r in rules:
         if any(_term(t)[2] is not None for t in r.head.args):
-            if len(r.body) != 1 or r.body[0].pred not in inputs:
+            if len(r.body) != 1 or r.body[0].pred not in input_names:
                 raise ValueError(f"a number in the head needs one input atom: {r.text!r}")
-            a = r.body[0]
-            src = np.asarray(inputs[a.pred], dtype=np.uint64).reshape(-1, arity[a.pred])
-            cols = []
-            for t in r.head.args:
-                v, k, c = _term(t)
-                cols.append(np.full(len(src), c, np.uint64) if c is not None
-                            else src[:, a.args.index(v)] + np.uint64(k))
-            seeds.setdefault(r.head.pred, []).append(np.stack(cols, axis=1))
-    rules = [r for r in rules if not any(_term(t)[2] is not None for t in r.head.args)]
+            seed_rules.append(r)
+    rules = [r for r in rules if r not in seed_rules]
 
     def sel_of(t, key, inner, io, outer, oo):
-        """The column selection of head term t in a join of inner and outer
-        on `key`."""
         v, k, _ = _term(t)
         si, so = _stored(inner, io), _stored(outer, oo)
         base = INNER(si.index(v)) if v in si else OUTER(so.index(v)) if v in so else None
@@ -317,14 +317,15 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
             raise ValueError(f"variable {v} is not in the join")
         return PLUS(base, k) if k else base
 
-    out = Compiled()
+    prog = Program(arity, deps, main, seed_rules, input_names, [])
+    heads = {r.head.pred for r in rules}
     tmp_n = [0]
     # predicates defined by number-headed rules only come first (their rows
     # are all seeds)
-    heads = {r.head.pred for r in rules}
-    for comp in [[p] for p in sorted(seeds) if p not in heads] + _components(rules):
+    for comp in [[p] for p in sorted({r.head.pred for r in seed_rules}) if p not in heads] + \
+            _components(rules):
         comp_set = set(comp)
-        comp_rules = [r for r in rules if r.head.pred in comp_set]
+        C = Component("+".join(comp), comp)
         mirrors = set()
 
         def need(a: Atom, key: str):
@@ -333,12 +334,17 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
                 mirrors.add(a.pred)
             return o
 
-        plan = []  # ("copy", ...) / ("join", ...) in rule order
-        tmps = []
-        for r in comp_rules:
+        def rel(pred, order):
+            r_ = (pred, order)
+            if pred not in comp_set and r_ not in C.statics and not pred.startswith("tmp_"):
+                C.statics.append(r_)
+            return r_
+
+        for r in [r for r in rules if r.head.pred in comp_set]:
             rec = [a.pred in comp_set for a in r.body]
             hterms = r.head.args
             pred = (PRED_NE, 0, 1) if r.ne else None
+            head = (r.head.pred, main[r.head.pred])
             if len(r.body) == 1:
                 a = r.body[0]
                 sel = []
@@ -346,8 +352,8 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
                     v, k, _ = _term(t)
                     s_ = SRC(a.args.index(v))
                     sel.append(PLUS(s_, k) if k else s_)
-                plan.append(("copy", a.pred, main[a.pred], DELTA if rec[0] else FULL,
-                             r.head.pred, tuple(sel)))
+                C.ops.append(OpSpec("copy", rel(a.pred, main[a.pred]), DELTA if rec[0] else FULL,
+                                    None, None, head, tuple(sel)))
                 continue
             if len(r.body) == 2:
                 a, b = r.body
@@ -355,13 +361,12 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
                 if len(sv) != 1:
                     raise ValueError(f"two atoms must share one variable: {r.text!r}")
                 v = sv[0]
-                variants = [i for i in (0, 1) if rec[i]] or [None]
-                for d in variants:
+                for d in ([i for i in (0, 1) if rec[i]] or [None]):
                     outer, inner = (r.body[d], r.body[1 - d]) if d is not None else (b, a)
                     oo, io = need(outer, v), need(inner, v)
                     sel = tuple(sel_of(t, v, inner, io, outer, oo) for t in hterms)
-                    plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
-                                 DELTA if d is not None else FULL, r.head.pred, sel, pred))
+                    C.ops.append(OpSpec("join", rel(inner.pred, io), FULL, rel(outer.pred, oo),
+                                        DELTA if d is not None else FULL, head, sel, pred))
                 continue
             a, b, c = r.body
             if any(len(x.args) != 2 for x in (a, b, c)) or len(hterms) != 2 or \
@@ -377,97 +382,127 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
                 raise ValueError(f"the head must hold the chain's two ends: {r.text!r}")
             if rec[0] or rec[1] or not any(rec):
                 # tmp(v2, ax) from a and b (a DELTA on a or on b), then c
-                t = f"tmp_{tmp_n[0]}"
+                t = (f"tmp_{tmp_n[0]}", 12)
                 tmp_n[0] += 1
-                tmps.append(t)
+                C.tmps.append(t)
                 for d in ([i for i in (0, 1) if rec[i]] or [None]):
                     outer, inner = ((a, b) if d == 0 else (b, a)) if d is not None else (b, a)
                     oo, io = need(outer, v1), need(inner, v1)
                     tsel = tuple(sel_of(x, v1, inner, io, outer, oo) for x in (v2, ax))
-                    plan.append(("join", inner.pred, io, FULL, outer.pred, oo,
-                                 DELTA if d is not None else FULL, t, tsel, None))
-                tmp_atom = Atom(t, (v2, ax))
+                    C.ops.append(OpSpec("join", rel(inner.pred, io), FULL, rel(outer.pred, oo),
+                                        DELTA if d is not None else FULL, t, tsel))
+                tmp_atom = Atom(t[0], (v2, ax))
                 co = need(c, v2)
                 sel = tuple(sel_of(x, v2, c, co, tmp_atom, 12) for x in (h0, h1))
-                plan.append(("join", c.pred, co, FULL, t, 12, NEWT, r.head.pred, sel, pred))
+                C.ops.append(OpSpec("join", rel(c.pred, co), FULL, t, NEWT, head, sel, pred))
             if rec[2]:
                 # a DELTA on c: tmp(v1, cy) from b and c, then a
-                t = f"tmp_{tmp_n[0]}"
+                t = (f"tmp_{tmp_n[0]}", 12)
                 tmp_n[0] += 1
-                tmps.append(t)
+                C.tmps.append(t)
                 oo, io = need(c, v2), need(b, v2)
                 tsel = tuple(sel_of(x, v2, b, io, c, oo) for x in (v1, cy))
-                plan.append(("join", b.pred, io, FULL, c.pred, oo, DELTA, t, tsel, None))
-                tmp_atom = Atom(t, (v1, cy))
+                C.ops.append(OpSpec("join", rel(b.pred, io), FULL, rel(c.pred, oo), DELTA, t,
+                                    tsel))
+                tmp_atom = Atom(t[0], (v1, cy))
                 ao = need(a, v1)
                 sel = tuple(sel_of(x, v1, a, ao, tmp_atom, 12) for x in (h0, h1))
-                plan.append(("join", a.pred, ao, FULL, t, 12, NEWT, r.head.pred, sel, pred))
-        # relations of this component (their input rows and seeds first)
-        for p in comp:
-            if (p, main[p]) not in rels:
-                rel = new_rel(p, main[p])
-                parts = ([rows_of(p, main[p])] if p in inputs else []) + seeds.get(p, [])
-                rows = np.concatenate(parts) if parts else np.zeros((0, arity[p]), np.uint64)
-                eng.load(rel, rows if len(rows) else None)
-                rels[(p, main[p])] = rel
-            if p in mirrors and (p, 21) not in rels:
-                rel = new_rel(p, 21)
-                base = rels[(p, 12)]
-                rows = base.rows() if base.size() else np.zeros((0, 2), np.uint64)
-                eng.load(rel, rows[:, ::-1].copy() if len(rows) else None)
-                rels[(p, 21)] = rel
-        tmp_rels = {}
-        for t in tmps:
-            tmp_rels[t] = eng.relation(t, index_flag=False)
-            eng.load(tmp_rels[t], None)
-        if not comp_rules:
-            for p in comp:
-                out.relations[p] = rels[(p, main[p])]
-            continue
-        lie = eng.lie()
-        statics = set()
-
-        def rel_of(pred, order):
-            if pred in tmp_rels:
-                return tmp_rels[pred]
-            if pred in comp_set:
-                return rels[(pred, order)]
-            r_ = static(pred, order)
-            if r_ not in statics:
-                statics.add(r_)
-                lie.add_relations(r_, True)
-            return r_
-
-        # the static relations first (their LIE role), then the
-        # component's relations and ops
-        for step in plan:
-            if step[0] == "copy":
-                rel_of(step[1], step[2])
-            else:
-                rel_of(step[1], step[2])
-                rel_of(step[4], step[5])
-        for p in comp:
-            lie.add_relations(rels[(p, main[p])], False)
-            if p in mirrors:
-                lie.add_relations(rels[(p, 21)], False)
-        for t in tmps:
-            lie.add_tmp_relation(tmp_rels[t])
-        for step in plan:
-            if step[0] == "copy":
-                _, src, so, ver, head, sel = step
-                lie.add_copy(rel_of(src, so), ver, rels[(head, main[head])], sel)
-            else:
-                _, ip, io, iv, op_, oo, ov, head, sel, pred = step
-                dest = tmp_rels[head] if head in tmp_rels else rels[(head, main[head])]
-                kw = {"pred": pred} if pred else {}
-                lie.add_join(rel_of(ip, io), iv, rel_of(op_, oo), ov, dest, sel, **kw)
+                C.ops.append(OpSpec("join", rel(a.pred, ao), FULL, t, NEWT, head, sel, pred))
         for p in sorted(mirrors):
-            lie.add_acopy(rels[(p, 12)], rels[(p, 21)], (SRC(1), SRC(0)))
-        name = "+".join(comp)
-        out.iterations[name] = lie.fixpoint()
-        out.lies[name] = lie
+            C.ops.append(OpSpec("acopy", (p, 12), NEWT, None, None, (p, 21), (SRC(1), SRC(0))))
         for p in comp:
-            out.relations[p] = rels[(p, main[p])]
+            C.update.append((p, main[p]))
+            if p in mirrors:
+                C.update.append((p, 21))
+        prog.comps.append(C)
+    return prog
+
+
+def seed_rows(prog: Program, inputs: dict) -> dict:
+    """Rows of the number-headed rules (predicate -> rows), from the inputs."""
+    seeds = {}
+    for r in prog.seed_rules:
+        a = r.body[0]
+        src = np.asarray(inputs[a.pred], dtype=np.uint64).reshape(-1, prog.arity[a.pred])
+        cols = []
+        for t in r.head.args:
+            v, k, c = _term(t)
+            cols.append(np.full(len(src), c, np.uint64) if c is not None
+                        else src[:, a.args.index(v)] + np.uint64(k))
+        seeds.setdefault(r.head.pred, []).append(np.stack(cols, axis=1) if len(src) else
+                                                 np.zeros((0, len(cols)), np.uint64))
+    return seeds
+
+
+def new_relation(eng: Engine, prog: Program, key: tuple, name: str | None = None):
+    pred, order = key
+    name = name or (pred if pred.startswith("tmp_") else _rel_name(pred, order))
+    if order == 123:
+        return eng.relation(name, arity=3, dependent_column_size=prog.deps.get(pred, 0))
+    return eng.relation(name, index_flag=not pred.startswith("tmp_"))
+
+
+def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = None) -> Compiled:
+    """Compile `text` and run it on `eng` over the input relations
+    (predicate -> rows); returns the head predicates' relations.  deps:
+    dependent columns of a ternary predicate (1: its last column, as
+    Souffle's choice-domain over the others)."""
+    prog = compile(text, inputs.keys(), deps)
+    seeds = seed_rows(prog, inputs)
+    rels = {}
+
+    def rows_of(pred, order):
+        if pred in inputs:
+            rows = np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, prog.arity[pred])
+        else:
+            rel = rels[(pred, prog.main[pred])]
+            rows = rel.rows() if rel.size() else np.zeros((0, prog.arity[pred]), np.uint64)
+        return rows[:, ::-1].copy() if order == 21 else rows
+
+    def load(rel, rows):
+        eng.load(rel, rows if len(rows) else None)
+
+    out = Compiled()
+    for C in prog.comps:
+        for key in C.statics:
+            if key not in rels:
+                rels[key] = new_relation(eng, prog, key)
+                load(rels[key], rows_of(*key))
+        for p in C.preds:
+            key = (p, prog.main[p])
+            if key not in rels:
+                rels[key] = new_relation(eng, prog, key)
+                parts = ([rows_of(*key)] if p in inputs else []) + seeds.get(p, [])
+                load(rels[key], np.concatenate(parts) if parts else
+                     np.zeros((0, prog.arity[p]), np.uint64))
+        for key in C.update:
+            if key not in rels:  # a mirror: the swapped rows of the predicate
+                rels[key] = new_relation(eng, prog, key)
+                load(rels[key], rows_of(key[0], 21))
+        for key in C.tmps:
+            rels[key] = new_relation(eng, prog, key)
+            load(rels[key], np.zeros((0, 2), np.uint64))
+        if C.ops:
+            lie = eng.lie()
+            for key in C.statics:
+                lie.add_relations(rels[key], True)
+            for key in C.update:
+                lie.add_relations(rels[key], False)
+            for key in C.tmps:
+                lie.add_tmp_relation(rels[key])
+            for op in C.ops:
+                if op.kind == "copy":
+                    lie.add_copy(rels[op.src], op.src_ver, rels[op.out], op.sel)
+                elif op.kind == "acopy":
+                    lie.add_acopy(rels[op.src], rels[op.out], op.sel)
+                else:
+                    kw = {"pred": op.pred} if op.pred else {}
+                    lie.add_join(rels[op.src], op.src_ver, rels[op.outer], op.outer_ver,
+                                 rels[op.out], op.sel, **kw)
+            out.iterations[C.name] = lie.fixpoint()
+            out.lies[C.name] = lie
+        for p in C.preds:
+            out.relations[p] = rels[(p, prog.main[p])]
     if sync:
         sync()
     return out
