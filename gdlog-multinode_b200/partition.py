@@ -39,7 +39,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-from gdlog_b200 import DELTA, FULL, INNER, OUTER, PRED_NE, SRC, Engine
+from gdlog_b200 import DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, SRC, Engine
 
 
 def owner(ids: np.ndarray, world: int) -> np.ndarray:
@@ -265,3 +265,295 @@ def gather_rows(rows: np.ndarray, world: int) -> np.ndarray:
     allr = np.concatenate([p.reshape(-1, 2) for p in parts]) if parts else np.zeros((0, 2))
     order = np.lexsort((allr[:, 1], allr[:, 0]))
     return allr[order]
+
+
+# ---------------------------------------------------------------------------
+# Any program of the Datalog front end, partitioned.
+
+
+def _select(rows: np.ndarray, sel: tuple) -> np.ndarray:
+    """A Copy's tuple generator on the host: column SRC(c) of the source,
+    plus the constant a GDL_PLUS term carries (bits 8 and up)."""
+    if not len(rows):
+        return np.zeros((0, len(sel)), np.uint64)
+    return np.stack([rows[:, g & 0xFF] + np.uint64(g >> 8) for g in sel], axis=1)
+
+
+def _route_owned(rows: np.ndarray, world: int, device) -> np.ndarray:
+    """Rows of two or three columns to the owner of their first column.  A
+    ternary row travels as two packed keys, (c0, c1) and (c0, c2), with the
+    same destinations, so the received halves line up."""
+    dest = owner(rows[:, 0], world) if len(rows) else np.zeros(0, np.int64)
+    if rows.shape[1] == 2:
+        return route(rows, dest, world, device)
+    a = route(rows[:, :2], dest, world, device)
+    b = route(rows[:, [0, 2]], dest, world, device)
+    return np.concatenate([a, b[:, 1:]], axis=1)
+
+
+def _sum_all(counts: list, device) -> list:
+    """Element-wise sum of a count vector over the ranks (one all_reduce)."""
+    t = torch.tensor(counts, dtype=torch.int64, device=device if device is not None else "cpu")
+    dist.all_reduce(t)
+    return [int(x) for x in t.tolist()]
+
+
+def _cat(parts: list, arity: int) -> np.ndarray:
+    return np.concatenate(parts) if parts else np.zeros((0, arity), np.uint64)
+
+
+class _Partition:
+    """This rank's FULL partition of an updated relation, grown by the
+    update step: received NEWT rows are copied into it by a one-pass LIE
+    whose set difference (over arity - dependent columns,
+    src/lie.cu:131-138) keeps the new ones as its DELTA."""
+
+    def __init__(self, eng: Engine, name: str, arity: int, dep: int, rows: np.ndarray):
+        self.eng, self.arity = eng, arity
+        self.full = eng.relation(name, arity=arity, dependent_column_size=dep, index_flag=False)
+        eng.load(self.full, rows if len(rows) else None)
+        self.recv = eng.relation(name + "_recv", arity=arity, dependent_column_size=dep,
+                                 index_flag=False)
+        self.lie = eng.lie()
+        self.lie.set_reload_full(False)
+        self.lie.add_relations(self.recv, False)
+        self.lie.add_relations(self.full, False)
+        self.lie.add_copy(self.recv, DELTA, self.full, tuple(SRC(c) for c in range(arity)))
+        self.lie.max_iteration = 0
+
+    def rows(self) -> np.ndarray:
+        return self.full.rows() if self.full.size() else np.zeros((0, self.arity), np.uint64)
+
+    def merge(self, rows: np.ndarray) -> np.ndarray:
+        # received rows deduplicated first: DELTA at LIE start is the first
+        # |FULL| rows in load order (src/lie.cu:49-59), a repeat would hide one
+        if len(rows):
+            rows = np.unique(rows, axis=0)
+        self.eng.load(self.recv, rows if len(rows) else None)
+        self.lie.fixpoint()
+        return self.full.rows(DELTA) if self.full.size(DELTA) else \
+            np.zeros((0, self.arity), np.uint64)
+
+
+@dataclass
+class PartProgram:
+    iterations: dict = field(default_factory=dict)  # component -> loop passes
+    full: dict = field(default_factory=dict)        # head predicate -> this rank's rows
+    relations: int = 0                              # engine relations used
+    lies: int = 0                                   # engine LIEs used
+
+
+def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: int,
+                        deps: dict | None = None, device=None) -> PartProgram:
+    """Run a Datalog program of the front end (datalog.py) with every
+    relation hash-partitioned on its first column; every rank passes the
+    same inputs (predicate -> rows; no row repeated, and none that a rule
+    with numbers in its head also yields) and gets its
+    partition of each head predicate, and the loop-pass count of each
+    component, which equal those of datalog.run on one engine.
+
+    The first column is each stored relation's join key (a swapped copy is
+    stored for a join on the second), so every join reads owned keys only.
+    Each component's LIE runs its ops in order, one pass at a time, as
+    LIE::fixpoint_loop does (src/lie.cu:62-87):
+      * a join is a one-pass LIE of the engine over the local rows of the
+        versions it reads (its inner's FULL; its outer's FULL, DELTA or a
+        tmp relation's NEWT); the rows it generates go to the owners of
+        their first column and collect there as the output's NEWT;
+      * a Copy or an ACopy applies its column selection on the host and
+        routes the same way; a Copy from FULL runs once per LIE
+        (src/lie.cu:69-75);
+      * the update step merges each relation's NEWT into its partition on
+        the engine (set difference and flush, src/lie.cu:93-198), DELTA
+        being what was new; the loop ends when no rank found a tuple.
+    The reference's rules on empty operands decide on global sizes (one
+    all_reduce): a join whose outer is empty does nothing, one whose inner
+    is empty zeroes its outer's version (src/join.cu:38-45), a Copy or
+    ACopy from an empty source clears its destination's NEWT
+    (src/copy.cu:24-27, src/acopy.cu:14-18).  A FULL zeroed that way stays
+    empty until a flush refills it, or the LIE ends (src/lie.cu:219-254)."""
+    import datalog as DL
+    prog = DL.compile(text, inputs.keys(), deps)
+    seeds = DL.seed_rows(prog, inputs)
+
+    def arity_of(key):
+        return 3 if key[1] == 123 else 2
+
+    def none(key):
+        return np.zeros((0, arity_of(key)), np.uint64)
+
+    def owned(rows):
+        return rows[owner(rows[:, 0], world) == rank] if len(rows) else rows
+
+    def input_rows(pred):
+        return np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, prog.arity[pred])
+
+    parts = {}       # updated (predicate, order) -> _Partition
+    static = {}      # (predicate, order) read from outside a component -> engine relation
+    host_full = {}   # (predicate, order) -> this rank's FULL rows
+    zero_full = set()
+    full_gen = {}    # updated key -> how many times its FULL changed
+    scratch = {}     # operand slot -> [relation, what it holds]
+    outs = {}
+    lies = {}
+    res = PartProgram()
+
+    def full_rows(key):
+        return none(key) if key in zero_full else host_full[key]
+
+    def operand(slot, key, token, rows):
+        """An engine relation holding `rows` (one per operand slot, loaded
+        again only when what it should hold changed)."""
+        if slot not in scratch:
+            name = f"{DL._rel_name(*key) if not key[0].startswith('tmp_') else key[0]}_{slot[1]}"
+            scratch[slot] = [DL.new_relation(eng, prog, key, name=name), None]
+        rel, held = scratch[slot]
+        if held != token:
+            eng.load(rel, rows if len(rows) else None)
+            scratch[slot][1] = token
+        return rel
+
+    def inner_of(key):
+        if key in static:
+            return static[key]
+        return operand((key, "full"), key, ("full", full_gen[key]), host_full[key])
+
+    for C in prog.comps:
+        for key in C.statics:
+            if key in static:
+                continue
+            pred, order = key
+            if pred in inputs:
+                rows = input_rows(pred)
+                rows = owned(rows[:, ::-1].copy() if order == 21 else rows)
+            else:  # a lower component's predicate: swapped rows go to new owners
+                base = full_rows((pred, prog.main[pred]))
+                rows = _route_owned(base[:, ::-1].copy(), world, device) if order == 21 else base
+                if order == 21 and len(rows):
+                    rows = np.unique(rows, axis=0)
+            rel = DL.new_relation(eng, prog, key)
+            eng.load(rel, rows if len(rows) else None)
+            static[key] = rel
+            host_full[key] = rel.rows() if rel.size() else none(key)
+
+        def start(key, rows):
+            name = DL._rel_name(*key) + "_part"
+            parts[key] = _Partition(eng, name, arity_of(key), prog.deps.get(key[0], 0)
+                                    if key[1] == 123 else 0, rows)
+            host_full[key] = parts[key].rows()
+            full_gen[key] = 0
+
+        for p in C.preds:
+            key = (p, prog.main[p])
+            rows = [input_rows(p)] if p in inputs else []
+            rows = owned(_cat(rows + seeds.get(p, []), prog.arity[p]))
+            start(key, rows)
+        for key in C.update:
+            if key in parts:
+                continue
+            # a swapped mirror: the predicate's input rows, else its rows so far
+            p = key[0]
+            if p in inputs:
+                start(key, owned(input_rows(p)[:, ::-1].copy()))
+            else:
+                base = host_full[(p, prog.main[p])]
+                start(key, _route_owned(base[:, ::-1].copy(), world, device))
+        if not C.ops:
+            continue
+        # LIE start: DELTA := FULL (src/lie.cu:49-59; inputs without repeats)
+        delta = {key: host_full[key] for key in C.update}
+        copied = set()
+        it = 0
+        while True:
+            it += 1
+            newt = {key: [] for key in C.update + C.tmps}
+            zero_delta = set()
+
+            def version(key, ver):
+                if ver == DELTA:
+                    return none(key) if key in zero_delta else delta[key]
+                if ver == NEWT:
+                    return _cat(newt[key], arity_of(key))
+                return full_rows(key)
+
+            for i, op in enumerate(C.ops):
+                if op.kind == "copy" and op.src_ver == FULL:
+                    if i in copied:
+                        continue
+                    copied.add(i)
+                if op.kind in ("copy", "acopy"):
+                    src = version(op.src, NEWT if op.kind == "acopy" else op.src_ver)
+                    if _sum_all([len(src)], device)[0] == 0:
+                        newt[op.out] = []
+                        continue
+                    got = _route_owned(_select(src, op.sel), world, device)
+                    newt[op.out] = [got] if op.kind == "acopy" else newt[op.out] + [got]
+                    continue
+                if op.src_ver != FULL:
+                    raise ValueError("a join's inner is read as FULL")
+                rin = version(op.src, op.src_ver)
+                rout = version(op.outer, op.outer_ver)
+                n_in, n_out = _sum_all([len(rin), len(rout)], device)
+                if n_out == 0:
+                    continue
+                if n_in == 0:
+                    if op.outer_ver == DELTA:
+                        zero_delta.add(op.outer)
+                    elif op.outer_ver == NEWT:
+                        newt[op.outer] = []
+                    else:
+                        zero_full.add(op.outer)
+                    continue
+                got = none(op.out)
+                if len(rin) and len(rout):
+                    inner = inner_of(op.src)
+                    if op.outer_ver == FULL:
+                        outer = inner_of(op.outer)
+                    else:
+                        tok = (it, i) if op.outer_ver == NEWT else ("delta", it)
+                        outer = operand((op.outer, "delta" if op.outer_ver == DELTA else "newt"),
+                                        op.outer, tok, rout)
+                    a = arity_of(op.out)
+                    if a not in outs:
+                        outs[a] = eng.relation(f"part_out{a}", arity=a, index_flag=False)
+                    lkey = (i, C.name)
+                    if lkey not in lies:
+                        lie = eng.lie()
+                        lie.add_relations(inner, True)
+                        if outer is not inner:
+                            lie.add_relations(outer, True)
+                        lie.add_relations(outs[a], False)
+                        kw = {"pred": op.pred} if op.pred else {}
+                        lie.add_join(inner, FULL, outer, FULL, outs[a], op.sel, **kw)
+                        lie.max_iteration = 0
+                        lies[lkey] = (lie, inner, outer)
+                    lie, bi, bo = lies[lkey]
+                    assert bi is inner and bo is outer
+                    eng.load(outs[a], None)
+                    lie.fixpoint()
+                    got = outs[a].rows() if outs[a].size() else got
+                newt[op.out].append(_route_owned(got, world, device))
+            # the update step (src/lie.cu:93-198)
+            new = []
+            for key in C.update:
+                rows = _cat(newt[key], arity_of(key))
+                delta[key] = parts[key].merge(rows) if len(rows) else none(key)
+                new.append(len(delta[key]))
+            grew = _sum_all(new, device)
+            for key, n, n_all in zip(C.update, new, grew):
+                if n:
+                    host_full[key] = parts[key].rows()
+                    full_gen[key] += 1
+                if n_all:
+                    zero_full.discard(key)
+            if sum(grew) == 0:
+                break
+        for key in C.update:  # LIE end: FULL flattened again (src/lie.cu:219-254)
+            zero_full.discard(key)
+        res.iterations[C.name] = it
+    for C in prog.comps:
+        for p in C.preds:
+            res.full[p] = host_full[(p, prog.main[p])]
+    res.relations = len(eng.relations)
+    res.lies = len(lies) + len(parts)
+    return res

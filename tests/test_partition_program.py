@@ -1,0 +1,123 @@
+"""Any Datalog program of the front end, partitioned (partition.py:
+partitioned_program): 2 and 3 gloo ranks, each with the oracle as its
+engine, against datalog.run on one oracle engine — the same rows for every
+head predicate (the union of the partitions, which are disjoint) and the
+same loop-pass count for every component."""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import datalog as D
+import partition as PT
+import workloads as W
+from gdlog_b200 import Engine
+
+TC = """
+path(x, y) :- edge(x, y).
+path(x, z) :- path(x, y), edge(y, z).
+"""
+
+SG = """
+sg(x, y) :- edge(p, x), edge(p, y), x != y.
+sg(x, y) :- edge(a, x), sg(a, b), edge(b, y).
+"""
+
+CSPA = """
+vf(y, y) :- assign(x, y).
+vf(x, x) :- assign(x, y).
+vf(x, y) :- assign(x, y).
+ma(y, y) :- assign(x, y).
+ma(x, x) :- assign(x, y).
+vf(x, y) :- vf(x, z), vf(z, y).
+va(x, y) :- vf(z, x), vf(z, y).
+vf(x, y) :- assign(x, z), ma(z, y).
+ma(x, w) :- deref(y, x), va(y, z), deref(z, w).
+va(x, y) :- vf(z, x), ma(z, w), vf(w, y).
+"""
+
+PLEN = """
+path(x, y, 1) :- edge(x, y).
+path(x, y, l+1) :- edge(x, m), path(m, y, l).
+"""
+
+STRATA = """
+sym(x, y) :- e(x, y).
+sym(x, y) :- e(y, x).
+reach(x, y) :- sym(x, y).
+reach(x, z) :- reach(x, y), sym(y, z).
+"""
+
+
+def _u(rows):
+    return np.unique(np.asarray(rows, dtype=np.uint64), axis=0)
+
+
+def _cspa():
+    assign, deref = W.cspa_facts(120, 240, 90, seed=1)
+    return {"assign": _u(assign), "deref": _u(deref)}
+
+
+CASES = {
+    "tc_grid_8": (TC, lambda: {"edge": _u(W.grid_edges(8, 8))}, None),
+    "tc_rmat_s7": (TC, lambda: {"edge": _u(W.rmat_edges(7, 300, seed=5))}, None),
+    "sg_rmat_s7": (SG, lambda: {"edge": _u(W.rmat_edges(7, 300, seed=3))}, None),
+    "cspa_120": (CSPA, _cspa, None),
+    "plen_rmat_s6": (PLEN, lambda: {"edge": _u(W.rmat_edges(6, 150, seed=6))}, {"path": 1}),
+    "strata_rmat_s6": (STRATA, lambda: {"e": _u(W.rmat_edges(6, 60, seed=8))}, None),
+}
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _sorted(rows):
+    return sorted(map(tuple, np.asarray(rows).tolist()))
+
+
+def _rank(rank, world, port, case, out_dir):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        text, inputs, deps = CASES[case]
+        with Engine("oracle", max_arity=3) as eng:
+            res = PT.partitioned_program(eng, text, inputs(), rank, world, deps=deps)
+        out = {"iterations": res.iterations, "relations": res.relations, "rows": {}, "n": {}}
+        for p, rows in sorted(res.full.items()):
+            parts = [None] * world
+            dist.all_gather_object(parts, np.asarray(rows, dtype=np.uint64))
+            out["rows"][p] = [list(r) for r in _sorted(np.concatenate(parts))]
+            out["n"][p] = len(rows)
+        with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+            json.dump(out, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case,world", [(c, 2) for c in sorted(CASES)] +
+                         [("cspa_120", 3), ("sg_rmat_s7", 3), ("plen_rmat_s6", 3)])
+def test_partitioned_program_equals_single(case, world, tmp_path):
+    mp.spawn(_rank, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
+    outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
+    text, inputs, deps = CASES[case]
+    with Engine("oracle", max_arity=3) as o:
+        r = D.run(o, text, inputs(), deps=deps)
+        want = {p: [list(x) for x in _sorted(rel.rows() if rel.size() else [])]
+                for p, rel in r.relations.items()}
+        iters = dict(r.iterations)
+    for o in outs:
+        assert o["iterations"] == iters
+        assert sorted(o["rows"]) == sorted(want)
+        for p in want:
+            assert o["rows"][p] == want[p], p
+        # the engine's relation table holds every relation a rank uses
+        assert o["relations"] <= 64
+    for p in want:  # disjoint partitions
+        assert sum(o["n"][p] for o in outs) == len(want[p])
