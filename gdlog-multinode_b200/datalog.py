@@ -35,7 +35,8 @@ dependent, as path_length's dependent_column_size 1),
 <facts_dir>/p.facts, else the `filename` given, relative to the program),
 `.output p` (<out_dir>/p.csv, sorted, tab-separated), `.printsize p`;
 `_` is a fresh variable.  `python datalog.py prog.dl --facts DIR --out DIR`
-runs a program file.
+runs a program file; under torchrun (WORLD_SIZE > 1) it runs with every
+relation partitioned over the ranks (partition.run_file_partitioned).
 """
 from __future__ import annotations
 
@@ -516,6 +517,34 @@ def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str 
     to <out_dir>/<name>.csv.  Returns (Compiled, {name: size} for the
     `.printsize` relations)."""
     import os
+    text, d, given = read_program(path, facts_dir, inputs)
+    res = run(eng, text, given, sync=sync, deps=d.dep)
+    if out_dir:
+        os.makedirs(out_dir, exist_ok=True)
+        for name in d.outputs:
+            res.relations[name].dump_tsv(os.path.join(out_dir, name + ".csv"))
+
+    def size(name):
+        if name in res.relations:
+            return res.relations[name].size()
+        return input_size(given, name)
+
+    sizes = {name: size(name) for name in d.printsize}
+    return res, sizes
+
+
+def input_size(given: dict, name: str) -> int:
+    """Tuples of an input relation (distinct rows; 0 when declared only)."""
+    if name in given and len(given[name]):
+        rows = np.asarray(given[name]).reshape(len(given[name]), -1)
+        return len(np.unique(rows, axis=0))
+    return 0
+
+
+def read_program(path: str, facts_dir: str | None = None, inputs: dict | None = None) -> tuple:
+    """A program file's text, its directives and its input rows (the
+    caller's, else <facts_dir>/<name>.facts, else the directive's file)."""
+    import os
     from gdlog_b200 import read_tsv
     text = open(path).read()
     d = directives(text)
@@ -535,21 +564,7 @@ def run_file(eng: Engine, path: str, facts_dir: str | None = None, out_dir: str 
         if found is None:
             raise FileNotFoundError(f"no facts for {name}: tried {cands}")
         given[name] = read_tsv(found, d.decl.get(name, 2))
-    res = run(eng, text, given, sync=sync, deps=d.dep)
-    if out_dir:
-        os.makedirs(out_dir, exist_ok=True)
-        for name in d.outputs:
-            res.relations[name].dump_tsv(os.path.join(out_dir, name + ".csv"))
-    def size(name):
-        if name in res.relations:
-            return res.relations[name].size()
-        if name in given and len(given[name]):
-            rows = np.asarray(given[name]).reshape(len(given[name]), -1)
-            return len(np.unique(rows, axis=0))
-        return 0  # declared, with neither rules nor facts
-
-    sizes = {name: size(name) for name in d.printsize}
-    return res, sizes
+    return text, d, given
 
 
 def main():
@@ -561,6 +576,30 @@ def main():
     ap.add_argument("--out", default=None, help="directory for <name>.csv outputs")
     ap.add_argument("--engine", default="gpu", choices=["gpu", "oracle"])
     a = ap.parse_args()
+    import os
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        # one rank per GPU (torchrun): every relation partitioned over the ranks
+        import torch
+        import torch.distributed as dist
+
+        import partition
+        device = None
+        if a.engine == "gpu":
+            device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+            torch.cuda.set_device(device)
+        dist.init_process_group("nccl" if device is not None else "gloo")
+        try:
+            rank = dist.get_rank()
+            with Engine(a.engine) as eng:
+                res, sizes = partition.run_file_partitioned(eng, a.program, rank, world, a.facts,
+                                                            a.out, device=device)
+            if rank == 0:
+                print(json.dumps({"sizes": sizes, "iterations": res.iterations,
+                                  "ranks": world}))
+        finally:
+            dist.destroy_process_group()
+        return
     with Engine(a.engine) as eng:
         res, sizes = run_file(eng, a.program, a.facts, a.out, sync=getattr(eng, "sync", None))
         print(json.dumps({"sizes": sizes, "iterations": res.iterations}))

@@ -557,3 +557,37 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
     res.relations = len(eng.relations)
     res.lies = len(lies) + len(parts)
     return res
+
+
+def run_file_partitioned(eng: Engine, path: str, rank: int, world: int,
+                         facts_dir: str | None = None, out_dir: str | None = None,
+                         inputs: dict | None = None, device=None) -> tuple:
+    """datalog.run_file with every relation partitioned over the ranks:
+    each rank reads the inputs (repeated rows dropped, as the reference's
+    load does, src/relation.cu:570-593) and runs its partition; rank 0
+    writes each `.output` relation (the union of the partitions, sorted,
+    tab-separated) to <out_dir>/<name>.csv.  Returns (PartProgram,
+    {name: size} for the `.printsize` relations), the sizes on every rank."""
+    import os
+
+    import datalog as DL
+    from gdlog_b200 import write_tsv
+    text, d, given = DL.read_program(path, facts_dir, inputs)
+    given = {k: np.unique(np.asarray(v, dtype=np.uint64).reshape(len(v), -1), axis=0)
+             for k, v in given.items()}
+    res = partitioned_program(eng, text, given, rank, world, deps=d.dep, device=device)
+    names = sorted(d.printsize)
+    counts = _sum_all([len(res.full[n]) if n in res.full else 0 for n in names], device)
+    sizes = {n: c if n in res.full else DL.input_size(given, n) for n, c in zip(names, counts)}
+    if out_dir:
+        if rank == 0:
+            os.makedirs(out_dir, exist_ok=True)
+        for n in d.outputs:
+            parts = [None] * world
+            dist.all_gather_object(parts, res.full.get(n))
+            if rank:
+                continue
+            rows = np.concatenate(parts) if n in res.full else given[n]
+            rows = rows[np.lexsort(rows.T[::-1])] if len(rows) else rows
+            write_tsv(os.path.join(out_dir, n + ".csv"), rows)
+    return res, sizes

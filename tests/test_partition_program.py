@@ -121,3 +121,39 @@ def test_partitioned_program_equals_single(case, world, tmp_path):
         assert o["relations"] <= 64
     for p in want:  # disjoint partitions
         assert sum(o["n"][p] for o in outs) == len(want[p])
+
+
+def test_program_file_under_torchrun(tmp_path):
+    """`datalog.py prog.dl` under torchrun (2 gloo ranks, the oracle as each
+    rank's engine) writes the same sorted output file and prints the same
+    sizes and loop-pass counts as a run on one engine."""
+    import subprocess
+    import sys
+    prog = tmp_path / "cspa.dl"
+    prog.write_text(".decl assign(a: number, b: number)\n.input assign\n"
+                    ".decl deref(a: number, b: number)\n.input deref\n"
+                    ".decl vf(a: number, b: number)\n.output vf\n.printsize vf\n"
+                    ".decl ma(a: number, b: number)\n.printsize ma\n"
+                    ".decl va(a: number, b: number)\n.output va\n.printsize assign\n" + CSPA)
+    assign, deref = W.cspa_facts(100, 200, 80, seed=4)
+    for name, rows in (("assign", assign), ("deref", deref)):
+        with open(tmp_path / f"{name}.facts", "w") as f:
+            for a, b in np.asarray(rows).tolist():
+                f.write(f"{a}\t{b}\n")
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = os.path.join(here, "gdlog-multinode_b200", "datalog.py")
+    common = [str(prog), "--facts", str(tmp_path), "--engine", "oracle"]
+    one = subprocess.run([sys.executable, script, *common, "--out", str(tmp_path / "one")],
+                         capture_output=True, text=True, check=True, timeout=300)
+    two = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                          "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                          "--master-port", str(free_port()), script, *common,
+                          "--out", str(tmp_path / "two")],
+                         capture_output=True, text=True, check=True, timeout=300)
+    a = json.loads(one.stdout.strip().splitlines()[-1])
+    b = json.loads([ln for ln in two.stdout.strip().splitlines() if ln.startswith("{")][-1])
+    assert b["ranks"] == 2
+    assert (b["sizes"], b["iterations"]) == (a["sizes"], a["iterations"])
+    for name in ("vf", "va"):
+        assert (tmp_path / "two" / f"{name}.csv").read_text() == \
+            (tmp_path / "one" / f"{name}.csv").read_text()
