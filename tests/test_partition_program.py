@@ -52,6 +52,13 @@ reach(x, y) :- sym(x, y).
 reach(x, z) :- reach(x, y), sym(y, z).
 """
 
+EMPTY = """
+p(x, y) :- e(x, y).
+p(x, z) :- p(x, y), f(y, z).
+q(x, y) :- f(x, y).
+q(x, z) :- q(x, y), e(y, z).
+"""
+
 
 def _u(rows):
     return np.unique(np.asarray(rows, dtype=np.uint64), axis=0)
@@ -69,6 +76,12 @@ CASES = {
     "cspa_120": (CSPA, _cspa, None),
     "plen_rmat_s6": (PLEN, lambda: {"edge": _u(W.rmat_edges(6, 150, seed=6))}, {"path": 1}),
     "strata_rmat_s6": (STRATA, lambda: {"e": _u(W.rmat_edges(6, 60, seed=8))}, None),
+    # an empty inner zeroes the outer's DELTA, a Copy from an empty input
+    # clears its destination's NEWT (src/join.cu:38-45, src/copy.cu:24-27)
+    "empty_inner": (EMPTY, lambda: {"e": _u(W.grid_edges(5, 5)),
+                                    "f": np.zeros((0, 2), np.uint64)}, None),
+    # every id a multiple of 6: at 2 and 3 ranks one rank owns every key
+    "one_owner": (TC, lambda: {"edge": _u(W.grid_edges(6, 6)) * np.uint64(6)}, None),
 }
 
 
@@ -102,7 +115,8 @@ def _rank(rank, world, port, case, out_dir):
 
 
 @pytest.mark.parametrize("case,world", [(c, 2) for c in sorted(CASES)] +
-                         [("cspa_120", 3), ("sg_rmat_s7", 3), ("plen_rmat_s6", 3)])
+                         [("cspa_120", 3), ("sg_rmat_s7", 3), ("plen_rmat_s6", 3),
+                          ("one_owner", 3)])
 def test_partitioned_program_equals_single(case, world, tmp_path):
     mp.spawn(_rank, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
     outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
