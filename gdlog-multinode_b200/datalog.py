@@ -477,9 +477,11 @@ def run(eng: Engine, text: str, inputs: dict, sync=None, deps: dict | None = Non
                 load(rels[key], np.concatenate(parts) if parts else
                      np.zeros((0, prog.arity[p]), np.uint64))
         for key in C.update:
-            if key not in rels:  # a mirror: the swapped rows of the predicate
+            if key not in rels:  # a mirror: the predicate's loaded rows, swapped
+                base = rels[(key[0], prog.main[key[0]])]
+                rows = base.rows() if base.size() else np.zeros((0, 2), np.uint64)
                 rels[key] = new_relation(eng, prog, key)
-                load(rels[key], rows_of(key[0], 21))
+                load(rels[key], rows[:, ::-1].copy())
         for key in C.tmps:
             rels[key] = new_relation(eng, prog, key)
             load(rels[key], np.zeros((0, 2), np.uint64))

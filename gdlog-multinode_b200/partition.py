@@ -451,13 +451,9 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
         for key in C.update:
             if key in parts:
                 continue
-            # a swapped mirror: the predicate's input rows, else its rows so far
-            p = key[0]
-            if p in inputs:
-                start(key, owned(input_rows(p)[:, ::-1].copy()))
-            else:
-                base = host_full[(p, prog.main[p])]
-                start(key, _route_owned(base[:, ::-1].copy(), world, device))
+            # a swapped mirror: the predicate's loaded rows, to their new owners
+            base = host_full[(key[0], prog.main[key[0]])]
+            start(key, _route_owned(base[:, ::-1].copy(), world, device))
         if not C.ops:
             continue
         # LIE start: DELTA := FULL (src/lie.cu:49-59; inputs without repeats)

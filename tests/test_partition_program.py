@@ -60,6 +60,17 @@ q(x, z) :- q(x, y), e(y, z).
 """
 
 
+MIRROR_SEEDS = """
+r(x, 0) :- e(x, y).
+r(x, z) :- r(x, y), e(y, z).
+"""
+
+
+def _mirror_seeds():
+    r = _u(W.rmat_edges(5, 20, seed=9))
+    return {"e": _u(W.rmat_edges(5, 40, seed=2)), "r": r[r[:, 1] != 0]}
+
+
 def _u(rows):
     return np.unique(np.asarray(rows, dtype=np.uint64), axis=0)
 
@@ -82,6 +93,7 @@ CASES = {
                                     "f": np.zeros((0, 2), np.uint64)}, None),
     # every id a multiple of 6: at 2 and 3 ranks one rank owns every key
     "one_owner": (TC, lambda: {"edge": _u(W.grid_edges(6, 6)) * np.uint64(6)}, None),
+    "mirror_seeds": (MIRROR_SEEDS, lambda: _mirror_seeds(), None),
 }
 
 
@@ -171,3 +183,22 @@ def test_program_file_under_torchrun(tmp_path):
     for name in ("vf", "va"):
         assert (tmp_path / "two" / f"{name}.csv").read_text() == \
             (tmp_path / "one" / f"{name}.csv").read_text()
+
+
+
+def test_mirror_holds_seeds_and_inputs():
+    """A predicate with input rows and a number-headed rule, joined on its
+    second column (a swapped mirror): the mirror starts from all its loaded
+    rows.  Checked against a closure computed here; the partitioned run is
+    the case mirror_seeds above."""
+    inputs = _mirror_seeds()
+    with Engine("oracle") as o:
+        got = _sorted(D.run(o, MIRROR_SEEDS, inputs).relations["r"].rows())
+    r = set(map(tuple, inputs["r"].tolist())) | {(x, 0) for x, _ in inputs["e"].tolist()}
+    e = inputs["e"].tolist()
+    while True:
+        new = {(x, z) for (x, y) in r for (y2, z) in e if y2 == y} - r
+        if not new:
+            break
+        r |= new
+    assert got == sorted(r)
