@@ -48,13 +48,15 @@ def owner(ids: np.ndarray, world: int) -> np.ndarray:
 
 
 def _pack(rows: np.ndarray) -> torch.Tensor:
-    r = np.asarray(rows, dtype=np.int64).reshape(-1, 2)
-    return torch.from_numpy((r[:, 0] << 32) | r[:, 1])
+    """Rows of two ids below 2^32 as one 64-bit key each (c0 << 32 | c1),
+    carried in an int64 tensor bit for bit."""
+    r = np.asarray(rows, dtype=np.uint64).reshape(-1, 2)
+    return torch.from_numpy(((r[:, 0] << np.uint64(32)) | r[:, 1]).view(np.int64))
 
 
 def _unpack(keys: torch.Tensor) -> np.ndarray:
-    k = keys.cpu().numpy().astype(np.int64)
-    return np.stack([k >> 32, k & 0xFFFFFFFF], axis=1).astype(np.uint64)
+    k = keys.cpu().numpy().view(np.uint64)
+    return np.stack([k >> np.uint64(32), k & np.uint64(0xFFFFFFFF)], axis=1)
 
 
 def route(rows: np.ndarray, dest: np.ndarray, world: int, device=None) -> np.ndarray:

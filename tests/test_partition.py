@@ -101,8 +101,10 @@ def test_partitioned_sg_equals_single(case, world, tmp_path):
 def test_owner_and_route_shapes():
     ids = np.array([0, 1, 2, 3, 7, 10])
     assert PT.owner(ids, 3).tolist() == [0, 1, 2, 0, 1, 1]
-    rows = np.array([[5, 1], [2, 3], [1 << 20, 7]], dtype=np.uint64)
+    rows = np.array([[5, 1], [2, 3], [1 << 20, 7], [(1 << 32) - 1, (1 << 31) + 5]],
+                    dtype=np.uint64)
     assert (PT._unpack(PT._pack(rows)) == rows).all()
+    assert PT._unpack(PT._pack(np.zeros((0, 2), np.uint64))).shape == (0, 2)
 
 
 @pytest.mark.gpu
