@@ -539,8 +539,8 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                 new.append(len(delta[key]))
             grew = _sum_all(new, device)
             for key, n, n_all in zip(C.update, new, grew):
-                if n:
-                    host_full[key] = parts[key].rows()
+                if n:  # DELTA is disjoint from FULL: the flushed FULL is their union
+                    host_full[key] = np.concatenate([host_full[key], delta[key]])
                     full_gen[key] += 1
                 if n_all:
                     zero_full.discard(key)
