@@ -173,6 +173,24 @@ def test_reference_souffle_programs_run(tmp_path):
     assert sizes["ValueFlow"] == len(want["ValueFlow"])
 
 
+@pytest.mark.skipif(not os.path.isdir(REF_SOUFFLE), reason="reference programs not present")
+def test_reference_tc_program_runs(tmp_path):
+    """The reference's tc.dl: closure by a rule whose two body atoms are
+    both path (each one's DELTA against the other's FULL, a swapped mirror
+    for the join on the first atom's second column); the same tuples as the
+    linear driver, in fewer loop passes."""
+    e = W.rmat_edges(7, 300, seed=5)
+    write_facts(tmp_path / "edge.facts", e)
+    with Engine("oracle") as o:
+        res, sizes = D.run_file(o, os.path.join(REF_SOUFFLE, "tc.dl"), facts_dir=str(tmp_path))
+        got = sorted_rows(res.relations["path"])
+        passes = res.iterations["path"]
+    with Engine("oracle") as o:
+        w = P.tc(o, e)
+        assert got == sorted_rows(w.output) and sizes["path"] == len(got)
+        assert passes < w.iterations["tc"]
+
+
 def test_command_line(tmp_path):
     import json
     import subprocess

@@ -22,6 +22,11 @@ path(x, y) :- edge(x, y).
 path(x, z) :- path(x, y), edge(y, z).
 """
 
+TC_NONLINEAR = """
+path(x, y) :- edge(x, y).
+path(x, z) :- path(x, y), path(y, z).
+"""
+
 SG = """
 sg(x, y) :- edge(p, x), edge(p, y), x != y.
 sg(x, y) :- edge(a, x), sg(a, b), edge(b, y).
@@ -83,6 +88,8 @@ def _cspa():
 CASES = {
     "tc_grid_8": (TC, lambda: {"edge": _u(W.grid_edges(8, 8))}, None),
     "tc_rmat_s7": (TC, lambda: {"edge": _u(W.rmat_edges(7, 300, seed=5))}, None),
+    "tc_nonlinear_rmat_s7": (TC_NONLINEAR, lambda: {"edge": _u(W.rmat_edges(7, 300, seed=5))},
+                             None),
     "sg_rmat_s7": (SG, lambda: {"edge": _u(W.rmat_edges(7, 300, seed=3))}, None),
     "cspa_120": (CSPA, _cspa, None),
     "plen_rmat_s6": (PLEN, lambda: {"edge": _u(W.rmat_edges(6, 150, seed=6))}, {"path": 1}),
