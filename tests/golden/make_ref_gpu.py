@@ -4,7 +4,7 @@ and record its answers as fixtures (tests/golden/ref_gpu.json).
 
 Needs a CUDA device.  Usage, from the repository root:
 
-    python tests/golden/make_ref_gpu.py --out gpurun_out/ref_gpu.json \
+    python tests/golden/make_ref_gpu.py --out tests/golden/ref_gpu.json \
         [--only NAME[,NAME...]] [--timeout SECONDS]
 
 For each workload it writes the TSV inputs the reference drivers read
