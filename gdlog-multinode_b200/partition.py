@@ -390,6 +390,16 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
     def input_rows(pred):
         return np.asarray(inputs[pred], dtype=np.uint64).reshape(-1, prog.arity[pred])
 
+    if 3 in prog.arity.values():
+        # The CUDA engine fixes the field widths of ternary keys at its first
+        # ternary load, from the largest value loaded until then; one row
+        # holding the largest input id, loaded first, makes them the same
+        # on every rank whatever its partition holds.
+        top = max((int(np.asarray(v, dtype=np.uint64).reshape(len(v), -1)[:, :2].max())
+                   for v in inputs.values() if len(v)), default=0)
+        ids = eng.relation("part_ids", index_flag=False)
+        eng.load(ids, np.array([[top, top]], dtype=np.uint64))
+
     parts = {}       # updated (predicate, order) -> _Partition
     static = {}      # (predicate, order) read from outside a component -> engine relation
     host_full = {}   # (predicate, order) -> this rank's FULL rows
