@@ -360,14 +360,17 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
     LIE::fixpoint_loop does (src/lie.cu:62-87):
       * a join is a one-pass LIE of the engine over the local rows of the
         versions it reads (its inner's FULL; its outer's FULL, DELTA or a
-        tmp relation's NEWT); the rows it generates go to the owners of
-        their first column and collect there as the output's NEWT;
-      * a Copy or an ACopy applies its column selection on the host and
-        routes the same way; a Copy from FULL runs once per LIE
+        tmp relation's NEWT); a Copy or an ACopy applies its column
+        selection on the host; a Copy from FULL runs once per LIE
         (src/lie.cu:69-75);
-      * the update step merges each relation's NEWT into its partition on
-        the engine (set difference and flush, src/lie.cu:93-198), DELTA
-        being what was new; the loop ends when no rank found a tuple.
+      * rows generated into a tmp relation go at once to the owners of
+        their first column (a later join of the pass reads them as its
+        outer); rows generated into an updated relation stay on the rank
+        that made them until the update step, which sends each relation's
+        NEWT to the owners of their first column in one exchange and merges
+        it into the partition on the engine (set difference and flush,
+        src/lie.cu:93-198), DELTA being what was new; the loop ends when no
+        rank found a tuple.
     The reference's rules on empty operands decide on global sizes (one
     all_reduce): a join whose outer is empty does nothing, one whose inner
     is empty zeroes its outer's version (src/join.cu:38-45), a Copy or
@@ -477,6 +480,14 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
             newt = {key: [] for key in C.update + C.tmps}
             zero_delta = set()
 
+            def placed(key, rows):
+                # a tmp relation's NEWT is read as a join's outer in this
+                # pass, so it goes to the owners of its join key now; an
+                # updated relation's NEWT is read only by ACopies (which
+                # route what they write) and by the update step, so its rows
+                # stay where they were generated and travel once, there
+                return _route_owned(rows, world, device) if key in C.tmps else rows
+
             def version(key, ver):
                 if ver == DELTA:
                     return none(key) if key in zero_delta else delta[key]
@@ -494,7 +505,7 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                     if _sum_all([len(src)], device)[0] == 0:
                         newt[op.out] = []
                         continue
-                    got = _route_owned(_select(src, op.sel), world, device)
+                    got = placed(op.out, _select(src, op.sel))
                     newt[op.out] = [got] if op.kind == "acopy" else newt[op.out] + [got]
                     continue
                 if op.src_ver != FULL:
@@ -540,11 +551,11 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                     eng.load(outs[a], None)
                     lie.fixpoint()
                     got = outs[a].rows() if outs[a].size() else got
-                newt[op.out].append(_route_owned(got, world, device))
+                newt[op.out].append(placed(op.out, got))
             # the update step (src/lie.cu:93-198)
             new = []
             for key in C.update:
-                rows = _cat(newt[key], arity_of(key))
+                rows = _route_owned(_cat(newt[key], arity_of(key)), world, device)
                 delta[key] = parts[key].merge(rows) if len(rows) else none(key)
                 new.append(len(delta[key]))
             grew = _sum_all(new, device)
