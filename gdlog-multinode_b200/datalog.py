@@ -590,7 +590,11 @@ def main():
         if a.engine == "gpu":
             device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
             torch.cuda.set_device(device)
-        dist.init_process_group("nccl" if device is not None else "gloo")
+        # every pass takes collectives: a rank that failed ends the others'
+        # next one with an error after this long instead of the default
+        from datetime import timedelta
+        dist.init_process_group("nccl" if device is not None else "gloo",
+                                timeout=timedelta(seconds=300))
         try:
             rank = dist.get_rank()
             with Engine(a.engine) as eng:
