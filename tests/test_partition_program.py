@@ -209,3 +209,41 @@ def test_mirror_holds_seeds_and_inputs():
             break
         r |= new
     assert got == sorted(r)
+
+
+def _rank_fails(rank, world, port, out_dir):
+    import time
+    from datetime import timedelta
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=timedelta(seconds=5))
+    t0 = time.time()
+    status = "ok"
+    try:
+        with Engine("oracle") as eng:
+            inputs = {"edge": _u(W.grid_edges(4, 4))}
+            if rank == 1:  # this rank's program names an input nobody passed
+                PT.partitioned_program(eng, TC + "q(x, y) :- missing(x, y).\n", inputs,
+                                       rank, world)
+            else:
+                PT.partitioned_program(eng, TC, inputs, rank, world)
+    except Exception as exc:  # noqa: BLE001 - the failure is the result
+        status = type(exc).__name__
+    with open(os.path.join(out_dir, f"f{rank}.json"), "w") as f:
+        json.dump({"status": status, "seconds": time.time() - t0}, f)
+    try:
+        dist.destroy_process_group()
+    except Exception:  # noqa: BLE001 - the group may already be broken
+        pass
+
+
+def test_a_failed_rank_ends_the_others():
+    """A rank that fails before its first exchange (on the host: a program
+    that names no given input) leaves the other rank's next collective
+    with an error within the process group's timeout, not waiting."""
+    import tempfile
+    d = tempfile.mkdtemp()
+    mp.spawn(_rank_fails, args=(2, free_port(), d), nprocs=2, join=True)
+    f0 = json.load(open(os.path.join(d, "f0.json")))
+    f1 = json.load(open(os.path.join(d, "f1.json")))
+    assert f1["status"] == "ValueError"
+    assert f0["status"] != "ok" and f0["seconds"] < 60
