@@ -236,12 +236,11 @@ def _rank_fails(rank, world, port, out_dir):
         pass
 
 
-def test_a_failed_rank_ends_the_others():
+def test_a_failed_rank_ends_the_others(tmp_path):
     """A rank that fails before its first exchange (on the host: a program
     that names no given input) leaves the other rank's next collective
     with an error within the process group's timeout, not waiting."""
-    import tempfile
-    d = tempfile.mkdtemp()
+    d = str(tmp_path)
     mp.spawn(_rank_fails, args=(2, free_port(), d), nprocs=2, join=True)
     f0 = json.load(open(os.path.join(d, "f0.json")))
     f1 = json.load(open(os.path.join(d, "f1.json")))
