@@ -408,6 +408,7 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
     host_full = {}   # (predicate, order) -> this rank's FULL rows
     zero_full = set()
     full_gen = {}    # updated key -> how many times its FULL changed
+    gfull = {}       # (predicate, order) -> its FULL's size over all ranks
     scratch = {}     # operand slot -> [relation, what it holds]
     outs = {}
     lies = {}
@@ -471,8 +472,15 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
             start(key, _route_owned(base[:, ::-1].copy(), world, device))
         if not C.ops:
             continue
+        # global sizes of the FULLs the component reads, one all_reduce; the
+        # update step's all_reduce keeps them (and DELTA's) current, so
+        # only NEWT sizes need one when an op reads them
+        fresh = [k for k in C.statics if k not in gfull] + list(C.update)
+        for k, n in zip(fresh, _sum_all([len(host_full[k]) for k in fresh], device)):
+            gfull[k] = n
         # LIE start: DELTA := FULL (src/lie.cu:49-59; inputs without repeats)
         delta = {key: host_full[key] for key in C.update}
+        gdelta = {key: gfull[key] for key in C.update}
         copied = set()
         it = 0
         while True:
@@ -488,6 +496,18 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                 # stay where they were generated and travel once, there
                 return _route_owned(rows, world, device) if key in C.tmps else rows
 
+            def global_sizes(*reads):
+                """Sizes over all ranks of (key, version, local rows) reads:
+                FULL and DELTA from the tracked sizes, NEWT by all_reduce."""
+                out = [None if ver == NEWT else
+                       0 if (key in zero_delta if ver == DELTA else key in zero_full) else
+                       (gdelta if ver == DELTA else gfull)[key] for key, ver, _ in reads]
+                ask = [i for i, x in enumerate(out) if x is None]
+                if ask:
+                    for i, n in zip(ask, _sum_all([len(reads[i][2]) for i in ask], device)):
+                        out[i] = n
+                return out
+
             def version(key, ver):
                 if ver == DELTA:
                     return none(key) if key in zero_delta else delta[key]
@@ -501,8 +521,9 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                         continue
                     copied.add(i)
                 if op.kind in ("copy", "acopy"):
-                    src = version(op.src, NEWT if op.kind == "acopy" else op.src_ver)
-                    if _sum_all([len(src)], device)[0] == 0:
+                    ver = NEWT if op.kind == "acopy" else op.src_ver
+                    src = version(op.src, ver)
+                    if global_sizes((op.src, ver, src))[0] == 0:
                         newt[op.out] = []
                         continue
                     got = placed(op.out, _select(src, op.sel))
@@ -512,7 +533,8 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                     raise ValueError("a join's inner is read as FULL")
                 rin = version(op.src, op.src_ver)
                 rout = version(op.outer, op.outer_ver)
-                n_in, n_out = _sum_all([len(rin), len(rout)], device)
+                n_in, n_out = global_sizes((op.src, op.src_ver, rin),
+                                           (op.outer, op.outer_ver, rout))
                 if n_out == 0:
                     continue
                 if n_in == 0:
@@ -563,6 +585,8 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                 if n:  # DELTA is disjoint from FULL: the flushed FULL is their union
                     host_full[key] = np.concatenate([host_full[key], delta[key]])
                     full_gen[key] += 1
+                gfull[key] += n_all
+                gdelta[key] = n_all
                 if n_all:
                     zero_full.discard(key)
             if sum(grew) == 0:
