@@ -371,8 +371,9 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
         it into the partition on the engine (set difference and flush,
         src/lie.cu:93-198), DELTA being what was new; the loop ends when no
         rank found a tuple.
-    The reference's rules on empty operands decide on global sizes (one
-    all_reduce): a join whose outer is empty does nothing, one whose inner
+    The reference's rules on empty operands decide on global sizes (those
+    of FULL and DELTA tracked from the update step's all_reduce, a NEWT's
+    reduced when an op reads it): a join whose outer is empty does nothing, one whose inner
     is empty zeroes its outer's version (src/join.cu:38-45), a Copy or
     ACopy from an empty source clears its destination's NEWT
     (src/copy.cu:24-27, src/acopy.cu:14-18).  A FULL zeroed that way stays
