@@ -521,14 +521,18 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                     if i in copied:
                         continue
                     copied.add(i)
-                if op.kind in ("copy", "acopy"):
-                    ver = NEWT if op.kind == "acopy" else op.src_ver
-                    src = version(op.src, ver)
-                    if global_sizes((op.src, ver, src))[0] == 0:
+                if op.kind == "acopy":
+                    # NEWT replaced by the selection of the source's NEWT
+                    # (cleared when that is empty everywhere, which is the
+                    # same): no size to agree on
+                    newt[op.out] = [placed(op.out, _select(version(op.src, NEWT), op.sel))]
+                    continue
+                if op.kind == "copy":
+                    src = version(op.src, op.src_ver)
+                    if global_sizes((op.src, op.src_ver, src))[0] == 0:
                         newt[op.out] = []
                         continue
-                    got = placed(op.out, _select(src, op.sel))
-                    newt[op.out] = [got] if op.kind == "acopy" else newt[op.out] + [got]
+                    newt[op.out].append(placed(op.out, _select(src, op.sel)))
                     continue
                 if op.src_ver != FULL:
                     raise ValueError("a join's inner is read as FULL")

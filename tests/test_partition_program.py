@@ -246,3 +246,39 @@ def test_a_failed_rank_ends_the_others(tmp_path):
     f1 = json.load(open(os.path.join(d, "f1.json")))
     assert f1["status"] == "ValueError"
     assert f0["status"] != "ok" and f0["seconds"] < 60
+
+
+def _rank_count(rank, world, port, out_dir):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    calls = {"all_reduce": 0, "all_to_all_single": 0}
+    for name in calls:
+        real = getattr(dist, name)
+
+        def counted(*a, _real=real, _name=name, **k):
+            calls[_name] += 1
+            return _real(*a, **k)
+        setattr(dist, name, counted)
+    try:
+        with Engine("oracle") as eng:
+            res = PT.partitioned_program(eng, TC, {"edge": _u(W.grid_edges(6, 6))}, rank, world)
+        with open(os.path.join(out_dir, f"c{rank}.json"), "w") as f:
+            json.dump({"passes": res.iterations["path"], **calls}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_collectives_per_pass(tmp_path):
+    """Transitive closure partitioned (path joined on its second column, so
+    a swapped mirror of path is kept too): one exchange of the mirror's
+    first rows and one all_reduce of sizes when the component starts, then
+    per pass one exchange of new rows for each of path and its mirror (an
+    all_to_all of counts and one of keys each) and one all_reduce of the
+    new-tuple counts.  The Copy and the join read FULL and DELTA, whose
+    global sizes are tracked, and the ACopy needs none, so they reduce
+    nothing."""
+    mp.spawn(_rank_count, args=(2, free_port(), str(tmp_path)), nprocs=2, join=True)
+    for r in range(2):
+        c = json.load(open(tmp_path / f"c{r}.json"))
+        assert c["all_reduce"] == 1 + c["passes"]
+        assert c["all_to_all_single"] == 2 + 4 * c["passes"]
