@@ -293,6 +293,59 @@ def _route_owned(rows: np.ndarray, world: int, device) -> np.ndarray:
     return np.concatenate([a, b[:, 1:]], axis=1)
 
 
+def _keys_of(rows: np.ndarray) -> np.ndarray:
+    """Packed keys of rows of two columns (one a row: c0 << 32 | c1) or
+    three (two a row: (c0, c1) then (c0, c2))."""
+    r = np.asarray(rows, dtype=np.uint64)
+    k = (r[:, 0] << np.uint64(32)) | r[:, 1]
+    if r.shape[1] == 2:
+        return k
+    return np.stack([k, (r[:, 0] << np.uint64(32)) | r[:, 2]], axis=1).reshape(-1)
+
+
+def _rows_of(keys: np.ndarray, arity: int) -> np.ndarray:
+    hi, lo = keys >> np.uint64(32), keys & np.uint64(0xFFFFFFFF)
+    if arity == 2:
+        return np.stack([hi, lo], axis=1)
+    return np.stack([hi[0::2], lo[0::2], lo[1::2]], axis=1)
+
+
+def _route_all(parts: list, world: int, device) -> list:
+    """Rows of several relations (each of two or three columns) to the
+    owners of their first column in one exchange: an all_to_all of a count
+    for every (destination, relation) pair, then one of all the keys."""
+    R = len(parts)
+    counts = np.zeros((world, R), np.int64)   # keys for (destination, relation)
+    chunks = [[None] * R for _ in range(world)]
+    for j, rows in enumerate(parts):
+        per = 1 if rows.shape[1] == 2 else 2
+        dest = owner(rows[:, 0], world) if len(rows) else np.zeros(0, np.int64)
+        order = np.argsort(dest, kind="stable")
+        keys = _keys_of(rows[order]) if len(rows) else np.zeros(0, np.uint64)
+        bounds = np.searchsorted(dest[order], np.arange(world + 1))
+        for d in range(world):
+            chunks[d][j] = keys[bounds[d] * per:bounds[d + 1] * per]
+            counts[d, j] = len(chunks[d][j])
+    send = np.concatenate([c for row in chunks for c in row]) if R else np.zeros(0, np.uint64)
+    dev = device if device is not None else "cpu"
+    sc = torch.from_numpy(counts.reshape(-1)).to(dev)
+    rc = torch.empty_like(sc)
+    dist.all_to_all_single(rc, sc)
+    recv_counts = rc.cpu().numpy().reshape(world, R)
+    out = torch.empty(int(recv_counts.sum()), dtype=torch.int64, device=dev)
+    dist.all_to_all_single(out, torch.from_numpy(send.view(np.int64)).to(dev),
+                           recv_counts.sum(axis=1).tolist(), counts.sum(axis=1).tolist())
+    got = out.cpu().numpy().view(np.uint64)
+    # laid out by source rank, then by relation within each source
+    ends = np.cumsum(recv_counts.reshape(-1))
+    starts = ends - recv_counts.reshape(-1)
+    res = []
+    for j, rows in enumerate(parts):
+        keys = np.concatenate([got[starts[s * R + j]:ends[s * R + j]] for s in range(world)])
+        res.append(_rows_of(keys, rows.shape[1]))
+    return res
+
+
 def _sum_all(counts: list, device) -> list:
     """Element-wise sum of a count vector over the ranks (one all_reduce)."""
     t = torch.tensor(counts, dtype=torch.int64, device=device if device is not None else "cpu")
@@ -581,8 +634,9 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
                 newt[op.out].append(placed(op.out, got))
             # the update step (src/lie.cu:93-198)
             new = []
-            for key in C.update:
-                rows = _route_owned(_cat(newt[key], arity_of(key)), world, device)
+            sent = _route_all([_cat(newt[key], arity_of(key)) for key in C.update], world,
+                              device)
+            for key, rows in zip(C.update, sent):
                 delta[key] = parts[key].merge(rows) if len(rows) else none(key)
                 new.append(len(delta[key]))
             grew = _sum_all(new, device)

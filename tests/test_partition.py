@@ -105,6 +105,9 @@ def test_owner_and_route_shapes():
                     dtype=np.uint64)
     assert (PT._unpack(PT._pack(rows)) == rows).all()
     assert PT._unpack(PT._pack(np.zeros((0, 2), np.uint64))).shape == (0, 2)
+    tri = np.array([[7, (1 << 32) - 1, 3], [0, 1, 2]], dtype=np.uint64)
+    assert (PT._rows_of(PT._keys_of(tri), 3) == tri).all()
+    assert (PT._rows_of(PT._keys_of(rows), 2) == rows).all()
 
 
 @pytest.mark.gpu

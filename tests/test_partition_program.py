@@ -272,8 +272,8 @@ def test_collectives_per_pass(tmp_path):
     """Transitive closure partitioned (path joined on its second column, so
     a swapped mirror of path is kept too): one exchange of the mirror's
     first rows and one all_reduce of sizes when the component starts, then
-    per pass one exchange of new rows for each of path and its mirror (an
-    all_to_all of counts and one of keys each) and one all_reduce of the
+    per pass one exchange of the new rows of path and its mirror together
+    (an all_to_all of counts and one of keys) and one all_reduce of the
     new-tuple counts.  The Copy and the join read FULL and DELTA, whose
     global sizes are tracked, and the ACopy needs none, so they reduce
     nothing."""
@@ -281,4 +281,4 @@ def test_collectives_per_pass(tmp_path):
     for r in range(2):
         c = json.load(open(tmp_path / f"c{r}.json"))
         assert c["all_reduce"] == 1 + c["passes"]
-        assert c["all_to_all_single"] == 2 + 4 * c["passes"]
+        assert c["all_to_all_single"] == 2 + 2 * c["passes"]
