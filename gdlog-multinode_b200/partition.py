@@ -419,9 +419,9 @@ def partitioned_program(eng: Engine, text: str, inputs: dict, rank: int, world: 
       * rows generated into a tmp relation go at once to the owners of
         their first column (a later join of the pass reads them as its
         outer); rows generated into an updated relation stay on the rank
-        that made them until the update step, which sends each relation's
-        NEWT to the owners of their first column in one exchange and merges
-        it into the partition on the engine (set difference and flush,
+        that made them until the update step, which sends every updated
+        relation's NEWT to the owners of their first column in one exchange
+        (_route_all) and merges each into its partition on the engine (set difference and flush,
         src/lie.cu:93-198), DELTA being what was new; the loop ends when no
         rank found a tuple.
     The reference's rules on empty operands decide on global sizes (those
