@@ -2855,11 +2855,19 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
   if (dev < 0 || dev >= 64) return noalloc_fail(GDL_E_UNSUPPORTED, "device ordinal above 63");
   unsigned char *base = nullptr;
   {
-    // Set-up, once per device, with that device current.
+    // Set-up, once per device, with that device current: the scratch
+    // array's device address and the kernels' shared-memory attributes,
+    // both under the lock so that two threads' first calls do not race.
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_addr[dev]) {
       void *p = nullptr;
       NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      NA_CK(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSortSmemBytes));
+      NA_CK(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSortSmemBytes));
+      NA_CK(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kMergeSmemBytes));
       g_noalloc_addr[dev] = p;
     }
     base = static_cast<unsigned char *>(g_noalloc_addr[dev]);
@@ -2867,16 +2875,6 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int sms = 148;
   NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  static bool smem_set[64] = {false};
-  if (!smem_set[dev]) {
-    NA_CK(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSortSmemBytes));
-    NA_CK(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSortSmemBytes));
-    NA_CK(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kMergeSmemBytes));
-    smem_set[dev] = true;
-  }
   // The array keeps the previous call's contents: zero the control state.
   NA_CK(cudaMemsetAsync(base + kNaCtrl, 0, kNaBytes - kNaCtrl, s));
   k_noalloc_init<<<1, 32, 0, s>>>(base, rows);

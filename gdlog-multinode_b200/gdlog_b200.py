@@ -13,8 +13,10 @@ test/cspa.cu):
                  gen=(INNER(1), OUTER(1)))
     iterations = lie.fixpoint()                   # LIE::fixpoint_loop
 
-The same class drives the CPU oracle (``Engine("oracle")``, test
-infrastructure) through its mirror C-ABI, so tests run one program on both.
+The same class drives the CPU oracles (``Engine("oracle")`` over sorted
+tuple lists and ``Engine("oracle_bitset")`` over bit matrices, both test
+infrastructure) through their mirror C-ABIs, so tests run one program on
+all of them.
 The GPU backend fails loudly when its shared library is missing: there is
 no CPU fallback.
 """
@@ -99,15 +101,19 @@ _SIGS = {
 _libs: dict = {}
 
 
+_PREFIX = {"gpu": "gdl_", "oracle": "orc_", "oracle_bitset": "orb_"}
+
+
 def load_library(kind: str) -> C.CDLL:
-    """Open the GPU engine ("gpu") or the CPU oracle ("oracle") library."""
+    """Open the GPU engine ("gpu") or a CPU oracle ("oracle",
+    "oracle_bitset") library."""
     if kind in _libs:
         return _libs[kind]
     path = GPU_LIB if kind == "gpu" else ORACLE_LIB
     if not os.path.exists(path):
         raise GdlError(4, f"{kind} library not built: {path} (run __graft_entry__.build())")
     lib = C.CDLL(path)
-    pre = "gdl_" if kind == "gpu" else "orc_"
+    pre = _PREFIX[kind]
     for name, args in _SIGS.items():
         f = getattr(lib, pre + name)
         f.argtypes = args
@@ -161,18 +167,19 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_relation_dump_tsv.argtypes = [_P, _I, _I, C.c_char_p, _PU64]
         lib.gdl_relation_dump_tsv.restype = _I
     else:
-        lib.orc_engine_create.argtypes = [_I, _I, C.POINTER(_P)]
-        lib.orc_engine_create.restype = _I
-        lib.orc_engine_destroy.argtypes = [_P]
-        lib.orc_engine_destroy.restype = _I
-        lib.orc_last_error.argtypes = [_P]
-        lib.orc_last_error.restype = C.c_char_p
-        lib.orc_engine_clear.argtypes = [_P]
-        lib.orc_engine_clear.restype = _I
-        lib.orc_threads.argtypes = [_P]
-        lib.orc_threads.restype = _I
-        lib.orc_lie_seconds.argtypes = [_P, _I, C.POINTER(C.c_double)]
-        lib.orc_lie_seconds.restype = _I
+        f = lambda n: getattr(lib, pre + n)  # noqa: E731
+        f("engine_create").argtypes = [_I, _I, C.POINTER(_P)]
+        f("engine_create").restype = _I
+        f("engine_destroy").argtypes = [_P]
+        f("engine_destroy").restype = _I
+        f("last_error").argtypes = [_P]
+        f("last_error").restype = C.c_char_p
+        f("engine_clear").argtypes = [_P]
+        f("engine_clear").restype = _I
+        f("threads").argtypes = [_P]
+        f("threads").restype = _I
+        f("lie_seconds").argtypes = [_P, _I, C.POINTER(C.c_double)]
+        f("lie_seconds").restype = _I
     _libs[kind] = lib
     return lib
 
@@ -334,7 +341,8 @@ class Lie:
     def stats(self) -> dict:
         if self.eng.kind != "gpu":
             s = C.c_double(0)
-            self.eng._check(self.eng.lib.orc_lie_seconds(self.eng.h, self.id, C.byref(s)))
+            self.eng._check(getattr(self.eng.lib, self.eng.pre + "lie_seconds")(
+                self.eng.h, self.id, C.byref(s)))
             return {"ms": s.value * 1e3}
         out = (C.c_double * 8)()
         self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 8))
@@ -350,20 +358,20 @@ class Engine:
 
     def __init__(self, kind: str = "gpu", device: int = 0, threads: int = 0,
                  max_arity: int = 2, stream: int | None = None, dedup: str | None = None):
-        if kind not in ("gpu", "oracle"):
+        if kind not in _PREFIX:
             raise ValueError(kind)
         self.kind = kind
         self.lib = load_library(kind)
-        self.pre = "gdl_" if kind == "gpu" else "orc_"
+        self.pre = _PREFIX[kind]
         h = _P()
         if kind == "gpu":
             code = self.lib.gdl_engine_create(device, stream, C.byref(h))
             if code:
                 raise GdlError(code, "gdl_engine_create failed (no CUDA device?)")
         else:
-            code = self.lib.orc_engine_create(max_arity, threads, C.byref(h))
+            code = getattr(self.lib, self.pre + "engine_create")(max_arity, threads, C.byref(h))
             if code:
-                raise GdlError(code, "orc_engine_create failed")
+                raise GdlError(code, f"{self.pre}engine_create failed")
         self.h = h
         self.relations: list[Relation] = []
         if kind == "gpu" and dedup is not None:
@@ -399,7 +407,7 @@ class Engine:
 
     @property
     def threads(self) -> int:
-        return int(self.lib.orc_threads(self.h)) if self.kind == "oracle" else 0
+        return 0 if self.kind == "gpu" else int(getattr(self.lib, self.pre + "threads")(self.h))
 
     def last_error(self) -> str:
         msg = getattr(self.lib, self.pre + "last_error")(self.h)
@@ -515,7 +523,7 @@ class Engine:
         if self.kind == "gpu":
             self._check(self.lib.gdl_engine_clear(self.h))
         else:
-            self._check(self.lib.orc_engine_clear(self.h))
+            self._check(getattr(self.lib, self.pre + "engine_clear")(self.h))
         self.relations = []
 
     def load_device(self, rel: Relation, ptr: int, n_rows: int) -> None:

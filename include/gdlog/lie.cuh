@@ -55,6 +55,7 @@ struct LIE {
     iteration_counter = it;
     for (auto *v : {&update_relations, &static_relations, &tmp_relations})
       for (Relation *r : *v) r->refresh();
+    if (!getenv("GDLOG_QUIET")) print_log(e, lie);
     if (profile) {
       double p[3 * 8] = {0};
       check(gdl_engine_profile(e, p, 3 * 8), "gdl_engine_profile");
@@ -73,6 +74,36 @@ struct LIE {
   }
 
  private:
+  // The per-iteration lines the reference prints inside its loop
+  // (src/lie.cu:114-121, 193-200), written once the device loop is done;
+  // GDLOG_QUIET=1 leaves them out.
+  void print_log(gdl_engine *e, int32_t lie) {
+    using namespace gdlog_compat;
+    uint64_t n = 0;
+    check(gdl_lie_trace(e, lie, nullptr, 0, &n), "gdl_lie_trace");
+    std::vector<uint64_t> rec(5 * n);
+    check(gdl_lie_trace(e, lie, rec.data(), n, &n), "gdl_lie_trace");
+    auto name = [&](uint64_t id) -> const char * {
+      for (Relation *r : update_relations)
+        if ((uint64_t)r->id == id) return r->name.c_str();
+      return "?";
+    };
+    for (uint64_t i = 0; i < n; i++) {
+      const uint64_t *x = &rec[5 * i];
+      if (x[2] == UINT64_MAX)
+        printf("iteration %llu relation %s no new tuple added\n", (unsigned long long)x[0],
+               name(x[1]));
+      else
+        printf("iteration %llu relation %s finish dedup new tuples : %llu delta tuple size: %llu "
+               "full counts %llu\n",
+               (unsigned long long)x[0], name(x[1]), (unsigned long long)x[2],
+               (unsigned long long)x[3], (unsigned long long)x[4]);
+      if (i + 1 == n || rec[5 * (i + 1)] != x[0])
+        printf("Iteration %llu finish populating\n", (unsigned long long)x[0]);
+    }
+    fflush(stdout);
+  }
+
   static void add_op(gdl_engine *e, int32_t lie, RelationalJoin &j) {
     using namespace gdlog_compat;
     int32_t gen[3];

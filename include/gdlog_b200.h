@@ -338,8 +338,10 @@ gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *siz
  *
  * Scratch is one fixed array of about 4.3 MB inside the library, present on
  * every GPU that loads the library until the process exits.  The first call
- * on a device looks up that array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls on a device
+ * on a device looks up that array's device address (cudaGetSymbolAddress).
+ * Every call waits for its stream and copies results to host memory, so it
+ * must not be called while its stream (or the legacy stream) is being
+ * captured into a CUDA graph.  All calls on a device
  * share the array: calls that can overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller.  On failure,
  * gdl_last_error(NULL) holds the message. */

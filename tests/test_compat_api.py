@@ -31,7 +31,9 @@ def test_headers_compile_standalone(tmp_path):
         assert r.returncode == 0, r.stderr[-2000:]
 
 
-REF_TEST = "/root/reference/test"
+from conftest import DROPIN, REF_ROOT
+
+REF_TEST = os.path.join(REF_ROOT, "test")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_TEST), reason="reference sources not present")
@@ -95,3 +97,99 @@ def test_compat_path_length_matches_oracle(tmp_path):
         want = (ro.relations["path"].size(), hex(ro.relations["path"].digest()),
                 ro.iterations["plen"])
     assert (got["sizes"]["path"], got["digests"]["path"], got["iterations"]["plen"]) == want
+
+
+# -- the reference's own drivers, unchanged, running on the GPU -------------
+
+def run_dropin(driver, *args, timeout=600):
+    exe = os.path.join(DROPIN, "bin", driver)
+    if not os.path.exists(exe):
+        pytest.skip("reference drivers not built (make -C oracle dropin REF=<reference root>)")
+    r = subprocess.run([exe, *args], capture_output=True, text=True, timeout=timeout)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    return r.stdout
+
+
+def last_lie_passes(out: str) -> int:
+    """Loop passes of the last LIE from the per-iteration log lines
+    ("Iteration i finish populating", src/lie.cu:199-200)."""
+    its = [int(ln.split()[1]) for ln in out.splitlines()
+           if ln.startswith("Iteration ") and ln.endswith("finish populating")]
+    last0 = max(i for i, v in enumerate(its) if v == 0)
+    return max(its[last0:]) + 1
+
+
+def count_after(out: str, label: str) -> int:
+    line = [ln for ln in out.splitlines() if ln.startswith(label)][-1]
+    return int(line[len(label):].split()[0])
+
+
+# Same generation on the reference's data files gives the sizes and loop
+# passes the reference publishes (README.md:101-103, test/cuDF/sg.json);
+# the closure gives what the bit-matrix oracle gives on the same file.
+DROPIN_CASES = [
+    ("sg", "data_21693.txt", "sg counts ", 23519, 58),
+    ("sg", "data_7035.txt", "sg counts ", 285431, 56),
+    ("sg", "data_5.txt", "sg counts ", 4, 3),
+    ("tc", "data_7035.txt", "Path counts ", None, None),
+    ("tc", "data_21693.txt", "Path counts ", None, None),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("driver,data,label,size,passes", DROPIN_CASES)
+def test_reference_drivers_run_on_reference_data(driver, data, label, size, passes):
+    """test/tc.cu and test/sg.cu, compiled unchanged against the drop-in
+    headers (oracle/Makefile `dropin`), run on the B200 on the reference's
+    own data files."""
+    import programs as P
+    from gdlog_b200 import Engine, read_tsv
+    path = os.path.join(DROPIN, "data", data)
+    out = run_dropin(driver, path)
+    got = (count_after(out, label), last_lie_passes(out))
+    if size is None:
+        with Engine("oracle_bitset") as o:
+            r = getattr(P, driver)(o, read_tsv(path))
+            size, passes = r.output.size(), list(r.iterations.values())[-1]
+    assert got == (size, passes)
+
+
+@pytest.mark.gpu
+def test_reference_cspa_driver_runs(tmp_path):
+    """test/cspa.cu, unchanged, on a facts directory (assign.facts,
+    dereference.facts): its relations' sizes as the oracle has them."""
+    import programs as P
+    from gdlog_b200 import Engine
+    assign, deref = W.cspa_facts(300, 600, 225, seed=3)
+    W.write_tsv(str(tmp_path / "assign.facts"), assign)
+    W.write_tsv(str(tmp_path / "dereference.facts"), deref)
+    out = run_dropin("cspa", str(tmp_path))
+    with Engine("oracle_bitset") as o:
+        r = P.cspa(o, assign, deref)
+        want = {k: v.size() for k, v in r.relations.items()}
+    full = {}
+    for ln in out.splitlines():
+        if ln.startswith("iteration ") and " full counts " in ln:
+            name = ln.split()[3]
+            full[name] = int(ln.rsplit(" ", 1)[1])
+    assert full["value_flow_2__1_2"] == want["value_flow"]
+    assert full["memory_alias_2__1_2"] == want["memory_alias"]
+    assert full["value_alias_2__1_2"] == want["value_alias"]
+    assert last_lie_passes(out) == r.iterations["analysis"]
+
+
+@pytest.mark.gpu
+def test_reference_path_length_driver_runs():
+    """test/path_length.cu, unchanged (arity 3, a dependent column and a
+    hook that adds 1): its closure size as the oracle has it."""
+    import programs as P
+    from gdlog_b200 import Engine, read_tsv
+    path = os.path.join(DROPIN, "data", "data_7035.txt")
+    out = run_dropin("path_length", path)
+    with Engine("oracle", max_arity=3) as o:
+        r = P.path_length(o, read_tsv(path))
+        want = r.output.size()
+    full = [int(ln.rsplit(" ", 1)[1]) for ln in out.splitlines()
+            if ln.startswith("iteration ") and " full counts " in ln]
+    assert full[-1] == want
+    assert last_lie_passes(out) == r.iterations["plen"]

@@ -10,6 +10,7 @@ import pytest
 import datalog as D
 import programs as P
 import workloads as W
+from conftest import REF_ROOT
 from gdlog_b200 import Engine
 
 TC = """
@@ -111,7 +112,7 @@ def test_rules_on_the_gpu_engine():
     assert tc_got == tc_want
 
 
-REF_SOUFFLE = os.path.join("/root/reference", "test", "souffle")
+REF_SOUFFLE = os.path.join(REF_ROOT, "test", "souffle")
 
 
 def write_facts(path, rows):

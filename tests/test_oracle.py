@@ -22,7 +22,9 @@ from gdlog_b200 import DELTA, FULL, INNER, NEWT, OUTER, PRED_NE, SRC, Engine, di
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "golden.json")))
-REF_DATA = "/root/reference/data"
+from conftest import REF_ROOT
+
+REF_DATA = os.path.join(REF_ROOT, "data")
 
 SMALL = [k for k, v in GOLDEN["workloads"].items() if v["oracle_seconds"] < 2.0]
 

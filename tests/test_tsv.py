@@ -12,7 +12,9 @@ import programs as P
 import workloads as W
 from gdlog_b200 import Engine, GdlError, read_tsv, write_tsv
 
-REF_DATA = "/root/reference/data"
+from conftest import REF_ROOT
+
+REF_DATA = os.path.join(REF_ROOT, "data")
 
 
 def reference_rules(text: str, arity: int):

@@ -6,7 +6,8 @@ HBM to a fixed pool up front): they pass their own input and output
 buffers, and all scratch comes from one fixed array inside the library.
 Here its output is checked, on two calls in a row (the scratch array keeps
 the previous call's contents), against the allocating entry points
-gdl_relation_load_device + gdl_relation_export on the same input, and a
+gdl_relation_load_device + gdl_relation_export on the same input and
+against numpy's sorted unique rows (which share no kernel with it), and a
 call above the fixed row limit must be refused with a clear error.
 Integer output, so the comparison is exact.
 
@@ -67,6 +68,10 @@ def test_noalloc_matches_load_and_export():
         want = reference_rows(torch, d_in, n)
         assert got_n.value == len(want)
         assert np.array_equal(got, want)
+        # and independently of the engine's kernels: numpy's lexicographic
+        # sorted unique rows
+        exact = np.unique(rows.astype(np.uint64), axis=0)
+        assert np.array_equal(got, exact)
 
 
 def test_noalloc_rejects_rows_above_limit():
