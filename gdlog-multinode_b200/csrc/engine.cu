@@ -87,6 +87,9 @@ struct OpHost {
   Pred pred{0, 0, 0};
   bool generic = false;  // arity 3 or a computed column: tuples from gen
   GenSpec gen{};
+  // The caller's kernel does the per-tuple work (gdl_lie_add_*_hooked).
+  gdl_hook_launch hook = nullptr;
+  void *hook_ctx = nullptr;
 };
 
 struct LieHost {
@@ -813,6 +816,31 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
 // One iteration.  in_graph: the body of the graph's while-node, which the
 // host opens with a k_begin before each launch and whose k_commit opens
 // the next iteration; otherwise the iteration opens itself.
+static_assert(sizeof(DArr) == sizeof(gdl_dev_rows), "gdl_dev_rows mirrors DArr");
+static_assert(sizeof(JoinRec) == sizeof(gdl_hook_state), "gdl_hook_state mirrors JoinRec");
+static_assert(offsetof(JoinRec, written) == offsetof(gdl_hook_state, written), "JoinRec layout");
+static_assert(offsetof(JoinRec, skip) == offsetof(gdl_hook_state, skip), "JoinRec layout");
+
+// What a hooked operator's kernel reads: device addresses that stay valid
+// for the launch being enqueued (the descriptors, not the arrays, whose
+// pointers change when the loop swaps versions).
+gdl_hook_work hook_work(gdl_engine *e, const OpHost &op, JoinRec *rec, const DArr *rows,
+                        DArr *out) {
+  gdl_hook_work w;
+  memset(&w, 0, sizeof w);
+  w.kind = op.kind;
+  w.in_arity = e->rels[op.inner].arity;
+  w.outer_arity = op.kind == 0 ? e->rels[op.outer].arity : 0;
+  w.out_arity = e->rels[op.out].arity;
+  w.k2 = e->k2;
+  w.sms = e->sms;
+  w.state = reinterpret_cast<gdl_hook_state *>(rec);
+  w.rows = reinterpret_cast<const gdl_dev_rows *>(rows);
+  w.out = reinterpret_cast<gdl_dev_rows *>(out);
+  w.error = &e->d_ctl->oob;
+  return w;
+}
+
 void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, bool in_graph) {
   cudaStream_t s = e->s;
   RelDev *R = e->d_rels;
@@ -887,6 +915,26 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       a.row_or = dense && e->row_or_joins && op.inner_ver != GDL_DELTA &&
                  e->h[op.inner].dense && e->h[op.inner].bmF && op.pred.kind == 0 &&
                  (op.sel.s0 == 2 || op.sel.s0 == 3) && op.sel.s1 == 1;
+      if (op.hook) {
+        // The count pass enumerates the candidates; the caller's kernel runs
+        // the hooks over them and appends what it keeps.
+        a.generic = 0;
+        a.pred = Pred{0, 0, 0};
+        const u64 ocap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap,
+                                   oh.full_next.cap, oh.newt.cap});
+        PLAUNCH(kc, kPJoinCount,
+                k_join_count<<<grid_for(e, ocap, kJoinTile, e->count_ctas_per_sm), kJoinBlock,
+                               0, s>>>(a));
+        PLAUNCH(kc, kPControl, k_hook_join_begin<<<1, 32, 0, s>>>(a));
+        gdl_hook_work w = hook_work(e, op, L.d_joinrec + oi, a.inner, &R[op.out].newt);
+        w.rec_offset = reinterpret_cast<const uint64_t *>(e->crow_off);
+        w.rec_start = e->crow_start;
+        w.rec_key = reinterpret_cast<const uint64_t *>(e->crow_key);
+        op.hook(op.hook_ctx, &w, (void *)s);
+        kc->add(kPJoinMat);
+        PLAUNCH(kc, kPControl, k_hook_join_end<<<1, 32, 0, s>>>(a));
+        continue;
+      }
       if (plan.pull[oi]) {
         const u32 *OT = oh.bmDT;
         const u64 side = 1ull << (L.dk - kPullMinBits);
@@ -971,6 +1019,15 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       c.dest_rel = op.out;
       c.replace = op.kind == 2;
       u64 cap = std::max({sh.full.cap, sh.delta.cap, sh.newt.cap, sh.delta_next.cap});
+      if (op.hook) {
+        JoinRec *rec = L.d_joinrec + oi;
+        PLAUNCH(kc, kPControl, k_hook_copy_begin<<<1, 32, 0, s>>>(c, rec));
+        gdl_hook_work w = hook_work(e, op, rec, c.src, &R[op.out].newt);
+        op.hook(op.hook_ctx, &w, (void *)s);
+        kc->add(kPCopy);
+        PLAUNCH(kc, kPControl, k_hook_copy_end<<<1, 32, 0, s>>>(c, rec));
+        continue;
+      }
       if (dense && op.kind == 2) {
         // RelationalACopy: dest NEWT := sel(src NEWT), bitmap to bitmap.
         const u64 tiles = words / kBmTileWords;
@@ -1631,8 +1688,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (c.oob & 32768u) {
       e->broken = true;
       return fail(e, GDL_E_UNSUPPORTED,
-                  "iteration %llu generated a value too large for its column (arity-3 keys "
-                  "hold column 1 below 2^%d and column 2 below 2^%d)",
+                  "iteration %llu generated a value too large for its column (arity-2 columns "
+                  "hold values below 2^32; arity-3 keys hold column 1 below 2^%d and column 2 "
+                  "below 2^%d)",
                   (unsigned long long)c.iteration, 32 - e->k2, e->k2);
     }
     if (c.timeout || c.oob) {
@@ -2488,6 +2546,69 @@ gdl_status gdl_lie_add_acopy(gdl_engine *e, int32_t lie, int32_t src, int32_t de
   e->lies[lie].ops.push_back(op);
   e->lies[lie].graph_dirty = true;
   return GDL_OK;
+}
+
+static gdl_status add_hooked(gdl_engine *e, int32_t lie, OpHost op, gdl_hook_launch launch,
+                             void *ctx) {
+  if (!launch) return fail(e, GDL_E_INVALID, "null hook launcher");
+  if ((int)e->lies[lie].ops.size() >= kMaxOps) return fail(e, GDL_E_UNSUPPORTED, "too many ops");
+  // Tuples come from the caller's kernel: the LIE runs on sorted lists.
+  op.generic = true;
+  op.gen.out_arity = e->rels[op.out].arity;
+  op.gen.in_arity = e->rels[op.inner].arity;
+  op.gen.outer_arity = op.kind == 0 ? e->rels[op.outer].arity : 0;
+  op.hook = launch;
+  op.hook_ctx = ctx;
+  e->lies[lie].ops.push_back(op);
+  e->lies[lie].graph_dirty = true;
+  return GDL_OK;
+}
+
+gdl_status gdl_lie_add_join_hooked(gdl_engine *e, int32_t lie, int32_t inner, int32_t inner_ver,
+                                   int32_t outer, int32_t outer_ver, int32_t output,
+                                   gdl_hook_launch launch, void *ctx) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, inner);
+  CHECK_REL(e, outer);
+  CHECK_REL(e, output);
+  if (inner_ver < 0 || inner_ver > 2 || outer_ver < 0 || outer_ver > 2)
+    return fail(e, GDL_E_INVALID, "bad version");
+  OpHost op;
+  op.kind = 0;
+  op.inner = inner;
+  op.inner_ver = inner_ver;
+  op.outer = outer;
+  op.outer_ver = outer_ver;
+  op.out = output;
+  return add_hooked(e, lie, op, launch, ctx);
+}
+
+gdl_status gdl_lie_add_copy_hooked(gdl_engine *e, int32_t lie, int32_t src, int32_t src_ver,
+                                   int32_t dest, gdl_hook_launch launch, void *ctx) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, src);
+  CHECK_REL(e, dest);
+  if (src_ver != GDL_DELTA && src_ver != GDL_FULL)
+    return fail(e, GDL_E_INVALID, "copy source must be DELTA or FULL");
+  OpHost op;
+  op.kind = 1;
+  op.inner = src;
+  op.inner_ver = src_ver;
+  op.out = dest;
+  return add_hooked(e, lie, op, launch, ctx);
+}
+
+gdl_status gdl_lie_add_acopy_hooked(gdl_engine *e, int32_t lie, int32_t src, int32_t dest,
+                                    gdl_hook_launch launch, void *ctx) {
+  CHECK_LIE(e, lie);
+  CHECK_REL(e, src);
+  CHECK_REL(e, dest);
+  OpHost op;
+  op.kind = 2;
+  op.inner = src;
+  op.inner_ver = GDL_NEWT;
+  op.out = dest;
+  return add_hooked(e, lie, op, launch, ctx);
 }
 
 gdl_status gdl_lie_set_max_iteration(gdl_engine *e, int32_t lie, int64_t m) {

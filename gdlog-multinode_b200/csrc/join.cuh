@@ -39,6 +39,8 @@ struct JoinRec {
   u64 nc;        // compacted records
   u64 base;      // append position in NEWT
   u64 overflow;  // the output does not fit NEWT (raised by the next kernel)
+  u64 written;   // hooked ops: rows the caller's kernel appended
+  u64 skip;      // hooked ops: nothing to do this iteration
 };
 
 struct JoinArgs {
@@ -437,6 +439,87 @@ __global__ void __launch_bounds__(kMatBlock) k_copy(CopyArgs c) {
     if (c.once_pending) *c.once_pending = 1;
     prof_add(c.ctl, kPCopy, 16 * n);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Operators whose per-tuple work is the caller's kernel (gdl_lie_add_*_hooked,
+// the reference's device-function-pointer hooks, src/relation.cu:290-403).
+// The engine brackets that kernel: the begin kernel decides whether the
+// operator runs this iteration and where its rows go, the end kernel
+// publishes NEWT's count.  JoinRec doubles as the caller-visible
+// gdl_hook_state.
+// ---------------------------------------------------------------------------
+
+// Join: after k_join_count (which applied src/join.cu:38-45 and checked NEWT
+// capacity for every candidate).
+__global__ void k_hook_join_begin(JoinArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  JoinRec *r = a.op;
+  r->written = 0;
+  r->skip = 1;
+  if (ctl_stop(a.ctl)) return;
+  if (r->overflow) {
+    atomicExch(&a.ctl->overflow, 1u);
+    return;
+  }
+  if (r->total == 0) return;
+  r->base = a.out_newt->n;
+  r->skip = 0;
+}
+
+// Appends are rounded up to an even count as everywhere else: an odd tail
+// repeats the last row the operator wrote (the update step deduplicates).
+__device__ __forceinline__ void hook_publish(DArr *out, JoinRec *r) {
+  const u64 w = r->written;
+  u64 *p = out->ptr + r->base;
+  if (w & 1) p[w] = p[w - 1];
+  out->n = r->base + ((w + 1) & ~1ull);
+}
+
+__global__ void k_hook_join_end(JoinArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  JoinRec *r = a.op;
+  if (r->skip || ctl_stop(a.ctl)) return;
+  hook_publish(a.out_newt, r);
+  prof_add(a.ctl, kPJoinMat, 16 * r->total + 24 * r->nc);
+}
+
+// Copy / ACopy: src/copy.cu:12-95, src/acopy.cu:12-50, as k_copy does them.
+__global__ void k_hook_copy_begin(CopyArgs c, JoinRec *r) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  r->written = 0;
+  r->skip = 1;
+  if (ctl_stop(c.ctl)) return;
+  if (c.once && *c.once) return;
+  const u64 n = eff_count(c.src, c.src_vis);
+  if (n == 0) {  // src/copy.cu:24-27 (dest NEWT count := 0); src/acopy.cu:14-18
+    c.dest->n = 0;
+    if (c.once_pending) *c.once_pending = 1;
+    return;
+  }
+  const u64 base = c.replace ? 0 : c.dest->n;
+  const u64 need = base + ((n + 1) & ~1ull);
+  if (need > c.dest->cap) {
+    atomicMax(&c.ctl->need[need_index(c.dest_rel, kNeedNewt)], need);
+    atomicExch(&c.ctl->overflow, 1u);
+    return;
+  }
+  r->total = n;
+  r->nc = 0;
+  r->base = base;
+  r->skip = 0;
+}
+
+__global__ void k_hook_copy_end(CopyArgs c, JoinRec *r) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (r->skip || ctl_stop(c.ctl)) return;
+  if (c.replace && r->written == 0) {
+    c.dest->n = 0;
+  } else if (r->written) {
+    hook_publish(c.dest, r);
+  }
+  if (c.once_pending) *c.once_pending = 1;
+  prof_add(c.ctl, kPCopy, 16 * r->total);
 }
 
 }  // namespace gdl

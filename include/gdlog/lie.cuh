@@ -8,6 +8,7 @@
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
+#include <deque>
 #include <type_traits>
 #include <vector>
 
@@ -47,6 +48,8 @@ struct LIE {
     for (Relation *r : static_relations) check(gdl_lie_add_relation(e, lie, r->id, 1), "add_relations");
     for (Relation *r : update_relations) check(gdl_lie_add_relation(e, lie, r->id, 0), "add_relations");
     for (Relation *r : tmp_relations) check(gdl_lie_add_tmp_relation(e, lie, r->id), "add_tmp_relation");
+    join_hooks_.clear();
+    copy_hooks_.clear();
     for (ra_op &op : ra_ops) std::visit([&](auto &o) { add_op(e, lie, o); }, op);
     check(gdl_lie_set_max_iteration(e, lie, max_iteration), "set_max_iteration");
     check(gdl_lie_set_reload_full(e, lie, reload_full_flag ? 1 : 0), "set_reload_full");
@@ -104,34 +107,75 @@ struct LIE {
     fflush(stdout);
   }
 
-  static void add_op(gdl_engine *e, int32_t lie, RelationalJoin &j) {
+  // Hook state the engine's launchers read while this LIE runs (a deque
+  // keeps element addresses fixed as it grows).
+  std::deque<gdlog_compat::JoinHooks> join_hooks_;
+  std::deque<tuple_copy_hook> copy_hooks_;
+
+  void add_op(gdl_engine *e, int32_t lie, RelationalJoin &j) {
     using namespace gdlog_compat;
-    int32_t gen[3];
+    if (!j.tuple_generator)  // the reference calls it unconditionally (src/relation.cu:348-358)
+      check(GDL_E_INVALID, "RelationalJoin: null tuple_generator_hook");
     const int out_arity = j.output_rel->arity;
-    if (!j.tuple_generator ||
-        !decode_generator(j.tuple_generator, j.inner_rel->arity, j.outer_rel->arity, out_arity, gen))
-      check(GDL_E_UNSUPPORTED,
-            "RelationalJoin: the generator hook must move columns (plus constants) only");
-    int32_t kind = GDL_PRED_NONE;
-    if (j.tuple_pred && !decode_predicate(j.tuple_pred, &kind))
-      check(GDL_E_UNSUPPORTED, "RelationalJoin: the predicate must compare t[0] with t[1]");
-    check(gdl_lie_add_join(e, lie, j.inner_rel->id, (int32_t)j.inner_ver, j.outer_rel->id,
-                           (int32_t)j.outer_ver, j.output_rel->id, gen, out_arity, kind, 0, 1),
-          "gdl_lie_add_join");
+    int32_t gen[4], kind = GDL_PRED_NONE, pa = 0, pb = 1;
+    bool sel = !exact_hooks() &&
+               decode_generator(j.tuple_generator, j.inner_rel->arity, j.outer_rel->arity,
+                                out_arity, gen);
+    if (sel && j.tuple_pred) {
+      // The engine's own predicate compares columns 0 and 1 of a plain
+      // arity-2 tuple; anything else runs through the hooks.
+      bool plain = out_arity == 2;
+      for (int c = 0; c < out_arity; c++) plain = plain && (gen[c] >> 8) == 0;
+      sel = plain && decode_predicate(j.tuple_pred, out_arity, &kind, &pa, &pb) && pa < 2 &&
+            pb < 2;
+    }
+    if (sel) {
+      log_hook("RelationalJoin", "column selection");
+      check(gdl_lie_add_join(e, lie, j.inner_rel->id, (int32_t)j.inner_ver, j.outer_rel->id,
+                             (int32_t)j.outer_ver, j.output_rel->id, gen, out_arity, kind, pa, pb),
+            "gdl_lie_add_join");
+      return;
+    }
+    log_hook("RelationalJoin", "device function pointers");
+    join_hooks_.push_back(JoinHooks{j.tuple_generator, j.tuple_pred});
+    check(gdl_lie_add_join_hooked(e, lie, j.inner_rel->id, (int32_t)j.inner_ver, j.outer_rel->id,
+                                  (int32_t)j.outer_ver, j.output_rel->id, launch_join_hooks,
+                                  &join_hooks_.back()),
+          "gdl_lie_add_join_hooked");
   }
-  static void add_op(gdl_engine *e, int32_t lie, RelationalCopy &c) {
+  void add_op(gdl_engine *e, int32_t lie, RelationalCopy &c) {
     using namespace gdlog_compat;
-    int32_t gen[2];
-    if (!c.tuple_generator || !decode_copy(c.tuple_generator, gen))
-      check(GDL_E_UNSUPPORTED, "RelationalCopy: the copy hook must move columns only");
-    check(gdl_lie_add_copy(e, lie, c.src_rel->id, (int32_t)c.src_ver, c.dest_rel->id, gen, 2),
-          "gdl_lie_add_copy");
+    if (!c.tuple_generator) check(GDL_E_INVALID, "RelationalCopy: null tuple_copy_hook");
+    int32_t gen[4];
+    const int out_arity = c.dest_rel->arity;
+    if (!exact_hooks() && decode_copy(c.tuple_generator, c.src_rel->arity, out_arity, gen)) {
+      log_hook("RelationalCopy", "column selection");
+      check(gdl_lie_add_copy(e, lie, c.src_rel->id, (int32_t)c.src_ver, c.dest_rel->id, gen,
+                             out_arity),
+            "gdl_lie_add_copy");
+      return;
+    }
+    log_hook("RelationalCopy", "device function pointers");
+    copy_hooks_.push_back(c.tuple_generator);
+    check(gdl_lie_add_copy_hooked(e, lie, c.src_rel->id, (int32_t)c.src_ver, c.dest_rel->id,
+                                  launch_copy_hook, &copy_hooks_.back()),
+          "gdl_lie_add_copy_hooked");
   }
-  static void add_op(gdl_engine *e, int32_t lie, RelationalACopy &c) {
+  void add_op(gdl_engine *e, int32_t lie, RelationalACopy &c) {
     using namespace gdlog_compat;
-    int32_t gen[2];
-    if (!c.tuple_generator || !decode_copy(c.tuple_generator, gen))
-      check(GDL_E_UNSUPPORTED, "RelationalACopy: the copy hook must move columns only");
-    check(gdl_lie_add_acopy(e, lie, c.src_rel->id, c.dest_rel->id, gen, 2), "gdl_lie_add_acopy");
+    if (!c.tuple_generator) check(GDL_E_INVALID, "RelationalACopy: null tuple_copy_hook");
+    int32_t gen[4];
+    const int out_arity = c.dest_rel->arity;
+    if (!exact_hooks() && decode_copy(c.tuple_generator, c.src_rel->arity, out_arity, gen)) {
+      log_hook("RelationalACopy", "column selection");
+      check(gdl_lie_add_acopy(e, lie, c.src_rel->id, c.dest_rel->id, gen, out_arity),
+            "gdl_lie_add_acopy");
+      return;
+    }
+    log_hook("RelationalACopy", "device function pointers");
+    copy_hooks_.push_back(c.tuple_generator);
+    check(gdl_lie_add_acopy_hooked(e, lie, c.src_rel->id, c.dest_rel->id, launch_copy_hook,
+                                   &copy_hooks_.back()),
+          "gdl_lie_add_acopy_hooked");
   }
 };

@@ -238,6 +238,73 @@ gdl_status gdl_lie_add_copy(gdl_engine *e, int32_t lie, int32_t src,
 gdl_status gdl_lie_add_acopy(gdl_engine *e, int32_t lie, int32_t src,
                              int32_t dest, const int32_t *gen, int32_t gen_len);
 
+/* Operators whose per-tuple work is the caller's own code.
+ *
+ * The reference calls a program's __device__ hooks through device function
+ * pointers, once per candidate tuple (get_join_result, src/relation.cu:
+ * 290-373, with tp_gen and tp_pred at :348-358; get_copy_result,
+ * src/relation.cu:390-403).  A hook that is not a column selection (plus a
+ * constant) cannot be given to gdl_lie_add_join as `gen`; these entry points
+ * take it as a launcher instead.  In every iteration the engine does what
+ * surrounds the hook (the count pass over the inner index, the reference's
+ * empty-operand rules, the once-per-LIE FULL copy, NEWT capacity), then
+ * calls `launch(ctx, &work, stream)`, which must only enqueue kernels on
+ * `stream` (it is also called while the engine captures its loop into a CUDA
+ * graph, and again whenever it re-captures).  The kernels read the work
+ * from device memory through `work`, call the hook on every candidate, and
+ * append the packed keys of the tuples they keep to `out` (see
+ * gdl_hook_work).  The drop-in C++ API (include/gdlog/engine.cuh) supplies
+ * such launchers for a program's hooks.  A LIE with one of these operators
+ * runs on sorted tuple lists (no bitmaps). */
+typedef struct gdl_dev_rows {
+  uint64_t *ptr; /* packed keys: c0 << 32 | c1, or c0 << 32 | c1 << k2 | c2 */
+  uint64_t n;    /* rows present */
+  uint64_t cap;  /* rows allocated */
+} gdl_dev_rows;
+
+typedef struct gdl_hook_state {
+  uint64_t total;    /* join: candidates; copy: source rows */
+  uint64_t records;  /* join: candidate records (see rec_offset) */
+  uint64_t base;     /* first position in out->ptr this operator writes */
+  uint64_t overflow; /* engine-internal */
+  uint64_t written;  /* rows appended so far: reserve with atomicAdd */
+  uint64_t skip;     /* nonzero: the operator does nothing this iteration */
+} gdl_hook_state;
+
+typedef struct gdl_hook_work {
+  int32_t kind;        /* 0 join, 1 copy, 2 acopy */
+  int32_t in_arity;    /* inner (join) or source (copy) arity */
+  int32_t outer_arity; /* join only */
+  int32_t out_arity;
+  int32_t k2;          /* bits of column 2 in arity-3 keys */
+  int32_t sms;         /* multiprocessors of the device, for grid sizing */
+  gdl_hook_state *state;     /* device */
+  const gdl_dev_rows *rows;  /* device: join inner version / copy source */
+  /* Join candidates, device: record k (k < state->records) covers candidate
+   * positions [rec_offset[k], rec_offset[k+1]); candidate p pairs inner row
+   * rows->ptr[rec_start[k] + p - rec_offset[k]] with outer row rec_key[k].
+   * Copy: candidate p is source row rows->ptr[p], p < state->total. */
+  const uint64_t *rec_offset;
+  const uint32_t *rec_start;
+  const uint64_t *rec_key;
+  gdl_dev_rows *out;  /* device: NEWT of the output; write out->ptr[state->base + i] */
+  uint32_t *error;    /* device: OR 32768 when a generated value does not fit its column */
+} gdl_hook_work;
+
+typedef void (*gdl_hook_launch)(void *ctx, const gdl_hook_work *work, void *stream);
+
+/* RelationalJoin with its generator and predicate run by `launch`. */
+gdl_status gdl_lie_add_join_hooked(gdl_engine *e, int32_t lie, int32_t inner,
+                                   int32_t inner_version, int32_t outer,
+                                   int32_t outer_version, int32_t output,
+                                   gdl_hook_launch launch, void *ctx);
+/* RelationalCopy / RelationalACopy with the copy hook run by `launch`. */
+gdl_status gdl_lie_add_copy_hooked(gdl_engine *e, int32_t lie, int32_t src,
+                                   int32_t src_version, int32_t dest,
+                                   gdl_hook_launch launch, void *ctx);
+gdl_status gdl_lie_add_acopy_hooked(gdl_engine *e, int32_t lie, int32_t src,
+                                    int32_t dest, gdl_hook_launch launch, void *ctx);
+
 /* LIE::max_iteration / LIE::reload_full_flag (include/lie.cuh:29-30). */
 gdl_status gdl_lie_set_max_iteration(gdl_engine *e, int32_t lie,
                                      int64_t max_iteration);

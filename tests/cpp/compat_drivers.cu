@@ -9,6 +9,9 @@
 //   compat_drivers cspa <assign.tsv> <dereference.tsv>
 //   compat_drivers path_length <edges.tsv>   (arity 3, dependent column,
 //                                             a hook that adds 1)
+//   compat_drivers hook_max | hook_pred | hook_copy <edges.tsv>
+//                      (hooks that are not column selections: run through
+//                       their device function pointers)
 //
 // Prints one line: RESULT {"sizes": ..., "digests": ..., "iterations": ...}
 #include <cstdio>
@@ -48,6 +51,26 @@ __device__ void path_step(tuple_type inner, tuple_type outer, tuple_type out) {
   out[2] = outer[2] + 1;
 }
 __device__ tuple_generator_hook path_step_d = path_step;
+
+// Hooks that are not column selections: the engine runs them through
+// their function pointers, as the reference does.
+__device__ void join_max(tuple_type inner, tuple_type outer, tuple_type out) {
+  out[0] = inner[1] > outer[1] ? inner[1] : outer[1];
+  out[1] = outer[1];
+}
+__device__ bool ne_and_below(tuple_type t) { return t[0] != t[1] && t[0] < 100; }
+__device__ void copy_xor(tuple_type src, tuple_type dst) {
+  dst[0] = src[1];
+  dst[1] = src[0] ^ 1;
+}
+__device__ void copy_swap_xor(tuple_type src, tuple_type dst) {
+  dst[0] = src[1] ^ 1;
+  dst[1] = src[0];
+}
+__device__ tuple_generator_hook join_max_d = join_max;
+__device__ tuple_predicate ne_and_below_d = ne_and_below;
+__device__ tuple_copy_hook copy_xor_d = copy_xor;
+__device__ tuple_copy_hook copy_swap_xor_d = copy_swap_xor;
 
 __device__ tuple_generator_hook join_i1_o1_d = join_i1_o1;
 __device__ tuple_generator_hook join_o1_i1_d = join_o1_i1;
@@ -117,6 +140,79 @@ int main(int argc, char **argv) {
     tc.fixpoint_loop();
     iters["tc"] = tc.iteration_counter;
     out["path"] = path;
+  } else if (prog == "hook_max") {
+    // path(max(x, z), z) :- edge(x, y), path(y, z): a generator that
+    // compares columns.
+    auto e = read_tsv(argv[2]);
+    auto re = swap_cols(e);
+    Relation *edge = new Relation();
+    Relation *path = new Relation();
+    path->index_flag = false;
+    load(path, "path_2__1_2", &e);
+    load(edge, "edge_2__2_1", &re);
+    LIE lie(grid, block);
+    lie.add_relations(edge, true);
+    lie.add_relations(path, false);
+    lie.add_ra(RelationalJoin(edge, FULL, path, DELTA, path, fetch(join_max_d), nullptr, LEFT,
+                              grid, block, detail));
+    lie.fixpoint_loop();
+    iters["lie"] = lie.iteration_counter;
+    out["path"] = path;
+  } else if (prog == "hook_pred") {
+    // same generation's first rule with the predicate t0 != t1 && t0 < 100,
+    // then the recursive rules as in test/sg.cu
+    auto e = read_tsv(argv[2]);
+    Relation *edge12 = new Relation(), *sg = new Relation(), *tmp = new Relation();
+    sg->index_flag = false;
+    load(edge12, "edge_2__1_2", &e);
+    load(sg, "sg_2__2_1", nullptr);
+    LIE init(grid, block);
+    init.add_relations(edge12, true);
+    init.add_relations(sg, false);
+    init.add_ra(RelationalJoin(edge12, FULL, edge12, FULL, sg, fetch(join_i1_o1_d),
+                               fetch(ne_and_below_d), LEFT, grid, block, detail));
+    init.fixpoint_loop();
+    load(tmp, "tmp", nullptr);
+    tmp->index_flag = false;
+    LIE lie(grid, block);
+    lie.add_relations(edge12, true);
+    lie.add_relations(sg, false);
+    lie.add_tmp_relation(tmp);
+    lie.add_ra(RelationalJoin(edge12, FULL, sg, DELTA, tmp, fetch(join_o1_i1_d), nullptr, LEFT,
+                              grid, block, detail));
+    lie.add_ra(RelationalJoin(edge12, FULL, tmp, NEWT, sg, fetch(join_o1_i1_d),
+                              fetch(ne_and_below_d), LEFT, grid, block, detail));
+    lie.fixpoint_loop();
+    iters["init"] = init.iteration_counter;
+    iters["lie"] = lie.iteration_counter;
+    out["sg"] = sg;
+  } else if (prog == "hook_copy") {
+    // r seeded by a copy hook that flips a bit, closed under the edges;
+    // m the ACopy of r's NEWT through another such hook; d a copy of r's
+    // DELTA through the first.
+    auto e = read_tsv(argv[2]);
+    auto re = swap_cols(e);
+    Relation *edge = new Relation(), *r = new Relation(), *m = new Relation(),
+             *d = new Relation();
+    load(edge, "edge_2__2_1", &re);
+    load(r, "r", nullptr);
+    load(m, "m", nullptr);
+    load(d, "d", nullptr);
+    LIE lie(grid, block);
+    lie.add_relations(edge, true);
+    lie.add_relations(r, false);
+    lie.add_relations(m, false);
+    lie.add_relations(d, false);
+    lie.add_ra(RelationalCopy(edge, FULL, r, fetch(copy_xor_d), nullptr, grid, block));
+    lie.add_ra(RelationalJoin(edge, FULL, r, DELTA, r, fetch(join_i1_o1_d), nullptr, LEFT, grid,
+                              block, detail));
+    lie.add_ra(RelationalCopy(r, DELTA, d, fetch(copy_xor_d), nullptr, grid, block));
+    lie.add_ra(RelationalACopy(r, m, fetch(copy_swap_xor_d), nullptr, grid, block));
+    lie.fixpoint_loop();
+    iters["lie"] = lie.iteration_counter;
+    out["r"] = r;
+    out["m"] = m;
+    out["d"] = d;
   } else if (prog == "sg") {
     auto e = read_tsv(argv[2]);
     auto re = swap_cols(e);
