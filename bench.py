@@ -23,7 +23,10 @@ the reference's semi-naive loop) on all host cores.
 
 --impl reference runs that same CPU implementation as the reference arm
 (the reference's own CPU path, its Souffle programs, cannot be built
-offline; its CUDA engine is timed separately as a GPU baseline).
+offline); on a GPU machine that line also carries `reference_gpu`: the
+reference's CUDA engine, built unmodified from its sources, timed live on
+the same input.  `e2e_phases_ms` splits one extra end-to-end step by
+public-API call.
 Under torchrun every rank runs one replica of the workload (the single
 fixpoint does not shard); value sums the ranks' tuples over the slowest
 rank's time.
@@ -53,6 +56,12 @@ WORKLOADS = {
         prog=P.sg, make=lambda: (W.rmat_edges(14, 40000, seed=14),),
         desc="same generation, R-MAT scale 14 (16,384 nodes), 40,000 edges, "
              "a,b,c,d=.57,.19,.19,.05, seed 14"),
+    # the same program and input on the sorted-list path (radix sort +
+    # merge-path dedup of every candidate), so the sort kernels dominate
+    "sg_rmat_s14_sort": dict(
+        prog=P.sg, make=lambda: (W.rmat_edges(14, 40000, seed=14),), tuning={"dedup": "sort"},
+        desc="same generation, R-MAT scale 14 (16,384 nodes), 40,000 edges, "
+             "a,b,c,d=.57,.19,.19,.05, seed 14; sorted-list path (dedup=sort)"),
     "tc_grid_64": dict(
         prog=P.tc, make=lambda: (W.grid_edges(64, 64),),
         desc="transitive closure, 64x64 directed grid, 8,064 edges"),
@@ -180,9 +189,13 @@ def roofline_of(prof: dict, workload: str, peaks: dict) -> dict:
     per_launch_ms = rec["ms"] / max(rec["launches"], 1)
     per_launch_bytes = rec["bytes"] / max(rec["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else 0.0
+    traffic = traffic_for(workload, kind, per_launch_bytes)
+    dram_gbs = traffic / (per_launch_ms / 1e3) / 1e9 if (traffic and per_launch_ms) else None
     return {"bound": "hbm", "kernel": kind, "achieved": achieved,
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-            "traffic": traffic_for(workload, kind, per_launch_bytes),
+            "traffic": traffic,
+            "dram_gbs": dram_gbs,
+            "frac_dram": dram_gbs / peaks["hbm_gbs"] if dram_gbs else None,
             "alg_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
             "launches": rec["launches"],
             "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)"}
@@ -208,20 +221,102 @@ def traffic_for(workload: str, kind: str, alg_bytes_per_launch: float):
     return rec["dram_bytes"] / rec["alg_bytes"] * alg_bytes_per_launch
 
 
-def reference_gpu(workload: str):
-    """Fixpoint seconds of the reference CUDA engine on this workload, as
-    recorded by tests/golden/make_ref_gpu.py on a B200."""
-    key = {"sg_rmat_s14": "sg_rmat_s14_40000_s14", "tc_grid_64": "tc_grid_64x64",
-           "cspa_v300": "cspa_v300_s3", "plen_grid_64": "plen_grid_64x64"}.get(workload)
-    p = os.path.join(REPO, "tests", "golden", "ref_gpu.json")
-    if not os.path.exists(p):
+# Workloads on which the reference CUDA build runs (oracle/_ref/ref_runner):
+# program and input files.  It is not run on the larger points-to inputs,
+# where it made an illegal memory access (2,000 variables) or ran out of
+# device memory (6,000 variables).
+REF_GPU_RUNS = {"sg_rmat_s14": "sg", "sg_rmat_s14_sort": "sg", "sg_rmat_s13": "sg",
+                "tc_grid_64": "tc", "cspa_v300": "cspa", "plen_grid_64": "plen"}
+
+
+def reference_gpu_live(workload: str, inputs, runs: int = 3):
+    """The reference CUDA engine (built unmodified from its sources into
+    oracle/_ref/ref_runner) on the same input, timed as its drivers time
+    fixpoint_loop (test/tc.cu:120-140): median fixpoint seconds of `runs`
+    runs, with the clocks sampled meanwhile.  None when the runner is not
+    built or the workload is not one it runs on."""
+    import tempfile
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_runner")
+    prog = REF_GPU_RUNS.get(workload)
+    if not prog or not os.path.exists(exe):
         return None
-    rec = json.load(open(p)).get(key)
-    if not rec or "seconds" not in rec:
-        return None
+    secs, rec = [], None
+    with tempfile.TemporaryDirectory() as d, ClockSampler(0) as clocks:
+        files = []
+        for i, rows in enumerate(inputs):
+            f = os.path.join(d, f"in{i}.tsv")
+            W.write_tsv(f, rows)
+            files.append(f)
+        for _ in range(runs):
+            r = subprocess.run([exe, prog, *files], stdout=subprocess.DEVNULL,
+                               stderr=subprocess.PIPE, text=True, timeout=600)
+            line = [ln for ln in r.stderr.splitlines() if ln.startswith("REF ")]
+            if r.returncode != 0 or not line:
+                return {"unavailable": f"ref_runner exit {r.returncode}"}
+            rec = json.loads(line[-1][4:])
+            secs.append(rec["seconds"])
     t = sum(rec["sizes"].values())
-    return {"seconds": rec["seconds"], "value": t / rec["seconds"], "unit": "tuples/s",
-            "source": "reference CUDA engine built from its own sources, same input, B200"}
+    sec = statistics.median(secs)
+    return {"value": t / sec, "unit": "tuples/s", "seconds": sec, "runs": runs,
+            "tuples": t, "iterations": rec["iterations"], "clocks": clocks.summary(),
+            "source": "reference CUDA engine built unmodified from its sources "
+                      "(oracle/_ref/ref_runner), same input, this GPU, timed like its drivers"}
+
+
+def e2e_phases(eng, wl: dict, pinned) -> dict:
+    """One more end-to-end step (untimed by the line's e2e number) with every
+    public-API call timed on the host and the engine stream synchronised
+    after each call, so the phases add up to where an e2e step's time goes:
+    engine clear, relation creation, loads (host->device copy, pack, sort,
+    deduplicate, index), LIE creation, the fixpoints (with their host setup,
+    graph capture and device time from gdl_lie_stats), size and digest."""
+    import gdlog_b200 as G
+    acc: dict = {}
+    patched = []
+
+    def wrap(obj, name, label):
+        fn = getattr(obj, name)
+        patched.append((obj, name, obj.__dict__.get(name)))
+
+        def timed(*args, **kw):
+            t0 = time.perf_counter()
+            out = fn(*args, **kw)
+            eng.sync()
+            acc[label] = acc.get(label, 0.0) + (time.perf_counter() - t0) * 1e3
+            return out
+        setattr(obj, name, timed)
+
+    wrap(eng, "relation", "create_relations")
+    wrap(eng, "load", "loads")
+    wrap(eng, "lie", "create_lies")
+    wrap(G.Lie, "fixpoint", "fixpoints")
+    wrap(G.Relation, "size", "size")
+    wrap(G.Relation, "digest", "digest")
+    try:
+        t_all = time.perf_counter()
+        t0 = time.perf_counter()
+        eng.clear()
+        eng.sync()
+        acc["clear"] = (time.perf_counter() - t0) * 1e3
+        r = wl["prog"](eng, *pinned)
+        for rel in r.relations.values():
+            rel.size()
+            rel.digest()
+        total = (time.perf_counter() - t_all) * 1e3
+    finally:
+        for obj, name, orig in reversed(patched):
+            if orig is None:
+                delattr(obj, name)
+            else:
+                setattr(obj, name, orig)
+    st = [lie.stats() for lie in r.lies.values()]
+    out = {k: round(v, 4) for k, v in acc.items()}
+    out["fixpoint_device_ms"] = round(sum(x["ms"] for x in st), 4)
+    out["fixpoint_host_setup_ms"] = round(sum(x["setup_ms"] for x in st), 4)
+    out["fixpoint_graph_ms"] = round(sum(x["graph_ms"] for x in st), 4)
+    out["other_host_ms"] = round(total - sum(acc.values()), 4)
+    out["total_ms"] = round(total, 4)
+    return out
 
 
 def run_ours(a) -> None:
@@ -253,6 +348,9 @@ def run_ours(a) -> None:
         return
     rec = tuner.apply(eng, wl["prog"], inputs)
     tuning = rec["config"] if rec else "engine defaults (no cached tuning for this size bucket)"
+    if wl.get("tuning"):
+        eng.set_tuning(**wl["tuning"])
+        tuning = {"workload_setting": wl["tuning"], "cached": tuning}
     dev_inputs = inputs if wl.get("host_inputs") else \
         [DeviceRows(torch.from_numpy(x.astype(np.int64)).to(dev)) for x in inputs]
     pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() for x in inputs]
@@ -320,6 +418,7 @@ def run_ours(a) -> None:
         barrier()
     e2e_ms = e0.elapsed_time(e1)
     host_per_step = {k: v / a.steps for k, v in host.items()}
+    phases = e2e_phases(eng, wl, pinned)
     # profiled step: an event pair around every launch
     eng.profile_reset()
     eng.set_profile(True)
@@ -351,26 +450,31 @@ def run_ours(a) -> None:
                    "tuples_per_step": tuples / a.steps / world,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "tuning": tuning,
-                   "l2": "flushed between steps (256 MB write); relations exceed L2"},
+                   "l2": "flushed between steps (256 MB write); within a step the working set "
+                         "(bitmaps of 2^(2*bits) bits, 32 MB each at 2^14 ids) fits the 126 MB "
+                         "L2"},
         "e2e": {"value": e2e_tuples / (e2e_ms / 1e3), "unit": "tuples/s",
                 "h2d_bytes_per_step": int(sum(x.nbytes for x in pinned)),
                 "d2h_bytes_per_step": 16 * n_out[0]},
         "gpu_launches": int(kernels),
         "roofline": roofline_of(prof, a.workload, peaks),
         "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4),
-                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] else None}
+                        "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] else None,
+                        "frac": (v["bytes"] / (v["ms"] / 1e3) / 1e9 / peaks["hbm_gbs"])
+                        if v["ms"] else None}
                     for k, v in prof.items() if v["launches"]},
         "clocks": clocks.summary(),
         "host_ms_per_step": host_per_step,
+        "e2e_phases_ms": phases,
     }
-    ref = reference_gpu(a.workload)
-    if ref:
-        line["reference_gpu"] = ref
     if world == 1 and not a.no_cpu_baseline and not wl.get("no_cpu"):
-        secs, t, threads = oracle_run(wl, inputs)
+        runs = [oracle_run(wl, inputs) for _ in range(3)]
+        secs = statistics.median(r[0] for r in runs)
+        t, threads = runs[0][1], runs[0][2]
         line["cpu_baseline"] = {"value": t / secs, "unit": "tuples/s", "cores": threads,
                                 "kind": "port",
-                                "sample": "one full run of the same workload on the CPU oracle"}
+                                "sample": "median of 3 full runs of the same workload on the "
+                                          "CPU oracle (fixpoint seconds)"}
     elif wl.get("no_cpu"):
         line["cpu_baseline"] = {"value": None, "unavailable":
                                 "the CPU oracle would need many minutes (or more host memory) "
@@ -393,7 +497,7 @@ def run_reference(a) -> None:
         return
     inputs = wl["make"]()
     secs0, _, _ = oracle_run(wl, inputs)  # one warm-up run (CPU caches, page faults)
-    budget = 240.0
+    budget = 330.0  # seconds of timed CPU work
     steps = max(1, min(a.steps, int(budget // max(secs0, 1e-3))))
     total, tuples, threads = 0.0, 0, 0
     for _ in range(steps):
@@ -401,11 +505,14 @@ def run_reference(a) -> None:
         total += s
         tuples += t
     v = tuples / total
-    print(json.dumps({
+    line = {
         "impl": "reference", "metric": "derived tuples/s (SG fixpoint)"
         if a.workload == "sg_rmat_s14" else "derived tuples/s",
-        "value": v, "unit": "tuples/s", "n_gpus": world, "steps": a.steps,
-        "steps_timed": steps, "warmup": a.warmup, "warmup_timed_out": max(a.warmup - 1, 0),
+        "value": v, "unit": "tuples/s", "n_gpus": world,
+        # what ran: `steps` timed runs after one warm-up run (each run is
+        # the whole workload; the steps are capped by a CPU-time budget)
+        "steps": steps, "warmup": 1, "steps_requested": a.steps,
+        "warmup_requested": a.warmup,
         "ms_per_step": total / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": wl["desc"], "program": wl["prog"].__name__,
@@ -414,7 +521,17 @@ def run_reference(a) -> None:
                          "sample": f"{steps} full run(s) of the workload, after one warm-up run"},
         "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-    }), flush=True)
+    }
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except Exception:
+        gpu = False
+    if gpu:
+        ref = reference_gpu_live(a.workload, inputs)
+        if ref:
+            line["reference_gpu"] = ref
+    print(json.dumps(line), flush=True)
 
 
 def run_reference_dag(a, world) -> None:

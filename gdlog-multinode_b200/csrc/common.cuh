@@ -99,6 +99,8 @@ struct RelDev {
   // outers; and NEWT's transposed twin that joins with a transposed output
   // write (folded into NEWT after each such join, zero between them).
   u32 *bmDT, *bmGT, *bmOT;
+  // DELTA's rows as they are, for row-gather joins that read DELTA (pull.cuh)
+  u32 *bmDN;
 };
 
 // Loop control of a running fixpoint (one per engine, device memory).

@@ -138,6 +138,11 @@ struct RelHost {
   bool bm_valid = false;       // bmF holds FULL (set by a dense LIE)
   bool full_resident = false;  // FULL exists only as bmF (batched form, or too large)
   int bm_dk = 0;               // square domain bits of that bitmap (plain form)
+  // In-edges of this relation's FULL (column-1 value -> column-0 values),
+  // built at the start of a LIE whose row-gather joins read it as inner.
+  u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr, *inv_ys = nullptr;
+  u64 inv_cap = 0;
+  int inv_dk = 0;
 };
 
 }  // namespace
@@ -190,6 +195,7 @@ struct gdl_engine {
   // 1: push form only, 2: pull form where eligible from 2^kPullAutoBits ids,
   // 3: pull form where eligible (pull.cuh)
   int pull_joins = 2;
+  int row_gather = 2;
   u64 *d_pull_count = nullptr;  // bit count of a transposed NEWT (zero between launches)
   // Device memory in bytes, read once at creation: cudaMemGetInfo can take
   // tens of milliseconds on a busy host, so the fixpoint sizes its lists
@@ -489,7 +495,7 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   RelHost &rh = e->rels[r];
   RelDev &h = e->h[r];
   if (rh.bm_words != words) {
-    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT, &h.bmOT}) {
+    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT, &h.bmOT, &h.bmDN}) {
       dfree(e, *p);
       *p = nullptr;
     }
@@ -640,6 +646,12 @@ struct Plan {
   std::vector<char> fold_late;            // per relation: its transposed twin is its NEWT
   std::vector<char> delta_t, newt_t;      // per relation: transposed DELTA / NEWT read
   std::vector<char> delta_list;           // per relation: DELTA read as a list by some op
+  std::vector<char> rows;                 // per op: row-gather form (pull.cuh, k_join_rows_bm)
+  std::vector<char> delta_n;              // per relation: DELTA rows kept non-transposed too
+  // per op: writes the output's transposed twin (pull form with output
+  // (inner column 1, outer column 1), or row-gather form with output
+  // (outer column 1, inner column 1))
+  std::vector<char> out_twin;
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -657,6 +669,9 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.delta_t.assign(n, 0);
   p.newt_t.assign(n, 0);
   p.delta_list.assign(n, 0);
+  p.rows.assign(L.ops.size(), 0);
+  p.delta_n.assign(n, 0);
+  p.out_twin.assign(L.ops.size(), 0);
   for (const OpHost &op : L.ops) {
     if (op.kind == 0 && op.outer_ver == GDL_DELTA) p.delta_list[op.outer] = 1;
     if (op.kind != 2 && op.inner_ver == GDL_DELTA) p.delta_list[op.inner] = 1;
@@ -711,11 +726,8 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
                           (op.outer_ver == GDL_NEWT && is_tmp[op.outer]);
     if ((fwd || rev) && outer_ok) {
       p.pull[oi] = 1;
-      if (rev) {
-        p.pull_t[oi] = 1;
-        p.out_t[op.out] = 1;
-      }
-      (op.outer_ver == GDL_DELTA ? p.delta_t : p.newt_t)[op.outer] = 1;
+      if (rev) p.pull_t[oi] = 1;
+      if (op.outer_ver == GDL_DELTA) p.delta_t[op.outer] = 1;
     } else if (op.outer_ver == GDL_NEWT) {
       p.newt_list[op.outer] = 1;
     } else if (op.outer_ver == GDL_DELTA) {
@@ -727,6 +739,30 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
   for (int r : L.update)
     if (!p.delta_list[r]) p.delta_t[r] = 1;
+  // Row-gather form (pull.cuh, k_join_rows_bm) for the pull-form joins over
+  // a static inner FULL small enough that reading one outer row per in-edge
+  // beats expanding candidates: |inner| rows of 2^(dk-5) words within
+  // kRowsBudget bytes (any size with row_gather = 3).  A DELTA outer must be
+  // a relation whose update step is the fused pass (it writes DELTA's rows).
+  std::vector<char> is_static(e->rels.size(), 0);
+  for (int r : L.statics) is_static[r] = 1;
+  for (size_t oi = 0; oi < L.ops.size(); oi++) {
+    const OpHost &op = L.ops[oi];
+    if (!p.pull[oi] || e->row_gather == 1 || L.dk < kRowsMinBits) continue;
+    if (op.inner_ver == GDL_DELTA || !is_static[op.inner]) continue;
+    const u64 bytes = e->h[op.inner].full.n * (4ull << (L.dk - 5));
+    if (e->row_gather != 3 && bytes > kRowsBudget) continue;
+    if (op.outer_ver == GDL_DELTA && !fused_update(p, op.outer)) continue;
+    p.rows[oi] = 1;
+    if (op.outer_ver == GDL_DELTA) p.delta_n[op.outer] = 1;
+  }
+  for (size_t oi = 0; oi < L.ops.size(); oi++) {
+    const OpHost &op = L.ops[oi];
+    if (!p.pull[oi]) continue;
+    if (op.outer_ver == GDL_NEWT && !p.rows[oi]) p.newt_t[op.outer] = 1;
+    p.out_twin[oi] = p.pull_t[oi] != p.rows[oi];
+    if (p.out_twin[oi]) p.out_t[op.out] = 1;
+  }
   // A relation written only by transposed-output joins, whose NEWT no op
   // reads and whose update step is the fused pass, keeps NEWT as the
   // transposed twin: no fold after each join, the update reads it.
@@ -735,7 +771,7 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
       continue;
     bool only_t = true;
     for (size_t oi = 0; oi < L.ops.size(); oi++)
-      if (L.ops[oi].out == r && !p.pull_t[oi]) only_t = false;
+      if (L.ops[oi].out == r && !p.out_twin[oi]) only_t = false;
     p.fold_late[r] = only_t;
   }
 }
@@ -743,6 +779,7 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
 // Transposed bitmaps of the relations pull-form joins read.
 gdl_status ensure_tbitmaps(gdl_engine *e, const Plan &p, int r, u64 words) {
   RelDev &h = e->h[r];
+  if (p.delta_n[r] && !h.bmDN) TRY(dalloc(e, (void **)&h.bmDN, words * 4));
   if (p.delta_t[r] && !h.bmDT) TRY(dalloc(e, (void **)&h.bmDT, words * 4));
   if (p.newt_t[r] && !h.bmGT) TRY(dalloc(e, (void **)&h.bmGT, words * 4));
   if (p.out_t[r] && !h.bmOT) TRY(dalloc(e, (void **)&h.bmOT, words * 4));
@@ -816,6 +853,50 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
 // One iteration.  in_graph: the body of the graph's while-node, which the
 // host opens with a k_begin before each launch and whose k_commit opens
 // the next iteration; otherwise the iteration opens itself.
+void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
+  const int g = (int)e->sms * 8;
+  switch (ra.dk) {
+    case 12: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<1><<<g, 256, 0, e->s>>>(ra)); break;
+    case 13: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<2><<<g, 256, 0, e->s>>>(ra)); break;
+    case 14: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<4><<<g, 256, 0, e->s>>>(ra)); break;
+    case 15: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<8><<<g, 256, 0, e->s>>>(ra)); break;
+    default: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<16><<<g, 256, 0, e->s>>>(ra)); break;
+  }
+}
+
+// In-edges of relation r's FULL list over 2^dk ids (k_inv_*, pull.cuh).
+gdl_status build_inverse(gdl_engine *e, int r, int dk) {
+  RelHost &rh = e->rels[r];
+  const u64 n = e->h[r].full.n;
+  const u32 ids = 1u << dk;
+  if (rh.inv_dk != dk) {
+    for (u32 **q : {&rh.inv_off, &rh.inv_cur}) {
+      dfree(e, *q);
+      *q = nullptr;
+    }
+    TRY(dalloc(e, (void **)&rh.inv_off, (ids + 1) * sizeof(u32)));
+    TRY(dalloc(e, (void **)&rh.inv_cur, ids * sizeof(u32)));
+    rh.inv_dk = dk;
+  }
+  if (rh.inv_cap < std::max<u64>(n, 1)) {
+    for (u32 **q : {&rh.inv_keys, &rh.inv_ys}) {
+      dfree(e, *q);
+      *q = nullptr;
+    }
+    rh.inv_cap = std::max<u64>(n, 1);
+    TRY(dalloc(e, (void **)&rh.inv_keys, rh.inv_cap * sizeof(u32)));
+    TRY(dalloc(e, (void **)&rh.inv_ys, rh.inv_cap * sizeof(u32)));
+  }
+  CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
+  const DArr *list = &e->d_rels[r].full;
+  k_inv_count<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, dk, e->d_ctl);
+  k_inv_scan<<<1, 1024, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
+  k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
+                                                       dk);
+  CK(e, cudaGetLastError());
+  return GDL_OK;
+}
+
 static_assert(sizeof(DArr) == sizeof(gdl_dev_rows), "gdl_dev_rows mirrors DArr");
 static_assert(sizeof(JoinRec) == sizeof(gdl_hook_state), "gdl_hook_state mirrors JoinRec");
 static_assert(offsetof(JoinRec, written) == offsetof(gdl_hook_state, written), "JoinRec layout");
@@ -933,6 +1014,30 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         op.hook(op.hook_ctx, &w, (void *)s);
         kc->add(kPJoinMat);
         PLAUNCH(kc, kPControl, k_hook_join_end<<<1, 32, 0, s>>>(a));
+        continue;
+      }
+      if (plan.pull[oi] && plan.rows[oi]) {
+        // gathered along the inner's in-edges from the outer's rows
+        RowsArgs ra;
+        memset(&ra, 0, sizeof ra);
+        ra.j = a;
+        ra.j.rec = &e->recs[6];
+        ra.O = op.outer_ver == GDL_DELTA ? oh.bmDN : oh.bmG;
+        ra.outer_clear = op.outer_ver == GDL_NEWT ? oh.bmG : nullptr;
+        const RelHost &ih = e->rels[op.inner];
+        ra.inv_off = ih.inv_off;
+        ra.inv_keys = ih.inv_keys;
+        ra.inv_ys = ih.inv_ys;
+        const RelDev &out = e->h[op.out];
+        ra.dst = plan.out_twin[oi] ? out.bmOT : out.bmG;
+        ra.dirty = plan.out_twin[oi] ? nullptr : out.dirty;
+        ra.dk = L.dk;
+        launch_rows(e, ra, kc);
+        if (plan.out_twin[oi] && !plan.fold_late[op.out]) {
+          const u64 side = 1ull << (L.dk - kPullMinBits);
+          PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
+                                    out.bmOT, out.bmG, out.dirty, L.dk, e->d_ctl));
+        }
         continue;
       }
       if (plan.pull[oi]) {
@@ -1119,7 +1224,8 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       const int r = (int)(a.rd - R);
       const u64 side = 1ull << (L.dk - kPullMinBits);
       PLAUNCH(kc, kPBitmap, k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                a, e->h[r].bmDT, L.dk, plan.fold_late[r] ? e->h[r].bmOT : nullptr));
+                                a, e->h[r].bmDT, L.dk, plan.fold_late[r] ? e->h[r].bmOT : nullptr,
+                                plan.delta_n[r] ? e->h[r].bmDN : nullptr));
     }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
     // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
@@ -1478,6 +1584,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           k_bm_from_list_t<<<grid_for(e, h.delta.n, 256, 8), 256, 0, e->s>>>(
               &e->d_rels[r].delta, h.bmDT, L.dk, e->d_ctl);
       }
+      if (plan.delta_n[r]) {
+        // ... and as rows, for the row-gather joins
+        CK(e, cudaMemsetAsync(h.bmDN, 0, words * 4, e->s));
+        if (h.delta.n)
+          k_bm_from_list<<<grid_for(e, h.delta.n, 256, 8), 256, 0, e->s>>>(
+              &e->d_rels[r].delta, h.bmDN, L.map, e->d_ctl);
+      }
       e->rels[r].bm_valid = true;
     }
     for (int r : L.tmps) {
@@ -1487,6 +1600,14 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     for (auto *v : {&L.update, &L.tmps})
       for (int r : *v)
         if (plan.out_t[r]) CK(e, cudaMemsetAsync(e->h[r].bmOT, 0, words * 4, e->s));
+    // the in-edges of the static inners of row-gather joins
+    std::vector<char> built(e->rels.size(), 0);
+    for (size_t oi = 0; oi < L.ops.size(); oi++) {
+      const int r = L.ops[oi].inner;
+      if (!plan.rows[oi] || built[r]) continue;
+      TRY(build_inverse(e, r, L.dk));
+      built[r] = 1;
+    }
     CK(e, cudaGetLastError());
   }
   mark("bitmaps");
@@ -1992,10 +2113,13 @@ static void release_program(gdl_engine *e) {
       if (a->ptr) cudaFreeAsync(a->ptr, e->s);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
       if (x->slots) cudaFreeAsync(x->slots, e->s);
-    for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT, r.bmOT})
+    for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT, r.bmOT, r.bmDN})
       if (bm) cudaFreeAsync(bm, e->s);
     if (r.bmD) cudaFreeAsync(r.bmD, e->s);
     if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);
+    const RelHost &rh = e->rels[i];
+    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_keys, rh.inv_ys})
+      if (q) cudaFreeAsync(q, e->s);
     if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
   }
   for (LieHost &L : e->lies) {
@@ -2673,7 +2797,8 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
                                   (t->index_slots_per_key & (t->index_slots_per_key - 1)))) ||
       (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
       t->dense_join_passes < 0 || t->dense_join_passes > 2 || t->join_aggregate < 0 ||
-      t->join_aggregate > 2 || t->pull_joins < 0 || t->pull_joins > 3)
+      t->join_aggregate > 2 || t->pull_joins < 0 || t->pull_joins > 3 || t->row_gather < 0 ||
+      t->row_gather > 3)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -2684,6 +2809,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->dense_join_passes) e->dense_join_passes = t->dense_join_passes;
   if (t->join_aggregate) e->join_aggregate = t->join_aggregate;
   if (t->pull_joins) e->pull_joins = t->pull_joins;
+  if (t->row_gather) e->row_gather = t->row_gather;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -2699,6 +2825,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->dense_join_passes = e->dense_join_passes;
   t->join_aggregate = e->join_aggregate;
   t->pull_joins = e->pull_joins;
+  t->row_gather = e->row_gather;
   return GDL_OK;
 }
 

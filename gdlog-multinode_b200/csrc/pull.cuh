@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
 // every join that writes the relation has a transposed output and nothing
 // reads its NEWT during the iteration, NEWT is only that transposed twin
 // (never folded): it is read transposed, tile by tile, and cleared.
-__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk, u32 *gt) {
+__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk, u32 *gt,
+                                                          u32 *dn) {
   __shared__ u32 s_t[256][9];
   __shared__ unsigned long long s_cnt[2];
   if (ctl_stop(a.ctl)) return;
@@ -229,6 +230,13 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
         n_newt += __popc(g[i]);
         any |= d[i] != 0u;
       }
+    }
+    if (dn) {
+      // DELTA's rows as they are, for row-gather joins (every word written)
+      uint4 *pn = reinterpret_cast<uint4 *>(dn + src);
+      pn[0] = make_uint4(d[0], d[1], d[2], d[3]);
+      pn[1] = make_uint4(d[4], d[5], d[6], d[7]);
+      moved += 32;
     }
     const bool tile_any = __syncthreads_or(any);
     if (tile_any) {
@@ -436,6 +444,215 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, u32 
   if ((tid & 31) == 0) prof_add(a.ctl, kPJoinMat, 4 * flushed);
   if (tid == 0) prof_add(a.ctl, kPJoinMat, 16 * keys + 8 * cand + 4 * row_words);
   if (launch_rec_finish(a.rec) && tid == 0) prof_add(a.ctl, kPJoinMat, 4ull * units * kPullUnit);
+}
+
+// ---------------------------------------------------------------------------
+// Row-gather joins.  The same joins as k_join_pull_bm, computed the other
+// way round: output column y (an inner column-1 value) is the union of the
+// outer's bitmap ROWS O[k] over the inner's in-edges (k, y):
+//     Out^T[y] = OR over k in inner^T[y] of O[k].
+// Its work is |inner| bitmap rows of 2^(dk-5) words, read coalesced,
+// whatever the number of candidate tuples (which the pull form expands one
+// shared-memory atomic each: 4-8x more work on same generation's dense
+// iterations).  It fits a small inner kept static through the LIE (an edge
+// relation): its in-edges are listed once per LIE (k_inv_*).  The output is
+// the transpose of the pull form's, so the two forms swap the roles of the
+// output's NEWT and its transposed twin.
+// ---------------------------------------------------------------------------
+constexpr int kRowsChunk = 8;      // in-edges per unit of work (a warp)
+constexpr int kRowsMinBits = 12;   // a bitmap row is at least 32 uint4 (one per lane)
+constexpr unsigned long long kRowsBudget = 256ull << 20;  // |inner| x row bytes, auto mode
+
+// In-edges of a sorted key list (k << 32 | y): counts per y.
+__global__ void __launch_bounds__(256) k_inv_count(const DArr *list, u32 *cnt, int dk, Ctl *ctl) {
+  const u64 n = list->n;
+  const u32 lim = 1u << dk;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u32 y = key_c1(list->ptr[i]);
+    if (y < lim && key_c0(list->ptr[i]) < lim)
+      atomicAdd(&cnt[y], 1u);
+    else
+      atomicOr(&ctl->oob, 8192u);
+  }
+}
+
+// Exclusive scan of the 2^dk counts into off[0..2^dk] (one block), and the
+// fill cursors (a copy of the offsets).
+__global__ void __launch_bounds__(1024) k_inv_scan(const u32 *cnt, u32 *off, u32 *cur, int dk) {
+  __shared__ u32 s_sum[32];
+  const u32 n = 1u << dk;
+  const u32 per = (n + blockDim.x - 1) / blockDim.x;
+  const u32 b = threadIdx.x * per;
+  u32 local = 0;
+  for (u32 i = 0; i < per && b + i < n; i++) local += cnt[b + i];
+  // block exclusive scan of `local`
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  u32 x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_sum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    u32 v = lane < (int)(blockDim.x / 32) ? s_sum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    s_sum[lane] = v;
+  }
+  __syncthreads();
+  u32 run = (w ? s_sum[w - 1] : 0) + x - local;
+  for (u32 i = 0; i < per && b + i < n; i++) {
+    const u32 c = cnt[b + i];  // read first: cur may be the count array
+    off[b + i] = run;
+    cur[b + i] = run;
+    run += c;
+  }
+  if (threadIdx.x == blockDim.x - 1) off[n] = s_sum[blockDim.x / 32 - 1];
+}
+
+// Scatter: the in-edges of y at [off[y], off[y+1]), each with its y (the
+// order inside a y does not matter: the gather ORs).
+__global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, u32 *ys,
+                                                  int dk) {
+  const u64 n = list->n;
+  const u32 lim = 1u << dk;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u64 kk = list->ptr[i];
+    const u32 y = key_c1(kk), k = key_c0(kk);
+    if (y >= lim || k >= lim) continue;
+    const u32 pos = atomicAdd(&cur[y], 1u);
+    keys[pos] = k;
+    ys[pos] = y;
+  }
+}
+
+struct RowsArgs {
+  JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record
+  const u32 *O;        // the outer's rows: DELTA (non-transposed copy) or a tmp NEWT
+  u32 *outer_clear;    // bitmap to clear if an empty inner zeroes a NEWT outer
+  const u32 *inv_off;  // in-edges of y: [inv_off[y], inv_off[y + 1])
+  const u32 *inv_keys;
+  const u32 *inv_ys;
+  u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
+  u8 *dirty;           // dirty map of dst, or null
+  int dk;
+};
+
+// One output row's words held by a warp: lane l holds uint4 number
+// j * 32 + l of the row (so each load instruction reads 512 contiguous
+// bytes).  V = 2^(dk-5) / 128 uint4 per lane.
+template <int V>
+__device__ __forceinline__ void rows_flush(const RowsArgs &a, u32 y, bool whole, uint4 *acc,
+                                           u64 &words_out) {
+  const int lane = threadIdx.x & 31;
+  const int rs = a.dk - 5;
+  uint4 *d = reinterpret_cast<uint4 *>(a.dst + ((u64)y << rs));
+#pragma unroll
+  for (int j = 0; j < V; j++) {
+    const uint4 v = acc[j];
+    if ((v.x | v.y | v.z | v.w) == 0u) continue;
+    const u32 q = (u32)j * 32 + lane;
+    if (whole) {
+      // this warp owns row y in this launch: plain read-OR-write
+      uint4 o = d[q];
+      o.x |= v.x;
+      o.y |= v.y;
+      o.z |= v.z;
+      o.w |= v.w;
+      d[q] = o;
+    } else {
+      u32 *w = reinterpret_cast<u32 *>(d + q);
+      if (v.x) asm volatile("red.global.or.b32 [%0], %1;" ::"l"(w + 0), "r"(v.x) : "memory");
+      if (v.y) asm volatile("red.global.or.b32 [%0], %1;" ::"l"(w + 1), "r"(v.y) : "memory");
+      if (v.z) asm volatile("red.global.or.b32 [%0], %1;" ::"l"(w + 2), "r"(v.z) : "memory");
+      if (v.w) asm volatile("red.global.or.b32 [%0], %1;" ::"l"(w + 3), "r"(v.w) : "memory");
+    }
+    if (a.dirty) a.dirty[(((u64)y << rs) + 4ull * q) / kBmChunkWords] = 1;
+    words_out += 4;
+  }
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
+  if (ctl_stop(a.j.ctl)) return;
+  if (eff_count(a.j.inner, a.j.inner_vis) == 0) {
+    // src/join.cu:42-45: an empty inner zeroes the outer's count
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (a.j.outer_vis)
+        *a.j.outer_vis = 0;
+      else
+        ((DArr *)a.j.outer)->n = 0;
+    }
+    if (a.outer_clear) {
+      uint4 *p = reinterpret_cast<uint4 *>(a.outer_clear);
+      const u64 n4 = (1ull << (2 * a.dk - 5)) / 4;
+      for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+           i += (u64)gridDim.x * blockDim.x)
+        p[i] = make_uint4(0, 0, 0, 0);
+    }
+    return;
+  }
+  // a DELTA outer zeroed earlier in the iteration reads as empty
+  if (a.j.outer_vis && eff_count(a.j.outer, a.j.outer_vis) == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int rs = a.dk - 5;
+  // the in-edges actually listed (k_inv_fill skips values outside the
+  // domain, which the fixpoint reports as an error)
+  const u32 n_edges = a.inv_off[1u << a.dk];
+  const u32 chunks = (n_edges + kRowsChunk - 1) / kRowsChunk;
+  u64 words_out = 0, edges = 0;
+  while (true) {
+    u32 c = 0;
+    if (lane == 0) c = atomicAdd(&a.j.rec->tile_ctr, 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= chunks) break;
+    const u32 i0 = c * kRowsChunk;
+    const u32 i1 = min(i0 + (u32)kRowsChunk, n_edges);
+    // this chunk's in-edges and their ys, one per lane
+    const u32 my_k = lane < (int)(i1 - i0) ? a.inv_keys[i0 + lane] : 0;
+    const u32 my_y = lane < (int)(i1 - i0) ? a.inv_ys[i0 + lane] : 0;
+    uint4 acc[V];
+#pragma unroll
+    for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
+    u32 cur_y = __shfl_sync(0xffffffffu, my_y, 0);
+    u32 seg0 = i0;
+    for (u32 i = i0; i < i1; i++) {
+      const u32 k = __shfl_sync(0xffffffffu, my_k, i - i0);
+      const u32 y = __shfl_sync(0xffffffffu, my_y, i - i0);
+      if (y != cur_y) {
+        const bool whole = seg0 == a.inv_off[cur_y] && i == a.inv_off[cur_y + 1];
+        rows_flush<V>(a, cur_y, whole, acc, words_out);
+#pragma unroll
+        for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
+        cur_y = y;
+        seg0 = i;
+      }
+      const uint4 *row = reinterpret_cast<const uint4 *>(a.O + ((u64)k << rs));
+#pragma unroll
+      for (int j = 0; j < V; j++) {
+        const uint4 v = row[j * 32 + lane];
+        acc[j].x |= v.x;
+        acc[j].y |= v.y;
+        acc[j].z |= v.z;
+        acc[j].w |= v.w;
+      }
+    }
+    const bool whole = seg0 == a.inv_off[cur_y] && i1 == a.inv_off[cur_y + 1];
+    rows_flush<V>(a, cur_y, whole, acc, words_out);
+    edges += i1 - i0;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) words_out += __shfl_xor_sync(0xffffffffu, words_out, o);
+  // algorithmic bytes: a row of the outer and an (edge, y) pair per
+  // in-edge, and each output word written (read and written back)
+  if (lane == 0)
+    prof_add(a.j.ctl, kPJoinMat, edges * ((4ull << rs) + 8) + 8 * words_out);
+  launch_rec_finish(a.j.rec);
 }
 
 // dst |= transpose(src), src cleared: the transposed output of the joins

@@ -61,7 +61,7 @@ class Tuning(C.Structure):
                 ("join_ctas_per_sm", C.c_int32), ("count_ctas_per_sm", C.c_int32),
                 ("index_slots_per_key", C.c_int32), ("dirty_min_log2_words", C.c_int32),
                 ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32),
-                ("pull_joins", C.c_int32)]
+                ("pull_joins", C.c_int32), ("row_gather", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -380,7 +380,9 @@ class Engine:
             elif dedup == "dense_push":  # bitmaps, every join in the push form
                 self.set_tuning(dedup="dense", pull_joins=1)
             elif dedup == "dense_pull":  # bitmaps, pull form wherever it applies
-                self.set_tuning(dedup="dense", pull_joins=3)
+                self.set_tuning(dedup="dense", pull_joins=3, row_gather=1)
+            elif dedup == "dense_rows":  # bitmaps, row-gather form wherever it applies
+                self.set_tuning(dedup="dense", pull_joins=3, row_gather=3)
             elif dedup == "dense_2pass":  # bitmaps, push joins as count + materialise passes
                 self.set_tuning(dedup="dense", dense_join_passes=2, pull_joins=1)
             elif dedup == "dense_agg":  # bitmaps, push joins with warp-aggregated bit-sets

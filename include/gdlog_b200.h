@@ -135,6 +135,11 @@ typedef struct gdl_tuning {
                                   row from the transposed outer) when ids
                                   reach 2^10 (default), 3 = pull form from
                                   2^8 ids */
+  int32_t row_gather;          /* those joins over a static inner when ids reach
+                                  2^12: 1 = off, 2 = gather the outer's bitmap
+                                  rows along the inner's in-edges when the
+                                  inner is small enough (|inner| x row bytes
+                                  <= 256 MB; default), 3 = whenever possible */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

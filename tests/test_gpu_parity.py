@@ -25,11 +25,13 @@ pytestmark = pytest.mark.gpu
 # bitmaps over the key domain (every workload here has a small domain, so
 # "dense" is what the engine picks by itself); bitmaps with every eligible
 # join in the pull form (gathered by output row) or every join in the push
-# form; bitmaps with dirty maps at every size (scans of listed dirty
+# form, or every eligible join gathered along its static inner's in-edges
+# (row-gather form); bitmaps with dirty maps at every size (scans of listed dirty
 # chunks), bitmaps with push joins as count + materialise passes instead of
 # one probe-and-expand pass, and bitmaps whose push joins combine a warp's
 # bits per word before the reduction.
-MODES = ["sort", "dense", "dense_pull", "dense_push", "dense_dirty", "dense_2pass", "dense_agg"]
+MODES = ["sort", "dense", "dense_pull", "dense_push", "dense_dirty", "dense_2pass", "dense_agg",
+         "dense_rows"]
 
 
 def summarize(r):

@@ -28,13 +28,17 @@ def summarize(r):
 
 
 def three_ways(prog, *args):
+    """The pull form, the push form and the oracle; the row-gather form
+    (gathered along a static inner's in-edges, from 2^12 ids) must give the
+    same as the pull form."""
     out = []
-    for mode in ("dense_pull", "dense_push"):
+    for mode in ("dense_pull", "dense_push", "dense_rows"):
         with Engine("gpu", dedup=mode) as g:
             out.append(summarize(prog(g, *args, sync=g.sync)))
     with Engine("oracle") as o:
         out.append(summarize(prog(o, *args)))
-    return out
+    assert out[2] == out[0]
+    return out[0], out[1], out[3]
 
 
 @pytest.mark.parametrize("scale,edges", [(8, 600), (12, 5000), (13, 12000), (16, 3000)])
@@ -62,10 +66,10 @@ def test_sg_scale14_pull_equals_push():
     """The default bench workload (R-MAT scale 14, 40,000 edges)."""
     e = W.rmat_edges(14, 40000, seed=14)
     out = []
-    for mode in ("dense_pull", "dense_push"):
+    for mode in ("dense_pull", "dense_push", "dense_rows", "dense"):
         with Engine("gpu", dedup=mode) as g:
             out.append(summarize(P.sg(g, e, sync=g.sync)))
-    assert out[0] == out[1]
+    assert out[0] == out[1] == out[2] == out[3]
     assert out[0]["sizes"]["sg"] == 38069132
 
 
@@ -80,13 +84,76 @@ def test_cspa_pull_matches_push_and_oracle(v, seed):
 
 def test_cspa_1000_pull_equals_push():
     """A larger CSPA (beyond the oracle's memory: value_alias grows with the
-    square of the variables): the two join forms agree."""
+    square of the variables): the join forms agree."""
     args = W.cspa_facts(1000, 2000, 750, seed=4)
     out = []
-    for mode in ("dense_pull", "dense_push"):
+    for mode in ("dense_pull", "dense_push", "dense_rows"):
         with Engine("gpu", dedup=mode) as g:
             out.append(summarize(P.cspa(g, *args, sync=g.sync)))
-    assert out[0] == out[1]
+    assert out[0] == out[1] == out[2]
+
+
+@pytest.mark.parametrize("scale,edges", [(12, 9000), (13, 20000), (15, 60000)])
+def test_sg_row_gather_matches_oracle(scale, edges):
+    """Both of SG's recursive joins in the row-gather form (a DELTA outer and
+    a tmp NEWT outer over the static edge relation), 2^12..2^15 ids."""
+    e = W.rmat_edges(scale, edges, seed=scale + 1)
+    with Engine("gpu", dedup="dense_rows") as g:
+        got = summarize(P.sg(g, e, sync=g.sync))
+    with Engine("gpu", dedup="dense_pull") as g:
+        pull = summarize(P.sg(g, e, sync=g.sync))
+    assert got == pull
+    if scale <= 13:
+        with Engine("oracle_bitset") as o:
+            assert got == summarize(P.sg(o, e))
+
+
+def rows_quirks(eng, sync=None):
+    """Row-gather joins at the reference's edges, over 2^13 ids: a DELTA
+    outer and a tmp NEWT outer over a static inner; the tmp NEWT also read
+    by a push join (its list); an empty static inner zeroing a DELTA outer
+    (src/join.cu:38-45) and another clearing a tmp NEWT outer."""
+    rng = np.random.default_rng(9)
+    a = eng.relation("a", index_flag=False)
+    c = eng.relation("c", index_flag=False)
+    e = eng.relation("e")
+    z = eng.relation("z")
+    t = eng.relation("t", index_flag=False, tmp_flag=True)
+    u = eng.relation("u", index_flag=False, tmp_flag=True)
+    eng.load(a, rng.integers(0, 6000, size=(2000, 2)).astype(np.uint64))
+    eng.load(c, rng.integers(0, 6000, size=(500, 2)).astype(np.uint64))
+    eng.load(e, rng.integers(0, 6000, size=(1500, 2)).astype(np.uint64))
+    eng.load(z, None)
+    eng.load(t, None)
+    eng.load(u, None)
+    lie = eng.lie()
+    lie.add_relations(e, True)
+    lie.add_relations(z, True)
+    lie.add_relations(a, False)
+    lie.add_relations(c, False)
+    lie.add_tmp_relation(t)
+    lie.add_tmp_relation(u)
+    lie.add_join(e, FULL, a, DELTA, t, (OUTER(1), INNER(1)))    # t(b, x) :- a(k, b), e(k, x)
+    lie.add_join(e, FULL, t, NEWT, a, (OUTER(1), INNER(1)))    # a(x, y) :- t(b, x), e(b, y)
+    lie.add_join(e, FULL, t, NEWT, c, (OUTER(0), INNER(1)))    # push form: t's list
+    lie.add_join(e, FULL, c, DELTA, u, (INNER(1), OUTER(1)))   # transposed output
+    lie.add_join(z, FULL, u, NEWT, a, (OUTER(1), INNER(1)))    # empty inner: u cleared
+    lie.add_join(z, FULL, c, DELTA, c, (OUTER(1), INNER(1)))   # empty inner: c's DELTA zeroed
+    lie.max_iteration = 5
+    it = lie.fixpoint()
+    return it, a.size(), a.digest(), c.size(), c.digest(), lie.trace().tolist()
+
+
+def test_row_gather_quirks_match_oracle():
+    got = []
+    for mode in ("dense_rows", "dense_pull", "dense_push"):
+        with Engine("gpu", dedup=mode) as g:
+            got.append(rows_quirks(g))
+    with Engine("oracle") as o:
+        want = rows_quirks(o)
+    assert got[0] == want
+    assert got[1] == want
+    assert got[2] == want
 
 
 def pull_quirks(eng, sync=None):
