@@ -780,6 +780,109 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 
 // Zero a NEWT bitmap in its dirty chunks (all of it without a dirty map)
 // and clear the dirty map.  One block per tile.
+// ---------------------------------------------------------------------------
+// One-pass listing of a square-domain bitmap (ids below 2^dk, rows of
+// 2^(dk-5) words) as its sorted key list: blocks take 2048-word tiles in
+// order, count them, take their output offset by decoupled look-back, and
+// write the tile's keys through a shared-memory window of kListStage keys,
+// so the stores are coalesced and no key needs a search.  Replaces the
+// count, scan and write passes for the lists written at the end of a LIE
+// (src/lie.cu:219-254: FULL flattened into a sorted array).
+// ---------------------------------------------------------------------------
+constexpr int kListStage = 4096;
+
+struct ListSmem {
+  u64 keys[kListStage];
+  u64 scan_tmp[kBmBlock / 32];
+  u64 base;
+  long long tile;
+};
+
+__global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, int rs, DArr *out,
+                                                      Lb lb, LaunchRec *rec, Ctl *ctl) {
+  __shared__ ListSmem sm;
+  if (ctl_stop(ctl)) return;
+  const u64 tiles = words / kBmTileWords;
+  const u32 gen = rec->gen;
+  const u64 row_mask = (1ull << rs) - 1;
+  u64 *dst = out->ptr;
+  const u64 cap = out->cap;
+  const int lane = threadIdx.x & 31;
+  u64 moved = 0;
+  while (true) {
+    const long long t = grab_tile(rec, &sm.tile);
+    if (t >= (long long)tiles) break;
+    const u64 w0 = (u64)t * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
+    u32 v[kBmWordsPerThread];
+    load8(bm + w0, v);
+    u32 c = 0;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) c += __popc(v[i]);
+    u64 tot;
+    const u64 ex = block_excl_scan<kBmBlock>((u64)c, sm.scan_tmp, &tot);
+    if (threadIdx.x < 32) {
+      u64 prefix = 0;
+      if (t == 0) {
+        if (lane == 0) lb_publish(lb, t, gen, true, tot);
+      } else {
+        if (lane == 0) lb_publish(lb, t, gen, false, tot);
+        prefix = lb_warp_prefix(lb, t, gen, ctl);
+        if (lane == 0) lb_publish(lb, t, gen, true, prefix + tot);
+      }
+      if (lane == 0) sm.base = prefix;
+    }
+    __syncthreads();
+    const u64 base = sm.base;
+    if ((u64)t == tiles - 1 && threadIdx.x == 0) {
+      // never publish more rows than the list holds (the host sized it
+      // from the bitmap's count; a mismatch is an error, reported)
+      const u64 total = base + tot;
+      out->n = total <= cap ? total : cap;
+      if (total > cap) atomicOr(&ctl->oob, 16384u);
+    }
+    moved += 4 * kBmWordsPerThread + 8 * (u64)c;
+    for (u64 r0 = 0; r0 < tot; r0 += kListStage) {
+      // this thread's keys at tile positions [ex, ex + c) that fall in the
+      // window [r0, r0 + kListStage)
+      if (c && ex < r0 + kListStage && ex + c > r0) {
+        u64 p = ex;
+#pragma unroll
+        for (int i = 0; i < kBmWordsPerThread; i++) {
+          u32 x = v[i];
+          if (!x) continue;
+          const u64 w = w0 + i;
+          const u64 kb = ((w >> rs) << 32) | ((w & row_mask) << 5);
+          const u32 n = __popc(x);
+          if (p + n <= r0 || p >= r0 + kListStage) {
+            p += n;
+            continue;
+          }
+          while (x) {
+            const int b = __ffs(x) - 1;
+            x &= x - 1;
+            if (p >= r0 && p < r0 + kListStage) sm.keys[p - r0] = kb + (u64)b;
+            p++;
+          }
+        }
+      }
+      __syncthreads();
+      const u64 m = min((u64)kListStage, tot - r0);
+      for (u64 i = threadIdx.x; i < m; i += kBmBlock) {
+        const u64 pos = base + r0 + i;
+        if (pos < cap)
+          dst[pos] = sm.keys[i];
+        else
+          atomicOr(&ctl->oob, 16384u);
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(0xffffffffu, moved, o);
+  if (lane == 0) prof_add(ctl, kPBitmap, moved);
+  launch_rec_finish(rec);
+}
+
 __device__ __forceinline__ void clear_newt_tiles(u32 *G, u8 *D, u64 words) {
   const u64 tiles = bm_tiles(words);
   for (u64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {

@@ -180,6 +180,8 @@ struct gdl_engine {
   // Dense scans: look-back state of the tile-count scan.
   Lb lb_bm{};
   u64 lb_bm_tiles = 0;
+  Lb lb_list{};  // k_bm_list: one look-back slot per 2048-word tile
+  u64 lb_list_tiles = 0;
   // Largest 2*bits domain kept as bitmaps (GDLOG_DENSE_MAX_BITS), and the
   // dedup path: 0 chosen by domain size, 1 always sort/merge, 2 always
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
@@ -211,7 +213,8 @@ struct gdl_engine {
   SegInfo *d_square_seg = nullptr;  // the one segment of the square domain
   u64 lb_cnt_tiles = 0, lb_nz_tiles = 0, lb_merge_tiles = 0;
   LaunchRec *recs = nullptr;  // [0] join count, [1] join mat, [2] merge, [3] copy,
-                              // [4] [5] bitmap scans, [6] pull join, [7] transpose
+                              // [4] [5] bitmap scans, [6] pull join, [7] transpose,
+                              // [8] bitmap listing
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
   u64 *d_u64 = nullptr;       // [4] small device scalars
   u32 *d_u32 = nullptr;       // [4]
@@ -652,6 +655,9 @@ struct Plan {
   // (inner column 1, outer column 1), or row-gather form with output
   // (outer column 1, inner column 1))
   std::vector<char> out_twin;
+  // per relation: DELTA is never read as a list, so the update step is one
+  // fused pass (k_bm_update_t) that writes DELTA as bitmaps only
+  std::vector<char> fused;
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -672,6 +678,7 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.rows.assign(L.ops.size(), 0);
   p.delta_n.assign(n, 0);
   p.out_twin.assign(L.ops.size(), 0);
+  p.fused.assign(n, 0);
   for (const OpHost &op : L.ops) {
     if (op.kind == 0 && op.outer_ver == GDL_DELTA) p.delta_list[op.outer] = 1;
     if (op.kind != 2 && op.inner_ver == GDL_DELTA) p.delta_list[op.inner] = 1;
@@ -689,26 +696,27 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
 }
 
 // The update step of relation r is one fused pass (pull.cuh, k_bm_update_t):
-// its DELTA is read only transposed and its FULL not as a list.
-bool fused_update(const Plan &p, int r) {
-  return p.delta_t[r] && !p.delta_list[r] && !p.full_list[r];
-}
+// its DELTA is read only as bitmaps (transposed by pull-form joins, as rows
+// by row-gather joins) and its FULL not as a list.
+bool fused_update(const Plan &p, int r) { return p.fused[r] != 0; }
 
 // Pull-form joins (pull.cuh), decided once the LIE's dense form is known: a
 // join into bitmaps over the square domain whose output is (outer column 1,
 // inner column 1), without predicate, over the DELTA of an update relation
 // or the NEWT of a tmp relation.  A NEWT read only by such joins needs no
 // list.
-// An update relation whose DELTA no op reads as a list then gets the
-// transposed DELTA too: its update step is the fused pass when FULL is not
-// read as a list either, and the transposed DELTA restores the list if the
-// loop ends with a DELTA left.
+// An update relation whose DELTA no op reads as a list and whose FULL is not
+// read as a list either has the fused update step; it keeps DELTA as the
+// bitmaps its readers need (transposed, rows), at least one of them, from
+// which the list is written if the loop ends with a DELTA left.
 void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   if (!L.dense || e->instances || L.dk < kPullMinBits) return;
   const bool pull_on = e->pull_joins == 3 || (e->pull_joins == 2 && L.dk >= kPullAutoBits);
-  for (int r : L.update)
-    if (!p.delta_list[r]) p.delta_t[r] = 1;
-  if (!pull_on) return;
+  if (!pull_on) {
+    for (int r : L.update)
+      if (!p.delta_list[r] && !p.full_list[r]) p.fused[r] = p.delta_n[r] = 1;
+    return;
+  }
   std::vector<char> is_update(e->rels.size(), 0), is_tmp(e->rels.size(), 0);
   for (int r : L.update) is_update[r] = 1;
   for (int r : L.tmps) is_tmp[r] = 1;
@@ -727,7 +735,6 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if ((fwd || rev) && outer_ok) {
       p.pull[oi] = 1;
       if (rev) p.pull_t[oi] = 1;
-      if (op.outer_ver == GDL_DELTA) p.delta_t[op.outer] = 1;
     } else if (op.outer_ver == GDL_NEWT) {
       p.newt_list[op.outer] = 1;
     } else if (op.outer_ver == GDL_DELTA) {
@@ -738,7 +745,7 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   for (size_t oi = 0; oi < L.ops.size(); oi++)
     if (L.ops[oi].kind == 1 && L.ops[oi].inner_ver == GDL_DELTA) p.delta_list[L.ops[oi].inner] = 1;
   for (int r : L.update)
-    if (!p.delta_list[r]) p.delta_t[r] = 1;
+    if (!p.delta_list[r] && !p.full_list[r]) p.fused[r] = 1;
   // Row-gather form (pull.cuh, k_join_rows_bm) for the pull-form joins over
   // a static inner FULL small enough that reading one outer row per in-edge
   // beats expanding candidates: |inner| rows of 2^(dk-5) words within
@@ -754,15 +761,20 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if (e->row_gather != 3 && bytes > kRowsBudget) continue;
     if (op.outer_ver == GDL_DELTA && !fused_update(p, op.outer)) continue;
     p.rows[oi] = 1;
-    if (op.outer_ver == GDL_DELTA) p.delta_n[op.outer] = 1;
   }
+  // Which orientations of DELTA and NEWT the joins read.  A fused update
+  // step keeps DELTA as rows when nothing reads it transposed (the record
+  // from which the list is written if max_iteration leaves a DELTA).
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
     const OpHost &op = L.ops[oi];
     if (!p.pull[oi]) continue;
     if (op.outer_ver == GDL_NEWT && !p.rows[oi]) p.newt_t[op.outer] = 1;
+    if (op.outer_ver == GDL_DELTA) (p.rows[oi] ? p.delta_n : p.delta_t)[op.outer] = 1;
     p.out_twin[oi] = p.pull_t[oi] != p.rows[oi];
     if (p.out_twin[oi]) p.out_t[op.out] = 1;
   }
+  for (int r : L.update)
+    if (p.fused[r] && !p.delta_t[r]) p.delta_n[r] = 1;
   // A relation written only by transposed-output joins, whose NEWT no op
   // reads and whose update step is the fused pass, keeps NEWT as the
   // transposed twin: no fold after each join, the update reads it.
@@ -1178,14 +1190,15 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       a.gated = 1;
       a.inst_delta = L.d_inst_delta;
       a.ex_a = kBmDelta;
-      if (plan.delta_list[r] || !plan.delta_t[r]) {
+      if (fused_update(plan, r) || (plan.delta_t[r] && !plan.delta_list[r])) {
+        // no op reads DELTA as a list (pull-form and row-gather joins read
+        // its bitmaps): only its size; the list is written from a bitmap
+        // if the loop ends with a DELTA left.  (k_bm_update_t stores
+        // through count_a: a fused relation always takes this branch.)
+        a.count_a = &R[r].delta_next.n;
+      } else {
         a.list_a = &R[r].delta_next;
         a.need_a = need_index(r, kNeedDelta);
-      } else {
-        // no op reads DELTA as a list (pull-form joins read its transposed
-        // bitmap): only its size; the list is written from the transposed
-        // bitmap if the loop ends with a DELTA left
-        a.count_a = &R[r].delta_next.n;
       }
       if (plan.full_list[r]) {
         a.ex_b = kBmUnion;
@@ -1198,7 +1211,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       a.gate_update = &L.d_lie->update[0];
       a.gate_n = (int)L.update.size();
       if (fused_update(plan, r)) {
-        // DELTA read only transposed, FULL not as a list: one fused pass
+        // DELTA read only as bitmaps, FULL not as a list: one fused pass
         // (pull.cuh, k_bm_update_t) after every count pass
         a.rec = &R[r].scan;
         a.lrec = &e->recs[5];
@@ -1224,7 +1237,8 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       const int r = (int)(a.rd - R);
       const u64 side = 1ull << (L.dk - kPullMinBits);
       PLAUNCH(kc, kPBitmap, k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                a, e->h[r].bmDT, L.dk, plan.fold_late[r] ? e->h[r].bmOT : nullptr,
+                                a, plan.delta_t[r] ? e->h[r].bmDT : nullptr, L.dk,
+                                plan.fold_late[r] ? e->h[r].bmOT : nullptr,
                                 plan.delta_n[r] ? e->h[r].bmDN : nullptr));
     }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
@@ -1927,8 +1941,17 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (any) {
       TRY(push(e));
       Counts kc;
+      if (!e->instances) TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles,
+                                       L.map.words / kBmTileWords + 2));
       for (int r : L.update) {
         if (!e->h[r].full_lazy) continue;
+        if (!e->instances) {
+          // square domain: one pass (k_bm_list)
+          k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
+              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
+              e->d_ctl);
+          continue;
+        }
         BmScanArgs a = scan_none(L.map);
         a.f = e->h[r].bmF;
         a.ex_b = kBmUnion;
@@ -1941,9 +1964,14 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     // DELTA lists that were not kept (read only transposed by pull-form
     // joins) and are not empty (max_iteration ended the loop): transposed
     // back into the (empty) NEWT bitmap and listed from it.
+    // (DELTA was only counted during the loop: a fused update step, or a
+    // DELTA read only transposed)
+    auto delta_unlisted = [&](int r) {
+      return plan.fused[r] || (plan.delta_t[r] && !plan.delta_list[r]);
+    };
     bool any_delta = false;
     for (int r : L.update)
-      if (plan.delta_t[r] && !plan.delta_list[r] && e->h[r].delta.n) {
+      if (delta_unlisted(r) && e->h[r].delta.n) {
         RelDev &h = e->h[r];
         TRY(ensure_arr(e, h.delta, h.delta.n, false));
         any_delta = true;
@@ -1951,21 +1979,37 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (any_delta) {
       TRY(push(e));
       Counts kc;
+      TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, L.map.words / kBmTileWords + 2));
       const u64 side = 1ull << (L.dk - kPullMinBits);
       for (int r : L.update) {
         const RelDev &h = e->h[r];
-        if (!(plan.delta_t[r] && !plan.delta_list[r] && h.delta.n)) continue;
-        TransposeArgs t{h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr, &e->recs[7], e->d_ctl};
-        k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
-        BmScanArgs a = scan_none(L.map);
-        a.g = h.bmG;
-        a.ex_b = kBmUnion;
-        a.list_b = &e->d_rels[r].delta;
-        launch_scan(e, a, r, &kc);
-        CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
+        if (!(delta_unlisted(r) && h.delta.n)) continue;
+        // DELTA's rows: kept as they are, or transposed back into the
+        // (empty) NEWT bitmap
+        const u32 *rows = h.bmDN;
+        if (!plan.delta_n[r]) {
+          TransposeArgs t{h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr, &e->recs[7], e->d_ctl};
+          k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
+          rows = h.bmG;
+        }
+        k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
+            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, e->lb_list, &e->recs[8],
+            e->d_ctl);
+        if (!plan.delta_n[r]) CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
       }
       CK(e, cudaGetLastError());
       TRY(pull(e));
+    }
+    {
+      // the listings' bounds checks
+      Ctl c3;
+      CK(e, cudaMemcpyAsync(&c3, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+      CK(e, cudaStreamSynchronize(e->s));
+      if (c3.timeout || c3.oob) {
+        e->broken = true;
+        return fail(e, GDL_E_TIMEOUT, "listing FULL/DELTA after the loop failed (timeout=%u oob=%u)",
+                    c3.timeout, c3.oob);
+      }
     }
     for (RelDev &h : e->h) {
       h.dense = h.full_lazy = 0;
@@ -2085,7 +2129,7 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
                                (int)(pull_acc_words(16) * 4))) ||
       bad(cudaMalloc(&e->d_rels, kMaxRels * sizeof(RelDev))) ||
       bad(cudaMalloc(&e->d_ctl, sizeof(Ctl))) || bad(cudaMallocHost(&e->h_ctl, sizeof(Ctl))) ||
-      bad(cudaMalloc(&e->recs, 8 * sizeof(LaunchRec))) ||
+      bad(cudaMalloc(&e->recs, 16 * sizeof(LaunchRec))) ||
       bad(cudaMalloc(&e->d_tmp, 4 * sizeof(DArr))) || bad(cudaMalloc(&e->d_u64, 4 * sizeof(u64))) ||
       bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) ||
       bad(cudaMalloc(&e->d_pull_count, sizeof(u64))) || bad(cudaEventCreate(&e->ev0)) ||
@@ -2094,7 +2138,7 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
       bad(cudaStreamCreateWithFlags(&e->cap_s, cudaStreamNonBlocking)) ||
       bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
       bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
-      bad(cudaMemsetAsync(e->recs, 0, 8 * sizeof(LaunchRec), e->s)) ||
+      bad(cudaMemsetAsync(e->recs, 0, 16 * sizeof(LaunchRec), e->s)) ||
       bad(cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s)) ||
       bad(cudaStreamSynchronize(e->s))) {
     gdl_engine_destroy(e);
@@ -2161,6 +2205,7 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->lb_nz.agg, (void *)e->lb_nz.inc, (void *)e->lb_merge.flag,
                   (void *)e->lb_merge.agg, (void *)e->lb_merge.inc, (void *)e->merge_parts,
                   (void *)e->lb_bm.flag, (void *)e->lb_bm.agg, (void *)e->lb_bm.inc,
+                  (void *)e->lb_list.flag, (void *)e->lb_list.agg, (void *)e->lb_list.inc,
                   (void *)e->d_segs,
                   (void *)e->d_tile_inst, (void *)e->d_square_seg,
                   (void *)e->recs,

@@ -174,6 +174,9 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
   const u64 tiles = per * per;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+  // the loop below may have no barrier (no transposed output): order the
+  // zeroing before any warp's atomicAdd into s_cnt
+  __syncthreads();
   u64 n_delta = 0, n_newt = 0, moved = 0;
   for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
     const u64 tr = t / per, tc = t % per;
@@ -238,23 +241,25 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
       pn[1] = make_uint4(d[4], d[5], d[6], d[7]);
       moved += 32;
     }
-    const bool tile_any = __syncthreads_or(any);
-    if (tile_any) {
+    if (dt) {  // (uniform over the launch)
+      const bool tile_any = __syncthreads_or(any);
+      if (tile_any) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(d[i], lane);
+        for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(d[i], lane);
+      }
+      __syncthreads();
+      uint4 *o = reinterpret_cast<uint4 *>(dt + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
+      if (tile_any) {
+        const u32 *q = s_t[threadIdx.x];
+        o[0] = make_uint4(q[0], q[1], q[2], q[3]);
+        o[1] = make_uint4(q[4], q[5], q[6], q[7]);
+      } else {
+        o[0] = make_uint4(0, 0, 0, 0);
+        o[1] = make_uint4(0, 0, 0, 0);
+      }
+      moved += 32;
+      __syncthreads();
     }
-    __syncthreads();
-    uint4 *o = reinterpret_cast<uint4 *>(dt + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
-    if (tile_any) {
-      const u32 *q = s_t[threadIdx.x];
-      o[0] = make_uint4(q[0], q[1], q[2], q[3]);
-      o[1] = make_uint4(q[4], q[5], q[6], q[7]);
-    } else {
-      o[0] = make_uint4(0, 0, 0, 0);
-      o[1] = make_uint4(0, 0, 0, 0);
-    }
-    moved += 32;
-    __syncthreads();
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
