@@ -791,6 +791,13 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kListStage = 4096;
 
+// Staging index of the q-th key of a window: within each group of 32 keys
+// the slot is XORed with the group number, so the lanes of a warp that
+// each write the j-th of their own consecutive keys (positions 32 apart in
+// dense tiles) hit different banks; the copy-out reads through the same
+// permutation.
+__device__ __forceinline__ u32 list_slot(u32 q) { return q ^ ((q >> 5) & 31u); }
+
 struct ListSmem {
   u64 keys[kListStage];
   u64 scan_tmp[kBmBlock / 32];
@@ -860,7 +867,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
           while (x) {
             const int b = __ffs(x) - 1;
             x &= x - 1;
-            if (p >= r0 && p < r0 + kListStage) sm.keys[p - r0] = kb + (u64)b;
+            if (p >= r0 && p < r0 + kListStage) sm.keys[list_slot((u32)(p - r0))] = kb + (u64)b;
             p++;
           }
         }
@@ -870,7 +877,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
       for (u64 i = threadIdx.x; i < m; i += kBmBlock) {
         const u64 pos = base + r0 + i;
         if (pos < cap)
-          dst[pos] = sm.keys[i];
+          dst[pos] = sm.keys[list_slot((u32)i)];
         else
           atomicOr(&ctl->oob, 16384u);
       }

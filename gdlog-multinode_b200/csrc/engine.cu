@@ -38,6 +38,8 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <map>
+#include <unordered_map>
 #include <chrono>
 #include <cstdarg>
 #include <cstddef>
@@ -140,6 +142,9 @@ struct RelHost {
   int bm_dk = 0;               // square domain bits of that bitmap (plain form)
   // In-edges of this relation's FULL (column-1 value -> column-0 values),
   // built at the start of a LIE whose row-gather joins read it as inner.
+  // A load committed on the device that the host mirror has not read back
+  // (its FULL count is known on the device only).
+  bool stale = false;
   u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr, *inv_ys = nullptr;
   u64 inv_cap = 0;
   int inv_dk = 0;
@@ -182,6 +187,10 @@ struct gdl_engine {
   u64 lb_bm_tiles = 0;
   Lb lb_list{};  // k_bm_list: one look-back slot per 2048-word tile
   u64 lb_list_tiles = 0;
+  // dalloc / dfree: bytes of each live block, and freed blocks for reuse
+  std::unordered_map<void *, size_t> alloc_size;
+  std::multimap<size_t, void *> spare;
+  size_t spare_bytes = 0;
   // Largest 2*bits domain kept as bitmaps (GDLOG_DENSE_MAX_BITS), and the
   // dedup path: 0 chosen by domain size, 1 always sort/merge, 2 always
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
@@ -217,7 +226,7 @@ struct gdl_engine {
                               // [8] bitmap listing
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
   u64 *d_u64 = nullptr;       // [4] small device scalars
-  u32 *d_u32 = nullptr;       // [4]
+  u32 *d_u32 = nullptr;       // [4]: [0] pack check, [3] device checks of async loads (sticky)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // Graph capture runs on its own stream, so that the engine stream can run
   // a loop's first iteration meanwhile; ev_first marks that iteration's end.
@@ -275,14 +284,51 @@ gdl_status fail(gdl_engine *e, gdl_status code, const char *fmt, ...) {
     if (_s != GDL_OK) return _s;   \
   } while (0)
 
+// Device blocks are recycled inside the engine: a freed block joins a spare
+// list (up to a quarter of the device's memory) and a later request of at
+// most its size, and at least half of it, takes it back, stream-ordered on
+// the engine stream like the pool's own reuse.  A program run after
+// gdl_engine_clear therefore makes no allocation calls once the first run
+// has sized everything.
 gdl_status dalloc(gdl_engine *e, void **p, size_t bytes) {
   *p = nullptr;
-  if (bytes == 0) bytes = 16;
-  CK(e, cudaMallocAsync(p, bytes, e->s));
+  bytes = round_up(std::max<size_t>(bytes, 16), 256);
+  auto it = e->spare.lower_bound(bytes);
+  if (it != e->spare.end() && it->first <= 2 * bytes) {
+    *p = it->second;
+    e->spare_bytes -= it->first;
+    e->alloc_size[*p] = it->first;
+    e->spare.erase(it);
+    return GDL_OK;
+  }
+  cudaError_t r = cudaMallocAsync(p, bytes, e->s);
+  if (r == cudaErrorMemoryAllocation && !e->spare.empty()) {
+    // give the spare blocks back and try once more
+    cudaGetLastError();
+    for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
+    e->spare.clear();
+    e->spare_bytes = 0;
+    r = cudaMallocAsync(p, bytes, e->s);
+  }
+  CK(e, r);
+  e->alloc_size[*p] = bytes;
   return GDL_OK;
 }
 void dfree(gdl_engine *e, void *p) {
-  if (p) cudaFreeAsync(p, e->s);
+  if (!p) return;
+  auto it = e->alloc_size.find(p);
+  if (it == e->alloc_size.end()) {
+    cudaFreeAsync(p, e->s);
+    return;
+  }
+  const size_t b = it->second;
+  e->alloc_size.erase(it);
+  if (e->spare_bytes + b > e->total_mem / 4) {
+    cudaFreeAsync(p, e->s);
+    return;
+  }
+  e->spare.emplace(b, p);
+  e->spare_bytes += b;
 }
 
 // Grow array `a` to hold at least `need` elements; keep its contents.
@@ -328,14 +374,31 @@ gdl_status ensure_index(gdl_engine *e, Index &ix, u64 cap) {
 
 gdl_status pull(gdl_engine *e) {
   if (e->rels.empty()) return GDL_OK;
+  u32 load_err = 0;
   CK(e, cudaMemcpyAsync(e->h.data(), e->d_rels, e->rels.size() * sizeof(RelDev),
                         cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaMemcpyAsync(&load_err, e->d_u32 + 3, sizeof load_err, cudaMemcpyDeviceToHost, e->s));
   CK(e, cudaStreamSynchronize(e->s));
   e->mirror_fresh = true;
+  for (RelHost &rh : e->rels) rh.stale = false;
+  if (load_err) {
+    e->broken = true;
+    return fail(e, GDL_E_TIMEOUT,
+                "a relation load failed its device checks (timeout %u, dropped write %u, "
+                "capacity %u)", load_err & 1u, (load_err >> 1) & 1u, (load_err >> 2) & 1u);
+  }
   return GDL_OK;
 }
 // pull() unless the mirror is known to equal the device table.
 gdl_status refresh(gdl_engine *e) { return e->mirror_fresh ? GDL_OK : pull(e); }
+// pull() only if relation r's mirror entry waits for a load's result.
+gdl_status refresh_rel(gdl_engine *e, int r) { return e->rels[r].stale ? pull(e) : GDL_OK; }
+// One relation's mirror entry to the device (the others stay as they are
+// there: an asynchronous load may have changed them).
+gdl_status push_rel(gdl_engine *e, int r) {
+  CK(e, cudaMemcpyAsync(e->d_rels + r, &e->h[r], sizeof(RelDev), cudaMemcpyHostToDevice, e->s));
+  return GDL_OK;
+}
 // The host mirror to the device, stream-ordered: a copy from pageable
 // memory is staged when the call returns, so the mirror may change at once.
 gdl_status push(gdl_engine *e) {
@@ -564,10 +627,14 @@ void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *
 
 u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e->sort_buf : buf0; }
 
-// FULL := unique(sort(keys[0..n))) for a load; DELTA/NEWT cleared.
+// FULL := unique(sort(keys[0..n))) for a load; DELTA/NEWT cleared.  The
+// load is committed on the device (k_load_commit) without a round trip: the
+// host mirror of this relation is marked stale and read back at the next
+// point that needs it, where the load's device checks are reported too.
+// Only this relation's entry is written to the device table.
 gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   RelHost &rh = e->rels[rel];
-  TRY(refresh(e));
+  TRY(refresh_rel(e, rel));
   RelDev &r = e->h[rel];
   rh.bm_valid = false;
   rh.full_resident = false;
@@ -594,9 +661,8 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     TRY(ensure_scratch(e));
     CK(e, cudaMemcpyAsync(r.newt.ptr, keys_dev, n * sizeof(u64), cudaMemcpyDeviceToDevice, e->s));
     r.newt.n = n;
-    TRY(push(e));
+    TRY(push_rel(e, rel));
     TRY(reset_ctl(e));
-    e->mirror_fresh = false;
     Counts kc;
     launch_sort(e, &e->d_rels[rel].newt, r.newt.ptr, r.newt.cap, &kc);
     MergeArgs m;
@@ -615,23 +681,18 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     m.rel = rel;
     k_merge_partition<<<grid_for(e, n / kMergeTile + 2, 256, 8), 256, 0, e->s>>>(m);
     k_merge_diff<<<grid_for(e, n, kMergeTile, 4), kMergeBlock, kMergeSmemBytes, e->s>>>(m);
+    k_load_commit<<<1, 32, 0, e->s>>>(&e->d_rels[rel], e->d_ctl, e->d_u32 + 3);
     CK(e, cudaGetLastError());
-    // the table and the control block in one round trip
-    Ctl c2;
-    CK(e, cudaMemcpyAsync(e->h.data(), e->d_rels, e->rels.size() * sizeof(RelDev),
-                          cudaMemcpyDeviceToHost, e->s));
-    CK(e, cudaMemcpyAsync(&c2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
-    CK(e, cudaStreamSynchronize(e->s));
-    e->mirror_fresh = true;
-    if (c2.timeout || c2.oob || c2.overflow)
-      return fail(e, GDL_E_TIMEOUT, "load of %s: device check failed (timeout=%u oob=%u overflow=%u)",
-                  rh.name.c_str(), c2.timeout, c2.oob, c2.overflow);
+    // the mirror as the device now has it, but for FULL's count
     std::swap(r.full, r.full_next);
     r.newt.n = 0;
     r.delta_next.n = 0;
     r.c_newt_n = 0;
+    rh.stale = true;
+    e->mirror_fresh = false;
+    return GDL_OK;
   }
-  TRY(push(e));
+  TRY(push_rel(e, rel));
   return GDL_OK;
 }
 
@@ -2139,6 +2200,7 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
       bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
       bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
       bad(cudaMemsetAsync(e->recs, 0, 16 * sizeof(LaunchRec), e->s)) ||
+      bad(cudaMemsetAsync(e->d_u32, 0, 4 * sizeof(u32), e->s)) ||
       bad(cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s)) ||
       bad(cudaStreamSynchronize(e->s))) {
     gdl_engine_destroy(e);
@@ -2154,27 +2216,26 @@ static void release_program(gdl_engine *e) {
   for (size_t i = 0; i < e->rels.size(); i++) {
     RelDev &r = e->h[i];
     for (DArr *a : {&r.full, &r.full_next, &r.delta, &r.delta_next, &r.newt})
-      if (a->ptr) cudaFreeAsync(a->ptr, e->s);
+      dfree(e, a->ptr);
     for (Index *x : {&r.full_idx, &r.full_idx_next, &r.delta_idx, &r.delta_idx_next})
-      if (x->slots) cudaFreeAsync(x->slots, e->s);
+      dfree(e, x->slots);
     for (u32 *bm : {r.bmF, r.bmG, r.bmDT, r.bmGT, r.bmOT, r.bmDN})
-      if (bm) cudaFreeAsync(bm, e->s);
-    if (r.bmD) cudaFreeAsync(r.bmD, e->s);
-    if (r.tile_prefix) cudaFreeAsync(r.tile_prefix, e->s);
+      dfree(e, bm);
+    dfree(e, r.bmD);
+    dfree(e, r.tile_prefix);
     const RelHost &rh = e->rels[i];
     for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_keys, rh.inv_ys})
-      if (q) cudaFreeAsync(q, e->s);
-    if (e->rels[i].raw && !e->rels[i].raw_is_full) cudaFreeAsync(e->rels[i].raw, e->s);
+      dfree(e, q);
+    if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
   }
   for (LieHost &L : e->lies) {
     if (L.gexec) cudaGraphExecDestroy(L.gexec);
     // stream-ordered frees (a cudaFree would wait for the whole device)
     for (void *p : {(void *)L.d_trace, (void *)L.d_lie, (void *)L.d_joinrec})
-      if (p) cudaFreeAsync(p, e->s);
-    if (L.d_inst_delta) cudaFreeAsync(L.d_inst_delta, e->s);
-    if (L.d_inst_last) cudaFreeAsync(L.d_inst_last, e->s);
+      dfree(e, p);
+    dfree(e, L.d_inst_delta);
+    dfree(e, L.d_inst_last);
   }
-  cudaStreamSynchronize(e->s);
   e->rels.clear();
   e->h.clear();
   e->lies.clear();
@@ -2186,10 +2247,11 @@ gdl_status gdl_engine_clear(gdl_engine *e) {
   if (!e) return GDL_E_INVALID;
   cudaSetDevice(e->device);
   if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
+  // (no LIE graph may be running while its executable is destroyed)
   CK(e, cudaStreamSynchronize(e->s));
   release_program(e);
+  // everything after this is stream-ordered behind the blocks released
   CK(e, cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s));
-  CK(e, cudaStreamSynchronize(e->s));
   return GDL_OK;
 }
 
@@ -2198,6 +2260,9 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   cudaSetDevice(e->device);
   if (e->s) cudaStreamSynchronize(e->s);
   release_program(e);
+  for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
+  e->spare.clear();
+  if (e->s) cudaStreamSynchronize(e->s);
   for (void *p : {(void *)e->sort_buf, (void *)e->sort_offsets, (void *)e->sort_counters,
                   (void *)e->sort_status, (void *)e->crow_off, (void *)e->crow_key,
                   (void *)e->crow_start, (void *)e->crow_len, (void *)e->lb_cnt.flag,
@@ -2255,9 +2320,7 @@ gdl_status gdl_relation_create(gdl_engine *e, const char *name, int32_t arity, i
   d.full_vis = d.delta_vis = d.w_full_vis = d.w_delta_vis = 1;
   e->h.push_back(d);
   *out = (int32_t)e->rels.size() - 1;
-  TRY(refresh(e));  // keep the mirror coherent, then write the new entry
-  e->h.back() = d;
-  TRY(push(e));
+  TRY(push_rel(e, *out));  // the new entry only (loads may be in flight)
   return GDL_OK;
 }
 
@@ -2305,14 +2368,22 @@ static gdl_status load_common(gdl_engine *e, int32_t rel, const uint64_t *rows, 
     e->max_value = std::max(e->max_value, m01);
     e->kbits = std::max(e->kbits, bits_for(e->max_value));
     gdl_status s = load_keys(e, rel, dk, n);
-    CK(e, cudaStreamSynchronize(e->s));
-    dfree(e, dk);
+    dfree(e, dk);  // stream-ordered behind the load
     return s;
   }
   u64 *d_rows = nullptr, *d_keys = nullptr;
+  u64 maxv = 0;
+  u32 badv = 0;
   if (on_device) {
     d_rows = (u64 *)rows;
   } else {
+    // host rows: the largest value and the range check on the host, so the
+    // load needs no round trip
+    u64 m = 0;
+    for (u64 i = 0; i < 2 * n; i++) m = std::max<u64>(m, rows[i]);
+    maxv = m;
+    badv = (m >> 32) != 0;
+    if (badv) return fail(e, GDL_E_UNSUPPORTED, "column values must be below 2^32");
     TRY(dalloc(e, (void **)&d_rows, n * 2 * sizeof(u64)));
     CK(e, cudaMemcpyAsync(d_rows, rows, n * 2 * sizeof(u64), cudaMemcpyHostToDevice, e->s));
   }
@@ -2321,11 +2392,11 @@ static gdl_status load_common(gdl_engine *e, int32_t rel, const uint64_t *rows, 
   CK(e, cudaMemsetAsync(e->d_u32, 0, sizeof(u32), e->s));
   k_pack_rows<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(d_rows, n, d_keys, e->d_u64, e->d_u32);
   CK(e, cudaGetLastError());
-  u64 maxv = 0;
-  u32 badv = 0;
-  CK(e, cudaMemcpyAsync(&maxv, e->d_u64, sizeof maxv, cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaMemcpyAsync(&badv, e->d_u32, sizeof badv, cudaMemcpyDeviceToHost, e->s));
-  CK(e, cudaStreamSynchronize(e->s));
+  if (on_device) {
+    CK(e, cudaMemcpyAsync(&maxv, e->d_u64, sizeof maxv, cudaMemcpyDeviceToHost, e->s));
+    CK(e, cudaMemcpyAsync(&badv, e->d_u32, sizeof badv, cudaMemcpyDeviceToHost, e->s));
+    CK(e, cudaStreamSynchronize(e->s));
+  }
   if (!on_device) dfree(e, d_rows);
   if (badv) {
     dfree(e, d_keys);

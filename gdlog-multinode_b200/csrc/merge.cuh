@@ -255,4 +255,23 @@ __global__ void __launch_bounds__(kMergeBlock) k_merge_diff(MergeArgs m) {
 
 constexpr size_t kMergeSmemBytes = sizeof(MergeSmem);
 
+// Commit of a load (the end of load_relation, src/relation.cu:815-838):
+// FULL' becomes FULL, NEWT and the merge's DELTA output are emptied.  A
+// failed device check is kept in a sticky word instead, for the host to
+// report at its next read of the relation table.
+__global__ void k_load_commit(RelDev *r, const Ctl *ctl, u32 *err) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const u32 bad = (ctl->timeout ? 1u : 0u) | (ctl->oob ? 2u : 0u) | (ctl->overflow ? 4u : 0u);
+  if (bad) {
+    atomicOr(err, bad);
+    return;
+  }
+  const DArr t = r->full;
+  r->full = r->full_next;
+  r->full_next = t;
+  r->newt.n = 0;
+  r->delta_next.n = 0;
+  r->c_newt_n = 0;
+}
+
 }  // namespace gdl
