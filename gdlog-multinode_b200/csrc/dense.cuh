@@ -784,23 +784,28 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 // One-pass listing of a square-domain bitmap (ids below 2^dk, rows of
 // 2^(dk-5) words) as its sorted key list: blocks take 2048-word tiles in
 // order, count them, take their output offset by decoupled look-back, and
-// write the tile's keys through a shared-memory window of kListStage keys,
-// so the stores are coalesced and no key needs a search.  Replaces the
-// count, scan and write passes for the lists written at the end of a LIE
-// (src/lie.cu:219-254: FULL flattened into a sorted array).
+// write the tile's keys through a shared-memory window, so the stores are
+// coalesced and no key needs a search.  Replaces the count, scan and write
+// passes for the lists written at the end of a LIE (src/lie.cu:219-254:
+// FULL flattened into a sorted array).
+//
+// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i), so
+// in every window each thread expands at most one word, 32 keys, and all
+// threads share the work of dense tiles.
 // ---------------------------------------------------------------------------
 constexpr int kListStage = 4096;
 
-// Staging index of the q-th key of a window: within each group of 32 keys
-// the slot is XORed with the group number, so the lanes of a warp that
-// each write the j-th of their own consecutive keys (positions 32 apart in
-// dense tiles) hit different banks; the copy-out reads through the same
+// Staging slot of the q-th key of a window: within each group of 32 keys
+// the slot is XORed with the group number, so that lanes whose keys are 32
+// apart hit different banks; the copy-out reads through the same
 // permutation.
 __device__ __forceinline__ u32 list_slot(u32 q) { return q ^ ((q >> 5) & 31u); }
 
 struct ListSmem {
   u64 keys[kListStage];
-  u64 scan_tmp[kBmBlock / 32];
+  u32 wtot[kBmWordsPerThread][kBmBlock / 32];  // per segment: warp totals, then offsets
+  u32 seg_tot[kBmWordsPerThread];
+  u32 seg_off[kBmWordsPerThread];
   u64 base;
   long long tile;
 };
@@ -814,19 +819,41 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
   const u64 row_mask = (1ull << rs) - 1;
   u64 *dst = out->ptr;
   const u64 cap = out->cap;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 moved = 0;
   while (true) {
     const long long t = grab_tile(rec, &sm.tile);
     if (t >= (long long)tiles) break;
-    const u64 w0 = (u64)t * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
-    u32 v[kBmWordsPerThread];
-    load8(bm + w0, v);
-    u32 c = 0;
+    const u64 w0 = (u64)t * kBmTileWords;
+    u32 v[kBmWordsPerThread], ex[kBmWordsPerThread];
 #pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) c += __popc(v[i]);
-    u64 tot;
-    const u64 ex = block_excl_scan<kBmBlock>((u64)c, sm.scan_tmp, &tot);
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      v[i] = bm[w0 + (u64)i * kBmBlock + threadIdx.x];
+      const u32 c = __popc(v[i]);
+      u32 x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      ex[i] = x - c;
+      if (lane == 31) sm.wtot[i][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kBmWordsPerThread) {
+      // per segment: exclusive warp offsets and the segment's total
+      u32 acc = 0;
+      for (int w = 0; w < kBmBlock / 32; w++) {
+        const u32 x = sm.wtot[threadIdx.x][w];
+        sm.wtot[threadIdx.x][w] = acc;
+        acc += x;
+      }
+      sm.seg_tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    u32 tot = 0;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) tot += sm.seg_tot[i];
     if (threadIdx.x < 32) {
       u64 prefix = 0;
       if (t == 0) {
@@ -836,7 +863,14 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
         prefix = lb_warp_prefix(lb, t, gen, ctl);
         if (lane == 0) lb_publish(lb, t, gen, true, prefix + tot);
       }
-      if (lane == 0) sm.base = prefix;
+      if (lane == 0) {
+        sm.base = prefix;
+        u32 a = 0;
+        for (int i = 0; i < kBmWordsPerThread; i++) {
+          sm.seg_off[i] = a;
+          a += sm.seg_tot[i];
+        }
+      }
     }
     __syncthreads();
     const u64 base = sm.base;
@@ -847,41 +881,37 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
       out->n = total <= cap ? total : cap;
       if (total > cap) atomicOr(&ctl->oob, 16384u);
     }
-    moved += 4 * kBmWordsPerThread + 8 * (u64)c;
-    for (u64 r0 = 0; r0 < tot; r0 += kListStage) {
-      // this thread's keys at tile positions [ex, ex + c) that fall in the
-      // window [r0, r0 + kListStage)
-      if (c && ex < r0 + kListStage && ex + c > r0) {
-        u64 p = ex;
-#pragma unroll
-        for (int i = 0; i < kBmWordsPerThread; i++) {
-          u32 x = v[i];
-          if (!x) continue;
-          const u64 w = w0 + i;
-          const u64 kb = ((w >> rs) << 32) | ((w & row_mask) << 5);
-          const u32 n = __popc(x);
-          if (p + n <= r0 || p >= r0 + kListStage) {
-            p += n;
-            continue;
-          }
+    moved += 4 * kBmWordsPerThread + 8 * (u64)(threadIdx.x == 0 ? tot : 0);
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u32 st = sm.seg_tot[i];  // block-uniform
+      if (st == 0) continue;
+      const u32 so = sm.seg_off[i];
+      const u32 p0 = sm.wtot[i][warp] + ex[i];  // this word's first key in the segment
+      const u64 w = w0 + (u64)i * kBmBlock + threadIdx.x;
+      const u64 kb = ((w >> rs) << 32) | ((w & row_mask) << 5);
+      for (u32 r0 = 0; r0 < st; r0 += kListStage) {
+        u32 x = v[i];
+        u32 p = p0;
+        const u32 n = __popc(x);
+        if (x && p < r0 + kListStage && p + n > r0) {
           while (x) {
             const int b = __ffs(x) - 1;
             x &= x - 1;
-            if (p >= r0 && p < r0 + kListStage) sm.keys[list_slot((u32)(p - r0))] = kb + (u64)b;
+            if (p >= r0 && p < r0 + kListStage) sm.keys[list_slot(p - r0)] = kb + (u64)b;
             p++;
           }
         }
+        __syncthreads();
+        const u32 m = min((u32)kListStage, st - r0);
+        for (u32 j = threadIdx.x; j < m; j += kBmBlock) {
+          const u64 pos = base + so + r0 + j;
+          if (pos < cap)
+            dst[pos] = sm.keys[list_slot(j)];
+          else
+            atomicOr(&ctl->oob, 16384u);
+        }
+        __syncthreads();
       }
-      __syncthreads();
-      const u64 m = min((u64)kListStage, tot - r0);
-      for (u64 i = threadIdx.x; i < m; i += kBmBlock) {
-        const u64 pos = base + r0 + i;
-        if (pos < cap)
-          dst[pos] = sm.keys[list_slot((u32)i)];
-        else
-          atomicOr(&ctl->oob, 16384u);
-      }
-      __syncthreads();
     }
   }
 #pragma unroll

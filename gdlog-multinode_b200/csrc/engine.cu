@@ -146,6 +146,8 @@ struct RelHost {
   // (its FULL count is known on the device only).
   bool stale = false;
   u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr, *inv_ys = nullptr;
+  u32 *inv_poff = nullptr;   // pieces of work per y, then their offsets (2^dk + 1)
+  uint2 *inv_pieces = nullptr;
   u64 inv_cap = 0;
   int inv_dk = 0;
 };
@@ -927,7 +929,8 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
 // host opens with a k_begin before each launch and whose k_commit opens
 // the next iteration; otherwise the iteration opens itself.
 void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
-  const int g = (int)e->sms * 8;
+  // one resident wave (the pieces are taken from a counter)
+  const int g = (int)e->sms * (ra.dk >= 16 ? 2 : 4);
   switch (ra.dk) {
     case 12: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<1><<<g, 256, 0, e->s>>>(ra)); break;
     case 13: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<2><<<g, 256, 0, e->s>>>(ra)); break;
@@ -942,23 +945,22 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   RelHost &rh = e->rels[r];
   const u64 n = e->h[r].full.n;
   const u32 ids = 1u << dk;
-  if (rh.inv_dk != dk) {
-    for (u32 **q : {&rh.inv_off, &rh.inv_cur}) {
+  if (rh.inv_dk != dk || rh.inv_cap < std::max<u64>(n, 1)) {
+    for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_poff, &rh.inv_keys, &rh.inv_ys}) {
       dfree(e, *q);
       *q = nullptr;
     }
+    dfree(e, rh.inv_pieces);
+    rh.inv_pieces = nullptr;
+    rh.inv_cap = std::max<u64>(n, 1);
+    rh.inv_dk = dk;
     TRY(dalloc(e, (void **)&rh.inv_off, (ids + 1) * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_cur, ids * sizeof(u32)));
-    rh.inv_dk = dk;
-  }
-  if (rh.inv_cap < std::max<u64>(n, 1)) {
-    for (u32 **q : {&rh.inv_keys, &rh.inv_ys}) {
-      dfree(e, *q);
-      *q = nullptr;
-    }
-    rh.inv_cap = std::max<u64>(n, 1);
+    TRY(dalloc(e, (void **)&rh.inv_poff, (ids + 1) * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_keys, rh.inv_cap * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_ys, rh.inv_cap * sizeof(u32)));
+    // pieces: at most one per in-edge, and one per y
+    TRY(dalloc(e, (void **)&rh.inv_pieces, (rh.inv_cap + ids) * sizeof(uint2)));
   }
   CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
   const DArr *list = &e->d_rels[r].full;
@@ -966,6 +968,11 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   k_inv_scan<<<1, 1024, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
   k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
                                                        dk);
+  // the pieces of work: counts per y (into inv_cur), offsets, pieces
+  k_inv_piece_count<<<grid_for(e, ids, 256, 8), 256, 0, e->s>>>(rh.inv_off, rh.inv_cur, dk);
+  k_inv_scan<<<1, 1024, 0, e->s>>>(rh.inv_cur, rh.inv_poff, rh.inv_cur, dk);
+  k_inv_piece_fill<<<grid_for(e, ids, 256, 8), 256, 0, e->s>>>(rh.inv_off, rh.inv_poff,
+                                                               rh.inv_pieces, dk);
   CK(e, cudaGetLastError());
   return GDL_OK;
 }
@@ -1101,6 +1108,8 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         ra.inv_off = ih.inv_off;
         ra.inv_keys = ih.inv_keys;
         ra.inv_ys = ih.inv_ys;
+        ra.pieces_off = ih.inv_poff;
+        ra.pieces = ih.inv_pieces;
         const RelDev &out = e->h[op.out];
         ra.dst = plan.out_twin[oi] ? out.bmOT : out.bmG;
         ra.dirty = plan.out_twin[oi] ? nullptr : out.dirty;
@@ -2224,8 +2233,9 @@ static void release_program(gdl_engine *e) {
     dfree(e, r.bmD);
     dfree(e, r.tile_prefix);
     const RelHost &rh = e->rels[i];
-    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_keys, rh.inv_ys})
+    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_poff, rh.inv_keys, rh.inv_ys})
       dfree(e, q);
+    dfree(e, rh.inv_pieces);
     if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
   }
   for (LieHost &L : e->lies) {

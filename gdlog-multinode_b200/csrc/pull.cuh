@@ -464,7 +464,6 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, u32 
 // the transpose of the pull form's, so the two forms swap the roles of the
 // output's NEWT and its transposed twin.
 // ---------------------------------------------------------------------------
-constexpr int kRowsChunk = 8;      // in-edges per unit of work (a warp)
 constexpr int kRowsMinBits = 12;   // a bitmap row is at least 32 uint4 (one per lane)
 constexpr unsigned long long kRowsBudget = 256ull << 20;  // |inner| x row bytes, auto mode
 
@@ -536,6 +535,31 @@ __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u3
   }
 }
 
+// Units of work of the row-gather join: the in-edges of one y, cut into
+// pieces of at most kRowsPiece (a y with more in-edges than that is shared
+// by several warps, which OR their parts into the output row).  First the
+// number of pieces per y, then (after k_inv_scan of those counts) the
+// pieces themselves as (first edge, end edge).
+constexpr u32 kRowsPiece = 32;
+
+__global__ void __launch_bounds__(256) k_inv_piece_count(const u32 *off, u32 *cnt, int dk) {
+  const u32 n = 1u << dk;
+  for (u32 y = blockIdx.x * blockDim.x + threadIdx.x; y < n; y += gridDim.x * blockDim.x) {
+    const u32 d = off[y + 1] - off[y];
+    cnt[y] = (d + kRowsPiece - 1) / kRowsPiece;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_inv_piece_fill(const u32 *off, const u32 *pieces_off,
+                                                        uint2 *pieces, int dk) {
+  const u32 n = 1u << dk;
+  for (u32 y = blockIdx.x * blockDim.x + threadIdx.x; y < n; y += gridDim.x * blockDim.x) {
+    const u32 s = off[y], e = off[y + 1];
+    u32 at = pieces_off[y];
+    for (u32 i = s; i < e; i += kRowsPiece) pieces[at++] = make_uint2(i, min(i + kRowsPiece, e));
+  }
+}
+
 struct RowsArgs {
   JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record
   const u32 *O;        // the outer's rows: DELTA (non-transposed copy) or a tmp NEWT
@@ -543,6 +567,8 @@ struct RowsArgs {
   const u32 *inv_off;  // in-edges of y: [inv_off[y], inv_off[y + 1])
   const u32 *inv_keys;
   const u32 *inv_ys;
+  const u32 *pieces_off;  // pieces_off[2^dk]: the number of pieces
+  const uint2 *pieces;
   u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
   u8 *dirty;           // dirty map of dst, or null
   int dk;
@@ -583,6 +609,19 @@ __device__ __forceinline__ void rows_flush(const RowsArgs &a, u32 y, bool whole,
 }
 
 template <int V>
+__device__ __forceinline__ void rows_or(uint4 *acc, const u32 *O, u32 k, int rs, int lane) {
+  const uint4 *row = reinterpret_cast<const uint4 *>(O + ((u64)k << rs));
+#pragma unroll
+  for (int j = 0; j < V; j++) {
+    const uint4 v = row[j * 32 + lane];
+    acc[j].x |= v.x;
+    acc[j].y |= v.y;
+    acc[j].z |= v.z;
+    acc[j].w |= v.w;
+  }
+}
+
+template <int V>
 __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   if (ctl_stop(a.j.ctl)) return;
   if (eff_count(a.j.inner, a.j.inner_vis) == 0) {
@@ -606,50 +645,45 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   if (a.j.outer_vis && eff_count(a.j.outer, a.j.outer_vis) == 0) return;
   const int lane = threadIdx.x & 31;
   const int rs = a.dk - 5;
-  // the in-edges actually listed (k_inv_fill skips values outside the
-  // domain, which the fixpoint reports as an error)
-  const u32 n_edges = a.inv_off[1u << a.dk];
-  const u32 chunks = (n_edges + kRowsChunk - 1) / kRowsChunk;
+  // the pieces actually built (values outside the domain are skipped by
+  // k_inv_fill and reported by the fixpoint)
+  const u32 n_pieces = a.pieces_off[1u << a.dk];
   u64 words_out = 0, edges = 0;
   while (true) {
     u32 c = 0;
     if (lane == 0) c = atomicAdd(&a.j.rec->tile_ctr, 1u);
     c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= chunks) break;
-    const u32 i0 = c * kRowsChunk;
-    const u32 i1 = min(i0 + (u32)kRowsChunk, n_edges);
-    // this chunk's in-edges and their ys, one per lane
-    const u32 my_k = lane < (int)(i1 - i0) ? a.inv_keys[i0 + lane] : 0;
-    const u32 my_y = lane < (int)(i1 - i0) ? a.inv_ys[i0 + lane] : 0;
+    if (c >= n_pieces) break;
+    const uint2 pc = a.pieces[c];
+    const u32 y = a.inv_ys[pc.x];
     uint4 acc[V];
 #pragma unroll
     for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
-    u32 cur_y = __shfl_sync(0xffffffffu, my_y, 0);
-    u32 seg0 = i0;
-    for (u32 i = i0; i < i1; i++) {
-      const u32 k = __shfl_sync(0xffffffffu, my_k, i - i0);
-      const u32 y = __shfl_sync(0xffffffffu, my_y, i - i0);
-      if (y != cur_y) {
-        const bool whole = seg0 == a.inv_off[cur_y] && i == a.inv_off[cur_y + 1];
-        rows_flush<V>(a, cur_y, whole, acc, words_out);
+    // this piece's keys, one per lane; two rows in flight per step
+    const u32 m = pc.y - pc.x;
+    const u32 my_k = lane < (int)m ? a.inv_keys[pc.x + lane] : 0;
+    u32 i = 0;
+    for (; i + 1 < m; i += 2) {
+      const u32 k0 = __shfl_sync(0xffffffffu, my_k, i);
+      const u32 k1 = __shfl_sync(0xffffffffu, my_k, i + 1);
+      uint4 b[V];
 #pragma unroll
-        for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
-        cur_y = y;
-        seg0 = i;
-      }
-      const uint4 *row = reinterpret_cast<const uint4 *>(a.O + ((u64)k << rs));
+      for (int j = 0; j < V; j++) b[j] = make_uint4(0, 0, 0, 0);
+      rows_or<V>(acc, a.O, k0, rs, lane);
+      rows_or<V>(b, a.O, k1, rs, lane);
 #pragma unroll
       for (int j = 0; j < V; j++) {
-        const uint4 v = row[j * 32 + lane];
-        acc[j].x |= v.x;
-        acc[j].y |= v.y;
-        acc[j].z |= v.z;
-        acc[j].w |= v.w;
+        acc[j].x |= b[j].x;
+        acc[j].y |= b[j].y;
+        acc[j].z |= b[j].z;
+        acc[j].w |= b[j].w;
       }
     }
-    const bool whole = seg0 == a.inv_off[cur_y] && i1 == a.inv_off[cur_y + 1];
-    rows_flush<V>(a, cur_y, whole, acc, words_out);
-    edges += i1 - i0;
+    if (i < m) rows_or<V>(acc, a.O, __shfl_sync(0xffffffffu, my_k, i), rs, lane);
+    // a y whose in-edges are all in this piece is this warp's alone
+    const bool whole = pc.x == a.inv_off[y] && pc.y == a.inv_off[y + 1];
+    rows_flush<V>(a, y, whole, acc, words_out);
+    edges += m;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) words_out += __shfl_xor_sync(0xffffffffu, words_out, o);
