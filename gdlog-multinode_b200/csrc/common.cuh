@@ -113,6 +113,10 @@ struct Ctl {
   u32 cond_set;  // graph conditional handle is valid
   u32 overflow_stage;  // 1: the overflow came from a dense update scan
   u32 pad_ctl;
+  u32 spin_limit;  // polls a bounded wait makes before it gives up (timeout)
+  u32 test_wait;   // nonzero: k_begin waits this many polls on `never` (tests)
+  u32 never;       // a flag no kernel sets
+  u32 pad_ctl2;
   u64 iteration;     // iteration_counter of the reference loop
   u64 stop_at;       // pause when iteration reaches this
   u64 max_iteration; // LIE::max_iteration
@@ -255,7 +259,8 @@ __device__ __forceinline__ bool ctl_stop(const Ctl *c) {
 // own slot, then a flag word [31:2] launch generation, [1:0] state (1
 // aggregate, 2 inclusive).  Words of another generation read as "not
 // ready", so the arrays are never cleared.  Every wait is bounded: after
-// kSpinLimit polls the waiter raises ctl->timeout and returns, and every
+// ctl->spin_limit polls (default kSpinLimit) the waiter raises ctl->timeout
+// and returns, and every
 // scatter that uses the result is bounds-checked, so a stuck predecessor
 // cannot hang or fault the GPU.
 // ---------------------------------------------------------------------------
@@ -293,7 +298,7 @@ __device__ __forceinline__ u64 lb_warp_prefix(Lb lb, long long tile, u32 gen, Ct
       ready = (f >> 2) == g && (f & 3u);
     }
     if (__all_sync(0xffffffffu, ready) == 0) {
-      if (++spins > kSpinLimit) {
+      if (++spins > ctl->spin_limit) {
         if (lane == 0) atomicOr(&ctl->timeout, 1u);
         return prefix;
       }

@@ -50,6 +50,16 @@ __device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L) {
 
 __global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
   if (ctl_stop(ctl) || threadIdx.x != 0) return;
+  if (ctl->test_wait) {
+    // gdl_engine_test_timeout: a bounded wait on a flag that nothing sets
+    u32 polls = 0;
+    while (!*((volatile u32 *)&ctl->never)) {
+      if (++polls > ctl->test_wait) {
+        atomicOr(&ctl->timeout, 1u);
+        return;
+      }
+    }
+  }
   begin_iteration(rels, L);
 }
 

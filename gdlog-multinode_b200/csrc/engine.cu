@@ -209,6 +209,8 @@ struct gdl_engine {
   // 3: pull form where eligible (pull.cuh)
   int pull_joins = 2;
   int row_gather = 2;
+  u32 spin_limit = kSpinLimit;  // polls of a bounded device wait
+  u32 test_wait = 0;            // gdl_engine_test_timeout (next fixpoint only)
   u64 *d_pull_count = nullptr;  // bit count of a transposed NEWT (zero between launches)
   // Device memory in bytes, read once at creation: cudaMemGetInfo can take
   // tens of milliseconds on a busy host, so the fixpoint sizes its lists
@@ -600,6 +602,7 @@ gdl_status reset_ctl(gdl_engine *e) {
   c.generation = ++e->generation;
   c.max_iteration = ~0ull;
   c.stop_at = ~0ull;
+  c.spin_limit = e->spin_limit;
   CK(e, cudaMemcpyAsync(e->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, e->s));
   return GDL_OK;
 }
@@ -1525,6 +1528,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - t_phase).count());
     t_phase = now;
   };
+  const u32 test_wait = e->test_wait;  // gdl_engine_test_timeout: this fixpoint only
+  e->test_wait = 0;
   TRY(reset_ctl(e));
   mark("reset_ctl");
   TRY(refresh(e));
@@ -1772,6 +1777,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   c.generation = ++e->generation;
   c.max_iteration = L.max_iteration < 0 ? 0 : (u64)L.max_iteration;
   c.trace_rows = trace_rows;
+  c.spin_limit = e->spin_limit;
+  c.test_wait = test_wait;
   L.trace.clear();
   L.retries = 0;
   L.grow_ms = L.graph_ms = 0;
@@ -2048,7 +2055,6 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       }
     if (any_delta) {
       TRY(push(e));
-      Counts kc;
       TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, L.map.words / kBmTileWords + 2));
       const u64 side = 1ull << (L.dk - kPullMinBits);
       for (int r : L.update) {
@@ -2208,6 +2214,8 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
       bad(cudaStreamCreateWithFlags(&e->cap_s, cudaStreamNonBlocking)) ||
       bad(cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s)) ||
       bad(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), e->s)) ||
+      bad(cudaMemcpyAsync(&e->d_ctl->spin_limit, &e->spin_limit, sizeof(u32),
+                          cudaMemcpyHostToDevice, e->s)) ||
       bad(cudaMemsetAsync(e->recs, 0, 16 * sizeof(LaunchRec), e->s)) ||
       bad(cudaMemsetAsync(e->d_u32, 0, 4 * sizeof(u32), e->s)) ||
       bad(cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s)) ||
@@ -2256,12 +2264,38 @@ static void release_program(gdl_engine *e) {
 gdl_status gdl_engine_clear(gdl_engine *e) {
   if (!e) return GDL_E_INVALID;
   cudaSetDevice(e->device);
-  if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
   // (no LIE graph may be running while its executable is destroyed)
   CK(e, cudaStreamSynchronize(e->s));
   release_program(e);
   // everything after this is stream-ordered behind the blocks released
   CK(e, cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s));
+  if (e->broken) {
+    // After a device-side check failed (a bounded wait gave up, a bounds
+    // check fired) the relations are dropped above; kernels of the failed
+    // launch may have stopped between counting and finishing, so the
+    // launch records and every look-back flag start afresh too.
+    CK(e, cudaMemsetAsync(e->recs, 0, 16 * sizeof(LaunchRec), e->s));
+    for (const Lb *lb : {&e->lb_cnt, &e->lb_nz, &e->lb_merge, &e->lb_bm, &e->lb_list})
+      if (lb->flag) CK(e, cudaMemsetAsync(lb->flag, 0, lb == &e->lb_cnt ? e->lb_cnt_tiles * 4
+                                                     : lb == &e->lb_nz ? e->lb_nz_tiles * 4
+                                                     : lb == &e->lb_merge ? e->lb_merge_tiles * 4
+                                                     : lb == &e->lb_bm ? e->lb_bm_tiles * 4
+                                                                        : e->lb_list_tiles * 4,
+                                          e->s));
+    if (e->sort_counters)
+      CK(e, cudaMemsetAsync(e->sort_counters, 0, (kMaxPasses + 1) * sizeof(u32), e->s));
+    CK(e, cudaMemsetAsync(e->d_u32, 0, 4 * sizeof(u32), e->s));
+    CK(e, cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s));
+    TRY(reset_ctl(e));
+    CK(e, cudaStreamSynchronize(e->s));
+    e->broken = false;
+  }
+  return GDL_OK;
+}
+
+gdl_status gdl_engine_test_timeout(gdl_engine *e, int32_t polls) {
+  if (!e || polls < 1) return GDL_E_INVALID;
+  e->test_wait = (u32)polls;
   return GDL_OK;
 }
 
@@ -2924,7 +2958,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
       t->dense_join_passes < 0 || t->dense_join_passes > 2 || t->join_aggregate < 0 ||
       t->join_aggregate > 2 || t->pull_joins < 0 || t->pull_joins > 3 || t->row_gather < 0 ||
-      t->row_gather > 3)
+      t->row_gather > 3 || t->spin_limit_log2 < 0 || t->spin_limit_log2 > 30)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -2936,6 +2970,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->join_aggregate) e->join_aggregate = t->join_aggregate;
   if (t->pull_joins) e->pull_joins = t->pull_joins;
   if (t->row_gather) e->row_gather = t->row_gather;
+  if (t->spin_limit_log2) e->spin_limit = 1u << t->spin_limit_log2;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -2952,6 +2987,8 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->join_aggregate = e->join_aggregate;
   t->pull_joins = e->pull_joins;
   t->row_gather = e->row_gather;
+  t->spin_limit_log2 = 0;
+  while (t->spin_limit_log2 < 31 && (1u << t->spin_limit_log2) < e->spin_limit) t->spin_limit_log2++;
   return GDL_OK;
 }
 
@@ -3182,6 +3219,8 @@ __global__ void k_noalloc_init(unsigned char *base, u64 rows) {
   d[1] = DArr{reinterpret_cast<u64 *>(base + kNaDelta), 0, 0};                   // empty FULL
   d[2] = DArr{reinterpret_cast<u64 *>(base + kNaUniq), 0, kNoAllocMaxRows};      // FULL'
   d[3] = DArr{reinterpret_cast<u64 *>(base + kNaDelta), 0, kNoAllocMaxRows};     // DELTA
+  // the bounded waits' limit (the control block was zeroed)
+  reinterpret_cast<Ctl *>(base + kNaCtl)->spin_limit = kSpinLimit;
 }
 
 __global__ void k_noalloc_unpack(const DArr *keys, u64 *rows) {

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) 
           u32 w = *((volatile u32 *)(status + (u64)t * kRadix + dg));
           u32 f = w >> 30;
           if (f == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > a.ctl->spin_limit) {
               atomicOr(&a.ctl->timeout, 1u);
               break;
             }

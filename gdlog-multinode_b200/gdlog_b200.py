@@ -61,7 +61,8 @@ class Tuning(C.Structure):
                 ("join_ctas_per_sm", C.c_int32), ("count_ctas_per_sm", C.c_int32),
                 ("index_slots_per_key", C.c_int32), ("dirty_min_log2_words", C.c_int32),
                 ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32),
-                ("pull_joins", C.c_int32), ("row_gather", C.c_int32)]
+                ("pull_joins", C.c_int32), ("row_gather", C.c_int32),
+                ("spin_limit_log2", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -150,6 +151,8 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_engine_set_dedup.restype = _I
         lib.gdl_engine_clear.argtypes = [_P]
         lib.gdl_engine_clear.restype = _I
+        lib.gdl_engine_test_timeout.argtypes = [_P, _I]
+        lib.gdl_engine_test_timeout.restype = _I
         lib.gdl_profile_kinds.argtypes = []
         lib.gdl_profile_kinds.restype = _I
         lib.gdl_profile_kind_name.argtypes = [_I]
@@ -527,6 +530,12 @@ class Engine:
         else:
             self._check(getattr(self.lib, self.pre + "engine_clear")(self.h))
         self.relations = []
+
+    def test_timeout(self, polls: int) -> None:
+        """The next fixpoint waits on a device flag nothing sets and gives
+        up after `polls` polls: it raises GdlError(TIMEOUT); clear()
+        recovers the engine (GPU engine only, for tests)."""
+        self._check(self.lib.gdl_engine_test_timeout(self.h, int(polls)))
 
     def load_device(self, rel: Relation, ptr: int, n_rows: int) -> None:
         """load_relation from rows already in device memory (n_rows x 2 u64)."""

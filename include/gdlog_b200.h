@@ -92,8 +92,18 @@ gdl_status gdl_engine_destroy(gdl_engine *e);
 /* Drop every relation and LIE of the engine, keeping its stream, scratch
  * buffers and memory pool, so the next program starts without device
  * allocation cost.  Relation and LIE ids restart at 0.  The reference has
- * no counterpart (its drivers leak relations at exit, test/tc.cu:80-149). */
+ * no counterpart (its drivers leak relations at exit, test/tc.cu:80-149).
+ * After a call failed with GDL_E_TIMEOUT (a device-side check: a bounded
+ * wait gave up or a bounds check fired), every call but this one and
+ * gdl_engine_destroy is refused; this one also resets the engine's device
+ * bookkeeping, after which the engine runs programs again. */
 gdl_status gdl_engine_clear(gdl_engine *e);
+
+/* Testing failure handling (no reference counterpart): the next fixpoint's
+ * first control kernel waits on a device flag that nothing sets, giving up
+ * after `polls` polls, so that fixpoint returns GDL_E_TIMEOUT without any
+ * GPU fault; gdl_engine_clear then recovers the engine. */
+gdl_status gdl_engine_test_timeout(gdl_engine *e, int32_t polls);
 
 /* How a fixpoint deduplicates NEWT and merges it into FULL.  SORT: radix
  * sort of NEWT, then one merge-path pass giving NEWT \ FULL and FULL ∪ NEWT
@@ -140,6 +150,9 @@ typedef struct gdl_tuning {
                                   rows along the inner's in-edges when the
                                   inner is small enough (|inner| x row bytes
                                   <= 256 MB; default), 3 = whenever possible */
+  int32_t spin_limit_log2;     /* a bounded device-side wait (look-back of a scan)
+                                  gives up after 2^this polls and the call
+                                  returns GDL_E_TIMEOUT (default 22; 1..30) */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

@@ -282,3 +282,52 @@ def test_collectives_per_pass(tmp_path):
         c = json.load(open(tmp_path / f"c{r}.json"))
         assert c["all_reduce"] == 1 + c["passes"]
         assert c["all_to_all_single"] == 2 + 2 * c["passes"]
+
+
+def _rank_gpu(rank, world, port, case, out_dir):
+    """One rank with the CUDA engine.  The ranks share one GPU; their only
+    connection is the gloo collectives on the host (no kernel waits on
+    another rank's)."""
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        text, inputs, deps = CASES[case]
+        with Engine("gpu", device=0) as eng:
+            res = PT.partitioned_program(eng, text, inputs(), rank, world, deps=deps)
+            out = {"iterations": res.iterations, "relations": res.relations, "rows": {},
+                   "n": {}}
+            for p, rows in sorted(res.full.items()):
+                parts = [None] * world
+                dist.all_gather_object(parts, np.asarray(rows, dtype=np.uint64))
+                out["rows"][p] = [list(r) for r in _sorted(np.concatenate(parts))]
+                out["n"][p] = len(rows)
+        with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+            json.dump(out, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["tc_grid_8", "tc_rmat_s7", "plen_rmat_s6", "sg_rmat_s7",
+                                  "cspa_120", "empty_inner"])
+def test_partitioned_program_on_the_cuda_engine(case, tmp_path):
+    """Two gloo ranks, each running its partition on the CUDA engine (the
+    engine's ternary keys, its relation table and LIE reuse across passes
+    in the partitioned driver), against datalog.run on one CUDA engine:
+    the same rows per head predicate, disjoint partitions, the same
+    loop-pass counts."""
+    world = 2
+    mp.spawn(_rank_gpu, args=(world, free_port(), case, str(tmp_path)), nprocs=world, join=True)
+    outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
+    text, inputs, deps = CASES[case]
+    with Engine("gpu", device=0) as g:
+        r = D.run(g, text, inputs(), deps=deps, sync=g.sync)
+        want = {p: [list(x) for x in _sorted(rel.rows() if rel.size() else [])]
+                for p, rel in r.relations.items()}
+        iters = dict(r.iterations)
+    for o in outs:
+        assert o["iterations"] == iters
+        for p in want:
+            assert o["rows"][p] == want[p], p
+    for p in want:
+        assert sum(o["n"][p] for o in outs) == len(want[p])
