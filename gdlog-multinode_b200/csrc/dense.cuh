@@ -1290,44 +1290,83 @@ __global__ void __launch_bounds__(256) k_inst_tile_pop(const u32 *bm, DenseMap m
 // digest terms of every tuple, summed per instance.
 __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map,
                                                      const u64 *tile_rank, u64 *acc) {
-  __shared__ u64 s_warp[kBmBlock / 32];
-  __shared__ WarpBits s_bits[kBmBlock / 32];
+  // Thread t holds words i * 256 + t of a tile (segments i = 0..7), so the
+  // ranks of its word's tuples follow from per-segment prefix sums and each
+  // thread walks its own bits: no per-tuple search.
+  __shared__ u32 s_wtot[kBmWordsPerThread][kBmBlock / 32];
+  __shared__ u32 s_seg_off[kBmWordsPerThread];
+  __shared__ u64 s_red[kBmBlock / 32];
   const u64 tiles = bm_tiles(map.words);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
     const u32 inst = dm_tile_inst(map, t);
     const SegInfo seg = map.seg[inst];
-    const u64 w0 = t * kBmTileWords + (u64)threadIdx.x * kBmWordsPerThread;
-    u32 x[kBmWordsPerThread];
-    u32 cnt = 0;
+    const u64 w0 = t * kBmTileWords;
+    u32 x[kBmWordsPerThread], ex[kBmWordsPerThread];
 #pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
-      x[i] = w0 + i < map.words ? bm[w0 + i] : 0u;
-      cnt += __popc(x[i]);
+      const u64 w = w0 + (u64)i * kBmBlock + threadIdx.x;
+      x[i] = w < map.words ? bm[w] : 0u;
+      const u32 c = __popc(x[i]);
+      u32 v = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      ex[i] = v - c;
+      if (lane == 31) s_wtot[i][warp] = v;
     }
-    u64 tile_n;
-    const u64 ex = block_excl_scan<kBmBlock>(cnt, s_warp, &tile_n);
-    if (tile_n == 0) continue;  // uniform: every thread saw the same total
-    // the warp's tuples, rank r of the warp by lane r % 32
-    const u64 ex0 = __shfl_sync(0xffffffffu, ex, 0);
-    const u64 end = __shfl_sync(0xffffffffu, ex + cnt, 31);
-    const u64 rank0 = tile_rank[t] + ex0;
-    const u64 ww = t * kBmTileWords + (u64)wid * 256;
+    __syncthreads();
+    if (threadIdx.x < kBmWordsPerThread) {
+      u32 a = 0;
+      for (int w = 0; w < kBmBlock / 32; w++) {
+        const u32 v = s_wtot[threadIdx.x][w];
+        s_wtot[threadIdx.x][w] = a;
+        a += v;
+      }
+      s_seg_off[threadIdx.x] = a;  // the segment's total, turned into offsets below
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u32 a = 0;
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        const u32 v = s_seg_off[i];
+        s_seg_off[i] = a;
+        a += v;
+      }
+    }
+    __syncthreads();
     u64 h_sum = 0;
-    warp_list_bits(x, (u32)(ex - ex0), (u32)(end - ex0), s_bits[wid], [&](u32 r, u32 k, u32 b) {
-      const u64 wl = ww + k - seg.base_word;
+#pragma unroll
+    for (int i = 0; i < kBmWordsPerThread; i++) {
+      u32 bits = x[i];
+      if (!bits) continue;
+      const u64 w = w0 + (u64)i * kBmBlock + threadIdx.x;
+      const u64 wl = w - seg.base_word;
       const u64 lx = wl >> seg.row_shift;
-      const u64 lz = ((wl & ((1ull << seg.row_shift) - 1)) << 5) + (u64)b;
-      u64 h = mix64(rank0 + r);
-      h = mix64(h ^ lx);
-      h = mix64(h ^ lz);
-      h_sum += h;
-    });
-    (void)lane;
+      const u64 lz0 = (wl & ((1ull << seg.row_shift) - 1)) << 5;
+      u64 rank = tile_rank[t] + s_seg_off[i] + s_wtot[i][warp] + ex[i];
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        u64 h = mix64(rank++);
+        h = mix64(h ^ lx);
+        h = mix64(h ^ (lz0 + (u64)b));
+        h_sum += h;
+      }
+    }
     // one atomic per tile: the tile's terms summed over the block
-    u64 dummy;
-    const u64 ex_h = block_excl_scan<kBmBlock>(h_sum, s_warp, &dummy);
-    if (threadIdx.x == kBmBlock - 1 && (ex_h + h_sum)) atomicAdd(&acc[inst], ex_h + h_sum);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h_sum += __shfl_xor_sync(0xffffffffu, h_sum, o);
+    if (lane == 0) s_red[warp] = h_sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u64 tot = 0;
+      for (int w = 0; w < kBmBlock / 32; w++) tot += s_red[w];
+      if (tot) atomicAdd(&acc[inst], tot);
+    }
+    __syncthreads();
   }
 }
 

@@ -2282,8 +2282,12 @@ gdl_status gdl_engine_clear(gdl_engine *e) {
                                                      : lb == &e->lb_bm ? e->lb_bm_tiles * 4
                                                                         : e->lb_list_tiles * 4,
                                           e->s));
+    // the sort's tile counters and digit histograms (an interrupted sort
+    // leaves them part-accumulated; they return to zero only at its end)
     if (e->sort_counters)
       CK(e, cudaMemsetAsync(e->sort_counters, 0, (kMaxPasses + 1) * sizeof(u32), e->s));
+    if (e->sort_offsets)
+      CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kRadix * sizeof(u32), e->s));
     CK(e, cudaMemsetAsync(e->d_u32, 0, 4 * sizeof(u32), e->s));
     CK(e, cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s));
     TRY(reset_ctl(e));
