@@ -178,15 +178,31 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
   // zeroing before any warp's atomicAdd into s_cnt
   __syncthreads();
   u64 n_delta = 0, n_newt = 0, moved = 0;
-  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+  // NEWT's words of a tile: from G (row-major, at `src`) or from gt (the
+  // transposed twin, at the mirrored tile).  Software-pipelined: the next
+  // tile's NEWT words load while this tile is processed.
+  auto newt_at = [&](u64 tt) {
+    const u64 r = tt / per, c = tt % per;
+    return gt ? ((c * 256 + (u64)threadIdx.x) << rs) + r * 8
+              : ((r * 256 + (u64)threadIdx.x) << rs) + c * 8;
+  };
+  const u32 *nsrc = gt ? gt : G;
+  u64 t = blockIdx.x;
+  u32 nx[8];
+  if (t < tiles) load8(nsrc + newt_at(t), nx);
+  for (; t < tiles; t += gridDim.x) {
     const u64 tr = t / per, tc = t % per;
     const u64 src = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
-    u32 g[8], d[8];
+    u32 g[8], d[8], cur[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) cur[i] = nx[i];
+    if (t + gridDim.x < tiles) load8(nsrc + newt_at(t + gridDim.x), nx);
     if (gt) {
       // NEWT's tile (tr, tc) is the transpose of gt's tile (tc, tr)
       const u64 tsrc = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
       u32 v[8];
-      load8(gt + tsrc, v);
+#pragma unroll
+      for (int i = 0; i < 8; i++) v[i] = cur[i];
       const bool any_v = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
       moved += 32;
       if (any_v) {
@@ -207,7 +223,8 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
         for (int i = 0; i < 8; i++) g[i] = 0;
       }
     } else {
-      load8(G + src, g);
+#pragma unroll
+      for (int i = 0; i < 8; i++) g[i] = cur[i];
       moved += 32;
     }
     const bool any_g = (g[0] | g[1] | g[2] | g[3] | g[4] | g[5] | g[6] | g[7]) != 0u;
@@ -707,11 +724,21 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *
   const u64 tiles = per * per;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   u64 moved = 0;
-  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+  // Software-pipelined over the block's tiles: the next tile's source words
+  // and this tile's destination words are loaded before this tile's
+  // barriers, so the two memory round trips of a tile overlap.
+  u64 t = blockIdx.x;
+  u32 v[8];
+  if (t < tiles) load8(src + ((((t / per) * 256 + (u64)threadIdx.x) << rs) + (t % per) * 8), v);
+  for (; t < tiles; t += gridDim.x) {
     const u64 tr = t / per, tc = t % per;
     const u64 at = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
-    u32 v[8];
-    load8(src + at, v);
+    const u64 dw = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
+    const u64 tn = t + gridDim.x;
+    u32 vn[8], d[8];
+    if (tn < tiles)
+      load8(src + ((((tn / per) * 256 + (u64)threadIdx.x) << rs) + (tn % per) * 8), vn);
+    load8(dst + dw, d);
     const bool any = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
     moved += 4 * 8;
     if (any) {
@@ -720,22 +747,24 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *
       ps[1] = make_uint4(0, 0, 0, 0);
       moved += 4 * 8;
     }
-    if (!__syncthreads_or(any)) continue;  // block-uniform
+    if (__syncthreads_or(any)) {  // block-uniform
 #pragma unroll
-    for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
-    __syncthreads();
-    const u32 *q = s_t[threadIdx.x];
-    if ((q[0] | q[1] | q[2] | q[3] | q[4] | q[5] | q[6] | q[7]) != 0u) {
-      const u64 dw = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
-      u32 d[8];
-      load8(dst + dw, d);
-      uint4 *pd = reinterpret_cast<uint4 *>(dst + dw);
-      pd[0] = make_uint4(d[0] | q[0], d[1] | q[1], d[2] | q[2], d[3] | q[3]);
-      pd[1] = make_uint4(d[4] | q[4], d[5] | q[5], d[6] | q[6], d[7] | q[7]);
-      if (dirty) dirty[dw / kBmChunkWords] = 1;
-      moved += 8 * 8;
+      for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+      __syncthreads();
+      const u32 *q = s_t[threadIdx.x];
+      if ((q[0] | q[1] | q[2] | q[3] | q[4] | q[5] | q[6] | q[7]) != 0u) {
+        uint4 *pd = reinterpret_cast<uint4 *>(dst + dw);
+        pd[0] = make_uint4(d[0] | q[0], d[1] | q[1], d[2] | q[2], d[3] | q[3]);
+        pd[1] = make_uint4(d[4] | q[4], d[5] | q[5], d[6] | q[6], d[7] | q[7]);
+        if (dirty) dirty[dw / kBmChunkWords] = 1;
+        moved += 8 * 8;
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    if (tn < tiles) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) v[i] = vn[i];
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(0xffffffffu, moved, o);
