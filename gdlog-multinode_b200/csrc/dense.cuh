@@ -810,8 +810,11 @@ struct ListSmem {
   long long tile;
 };
 
+// expect_n: the bit count the host sized the list for (and keeps as its
+// size); a listing that finds another count raises the bounds flag.
 __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, int rs, DArr *out,
-                                                      Lb lb, LaunchRec *rec, Ctl *ctl) {
+                                                      u64 expect_n, Lb lb, LaunchRec *rec,
+                                                      Ctl *ctl) {
   __shared__ ListSmem sm;
   if (ctl_stop(ctl)) return;
   const u64 tiles = words / kBmTileWords;
@@ -879,7 +882,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
       // from the bitmap's count; a mismatch is an error, reported)
       const u64 total = base + tot;
       out->n = total <= cap ? total : cap;
-      if (total > cap) atomicOr(&ctl->oob, 16384u);
+      if (total > cap || total != expect_n) atomicOr(&ctl->oob, 16384u);
     }
     moved += 4 * kBmWordsPerThread + 8 * (u64)(threadIdx.x == 0 ? tot : 0);
     for (int i = 0; i < kBmWordsPerThread; i++) {

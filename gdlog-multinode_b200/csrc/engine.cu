@@ -38,6 +38,8 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <condition_variable>
+#include <thread>
 #include <map>
 #include <unordered_map>
 #include <chrono>
@@ -189,6 +191,15 @@ struct gdl_engine {
   u64 lb_bm_tiles = 0;
   Lb lb_list{};  // k_bm_list: one look-back slot per 2048-word tile
   u64 lb_list_tiles = 0;
+  // Graph executables of dropped LIEs: destroyed by a worker thread of the
+  // engine (destroying one takes ~0.1 ms of host time that the caller's
+  // next program need not wait for; none of them can be running).
+  std::vector<cudaGraphExec_t> graveyard;
+  std::mutex reap_mu;
+  std::condition_variable reap_cv;
+  std::vector<cudaGraphExec_t> reap_list;  // handed to the worker
+  std::thread reaper;
+  bool reap_stop = false;
   // dalloc / dfree: bytes of each live block, and freed blocks for reuse
   std::unordered_map<void *, size_t> alloc_size;
   std::multimap<size_t, void *> spare;
@@ -374,6 +385,35 @@ gdl_status ensure_index(gdl_engine *e, Index &ix, u64 cap) {
   ix.hash_mode = mode;
   ix.epoch = 0;
   return GDL_OK;
+}
+
+// Hand the executables of dropped LIEs to the engine's worker thread, which
+// destroys them (none of them can be running: the stream was synchronised
+// when they were dropped).
+void reap_graphs(gdl_engine *e) {
+  if (e->graveyard.empty()) return;
+  {
+    std::lock_guard<std::mutex> lock(e->reap_mu);
+    if (!e->reaper.joinable()) {
+      const int dev = e->device;
+      e->reaper = std::thread([e, dev] {
+        cudaSetDevice(dev);
+        std::unique_lock<std::mutex> lk(e->reap_mu);
+        while (true) {
+          e->reap_cv.wait(lk, [e] { return e->reap_stop || !e->reap_list.empty(); });
+          std::vector<cudaGraphExec_t> work;
+          work.swap(e->reap_list);
+          lk.unlock();
+          for (cudaGraphExec_t x : work) cudaGraphExecDestroy(x);
+          lk.lock();
+          if (e->reap_stop && e->reap_list.empty()) return;
+        }
+      });
+    }
+    e->reap_list.insert(e->reap_list.end(), e->graveyard.begin(), e->graveyard.end());
+  }
+  e->graveyard.clear();
+  e->reap_cv.notify_one();
 }
 
 gdl_status pull(gdl_engine *e) {
@@ -1988,6 +2028,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     batch = std::min<u64>(batch * 2, 64);
   }
   e->mirror_fresh = false;  // (a pull while growing buffers preceded more launches)
+  bool listed = false;
   if (L.dense) {
     // FULL lists that were not kept during the loop are written from the
     // FULL bitmaps, sorted (bit order is tuple order).
@@ -2025,8 +2066,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         if (!e->instances) {
           // square domain: one pass (k_bm_list)
           k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
-              e->d_ctl);
+              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->h[r].full.n,
+              e->lb_list, &e->recs[8], e->d_ctl);
           continue;
         }
         BmScanArgs a = scan_none(L.map);
@@ -2036,7 +2077,10 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         launch_scan(e, a, r, &kc);
       }
       CK(e, cudaGetLastError());
-      TRY(pull(e));
+      // The square-domain listing publishes the sizes the host already
+      // holds; the batched form's scans need the table read back.
+      if (e->instances) TRY(pull(e));
+      listed = true;
     }
     // DELTA lists that were not kept (read only transposed by pull-form
     // joins) and are not empty (max_iteration ended the loop): transposed
@@ -2069,24 +2113,16 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           rows = h.bmG;
         }
         k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, e->lb_list, &e->recs[8],
-            e->d_ctl);
+            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, h.delta.n, e->lb_list,
+            &e->recs[8], e->d_ctl);
         if (!plan.delta_n[r]) CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
       }
       CK(e, cudaGetLastError());
-      TRY(pull(e));
+      listed = true;
     }
-    {
-      // the listings' bounds checks
-      Ctl c3;
-      CK(e, cudaMemcpyAsync(&c3, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
-      CK(e, cudaStreamSynchronize(e->s));
-      if (c3.timeout || c3.oob) {
-        e->broken = true;
-        return fail(e, GDL_E_TIMEOUT, "listing FULL/DELTA after the loop failed (timeout=%u oob=%u)",
-                    c3.timeout, c3.oob);
-      }
-    }
+    // the listings' device checks, read back with the end of the fixpoint
+    if (listed)
+      CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
     for (RelDev &h : e->h) {
       h.dense = h.full_lazy = 0;
       h.dirty = nullptr;
@@ -2096,6 +2132,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   }
   CK(e, cudaEventRecord(e->ev1, e->s));
   CK(e, cudaEventSynchronize(e->ev1));
+  if (listed && (e->h_ctl->timeout || e->h_ctl->oob)) {
+    e->broken = true;
+    return fail(e, GDL_E_TIMEOUT, "listing FULL/DELTA after the loop failed (timeout=%u oob=%u)",
+                e->h_ctl->timeout, e->h_ctl->oob);
+  }
   float ms = 0;
   CK(e, cudaEventElapsedTime(&ms, e->ev0, e->ev1));
   L.ms = ms;
@@ -2247,7 +2288,7 @@ static void release_program(gdl_engine *e) {
     if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
   }
   for (LieHost &L : e->lies) {
-    if (L.gexec) cudaGraphExecDestroy(L.gexec);
+    if (L.gexec) e->graveyard.push_back(L.gexec);
     // stream-ordered frees (a cudaFree would wait for the whole device)
     for (void *p : {(void *)L.d_trace, (void *)L.d_lie, (void *)L.d_joinrec})
       dfree(e, p);
@@ -2267,6 +2308,7 @@ gdl_status gdl_engine_clear(gdl_engine *e) {
   // (no LIE graph may be running while its executable is destroyed)
   CK(e, cudaStreamSynchronize(e->s));
   release_program(e);
+  reap_graphs(e);
   // everything after this is stream-ordered behind the blocks released
   CK(e, cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s));
   if (e->broken) {
@@ -2308,6 +2350,16 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   cudaSetDevice(e->device);
   if (e->s) cudaStreamSynchronize(e->s);
   release_program(e);
+  for (cudaGraphExec_t x : e->graveyard) cudaGraphExecDestroy(x);
+  e->graveyard.clear();
+  if (e->reaper.joinable()) {
+    {
+      std::lock_guard<std::mutex> lock(e->reap_mu);
+      e->reap_stop = true;
+    }
+    e->reap_cv.notify_one();
+    e->reaper.join();
+  }
   for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
   e->spare.clear();
   if (e->s) cudaStreamSynchronize(e->s);
