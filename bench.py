@@ -62,6 +62,11 @@ WORKLOADS = {
         prog=P.sg, make=lambda: (W.rmat_edges(14, 40000, seed=14),), tuning={"dedup": "sort"},
         desc="same generation, R-MAT scale 14 (16,384 nodes), 40,000 edges, "
              "a,b,c,d=.57,.19,.19,.05, seed 14; sorted-list path (dedup=sort)"),
+    # the sorted-list path on a small case (profiling the sort kernels)
+    "sg_rmat_s12_sort": dict(
+        prog=P.sg, make=lambda: (W.rmat_edges(12, 8000, seed=12),), tuning={"dedup": "sort"},
+        desc="same generation, R-MAT scale 12 (4,096 nodes), 8,000 edges, seed 12; "
+             "sorted-list path (dedup=sort)"),
     "tc_grid_64": dict(
         prog=P.tc, make=lambda: (W.grid_edges(64, 64),),
         desc="transitive closure, 64x64 directed grid, 8,064 edges"),
