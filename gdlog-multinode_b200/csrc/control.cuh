@@ -180,16 +180,22 @@ __global__ void k_unpack_rows(const u64 *keys, u64 n, u64 *rows) {
 }
 
 // Digest of sorted keys: sum over i of a hash of (i, c0, c1).
+__device__ __forceinline__ u64 digest_term(u64 i, u64 k) {
+  return mix64(mix64(mix64(i) ^ (u64)key_c0(k)) ^ (u64)key_c1(k));
+}
 __global__ void k_digest(const u64 *keys, u64 n, u64 *acc) {
   u64 s = 0;
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (u64)gridDim.x * blockDim.x) {
-    u64 k = keys[i];
-    u64 h = mix64(i);
-    h = mix64(h ^ (u64)key_c0(k));
-    h = mix64(h ^ (u64)key_c1(k));
-    s += h;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  // four keys in flight per thread (the hash chain is long; the loads are
+  // issued together ahead of it)
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    const u64 k0 = keys[i], k1 = keys[i + stride], k2 = keys[i + 2 * stride],
+              k3 = keys[i + 3 * stride];
+    s += digest_term(i, k0) + digest_term(i + stride, k1) + digest_term(i + 2 * stride, k2) +
+         digest_term(i + 3 * stride, k3);
   }
+  for (; i < n; i += stride) s += digest_term(i, keys[i]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);

@@ -789,20 +789,19 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 // passes for the lists written at the end of a LIE (src/lie.cu:219-254:
 // FULL flattened into a sorted array).
 //
-// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i), so
-// in every window each thread expands at most one word, 32 keys, and all
-// threads share the work of dense tiles.
+// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i).
+// A segment is 256 words, 8192 bit positions, so the keys of one segment
+// always fit one staging buffer: each is staged as its 13-bit position in
+// the segment (2 bytes; the row and column are rebuilt at the copy-out),
+// each thread expands one word per segment, and the copy-out is one
+// coalesced pass.  Two buffers alternate between the segments that hold
+// keys, so one barrier per segment separates a buffer's expansion from its
+// copy-out and the copy-out from the buffer's next expansion.
 // ---------------------------------------------------------------------------
-constexpr int kListStage = 4096;
-
-// Staging slot of the q-th key of a window: within each group of 32 keys
-// the slot is XORed with the group number, so that lanes whose keys are 32
-// apart hit different banks; the copy-out reads through the same
-// permutation.
-__device__ __forceinline__ u32 list_slot(u32 q) { return q ^ ((q >> 5) & 31u); }
+constexpr int kListStage = kBmBlock * 32;  // 8192 positions per segment
 
 struct ListSmem {
-  u64 keys[kListStage];
+  unsigned short stage[2][kListStage];
   u32 wtot[kBmWordsPerThread][kBmBlock / 32];  // per segment: warp totals, then offsets
   u32 seg_tot[kBmWordsPerThread];
   u32 seg_off[kBmWordsPerThread];
@@ -824,6 +823,7 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
   const u64 cap = out->cap;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 moved = 0;
+  u32 nbuf = 0;  // segments with keys staged so far (buffer parity)
   while (true) {
     const long long t = grab_tile(rec, &sm.tile);
     if (t >= (long long)tiles) break;
@@ -888,32 +888,35 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
     for (int i = 0; i < kBmWordsPerThread; i++) {
       const u32 st = sm.seg_tot[i];  // block-uniform
       if (st == 0) continue;
-      const u32 so = sm.seg_off[i];
-      const u32 p0 = sm.wtot[i][warp] + ex[i];  // this word's first key in the segment
-      const u64 w = w0 + (u64)i * kBmBlock + threadIdx.x;
-      const u64 kb = ((w >> rs) << 32) | ((w & row_mask) << 5);
-      for (u32 r0 = 0; r0 < st; r0 += kListStage) {
-        u32 x = v[i];
-        u32 p = p0;
-        const u32 n = __popc(x);
-        if (x && p < r0 + kListStage && p + n > r0) {
-          while (x) {
-            const int b = __ffs(x) - 1;
-            x &= x - 1;
-            if (p >= r0 && p < r0 + kListStage) sm.keys[list_slot(p - r0)] = kb + (u64)b;
-            p++;
-          }
+      unsigned short *stg = sm.stage[nbuf++ & 1];
+      // expand this thread's word: its keys' positions in the segment
+      u32 x = v[i];
+      u32 p = sm.wtot[i][warp] + ex[i];
+      const u32 q0 = threadIdx.x * 32;
+      while (x) {
+        stg[p++] = (unsigned short)(q0 + (u32)(__ffs(x) - 1));
+        x &= x - 1;
+      }
+      __syncthreads();
+      // copy-out: position q of segment word ws = q / 32, bit q % 32
+      const u64 ws = w0 + (u64)i * kBmBlock;
+      const u64 pos0 = base + sm.seg_off[i];
+      u64 *o = dst + pos0;
+      if (pos0 + st <= cap) {
+        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
+          const u32 q = stg[j];
+          const u64 w = ws + (q >> 5);
+          o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
         }
-        __syncthreads();
-        const u32 m = min((u32)kListStage, st - r0);
-        for (u32 j = threadIdx.x; j < m; j += kBmBlock) {
-          const u64 pos = base + so + r0 + j;
-          if (pos < cap)
-            dst[pos] = sm.keys[list_slot(j)];
+      } else {
+        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
+          const u32 q = stg[j];
+          const u64 w = ws + (q >> 5);
+          if (pos0 + j < cap)
+            o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
           else
             atomicOr(&ctl->oob, 16384u);
         }
-        __syncthreads();
       }
     }
   }

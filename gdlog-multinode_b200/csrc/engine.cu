@@ -114,6 +114,8 @@ struct LieHost {
   double setup_ms = 0, grow_ms = 0, graph_ms = 0;
   cudaGraphExec_t gexec = nullptr;
   unsigned long long cond_handle = 0;
+  int gslot = -1;             // gexec's entry in the engine's executable cache
+  bool graph_reused = false;  // the last fixpoint's executable came from it
   bool graph_dirty = true;
   Counts per_iter;  // launches of one enqueued iteration
   // Dense form of the running fixpoint (dense.cuh): bits per column (square
@@ -203,7 +205,25 @@ struct gdl_engine {
   // dalloc / dfree: bytes of each live block, and freed blocks for reuse
   std::unordered_map<void *, size_t> alloc_size;
   std::multimap<size_t, void *> spare;
+  std::unordered_map<void *, std::multimap<size_t, void *>::iterator> spare_at;
   size_t spare_bytes = 0;
+  // The blocks the program before the last gdl_engine_clear got, per
+  // request size in request order (replayed by dalloc), and this program's.
+  std::unordered_map<size_t, std::vector<void *>> replay, alloc_log;
+  std::unordered_map<size_t, size_t> replay_seen;
+  // Executables of iteration graphs, kept across programs (build_graph).
+  struct CachedGraph {
+    cudaGraph_t body = nullptr;  // the iteration as captured, for comparison
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long handle = 0;
+    Counts per_iter;
+    size_t nodes = 0;
+    bool in_use = false;
+    u64 used = 0;  // last use, for eviction
+  };
+  std::vector<CachedGraph> gcache;
+  u64 gcache_clock = 0;
+  std::unordered_map<const void *, std::vector<size_t>> param_sizes;
   // Largest 2*bits domain kept as bitmaps (GDLOG_DENSE_MAX_BITS), and the
   // dedup path: 0 chosen by domain size, 1 always sort/merge, 2 always
   // bitmaps where the domain allows (GDLOG_DEDUP=auto|sort|dense).
@@ -305,28 +325,51 @@ gdl_status fail(gdl_engine *e, gdl_status code, const char *fmt, ...) {
 // the engine stream like the pool's own reuse.  A program run after
 // gdl_engine_clear therefore makes no allocation calls once the first run
 // has sized everything.
+//
+// The same program run again gets the same blocks: the j-th request of a
+// given size takes back, when it is spare, the block the j-th request of
+// that size got in the program before the last gdl_engine_clear.  Device
+// addresses in the program's kernel arguments then repeat, and its
+// iteration graphs are found in the executable cache (build_graph).
+void *take_spare(gdl_engine *e, std::multimap<size_t, void *>::iterator it) {
+  void *p = it->second;
+  e->spare_bytes -= it->first;
+  e->alloc_size[p] = it->first;
+  e->spare_at.erase(p);
+  e->spare.erase(it);
+  return p;
+}
+void drop_spare(gdl_engine *e) {
+  for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
+  e->spare.clear();
+  e->spare_at.clear();
+  e->spare_bytes = 0;
+}
 gdl_status dalloc(gdl_engine *e, void **p, size_t bytes) {
   *p = nullptr;
   bytes = round_up(std::max<size_t>(bytes, 16), 256);
-  auto it = e->spare.lower_bound(bytes);
-  if (it != e->spare.end() && it->first <= 2 * bytes) {
-    *p = it->second;
-    e->spare_bytes -= it->first;
-    e->alloc_size[*p] = it->first;
-    e->spare.erase(it);
-    return GDL_OK;
+  const size_t j = e->replay_seen[bytes]++;
+  auto rp = e->replay.find(bytes);
+  if (rp != e->replay.end() && j < rp->second.size()) {
+    auto at = e->spare_at.find(rp->second[j]);
+    if (at != e->spare_at.end()) *p = take_spare(e, at->second);
   }
-  cudaError_t r = cudaMallocAsync(p, bytes, e->s);
-  if (r == cudaErrorMemoryAllocation && !e->spare.empty()) {
-    // give the spare blocks back and try once more
-    cudaGetLastError();
-    for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
-    e->spare.clear();
-    e->spare_bytes = 0;
-    r = cudaMallocAsync(p, bytes, e->s);
+  if (!*p) {
+    auto it = e->spare.lower_bound(bytes);
+    if (it != e->spare.end() && it->first <= 2 * bytes) *p = take_spare(e, it);
   }
-  CK(e, r);
-  e->alloc_size[*p] = bytes;
+  if (!*p) {
+    cudaError_t r = cudaMallocAsync(p, bytes, e->s);
+    if (r == cudaErrorMemoryAllocation && !e->spare.empty()) {
+      // give the spare blocks back and try once more
+      cudaGetLastError();
+      drop_spare(e);
+      r = cudaMallocAsync(p, bytes, e->s);
+    }
+    CK(e, r);
+    e->alloc_size[*p] = bytes;
+  }
+  e->alloc_log[bytes].push_back(*p);
   return GDL_OK;
 }
 void dfree(gdl_engine *e, void *p) {
@@ -342,7 +385,7 @@ void dfree(gdl_engine *e, void *p) {
     cudaFreeAsync(p, e->s);
     return;
   }
-  e->spare.emplace(b, p);
+  e->spare_at[p] = e->spare.emplace(b, p);
   e->spare_bytes += b;
 }
 
@@ -652,6 +695,7 @@ gdl_status reset_ctl(gdl_engine *e) {
 // ---------------------------------------------------------------------------
 void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *kc) {
   SortArgs a;
+  memset(&a, 0, sizeof a);
   a.keys = d_keys;
   a.buf0 = buf0;
   a.buf1 = e->sort_buf;
@@ -711,6 +755,7 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
     Counts kc;
     launch_sort(e, &e->d_rels[rel].newt, r.newt.ptr, r.newt.cap, &kc);
     MergeArgs m;
+    memset(&m, 0, sizeof m);
     m.newt = &e->d_rels[rel].newt;
     m.a = sorted_location(e, r.newt.ptr);
     // B = empty FULL
@@ -965,6 +1010,23 @@ BmScanArgs scan_none(const DenseMap &map) {
   return a;
 }
 
+// (zeroed first: argument bytes, padding included, are compared by the
+// executable cache)
+TransposeArgs transpose_args(const u32 *g, const u32 *f, u32 *dst, int dk, DArr *count_to,
+                             u64 *count_acc, LaunchRec *lrec, Ctl *ctl) {
+  TransposeArgs t;
+  memset(&t, 0, sizeof t);
+  t.g = g;
+  t.f = f;
+  t.dst = dst;
+  t.dk = dk;
+  t.count_to = count_to;
+  t.count_acc = count_acc;
+  t.lrec = lrec;
+  t.ctl = ctl;
+  return t;
+}
+
 void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc,
                          bool begin_next);
 
@@ -1169,8 +1231,8 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         const u32 *OT = oh.bmDT;
         const u64 side = 1ull << (L.dk - kPullMinBits);
         if (op.outer_ver == GDL_NEWT) {
-          TransposeArgs t{oh.bmG, nullptr, oh.bmGT, L.dk, &R[op.outer].newt, e->d_pull_count,
-                          &e->recs[7], e->d_ctl};
+          TransposeArgs t = transpose_args(oh.bmG, nullptr, oh.bmGT, L.dk, &R[op.outer].newt,
+                                           e->d_pull_count, &e->recs[7], e->d_ctl);
           PLAUNCH(kc, kPBitmap,
                   k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(t));
           OT = oh.bmGT;
@@ -1192,7 +1254,8 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       }
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
                                 oh.newt.cap});
-      JoinArgs b = a;
+      JoinArgs b;
+      memcpy(&b, &a, sizeof b);
       b.rec = &e->recs[1];
       if (dense && e->dense_join_passes == 1) {
         const int jg = grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm);
@@ -1341,8 +1404,8 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
       const int r = (int)(a.rd - R);
       if (plan.delta_t[r]) {
         const u64 side = 1ull << (L.dk - kPullMinBits);
-        TransposeArgs t{e->h[r].bmG, e->h[r].bmF, e->h[r].bmDT, L.dk, nullptr, nullptr,
-                        &e->recs[7], e->d_ctl};
+        TransposeArgs t = transpose_args(e->h[r].bmG, e->h[r].bmF, e->h[r].bmDT, L.dk, nullptr,
+                                         nullptr, &e->recs[7], e->d_ctl);
         PLAUNCH(kc, kPBitmap, k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(t));
       }
     }
@@ -1366,6 +1429,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
     if (!dense) {
       launch_sort(e, &R[r].newt, rh.newt.ptr, rh.newt.cap, kc);
       MergeArgs m;
+      memset(&m, 0, sizeof m);
       m.newt = &R[r].newt;
       m.a = sorted_location(e, rh.newt.ptr);
       m.full = &R[r].full;
@@ -1406,17 +1470,177 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
   PLAUNCH(kc, kPControl, k_commit<<<1, 32, 0, s>>>(R, L.d_lie, e->d_ctl, begin_next ? 1 : 0));
 }
 
+// ---------------------------------------------------------------------------
+// Executable cache.  Instantiating the loop's graph takes ~0.15 ms of host
+// time and destroying it ~0.17 ms, during which the driver also holds off
+// the caller's next CUDA calls.  A program run again after
+// gdl_engine_clear (a service answering the same query shape, a benchmark)
+// captures the same iteration: the same kernels with the same launch shapes
+// and, because dalloc replays the previous program's blocks, the same
+// argument bytes.  Such an iteration takes the cached executable, compared
+// node by node (kind; kernel, grid, block, shared memory and every argument
+// byte, sized by cudaFuncGetParamInfo; memset and memcpy parameters;
+// edges), so a reuse is exact by construction.
+// ---------------------------------------------------------------------------
+constexpr size_t kGraphCacheMax = 32;
+
+const std::vector<size_t> &param_sizes(gdl_engine *e, const void *func) {
+  auto it = e->param_sizes.find(func);
+  if (it != e->param_sizes.end()) return it->second;
+  std::vector<size_t> v;
+  for (size_t i = 0; i < 256; i++) {
+    size_t off = 0, sz = 0;
+    if (cudaFuncGetParamInfo(func, i, &off, &sz) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    v.push_back(sz);
+  }
+  return e->param_sizes.emplace(func, std::move(v)).first->second;
+}
+
+bool nodes_equal(gdl_engine *e, cudaGraphNode_t a, cudaGraphNode_t b) {
+  cudaGraphNodeType ta, tb;
+  if (cudaGraphNodeGetType(a, &ta) != cudaSuccess || cudaGraphNodeGetType(b, &tb) != cudaSuccess ||
+      ta != tb)
+    return false;
+  if (ta == cudaGraphNodeTypeEmpty) return true;
+  if (ta == cudaGraphNodeTypeKernel) {
+    cudaKernelNodeParams pa, pb;
+    if (cudaGraphKernelNodeGetParams(a, &pa) != cudaSuccess ||
+        cudaGraphKernelNodeGetParams(b, &pb) != cudaSuccess)
+      return false;
+    if (pa.func != pb.func || pa.sharedMemBytes != pb.sharedMemBytes || pa.extra || pb.extra ||
+        pa.gridDim.x != pb.gridDim.x || pa.gridDim.y != pb.gridDim.y ||
+        pa.gridDim.z != pb.gridDim.z || pa.blockDim.x != pb.blockDim.x ||
+        pa.blockDim.y != pb.blockDim.y || pa.blockDim.z != pb.blockDim.z)
+      return false;
+    // every engine kernel takes arguments: none known means none compared
+    const std::vector<size_t> &sz = param_sizes(e, pa.func);
+    if (sz.empty() || !pa.kernelParams || !pb.kernelParams) return false;
+    for (size_t i = 0; i < sz.size(); i++)
+      if (memcmp(pa.kernelParams[i], pb.kernelParams[i], sz[i]) != 0) return false;
+    return true;
+  }
+  if (ta == cudaGraphNodeTypeMemset) {
+    cudaMemsetParams ma, mb;
+    if (cudaGraphMemsetNodeGetParams(a, &ma) != cudaSuccess ||
+        cudaGraphMemsetNodeGetParams(b, &mb) != cudaSuccess)
+      return false;
+    return ma.dst == mb.dst && ma.pitch == mb.pitch && ma.value == mb.value &&
+           ma.elementSize == mb.elementSize && ma.width == mb.width && ma.height == mb.height;
+  }
+  if (ta == cudaGraphNodeTypeMemcpy) {
+    cudaMemcpy3DParms ca, cb;
+    if (cudaGraphMemcpyNodeGetParams(a, &ca) != cudaSuccess ||
+        cudaGraphMemcpyNodeGetParams(b, &cb) != cudaSuccess)
+      return false;
+    auto same_pos = [](const cudaPos &x, const cudaPos &y) {
+      return x.x == y.x && x.y == y.y && x.z == y.z;
+    };
+    auto same_ptr = [](const cudaPitchedPtr &x, const cudaPitchedPtr &y) {
+      return x.ptr == y.ptr && x.pitch == y.pitch && x.xsize == y.xsize && x.ysize == y.ysize;
+    };
+    return ca.srcArray == cb.srcArray && ca.dstArray == cb.dstArray && ca.kind == cb.kind &&
+           same_pos(ca.srcPos, cb.srcPos) && same_pos(ca.dstPos, cb.dstPos) &&
+           same_ptr(ca.srcPtr, cb.srcPtr) && same_ptr(ca.dstPtr, cb.dstPtr) &&
+           ca.extent.width == cb.extent.width && ca.extent.height == cb.extent.height &&
+           ca.extent.depth == cb.extent.depth;
+  }
+  return false;  // (the iteration records no other kind of node)
+}
+
+bool graphs_equal(gdl_engine *e, cudaGraph_t a, cudaGraph_t b) {
+  size_t na = 0, nb = 0;
+  if (cudaGraphGetNodes(a, nullptr, &na) != cudaSuccess ||
+      cudaGraphGetNodes(b, nullptr, &nb) != cudaSuccess || na != nb)
+    return false;
+  std::vector<cudaGraphNode_t> xa(na), xb(nb);
+  if (na && (cudaGraphGetNodes(a, xa.data(), &na) != cudaSuccess ||
+             cudaGraphGetNodes(b, xb.data(), &nb) != cudaSuccess))
+    return false;
+  for (size_t i = 0; i < na; i++)
+    if (!nodes_equal(e, xa[i], xb[i])) return false;
+  // the same dependencies between corresponding nodes
+  size_t ea = 0, eb = 0;
+  if (cudaGraphGetEdges(a, nullptr, nullptr, &ea) != cudaSuccess ||
+      cudaGraphGetEdges(b, nullptr, nullptr, &eb) != cudaSuccess || ea != eb)
+    return false;
+  auto edges = [&](cudaGraph_t g, const std::vector<cudaGraphNode_t> &x, size_t n,
+                   std::vector<std::pair<size_t, size_t>> &out) {
+    std::vector<cudaGraphNode_t> from(n), to(n);
+    size_t m = n;
+    if (n && cudaGraphGetEdges(g, from.data(), to.data(), &m) != cudaSuccess) return false;
+    std::unordered_map<cudaGraphNode_t, size_t> at;
+    for (size_t i = 0; i < x.size(); i++) at[x[i]] = i;
+    for (size_t i = 0; i < m; i++) out.emplace_back(at[from[i]], at[to[i]]);
+    std::sort(out.begin(), out.end());
+    return true;
+  };
+  std::vector<std::pair<size_t, size_t>> pa, pb;
+  if (!edges(a, xa, ea, pa) || !edges(b, xb, eb, pb)) return false;
+  cudaGetLastError();
+  return pa == pb;
+}
+
+// The LIE's executable back to the cache (or, when it is not cached, to
+// the engine's worker for destruction).
+void release_graph(gdl_engine *e, LieHost &L) {
+  if (L.gslot >= 0) {
+    e->gcache[L.gslot].in_use = false;
+  } else if (L.gexec) {
+    e->graveyard.push_back(L.gexec);
+  }
+  L.gexec = nullptr;
+  L.gslot = -1;
+}
+
 gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
-  if (L.gexec) {
-    cudaGraphExecDestroy(L.gexec);
-    L.gexec = nullptr;
+  release_graph(e, L);
+  L.graph_reused = false;
+  struct Swap {
+    gdl_engine *e;
+    cudaStream_t keep;
+    ~Swap() { e->s = keep; }
+  } swap{e, e->s};
+  // captured on the capture stream (the engine stream may be running the
+  // loop's first iteration)
+  e->s = e->cap_s;
+  // Hooked operators launch the caller's kernels: not cached.
+  bool cacheable = getenv("GDLOG_NO_GRAPH_CACHE") == nullptr;
+  for (const OpHost &op : L.ops) cacheable = cacheable && !op.hook;
+  cudaGraph_t iter = nullptr;
+  if (cacheable) {
+    CK(e, cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
+    Counts kc;
+    enqueue_iteration(e, L, plan, &kc, true);
+    cudaError_t r = cudaStreamEndCapture(e->s, &iter);
+    if (r != cudaSuccess) return fail(e, GDL_E_CUDA, "capture of the iteration failed: %s",
+                                      cudaGetErrorString(r));
+    size_t n = 0;
+    CK(e, cudaGraphGetNodes(iter, nullptr, &n));
+    for (size_t i = 0; i < e->gcache.size(); i++) {
+      gdl_engine::CachedGraph &c = e->gcache[i];
+      if (c.in_use || c.nodes != n || !graphs_equal(e, iter, c.body)) continue;
+      cudaGraphDestroy(iter);
+      c.in_use = true;
+      c.used = ++e->gcache_clock;
+      L.gexec = c.exec;
+      L.cond_handle = c.handle;
+      L.per_iter = c.per_iter;
+      L.gslot = (int)i;
+      L.graph_reused = true;
+      L.graph_dirty = false;
+      return GDL_OK;
+    }
   }
   cudaGraph_t g = nullptr;
-  CK(e, cudaGraphCreate(&g, 0));
+  cudaError_t r = cudaGraphCreate(&g, 0);
   cudaGraphConditionalHandle h;
-  cudaError_t r = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (r == cudaSuccess) r = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
   if (r != cudaSuccess) {
-    cudaGraphDestroy(g);
+    if (g) cudaGraphDestroy(g);
+    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(r));
   }
   cudaGraphNodeParams p = {};
@@ -1428,33 +1652,61 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   r = cudaGraphAddNode(&node, g, nullptr, 0, &p);
   if (r != cudaSuccess) {
     cudaGraphDestroy(g);
+    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "cudaGraphAddNode(conditional): %s", cudaGetErrorString(r));
   }
   cudaGraph_t body = p.conditional.phGraph_out[0];
-  // captured on the capture stream (the engine stream may be running the
-  // loop's first iteration)
-  struct Swap {
-    gdl_engine *e;
-    cudaStream_t keep;
-    ~Swap() { e->s = keep; }
-  } swap{e, e->s};
-  e->s = e->cap_s;
-  CK(e, cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
-                                      cudaStreamCaptureModeThreadLocal));
+  r = cudaStreamBeginCaptureToGraph(e->s, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
   Counts kc;
-  enqueue_iteration(e, L, plan, &kc, true);
-  cudaGraph_t captured = nullptr;
-  r = cudaStreamEndCapture(e->s, &captured);
+  if (r == cudaSuccess) {
+    enqueue_iteration(e, L, plan, &kc, true);
+    cudaGraph_t captured = nullptr;
+    r = cudaStreamEndCapture(e->s, &captured);
+  }
   if (r != cudaSuccess) {
     cudaGraphDestroy(g);
+    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "capture of the iteration failed: %s", cudaGetErrorString(r));
   }
   r = cudaGraphInstantiate(&L.gexec, g, 0);
   cudaGraphDestroy(g);
-  if (r != cudaSuccess) return fail(e, GDL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(r));
+  if (r != cudaSuccess) {
+    L.gexec = nullptr;
+    if (iter) cudaGraphDestroy(iter);
+    return fail(e, GDL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(r));
+  }
   L.cond_handle = (unsigned long long)h;
   L.per_iter = kc;
   L.graph_dirty = false;
+  if (iter) {
+    // into the cache: a free slot, else the least recently used idle one
+    size_t n = 0;
+    cudaGraphGetNodes(iter, nullptr, &n);
+    gdl_engine::CachedGraph c;
+    c.body = iter;
+    c.exec = L.gexec;
+    c.handle = L.cond_handle;
+    c.per_iter = kc;
+    c.nodes = n;
+    c.in_use = true;
+    c.used = ++e->gcache_clock;
+    int slot = -1;
+    if (e->gcache.size() >= kGraphCacheMax) {
+      for (size_t i = 0; i < e->gcache.size(); i++)
+        if (!e->gcache[i].in_use && (slot < 0 || e->gcache[i].used < e->gcache[slot].used))
+          slot = (int)i;
+    }
+    if (slot >= 0) {
+      e->graveyard.push_back(e->gcache[slot].exec);
+      cudaGraphDestroy(e->gcache[slot].body);
+      e->gcache[slot] = c;
+    } else {
+      slot = (int)e->gcache.size();
+      e->gcache.push_back(c);
+    }
+    L.gslot = slot;
+  }
   return GDL_OK;
 }
 
@@ -2108,7 +2360,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         // (empty) NEWT bitmap
         const u32 *rows = h.bmDN;
         if (!plan.delta_n[r]) {
-          TransposeArgs t{h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr, &e->recs[7], e->d_ctl};
+          TransposeArgs t = transpose_args(h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr,
+                                           &e->recs[7], e->d_ctl);
           k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
           rows = h.bmG;
         }
@@ -2288,7 +2541,7 @@ static void release_program(gdl_engine *e) {
     if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
   }
   for (LieHost &L : e->lies) {
-    if (L.gexec) e->graveyard.push_back(L.gexec);
+    release_graph(e, L);
     // stream-ordered frees (a cudaFree would wait for the whole device)
     for (void *p : {(void *)L.d_trace, (void *)L.d_lie, (void *)L.d_joinrec})
       dfree(e, p);
@@ -2309,6 +2562,10 @@ gdl_status gdl_engine_clear(gdl_engine *e) {
   CK(e, cudaStreamSynchronize(e->s));
   release_program(e);
   reap_graphs(e);
+  // the next program's requests take back this program's blocks
+  e->replay.swap(e->alloc_log);
+  e->alloc_log.clear();
+  e->replay_seen.clear();
   // everything after this is stream-ordered behind the blocks released
   CK(e, cudaMemsetAsync(e->d_rels, 0, kMaxRels * sizeof(RelDev), e->s));
   if (e->broken) {
@@ -2350,6 +2607,11 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   cudaSetDevice(e->device);
   if (e->s) cudaStreamSynchronize(e->s);
   release_program(e);
+  for (auto &g : e->gcache) {
+    e->graveyard.push_back(g.exec);
+    cudaGraphDestroy(g.body);
+  }
+  e->gcache.clear();
   for (cudaGraphExec_t x : e->graveyard) cudaGraphExecDestroy(x);
   e->graveyard.clear();
   if (e->reaper.joinable()) {
@@ -2360,8 +2622,7 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
     e->reap_cv.notify_one();
     e->reaper.join();
   }
-  for (auto &kv : e->spare) cudaFreeAsync(kv.second, e->s);
-  e->spare.clear();
+  drop_spare(e);
   if (e->s) cudaStreamSynchronize(e->s);
   for (void *p : {(void *)e->sort_buf, (void *)e->sort_offsets, (void *)e->sort_counters,
                   (void *)e->sort_status, (void *)e->crow_off, (void *)e->crow_key,
@@ -3211,10 +3472,10 @@ gdl_status gdl_relation_instance_stats(gdl_engine *e, int32_t rel, uint64_t *siz
 gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out, int32_t n_out) {
   CHECK_LIE(e, lie);
   const LieHost &L = e->lies[lie];
-  double v[8] = {L.ms,      (double)L.kernels,        (double)L.iterations,
+  double v[9] = {L.ms,      (double)L.kernels,        (double)L.iterations,
                  (double)L.retries, (double)L.graph_launches, L.setup_ms,
-                 L.grow_ms, L.graph_ms};
-  for (int i = 0; i < n_out && i < 8; i++) out[i] = v[i];
+                 L.grow_ms, L.graph_ms, L.graph_reused ? 1.0 : 0.0};
+  for (int i = 0; i < n_out && i < 9; i++) out[i] = v[i];
   return GDL_OK;
 }
 
@@ -3368,6 +3629,7 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
   DArr *d = reinterpret_cast<DArr *>(base + kNaDarr);
   LaunchRec *recs = reinterpret_cast<LaunchRec *>(base + kNaRecs);
   SortArgs a;
+  memset(&a, 0, sizeof a);
   a.keys = &d[0];
   a.buf0 = keys;
   a.buf1 = reinterpret_cast<u64 *>(base + kNaPing);
@@ -3383,6 +3645,7 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
   for (int p = 0; p < a.passes; p++)
     k_sort_pass<<<blocks(rows, kSortTile, 4), kSortBlock, kSortSmemBytes, s>>>(a, p);
   MergeArgs m;
+  memset(&m, 0, sizeof m);
   m.newt = &d[0];
   m.a = (a.passes & 1) ? a.buf1 : a.buf0;
   m.full = &d[1];

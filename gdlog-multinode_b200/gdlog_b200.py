@@ -347,11 +347,11 @@ class Lie:
             self.eng._check(getattr(self.eng.lib, self.eng.pre + "lie_seconds")(
                 self.eng.h, self.id, C.byref(s)))
             return {"ms": s.value * 1e3}
-        out = (C.c_double * 8)()
-        self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 8))
+        out = (C.c_double * 9)()
+        self.eng._check(self.eng.lib.gdl_lie_stats(self.eng.h, self.id, out, 9))
         return {"ms": out[0], "kernels": int(out[1]), "iterations": int(out[2]),
                 "retries": int(out[3]), "graph_launches": int(out[4]), "setup_ms": out[5],
-                "grow_ms": out[6], "graph_ms": out[7]}
+                "grow_ms": out[6], "graph_ms": out[7], "graph_reused": int(out[8])}
 
 
 class Engine:

@@ -93,6 +93,11 @@ gdl_status gdl_engine_destroy(gdl_engine *e);
  * buffers and memory pool, so the next program starts without device
  * allocation cost.  Relation and LIE ids restart at 0.  The reference has
  * no counterpart (its drivers leak relations at exit, test/tc.cu:80-149).
+ * A program that repeats the previous one (the same relations, loads and
+ * LIEs in the same order, as a service answering one query shape does)
+ * gets the same device blocks back, and its loops reuse the executable
+ * graphs of the previous program's (compared node by node) instead of
+ * instantiating new ones.
  * After a call failed with GDL_E_TIMEOUT (a device-side check: a bounded
  * wait gave up or a bounds check fired), every call but this one and
  * gdl_engine_destroy is refused; this one also resets the engine's device
@@ -352,7 +357,9 @@ gdl_status gdl_lie_set_trace(gdl_engine *e, int32_t lie, int32_t flag);
  * out[0] = fixpoint device milliseconds, out[1] = kernels launched,
  * out[2] = iterations, out[3] = capacity retries, out[4] = graph launches,
  * out[5] = host setup ms, out[6] = host ms growing buffers after capacity
- * overflows, out[7] = host ms capturing and instantiating graphs.
+ * overflows, out[7] = host ms capturing and instantiating graphs,
+ * out[8] = 1 if the loop's executable graph was taken from the engine's
+ * cache (an equal iteration of an earlier program, see gdl_engine_clear).
  * n_out is the number of doubles the caller provides. */
 gdl_status gdl_lie_stats(gdl_engine *e, int32_t lie, double *out,
                          int32_t n_out);
