@@ -1296,17 +1296,24 @@ __global__ void __launch_bounds__(256) k_inst_tile_pop(const u32 *bm, DenseMap m
 // digest terms of every tuple, summed per instance.
 __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map,
                                                      const u64 *tile_rank, u64 *acc) {
-  // Thread t holds words i * 256 + t of a tile (segments i = 0..7), so the
-  // ranks of its word's tuples follow from per-segment prefix sums and each
-  // thread walks its own bits: no per-tuple search.
+  // Thread t holds words i * 256 + t of a tile (segments i = 0..7).  Each
+  // thread expands its word's bits into the segment's staging buffer at
+  // their ranks (per-segment prefix sums: no per-tuple search), as 13-bit
+  // positions in the segment; then all threads hash the staged tuples
+  // together, so the hash chain, the costly part, runs without divergence.
+  // Two buffers alternate between segments with tuples (one barrier each).
+  __shared__ unsigned short s_stage[2][kBmBlock * 32];
   __shared__ u32 s_wtot[kBmWordsPerThread][kBmBlock / 32];
+  __shared__ u32 s_seg_tot[kBmWordsPerThread];
   __shared__ u32 s_seg_off[kBmWordsPerThread];
   __shared__ u64 s_red[kBmBlock / 32];
   const u64 tiles = bm_tiles(map.words);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32 nbuf = 0;
   for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
     const u32 inst = dm_tile_inst(map, t);
     const SegInfo seg = map.seg[inst];
+    const u64 row_mask = (1ull << seg.row_shift) - 1;
     const u64 w0 = t * kBmTileWords;
     u32 x[kBmWordsPerThread], ex[kBmWordsPerThread];
 #pragma unroll
@@ -1331,35 +1338,39 @@ __global__ void __launch_bounds__(256) k_inst_digest(const u32 *bm, DenseMap map
         s_wtot[threadIdx.x][w] = a;
         a += v;
       }
-      s_seg_off[threadIdx.x] = a;  // the segment's total, turned into offsets below
+      s_seg_tot[threadIdx.x] = a;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       u32 a = 0;
       for (int i = 0; i < kBmWordsPerThread; i++) {
-        const u32 v = s_seg_off[i];
         s_seg_off[i] = a;
-        a += v;
+        a += s_seg_tot[i];
       }
     }
     __syncthreads();
     u64 h_sum = 0;
-#pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
+      const u32 st = s_seg_tot[i];  // block-uniform
+      if (st == 0) continue;
+      unsigned short *stg = s_stage[nbuf++ & 1];
       u32 bits = x[i];
-      if (!bits) continue;
-      const u64 w = w0 + (u64)i * kBmBlock + threadIdx.x;
-      const u64 wl = w - seg.base_word;
-      const u64 lx = wl >> seg.row_shift;
-      const u64 lz0 = (wl & ((1ull << seg.row_shift) - 1)) << 5;
-      u64 rank = tile_rank[t] + s_seg_off[i] + s_wtot[i][warp] + ex[i];
+      u32 p = s_wtot[i][warp] + ex[i];
+      const u32 q0 = threadIdx.x * 32;
       while (bits) {
-        const int b = __ffs(bits) - 1;
+        stg[p++] = (unsigned short)(q0 + (u32)(__ffs(bits) - 1));
         bits &= bits - 1;
-        u64 h = mix64(rank++);
-        h = mix64(h ^ lx);
-        h = mix64(h ^ (lz0 + (u64)b));
-        h_sum += h;
+      }
+      __syncthreads();
+      // staged position j holds the tuple of rank r0 + j
+      const u64 r0 = tile_rank[t] + s_seg_off[i];
+      const u64 wl0 = w0 + (u64)i * kBmBlock - seg.base_word;
+      for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
+        const u32 q = stg[j];
+        const u64 wl = wl0 + (q >> 5);
+        const u64 lx = wl >> seg.row_shift;
+        const u64 lz = ((wl & row_mask) << 5) | (q & 31u);
+        h_sum += mix64(mix64(mix64(r0 + j) ^ lx) ^ lz);
       }
     }
     // one atomic per tile: the tile's terms summed over the block

@@ -213,11 +213,13 @@ struct gdl_engine {
   std::unordered_map<size_t, size_t> replay_seen;
   // Executables of iteration graphs, kept across programs (build_graph).
   struct CachedGraph {
-    cudaGraph_t body = nullptr;  // the iteration as captured, for comparison
+    cudaGraph_t graph = nullptr;  // the loop graph (owns body)
+    cudaGraph_t body = nullptr;   // the iteration as captured, for comparison
     cudaGraphExec_t exec = nullptr;
     unsigned long long handle = 0;
     Counts per_iter;
     size_t nodes = 0;
+    u64 sig = 0;  // graph_signature of body
     bool in_use = false;
     u64 used = 0;  // last use, for eviction
   };
@@ -1550,6 +1552,53 @@ bool nodes_equal(gdl_engine *e, cudaGraphNode_t a, cudaGraphNode_t b) {
   return false;  // (the iteration records no other kind of node)
 }
 
+// A 64-bit signature of a graph's nodes (the fields nodes_equal compares)
+// and its edge count: entries whose signature differs are not compared.
+u64 graph_signature(gdl_engine *e, cudaGraph_t g, size_t *n_nodes) {
+  size_t n = 0;
+  *n_nodes = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+  std::vector<cudaGraphNode_t> x(n);
+  if (n && cudaGraphGetNodes(g, x.data(), &n) != cudaSuccess) return 0;
+  u64 h = mix64(n);
+  auto put = [&h](u64 v) { h = mix64(h ^ v); };
+  auto put_bytes = [&put](const void *p, size_t len) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < len; i += 8) {
+      u64 w = 0;
+      memcpy(&w, b + i, std::min<size_t>(8, len - i));
+      put(w);
+    }
+  };
+  for (cudaGraphNode_t node : x) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(node, &t) != cudaSuccess) return 0;
+    put((u64)t);
+    if (t == cudaGraphNodeTypeKernel) {
+      cudaKernelNodeParams p;
+      if (cudaGraphKernelNodeGetParams(node, &p) != cudaSuccess) return 0;
+      put((u64)(uintptr_t)p.func);
+      put(((u64)p.gridDim.x << 32) ^ ((u64)p.gridDim.y << 16) ^ p.gridDim.z);
+      put(((u64)p.blockDim.x << 32) ^ ((u64)p.blockDim.y << 16) ^ p.blockDim.z);
+      put(p.sharedMemBytes);
+      const std::vector<size_t> &sz = param_sizes(e, p.func);
+      for (size_t i = 0; i < sz.size() && p.kernelParams; i++) put_bytes(p.kernelParams[i], sz[i]);
+    } else if (t == cudaGraphNodeTypeMemset) {
+      cudaMemsetParams m;
+      if (cudaGraphMemsetNodeGetParams(node, &m) != cudaSuccess) return 0;
+      put((u64)(uintptr_t)m.dst);
+      put(m.value);
+      put(m.width);
+    }
+  }
+  size_t ne = 0;
+  if (cudaGraphGetEdges(g, nullptr, nullptr, &ne) != cudaSuccess) return 0;
+  put(ne);
+  cudaGetLastError();
+  *n_nodes = n;
+  return h;
+}
+
 bool graphs_equal(gdl_engine *e, cudaGraph_t a, cudaGraph_t b) {
   size_t na = 0, nb = 0;
   if (cudaGraphGetNodes(a, nullptr, &na) != cudaSuccess ||
@@ -1606,41 +1655,13 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   // captured on the capture stream (the engine stream may be running the
   // loop's first iteration)
   e->s = e->cap_s;
-  // Hooked operators launch the caller's kernels: not cached.
-  bool cacheable = getenv("GDLOG_NO_GRAPH_CACHE") == nullptr;
-  for (const OpHost &op : L.ops) cacheable = cacheable && !op.hook;
-  cudaGraph_t iter = nullptr;
-  if (cacheable) {
-    CK(e, cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
-    Counts kc;
-    enqueue_iteration(e, L, plan, &kc, true);
-    cudaError_t r = cudaStreamEndCapture(e->s, &iter);
-    if (r != cudaSuccess) return fail(e, GDL_E_CUDA, "capture of the iteration failed: %s",
-                                      cudaGetErrorString(r));
-    size_t n = 0;
-    CK(e, cudaGraphGetNodes(iter, nullptr, &n));
-    for (size_t i = 0; i < e->gcache.size(); i++) {
-      gdl_engine::CachedGraph &c = e->gcache[i];
-      if (c.in_use || c.nodes != n || !graphs_equal(e, iter, c.body)) continue;
-      cudaGraphDestroy(iter);
-      c.in_use = true;
-      c.used = ++e->gcache_clock;
-      L.gexec = c.exec;
-      L.cond_handle = c.handle;
-      L.per_iter = c.per_iter;
-      L.gslot = (int)i;
-      L.graph_reused = true;
-      L.graph_dirty = false;
-      return GDL_OK;
-    }
-  }
+  // The loop: a while node whose body is one captured iteration.
   cudaGraph_t g = nullptr;
   cudaError_t r = cudaGraphCreate(&g, 0);
   cudaGraphConditionalHandle h;
   if (r == cudaSuccess) r = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
   if (r != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
-    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(r));
   }
   cudaGraphNodeParams p = {};
@@ -1652,7 +1673,6 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   r = cudaGraphAddNode(&node, g, nullptr, 0, &p);
   if (r != cudaSuccess) {
     cudaGraphDestroy(g);
-    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "cudaGraphAddNode(conditional): %s", cudaGetErrorString(r));
   }
   cudaGraph_t body = p.conditional.phGraph_out[0];
@@ -1666,47 +1686,72 @@ gdl_status build_graph(gdl_engine *e, LieHost &L, const Plan &plan) {
   }
   if (r != cudaSuccess) {
     cudaGraphDestroy(g);
-    if (iter) cudaGraphDestroy(iter);
     return fail(e, GDL_E_CUDA, "capture of the iteration failed: %s", cudaGetErrorString(r));
   }
+  // An equal iteration in the cache: its executable, and this graph goes.
+  // (Hooked operators launch the caller's kernels: never cached.)
+  bool cacheable = getenv("GDLOG_NO_GRAPH_CACHE") == nullptr;
+  for (const OpHost &op : L.ops) cacheable = cacheable && !op.hook;
+  u64 sig = 0;
+  size_t n_nodes = 0;
+  if (cacheable) {
+    sig = graph_signature(e, body, &n_nodes);
+    for (size_t i = 0; i < e->gcache.size(); i++) {
+      gdl_engine::CachedGraph &c = e->gcache[i];
+      if (c.in_use || c.nodes != n_nodes || c.sig != sig || !graphs_equal(e, body, c.body))
+        continue;
+      cudaGraphDestroy(g);
+      c.in_use = true;
+      c.used = ++e->gcache_clock;
+      L.gexec = c.exec;
+      L.cond_handle = c.handle;
+      L.per_iter = c.per_iter;
+      L.gslot = (int)i;
+      L.graph_reused = true;
+      L.graph_dirty = false;
+      return GDL_OK;
+    }
+  }
   r = cudaGraphInstantiate(&L.gexec, g, 0);
-  cudaGraphDestroy(g);
   if (r != cudaSuccess) {
     L.gexec = nullptr;
-    if (iter) cudaGraphDestroy(iter);
+    cudaGraphDestroy(g);
     return fail(e, GDL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(r));
   }
   L.cond_handle = (unsigned long long)h;
   L.per_iter = kc;
   L.graph_dirty = false;
-  if (iter) {
-    // into the cache: a free slot, else the least recently used idle one
-    size_t n = 0;
-    cudaGraphGetNodes(iter, nullptr, &n);
-    gdl_engine::CachedGraph c;
-    c.body = iter;
-    c.exec = L.gexec;
-    c.handle = L.cond_handle;
-    c.per_iter = kc;
-    c.nodes = n;
-    c.in_use = true;
-    c.used = ++e->gcache_clock;
-    int slot = -1;
-    if (e->gcache.size() >= kGraphCacheMax) {
-      for (size_t i = 0; i < e->gcache.size(); i++)
-        if (!e->gcache[i].in_use && (slot < 0 || e->gcache[i].used < e->gcache[slot].used))
-          slot = (int)i;
-    }
-    if (slot >= 0) {
-      e->graveyard.push_back(e->gcache[slot].exec);
-      cudaGraphDestroy(e->gcache[slot].body);
-      e->gcache[slot] = c;
-    } else {
-      slot = (int)e->gcache.size();
-      e->gcache.push_back(c);
-    }
-    L.gslot = slot;
+  if (!cacheable) {
+    cudaGraphDestroy(g);
+    return GDL_OK;
   }
+  // Into the cache (the graph kept for its body): a free slot, else the
+  // least recently used idle one.
+  gdl_engine::CachedGraph c;
+  c.graph = g;
+  c.body = body;
+  c.exec = L.gexec;
+  c.handle = L.cond_handle;
+  c.per_iter = kc;
+  c.nodes = n_nodes;
+  c.sig = sig;
+  c.in_use = true;
+  c.used = ++e->gcache_clock;
+  int slot = -1;
+  if (e->gcache.size() >= kGraphCacheMax) {
+    for (size_t i = 0; i < e->gcache.size(); i++)
+      if (!e->gcache[i].in_use && (slot < 0 || e->gcache[i].used < e->gcache[slot].used))
+        slot = (int)i;
+  }
+  if (slot >= 0) {
+    e->graveyard.push_back(e->gcache[slot].exec);
+    cudaGraphDestroy(e->gcache[slot].graph);
+    e->gcache[slot] = c;
+  } else {
+    slot = (int)e->gcache.size();
+    e->gcache.push_back(c);
+  }
+  L.gslot = slot;
   return GDL_OK;
 }
 
@@ -2609,7 +2654,7 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
   release_program(e);
   for (auto &g : e->gcache) {
     e->graveyard.push_back(g.exec);
-    cudaGraphDestroy(g.body);
+    cudaGraphDestroy(g.graph);
   }
   e->gcache.clear();
   for (cudaGraphExec_t x : e->graveyard) cudaGraphExecDestroy(x);
