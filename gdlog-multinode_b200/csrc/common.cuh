@@ -82,7 +82,10 @@ struct RelDev {
   u32 w_full_vis, w_delta_vis;
   u64 c_newt_n;  // NEWT count seen by the last merge step (0: empty branch)
   u32 sorted_in_scratch;
-  u32 pad;
+  // set in an iteration where a join over static FULLs, skipped because an
+  // earlier iteration of the LIE ran it, would have put tuples into this
+  // NEWT (all of them already in FULL): NEWT counts as non-empty
+  u32 newt_phantom;
   // Dense form (dense.cuh): FULL bitmap, NEWT bitmap and the dirty map of
   // NEWT (one bit per 64-word chunk), the tile counts / prefixes of this
   // relation's update scan and its record.

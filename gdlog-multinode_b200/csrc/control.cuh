@@ -20,47 +20,66 @@ struct LieDev {
   int update[kMaxRels];
   int statics[kMaxRels];
   int tmps[kMaxRels];
+  // Joins whose inner and outer are FULLs of static relations derive the
+  // same tuples in every iteration: after one iteration that ran them with
+  // both sides non-empty they add nothing new (semi-naive evaluation runs
+  // such a rule once).  Per fixpoint call: ran (committed), ran this
+  // iteration, and whether the run set any tuple.
+  u32 jonce[kMaxOps];
+  u32 jonce_pending[kMaxOps];
+  u32 produced[kMaxOps];
   u32 once[kMaxOps];          // RelationalCopy::copied (committed)
   u32 once_pending[kMaxOps];  // set by this iteration's copies
   u64 *trace;                 // [trace rows][n_update][3]
 };
 
 // Open an iteration: working visibilities from the committed ones, NEWT
-// emptied, this iteration's Copy-once flags cleared.
-__device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L) {
-  for (int i = 0; i < L->n_update; i++) {
+// emptied, this iteration's Copy-once flags cleared.  Run by one warp, lane
+// l taking entries l, l + 32, ... of each list (each relation is in one
+// list; k_commit gives every entry to the same lane).
+__device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L, int lane) {
+  const int nu = L->n_update, ns = L->n_static, nt = L->n_tmp, no = L->n_ops;
+  for (int i = lane; i < nu; i += 32) {
     RelDev &r = rels[L->update[i]];
     r.w_full_vis = r.full_vis;
     r.w_delta_vis = r.delta_vis;
     r.newt.n = 0;
   }
-  for (int i = 0; i < L->n_static; i++) {
+  for (int i = lane; i < ns; i += 32) {
     RelDev &r = rels[L->statics[i]];
     r.w_full_vis = r.full_vis;
     r.w_delta_vis = r.delta_vis;
   }
-  for (int i = 0; i < L->n_tmp; i++) {
+  for (int i = lane; i < nt; i += 32) {
     RelDev &r = rels[L->tmps[i]];
     r.w_full_vis = r.full_vis;
     r.w_delta_vis = r.delta_vis;
     r.newt.n = 0;
   }
-  for (int i = 0; i < L->n_ops; i++) L->once_pending[i] = 0;
+  for (int i = lane; i < no; i += 32) {
+    L->once_pending[i] = 0;
+    L->jonce_pending[i] = 0;
+  }
 }
 
+// One warp.
 __global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
-  if (ctl_stop(ctl) || threadIdx.x != 0) return;
-  if (ctl->test_wait) {
+  const int lane = threadIdx.x;
+  if (lane >= 32 || ctl_stop(ctl)) return;
+  int ok = 1;
+  if (lane == 0 && ctl->test_wait) {
     // gdl_engine_test_timeout: a bounded wait on a flag that nothing sets
     u32 polls = 0;
     while (!*((volatile u32 *)&ctl->never)) {
       if (++polls > ctl->test_wait) {
         atomicOr(&ctl->timeout, 1u);
-        return;
+        ok = 0;
+        break;
       }
     }
   }
-  begin_iteration(rels, L);
+  if (!__shfl_sync(0xffffffffu, ok, 0)) return;
+  begin_iteration(rels, L, lane);
 }
 
 template <class T>
@@ -72,20 +91,25 @@ __device__ __forceinline__ void dswap(T &a, T &b) {
 
 // begin_next: when the loop goes on, also open the next iteration (the
 // graph body then needs no k_begin of its own; the host launches one
-// before each graph launch).
+// before each graph launch).  One warp: lane l commits entries l, l + 32,
+// ... of each list; the loop-level decisions are warp-uniform.
 __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x;
+  if (lane >= 32) return;
   bool stop = ctl->done | ctl->pause | ctl->overflow | ctl->timeout;
   if (!stop) {
     const u64 it = ctl->iteration;
     const u64 row = it - ctl->trace_base;
-    bool fixpoint = true;
-    for (int i = 0; i < L->n_update; i++) {
+    const u64 trace_rows = ctl->trace_rows, max_it = ctl->max_iteration, stop_at = ctl->stop_at;
+    const int nu = L->n_update;
+    u64 *trace = L->trace;
+    bool grew = false;
+    for (int i = lane; i < nu; i += 32) {
       RelDev &r = rels[L->update[i]];
-      u64 *tr = (L->trace && row < ctl->trace_rows) ? L->trace + (row * L->n_update + i) * 3 : 0;
+      u64 *tr = (trace && row < trace_rows) ? trace + (row * nu + i) * 3 : 0;
       // (Dense form: the update scan has already merged NEWT into the FULL
       // bitmap in place, dense.cuh.)
-      if (r.c_newt_n == 0) {
+      if (r.c_newt_n == 0 && !r.newt_phantom) {
         // src/lie.cu:114-121: no new tuple -> a fresh, empty DELTA.
         r.delta.n = 0;
         r.delta_vis = 1;
@@ -108,7 +132,7 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
             dswap(r.full_idx, r.full_idx_next);
           }
           r.full_vis = 1;
-          fixpoint = false;
+          grew = true;
         } else {
           r.full_vis = r.w_full_vis;
         }
@@ -120,29 +144,40 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
       }
       r.newt.n = 0;
       r.c_newt_n = 0;
+      r.newt_phantom = 0;
     }
-    for (int i = 0; i < L->n_static; i++) {
+    const bool fixpoint = !__any_sync(0xffffffffu, grew);
+    for (int i = lane; i < L->n_static; i += 32) {
       RelDev &r = rels[L->statics[i]];
       r.full_vis = r.w_full_vis;
       r.delta_vis = r.w_delta_vis;
     }
-    for (int i = 0; i < L->n_tmp; i++) {
+    for (int i = lane; i < L->n_tmp; i += 32) {
       RelDev &r = rels[L->tmps[i]];
       r.newt.n = 0;  // src/lie.cu:85-87
     }
-    for (int i = 0; i < L->n_ops; i++) L->once[i] |= L->once_pending[i];
+    for (int i = lane; i < L->n_ops; i += 32) {
+      L->once[i] |= L->once_pending[i];
+      L->jonce[i] |= L->jonce_pending[i];
+    }
     const u64 next = it + 1;
-    ctl->iteration = next;
-    ctl->generation = ctl->generation + 1;
-    if (fixpoint || next > ctl->max_iteration)
-      ctl->done = 1;
-    else if (next >= ctl->stop_at)
-      ctl->pause = 1;
-    stop = ctl->done | ctl->pause;
-    if (begin_next && !stop) begin_iteration(rels, L);
+    const bool done = fixpoint || next > max_it;
+    const bool pause = !done && next >= stop_at;
+    if (lane == 0) {
+      ctl->iteration = next;
+      ctl->generation = ctl->generation + 1;
+      if (done)
+        ctl->done = 1;
+      else if (pause)
+        ctl->pause = 1;
+    }
+    stop = done || pause;
+    __syncwarp();
+    if (begin_next && !stop) begin_iteration(rels, L, lane);
     __threadfence();
   }
-  if (ctl->cond_set) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
+  if (lane == 0 && ctl->cond_set)
+    cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
 }
 
 // Point the control block at a graph's while-node condition: the loop's
@@ -151,6 +186,19 @@ __global__ void k_arm_graph(Ctl *ctl, unsigned long long handle) {
   if (threadIdx.x != 0) return;
   ctl->cond_handle = handle;
   ctl->cond_set = 1;
+}
+
+// After a loop batch, when the loop reached its fixpoint (or max_iteration)
+// with no error: clear `done`, so that the listings enqueued behind the
+// loop run.  Otherwise set `pause`, so that they return at once (the host
+// reads the loop's state from a copy taken before this, and writes the
+// control block again before the next batch).
+__global__ void k_ctl_resume(Ctl *ctl) {
+  if (threadIdx.x != 0) return;
+  if (ctl->done && !ctl->pause && !ctl->overflow && !ctl->timeout && !ctl->oob)
+    ctl->done = 0;
+  else
+    ctl->pause = 1;  // (the host restores the control block before the next batch)
 }
 
 // Pack host-layout rows (two u64 columns) into keys; raise bit 0 of *bad if

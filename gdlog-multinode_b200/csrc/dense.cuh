@@ -809,11 +809,11 @@ struct ListSmem {
   long long tile;
 };
 
-// expect_n: the bit count the host sized the list for (and keeps as its
-// size); a listing that finds another count raises the bounds flag.
+// out->n on entry: the bit count the loop kept for this version (the host
+// sizes the list for it, or the list is as large as the key domain); a
+// listing that finds another count raises the bounds flag.
 __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, int rs, DArr *out,
-                                                      u64 expect_n, Lb lb, LaunchRec *rec,
-                                                      Ctl *ctl) {
+                                                      Lb lb, LaunchRec *rec, Ctl *ctl) {
   __shared__ ListSmem sm;
   if (ctl_stop(ctl)) return;
   const u64 tiles = words / kBmTileWords;
@@ -878,9 +878,11 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
     __syncthreads();
     const u64 base = sm.base;
     if ((u64)t == tiles - 1 && threadIdx.x == 0) {
-      // never publish more rows than the list holds (the host sized it
-      // from the bitmap's count; a mismatch is an error, reported)
+      // never publish more rows than the list holds (sized from the
+      // bitmap's count, or for the whole domain; a mismatch is an error,
+      // reported).  Only this thread reads or writes out->n.
       const u64 total = base + tot;
+      const u64 expect_n = out->n;
       out->n = total <= cap ? total : cap;
       if (total > cap || total != expect_n) atomicOr(&ctl->oob, 16384u);
     }
@@ -1046,6 +1048,15 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
     join_empty_side(a, n_outer);
     return;
   }
+  if (a.once) {
+    // a join over static FULLs that an earlier iteration ran with both
+    // sides non-empty: the same tuples, all in the output's FULL already
+    if (*a.once) {
+      if (blockIdx.x == 0 && threadIdx.x == 0 && *a.produced) *a.phantom = 1;
+      return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.once_pending = 1;
+  }
   u32 *G = out_rd->bmG;
   u8 *D = out_rd->dirty;
   const Index ix = *a.inner_idx;
@@ -1055,6 +1066,7 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
   const u64 chunks = (n_outer + 31) / 32;
   const u64 nw = (u64)gridDim.x * (kFuseBlock / 32);
   u64 cand = 0;  // candidates expanded by this warp
+  bool emitted = false;
   for (u64 c = (u64)blockIdx.x * (kFuseBlock / 32) + wid; c < chunks; c += nw) {
     const u64 i = c * 32 + lane;
     u64 row = 0;
@@ -1124,6 +1136,7 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
         const u64 t = gen_join(a.sel, inner[sm.start[wid][r] + (p - sm.excl[wid][r])],
                                sm.row[wid][r]);
         if (pred_ok(a.pred, t)) {
+          emitted = true;
           if (AGG)
             dm_word(map, t, a.ctl, &w, &bit);
           else
@@ -1135,6 +1148,8 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
     __syncwarp();
     cand += total;
   }
+  // (run pieces appended for k_join_heavy_bm report from there)
+  if (a.produced && __any_sync(0xffffffffu, emitted) && lane == 0) *a.produced = 1;
   if (lane == 0) prof_add(a.ctl, kPJoinMat, cand * 12);
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, n_outer * 16);
 }
@@ -1157,6 +1172,7 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
   u64 cand = 0;
   const u32 *F = a.row_or ? a.inner_rd->bmF : nullptr;
   u64 row_bytes = 0;
+  bool emitted = false;
   for (u64 k = blockIdx.x; k < np; k += gridDim.x) {
     const u64 row = a.crow_key[k];
     const u32 s = a.crow_start[k], l = a.crow_len[k];
@@ -1167,6 +1183,7 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
       for (u32 j = threadIdx.x; j < nw; j += blockDim.x) {
         const u32 v = F[zw + j];
         if (v) {
+          emitted = true;
           asm volatile("red.global.or.b32 [%0], %1;" ::"l"(G + row + j), "r"(v) : "memory");
           if (D) D[(row + j) / kBmChunkWords] = 1;
         }
@@ -1181,6 +1198,7 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
       if (j < l) {
         const u64 t = gen_join(a.sel, inner[s + j], row);
         if (pred_ok(a.pred, t)) {
+          emitted = true;
           if (AGG)
             dm_word(map, t, a.ctl, &w, &bit);
           else
@@ -1191,6 +1209,7 @@ __global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const 
     }
     cand += l;
   }
+  if (a.produced && __any_sync(0xffffffffu, emitted) && (threadIdx.x & 31) == 0) *a.produced = 1;
   if (threadIdx.x == 0) prof_add(a.ctl, kPJoinMat, cand * 12 + row_bytes);
   if (launch_rec_finish(a.rec) && threadIdx.x == 0) {
     a.op->nc = 0;

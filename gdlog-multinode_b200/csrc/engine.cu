@@ -36,6 +36,7 @@
 #include "merge.cuh"
 #include "pull.cuh"
 #include "sort.cuh"
+#include "tma.cuh"
 
 #include <algorithm>
 #include <condition_variable>
@@ -58,6 +59,7 @@ namespace {
 constexpr u64 kMinCap = 1ull << 16;
 constexpr int kIdentityMaxBits = 22;
 constexpr u64 kMaxRows = (1ull << 30) - 4096;  // sort status keeps 30 bits
+constexpr u64 kTraceRows = 256;  // iterations a loop batch logs (one device buffer)
 
 u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
 double host_ms_since(std::chrono::steady_clock::time_point t) {
@@ -169,6 +171,12 @@ struct gdl_engine {
   RelDev *d_rels = nullptr;
   Ctl *d_ctl = nullptr;
   Ctl *h_ctl = nullptr;  // pinned
+  // Pinned copies taken behind a loop batch before its one host wait: the
+  // control block after the listings enqueued behind the loop, the batch's
+  // trace rows and the relation table.
+  Ctl *h_ctl2 = nullptr;
+  u64 *h_trace = nullptr;  // [kTraceRows][kMaxRels][3]
+  RelDev *h_rels_pin = nullptr;
   int kbits = 1;         // bits of the largest column value loaded
   // Arity 3 (common.cuh, key_col): once a relation of arity 3 exists every
   // sort covers the whole low half of the keys; k2 = bits of column 2, fixed
@@ -196,6 +204,12 @@ struct gdl_engine {
   // Graph executables of dropped LIEs: destroyed by a worker thread of the
   // engine (destroying one takes ~0.1 ms of host time that the caller's
   // next program need not wait for; none of them can be running).
+  // Tensor maps of the square-domain bitmaps for the TMA passes (tma.cuh),
+  // by (base address, domain bits); tma_ok: the driver's encoder was found
+  // (GDLOG_NO_TMA=1 keeps the LDG/STG passes of pull.cuh).
+  bool tma_ok = false;
+  void *tma_encode = nullptr;
+  std::map<std::pair<const void *, int>, CUtensorMap> tmaps;
   std::vector<cudaGraphExec_t> graveyard;
   std::mutex reap_mu;
   std::condition_variable reap_cv;
@@ -495,6 +509,30 @@ gdl_status push(gdl_engine *e) {
   CK(e, cudaMemcpyAsync(e->d_rels, e->h.data(), e->rels.size() * sizeof(RelDev),
                         cudaMemcpyHostToDevice, e->s));
   return GDL_OK;
+}
+
+// The 2-D tensor map of a square-domain bitmap (2^dk rows of 2^(dk-5)
+// words) with a box of one 256 x 256-bit tile; null if it cannot be made.
+const CUtensorMap *bm_tmap(gdl_engine *e, const u32 *bm, int dk) {
+  if (!e->tma_ok || !bm || dk < 8) return nullptr;
+  auto key = std::make_pair((const void *)bm, dk);
+  auto it = e->tmaps.find(key);
+  if (it != e->tmaps.end()) return &it->second;
+  using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                              const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                              const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {1ull << (dk - 5), 1ull << dk};
+  const cuuint64_t strides[1] = {(1ull << (dk - 5)) * 4};
+  const cuuint32_t box[2] = {8, 256};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = reinterpret_cast<Encode>(e->tma_encode)(
+      &m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<u32 *>(bm), dims, strides, box, estr,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return nullptr;
+  return &(e->tmaps[key] = m);
 }
 
 int grid_for(gdl_engine *e, u64 work, u64 per_block, int per_sm) {
@@ -811,6 +849,19 @@ struct Plan {
   // per relation: DELTA is never read as a list, so the update step is one
   // fused pass (k_bm_update_t) that writes DELTA as bitmaps only
   std::vector<char> fused;
+  // per op: its fold (k_bm_fold_t) is the first thing of the iteration to
+  // touch the output, a tmp relation, so it may overwrite that NEWT bitmap
+  // instead of ORing into it (when the bitmap has no dirty map); per tmp
+  // relation: its first op is such a fold, so its NEWT needs no clearing
+  // after the operators (k_bm_clear_dirty)
+  std::vector<char> fold_over, tmp_overwritten;
+  // per op: a join over FULLs of static relations into an update relation
+  // whose NEWT no op reads (run once per fixpoint in the dense push form,
+  // k_join_bm)
+  std::vector<char> static_once;
+  // per op: a row-gather join whose output bitmap (a transposed twin) is
+  // all zero when it starts (pull.cuh, RowsArgs::dst_zero)
+  std::vector<char> twin_zero;
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -832,6 +883,25 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.delta_n.assign(n, 0);
   p.out_twin.assign(L.ops.size(), 0);
   p.fused.assign(n, 0);
+  p.fold_over.assign(L.ops.size(), 0);
+  p.tmp_overwritten.assign(n, 0);
+  p.static_once.assign(L.ops.size(), 0);
+  p.twin_zero.assign(L.ops.size(), 0);
+  {
+    std::vector<char> is_static(n, 0), is_update(n, 0), newt_read(n, 0);
+    for (int r : L.statics) is_static[r] = 1;
+    for (int r : L.update) is_update[r] = 1;
+    for (const OpHost &op : L.ops) {
+      if (op.kind == 0 && op.outer_ver == GDL_NEWT) newt_read[op.outer] = 1;
+      if (op.kind == 2 || (op.kind == 1 && op.inner_ver == GDL_NEWT)) newt_read[op.inner] = 1;
+    }
+    for (size_t oi = 0; oi < L.ops.size(); oi++) {
+      const OpHost &op = L.ops[oi];
+      p.static_once[oi] = op.kind == 0 && !op.hook && op.inner_ver == GDL_FULL &&
+                          op.outer_ver == GDL_FULL && is_static[op.inner] && is_static[op.outer] &&
+                          is_update[op.out] && !newt_read[op.out];
+    }
+  }
   for (const OpHost &op : L.ops) {
     if (op.kind == 0 && op.outer_ver == GDL_DELTA) p.delta_list[op.outer] = 1;
     if (op.kind != 2 && op.inner_ver == GDL_DELTA) p.delta_list[op.inner] = 1;
@@ -938,6 +1008,31 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     for (size_t oi = 0; oi < L.ops.size(); oi++)
       if (L.ops[oi].out == r && !p.out_twin[oi]) only_t = false;
     p.fold_late[r] = only_t;
+  }
+  // A transposed twin is zero when the op that writes it starts: folded
+  // (and cleared) after each writer, or read and cleared by the update step
+  // when it has one writer.
+  {
+    std::vector<int> twin_writers(e->rels.size(), 0);
+    for (size_t oi = 0; oi < L.ops.size(); oi++)
+      if (p.out_twin[oi]) twin_writers[L.ops[oi].out]++;
+    for (size_t oi = 0; oi < L.ops.size(); oi++) {
+      const int r = L.ops[oi].out;
+      p.twin_zero[oi] = p.out_twin[oi] && p.rows[oi] && (!p.fold_late[r] || twin_writers[r] == 1);
+    }
+  }
+  // tmp relations whose first op in the iteration writes them through a
+  // fold (src/lie.cu:85-87: a tmp NEWT is empty when the operators start)
+  for (int r : L.tmps) {
+    for (size_t oi = 0; oi < L.ops.size(); oi++) {
+      const OpHost &op = L.ops[oi];
+      if (op.inner != r && op.outer != r && op.out != r) continue;
+      if (op.out == r && op.inner != r && op.outer != r && p.out_twin[oi] && !p.fold_late[r]) {
+        p.fold_over[oi] = 1;
+        p.tmp_overwritten[r] = 1;
+      }
+      break;
+    }
   }
 }
 
@@ -1047,6 +1142,49 @@ void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
   }
 }
 
+// dst |= transpose(src) (or := with over), src cleared: the TMA pass
+// (tma.cuh) when both bitmaps have tensor maps, else the LDG/STG pass.
+void launch_fold(gdl_engine *e, u32 *src, u32 *dst, u8 *dirty, int dk, int over, Counts *kc,
+                 cudaStream_t s) {
+  const u64 side = 1ull << (dk - kPullMinBits);
+  const CUtensorMap *ms = bm_tmap(e, src, dk), *md = bm_tmap(e, dst, dk);
+  if (ms && md) {
+    FoldMaps m;
+    m.src = *ms;
+    m.dst = *md;
+    PLAUNCH(kc, kPBitmap,
+            k_bm_fold_tma<<<grid_for(e, side * side, 1, 2), kTrBlock, fold_tma_smem(), s>>>(
+                m, dirty, dk, over, e->d_ctl));
+    return;
+  }
+  PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
+                            src, dst, dirty, dk, over, e->d_ctl));
+}
+
+// The fused update step of relation r (k_bm_update_t): NEWT from its
+// transposed twin gt or its rows, DELTA written as rows dn and/or
+// transposed dt; the TMA pass when every bitmap has a tensor map.
+void launch_update_t(gdl_engine *e, const BmScanArgs &a, int r, u32 *gt, u32 *dn, u32 *dt,
+                     int dk, Counts *kc, cudaStream_t s) {
+  const RelDev &h = e->h[r];
+  const u64 side = 1ull << (dk - kPullMinBits);
+  const CUtensorMap *mn = bm_tmap(e, gt ? gt : h.bmG, dk), *mf = bm_tmap(e, h.bmF, dk);
+  const CUtensorMap *mdn = dn ? bm_tmap(e, dn, dk) : mf, *mdt = dt ? bm_tmap(e, dt, dk) : mf;
+  if (mn && mf && mdn && mdt) {
+    UpdMaps m;
+    m.nsrc = *mn;
+    m.f = *mf;
+    m.dn = *mdn;
+    m.dt = *mdt;
+    PLAUNCH(kc, kPBitmap,
+            k_bm_update_tma<<<grid_for(e, side * side, 1, 2), kTrBlock, upd_tma_smem(dt != nullptr),
+                              s>>>(a, m, dk, gt != nullptr, dn != nullptr, dt != nullptr));
+    return;
+  }
+  PLAUNCH(kc, kPBitmap,
+          k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(a, dt, dk, gt, dn));
+}
+
 // In-edges of relation r's FULL list over 2^dk ids (k_inv_*, pull.cuh).
 gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   RelHost &rh = e->rels[r];
@@ -1072,14 +1210,11 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
   const DArr *list = &e->d_rels[r].full;
   k_inv_count<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, dk, e->d_ctl);
-  k_inv_scan<<<1, 1024, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
+  // edge offsets, fill cursors and the pieces of work, in one block
+  k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, rh.inv_poff,
+                                           rh.inv_pieces, dk);
   k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
                                                        dk);
-  // the pieces of work: counts per y (into inv_cur), offsets, pieces
-  k_inv_piece_count<<<grid_for(e, ids, 256, 8), 256, 0, e->s>>>(rh.inv_off, rh.inv_cur, dk);
-  k_inv_scan<<<1, 1024, 0, e->s>>>(rh.inv_cur, rh.inv_poff, rh.inv_cur, dk);
-  k_inv_piece_fill<<<grid_for(e, ids, 256, 8), 256, 0, e->s>>>(rh.inv_off, rh.inv_poff,
-                                                               rh.inv_pieces, dk);
   CK(e, cudaGetLastError());
   return GDL_OK;
 }
@@ -1220,13 +1355,12 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         const RelDev &out = e->h[op.out];
         ra.dst = plan.out_twin[oi] ? out.bmOT : out.bmG;
         ra.dirty = plan.out_twin[oi] ? nullptr : out.dirty;
+        ra.dst_zero = plan.twin_zero[oi];
         ra.dk = L.dk;
         launch_rows(e, ra, kc);
-        if (plan.out_twin[oi] && !plan.fold_late[op.out]) {
-          const u64 side = 1ull << (L.dk - kPullMinBits);
-          PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                    out.bmOT, out.bmG, out.dirty, L.dk, e->d_ctl));
-        }
+        if (plan.out_twin[oi] && !plan.fold_late[op.out])
+          launch_fold(e, out.bmOT, out.bmG, out.dirty, L.dk, plan.fold_over[oi] && !out.dirty, kc,
+                      s);
         continue;
       }
       if (plan.pull[oi]) {
@@ -1250,8 +1384,8 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
                     a, plan.pull_t[oi] ? out.bmOT : out.bmG,
                     plan.pull_t[oi] ? nullptr : out.dirty, OT, L.dk));
         if (plan.pull_t[oi] && !plan.fold_late[op.out])
-          PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                    out.bmOT, out.bmG, out.dirty, L.dk, e->d_ctl));
+          launch_fold(e, out.bmOT, out.bmG, out.dirty, L.dk, plan.fold_over[oi] && !out.dirty, kc,
+                      s);
         continue;
       }
       u64 outer_cap = std::max({oh.delta.cap, oh.delta_next.cap, oh.full.cap, oh.full_next.cap,
@@ -1261,6 +1395,13 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       b.rec = &e->recs[1];
       if (dense && e->dense_join_passes == 1) {
         const int jg = grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm);
+        if (plan.static_once[oi]) {
+          a.once = &L.d_lie->jonce[oi];
+          a.once_pending = &L.d_lie->jonce_pending[oi];
+          a.produced = &L.d_lie->produced[oi];
+          a.phantom = &R[op.out].newt_phantom;
+          b.produced = a.produced;
+        }
         if (e->join_aggregate == 2) {
           PLAUNCH(kc, kPJoinMat, k_join_bm<true><<<jg, kFuseBlock, 0, s>>>(a, &R[op.out], map));
           PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<true><<<(int)e->sms * 4, kFuseBlock, 0, s>>>(
@@ -1413,18 +1554,18 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
     }
     for (const BmScanArgs &a : fused) {
       const int r = (int)(a.rd - R);
-      const u64 side = 1ull << (L.dk - kPullMinBits);
-      PLAUNCH(kc, kPBitmap, k_bm_update_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
-                                a, plan.delta_t[r] ? e->h[r].bmDT : nullptr, L.dk,
-                                plan.fold_late[r] ? e->h[r].bmOT : nullptr,
-                                plan.delta_n[r] ? e->h[r].bmDN : nullptr));
+      launch_update_t(e, a, r, plan.fold_late[r] ? e->h[r].bmOT : nullptr,
+                      plan.delta_n[r] ? e->h[r].bmDN : nullptr,
+                      plan.delta_t[r] ? e->h[r].bmDT : nullptr, L.dk, kc, s);
     }
     for (const BmScanArgs &a : scans) launch_scan_write(e, a, kc);
-    // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87)
+    // tmp relations: NEWT is cleared after the operators (src/lie.cu:85-87),
+    // unless the next iteration's first op overwrites it whole
     const u64 tiles = L.map.words / kBmTileWords;
     for (int r : L.tmps)
-      PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
-                                &R[r], L.map, e->d_ctl));
+      if (!(plan.tmp_overwritten[r] && !e->h[r].dirty))
+        PLAUNCH(kc, kPBitmap, k_bm_clear_dirty<<<grid_for(e, tiles, 1, 8), 256, 0, s>>>(
+                                  &R[r], L.map, e->d_ctl));
   }
   for (int r : L.update) {
     const RelDev &rh = e->h[r];
@@ -1821,6 +1962,10 @@ gdl_status presize_lists(gdl_engine *e, LieHost &L, const Plan &plan, u64 cap) {
         TRY(ensure_index(e, h.full_idx, h.full.cap));
         TRY(ensure_index(e, h.full_idx_next, h.full_next.cap));
       }
+    } else if (!e->instances) {
+      // FULL listed once when the LIE ends: sized now, so that the listing
+      // can be enqueued behind the loop without a host round trip
+      TRY(ensure_arr(e, h.full, cap, true));
     }
     if (plan.delta_idx[r]) {
       TRY(ensure_index(e, h.delta_idx, h.delta.cap));
@@ -1893,6 +2038,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     h.delta_vis = 1;
     rh.delta_sorted = rh.raw_is_full;
     h.newt.n = 0;
+    h.newt_phantom = 0;
   }
   for (int r : L.tmps) {
     RelDev &h = e->h[r];
@@ -1972,7 +2118,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     u64 lists = 0;
     for (int r : L.update)
       lists += 2 + ((plan.newt_list[r] || plan.acopy_src[r]) ? 1 : 0) +
-               (plan.full_list[r] ? 2 : 0);
+               (plan.full_list[r] ? 2 : (e->instances ? 0 : 1));
     lists += L.tmps.size();
     const u64 domain = words * 32;
     const u64 cap = std::min<u64>(
@@ -2103,7 +2249,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   for (size_t i = 0; i < L.statics.size(); i++) ld.statics[i] = L.statics[i];
   for (size_t i = 0; i < L.tmps.size(); i++) ld.tmps[i] = L.tmps[i];
   // trace buffer: rows for one batch
-  const u64 trace_rows = 256;
+  const u64 trace_rows = kTraceRows;
   if (!L.d_trace) TRY(dalloc(e, (void **)&L.d_trace, trace_rows * kMaxRels * 3 * sizeof(u64)));
   ld.trace = L.d_trace;
   CK(e, cudaMemcpyAsync(L.d_lie, &ld, offsetof(LieDev, once), cudaMemcpyHostToDevice, e->s));
@@ -2132,7 +2278,47 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   const bool use_graph = getenv("GDLOG_NO_GRAPH") == nullptr && !e->profile;
   u64 batch = 4;
   bool first_batch = true;
+  bool tail_listed = false;
   e->mirror_fresh = false;
+  // The FULL lists kept only as bitmaps during the loop are listed behind
+  // every loop batch, before the host waits for it (k_ctl_resume lets the
+  // listings run only once the loop ended without error), when each list
+  // was sized for the whole key domain at setup; the batch's one wait then
+  // also brings back the listings' checks and the relation table.
+  bool spec_list = L.dense && !e->instances;
+  if (spec_list) {
+    const u64 domain = L.map.words * 32;
+    bool any_lazy = false;
+    for (int r : L.update)
+      if (e->h[r].full_lazy) {
+        any_lazy = true;
+        if (e->h[r].full.cap < domain) spec_list = false;
+      }
+    spec_list = spec_list && any_lazy;
+    if (spec_list) TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, L.map.words / kBmTileWords + 2));
+  }
+  auto enqueue_tail = [&](u64 it0, u64 stop_at) -> gdl_status {
+    CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    if (L.trace_on) {
+      const u64 rows = std::min<u64>(stop_at - it0, trace_rows) * L.update.size() * 3;
+      if (rows)
+        CK(e, cudaMemcpyAsync(e->h_trace, ld.trace, rows * sizeof(u64), cudaMemcpyDeviceToHost,
+                              e->s));
+    }
+    if (!spec_list) return GDL_OK;
+    k_ctl_resume<<<1, 32, 0, e->s>>>(e->d_ctl);
+    for (int r : L.update)
+      if (e->h[r].full_lazy)
+        k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
+            e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
+            e->d_ctl);
+    CK(e, cudaGetLastError());
+    CK(e, cudaMemcpyAsync(e->h_ctl2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    CK(e, cudaEventRecord(e->ev1, e->s));
+    CK(e, cudaMemcpyAsync(e->h_rels_pin, e->d_rels, e->rels.size() * sizeof(RelDev),
+                          cudaMemcpyDeviceToHost, e->s));
+    return GDL_OK;
+  };
   while (true) {
     c.pause = 0;
     c.stop_at = c.iteration + (use_graph ? std::min<u64>(trace_rows, 1u << 20) : batch);
@@ -2204,11 +2390,13 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       }
       CK(e, cudaGetLastError());
     }
-    CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    TRY(enqueue_tail(it0, c.stop_at));
     CK(e, cudaStreamSynchronize(e->s));
     prof_collect(e);
     c = *e->h_ctl;
     e->generation = c.generation;
+    // the listings behind the loop ran (k_ctl_resume's condition)
+    tail_listed = spec_list && c.done && !c.pause && !c.overflow && !c.timeout && !c.oob;
     const u64 ran = c.iteration - it0;
     // In a graph, the body runs once per committed iteration plus once for
     // an iteration that overflowed (after a first iteration on the stream,
@@ -2224,10 +2412,9 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     L.kernels += bodies * (u64)L.per_iter.total;
     for (int k = 0; k < kPKinds; k++) e->prof_launches[k] += bodies * (u64)L.per_iter.kind[k];
     if (L.trace_on && ran) {
-      std::vector<u64> rows(ran * L.update.size() * 3);
-      CK(e, cudaMemcpyAsync(rows.data(), ld.trace, rows.size() * sizeof(u64),
-                            cudaMemcpyDeviceToHost, e->s));
-      CK(e, cudaStreamSynchronize(e->s));
+      // (a batch commits at most stop_at - it0 <= trace_rows iterations: all
+      // their rows came back with the batch's wait)
+      const u64 *rows = e->h_trace;
       for (u64 t = 0; t < ran; t++)
         for (size_t i = 0; i < L.update.size(); i++) {
           const u64 *x = &rows[(t * L.update.size() + i) * 3];
@@ -2266,9 +2453,12 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           for (int r : *v) {
             CK(e, cudaMemsetAsync(e->h[r].bmG, 0, words * 4, e->s));
             CK(e, cudaMemsetAsync(e->h[r].bmD, 0, words / kBmChunkWords, e->s));
+            // (and the transposed twins, zero between their uses)
+            if (e->h[r].bmOT) CK(e, cudaMemsetAsync(e->h[r].bmOT, 0, words * 4, e->s));
           }
       }
       if (resume) {
+        tail_listed = false;
         // Re-run only the update step and the commit of the iteration that
         // overflowed, launch by launch, until its lists fit.
         while (true) {
@@ -2326,12 +2516,33 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   }
   e->mirror_fresh = false;  // (a pull while growing buffers preceded more launches)
   bool listed = false;
+  // ev1 was recorded behind the listings of the last batch, before its wait
+  bool ev1_recorded = false;
+  const Ctl *lc = e->h_ctl;  // the listings' device checks
+  if (L.dense && tail_listed) {
+    // FULL lists written behind the loop; the table came back with them
+    if (e->h_ctl2->timeout || e->h_ctl2->oob) {
+      e->broken = true;
+      return fail(e, GDL_E_TIMEOUT, "listing FULL after the loop failed (timeout=%u oob=%u)",
+                  e->h_ctl2->timeout, e->h_ctl2->oob);
+    }
+    memcpy(e->h.data(), e->h_rels_pin, e->rels.size() * sizeof(RelDev));
+    e->mirror_fresh = true;
+    for (RelHost &rh : e->rels) rh.stale = false;
+    ev1_recorded = true;
+    for (int r : L.update) e->h[r].full_lazy = 0;
+  }
   if (L.dense) {
     // FULL lists that were not kept during the loop are written from the
     // FULL bitmaps, sorted (bit order is tuple order).
     const u64 kept_iteration = c.iteration;
-    TRY(reset_ctl(e));  // clear done/pause so that the scans below run
-    TRY(pull(e));
+    TRY(refresh(e));
+    bool ctl_reset = false;
+    auto resume_ctl = [&]() -> gdl_status {  // clear done/pause so that the scans below run
+      if (!ctl_reset) TRY(reset_ctl(e));
+      ctl_reset = true;
+      return GDL_OK;
+    };
     bool any = false;
     for (int r : L.update)
       if (e->h[r].full_lazy) {
@@ -2354,6 +2565,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         any = true;
       }
     if (any) {
+      TRY(resume_ctl());
       TRY(push(e));
       Counts kc;
       if (!e->instances) TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles,
@@ -2363,8 +2575,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         if (!e->instances) {
           // square domain: one pass (k_bm_list)
           k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->h[r].full.n,
-              e->lb_list, &e->recs[8], e->d_ctl);
+              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
+              e->d_ctl);
           continue;
         }
         BmScanArgs a = scan_none(L.map);
@@ -2378,6 +2590,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       // holds; the batched form's scans need the table read back.
       if (e->instances) TRY(pull(e));
       listed = true;
+      ev1_recorded = false;
     }
     // DELTA lists that were not kept (read only transposed by pull-form
     // joins) and are not empty (max_iteration ended the loop): transposed
@@ -2395,6 +2608,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         any_delta = true;
       }
     if (any_delta) {
+      TRY(resume_ctl());
       TRY(push(e));
       TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, L.map.words / kBmTileWords + 2));
       const u64 side = 1ull << (L.dk - kPullMinBits);
@@ -2411,16 +2625,19 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           rows = h.bmG;
         }
         k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, h.delta.n, e->lb_list,
-            &e->recs[8], e->d_ctl);
+            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, e->lb_list, &e->recs[8],
+            e->d_ctl);
         if (!plan.delta_n[r]) CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
       }
       CK(e, cudaGetLastError());
       listed = true;
+      ev1_recorded = false;
     }
     // the listings' device checks, read back with the end of the fixpoint
-    if (listed)
+    if (listed && !ev1_recorded)
       CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+    else
+      listed = false;  // (the listings behind the loop were checked above)
     for (RelDev &h : e->h) {
       h.dense = h.full_lazy = 0;
       h.dirty = nullptr;
@@ -2428,12 +2645,12 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     TRY(push(e));
     c.iteration = kept_iteration;
   }
-  CK(e, cudaEventRecord(e->ev1, e->s));
+  if (!ev1_recorded) CK(e, cudaEventRecord(e->ev1, e->s));
   CK(e, cudaEventSynchronize(e->ev1));
-  if (listed && (e->h_ctl->timeout || e->h_ctl->oob)) {
+  if (listed && (lc->timeout || lc->oob)) {
     e->broken = true;
     return fail(e, GDL_E_TIMEOUT, "listing FULL/DELTA after the loop failed (timeout=%u oob=%u)",
-                e->h_ctl->timeout, e->h_ctl->oob);
+                lc->timeout, lc->oob);
   }
   float ms = 0;
   CK(e, cudaEventElapsedTime(&ms, e->ev0, e->ev1));
@@ -2544,6 +2761,9 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
                                (int)(pull_acc_words(16) * 4))) ||
       bad(cudaMalloc(&e->d_rels, kMaxRels * sizeof(RelDev))) ||
       bad(cudaMalloc(&e->d_ctl, sizeof(Ctl))) || bad(cudaMallocHost(&e->h_ctl, sizeof(Ctl))) ||
+      bad(cudaMallocHost(&e->h_ctl2, sizeof(Ctl))) ||
+      bad(cudaMallocHost(&e->h_trace, kTraceRows * kMaxRels * 3 * sizeof(u64))) ||
+      bad(cudaMallocHost(&e->h_rels_pin, kMaxRels * sizeof(RelDev))) ||
       bad(cudaMalloc(&e->recs, 16 * sizeof(LaunchRec))) ||
       bad(cudaMalloc(&e->d_tmp, 4 * sizeof(DArr))) || bad(cudaMalloc(&e->d_u64, 4 * sizeof(u64))) ||
       bad(cudaMalloc(&e->d_u32, 4 * sizeof(u32))) ||
@@ -2561,6 +2781,22 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
       bad(cudaStreamSynchronize(e->s))) {
     gdl_engine_destroy(e);
     return GDL_E_CUDA;
+  }
+  // TMA passes: the driver's tensor-map encoder, and their shared memory
+  if (!getenv("GDLOG_NO_TMA")) {
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn &&
+        cudaFuncSetAttribute(k_bm_update_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)upd_tma_smem(1)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_bm_fold_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fold_tma_smem()) == cudaSuccess) {
+      e->tma_encode = fn;
+      e->tma_ok = true;
+    }
+    cudaGetLastError();
   }
   *out = e;
   return GDL_OK;
@@ -2685,6 +2921,9 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->d_ctl})
     if (p) cudaFree(p);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
+  if (e->h_ctl2) cudaFreeHost(e->h_ctl2);
+  if (e->h_trace) cudaFreeHost(e->h_trace);
+  if (e->h_rels_pin) cudaFreeHost(e->h_rels_pin);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->ev_first) cudaEventDestroy(e->ev_first);

@@ -77,6 +77,13 @@ struct JoinArgs {
   // arity 3 or computed columns: tuples come from gen (list form only)
   int generic;
   GenSpec gen;
+  // A join over static FULLs (push form, dense): `once` = ran in an earlier
+  // iteration of this fixpoint, `once_pending` = ran in this one, `produced`
+  // = that run set a tuple, `phantom` = the output's RelDev::newt_phantom.
+  const u32 *once;
+  u32 *once_pending;
+  u32 *produced;
+  u32 *phantom;
 };
 
 __device__ __forceinline__ u64 join_out(const JoinArgs &a, u64 inner, u64 outer) {

@@ -110,7 +110,10 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
     }
 #pragma unroll
     for (int i = 0; i < 8; i++) bits += __popc(v[i]);
+    // (a tile's reads of s_t are ordered before the next tile's writes by
+    // the next tile's __syncthreads_or)
     const bool tile_any = __syncthreads_or(any);
+    uint4 *d = reinterpret_cast<uint4 *>(a.dst + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
     if (tile_any) {
 #pragma unroll
       for (int i = 0; i < 8; i++) {
@@ -118,10 +121,7 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
         // the input rows 256 tr + 32 wid + l = output word 8 tr + wid
         s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
       }
-    }
-    __syncthreads();
-    uint4 *d = reinterpret_cast<uint4 *>(a.dst + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
-    if (tile_any) {
+      __syncthreads();
       const u32 *q = s_t[threadIdx.x];
       d[0] = make_uint4(q[0], q[1], q[2], q[3]);
       d[1] = make_uint4(q[4], q[5], q[6], q[7]);
@@ -130,7 +130,6 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
       d[1] = make_uint4(0, 0, 0, 0);
     }
     moved += 32;
-    __syncthreads();
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -160,7 +159,7 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_transpose(TransposeArgs a) {
 // every join that writes the relation has a transposed output and nothing
 // reads its NEWT during the iteration, NEWT is only that transposed twin
 // (never folded): it is read transposed, tile by tile, and cleared.
-__global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt, int dk, u32 *gt,
+__global__ void __launch_bounds__(kTrBlock, 4) k_bm_update_t(BmScanArgs a, u32 *dt, int dk, u32 *gt,
                                                           u32 *dn) {
   __shared__ u32 s_t[256][9];
   __shared__ unsigned long long s_cnt[2];
@@ -190,20 +189,20 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
   u64 t = blockIdx.x;
   u32 nx[8];
   if (t < tiles) load8(nsrc + newt_at(t), nx);
+  // A tile's reads of s_t are ordered before the next writes of s_t by the
+  // __syncthreads_or that precedes every write.
   for (; t < tiles; t += gridDim.x) {
     const u64 tr = t / per, tc = t % per;
     const u64 src = ((tr * 256 + (u64)threadIdx.x) << rs) + tc * 8;
-    u32 g[8], d[8], cur[8];
+    u32 g[8], d[8], cur[8], f[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) cur[i] = nx[i];
     if (t + gridDim.x < tiles) load8(nsrc + newt_at(t + gridDim.x), nx);
+    bool have_f = false;
     if (gt) {
       // NEWT's tile (tr, tc) is the transpose of gt's tile (tc, tr)
       const u64 tsrc = ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8;
-      u32 v[8];
-#pragma unroll
-      for (int i = 0; i < 8; i++) v[i] = cur[i];
-      const bool any_v = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
+      const bool any_v = (cur[0] | cur[1] | cur[2] | cur[3] | cur[4] | cur[5] | cur[6] | cur[7]) != 0u;
       moved += 32;
       if (any_v) {
         uint4 *pv = reinterpret_cast<uint4 *>(gt + tsrc);
@@ -212,12 +211,15 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
         moved += 32;
       }
       if (__syncthreads_or(any_v)) {
+        // FULL's words of the tile load while it is transposed
+        load8(F + src, f);
+        have_f = true;
+        moved += 32;
 #pragma unroll
-        for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+        for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(cur[i], lane);
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < 8; i++) g[i] = s_t[threadIdx.x][i];
-        __syncthreads();
       } else {
 #pragma unroll
         for (int i = 0; i < 8; i++) g[i] = 0;
@@ -232,17 +234,20 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
 #pragma unroll
     for (int i = 0; i < 8; i++) d[i] = 0;
     if (any_g) {
-      u32 f[8];
-      load8(F + src, f);
+      if (!have_f) {
+        load8(F + src, f);
+        moved += 32;
+      }
       uint4 *pf = reinterpret_cast<uint4 *>(F + src);
       pf[0] = make_uint4(f[0] | g[0], f[1] | g[1], f[2] | g[2], f[3] | g[3]);
       pf[1] = make_uint4(f[4] | g[4], f[5] | g[5], f[6] | g[6], f[7] | g[7]);
+      moved += 32;
       if (!gt) {
         uint4 *pg = reinterpret_cast<uint4 *>(G + src);
         pg[0] = make_uint4(0, 0, 0, 0);
         pg[1] = make_uint4(0, 0, 0, 0);
+        moved += 32;
       }
-      moved += gt ? 64 : 96;
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         d[i] = g[i] & ~f[i];
@@ -260,13 +265,11 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
     }
     if (dt) {  // (uniform over the launch)
       const bool tile_any = __syncthreads_or(any);
+      uint4 *o = reinterpret_cast<uint4 *>(dt + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
       if (tile_any) {
 #pragma unroll
         for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(d[i], lane);
-      }
-      __syncthreads();
-      uint4 *o = reinterpret_cast<uint4 *>(dt + ((tc * 256 + (u64)threadIdx.x) << rs) + tr * 8);
-      if (tile_any) {
+        __syncthreads();
         const u32 *q = s_t[threadIdx.x];
         o[0] = make_uint4(q[0], q[1], q[2], q[3]);
         o[1] = make_uint4(q[4], q[5], q[6], q[7]);
@@ -275,7 +278,6 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_update_t(BmScanArgs a, u32 *dt,
         o[1] = make_uint4(0, 0, 0, 0);
       }
       moved += 32;
-      __syncthreads();
     }
   }
 #pragma unroll
@@ -497,45 +499,6 @@ __global__ void __launch_bounds__(256) k_inv_count(const DArr *list, u32 *cnt, i
   }
 }
 
-// Exclusive scan of the 2^dk counts into off[0..2^dk] (one block), and the
-// fill cursors (a copy of the offsets).
-__global__ void __launch_bounds__(1024) k_inv_scan(const u32 *cnt, u32 *off, u32 *cur, int dk) {
-  __shared__ u32 s_sum[32];
-  const u32 n = 1u << dk;
-  const u32 per = (n + blockDim.x - 1) / blockDim.x;
-  const u32 b = threadIdx.x * per;
-  u32 local = 0;
-  for (u32 i = 0; i < per && b + i < n; i++) local += cnt[b + i];
-  // block exclusive scan of `local`
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  u32 x = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const u32 y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_sum[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    u32 v = lane < (int)(blockDim.x / 32) ? s_sum[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const u32 y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
-    }
-    s_sum[lane] = v;
-  }
-  __syncthreads();
-  u32 run = (w ? s_sum[w - 1] : 0) + x - local;
-  for (u32 i = 0; i < per && b + i < n; i++) {
-    const u32 c = cnt[b + i];  // read first: cur may be the count array
-    off[b + i] = run;
-    cur[b + i] = run;
-    run += c;
-  }
-  if (threadIdx.x == blockDim.x - 1) off[n] = s_sum[blockDim.x / 32 - 1];
-}
-
 // Scatter: the in-edges of y at [off[y], off[y+1]), each with its y (the
 // order inside a y does not matter: the gather ORs).
 __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, u32 *ys,
@@ -554,26 +517,64 @@ __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u3
 
 // Units of work of the row-gather join: the in-edges of one y, cut into
 // pieces of at most kRowsPiece (a y with more in-edges than that is shared
-// by several warps, which OR their parts into the output row).  First the
-// number of pieces per y, then (after k_inv_scan of those counts) the
-// pieces themselves as (first edge, end edge).
+// by several warps, which OR their parts into the output row).
 constexpr u32 kRowsPiece = 32;
+constexpr int kInvBlock = 1024;
+constexpr int kInvPer = 8;  // consecutive ids per thread and chunk
 
-__global__ void __launch_bounds__(256) k_inv_piece_count(const u32 *off, u32 *cnt, int dk) {
-  const u32 n = 1u << dk;
-  for (u32 y = blockIdx.x * blockDim.x + threadIdx.x; y < n; y += gridDim.x * blockDim.x) {
-    const u32 d = off[y + 1] - off[y];
-    cnt[y] = (d + kRowsPiece - 1) / kRowsPiece;
+// One block: from the in-degree counts cnt[y] (2^dk of them), the edge
+// offsets off[0..2^dk] (and the fill cursors cur, a copy; cur may be cnt),
+// the piece offsets poff[0..2^dk] and the pieces themselves as
+// (first edge, end edge).  Chunks of kInvBlock x kInvPer ids, each thread
+// kInvPer consecutive ones read and written as 16-byte vectors; the two
+// prefix sums (edges low, pieces high) share one 64-bit block scan.
+__global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *off, u32 *cur,
+                                                           u32 *poff, uint2 *pieces, int dk) {
+  __shared__ u64 s_warp[kInvBlock / 32];
+  const u32 n = 1u << dk;  // a multiple of kInvPer
+  u64 carry = 0;           // (pieces << 32) | edges of the chunks before
+  for (u32 c0 = 0; c0 < n; c0 += kInvBlock * kInvPer) {
+    const u32 b = c0 + kInvPer * threadIdx.x;
+    u32 v[kInvPer];
+    if (b < n) {
+      const uint4 x = reinterpret_cast<const uint4 *>(cnt + b)[0];
+      const uint4 y = reinterpret_cast<const uint4 *>(cnt + b)[1];
+      v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
+      v[4] = y.x, v[5] = y.y, v[6] = y.z, v[7] = y.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < kInvPer; i++) v[i] = 0;
+    }
+    u64 local = 0;
+#pragma unroll
+    for (int i = 0; i < kInvPer; i++)
+      local += ((u64)((v[i] + kRowsPiece - 1) / kRowsPiece) << 32) | v[i];
+    u64 tot;
+    const u64 ex = block_excl_scan<kInvBlock>(local, s_warp, &tot) + carry;
+    carry += tot;
+    if (b >= n) continue;
+    u32 e = (u32)ex, p = (u32)(ex >> 32);
+    u32 o[kInvPer], po[kInvPer];
+#pragma unroll
+    for (int i = 0; i < kInvPer; i++) {
+      o[i] = e;
+      po[i] = p;
+      const u32 end = e + v[i];
+      for (u32 s = e; s < end; s += kRowsPiece) pieces[p++] = make_uint2(s, min(s + kRowsPiece, end));
+      e = end;
+    }
+    uint4 *po4 = reinterpret_cast<uint4 *>(off + b), *pc4 = reinterpret_cast<uint4 *>(cur + b),
+          *pp4 = reinterpret_cast<uint4 *>(poff + b);
+    po4[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    po4[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    pc4[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    pc4[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    pp4[0] = make_uint4(po[0], po[1], po[2], po[3]);
+    pp4[1] = make_uint4(po[4], po[5], po[6], po[7]);
   }
-}
-
-__global__ void __launch_bounds__(256) k_inv_piece_fill(const u32 *off, const u32 *pieces_off,
-                                                        uint2 *pieces, int dk) {
-  const u32 n = 1u << dk;
-  for (u32 y = blockIdx.x * blockDim.x + threadIdx.x; y < n; y += gridDim.x * blockDim.x) {
-    const u32 s = off[y], e = off[y + 1];
-    u32 at = pieces_off[y];
-    for (u32 i = s; i < e; i += kRowsPiece) pieces[at++] = make_uint2(i, min(i + kRowsPiece, e));
+  if (threadIdx.x == 0) {
+    off[n] = (u32)carry;
+    poff[n] = (u32)(carry >> 32);
   }
 }
 
@@ -588,6 +589,7 @@ struct RowsArgs {
   const uint2 *pieces;
   u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
   u8 *dirty;           // dirty map of dst, or null
+  int dst_zero;        // dst is all zero when the launch starts
   int dk;
 };
 
@@ -605,7 +607,10 @@ __device__ __forceinline__ void rows_flush(const RowsArgs &a, u32 y, bool whole,
     const uint4 v = acc[j];
     if ((v.x | v.y | v.z | v.w) == 0u) continue;
     const u32 q = (u32)j * 32 + lane;
-    if (whole) {
+    if (whole && a.dst_zero) {
+      // this warp owns row y in this launch, and the row is zero: a store
+      d[q] = v;
+    } else if (whole) {
       // this warp owns row y in this launch: plain read-OR-write
       uint4 o = d[q];
       o.x |= v.x;
@@ -676,27 +681,32 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
     uint4 acc[V];
 #pragma unroll
     for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
-    // this piece's keys, one per lane; two rows in flight per step
+    // this piece's keys, one per lane; kFly rows in flight per step (all
+    // their loads issued before the ORs)
+    constexpr int kFly = V <= 4 ? 4 : 2;
     const u32 m = pc.y - pc.x;
     const u32 my_k = lane < (int)m ? a.inv_keys[pc.x + lane] : 0;
     u32 i = 0;
-    for (; i + 1 < m; i += 2) {
-      const u32 k0 = __shfl_sync(0xffffffffu, my_k, i);
-      const u32 k1 = __shfl_sync(0xffffffffu, my_k, i + 1);
-      uint4 b[V];
+    for (; i + kFly <= m; i += kFly) {
+      uint4 b[kFly][V];
 #pragma unroll
-      for (int j = 0; j < V; j++) b[j] = make_uint4(0, 0, 0, 0);
-      rows_or<V>(acc, a.O, k0, rs, lane);
-      rows_or<V>(b, a.O, k1, rs, lane);
+      for (int f = 0; f < kFly; f++) {
+        const u32 k = __shfl_sync(0xffffffffu, my_k, i + f);
+        const uint4 *row = reinterpret_cast<const uint4 *>(a.O + ((u64)k << rs));
 #pragma unroll
-      for (int j = 0; j < V; j++) {
-        acc[j].x |= b[j].x;
-        acc[j].y |= b[j].y;
-        acc[j].z |= b[j].z;
-        acc[j].w |= b[j].w;
+        for (int j = 0; j < V; j++) b[f][j] = row[j * 32 + lane];
       }
+#pragma unroll
+      for (int f = 0; f < kFly; f++)
+#pragma unroll
+        for (int j = 0; j < V; j++) {
+          acc[j].x |= b[f][j].x;
+          acc[j].y |= b[f][j].y;
+          acc[j].z |= b[f][j].z;
+          acc[j].w |= b[f][j].w;
+        }
     }
-    if (i < m) rows_or<V>(acc, a.O, __shfl_sync(0xffffffffu, my_k, i), rs, lane);
+    for (; i < m; i++) rows_or<V>(acc, a.O, __shfl_sync(0xffffffffu, my_k, i), rs, lane);
     // a y whose in-edges are all in this piece is this warp's alone
     const bool whole = pc.x == a.inv_off[y] && pc.y == a.inv_off[y + 1];
     rows_flush<V>(a, y, whole, acc, words_out);
@@ -714,9 +724,12 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
 // dst |= transpose(src), src cleared: the transposed output of the joins
 // whose output is (inner column 1, outer column 1), folded into the output
 // relation's NEWT (and its dirty map) after each such join.  Every word of
-// dst comes from one tile of src, so the ORs need no atomics.
+// dst comes from one tile of src, so the ORs need no atomics.  overwrite:
+// dst := transpose(src), every word written and none read (the first
+// writer of a tmp relation's NEWT in an iteration, without a dirty map: what
+// dst held before is not part of this iteration's NEWT).
 __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *dirty, int dk,
-                                                        Ctl *ctl) {
+                                                        int overwrite, Ctl *ctl) {
   __shared__ u32 s_t[256][9];
   if (ctl_stop(ctl)) return;
   const int rs = dk - 5;
@@ -726,7 +739,9 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *
   u64 moved = 0;
   // Software-pipelined over the block's tiles: the next tile's source words
   // and this tile's destination words are loaded before this tile's
-  // barriers, so the two memory round trips of a tile overlap.
+  // barriers, so the two memory round trips of a tile overlap.  A tile's
+  // reads of s_t are ordered before the next tile's writes by that tile's
+  // __syncthreads_or.
   u64 t = blockIdx.x;
   u32 v[8];
   if (t < tiles) load8(src + ((((t / per) * 256 + (u64)threadIdx.x) << rs) + (t % per) * 8), v);
@@ -738,7 +753,7 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *
     u32 vn[8], d[8];
     if (tn < tiles)
       load8(src + ((((tn / per) * 256 + (u64)threadIdx.x) << rs) + (tn % per) * 8), vn);
-    load8(dst + dw, d);
+    if (!overwrite) load8(dst + dw, d);
     const bool any = (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) != 0u;
     moved += 4 * 8;
     if (any) {
@@ -747,20 +762,28 @@ __global__ void __launch_bounds__(kTrBlock) k_bm_fold_t(u32 *src, u32 *dst, u8 *
       ps[1] = make_uint4(0, 0, 0, 0);
       moved += 4 * 8;
     }
+    uint4 *pd = reinterpret_cast<uint4 *>(dst + dw);
     if (__syncthreads_or(any)) {  // block-uniform
 #pragma unroll
       for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
       __syncthreads();
       const u32 *q = s_t[threadIdx.x];
-      if ((q[0] | q[1] | q[2] | q[3] | q[4] | q[5] | q[6] | q[7]) != 0u) {
-        uint4 *pd = reinterpret_cast<uint4 *>(dst + dw);
+      if (overwrite) {
+        pd[0] = make_uint4(q[0], q[1], q[2], q[3]);
+        pd[1] = make_uint4(q[4], q[5], q[6], q[7]);
+        moved += 4 * 8;
+      } else if ((q[0] | q[1] | q[2] | q[3] | q[4] | q[5] | q[6] | q[7]) != 0u) {
         pd[0] = make_uint4(d[0] | q[0], d[1] | q[1], d[2] | q[2], d[3] | q[3]);
         pd[1] = make_uint4(d[4] | q[4], d[5] | q[5], d[6] | q[6], d[7] | q[7]);
         if (dirty) dirty[dw / kBmChunkWords] = 1;
-        moved += 8 * 8;
+        moved += 4 * 8;
       }
-      __syncthreads();
+    } else if (overwrite) {
+      pd[0] = make_uint4(0, 0, 0, 0);
+      pd[1] = make_uint4(0, 0, 0, 0);
+      moved += 4 * 8;
     }
+    if (!overwrite) moved += 4 * 8;
     if (tn < tiles) {
 #pragma unroll
       for (int i = 0; i < 8; i++) v[i] = vn[i];
