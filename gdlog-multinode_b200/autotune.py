@@ -6,16 +6,19 @@ Here the engine exposes, through gdl_tuning, the choices whose best value
 depends on the instance: the dedup path (bitmaps or radix sort + merge), the
 largest domain kept as bitmaps, the form of a join into bitmaps (one
 probe-and-expand pass, or count + materialise passes), the CTAs per SM of
-the join's count and materialisation passes, and the slots per key of the
-hashed index.  The
-radix sort's digit width is fixed at 8 bits; its number of passes already
-follows the key width.
+the join's count and materialisation passes, the slots per key of the
+hashed index (its load factor), the block size of the one-pass join, the
+radix sort's digit width (6, 8 or 10 bits; the number of passes follows
+the key width) and the join tile of the row-gather form (in-edges per unit
+of work).
 
 The tuner buckets a workload by program and by log2 of its node and tuple
-counts, times each candidate configuration on the workload (device time of
-the fixpoints, best of `reps`), keeps the fastest, and remembers it per
-(GPU, bucket) in a JSON cache.  Results never depend on the choice: every
-configuration gives the same tuples, sizes and loop-pass counts.
+counts.  It times every combination of SPACE on the workload (device time
+of the fixpoints, best of `reps`), then, from the fastest, tries each value
+of every REFINE parameter in turn and keeps what is faster (coordinate
+descent), and remembers the result per (GPU, bucket) in a JSON cache.
+Results never depend on the choice: every configuration gives the same
+tuples, sizes and loop-pass counts.
 """
 from __future__ import annotations
 
@@ -38,6 +41,12 @@ SPACE = {
     "count_ctas_per_sm": [2, 4, 8],
     "index_slots_per_key": [2, 4],
     "pull_joins": [2, 1],
+}
+# Tried one at a time from the best of SPACE (default first).
+REFINE = {
+    "join_block": [256, 128, 512],
+    "radix_bits": [8, 6, 10],
+    "rows_piece": [32, 16, 8],
 }
 
 
@@ -126,17 +135,32 @@ class Tuner:
             return sum(lie.stats()["ms"] for lie in r.lies.values())
         return self.tune_runner(eng, self.key(prog.__name__, inputs), run, space, reps, save)
 
-    def tune_runner(self, eng, key: str, run, space=SPACE, reps=2, save=True) -> dict:
+    def tune_runner(self, eng, key: str, run, space=SPACE, reps=2, save=True,
+                    refine=None) -> dict:
         """tune() for any run(eng) -> device milliseconds (e.g. a batched
-        fixpoint over many instances), cached under `key`."""
+        fixpoint over many instances), cached under `key`.  `refine`
+        (default REFINE when `space` is SPACE, else none): parameters tried
+        one at a time from the best of `space`."""
+        if refine is None:
+            refine = REFINE if space is SPACE else {}
+        defaults = {k: v[0] for k, v in refine.items()}
         results = []
         for cfg in candidates(space):
+            cfg = {**cfg, **defaults}
             results.append((measure_runner(eng, run, cfg, reps), cfg))
         results.sort(key=lambda x: x[0])
         best_ms, best = results[0]
-        default_ms = next((ms for ms, c in results if c == candidates(space)[0]), None)
-        rec = {"config": best, "ms": best_ms, "default_ms": default_ms,
-               "tried": len(results)}
+        first = {**candidates(space)[0], **defaults}
+        default_ms = next((ms for ms, c in results if c == first), None)
+        tried = len(results)
+        for name, values in refine.items():
+            for v in values[1:]:
+                cfg = {**best, name: v}
+                ms = measure_runner(eng, run, cfg, reps)
+                tried += 1
+                if ms < best_ms:
+                    best_ms, best = ms, cfg
+        rec = {"config": best, "ms": best_ms, "default_ms": default_ms, "tried": tried}
         self.cache[key] = rec
         if save:
             with open(self.path, "w") as f:

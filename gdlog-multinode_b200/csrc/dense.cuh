@@ -781,53 +781,113 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 // Zero a NEWT bitmap in its dirty chunks (all of it without a dirty map)
 // and clear the dirty map.  One block per tile.
 // ---------------------------------------------------------------------------
-// One-pass listing of a square-domain bitmap (ids below 2^dk, rows of
-// 2^(dk-5) words) as its sorted key list: blocks take 2048-word tiles in
-// order, count them, take their output offset by decoupled look-back, and
-// write the tile's keys through a shared-memory window, so the stores are
-// coalesced and no key needs a search.  Replaces the count, scan and write
-// passes for the lists written at the end of a LIE (src/lie.cu:219-254:
-// FULL flattened into a sorted array).
+// Listing of a square-domain bitmap (ids below 2^dk, rows of 2^(dk-5)
+// words) as its sorted key list, in three passes over 2048-word tiles:
+// k_bm_list_count (a popcount per tile, streaming), k_bm_list_offsets (one
+// block: the tiles' output offsets and the list's size) and k_bm_list_write
+// (a block per tile with keys, the keys written at their offset with
+// coalesced stores and no search per key; an empty tile costs one read of
+// its count).  Replaces the sort of the flattened FULL at the end of a LIE
+// (src/lie.cu:219-254).
 //
-// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i).
-// A segment is 256 words, 8192 bit positions, so the keys of one segment
-// always fit one staging buffer: each is staged as its 13-bit position in
-// the segment (2 bytes; the row and column are rebuilt at the copy-out),
-// each thread expands one word per segment, and the copy-out is one
-// coalesced pass.  Two buffers alternate between the segments that hold
-// keys, so one barrier per segment separates a buffer's expansion from its
-// copy-out and the copy-out from the buffer's next expansion.
+// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i), so
+// warp w of segment i owns 32 consecutive words (lane l the word
+// i * 256 + 32 w + l).
 // ---------------------------------------------------------------------------
-constexpr int kListStage = kBmBlock * 32;  // 8192 positions per segment
+constexpr int kListScanBlock = 1024;
+
+__global__ void __launch_bounds__(kBmBlock) k_bm_list_count(const u32 *bm, u64 tiles, u32 *cnt,
+                                                            Ctl *ctl) {
+  __shared__ u32 s_w[kBmBlock / 32];
+  if (ctl_stop(ctl)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x) {
+    // words 4 t' .. 4 t' + 3 and 1024 + 4 t' .. of the tile (t' = thread)
+    const uint4 *p = reinterpret_cast<const uint4 *>(bm + t * kBmTileWords);
+    const uint4 x = p[threadIdx.x], y = p[kBmBlock + threadIdx.x];
+    u32 c = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w) + __popc(y.x) + __popc(y.y) +
+            __popc(y.z) + __popc(y.w);
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) s_w[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u32 sum = 0;
+#pragma unroll
+      for (int i = 0; i < kBmBlock / 32; i++) sum += s_w[i];
+      cnt[t] = sum;
+    }
+    __syncthreads();
+  }
+}
+
+// One block: off[t] = keys of the tiles before t; out->n = the total
+// (within the list's capacity).  out->n on entry is the bit count the loop
+// kept for this version; another total raises the bounds flag.
+__global__ void __launch_bounds__(kListScanBlock) k_bm_list_offsets(const u32 *cnt, u64 tiles,
+                                                                    u64 *off, DArr *out,
+                                                                    Ctl *ctl) {
+  __shared__ u64 s_warp[kListScanBlock / 32];
+  if (ctl_stop(ctl)) return;
+  u64 carry = 0;
+  for (u64 c0 = 0; c0 < tiles; c0 += kListScanBlock * 4) {
+    const u64 b = c0 + 4ull * threadIdx.x;
+    u32 v[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) v[i] = b + i < tiles ? cnt[b + i] : 0u;
+    const u64 local = (u64)v[0] + v[1] + v[2] + v[3];
+    u64 tot;
+    u64 ex = block_excl_scan<kListScanBlock>(local, s_warp, &tot) + carry;
+    carry += tot;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (b + i < tiles) {
+        off[b + i] = ex;
+        ex += v[i];
+      }
+  }
+  if (threadIdx.x == 0) {
+    const u64 expect_n = out->n, cap = out->cap;
+    out->n = carry <= cap ? carry : cap;
+    if (carry > cap || carry != expect_n) atomicOr(&ctl->oob, 16384u);
+  }
+}
 
 struct ListSmem {
-  unsigned short stage[2][kListStage];
   u32 wtot[kBmWordsPerThread][kBmBlock / 32];  // per segment: warp totals, then offsets
-  u32 seg_tot[kBmWordsPerThread];
-  u32 seg_off[kBmWordsPerThread];
-  u64 base;
+  u32 seg_off[kBmWordsPerThread + 1];
+  unsigned char lut[256 * 8];  // position of the r-th set bit of a byte: lut[byte * 8 + r]
   long long tile;
 };
 
-// out->n on entry: the bit count the loop kept for this version (the host
-// sizes the list for it, or the list is as large as the key domain); a
-// listing that finds another count raises the bounds flag.
-__global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, int rs, DArr *out,
-                                                      Lb lb, LaunchRec *rec, Ctl *ctl) {
+// Keys leave warp by warp: each warp writes the keys of its 32 words at
+// their offset, 32 consecutive keys per step.  Key j of the warp comes from
+// the last lane whose exclusive prefix is <= j (a 5-step search over the
+// lanes' prefixes), as the r-th set bit of that lane's word (two popcount
+// steps, then a byte table).  No staging, no barrier per segment, and no
+// lane waits on a denser neighbour.  Tiles are taken from a counter (dense
+// tiles cluster at the low ids of skewed graphs).
+__global__ void __launch_bounds__(kBmBlock) k_bm_list_write(const u32 *bm, u64 tiles, int rs,
+                                                            const u32 *cnt, const u64 *off,
+                                                            DArr *out, LaunchRec *rec, Ctl *ctl) {
   __shared__ ListSmem sm;
   if (ctl_stop(ctl)) return;
-  const u64 tiles = words / kBmTileWords;
-  const u32 gen = rec->gen;
+  for (int b = threadIdx.x; b < 256; b += kBmBlock) {
+    int r = 0;
+    for (int k = 0; k < 8; k++)
+      if (b >> k & 1) sm.lut[b * 8 + r++] = (unsigned char)k;
+    for (; r < 8; r++) sm.lut[b * 8 + r] = 0;
+  }
   const u64 row_mask = (1ull << rs) - 1;
   u64 *dst = out->ptr;
   const u64 cap = out->cap;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 moved = 0;
-  u32 nbuf = 0;  // segments with keys staged so far (buffer parity)
   while (true) {
-    const long long t = grab_tile(rec, &sm.tile);
-    if (t >= (long long)tiles) break;
-    const u64 w0 = (u64)t * kBmTileWords;
+    const long long tl = grab_tile(rec, &sm.tile);  // (its barriers order the table's writes)
+    if (tl >= (long long)tiles) break;
+    const u64 t = (u64)tl;
+    if (cnt[t] == 0) continue;  // (block-uniform)
+    const u64 w0 = t * kBmTileWords;
     u32 v[kBmWordsPerThread], ex[kBmWordsPerThread];
 #pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
@@ -843,83 +903,63 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list(const u32 *bm, u64 words, 
       if (lane == 31) sm.wtot[i][warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x < kBmWordsPerThread) {
-      // per segment: exclusive warp offsets and the segment's total
+    if (threadIdx.x == 0) {
+      // offsets of (segment, warp) in the tile's keys, in key order
       u32 acc = 0;
-      for (int w = 0; w < kBmBlock / 32; w++) {
-        const u32 x = sm.wtot[threadIdx.x][w];
-        sm.wtot[threadIdx.x][w] = acc;
-        acc += x;
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        sm.seg_off[i] = acc;
+        for (int w = 0; w < kBmBlock / 32; w++) {
+          const u32 x = sm.wtot[i][w];
+          sm.wtot[i][w] = acc;
+          acc += x;
+        }
       }
-      sm.seg_tot[threadIdx.x] = acc;
+      sm.seg_off[kBmWordsPerThread] = acc;
     }
     __syncthreads();
-    u32 tot = 0;
+    const u64 base = off[t];
+    moved += 4 * kBmWordsPerThread;
 #pragma unroll
-    for (int i = 0; i < kBmWordsPerThread; i++) tot += sm.seg_tot[i];
-    if (threadIdx.x < 32) {
-      u64 prefix = 0;
-      if (t == 0) {
-        if (lane == 0) lb_publish(lb, t, gen, true, tot);
-      } else {
-        if (lane == 0) lb_publish(lb, t, gen, false, tot);
-        prefix = lb_warp_prefix(lb, t, gen, ctl);
-        if (lane == 0) lb_publish(lb, t, gen, true, prefix + tot);
-      }
-      if (lane == 0) {
-        sm.base = prefix;
-        u32 a = 0;
-        for (int i = 0; i < kBmWordsPerThread; i++) {
-          sm.seg_off[i] = a;
-          a += sm.seg_tot[i];
-        }
-      }
-    }
-    __syncthreads();
-    const u64 base = sm.base;
-    if ((u64)t == tiles - 1 && threadIdx.x == 0) {
-      // never publish more rows than the list holds (sized from the
-      // bitmap's count, or for the whole domain; a mismatch is an error,
-      // reported).  Only this thread reads or writes out->n.
-      const u64 total = base + tot;
-      const u64 expect_n = out->n;
-      out->n = total <= cap ? total : cap;
-      if (total > cap || total != expect_n) atomicOr(&ctl->oob, 16384u);
-    }
-    moved += 4 * kBmWordsPerThread + 8 * (u64)(threadIdx.x == 0 ? tot : 0);
     for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u32 st = sm.seg_tot[i];  // block-uniform
-      if (st == 0) continue;
-      unsigned short *stg = sm.stage[nbuf++ & 1];
-      // expand this thread's word: its keys' positions in the segment
-      u32 x = v[i];
-      u32 p = sm.wtot[i][warp] + ex[i];
-      const u32 q0 = threadIdx.x * 32;
-      while (x) {
-        stg[p++] = (unsigned short)(q0 + (u32)(__ffs(x) - 1));
-        x &= x - 1;
-      }
-      __syncthreads();
-      // copy-out: position q of segment word ws = q / 32, bit q % 32
-      const u64 ws = w0 + (u64)i * kBmBlock;
-      const u64 pos0 = base + sm.seg_off[i];
-      u64 *o = dst + pos0;
-      if (pos0 + st <= cap) {
-        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
-          const u32 q = stg[j];
-          const u64 w = ws + (q >> 5);
-          o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
+      const u32 wofs = sm.wtot[i][warp];
+      const u32 wend = warp + 1 < kBmBlock / 32 ? sm.wtot[i][warp + 1] : sm.seg_off[i + 1];
+      const u32 total = wend - wofs;  // (warp-uniform)
+      if (total == 0) continue;
+      const u64 ws = w0 + (u64)i * kBmBlock + (u64)warp * 32;
+      const u64 pos0 = base + wofs;
+      for (u32 j0 = 0; j0 < total; j0 += 32) {
+        const u32 j = j0 + lane;
+        int sl = 0;
+#pragma unroll
+        for (int h = 16; h > 0; h >>= 1) {
+          const u32 e = __shfl_sync(0xffffffffu, ex[i], sl + h);
+          if (e <= j) sl += h;
         }
-      } else {
-        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
-          const u32 q = stg[j];
-          const u64 w = ws + (q >> 5);
-          if (pos0 + j < cap)
-            o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
-          else
-            atomicOr(&ctl->oob, 16384u);
+        u32 word = __shfl_sync(0xffffffffu, v[i], sl);
+        u32 r = j - __shfl_sync(0xffffffffu, ex[i], sl);
+        if (j >= total) continue;
+        u32 pos = 0;
+        u32 c = __popc(word & 0xFFFFu);
+        if (r >= c) {
+          r -= c;
+          word >>= 16;
+          pos = 16;
         }
+        c = __popc(word & 0xFFu);
+        if (r >= c) {
+          r -= c;
+          word >>= 8;
+          pos += 8;
+        }
+        pos += sm.lut[(word & 0xFFu) * 8 + r];
+        const u64 w = ws + (u64)sl;
+        const u64 key = ((w >> rs) << 32) | ((w & row_mask) << 5) | pos;
+        if (pos0 + j < cap)
+          dst[pos0 + j] = key;
+        else
+          atomicOr(&ctl->oob, 16384u);
       }
+      moved += 8 * (u64)(lane == 0 ? total : 0);
     }
   }
 #pragma unroll
@@ -1030,17 +1070,21 @@ constexpr u32 kHeavyPiece = 2048;
 constexpr u32 kRowPiece = 256;
 constexpr u32 kRowFlag = 0x80000000u;
 
+// The block size is a tuning choice (128, 256 or 512 threads; the same
+// warps per SM at each).
+template <int BLOCK>
 struct FuseSmem {
-  u64 row[kFuseBlock / 32][32];
-  u64 excl[kFuseBlock / 32][32];
-  u32 start[kFuseBlock / 32][32];
-  u32 agg[kFuseBlock / 32][32];  // warp_set_bits slots
+  u64 row[BLOCK / 32][32];
+  u64 excl[BLOCK / 32][32];
+  u32 start[BLOCK / 32][32];
+  u32 agg[BLOCK / 32][32];  // warp_set_bits slots
 };
 
-template <bool AGG>
-__global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
+template <bool AGG, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, kFuseCtasPerSm * kFuseBlock / BLOCK)
     k_join_bm(JoinArgs a, const RelDev *out_rd, DenseMap map) {
-  __shared__ FuseSmem sm;
+  constexpr int kFuseBlock = BLOCK;
+  __shared__ FuseSmem<BLOCK> sm;
   if (ctl_stop(a.ctl)) return;
   const u64 n_outer = eff_count(a.outer, a.outer_vis);
   const u64 n_inner = eff_count(a.inner, a.inner_vis);
@@ -1157,10 +1201,10 @@ __global__ void __launch_bounds__(kFuseBlock, kFuseCtasPerSm)
 // The pieces of long runs appended by k_join_bm, a block per piece; the
 // last block empties the piece list for the next launch (so does block 0
 // of a stopped launch, which expands nothing).
-template <bool AGG>
-__global__ void __launch_bounds__(kFuseBlock) k_join_heavy_bm(JoinArgs a, const RelDev *out_rd,
-                                                             DenseMap map) {
-  __shared__ u32 s_agg[kFuseBlock / 32][32];
+template <bool AGG, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_join_heavy_bm(JoinArgs a, const RelDev *out_rd,
+                                                        DenseMap map) {
+  __shared__ u32 s_agg[BLOCK / 32][32];
   if (ctl_stop(a.ctl)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.op->nc = 0;
     return;

@@ -37,6 +37,7 @@
 #include "pull.cuh"
 #include "sort.cuh"
 #include "tma.cuh"
+#include "exchange.cuh"
 
 #include <algorithm>
 #include <condition_variable>
@@ -191,6 +192,13 @@ struct gdl_engine {
   u32 *sort_offsets = nullptr, *sort_counters = nullptr, *sort_status = nullptr;
   u64 sort_status_tiles = 0;
   int sort_status_passes = 0;
+  int sort_status_radix = 0;
+  // Tuned shapes (gdl_tuning): radix sort digit width, block size of the
+  // probe-and-expand join (k_join_bm), in-edges per piece of a row-gather
+  // join (k_join_rows_bm).
+  int radix_bits = kRadixBits;
+  int join_block = 256;
+  int rows_piece = 32;
   u64 *crow_off = nullptr, *crow_key = nullptr;
   u32 *crow_start = nullptr, *crow_len = nullptr;
   u64 crow_cap = 0;
@@ -199,7 +207,7 @@ struct gdl_engine {
   // Dense scans: look-back state of the tile-count scan.
   Lb lb_bm{};
   u64 lb_bm_tiles = 0;
-  Lb lb_list{};  // k_bm_list: one look-back slot per 2048-word tile
+  Lb lb_list{};  // listings (k_bm_list_*): per 2048-word tile its count (flag) and offset (agg)
   u64 lb_list_tiles = 0;
   // Graph executables of dropped LIEs: destroyed by a worker thread of the
   // engine (destroying one takes ~0.1 ms of host time that the caller's
@@ -276,6 +284,8 @@ struct gdl_engine {
                               // [4] [5] bitmap scans, [6] pull join, [7] transpose,
                               // [8] bitmap listing
   DArr *d_tmp = nullptr;      // [4] temporary descriptors for loads
+  void *d_count = nullptr;    // gdl_join_count's scratch (CountScratch)
+  void *d_part = nullptr;     // gdl_partition_rows: counts and cursors per destination
   u64 *d_u64 = nullptr;       // [4] small device scalars
   u32 *d_u32 = nullptr;       // [4]: [0] pack check, [3] device checks of async loads (sticky)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -546,7 +556,16 @@ int grid_for(gdl_engine *e, u64 work, u64 per_block, int per_sm) {
 // Sorts radix the significant bits only: column 0's kbits and the low half's
 // kbits (arity 2) or all 32 (once arity-3 keys exist).
 int sort_lo_bits(const gdl_engine *e) { return e->wide ? 32 : e->kbits; }
-int sort_passes(const gdl_engine *e) { return std::max(1, (e->kbits + sort_lo_bits(e) + 7) / 8); }
+// Digit width of the radix sort: the tuned one (6, 8 or 10 bits) unless it
+// would take more than kMaxPasses passes over the significant bits.
+int sort_bits(const gdl_engine *e) {
+  const int b = e->radix_bits, bits = e->kbits + sort_lo_bits(e);
+  return (bits + b - 1) / b <= kMaxPasses ? b : kRadixBits;
+}
+int sort_passes(const gdl_engine *e) {
+  const int b = sort_bits(e);
+  return std::max(1, (e->kbits + sort_lo_bits(e) + b - 1) / b);
+}
 
 // The key bits of a relation's dependent columns (cleared to compare the
 // set difference's prefix, merge.cuh k_dep_mask); 0 without any.
@@ -637,17 +656,20 @@ gdl_status ensure_scratch(gdl_engine *e) {
   }
   const u64 tiles = e->sort_cap / kSortTile + 2;
   const int passes = std::max(sort_passes(e), 1);
-  if (tiles > e->sort_status_tiles || passes > e->sort_status_passes || !e->sort_status) {
+  const int radix = 1 << sort_bits(e);
+  if (tiles > e->sort_status_tiles || passes > e->sort_status_passes ||
+      radix > e->sort_status_radix || !e->sort_status) {
     dfree(e, e->sort_status);
     e->sort_status_tiles = tiles;
     e->sort_status_passes = std::max(passes, 4);
+    e->sort_status_radix = std::max(radix, kRadix);
     TRY(dalloc(e, (void **)&e->sort_status,
-               (u64)e->sort_status_passes * tiles * kRadix * sizeof(u32)));
+               (u64)e->sort_status_passes * tiles * e->sort_status_radix * sizeof(u32)));
   }
   if (!e->sort_offsets) {
-    TRY(dalloc(e, (void **)&e->sort_offsets, kMaxPasses * kRadix * sizeof(u32)));
+    TRY(dalloc(e, (void **)&e->sort_offsets, kMaxPasses * kMaxRadix * sizeof(u32)));
     TRY(dalloc(e, (void **)&e->sort_counters, (kMaxPasses + 1) * sizeof(u32)));
-    CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kRadix * sizeof(u32), e->s));
+    CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kMaxRadix * sizeof(u32), e->s));
     CK(e, cudaMemsetAsync(e->sort_counters, 0, (kMaxPasses + 1) * sizeof(u32), e->s));
   }
   // join records
@@ -749,9 +771,21 @@ void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *
   a.ctl = e->d_ctl;
   int gh = grid_for(e, cap, (u64)kSortTile * 4, 2);
   int gp = grid_for(e, cap, kSortTile, 4);
-  PLAUNCH(kc, kPSortHist, k_sort_hist<<<gh, kSortBlock, kSortSmemBytes, e->s>>>(a));
-  for (int p = 0; p < a.passes; p++)
-    PLAUNCH(kc, kPSortPass, k_sort_pass<<<gp, kSortBlock, kSortSmemBytes, e->s>>>(a, p));
+  switch (sort_bits(e)) {
+#define GDL_SORT(B)                                                                         \
+  case B:                                                                                   \
+    PLAUNCH(kc, kPSortHist,                                                                 \
+            k_sort_hist<B><<<gh, kSortBlock, sort_smem_bytes<B>(), e->s>>>(a));             \
+    for (int p = 0; p < a.passes; p++)                                                      \
+      PLAUNCH(kc, kPSortPass,                                                               \
+              k_sort_pass<B><<<gp, kSortBlock, sort_smem_bytes<B>(), e->s>>>(a, p));       \
+    break;
+    GDL_SORT(6)
+    GDL_SORT(10)
+    default:
+    GDL_SORT(8)
+#undef GDL_SORT
+  }
 }
 
 u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e->sort_buf : buf0; }
@@ -1142,6 +1176,22 @@ void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
   }
 }
 
+// The sorted key list of a square-domain bitmap of `words` words (rows of
+// 2^rs words) into `out` (k_bm_list_*, dense.cuh): tile counts, offsets and
+// the list's size, keys.  out->n must hold the expected count.
+gdl_status launch_list(gdl_engine *e, const u32 *bm, u64 words, int rs, DArr *out) {
+  const u64 tiles = words / kBmTileWords;
+  TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, tiles + 2));
+  k_bm_list_count<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(bm, tiles, e->lb_list.flag,
+                                                                   e->d_ctl);
+  k_bm_list_offsets<<<1, kListScanBlock, 0, e->s>>>(e->lb_list.flag, tiles, e->lb_list.agg, out,
+                                                    e->d_ctl);
+  k_bm_list_write<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(
+      bm, tiles, rs, e->lb_list.flag, e->lb_list.agg, out, &e->recs[8], e->d_ctl);
+  CK(e, cudaGetLastError());
+  return GDL_OK;
+}
+
 // dst |= transpose(src) (or := with over), src cleared: the TMA pass
 // (tma.cuh) when both bitmaps have tensor maps, else the LDG/STG pass.
 void launch_fold(gdl_engine *e, u32 *src, u32 *dst, u8 *dirty, int dk, int over, Counts *kc,
@@ -1152,9 +1202,10 @@ void launch_fold(gdl_engine *e, u32 *src, u32 *dst, u8 *dirty, int dk, int over,
     FoldMaps m;
     m.src = *ms;
     m.dst = *md;
+    const int ns = fold_tma_stages(over);
     PLAUNCH(kc, kPBitmap,
-            k_bm_fold_tma<<<grid_for(e, side * side, 1, 2), kTrBlock, fold_tma_smem(), s>>>(
-                m, dirty, dk, over, e->d_ctl));
+            k_bm_fold_tma<<<grid_for(e, side * side, 1, over ? 3 : 2), kTrBlock,
+                            fold_tma_smem(ns, over), s>>>(m, dirty, dk, over, ns, e->d_ctl));
     return;
   }
   PLAUNCH(kc, kPBitmap, k_bm_fold_t<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, s>>>(
@@ -1176,9 +1227,11 @@ void launch_update_t(gdl_engine *e, const BmScanArgs &a, int r, u32 *gt, u32 *dn
     m.f = *mf;
     m.dn = *mdn;
     m.dt = *mdt;
+    const int ns = upd_tma_stages(dt != nullptr);
     PLAUNCH(kc, kPBitmap,
-            k_bm_update_tma<<<grid_for(e, side * side, 1, 2), kTrBlock, upd_tma_smem(dt != nullptr),
-                              s>>>(a, m, dk, gt != nullptr, dn != nullptr, dt != nullptr));
+            k_bm_update_tma<<<grid_for(e, side * side, 1, 2), kTrBlock,
+                              upd_tma_smem(ns, dt != nullptr), s>>>(
+                a, m, dk, gt != nullptr, dn != nullptr, dt != nullptr, ns));
     return;
   }
   PLAUNCH(kc, kPBitmap,
@@ -1212,7 +1265,7 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   k_inv_count<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, dk, e->d_ctl);
   // edge offsets, fill cursors and the pieces of work, in one block
   k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, rh.inv_poff,
-                                           rh.inv_pieces, dk);
+                                           rh.inv_pieces, dk, (u32)e->rows_piece);
   k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
                                                        dk);
   CK(e, cudaGetLastError());
@@ -1394,7 +1447,9 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
       memcpy(&b, &a, sizeof b);
       b.rec = &e->recs[1];
       if (dense && e->dense_join_passes == 1) {
-        const int jg = grid_for(e, outer_cap, kFuseBlock, kFuseCtasPerSm);
+        const int jb = e->join_block;
+        const int jg = grid_for(e, outer_cap, jb, kFuseCtasPerSm * kFuseBlock / jb);
+        const int hg = (int)e->sms * 4 * kFuseBlock / jb;
         if (plan.static_once[oi]) {
           a.once = &L.d_lie->jonce[oi];
           a.once_pending = &L.d_lie->jonce_pending[oi];
@@ -1402,15 +1457,20 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
           a.phantom = &R[op.out].newt_phantom;
           b.produced = a.produced;
         }
-        if (e->join_aggregate == 2) {
-          PLAUNCH(kc, kPJoinMat, k_join_bm<true><<<jg, kFuseBlock, 0, s>>>(a, &R[op.out], map));
-          PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<true><<<(int)e->sms * 4, kFuseBlock, 0, s>>>(
-                                     b, &R[op.out], map));
+#define GDL_PUSH(AG, B)                                                                      \
+  do {                                                                                       \
+    PLAUNCH(kc, kPJoinMat, k_join_bm<AG, B><<<jg, B, 0, s>>>(a, &R[op.out], map));           \
+    PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<AG, B><<<hg, B, 0, s>>>(b, &R[op.out], map));     \
+  } while (0)
+        const bool ag = e->join_aggregate == 2;
+        if (jb == 128) {
+          if (ag) GDL_PUSH(true, 128); else GDL_PUSH(false, 128);
+        } else if (jb == 512) {
+          if (ag) GDL_PUSH(true, 512); else GDL_PUSH(false, 512);
         } else {
-          PLAUNCH(kc, kPJoinMat, k_join_bm<false><<<jg, kFuseBlock, 0, s>>>(a, &R[op.out], map));
-          PLAUNCH(kc, kPJoinMat, k_join_heavy_bm<false><<<(int)e->sms * 4, kFuseBlock, 0, s>>>(
-                                     b, &R[op.out], map));
+          if (ag) GDL_PUSH(true, 256); else GDL_PUSH(false, 256);
         }
+#undef GDL_PUSH
         continue;
       }
       PLAUNCH(kc, kPJoinCount,
@@ -2309,9 +2369,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     k_ctl_resume<<<1, 32, 0, e->s>>>(e->d_ctl);
     for (int r : L.update)
       if (e->h[r].full_lazy)
-        k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-            e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
-            e->d_ctl);
+        TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full));
     CK(e, cudaGetLastError());
     CK(e, cudaMemcpyAsync(e->h_ctl2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
     CK(e, cudaEventRecord(e->ev1, e->s));
@@ -2568,15 +2626,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       TRY(resume_ctl());
       TRY(push(e));
       Counts kc;
-      if (!e->instances) TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles,
-                                       L.map.words / kBmTileWords + 2));
       for (int r : L.update) {
         if (!e->h[r].full_lazy) continue;
         if (!e->instances) {
-          // square domain: one pass (k_bm_list)
-          k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-              e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, e->lb_list, &e->recs[8],
-              e->d_ctl);
+          // square domain (k_bm_list_*)
+          TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full));
           continue;
         }
         BmScanArgs a = scan_none(L.map);
@@ -2610,7 +2664,6 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     if (any_delta) {
       TRY(resume_ctl());
       TRY(push(e));
-      TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, L.map.words / kBmTileWords + 2));
       const u64 side = 1ull << (L.dk - kPullMinBits);
       for (int r : L.update) {
         const RelDev &h = e->h[r];
@@ -2624,9 +2677,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
           rows = h.bmG;
         }
-        k_bm_list<<<grid_for(e, L.map.words / kBmTileWords, 1, 4), kBmBlock, 0, e->s>>>(
-            rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, e->lb_list, &e->recs[8],
-            e->d_ctl);
+        TRY(launch_list(e, rows, L.map.words, L.dk - 5, &e->d_rels[r].delta));
         if (!plan.delta_n[r]) CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
       }
       CK(e, cudaGetLastError());
@@ -2751,10 +2802,18 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
     u64 thr = ~0ull;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-  if (bad(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSortSmemBytes)) ||
-      bad(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSortSmemBytes)) ||
+  if (bad(cudaFuncSetAttribute(k_sort_hist<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<6>())) ||
+      bad(cudaFuncSetAttribute(k_sort_pass<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<6>())) ||
+      bad(cudaFuncSetAttribute(k_sort_hist<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<8>())) ||
+      bad(cudaFuncSetAttribute(k_sort_pass<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<8>())) ||
+      bad(cudaFuncSetAttribute(k_sort_hist<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<10>())) ||
+      bad(cudaFuncSetAttribute(k_sort_pass<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sort_smem_bytes<10>())) ||
       bad(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kMergeSmemBytes)) ||
       bad(cudaFuncSetAttribute(k_join_pull_bm, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2790,9 +2849,11 @@ gdl_status gdl_engine_create(int32_t device, void *stream, gdl_engine **out) {
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess && fn &&
         cudaFuncSetAttribute(k_bm_update_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)upd_tma_smem(1)) == cudaSuccess &&
+                             (int)std::max(upd_tma_smem(upd_tma_stages(0), 0),
+                                           upd_tma_smem(upd_tma_stages(1), 1))) == cudaSuccess &&
         cudaFuncSetAttribute(k_bm_fold_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)fold_tma_smem()) == cudaSuccess) {
+                             (int)std::max(fold_tma_smem(fold_tma_stages(0), 0),
+                                           fold_tma_smem(fold_tma_stages(1), 1))) == cudaSuccess) {
       e->tma_encode = fn;
       e->tma_ok = true;
     }
@@ -2867,7 +2928,7 @@ gdl_status gdl_engine_clear(gdl_engine *e) {
     if (e->sort_counters)
       CK(e, cudaMemsetAsync(e->sort_counters, 0, (kMaxPasses + 1) * sizeof(u32), e->s));
     if (e->sort_offsets)
-      CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kRadix * sizeof(u32), e->s));
+      CK(e, cudaMemsetAsync(e->sort_offsets, 0, kMaxPasses * kMaxRadix * sizeof(u32), e->s));
     CK(e, cudaMemsetAsync(e->d_u32, 0, 4 * sizeof(u32), e->s));
     CK(e, cudaMemsetAsync(e->d_pull_count, 0, sizeof(u64), e->s));
     TRY(reset_ctl(e));
@@ -2917,6 +2978,7 @@ gdl_status gdl_engine_destroy(gdl_engine *e) {
                   (void *)e->d_tile_inst, (void *)e->d_square_seg,
                   (void *)e->recs,
                   (void *)e->d_tmp, (void *)e->d_u64, (void *)e->d_u32, (void *)e->d_pull_count,
+                  e->d_count, e->d_part,
                   (void *)e->d_rels,
                   (void *)e->d_ctl})
     if (p) cudaFree(p);
@@ -3145,6 +3207,57 @@ gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t ver, uint64_t
   return GDL_OK;
 }
 
+gdl_status gdl_relation_export_device(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *rows,
+                                      uint64_t cap, uint64_t *out_n) {
+  CHECK_REL(e, rel);
+  if (!out_n) return GDL_E_INVALID;
+  if (e->rels[rel].arity != 2)
+    return fail(e, GDL_E_UNSUPPORTED, "device export: arity-2 relations only");
+  const u64 *p = nullptr;
+  u64 n = 0;
+  bool sorted;
+  TRY(version_view(e, rel, ver, &p, &n, &sorted));
+  if (!sorted)
+    return fail(e, GDL_E_UNSUPPORTED,
+                "device export: this version of %s is in load order (export it to the host)",
+                e->rels[rel].name.c_str());
+  *out_n = n;
+  if (n > cap) return fail(e, GDL_E_CAPACITY, "device export needs %llu rows",
+                           (unsigned long long)n);
+  if (n && !rows) return GDL_E_INVALID;
+  if (n)
+    k_unpack_rows<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(p, n, reinterpret_cast<u64 *>(rows));
+  CK(e, cudaGetLastError());
+  CK(e, cudaStreamSynchronize(e->s));
+  return GDL_OK;
+}
+
+gdl_status gdl_partition_rows(gdl_engine *e, const uint64_t *rows, uint64_t n, int32_t column,
+                              int32_t world, uint64_t *out_rows, uint64_t *counts) {
+  if (!e) return GDL_E_INVALID;
+  if (column < 0 || column > 1 || world < 1 || world > kPartMaxWorld || !counts ||
+      (n && (!rows || !out_rows)))
+    return fail(e, GDL_E_INVALID, "partition: column 0 or 1, 1 <= world <= %d", kPartMaxWorld);
+  cudaSetDevice(e->device);
+  if (!e->d_part) CK(e, cudaMalloc(&e->d_part, 2 * kPartMaxWorld * sizeof(u64)));
+  u64 *cnt = reinterpret_cast<u64 *>(e->d_part), *cur = cnt + kPartMaxWorld;
+  CK(e, cudaMemsetAsync(cnt, 0, world * sizeof(u64), e->s));
+  if (n) {
+    const int g = grid_for(e, n, 256, 8);
+    const u64 *in = reinterpret_cast<const u64 *>(rows);
+    k_part_count<<<g, 256, 0, e->s>>>(in, n, column, (u32)world, cnt);
+    k_part_offsets<<<1, 32, 0, e->s>>>(cnt, (u32)world, cur);
+    k_part_scatter<<<g, 256, 0, e->s>>>(in, n, column, (u32)world, cur,
+                                        reinterpret_cast<u64 *>(out_rows));
+    CK(e, cudaGetLastError());
+  }
+  std::vector<u64> h(world);
+  CK(e, cudaMemcpyAsync(h.data(), cnt, world * sizeof(u64), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  for (int d = 0; d < world; d++) counts[d] = h[d];
+  return GDL_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Files (get_row_size + get_relation_from_file, test/tc.cu:17-57)
 // ---------------------------------------------------------------------------
@@ -3245,6 +3358,87 @@ gdl_status gdl_relation_dump_tsv(gdl_engine *e, int32_t rel, int32_t ver, const 
 static gdl_status bitmap_stats(gdl_engine *e, const u32 *bm, const DenseMap &map,
                                const std::vector<SegInfo> &segs, std::vector<u64> &size,
                                std::vector<u64> &digest);
+
+// Device scratch of gdl_join_count: the op record and the two visibility
+// words the count kernel reads (and zeroes, for an empty side) instead of
+// the relations' own.
+struct CountScratch {
+  JoinRec rec;
+  DArr newt;
+  u32 outer_vis, inner_vis;
+};
+
+gdl_status gdl_join_count(gdl_engine *e, int32_t inner, int32_t inner_ver, int32_t outer,
+                          int32_t outer_ver, uint64_t *out) {
+  CHECK_REL(e, inner);
+  CHECK_REL(e, outer);
+  if (!out) return GDL_E_INVALID;
+  if (e->broken) return fail(e, GDL_E_TIMEOUT, "engine is in a failed state; destroy it");
+  auto ver_ok = [](int32_t v) { return v == GDL_FULL || v == GDL_DELTA; };
+  if (!ver_ok(inner_ver) || !ver_ok(outer_ver))
+    return fail(e, GDL_E_INVALID, "join count: versions must be GDL_FULL or GDL_DELTA");
+  if (e->instances) return fail(e, GDL_E_UNSUPPORTED, "join count: not in the batched form");
+  for (int r : {inner, outer})
+    if (e->rels[r].full_resident)
+      return fail(e, GDL_E_UNSUPPORTED, "join count: %s is kept as a bitmap only",
+                  e->rels[r].name.c_str());
+  TRY(refresh(e));
+  const RelDev &ih = e->h[inner], &oh = e->h[outer];
+  const Index &ix = inner_ver == GDL_FULL ? ih.full_idx : ih.delta_idx;
+  const DArr &ia = inner_ver == GDL_FULL ? ih.full : ih.delta;
+  const DArr &oa = outer_ver == GDL_FULL ? oh.full : oh.delta;
+  const u64 ni = (inner_ver == GDL_FULL ? ih.full_vis : ih.delta_vis) ? ia.n : 0;
+  const u64 no = (outer_ver == GDL_FULL ? oh.full_vis : oh.delta_vis) ? oa.n : 0;
+  if (ni && !ix.slots)
+    return fail(e, GDL_E_INVALID, "join count: %s has no index of that version (index_flag)",
+                e->rels[inner].name.c_str());
+  if (ni == 0 || no == 0) {
+    *out = 0;
+    return GDL_OK;
+  }
+  TRY(ensure_scratch(e));
+  // (outside the engine's replayed allocation sequence: kept until destroy)
+  if (!e->d_count) CK(e, cudaMalloc(&e->d_count, sizeof(CountScratch)));
+  CountScratch cs;
+  memset(&cs, 0, sizeof cs);
+  cs.outer_vis = cs.inner_vis = 1;
+  CK(e, cudaMemcpyAsync(e->d_count, &cs, sizeof cs, cudaMemcpyHostToDevice, e->s));
+  TRY(reset_ctl(e));
+  CountScratch *d = reinterpret_cast<CountScratch *>(e->d_count);
+  RelDev *R = e->d_rels;
+  JoinArgs a;
+  memset(&a, 0, sizeof a);
+  a.outer = outer_ver == GDL_FULL ? &R[outer].full : &R[outer].delta;
+  a.outer_vis = &d->outer_vis;
+  a.inner = inner_ver == GDL_FULL ? &R[inner].full : &R[inner].delta;
+  a.inner_vis = &d->inner_vis;
+  a.inner_idx = inner_ver == GDL_FULL ? &R[inner].full_idx : &R[inner].delta_idx;
+  a.out_newt = &d->newt;
+  a.dense = 1;  // (no NEWT to check for room)
+  a.op = &d->rec;
+  a.rec = &e->recs[0];
+  a.lb_cnt = e->lb_cnt;
+  a.lb_nz = e->lb_nz;
+  a.crow_off = e->crow_off;
+  a.crow_start = e->crow_start;
+  a.crow_len = e->crow_len;
+  a.crow_key = e->crow_key;
+  a.crow_cap = e->crow_cap;
+  a.ctl = e->d_ctl;
+  k_join_count<<<grid_for(e, no, kJoinTile, e->count_ctas_per_sm), kJoinBlock, 0, e->s>>>(a);
+  CK(e, cudaGetLastError());
+  JoinRec rec;
+  CK(e, cudaMemcpyAsync(&rec, &d->rec, sizeof rec, cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
+  CK(e, cudaStreamSynchronize(e->s));
+  if (e->h_ctl->timeout || e->h_ctl->oob) {
+    e->broken = true;
+    return fail(e, GDL_E_TIMEOUT, "join count: device-side check failed (timeout=%u oob=%u)",
+                e->h_ctl->timeout, e->h_ctl->oob);
+  }
+  *out = rec.total;
+  return GDL_OK;
+}
 
 gdl_status gdl_relation_digest(gdl_engine *e, int32_t rel, int32_t ver, uint64_t *out) {
   CHECK_REL(e, rel);
@@ -3559,7 +3753,10 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       (t->dirty_min_log2_words && (t->dirty_min_log2_words < 11 || t->dirty_min_log2_words > 40)) ||
       t->dense_join_passes < 0 || t->dense_join_passes > 2 || t->join_aggregate < 0 ||
       t->join_aggregate > 2 || t->pull_joins < 0 || t->pull_joins > 3 || t->row_gather < 0 ||
-      t->row_gather > 3 || t->spin_limit_log2 < 0 || t->spin_limit_log2 > 30)
+      t->row_gather > 3 || t->spin_limit_log2 < 0 || t->spin_limit_log2 > 30 ||
+      (t->radix_bits && t->radix_bits != 6 && t->radix_bits != 8 && t->radix_bits != 10) ||
+      (t->join_block && t->join_block != 128 && t->join_block != 256 && t->join_block != 512) ||
+      (t->rows_piece && t->rows_piece != 8 && t->rows_piece != 16 && t->rows_piece != 32))
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -3572,6 +3769,9 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->pull_joins) e->pull_joins = t->pull_joins;
   if (t->row_gather) e->row_gather = t->row_gather;
   if (t->spin_limit_log2) e->spin_limit = 1u << t->spin_limit_log2;
+  if (t->radix_bits) e->radix_bits = t->radix_bits;
+  if (t->join_block) e->join_block = t->join_block;
+  if (t->rows_piece) e->rows_piece = t->rows_piece;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -3590,6 +3790,9 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->row_gather = e->row_gather;
   t->spin_limit_log2 = 0;
   while (t->spin_limit_log2 < 31 && (1u << t->spin_limit_log2) < e->spin_limit) t->spin_limit_log2++;
+  t->radix_bits = e->radix_bits;
+  t->join_block = e->join_block;
+  t->rows_piece = e->rows_piece;
   return GDL_OK;
 }
 
@@ -3876,10 +4079,10 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
     if (!g_noalloc_addr[dev]) {
       void *p = nullptr;
       NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      NA_CK(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSortSmemBytes));
-      NA_CK(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSortSmemBytes));
+      NA_CK(cudaFuncSetAttribute(k_sort_hist<kRadixBits>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmemBytes));
+      NA_CK(cudaFuncSetAttribute(k_sort_pass<kRadixBits>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmemBytes));
       NA_CK(cudaFuncSetAttribute(k_merge_diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kMergeSmemBytes));
       g_noalloc_addr[dev] = p;
@@ -3925,9 +4128,9 @@ extern "C" gdl_status gdl_sort_unique_rows_noalloc(const uint64_t *device_rows, 
   a.max_tiles = kNoAllocSortTiles;
   a.counters = reinterpret_cast<u32 *>(base + kNaCounters);
   a.ctl = ctl;
-  k_sort_hist<<<blocks(rows, (u64)kSortTile * 4, 2), kSortBlock, kSortSmemBytes, s>>>(a);
+  k_sort_hist<kRadixBits><<<blocks(rows, (u64)kSortTile * 4, 2), kSortBlock, kSortSmemBytes, s>>>(a);
   for (int p = 0; p < a.passes; p++)
-    k_sort_pass<<<blocks(rows, kSortTile, 4), kSortBlock, kSortSmemBytes, s>>>(a, p);
+    k_sort_pass<kRadixBits><<<blocks(rows, kSortTile, 4), kSortBlock, kSortSmemBytes, s>>>(a, p);
   MergeArgs m;
   memset(&m, 0, sizeof m);
   m.newt = &d[0];

@@ -516,9 +516,9 @@ __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u3
 }
 
 // Units of work of the row-gather join: the in-edges of one y, cut into
-// pieces of at most kRowsPiece (a y with more in-edges than that is shared
-// by several warps, which OR their parts into the output row).
-constexpr u32 kRowsPiece = 32;
+// pieces of at most `piece` (<= 32, a tuning choice; a y with more in-edges
+// than that is shared by several warps, which OR their parts into the
+// output row).
 constexpr int kInvBlock = 1024;
 constexpr int kInvPer = 8;  // consecutive ids per thread and chunk
 
@@ -529,7 +529,8 @@ constexpr int kInvPer = 8;  // consecutive ids per thread and chunk
 // kInvPer consecutive ones read and written as 16-byte vectors; the two
 // prefix sums (edges low, pieces high) share one 64-bit block scan.
 __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *off, u32 *cur,
-                                                           u32 *poff, uint2 *pieces, int dk) {
+                                                           u32 *poff, uint2 *pieces, int dk,
+                                                           u32 piece) {
   __shared__ u64 s_warp[kInvBlock / 32];
   const u32 n = 1u << dk;  // a multiple of kInvPer
   u64 carry = 0;           // (pieces << 32) | edges of the chunks before
@@ -548,7 +549,7 @@ __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *
     u64 local = 0;
 #pragma unroll
     for (int i = 0; i < kInvPer; i++)
-      local += ((u64)((v[i] + kRowsPiece - 1) / kRowsPiece) << 32) | v[i];
+      local += ((u64)((v[i] + piece - 1) / piece) << 32) | v[i];
     u64 tot;
     const u64 ex = block_excl_scan<kInvBlock>(local, s_warp, &tot) + carry;
     carry += tot;
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *
       o[i] = e;
       po[i] = p;
       const u32 end = e + v[i];
-      for (u32 s = e; s < end; s += kRowsPiece) pieces[p++] = make_uint2(s, min(s + kRowsPiece, end));
+      for (u32 s = e; s < end; s += piece) pieces[p++] = make_uint2(s, min(s + piece, end));
       e = end;
     }
     uint4 *po4 = reinterpret_cast<uint4 *>(off + b), *pc4 = reinterpret_cast<uint4 *>(cur + b),

@@ -26,7 +26,12 @@ constexpr int kSortBlock = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kRadix = 256;
+// Digit width: 8 bits by default (kRadix buckets); the kernels are
+// templates over the width (6, 8 or 10 bits: 64, 256 or 1024 buckets), a
+// tuning choice (fewer, wider passes against larger histograms).
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kMaxRadix = 1024;
 constexpr int kMaxPasses = 8;
 
 struct SortArgs {
@@ -43,10 +48,11 @@ struct SortArgs {
   Ctl *ctl;
 };
 
+template <int BITS>
 __device__ __forceinline__ u32 sort_vkey_digit(u64 k, int kbits, int pass) {
   u64 mask = (kbits >= 32) ? 0xFFFFFFFFull : ((1ull << kbits) - 1);
   u64 v = ((k >> 32) << kbits) | (k & mask);
-  return (u32)(v >> (8 * pass)) & 0xFFu;
+  return (u32)(v >> (BITS * pass)) & ((1u << BITS) - 1u);
 }
 
 // Stable rank of the keys a block holds, for one digit position.  Keys are
@@ -55,16 +61,41 @@ __device__ __forceinline__ u32 sort_vkey_digit(u64 k, int kbits, int pass) {
 // Returns, per item, the key's position in the digit-sorted tile; also
 // leaves per-digit tile counts in s_cnt and exclusive digit starts in
 // s_start.  Invalid keys (past n) get digit kRadix and no position.
+template <int RADIX>
 struct RankSmem {
-  u32 whist[kSortWarps][kRadix + 1];
-  u32 cnt[kRadix + 1];
-  u32 start[kRadix + 1];
+  u32 whist[kSortWarps][RADIX + 1];
+  u32 cnt[RADIX + 1];
+  u32 start[RADIX + 1];
   u64 scan_tmp[kSortWarps];
 };
 
-template <int ITEMS>
+// Exclusive scan of n (<= kSortBlock * PER) counts in shared memory into
+// `out`, each thread PER consecutive ones; out[n] = the total.
+template <int PER>
+__device__ __forceinline__ void scan_counts(const u32 *cnt, u32 *out, int n, u64 *scan_tmp) {
+  u32 c[PER];
+  u64 v = 0;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int d = threadIdx.x * PER + j;
+    c[j] = d < n ? cnt[d] : 0u;
+    v += c[j];
+  }
+  u64 total;
+  u64 ex = block_excl_scan<kSortBlock>(v, scan_tmp, &total);
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int d = threadIdx.x * PER + j;
+    if (d < n) out[d] = (u32)ex;
+    ex += c[j];
+  }
+  if (threadIdx.x == 0) out[n] = (u32)total;
+}
+
+template <int ITEMS, int RADIX>
 __device__ __forceinline__ void rank_tile(const u32 (&digit)[ITEMS], u32 (&pos)[ITEMS],
-                                          RankSmem &sm) {
+                                          RankSmem<RADIX> &sm) {
+  constexpr int kRadix = RADIX;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int d = threadIdx.x; d < kSortWarps * (kRadix + 1); d += blockDim.x)
     (&sm.whist[0][0])[d] = 0;
@@ -95,14 +126,8 @@ __device__ __forceinline__ void rank_tile(const u32 (&digit)[ITEMS], u32 (&pos)[
     sm.cnt[d] = acc;
   }
   __syncthreads();
-  // Exclusive scan of the 256 digit counts (digit kRadix excluded).
-  {
-    u64 total;
-    u64 v = threadIdx.x < kRadix ? sm.cnt[threadIdx.x] : 0;
-    u64 ex = block_excl_scan<kSortBlock>(v, sm.scan_tmp, &total);
-    if (threadIdx.x < kRadix) sm.start[threadIdx.x] = (u32)ex;
-    if (threadIdx.x == 0) sm.start[kRadix] = (u32)total;
-  }
+  // Exclusive scan of the digit counts (digit kRadix, past n, excluded).
+  scan_counts<(kRadix + kSortBlock - 1) / kSortBlock>(sm.cnt, sm.start, kRadix, sm.scan_tmp);
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < ITEMS; i++) {
@@ -111,10 +136,11 @@ __device__ __forceinline__ void rank_tile(const u32 (&digit)[ITEMS], u32 (&pos)[
   }
 }
 
+template <int RADIX>
 struct SortSmem {
-  RankSmem rk;
+  RankSmem<RADIX> rk;
   u64 keys[kSortTile];
-  u32 gbase[kRadix];
+  u32 gbase[RADIX];
   long long tile;
 };
 
@@ -131,15 +157,18 @@ __device__ __forceinline__ void load_tile_keys(const u64 *src, u64 n, long long 
 }
 
 // Block 0 sorts a single tile entirely in shared memory.
-__device__ void small_sort(const SortArgs &a, u64 n, SortSmem &sm) {
+template <int BITS>
+__device__ void small_sort(const SortArgs &a, u64 n, SortSmem<1 << BITS> &sm) {
+  constexpr int kRadix = 1 << BITS;
   u64 k[kSortItems];
   bool valid[kSortItems];
   load_tile_keys(a.buf0, n, 0, k, valid);
   for (int p = 0; p < a.passes; p++) {
     u32 d[kSortItems], pos[kSortItems];
 #pragma unroll
-    for (int i = 0; i < kSortItems; i++) d[i] = valid[i] ? sort_vkey_digit(k[i], a.kbits, p) : kRadix;
-    rank_tile<kSortItems>(d, pos, sm.rk);
+    for (int i = 0; i < kSortItems; i++)
+      d[i] = valid[i] ? sort_vkey_digit<BITS>(k[i], a.kbits, p) : kRadix;
+    rank_tile<kSortItems, kRadix>(d, pos, sm.rk);
 #pragma unroll
     for (int i = 0; i < kSortItems; i++)
       if (valid[i]) sm.keys[pos[i]] = k[i];
@@ -164,9 +193,11 @@ __device__ void small_sort(const SortArgs &a, u64 n, SortSmem &sm) {
   }
 }
 
+template <int BITS>
 __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
+  constexpr int kRadix = 1 << BITS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SortSmem &sm = *reinterpret_cast<SortSmem *>(smem_raw);
+  SortSmem<kRadix> &sm = *reinterpret_cast<SortSmem<kRadix> *>(smem_raw);
   __shared__ u32 s_hist[kMaxPasses][kRadix];
   if (ctl_stop(a.ctl)) return;
   const u64 n = a.keys->n;
@@ -174,7 +205,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0)
     prof_add(a.ctl, kPSortHist, n <= (u64)kSortTile ? 16 * n : 8 * n);
   if (n <= (u64)kSortTile) {
-    if (blockIdx.x == 0) small_sort(a, n, sm);
+    if (blockIdx.x == 0) small_sort<BITS>(a, n, sm);
     return;
   }
   const u64 tiles = (n + kSortTile - 1) / kSortTile;
@@ -194,7 +225,8 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
     u64 k = a.buf0[i];
-    for (int p = 0; p < a.passes; p++) atomicAdd(&s_hist[p][sort_vkey_digit(k, a.kbits, p)], 1u);
+    for (int p = 0; p < a.passes; p++)
+      atomicAdd(&s_hist[p][sort_vkey_digit<BITS>(k, a.kbits, p)], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < a.passes * kRadix; i += blockDim.x) {
@@ -212,10 +244,14 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   if (!s_last) return;
   __threadfence();
   for (int p = 0; p < a.passes; p++) {
-    u64 total;
-    u64 v = threadIdx.x < kRadix ? *((volatile u32 *)&a.offsets[p * kRadix + threadIdx.x]) : 0;
-    u64 ex = block_excl_scan<kSortBlock>(v, sm.rk.scan_tmp, &total);
-    if (threadIdx.x < kRadix) a.offsets[p * kRadix + threadIdx.x] = (u32)ex;
+    // (through shared memory: the counts, then their exclusive offsets)
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x)
+      sm.rk.cnt[d] = *((volatile u32 *)&a.offsets[p * kRadix + d]);
+    __syncthreads();
+    scan_counts<(kRadix + kSortBlock - 1) / kSortBlock>(sm.rk.cnt, sm.rk.start, kRadix,
+                                                        sm.rk.scan_tmp);
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) a.offsets[p * kRadix + d] = sm.rk.start[d];
     __syncthreads();
   }
   if (threadIdx.x == 0) {
@@ -225,9 +261,11 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   }
 }
 
+template <int BITS>
 __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) {
+  constexpr int kRadix = 1 << BITS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SortSmem &sm = *reinterpret_cast<SortSmem *>(smem_raw);
+  SortSmem<kRadix> &sm = *reinterpret_cast<SortSmem<kRadix> *>(smem_raw);
   if (ctl_stop(a.ctl)) return;
   const u64 n = a.keys->n;
   if (n <= (u64)kSortTile) return;
@@ -249,11 +287,12 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) 
     load_tile_keys(src, n, tile, k, valid);
     u32 d[kSortItems], pos[kSortItems];
 #pragma unroll
-    for (int i = 0; i < kSortItems; i++) d[i] = valid[i] ? sort_vkey_digit(k[i], a.kbits, pass) : kRadix;
-    rank_tile<kSortItems>(d, pos, sm.rk);
-    // Publish this tile's per-digit count, look back for the prefix.
-    if (threadIdx.x < kRadix) {
-      const int dg = threadIdx.x;
+    for (int i = 0; i < kSortItems; i++)
+      d[i] = valid[i] ? sort_vkey_digit<BITS>(k[i], a.kbits, pass) : kRadix;
+    rank_tile<kSortItems, kRadix>(d, pos, sm.rk);
+    // Publish this tile's per-digit count, look back for the prefix (a
+    // thread per digit, or per kRadix / kSortBlock digits in turn).
+    for (int dg = threadIdx.x; dg < kRadix; dg += blockDim.x) {
       const u32 c = sm.rk.cnt[dg];
       u32 *st = status + (u64)tile * kRadix + dg;
       if (tile == 0) {
@@ -288,7 +327,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) 
     const u64 in_tile = min((u64)kSortTile, n - (u64)tile * kSortTile);
     for (u32 i = threadIdx.x; i < in_tile; i += blockDim.x) {
       u64 key = sm.keys[i];
-      u32 dg = sort_vkey_digit(key, a.kbits, pass);
+      u32 dg = sort_vkey_digit<BITS>(key, a.kbits, pass);
       u64 g = (u64)sm.gbase[dg] + (i - sm.rk.start[dg]);
       if (g < n && g < a.cap)
         dst[g] = key;
@@ -316,6 +355,10 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_pass(SortArgs a, int pass) 
   }
 }
 
-constexpr size_t kSortSmemBytes = sizeof(SortSmem);
+template <int BITS>
+constexpr size_t sort_smem_bytes() {
+  return sizeof(SortSmem<1 << BITS>);
+}
+constexpr size_t kSortSmemBytes = sort_smem_bytes<kRadixBits>();
 
 }  // namespace gdl

@@ -11,11 +11,11 @@
 // registers (transpose32) and exchanged through a padded shared buffer.
 //
 // Pipeline per block (a persistent grid, tiles t = blockIdx.x + k*gridDim.x):
-// the loads of tile k+1 are issued into the other slot while tile k is
-// processed; tile k's outputs are written into an output slot and stored
-// with one bulk group after the block's barrier; before that barrier the
-// issuing thread waits until the group of tile k-1 has read its slot, so
-// tile k+1 may overwrite it.  Every mbarrier wait is bounded (Ctl::spin_limit
+// the loads of tiles k+1 .. k+ns-1 are in flight in the other input stages
+// while tile k is processed; tile k's outputs are written into one of two
+// output slots and stored with one bulk group after the block's barrier;
+// before that barrier the issuing thread waits until the group of tile k-1
+// has read its slot, so tile k+1 may overwrite it.  Every mbarrier wait is bounded (Ctl::spin_limit
 // polls): a wait that gives up raises Ctl::timeout, the block stores
 // nothing more, waits (bounded) for its loads in flight and its stores, and
 // returns.  No multicast, no cluster: every load reads this GPU's memory.
@@ -120,30 +120,37 @@ __device__ __forceinline__ u32 block_flags(u32 *s_wf, u32 f, int wid) {
   return r;
 }
 
-// Shared memory: dynamic, 1024-byte aligned by hand.
-__host__ __device__ constexpr u32 upd_tma_smem(int has_dt) {
-  // in: 2 slots x (NEWT, FULL); out: 2 slots x (FULL', DELTA rows[, DELTA^T]);
-  // one zero tile; alignment slack
-  return 2 * 2 * kTmaTile + 2 * (has_dt ? 3 : 2) * kTmaTile + kTmaTile + 1024;
+// Input stages: loads run ns - 1 tiles ahead of the tile being processed.
+constexpr int kTmaMaxStages = 4;
+// Shared memory: dynamic, 1024-byte aligned by hand.  Update pass: ns
+// stages of (NEWT, FULL) tiles, 2 output slots of (FULL', DELTA rows[,
+// DELTA^T]), one zero tile, alignment slack.
+__host__ __device__ constexpr u32 upd_tma_smem(int ns, int has_dt) {
+  return ns * 2 * kTmaTile + 2 * (has_dt ? 3 : 2) * kTmaTile + kTmaTile + 1024;
 }
-__host__ __device__ constexpr u32 fold_tma_smem() {
-  // in: 2 slots x (src, dst); out: 2 slots x dst; one zero tile
-  return 2 * 2 * kTmaTile + 2 * kTmaTile + kTmaTile + 1024;
+// Fold: ns stages of the source tile (and the destination's, unless it is
+// overwritten), 2 output slots, one zero tile.
+__host__ __device__ constexpr u32 fold_tma_smem(int ns, int overwrite) {
+  return ns * (overwrite ? 1 : 2) * kTmaTile + 2 * kTmaTile + kTmaTile + 1024;
 }
+// Stages that keep two blocks of 256 threads on an SM (static shared memory
+// about 10 KB a block) for the update pass, three for an overwriting fold.
+__host__ __device__ constexpr int upd_tma_stages(int has_dt) { return has_dt ? 2 : 3; }
+__host__ __device__ constexpr int fold_tma_stages(int overwrite) { return overwrite ? 4 : 3; }
 
 enum UpdFlag : u32 { kFAnyN = 1, kFAnyG = 2, kFFail = 4 };
 
 // k_bm_update_t (pull.cuh) with TMA tiles.  gt: NEWT is the transposed
 // twin (m.nsrc over it; cleared where it has bits); else NEWT is the row
 // bitmap G (m.nsrc over G; cleared where it has bits).  has_dn / has_dt:
-// write DELTA's rows / DELTA transposed (every word).
+// write DELTA's rows / DELTA transposed (every word).  ns input stages.
 __global__ void __launch_bounds__(kTrBlock, 2)
     k_bm_update_tma(BmScanArgs a, const __grid_constant__ UpdMaps m, int dk, int gt, int has_dn,
-                    int has_dt) {
+                    int has_dt, int ns) {
   extern __shared__ unsigned char tma_smem_raw[];
   __shared__ u32 s_t[256][9];
   __shared__ u32 s_wf[2][kTrBlock / 32];
-  __shared__ __align__(8) u64 s_bar[2];
+  __shared__ __align__(8) u64 s_bar[kTmaMaxStages];
   __shared__ unsigned long long s_cnt[2];
   __shared__ int s_skip;
   if (threadIdx.x == 0) s_skip = ctl_stop(a.ctl) || write_gate_closed(a);
@@ -151,16 +158,16 @@ __global__ void __launch_bounds__(kTrBlock, 2)
   if (s_skip) return;
   unsigned char *base = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tma_smem_raw) + 1023) & ~uintptr_t(1023));
-  // slot s: NEWT tile at 2s, FULL tile at 2s + 1; outputs from tile 4 on,
-  // nout per slot; then the zero tile
+  // stage s: NEWT tile at 2s, FULL tile at 2s + 1; output slot o from tile
+  // 2 ns + o nout on; then the zero tile
   const int nout = has_dt ? 3 : 2;
   auto tile_at = [&](int i) { return reinterpret_cast<u32 *>(base + i * kTmaTile); };
-  auto in_n = [&](int s) { return tile_at(2 * s); };
-  auto in_f = [&](int s) { return tile_at(2 * s + 1); };
-  auto out_f = [&](int s) { return tile_at(4 + s * nout); };
-  auto out_dn = [&](int s) { return tile_at(4 + s * nout + 1); };
-  auto out_dt = [&](int s) { return tile_at(4 + s * nout + 2); };
-  u32 *zero = tile_at(4 + 2 * nout);
+  auto in_n = [&](int st) { return tile_at(2 * st); };
+  auto in_f = [&](int st) { return tile_at(2 * st + 1); };
+  auto out_f = [&](int o) { return tile_at(2 * ns + o * nout); };
+  auto out_dn = [&](int o) { return tile_at(2 * ns + o * nout + 1); };
+  auto out_dt = [&](int o) { return tile_at(2 * ns + o * nout + 2); };
+  u32 *zero = tile_at(2 * ns + 2 * nout);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const u64 per = 1ull << (dk - 8);
   const u64 tiles = per * per;
@@ -169,34 +176,38 @@ __global__ void __launch_bounds__(kTrBlock, 2)
     reinterpret_cast<uint4 *>(zero)[i] = make_uint4(0, 0, 0, 0);
   fence_async_smem();
   if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+    for (int i = 0; i < ns; i++) mbar_init(&s_bar[i], 1);
     s_cnt[0] = s_cnt[1] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // tile t's NEWT tile: (tr, tc) of G, or (tc, tr) of the twin
-  auto issue = [&](u64 t, int slot) {
-    const int tr = (int)(t / per), tc = (int)(t % per);
-    mbar_expect_tx(&s_bar[slot], 2 * kTmaTile);
+  // the block's j-th tile is blockIdx.x + j gridDim.x, in stage j % ns;
+  // its NEWT tile is (tr, tc) of G, or (tc, tr) of the twin
+  const u64 mine = tiles > blockIdx.x ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto issue = [&](u64 j) {
+    const u64 t = blockIdx.x + j * gridDim.x;
+    const int tr = (int)(t / per), tc = (int)(t % per), st = (int)(j % ns);
+    mbar_expect_tx(&s_bar[st], 2 * kTmaTile);
     if (gt)
-      tma_load(in_n(slot), &m.nsrc, tr * 8, tc * 256, &s_bar[slot]);
+      tma_load(in_n(st), &m.nsrc, tr * 8, tc * 256, &s_bar[st]);
     else
-      tma_load(in_n(slot), &m.nsrc, tc * 8, tr * 256, &s_bar[slot]);
-    tma_load(in_f(slot), &m.f, tc * 8, tr * 256, &s_bar[slot]);
+      tma_load(in_n(st), &m.nsrc, tc * 8, tr * 256, &s_bar[st]);
+    tma_load(in_f(st), &m.f, tc * 8, tr * 256, &s_bar[st]);
   };
-  if (tid == 0 && (u64)blockIdx.x < tiles) issue(blockIdx.x, 0);
+  if (tid == 0)
+    for (u64 j = 0; j + 1 < (u64)ns && j < mine; j++) issue(j);
   u64 n_delta = 0, n_newt = 0, moved = 0;
-  bool failed = false, next_issued = false;
-  int k = 0;
-  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x, k++) {
-    const int slot = k & 1;
+  bool failed = false;
+  u64 k = 0;
+  for (; k < mine; k++) {
+    const u64 t = blockIdx.x + k * gridDim.x;
+    const int st = (int)(k % ns), slot = (int)(k & 1);
     const int tr = (int)(t / per), tc = (int)(t % per);
-    next_issued = t + gridDim.x < tiles;
-    if (tid == 0 && next_issued) issue(t + gridDim.x, slot ^ 1);
-    const bool ok = mbar_wait(&s_bar[slot], (u32)(k >> 1) & 1u, limit);
+    // (stage (k + ns - 1) % ns held tile k - 1, read before the last barrier)
+    if (tid == 0 && k + ns - 1 < mine) issue(k + ns - 1);
+    const bool ok = mbar_wait(&s_bar[st], (u32)(k / ns) & 1u, limit);
     u32 v[8], g[8], f[8], d[8];
-    lds8(in_n(slot) + tid * 8, v);
+    lds8(in_n(st) + tid * 8, v);
     const bool any_n = any8(v);
     if (gt) {
       // the twin's rows are NEWT's columns: transpose (lane j of warp w,
@@ -210,7 +221,7 @@ __global__ void __launch_bounds__(kTrBlock, 2)
 #pragma unroll
       for (int i = 0; i < 8; i++) g[i] = v[i];
     }
-    lds8(in_f(slot) + tid * 8, f);
+    lds8(in_f(st) + tid * 8, f);
     const bool any_g = any8(g);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -264,9 +275,9 @@ __global__ void __launch_bounds__(kTrBlock, 2)
   if (failed && tid == 0) {
     atomicOr(&a.ctl->timeout, 1u);
     // loads that may still be in flight into this block's shared memory:
-    // the tile whose wait gave up, and the next one (bounded waits)
-    mbar_wait(&s_bar[k & 1], (u32)(k >> 1) & 1u, limit);
-    if (next_issued) mbar_wait(&s_bar[(k & 1) ^ 1], (u32)((k + 1) >> 1) & 1u, limit);
+    // tile k (whose wait gave up) and the ones issued after it (bounded)
+    for (u64 j = k; j < k + ns - 1 && j < mine; j++)
+      mbar_wait(&s_bar[j % ns], (u32)(j / ns) & 1u, limit);
   }
   if (tid == 0) tma_wait_done();
 #pragma unroll
@@ -295,23 +306,25 @@ __global__ void __launch_bounds__(kTrBlock, 2)
 
 // k_bm_fold_t (pull.cuh) with TMA tiles: dst |= transpose(src) (or, with
 // overwrite, dst := transpose(src), every word stored), src cleared where it
-// has bits, the dirty map of dst set for its non-zero rows.
+// has bits, the dirty map of dst set for its non-zero rows.  ns input stages.
 __global__ void __launch_bounds__(kTrBlock, 2)
-    k_bm_fold_tma(const __grid_constant__ FoldMaps m, u8 *dirty, int dk, int overwrite, Ctl *ctl) {
+    k_bm_fold_tma(const __grid_constant__ FoldMaps m, u8 *dirty, int dk, int overwrite, int ns,
+                  Ctl *ctl) {
   extern __shared__ unsigned char tma_smem_raw[];
   __shared__ u32 s_t[256][9];
   __shared__ u32 s_wf[2][kTrBlock / 32];
-  __shared__ __align__(8) u64 s_bar[2];
+  __shared__ __align__(8) u64 s_bar[kTmaMaxStages];
   if (ctl_stop(ctl)) return;
   unsigned char *base = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tma_smem_raw) + 1023) & ~uintptr_t(1023));
-  // slot s: source tile at 2s, destination tile at 2s + 1, output at 4 + s;
-  // then the zero tile
+  // stage s: source tile at ni s, destination tile at ni s + 1 (ni = 2
+  // unless overwriting); output slot o at ni ns + o; then the zero tile
+  const int ni = overwrite ? 1 : 2;
   auto tile_at = [&](int i) { return reinterpret_cast<u32 *>(base + i * kTmaTile); };
-  auto in_s = [&](int s) { return tile_at(2 * s); };
-  auto in_d = [&](int s) { return tile_at(2 * s + 1); };
-  auto out = [&](int s) { return tile_at(4 + s); };
-  u32 *zero = tile_at(6);
+  auto in_s = [&](int st) { return tile_at(ni * st); };
+  auto in_d = [&](int st) { return tile_at(ni * st + 1); };
+  auto out = [&](int o) { return tile_at(ni * ns + o); };
+  u32 *zero = tile_at(ni * ns + 2);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int rs = dk - 5;
   const u64 per = 1ull << (dk - 8);
@@ -321,30 +334,32 @@ __global__ void __launch_bounds__(kTrBlock, 2)
     reinterpret_cast<uint4 *>(zero)[i] = make_uint4(0, 0, 0, 0);
   fence_async_smem();
   if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+    for (int i = 0; i < ns; i++) mbar_init(&s_bar[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // tile t: src tile (tr, tc), dst tile (tc, tr)
-  auto issue = [&](u64 t, int slot) {
-    const int tr = (int)(t / per), tc = (int)(t % per);
-    mbar_expect_tx(&s_bar[slot], (overwrite ? 1 : 2) * kTmaTile);
-    tma_load(in_s(slot), &m.src, tc * 8, tr * 256, &s_bar[slot]);
-    if (!overwrite) tma_load(in_d(slot), &m.dst, tr * 8, tc * 256, &s_bar[slot]);
+  // the block's j-th tile: src tile (tr, tc), dst tile (tc, tr)
+  const u64 mine = tiles > blockIdx.x ? (tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto issue = [&](u64 j) {
+    const u64 t = blockIdx.x + j * gridDim.x;
+    const int tr = (int)(t / per), tc = (int)(t % per), st = (int)(j % ns);
+    mbar_expect_tx(&s_bar[st], ni * kTmaTile);
+    tma_load(in_s(st), &m.src, tc * 8, tr * 256, &s_bar[st]);
+    if (!overwrite) tma_load(in_d(st), &m.dst, tr * 8, tc * 256, &s_bar[st]);
   };
-  if (tid == 0 && (u64)blockIdx.x < tiles) issue(blockIdx.x, 0);
+  if (tid == 0)
+    for (u64 j = 0; j + 1 < (u64)ns && j < mine; j++) issue(j);
   u64 moved = 0;
-  bool failed = false, next_issued = false;
-  int k = 0;
-  for (u64 t = blockIdx.x; t < tiles; t += gridDim.x, k++) {
-    const int slot = k & 1;
+  bool failed = false;
+  u64 k = 0;
+  for (; k < mine; k++) {
+    const u64 t = blockIdx.x + k * gridDim.x;
+    const int st = (int)(k % ns), slot = (int)(k & 1);
     const int tr = (int)(t / per), tc = (int)(t % per);
-    next_issued = t + gridDim.x < tiles;
-    if (tid == 0 && next_issued) issue(t + gridDim.x, slot ^ 1);
-    const bool ok = mbar_wait(&s_bar[slot], (u32)(k >> 1) & 1u, limit);
+    if (tid == 0 && k + ns - 1 < mine) issue(k + ns - 1);
+    const bool ok = mbar_wait(&s_bar[st], (u32)(k / ns) & 1u, limit);
     u32 v[8], q[8];
-    lds8(in_s(slot) + tid * 8, v);
+    lds8(in_s(st) + tid * 8, v);
     const bool any_s = __syncthreads_or(any8(v));  // (block-uniform)
     bool any_q = false;
     if (any_s) {
@@ -360,7 +375,7 @@ __global__ void __launch_bounds__(kTrBlock, 2)
     }
     if (!overwrite) {
       u32 dd[8];
-      lds8(in_d(slot) + tid * 8, dd);
+      lds8(in_d(st) + tid * 8, dd);
 #pragma unroll
       for (int i = 0; i < 8; i++) q[i] |= dd[i];
       if (any_q && dirty)
@@ -383,8 +398,8 @@ __global__ void __launch_bounds__(kTrBlock, 2)
   }
   if (failed && tid == 0) {
     atomicOr(&ctl->timeout, 1u);
-    mbar_wait(&s_bar[k & 1], (u32)(k >> 1) & 1u, limit);
-    if (next_issued) mbar_wait(&s_bar[(k & 1) ^ 1], (u32)((k + 1) >> 1) & 1u, limit);
+    for (u64 j = k; j < k + ns - 1 && j < mine; j++)
+      mbar_wait(&s_bar[j % ns], (u32)(j / ns) & 1u, limit);
   }
   if (tid == 0) tma_wait_done();
 #pragma unroll

@@ -62,7 +62,8 @@ class Tuning(C.Structure):
                 ("index_slots_per_key", C.c_int32), ("dirty_min_log2_words", C.c_int32),
                 ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32),
                 ("pull_joins", C.c_int32), ("row_gather", C.c_int32),
-                ("spin_limit_log2", C.c_int32)]
+                ("spin_limit_log2", C.c_int32), ("radix_bits", C.c_int32),
+                ("join_block", C.c_int32), ("rows_piece", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -169,6 +170,12 @@ def load_library(kind: str) -> C.CDLL:
         lib.gdl_relation_load_tsv.restype = _I
         lib.gdl_relation_dump_tsv.argtypes = [_P, _I, _I, C.c_char_p, _PU64]
         lib.gdl_relation_dump_tsv.restype = _I
+        lib.gdl_join_count.argtypes = [_P, _I, _I, _I, _I, _PU64]
+        lib.gdl_join_count.restype = _I
+        lib.gdl_relation_export_device.argtypes = [_P, _I, _I, _P, _U64, _PU64]
+        lib.gdl_relation_export_device.restype = _I
+        lib.gdl_partition_rows.argtypes = [_P, _P, _U64, _I, _I, _P, _PU64]
+        lib.gdl_partition_rows.restype = _I
     else:
         f = lambda n: getattr(lib, pre + n)  # noqa: E731
         f("engine_create").argtypes = [_I, _I, C.POINTER(_P)]
@@ -183,6 +190,9 @@ def load_library(kind: str) -> C.CDLL:
         f("threads").restype = _I
         f("lie_seconds").argtypes = [_P, _I, C.POINTER(C.c_double)]
         f("lie_seconds").restype = _I
+        if kind == "oracle":
+            f("join_count").argtypes = [_P, _I, _I, _I, _I, _PU64]
+            f("join_count").restype = _I
     _libs[kind] = lib
     return lib
 
@@ -488,6 +498,17 @@ class Engine:
         self._call("relation_digest", rel.id, version, C.byref(out))
         return int(out.value)
 
+    def join_count(self, inner: Relation, inner_version: int, outer: Relation,
+                   outer_version: int) -> int:
+        """Output size of a join before deduplication: (outer row, inner row)
+        pairs that agree on column 0 (the join's count pass; the reference's
+        get_join_result_size summed, src/relation.cu:221-288)."""
+        if self.kind not in ("gpu", "oracle"):
+            raise GdlError(4, f"join_count is not available on the {self.kind} engine")
+        out = C.c_uint64(0)
+        self._call("join_count", inner.id, inner_version, outer.id, outer_version, C.byref(out))
+        return int(out.value)
+
     def lie(self) -> Lie:
         lid = C.c_int32(-1)
         self._call("lie_create", C.byref(lid))
@@ -540,6 +561,24 @@ class Engine:
     def load_device(self, rel: Relation, ptr: int, n_rows: int) -> None:
         """load_relation from rows already in device memory (n_rows x 2 u64)."""
         self._check(self.lib.gdl_relation_load_device(self.h, rel.id, C.c_void_p(ptr), n_rows))
+
+    def export_device(self, rel: Relation, version: int, ptr: int, cap_rows: int) -> int:
+        """One version's sorted rows (arity 2) into device memory at ptr
+        (room for cap_rows rows of two u64); returns the row count."""
+        n = C.c_uint64(0)
+        self._check(self.lib.gdl_relation_export_device(self.h, rel.id, version, C.c_void_p(ptr),
+                                                        cap_rows, C.byref(n)))
+        return int(n.value)
+
+    def partition_rows(self, ptr: int, n_rows: int, column: int, world: int,
+                       out_ptr: int) -> list:
+        """Group n_rows device rows (two u64 columns) by owner = column value
+        % world into out_ptr, one block per destination in rank order;
+        returns the block sizes."""
+        counts = (C.c_uint64 * world)()
+        self._check(self.lib.gdl_partition_rows(self.h, C.c_void_p(ptr), n_rows, column, world,
+                                                C.c_void_p(out_ptr), counts))
+        return [int(x) for x in counts]
 
     # -- per-kernel accounting (GPU only) -----------------------------------
     def set_profile(self, flag: bool) -> None:

@@ -30,6 +30,13 @@ tmp(b, x) :- edge(a, x), sg(a, b) and sg(x, y) :- edge(b, y), tmp(b, x) —
 read only owned keys; a pass routes tmp candidates to owner(b), then sg
 candidates to owner(x).  Its non-recursive rule sg(x, y) :- edge(p, x),
 edge(p, y), x != y runs as its own loop, as the driver's first LIE does.
+
+On the CUDA engine both drivers keep the exchange on the device
+(`DeviceExchange`): a pass exports its candidates into a device tensor,
+groups them by owner with a kernel, sends them with one all_to_all_single
+of the grouped rows and loads what it receives from device memory, where
+the engine sorts and deduplicates it; the host handles the per-destination
+counts only.  On the oracle the rows go through the host (`route`).
 """
 from __future__ import annotations
 
@@ -74,6 +81,71 @@ def route(rows: np.ndarray, dest: np.ndarray, world: int, device=None) -> np.nda
     return _unpack(out)
 
 
+class DeviceExchange:
+    """A rank's exchange kept in device memory (GPU engine):
+      * rows(rel, version): the version's sorted rows as an (n, 2) int64
+        tensor (gdl_relation_export_device);
+      * route(rows, col): every row to the owner of its column `col`
+        (rows grouped by gdl_partition_rows, one all_to_all_single of the
+        counts, one of the grouped rows: NCCL moves device memory directly;
+        the gloo backend stages the grouped rows through host memory for
+        the collective itself);
+      * load(rel, rows): load_relation from device memory (sorted and
+        deduplicated by the engine);
+      * load_set(rel, rows): the same for rows that may repeat, loaded so
+        that the relation's raw order holds each tuple once (an update
+        relation's DELTA at LIE start is the first |FULL| of its rows in
+        load order, src/lie.cu:49-59: a repeat would hide a tuple): the
+        rows are deduplicated through a scratch relation first.
+    The engine's calls return after its stream has finished; collectives
+    run on torch's stream, which is synchronised before the engine reads
+    their output."""
+
+    def __init__(self, eng: Engine, world: int, device):
+        self.eng, self.world = eng, world
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None \
+            else torch.device(device)
+        self.nccl = dist.get_backend() == "nccl"
+        self.scratch = eng.relation("_exchange_set", index_flag=False)
+
+    def rows(self, rel, version=FULL) -> torch.Tensor:
+        n = self.eng.size(rel, version)
+        if n == 0:
+            return torch.zeros((0, 2), dtype=torch.int64, device=self.device)
+        t = torch.empty((n, 2), dtype=torch.int64, device=self.device)
+        got = self.eng.export_device(rel, version, t.data_ptr(), n)
+        return t[:got]
+
+    def route(self, rows: torch.Tensor, col: int) -> torch.Tensor:
+        n = rows.shape[0]
+        grouped = torch.empty_like(rows)
+        counts = self.eng.partition_rows(rows.data_ptr() if n else 0, n, col, self.world,
+                                         grouped.data_ptr() if n else 0)
+        cdev = self.device if self.nccl else "cpu"
+        sc = torch.tensor(counts, dtype=torch.int64, device=cdev)
+        rc = torch.empty_like(sc)
+        dist.all_to_all_single(rc, sc)
+        recv = rc.tolist()
+        src = grouped if self.nccl else grouped.cpu()
+        out = torch.empty((sum(recv), 2), dtype=torch.int64, device=src.device)
+        dist.all_to_all_single(out, src, recv, counts)
+        if not self.nccl:
+            out = out.to(self.device)
+        torch.cuda.synchronize(self.device)
+        return out
+
+    def load(self, rel, rows: torch.Tensor) -> None:
+        if rows.shape[0] == 0:
+            self.eng.load(rel, None)
+        else:
+            rows = rows.contiguous()
+            self.eng.load_device(rel, rows.data_ptr(), rows.shape[0])
+
+    def load_set(self, rel, rows: torch.Tensor) -> None:
+        self.load(self.scratch, rows)
+        self.load(rel, self.rows(self.scratch))
+
+
 @dataclass
 class PartResult:
     passes: int = 0
@@ -82,10 +154,13 @@ class PartResult:
 
 
 def partitioned_tc(eng: Engine, edges: np.ndarray, rank: int, world: int,
-                   device=None) -> PartResult:
+                   device=None, resident: bool | None = None) -> PartResult:
     """Transitive closure of `edges` (every rank passes the same edges) with
     path partitioned over the ranks; returns this rank's FULL partition and
-    the pass count (equal on every rank)."""
+    the pass count (equal on every rank).  resident (default: on the CUDA
+    engine): the exchange stays on the device (DeviceExchange)."""
+    if resident is None:
+        resident = eng.kind == "gpu"
     e = np.asarray(edges, dtype=np.uint64).reshape(-1, 2)
     mine_e = e[owner(e[:, 1], world) == rank]
     mine_p = e[owner(e[:, 0], world) == rank]
@@ -115,6 +190,26 @@ def partitioned_tc(eng: Engine, edges: np.ndarray, rank: int, world: int,
     merge.max_iteration = 0
     res = PartResult()
     empty = np.zeros((0, 2), dtype=np.uint64)
+    if resident:
+        x = DeviceExchange(eng, world, device)
+        while True:
+            res.passes += 1
+            eng.load(C, None)
+            join.fixpoint()
+            # candidates to the owners of their first column, deduplicated
+            # on the device; the new ones are the next pass's outer
+            x.load_set(R, x.route(x.rows(C), 0))
+            merge.fixpoint()
+            new = x.rows(P, DELTA)
+            x.load(D, new)
+            n = torch.tensor([new.shape[0]], dtype=torch.int64,
+                             device=x.device if x.nccl else "cpu")
+            dist.all_reduce(n)
+            res.per_pass_new.append(int(n.item()))
+            if n.item() == 0:
+                break
+        res.full = P.rows() if P.size() else empty
+        return res
     while True:
         res.passes += 1
         # 1. candidates of the local join
@@ -220,10 +315,13 @@ class PartSG:
 
 
 def partitioned_sg(eng: Engine, edges: np.ndarray, rank: int, world: int,
-                   device=None) -> PartSG:
+                   device=None, resident: bool | None = None) -> PartSG:
     """Same generation of `edges` (every rank passes the same edges) with sg
     partitioned over the ranks; returns this rank's sg partition and the
-    loop-pass counts of the two LIEs (equal on every rank)."""
+    loop-pass counts of the two LIEs (equal on every rank).  resident
+    (default: on the CUDA engine): the exchange stays on the device."""
+    if resident is None:
+        resident = eng.kind == "gpu"
     e = np.asarray(edges, dtype=np.uint64).reshape(-1, 2)
     E = eng.relation("edge_2__1_2")
     mine = e[owner(e[:, 0], world) == rank]
@@ -232,6 +330,8 @@ def partitioned_sg(eng: Engine, edges: np.ndarray, rank: int, world: int,
     D = eng.relation("sg_delta")
     T = eng.relation("tmp")
     res = PartSG()
+    if resident:
+        return _partitioned_sg_resident(eng, E, sg, D, T, world, device, res)
     # sg(x, y) :- edge(p, x), edge(p, y), x != y: its own loop (the second
     # pass finds nothing new, as the driver's first LIE does)
     init = _Join(eng, E, E, (INNER(1), OUTER(1)), pred=(PRED_NE, 0, 1), name="cand_init")
@@ -255,6 +355,48 @@ def partitioned_sg(eng: Engine, edges: np.ndarray, rank: int, world: int,
         # sg(x, y) :- edge(b, y), tmp(b, x): to owner(x), deduplicated there
         delta = sg.merge(_to_owners(sg_join.run(), 0, world, device))
         if _any(len(delta), device) == 0:
+            break
+    res.full = sg.rows()
+    return res
+
+
+def _partitioned_sg_resident(eng, E, sg, D, T, world, device, res) -> PartSG:
+    """partitioned_sg with every pass's rows kept on the device."""
+    x = DeviceExchange(eng, world, device)
+
+    def merge(rows: torch.Tensor) -> torch.Tensor:
+        # sg's update: the received rows copied into its FULL partition
+        # (deduplicated first, see DeviceExchange.load_set); the new ones
+        x.load_set(sg.recv, rows)
+        sg.lie.fixpoint()
+        return x.rows(sg.full, DELTA)
+
+    def any_rank(n: int) -> int:
+        t = torch.tensor([n], dtype=torch.int64, device=x.device if x.nccl else "cpu")
+        dist.all_reduce(t)
+        return int(t.item())
+
+    init = _Join(eng, E, E, (INNER(1), OUTER(1)), pred=(PRED_NE, 0, 1), name="cand_init")
+    while True:
+        res.init_passes += 1
+        eng.load(init.out, None)
+        init.lie.fixpoint()
+        new = merge(x.route(x.rows(init.out), 0))
+        if any_rank(new.shape[0]) == 0:
+            break
+    delta = x.rows(sg.full)
+    tmp_join = _Join(eng, E, D, (OUTER(1), INNER(1)), name="cand_tmp")
+    sg_join = _Join(eng, E, T, (OUTER(1), INNER(1)), name="cand_sg")
+    while True:
+        res.passes += 1
+        x.load(D, delta)
+        eng.load(tmp_join.out, None)
+        tmp_join.lie.fixpoint()
+        x.load(T, x.route(x.rows(tmp_join.out), 0))
+        eng.load(sg_join.out, None)
+        sg_join.lie.fixpoint()
+        delta = merge(x.route(x.rows(sg_join.out), 0))
+        if any_rank(delta.shape[0]) == 0:
             break
     res.full = sg.rows()
     return res

@@ -13,9 +13,13 @@ streams).  Relations live on the device from load to result.
 
 Admission uses an HBM estimate per query: the bitmaps of its relations
 (n^2 / 8 bytes each, three per updated relation plus NEWT of the tmp
-relation) plus 16 bytes per candidate of its first join, which is the
-sum k_join_count forms (per outer row, the length of the inner run it
-probes) taken here from the graph's degrees.  The same candidate count
+relation) plus 16 bytes per candidate of its first join.  The candidates
+come from that join's count pass on the device (gdl_join_count: the
+query's relations are loaded into an estimator engine as its program loads
+them, and k_join_count sums, per outer row, the length of the inner run it
+probes), taken as each query arrives; `hbm_estimate` derives the same count
+from the graph's degrees on the host and serves as its cross-check and for
+streams that are not served on a GPU.  The same candidate count
 bounds the largest list the batch's first fixpoint hands to the next one,
 so a batch is also capped at half of the engine's list limit (2^30 rows)
 in summed candidates.  Later iterations can still outgrow a list (a batch of
@@ -48,7 +52,7 @@ import numpy as np
 import batch as B
 import programs as P
 import workloads as W
-from gdlog_b200 import Engine, GdlError
+from gdlog_b200 import FULL, Engine, GdlError
 
 # gdl_status codes of a batch too large for the engine (include/gdlog_b200.h)
 _TOO_LARGE = (3, 4)  # GDL_E_NOMEM, GDL_E_UNSUPPORTED
@@ -113,6 +117,31 @@ def hbm_estimate(r: Request) -> tuple[int, int]:
     return bitmaps * bitmap + 16 * (cands + len(e)), cands + len(e)
 
 
+def device_estimate(eng: Engine, r: Request) -> tuple[int, int]:
+    """hbm_estimate with the first join's candidates from its count pass on
+    the device: the relations that join reads, loaded as the program loads
+    them (programs.tc: path(x, y) probes edge reversed on y; programs.sg:
+    edge joined with itself on the source), then gdl_join_count."""
+    n = r.nodes
+    e = r.inputs[0]
+    bitmap = (n * max(32, 1 << int(np.ceil(np.log2(max(n, 32) / 32)) + 5))) // 8
+    eng.clear()
+    if r.kind == "tc":
+        edge_rev = eng.relation("edge_2__2_1")
+        path = eng.relation("path_2__1_2", index_flag=False)
+        eng.load(path, e)
+        eng.load(edge_rev, W.reverse(e))
+        # the first iteration's DELTA of path is its FULL (src/lie.cu:49-59)
+        cands = eng.join_count(edge_rev, FULL, path, FULL)
+        bitmaps = 3
+    else:
+        edge = eng.relation("edge_2__1_2")
+        eng.load(edge, e)
+        cands = eng.join_count(edge, FULL, edge, FULL)
+        bitmaps = 4
+    return bitmaps * bitmap + 16 * (cands + len(e)), cands + len(e)
+
+
 def percentiles(lat):
     if not lat:
         return {"p50_ms": None, "p99_ms": None, "mean_ms": None}
@@ -123,8 +152,9 @@ def percentiles(lat):
 
 class Server:
     def __init__(self, slots=2, budget_bytes=24 << 30, max_batch=256, batched=True, device=0,
-                 tuple_cap=1 << 29, plain_min_nodes=1 << 12):
+                 tuple_cap=1 << 29, plain_min_nodes=1 << 12, device_admission=True):
         self.slots = slots
+        self.device_admission = device_admission and batched
         self.plain_min_nodes = plain_min_nodes
         self.budget = budget_bytes
         self.tuple_cap = tuple_cap
@@ -214,21 +244,30 @@ class Server:
             return self._run(eng, prog, reqs[:h]) + self._run(eng, prog, reqs[h:])
 
     def serve(self, requests, time_scale=1.0):
-        """Release requests at their arrival times (scaled) and serve them."""
+        """Release requests at their arrival times (scaled) and serve them.
+        Each request's HBM estimate is taken on arrival from its first
+        join's count pass (device_estimate) when `device_admission`."""
         t0 = time.perf_counter()
         workers = [threading.Thread(target=self._worker, args=(t0,)) for _ in range(self.slots)]
+        est = Engine("gpu", device=self.device) if self.device_admission else None
         for w in workers:
             w.start()
-        for r in requests:
-            delay = r.arrival * time_scale - (time.perf_counter() - t0)
-            if delay > 0:
-                time.sleep(delay)
-            r.arrival = r.arrival * time_scale
-            with self.cv:
-                if self.error is not None:
-                    break
-                self.queue.append(r)
-                self.cv.notify()
+        try:
+            for r in requests:
+                delay = r.arrival * time_scale - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                r.arrival = r.arrival * time_scale
+                if est is not None:
+                    r.est_bytes, r.est_tuples = device_estimate(est, r)
+                with self.cv:
+                    if self.error is not None:
+                        break
+                    self.queue.append(r)
+                    self.cv.notify()
+        finally:
+            if est is not None:
+                est.close()
         with self.cv:
             self.done = True
             self.cv.notify_all()

@@ -158,6 +158,14 @@ typedef struct gdl_tuning {
   int32_t spin_limit_log2;     /* a bounded device-side wait (look-back of a scan)
                                   gives up after 2^this polls and the call
                                   returns GDL_E_TIMEOUT (default 22; 1..30) */
+  int32_t radix_bits;          /* digit width of the radix sort: 6, 8 (default) or
+                                  10 bits (64 / 256 / 1024 buckets a pass); a
+                                  width that would need more than 8 passes
+                                  falls back to 8 */
+  int32_t join_block;          /* threads per block of the one-pass join into
+                                  bitmaps: 128, 256 (default) or 512 */
+  int32_t rows_piece;          /* row-gather joins: in-edges of one output row
+                                  per unit of work, 8, 16 or 32 (default) */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);
@@ -197,6 +205,39 @@ gdl_status gdl_relation_size(gdl_engine *e, int32_t rel, int32_t version,
 gdl_status gdl_relation_export(gdl_engine *e, int32_t rel, int32_t version,
                                uint64_t *host_rows, uint64_t cap_rows,
                                uint64_t *out_rows);
+
+/* Device-side gdl_relation_export: one version's tuples, sorted, as rows
+ * of two uint64 columns into `device_rows` (device memory, room for
+ * cap_rows rows); *out_rows receives the count (GDL_E_CAPACITY when it
+ * exceeds cap_rows).  Arity 2; a DELTA still in load order is refused (the
+ * host export sorts it).  With gdl_partition_rows and
+ * gdl_relation_load_device it keeps a partitioned fixpoint's exchange on
+ * the device; no reference counterpart (the reference is one GPU). */
+gdl_status gdl_relation_export_device(gdl_engine *e, int32_t rel, int32_t version,
+                                      uint64_t *device_rows, uint64_t cap_rows,
+                                      uint64_t *out_rows);
+
+/* Group `rows` rows of two uint64 columns (device memory) by owning rank,
+ * owner = rows[i][column] % world (column 0 or 1, world <= 1024): rank d's
+ * rows go, in no particular order, to out_rows[off_d .. off_d + counts[d])
+ * with off_d the sum of the counts before d (device memory, room for `rows`
+ * rows); counts[0 .. world) is written to host memory.  Returns after the
+ * engine's stream has finished.  No reference counterpart. */
+gdl_status gdl_partition_rows(gdl_engine *e, const uint64_t *device_rows, uint64_t rows,
+                              int32_t column, int32_t world, uint64_t *device_out_rows,
+                              uint64_t *counts);
+
+/* Size of a join's output before any deduplication: the number of (outer
+ * row, inner row) pairs that agree on column 0, as the count pass of a
+ * join computes it on the device (k_join_count: one index probe per outer
+ * row, the run lengths summed).  Replaces get_join_result_size
+ * (src/relation.cu:221-288) followed by the reduce in
+ * RelationalJoin::operator() (src/join.cu:77-102).  The inner version must
+ * be indexed (index_flag at load for FULL); versions are GDL_FULL or
+ * GDL_DELTA.  Nothing is materialised; the relations are not changed.
+ * Serving admission sizes a query's first join with it. */
+gdl_status gdl_join_count(gdl_engine *e, int32_t inner, int32_t inner_version, int32_t outer,
+                          int32_t outer_version, uint64_t *out_candidates);
 
 /* Order-sensitive 64-bit digest of one version's sorted tuples, computed on
  * the device (no reference counterpart; used for bit-exact parity of large

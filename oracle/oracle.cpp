@@ -40,6 +40,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -552,6 +553,41 @@ int32_t orc_relation_digest(orc_engine *e, int32_t rel, int32_t ver, uint64_t *o
   CHECK_REL(e, rel);
   if (ver < 0 || ver > 2 || !out) return e->impl->fail(E_INVALID, "bad version");
   return e->impl->rel_digest(rel, ver, out);
+}
+
+// get_join_result_size (src/relation.cu:221-288: per outer row, the length
+// of the inner run its column 0 selects) summed as RelationalJoin::operator()
+// does (src/join.cu:77-102).  Restated over the exported sorted rows.
+int32_t orc_join_count(orc_engine *e, int32_t inner, int32_t inner_ver, int32_t outer,
+                       int32_t outer_ver, uint64_t *out) {
+  CHECK_REL(e, inner);
+  CHECK_REL(e, outer);
+  auto ver_ok = [](int32_t v) { return v == FULL || v == DELTA; };
+  if (!out || !ver_ok(inner_ver) || !ver_ok(outer_ver))
+    return e->impl->fail(E_INVALID, "join_count: versions must be FULL or DELTA");
+  auto rows = [&](int32_t r, int32_t v, std::vector<uint64_t> &dst) -> int32_t {
+    uint64_t n = 0;
+    int32_t st = e->impl->rel_size(r, v, &n);
+    if (st != OK) return st;
+    dst.resize(n * (uint64_t)e->impl->arity(r) + 1);
+    uint64_t got = 0;
+    return e->impl->rel_export(r, v, dst.data(), n, &got);
+  };
+  std::vector<uint64_t> in, ou;
+  int32_t st = rows(inner, inner_ver, in);
+  if (st != OK) return st;
+  st = rows(outer, outer_ver, ou);
+  if (st != OK) return st;
+  const int ai = e->impl->arity(inner), ao = e->impl->arity(outer);
+  std::unordered_map<uint64_t, uint64_t> run;  // column 0 -> inner rows with it
+  for (size_t i = 0; i + ai <= in.size() - 1; i += ai) run[in[i]]++;
+  uint64_t total = 0;
+  for (size_t i = 0; i + ao <= ou.size() - 1; i += ao) {
+    auto it = run.find(ou[i]);
+    if (it != run.end()) total += it->second;
+  }
+  *out = total;
+  return OK;
 }
 
 int32_t orc_lie_create(orc_engine *e, int32_t *out) {

@@ -47,6 +47,10 @@ int32_t orc_relation_export(orc_engine *e, int32_t rel, int32_t version,
 int32_t orc_relation_digest(orc_engine *e, int32_t rel, int32_t version,
                             uint64_t *out_digest);
 
+/* gdl_join_count: (outer row, inner row) pairs agreeing on column 0. */
+int32_t orc_join_count(orc_engine *e, int32_t inner, int32_t inner_version, int32_t outer,
+                       int32_t outer_version, uint64_t *out_candidates);
+
 int32_t orc_lie_create(orc_engine *e, int32_t *out_lie);
 int32_t orc_lie_add_relation(orc_engine *e, int32_t lie, int32_t rel,
                              int32_t static_flag);

@@ -23,6 +23,15 @@ def test_bucket_and_candidates():
     assert {c["pull_joins"] for c in cands} == {1, 2}
 
 
+def test_refine_parameters_start_from_the_default():
+    """The block size, radix digit width and row-gather join tile are tried
+    one at a time, the engine's default first."""
+    assert A.REFINE["join_block"][0] == 256
+    assert A.REFINE["radix_bits"][0] == 8
+    assert A.REFINE["rows_piece"][0] == 32
+    assert set(A.REFINE["radix_bits"]) == {6, 8, 10}
+
+
 @pytest.mark.gpu
 def test_tuning_values_validated():
     with Engine("gpu") as g:
@@ -30,9 +39,49 @@ def test_tuning_values_validated():
             g.set_tuning(index_slots_per_key=3)
         with pytest.raises(GdlError):
             g.set_tuning(dense_max_bits=40)
-        g.set_tuning(join_ctas_per_sm=16, dedup="sort")
+        for bad in ({"radix_bits": 7}, {"join_block": 64}, {"rows_piece": 64}):
+            with pytest.raises(GdlError):
+                g.set_tuning(**bad)
+        g.set_tuning(join_ctas_per_sm=16, dedup="sort", radix_bits=10, join_block=512,
+                     rows_piece=8)
         t = g.get_tuning().as_dict()
         assert t["join_ctas_per_sm"] == 16 and t["dedup"] == 1
+        assert (t["radix_bits"], t["join_block"], t["rows_piece"]) == (10, 512, 8)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bits", [6, 8, 10])
+def test_radix_digit_widths_agree(bits):
+    """The sorted-list path gives the same tuples, sizes and passes with 6-,
+    8- and 10-bit digits (ids of 9 and 13 bits: odd pass counts included)."""
+    for scale, n in ((9, 900), (13, 6000)):
+        e = W.rmat_edges(scale, n, seed=scale)
+        with Engine("oracle") as o:
+            ro = P.sg(o, e)
+            want = (ro.output.size(), ro.output.digest(), tuple(sorted(ro.iterations.items())))
+        with Engine("gpu") as g:
+            g.set_tuning(dedup="sort", radix_bits=bits)
+            r = P.sg(g, e, sync=g.sync)
+            assert (r.output.size(), r.output.digest(),
+                    tuple(sorted(r.iterations.items()))) == want
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("block,piece", [(128, 8), (512, 16), (256, 32)])
+def test_join_block_and_rows_piece_agree(block, piece):
+    """The one-pass join's block size and the row-gather join tile change
+    no result (same generation through the push form at 2^9 ids and the
+    row-gather form at 2^12)."""
+    for scale, n in ((9, 900), (12, 5000)):
+        e = W.rmat_edges(scale, n, seed=scale + 1)
+        with Engine("oracle") as o:
+            ro = P.sg(o, e)
+            want = (ro.output.size(), ro.output.digest(), tuple(sorted(ro.iterations.items())))
+        with Engine("gpu") as g:
+            g.set_tuning(join_block=block, rows_piece=piece)
+            r = P.sg(g, e, sync=g.sync)
+            assert (r.output.size(), r.output.digest(),
+                    tuple(sorted(r.iterations.items()))) == want
 
 
 @pytest.mark.gpu

@@ -126,3 +126,77 @@ def test_partitioned_tc_one_rank_on_the_gpu():
         assert full.tolist() == want[np.lexsort((want[:, 1], want[:, 0]))].tolist()
     finally:
         dist.destroy_process_group()
+
+
+def _rank_gpu(rank, world, port, prog, case, out_dir):
+    """A rank of a partitioned fixpoint over the CUDA engine with the
+    exchange kept on the device (DeviceExchange); the ranks share one GPU
+    and synchronise only through gloo collectives on the host."""
+    import torch
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        with Engine("gpu") as eng:
+            if prog == "tc":
+                res = PT.partitioned_tc(eng, CASES[case](), rank, world)
+                passes = {"tc": res.passes}
+            else:
+                res = PT.partitioned_sg(eng, SG_CASES[case](), rank, world)
+                passes = {"init": res.init_passes, "sg": res.passes}
+        rows = PT.gather_rows(res.full, world)
+        with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+            json.dump({"passes": passes, "n": len(res.full), "rows": rows.tolist()}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,case", [("tc", "grid_10"), ("tc", "rmat_s7"), ("sg", "rmat_s8"),
+                                       ("sg", "dag_L8_W6")])
+def test_device_resident_exchange_two_ranks(prog, case, tmp_path):
+    """Two ranks, each over the CUDA engine with its candidates exported,
+    grouped by owner, exchanged and reloaded in device memory, give the
+    single-engine result and loop-pass counts."""
+    world = 2
+    mp.spawn(_rank_gpu, args=(world, free_port(), prog, case, str(tmp_path)), nprocs=world,
+             join=True)
+    outs = [json.load(open(tmp_path / f"r{r}.json")) for r in range(world)]
+    with Engine("oracle") as o:
+        if prog == "tc":
+            r = P.tc(o, CASES[case]())
+        else:
+            r = P.sg(o, SG_CASES[case]())
+        want = r.output.rows()
+        want = want[np.lexsort((want[:, 1], want[:, 0]))].tolist()
+        iters = dict(r.iterations)
+    for o in outs:
+        assert o["passes"] == iters
+        assert o["rows"] == want
+    assert sum(o["n"] for o in outs) == len(want)
+
+
+@pytest.mark.gpu
+def test_partition_rows_groups_by_owner():
+    """gdl_partition_rows: each row lands in its owner's block, block sizes
+    are the owners' counts, nothing is lost or repeated."""
+    import torch
+    rng = np.random.default_rng(5)
+    rows = np.stack([rng.integers(0, 1 << 32, 5000, dtype=np.uint64),
+                     rng.integers(0, 1 << 20, 5000, dtype=np.uint64)], axis=1)
+    with Engine("gpu") as g:
+        src = torch.from_numpy(rows.view(np.int64)).cuda()
+        out = torch.empty_like(src)
+        for col, world in ((0, 3), (1, 7), (0, 1)):
+            counts = g.partition_rows(src.data_ptr(), len(rows), col, world, out.data_ptr())
+            got = out.cpu().numpy().view(np.uint64)
+            assert counts == np.bincount((rows[:, col] % world).astype(np.int64),
+                                         minlength=world).tolist()
+            at = 0
+            for d, c in enumerate(counts):
+                block = got[at:at + c]
+                assert (block[:, col] % world == d).all()
+                at += c
+            key = lambda a: np.lexsort((a[:, 1], a[:, 0]))  # noqa: E731
+            assert (got[key(got)] == rows[key(rows)]).all()
+        assert g.partition_rows(0, 0, 0, 4, 0) == [0, 0, 0, 0]

@@ -65,6 +65,78 @@ def test_large_sg_queries_are_taken_alone():
     assert max(sizes) > 1
 
 
+def test_count_pass_estimate_matches_degrees_on_the_oracle():
+    """The admission estimate from the first join's count pass (here the
+    oracle's restatement of get_join_result_size) equals the host's
+    degree-based cross-check, for transitive-closure and same-generation
+    queries."""
+    reqs = S.make_stream(24, rate=2000.0, seed=11, min_scale=5, max_scale=8, l_range=(3, 12),
+                         w_range=(3, 12))
+    assert {r.kind for r in reqs} == {"tc", "sg"}
+    with Engine("oracle") as o:
+        for r in reqs:
+            assert S.device_estimate(o, r) == S.hbm_estimate(r), r.id
+
+
+def test_join_count_edge_cases_on_the_oracle():
+    """Empty sides count zero (a loaded relation's DELTA is empty until a
+    LIE starts, src/lie.cu:49-59); keys present on one side only add
+    nothing."""
+    import numpy as np
+    from gdlog_b200 import DELTA, FULL
+    with Engine("oracle") as o:
+        a = o.relation("a")
+        b = o.relation("b")
+        empty = o.relation("empty")
+        o.load(a, np.array([[1, 2], [1, 3], [2, 5], [7, 7]], dtype=np.uint64))
+        o.load(b, np.array([[1, 9], [2, 8], [2, 9], [4, 4]], dtype=np.uint64))
+        o.load(empty, None)
+        assert o.join_count(a, FULL, b, FULL) == 2 * 1 + 1 * 2  # keys 1 and 2
+        assert o.join_count(b, FULL, a, FULL) == 1 * 2 + 2 * 1
+        assert o.join_count(a, DELTA, b, FULL) == 0
+        assert o.join_count(b, FULL, a, DELTA) == 0
+        assert o.join_count(empty, FULL, a, FULL) == 0
+        assert o.join_count(a, FULL, empty, FULL) == 0
+
+
+@pytest.mark.gpu
+def test_device_count_pass_matches_oracle_and_degrees():
+    """gdl_join_count on the GPU (k_join_count over the loaded relations)
+    gives the oracle's count and the host's degree estimate."""
+    reqs = S.make_stream(24, rate=2000.0, seed=11, min_scale=6, max_scale=12, l_range=(3, 40),
+                         w_range=(3, 40))
+    with Engine("gpu") as g, Engine("oracle") as o:
+        for r in reqs:
+            want = S.hbm_estimate(r)
+            assert S.device_estimate(g, r) == want, r.id
+            assert S.device_estimate(o, r) == want, r.id
+
+
+@pytest.mark.gpu
+def test_device_join_count_edge_cases():
+    import numpy as np
+    from gdlog_b200 import DELTA, FULL, GdlError
+    with Engine("gpu") as g:
+        a = g.relation("a")
+        b = g.relation("b")
+        empty = g.relation("empty")
+        noidx = g.relation("noidx", index_flag=False)
+        g.load(a, np.array([[1, 2], [1, 3], [2, 5], [7, 7]], dtype=np.uint64))
+        g.load(b, np.array([[1, 9], [2, 8], [2, 9], [4, 4]], dtype=np.uint64))
+        g.load(empty, None)
+        g.load(noidx, np.array([[1, 1]], dtype=np.uint64))
+        assert g.join_count(a, FULL, b, FULL) == 4
+        assert g.join_count(b, FULL, a, FULL) == 4
+        assert g.join_count(empty, FULL, a, FULL) == 0
+        assert g.join_count(a, FULL, empty, FULL) == 0
+        assert g.join_count(b, FULL, a, DELTA) == 0
+        assert g.size(a) == 4 and g.size(b) == 4  # nothing changed
+        with pytest.raises(GdlError):
+            g.join_count(noidx, FULL, a, FULL)
+        with pytest.raises(GdlError):
+            g.join_count(a, 2, b, FULL)  # NEWT is not a count-pass version
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("plain_min_nodes", [0, 1 << 6])
 def test_results_same_alone_and_in_the_mix(plain_min_nodes):
