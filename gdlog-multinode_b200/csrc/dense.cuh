@@ -790,9 +790,9 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_groupwrite(BmScanArgs a) {
 // its count).  Replaces the sort of the flattened FULL at the end of a LIE
 // (src/lie.cu:219-254).
 //
-// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i), so
-// warp w of segment i owns 32 consecutive words (lane l the word
-// i * 256 + 32 w + l).
+// Thread t holds words i * 256 + t of the tile (i = 0..7, "segment" i).  A
+// segment is 256 words, 8192 bit positions, so the keys of one segment
+// always fit one staging buffer.
 // ---------------------------------------------------------------------------
 constexpr int kListScanBlock = 1024;
 
@@ -852,38 +852,37 @@ __global__ void __launch_bounds__(kListScanBlock) k_bm_list_offsets(const u32 *c
   }
 }
 
+constexpr int kListStage = kBmBlock * 32;  // 8192 positions per segment
+
 struct ListSmem {
+  unsigned short stage[2][kListStage];
   u32 wtot[kBmWordsPerThread][kBmBlock / 32];  // per segment: warp totals, then offsets
-  u32 seg_off[kBmWordsPerThread + 1];
-  unsigned char lut[256 * 8];  // position of the r-th set bit of a byte: lut[byte * 8 + r]
+  u32 seg_tot[kBmWordsPerThread];
+  u32 seg_off[kBmWordsPerThread];
   long long tile;
 };
 
-// Keys leave warp by warp: each warp writes the keys of its 32 words at
-// their offset, 32 consecutive keys per step.  Key j of the warp comes from
-// the last lane whose exclusive prefix is <= j (a 5-step search over the
-// lanes' prefixes), as the r-th set bit of that lane's word (two popcount
-// steps, then a byte table).  No staging, no barrier per segment, and no
-// lane waits on a denser neighbour.  Tiles are taken from a counter (dense
-// tiles cluster at the low ids of skewed graphs).
+// Keys leave through a shared-memory window: each segment's keys are staged
+// as their 13-bit positions in the segment (2 bytes; the row and column are
+// rebuilt at the copy-out), each thread expanding its own word, then copied
+// out in one coalesced pass.  Two buffers alternate between the segments
+// that hold keys, so one barrier per segment separates a buffer's expansion
+// from its copy-out and the copy-out from the buffer's next expansion.
+// Tiles are taken from a counter (dense tiles cluster at the low ids of
+// skewed graphs); a tile's offset comes from k_bm_list_offsets.
 __global__ void __launch_bounds__(kBmBlock) k_bm_list_write(const u32 *bm, u64 tiles, int rs,
                                                             const u32 *cnt, const u64 *off,
                                                             DArr *out, LaunchRec *rec, Ctl *ctl) {
   __shared__ ListSmem sm;
   if (ctl_stop(ctl)) return;
-  for (int b = threadIdx.x; b < 256; b += kBmBlock) {
-    int r = 0;
-    for (int k = 0; k < 8; k++)
-      if (b >> k & 1) sm.lut[b * 8 + r++] = (unsigned char)k;
-    for (; r < 8; r++) sm.lut[b * 8 + r] = 0;
-  }
   const u64 row_mask = (1ull << rs) - 1;
   u64 *dst = out->ptr;
   const u64 cap = out->cap;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 moved = 0;
+  u32 nbuf = 0;  // segments with keys staged so far (buffer parity)
   while (true) {
-    const long long tl = grab_tile(rec, &sm.tile);  // (its barriers order the table's writes)
+    const long long tl = grab_tile(rec, &sm.tile);
     if (tl >= (long long)tiles) break;
     const u64 t = (u64)tl;
     if (cnt[t] == 0) continue;  // (block-uniform)
@@ -903,63 +902,61 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list_write(const u32 *bm, u64 t
       if (lane == 31) sm.wtot[i][warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      // offsets of (segment, warp) in the tile's keys, in key order
+    if (threadIdx.x < kBmWordsPerThread) {
+      // per segment: exclusive warp offsets and the segment's total
       u32 acc = 0;
-      for (int i = 0; i < kBmWordsPerThread; i++) {
-        sm.seg_off[i] = acc;
-        for (int w = 0; w < kBmBlock / 32; w++) {
-          const u32 x = sm.wtot[i][w];
-          sm.wtot[i][w] = acc;
-          acc += x;
-        }
+      for (int w = 0; w < kBmBlock / 32; w++) {
+        const u32 x = sm.wtot[threadIdx.x][w];
+        sm.wtot[threadIdx.x][w] = acc;
+        acc += x;
       }
-      sm.seg_off[kBmWordsPerThread] = acc;
+      sm.seg_tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u32 a = 0;
+      for (int i = 0; i < kBmWordsPerThread; i++) {
+        sm.seg_off[i] = a;
+        a += sm.seg_tot[i];
+      }
     }
     __syncthreads();
     const u64 base = off[t];
     moved += 4 * kBmWordsPerThread;
-#pragma unroll
     for (int i = 0; i < kBmWordsPerThread; i++) {
-      const u32 wofs = sm.wtot[i][warp];
-      const u32 wend = warp + 1 < kBmBlock / 32 ? sm.wtot[i][warp + 1] : sm.seg_off[i + 1];
-      const u32 total = wend - wofs;  // (warp-uniform)
-      if (total == 0) continue;
-      const u64 ws = w0 + (u64)i * kBmBlock + (u64)warp * 32;
-      const u64 pos0 = base + wofs;
-      for (u32 j0 = 0; j0 < total; j0 += 32) {
-        const u32 j = j0 + lane;
-        int sl = 0;
-#pragma unroll
-        for (int h = 16; h > 0; h >>= 1) {
-          const u32 e = __shfl_sync(0xffffffffu, ex[i], sl + h);
-          if (e <= j) sl += h;
-        }
-        u32 word = __shfl_sync(0xffffffffu, v[i], sl);
-        u32 r = j - __shfl_sync(0xffffffffu, ex[i], sl);
-        if (j >= total) continue;
-        u32 pos = 0;
-        u32 c = __popc(word & 0xFFFFu);
-        if (r >= c) {
-          r -= c;
-          word >>= 16;
-          pos = 16;
-        }
-        c = __popc(word & 0xFFu);
-        if (r >= c) {
-          r -= c;
-          word >>= 8;
-          pos += 8;
-        }
-        pos += sm.lut[(word & 0xFFu) * 8 + r];
-        const u64 w = ws + (u64)sl;
-        const u64 key = ((w >> rs) << 32) | ((w & row_mask) << 5) | pos;
-        if (pos0 + j < cap)
-          dst[pos0 + j] = key;
-        else
-          atomicOr(&ctl->oob, 16384u);
+      const u32 st = sm.seg_tot[i];  // block-uniform
+      if (st == 0) continue;
+      unsigned short *stg = sm.stage[nbuf++ & 1];
+      // expand this thread's word: its keys' positions in the segment
+      u32 x = v[i];
+      u32 p = sm.wtot[i][warp] + ex[i];
+      const u32 q0 = threadIdx.x * 32;
+      while (x) {
+        stg[p++] = (unsigned short)(q0 + (u32)(__ffs(x) - 1));
+        x &= x - 1;
       }
-      moved += 8 * (u64)(lane == 0 ? total : 0);
+      __syncthreads();
+      // copy-out: position q of segment word ws = q / 32, bit q % 32
+      const u64 ws = w0 + (u64)i * kBmBlock;
+      const u64 pos0 = base + sm.seg_off[i];
+      u64 *o = dst + pos0;
+      moved += 8 * (u64)(threadIdx.x == 0 ? st : 0);
+      if (pos0 + st <= cap) {
+        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
+          const u32 q = stg[j];
+          const u64 w = ws + (q >> 5);
+          o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
+        }
+      } else {
+        for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
+          const u32 q = stg[j];
+          const u64 w = ws + (q >> 5);
+          if (pos0 + j < cap)
+            o[j] = ((w >> rs) << 32) | ((w & row_mask) << 5) | (q & 31u);
+          else
+            atomicOr(&ctl->oob, 16384u);
+        }
+      }
     }
   }
 #pragma unroll

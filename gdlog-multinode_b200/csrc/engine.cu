@@ -152,9 +152,9 @@ struct RelHost {
   // A load committed on the device that the host mirror has not read back
   // (its FULL count is known on the device only).
   bool stale = false;
-  u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr, *inv_ys = nullptr;
+  u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr;
   u32 *inv_poff = nullptr;   // pieces of work per y, then their offsets (2^dk + 1)
-  uint2 *inv_pieces = nullptr;
+  uint4 *inv_pieces = nullptr;  // {first edge, end edge, y, whole}
   u64 inv_cap = 0;
   int inv_dk = 0;
 };
@@ -1165,8 +1165,10 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
 // host opens with a k_begin before each launch and whose k_commit opens
 // the next iteration; otherwise the iteration opens itself.
 void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
-  // one resident wave (the pieces are taken from a counter)
-  const int g = (int)e->sms * (ra.dk >= 16 ? 2 : 4);
+  // one resident wave (warps take the pieces round robin): 4 blocks an SM
+  // at 2^12 ids, 2 at 2^13..2^15 (the row accumulators hold 2^(dk-5)
+  // words a warp), 1 from 2^16
+  const int g = (int)e->sms * (ra.dk >= 16 ? 1 : ra.dk >= 13 ? 2 : 4);
   switch (ra.dk) {
     case 12: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<1><<<g, 256, 0, e->s>>>(ra)); break;
     case 13: PLAUNCH(kc, kPJoinMat, k_join_rows_bm<2><<<g, 256, 0, e->s>>>(ra)); break;
@@ -1244,7 +1246,7 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   const u64 n = e->h[r].full.n;
   const u32 ids = 1u << dk;
   if (rh.inv_dk != dk || rh.inv_cap < std::max<u64>(n, 1)) {
-    for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_poff, &rh.inv_keys, &rh.inv_ys}) {
+    for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_poff, &rh.inv_keys}) {
       dfree(e, *q);
       *q = nullptr;
     }
@@ -1256,9 +1258,8 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
     TRY(dalloc(e, (void **)&rh.inv_cur, ids * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_poff, (ids + 1) * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_keys, rh.inv_cap * sizeof(u32)));
-    TRY(dalloc(e, (void **)&rh.inv_ys, rh.inv_cap * sizeof(u32)));
     // pieces: at most one per in-edge, and one per y
-    TRY(dalloc(e, (void **)&rh.inv_pieces, (rh.inv_cap + ids) * sizeof(uint2)));
+    TRY(dalloc(e, (void **)&rh.inv_pieces, (rh.inv_cap + ids) * sizeof(uint4)));
   }
   CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
   const DArr *list = &e->d_rels[r].full;
@@ -1266,8 +1267,7 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   // edge offsets, fill cursors and the pieces of work, in one block
   k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, rh.inv_poff,
                                            rh.inv_pieces, dk, (u32)e->rows_piece);
-  k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
-                                                       dk);
+  k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, dk);
   CK(e, cudaGetLastError());
   return GDL_OK;
 }
@@ -1400,9 +1400,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         ra.O = op.outer_ver == GDL_DELTA ? oh.bmDN : oh.bmG;
         ra.outer_clear = op.outer_ver == GDL_NEWT ? oh.bmG : nullptr;
         const RelHost &ih = e->rels[op.inner];
-        ra.inv_off = ih.inv_off;
         ra.inv_keys = ih.inv_keys;
-        ra.inv_ys = ih.inv_ys;
         ra.pieces_off = ih.inv_poff;
         ra.pieces = ih.inv_pieces;
         const RelDev &out = e->h[op.out];
@@ -2725,6 +2723,8 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       h.delta_vis = 1;
       h.newt.n = 0;
     }
+    // DELTA is now what the last iteration's update step wrote: sorted
+    rh.delta_sorted = true;
   }
   TRY(push(e));
   *out_iters = c.iteration;
@@ -2877,7 +2877,7 @@ static void release_program(gdl_engine *e) {
     dfree(e, r.bmD);
     dfree(e, r.tile_prefix);
     const RelHost &rh = e->rels[i];
-    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_poff, rh.inv_keys, rh.inv_ys})
+    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_poff, rh.inv_keys})
       dfree(e, q);
     dfree(e, rh.inv_pieces);
     if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
@@ -3383,27 +3383,43 @@ gdl_status gdl_join_count(gdl_engine *e, int32_t inner, int32_t inner_ver, int32
       return fail(e, GDL_E_UNSUPPORTED, "join count: %s is kept as a bitmap only",
                   e->rels[r].name.c_str());
   TRY(refresh(e));
-  const RelDev &ih = e->h[inner], &oh = e->h[outer];
-  const Index &ix = inner_ver == GDL_FULL ? ih.full_idx : ih.delta_idx;
+  RelDev &ih = e->h[inner];
+  const RelDev &oh = e->h[outer];
   const DArr &ia = inner_ver == GDL_FULL ? ih.full : ih.delta;
   const DArr &oa = outer_ver == GDL_FULL ? oh.full : oh.delta;
   const u64 ni = (inner_ver == GDL_FULL ? ih.full_vis : ih.delta_vis) ? ia.n : 0;
   const u64 no = (outer_ver == GDL_FULL ? oh.full_vis : oh.delta_vis) ? oa.n : 0;
-  if (ni && !ix.slots)
-    return fail(e, GDL_E_INVALID, "join count: %s has no index of that version (index_flag)",
+  if (ni && !e->rels[inner].index_flag)
+    return fail(e, GDL_E_INVALID, "join count: %s is not indexed (index_flag)",
+                e->rels[inner].name.c_str());
+  if (ni && inner_ver == GDL_DELTA && !e->rels[inner].delta_sorted)
+    return fail(e, GDL_E_UNSUPPORTED, "join count: DELTA of %s is in load order",
                 e->rels[inner].name.c_str());
   if (ni == 0 || no == 0) {
     *out = 0;
     return GDL_OK;
   }
   TRY(ensure_scratch(e));
+  // the inner version's index, built now (as a LIE builds the indexes its
+  // joins probe, with a fresh epoch)
+  TRY(reset_ctl(e));
+  {
+    Index &ixm = inner_ver == GDL_FULL ? ih.full_idx : ih.delta_idx;
+    TRY(ensure_index(e, ixm, ia.cap));
+    ixm.epoch = (u32)(e->generation + 1);
+    TRY(push_rel(e, inner));
+    k_index_build<<<grid_for(e, ni, kIndexBlock, 8), kIndexBlock, 0, e->s>>>(
+        inner_ver == GDL_FULL ? &e->d_rels[inner].full : &e->d_rels[inner].delta,
+        inner_ver == GDL_FULL ? &e->d_rels[inner].full_idx : &e->d_rels[inner].delta_idx,
+        nullptr, e->d_ctl);
+    CK(e, cudaGetLastError());
+  }
   // (outside the engine's replayed allocation sequence: kept until destroy)
   if (!e->d_count) CK(e, cudaMalloc(&e->d_count, sizeof(CountScratch)));
   CountScratch cs;
   memset(&cs, 0, sizeof cs);
   cs.outer_vis = cs.inner_vis = 1;
   CK(e, cudaMemcpyAsync(e->d_count, &cs, sizeof cs, cudaMemcpyHostToDevice, e->s));
-  TRY(reset_ctl(e));
   CountScratch *d = reinterpret_cast<CountScratch *>(e->d_count);
   RelDev *R = e->d_rels;
   JoinArgs a;

@@ -499,10 +499,9 @@ __global__ void __launch_bounds__(256) k_inv_count(const DArr *list, u32 *cnt, i
   }
 }
 
-// Scatter: the in-edges of y at [off[y], off[y+1]), each with its y (the
-// order inside a y does not matter: the gather ORs).
-__global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, u32 *ys,
-                                                  int dk) {
+// Scatter: the in-edges of y at [off[y], off[y+1]) (the order inside a y
+// does not matter: the gather ORs).
+__global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, int dk) {
   const u64 n = list->n;
   const u32 lim = 1u << dk;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
@@ -511,25 +510,25 @@ __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u3
     if (y >= lim || k >= lim) continue;
     const u32 pos = atomicAdd(&cur[y], 1u);
     keys[pos] = k;
-    ys[pos] = y;
   }
 }
 
 // Units of work of the row-gather join: the in-edges of one y, cut into
 // pieces of at most `piece` (<= 32, a tuning choice; a y with more in-edges
 // than that is shared by several warps, which OR their parts into the
-// output row).
+// output row).  A piece is {first edge, end edge, y, whole}: whole when it
+// holds all of y's in-edges.
 constexpr int kInvBlock = 1024;
 constexpr int kInvPer = 8;  // consecutive ids per thread and chunk
 
 // One block: from the in-degree counts cnt[y] (2^dk of them), the edge
 // offsets off[0..2^dk] (and the fill cursors cur, a copy; cur may be cnt),
-// the piece offsets poff[0..2^dk] and the pieces themselves as
-// (first edge, end edge).  Chunks of kInvBlock x kInvPer ids, each thread
+// the piece offsets poff[0..2^dk] and the pieces themselves (the poff
+// array is no longer read by the join: a piece names its y).  Chunks of kInvBlock x kInvPer ids, each thread
 // kInvPer consecutive ones read and written as 16-byte vectors; the two
 // prefix sums (edges low, pieces high) share one 64-bit block scan.
 __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *off, u32 *cur,
-                                                           u32 *poff, uint2 *pieces, int dk,
+                                                           u32 *poff, uint4 *pieces, int dk,
                                                            u32 piece) {
   __shared__ u64 s_warp[kInvBlock / 32];
   const u32 n = 1u << dk;  // a multiple of kInvPer
@@ -561,7 +560,8 @@ __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *
       o[i] = e;
       po[i] = p;
       const u32 end = e + v[i];
-      for (u32 s = e; s < end; s += piece) pieces[p++] = make_uint2(s, min(s + piece, end));
+      for (u32 s = e; s < end; s += piece)
+        pieces[p++] = make_uint4(s, min(s + piece, end), b + i, v[i] <= piece ? 1u : 0u);
       e = end;
     }
     uint4 *po4 = reinterpret_cast<uint4 *>(off + b), *pc4 = reinterpret_cast<uint4 *>(cur + b),
@@ -583,11 +583,9 @@ struct RowsArgs {
   JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record
   const u32 *O;        // the outer's rows: DELTA (non-transposed copy) or a tmp NEWT
   u32 *outer_clear;    // bitmap to clear if an empty inner zeroes a NEWT outer
-  const u32 *inv_off;  // in-edges of y: [inv_off[y], inv_off[y + 1])
-  const u32 *inv_keys;
-  const u32 *inv_ys;
+  const u32 *inv_keys;    // in-edge sources, grouped by y
   const u32 *pieces_off;  // pieces_off[2^dk]: the number of pieces
-  const uint2 *pieces;
+  const uint4 *pieces;    // {first edge, end edge, y, whole}
   u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
   u8 *dirty;           // dirty map of dst, or null
   int dst_zero;        // dst is all zero when the launch starts
@@ -672,21 +670,22 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   // k_inv_fill and reported by the fixpoint)
   const u32 n_pieces = a.pieces_off[1u << a.dk];
   u64 words_out = 0, edges = 0;
-  while (true) {
-    u32 c = 0;
-    if (lane == 0) c = atomicAdd(&a.j.rec->tile_ctr, 1u);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= n_pieces) break;
-    const uint2 pc = a.pieces[c];
-    const u32 y = a.inv_ys[pc.x];
+  // Pieces are bounded (<= 32 rows), so warps take them round robin; the
+  // next piece's descriptor and keys load while this one's rows are read.
+  const u32 nw = (gridDim.x * blockDim.x) >> 5;
+  u32 c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint4 pc = c < n_pieces ? a.pieces[c] : make_uint4(0, 0, 0, 0);
+  u32 my_k = (c < n_pieces && lane < (int)(pc.y - pc.x)) ? a.inv_keys[pc.x + lane] : 0;
+  constexpr int kFly = V <= 4 ? 4 : 2;
+  while (c < n_pieces) {
+    const u32 cn = c + nw;
+    const uint4 pn = cn < n_pieces ? a.pieces[cn] : make_uint4(0, 0, 0, 0);
     uint4 acc[V];
 #pragma unroll
     for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
     // this piece's keys, one per lane; kFly rows in flight per step (all
     // their loads issued before the ORs)
-    constexpr int kFly = V <= 4 ? 4 : 2;
     const u32 m = pc.y - pc.x;
-    const u32 my_k = lane < (int)m ? a.inv_keys[pc.x + lane] : 0;
     u32 i = 0;
     for (; i + kFly <= m; i += kFly) {
       uint4 b[kFly][V];
@@ -708,10 +707,14 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
         }
     }
     for (; i < m; i++) rows_or<V>(acc, a.O, __shfl_sync(0xffffffffu, my_k, i), rs, lane);
+    // the next piece's keys (its descriptor has arrived)
+    const u32 kn = (cn < n_pieces && lane < (int)(pn.y - pn.x)) ? a.inv_keys[pn.x + lane] : 0;
     // a y whose in-edges are all in this piece is this warp's alone
-    const bool whole = pc.x == a.inv_off[y] && pc.y == a.inv_off[y + 1];
-    rows_flush<V>(a, y, whole, acc, words_out);
+    rows_flush<V>(a, pc.z, pc.w != 0, acc, words_out);
     edges += m;
+    c = cn;
+    pc = pn;
+    my_k = kn;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) words_out += __shfl_xor_sync(0xffffffffu, words_out, o);
