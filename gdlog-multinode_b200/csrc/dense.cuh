@@ -821,11 +821,12 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list_count(const u32 *bm, u64 t
 }
 
 // One block: off[t] = keys of the tiles before t; out->n = the total
-// (within the list's capacity).  out->n on entry is the bit count the loop
-// kept for this version; another total raises the bounds flag.
+// (within the list's capacity).  check_n: out->n on entry is the bit count
+// the loop kept for this version, and another total raises the bounds flag
+// (a load's listing has no such count).
 __global__ void __launch_bounds__(kListScanBlock) k_bm_list_offsets(const u32 *cnt, u64 tiles,
                                                                     u64 *off, DArr *out,
-                                                                    Ctl *ctl) {
+                                                                    int check_n, Ctl *ctl) {
   __shared__ u64 s_warp[kListScanBlock / 32];
   if (ctl_stop(ctl)) return;
   u64 carry = 0;
@@ -848,7 +849,7 @@ __global__ void __launch_bounds__(kListScanBlock) k_bm_list_offsets(const u32 *c
   if (threadIdx.x == 0) {
     const u64 expect_n = out->n, cap = out->cap;
     out->n = carry <= cap ? carry : cap;
-    if (carry > cap || carry != expect_n) atomicOr(&ctl->oob, 16384u);
+    if (carry > cap || (check_n && carry != expect_n)) atomicOr(&ctl->oob, 16384u);
   }
 }
 
@@ -991,6 +992,28 @@ __global__ void __launch_bounds__(256) k_bm_from_list(const DArr *list, u32 *bm,
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
     dm_set(map, bm, nullptr, k[i], ctl);
   if (blockIdx.x == 0 && threadIdx.x == 0) prof_add(ctl, kPBitmap, 8 * n);
+}
+
+// load_relation's sort + unique over a small square domain (ids below
+// 2^dk): every row sets its bit (c0, c1) of a zeroed bitmap, word
+// c0 * 2^(dk-5) + c1 / 32, and the listing passes read the bitmap back in
+// key order, each tuple once.  A key outside the domain is dropped and
+// raises the bounds flag (the host sizes dk from the largest value).
+__global__ void __launch_bounds__(256) k_bm_set_keys(const u64 *keys, u64 n, u32 *bm, int dk,
+                                                     Ctl *ctl) {
+  if (ctl_stop(ctl)) return;
+  const u32 lim = 1u << dk;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 k = keys[i];
+    const u32 c0 = key_c0(k), c1 = key_c1(k);
+    if (c0 >= lim || c1 >= lim) {
+      atomicOr(&ctl->oob, 65536u);
+      continue;
+    }
+    const u64 bit = ((u64)c0 << dk) | c1;
+    atomicOr(&bm[bit >> 5], 1u << (bit & 31));
+  }
 }
 
 // RelationalJoin materialisation into the output's NEWT bitmap.  Balanced

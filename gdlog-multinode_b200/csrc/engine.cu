@@ -60,6 +60,9 @@ namespace {
 constexpr u64 kMinCap = 1ull << 16;
 constexpr int kIdentityMaxBits = 22;
 constexpr u64 kMaxRows = (1ull << 30) - 4096;  // sort status keeps 30 bits
+// Loads over ids below 2^this deduplicate through a domain bitmap (128 MB
+// at 15 bits); wider ids use the radix sort.
+constexpr int kLoadBitmapMaxBits = 15;
 constexpr u64 kTraceRows = 256;  // iterations a loop batch logs (one device buffer)
 
 u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
@@ -199,6 +202,7 @@ struct gdl_engine {
   int radix_bits = kRadixBits;
   int join_block = 256;
   int rows_piece = 32;
+  int load_dedup = 2;  // loads: 1 radix sort + merge, 2 bitmap listing where it fits
   u64 *crow_off = nullptr, *crow_key = nullptr;
   u32 *crow_start = nullptr, *crow_len = nullptr;
   u64 crow_cap = 0;
@@ -769,7 +773,7 @@ void launch_sort(gdl_engine *e, const DArr *d_keys, u64 *buf0, u64 cap, Counts *
   a.max_tiles = e->sort_status_tiles;
   a.counters = e->sort_counters;
   a.ctl = e->d_ctl;
-  int gh = grid_for(e, cap, (u64)kSortTile * 4, 2);
+  int gh = grid_for(e, cap, (u64)kSortTile, 2);
   int gp = grid_for(e, cap, kSortTile, 4);
   switch (sort_bits(e)) {
 #define GDL_SORT(B)                                                                         \
@@ -795,6 +799,9 @@ u64 *sorted_location(gdl_engine *e, u64 *buf0) { return (sort_passes(e) & 1) ? e
 // host mirror of this relation is marked stale and read back at the next
 // point that needs it, where the load's device checks are reported too.
 // Only this relation's entry is written to the device table.
+gdl_status launch_list(gdl_engine *e, const u32 *bm, u64 words, int rs, DArr *out,
+                       int check_n);
+
 gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   RelHost &rh = e->rels[rel];
   TRY(refresh_rel(e, rel));
@@ -817,6 +824,32 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   r.full_idx.epoch = r.full_idx_next.epoch = r.delta_idx.epoch = r.delta_idx_next.epoch = 0;
   TRY(ensure_arr(e, r.full, n, false));
   TRY(ensure_arr(e, r.full_next, n, false));
+  const int ldk = std::max(e->kbits, kPullMinBits);
+  if (n > (u64)kSortTile && e->load_dedup == 2 && !e->wide && rh.arity == 2 &&
+      ldk <= kLoadBitmapMaxBits) {
+    // Sort + unique through a bitmap over the key domain (2^(2 ldk) bits,
+    // at most 128 MB): the rows' bits set, then listed in key order into
+    // full_next, which k_load_commit swaps in.  Five streaming launches in
+    // place of the radix sort's and merge's latency-bound passes.
+    const u64 words = 1ull << (2 * ldk - 5);
+    u32 *bm = nullptr;
+    TRY(dalloc(e, (void **)&bm, words * sizeof(u32)));
+    CK(e, cudaMemsetAsync(bm, 0, words * sizeof(u32), e->s));
+    TRY(push_rel(e, rel));
+    TRY(reset_ctl(e));
+    k_bm_set_keys<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(keys_dev, n, bm, ldk, e->d_ctl);
+    TRY(launch_list(e, bm, words, ldk - 5, &e->d_rels[rel].full_next, 0));
+    k_load_commit<<<1, 32, 0, e->s>>>(&e->d_rels[rel], e->d_ctl, e->d_u32 + 3);
+    CK(e, cudaGetLastError());
+    dfree(e, bm);  // stream-ordered behind the listing
+    std::swap(r.full, r.full_next);
+    r.newt.n = 0;
+    r.delta_next.n = 0;
+    r.c_newt_n = 0;
+    rh.stale = true;
+    e->mirror_fresh = false;
+    return GDL_OK;
+  }
   if (n) {
     // sort a copy in the NEWT buffer, then dedup it into FULL
     TRY(ensure_arr(e, r.newt, n, false));
@@ -1181,13 +1214,14 @@ void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
 // The sorted key list of a square-domain bitmap of `words` words (rows of
 // 2^rs words) into `out` (k_bm_list_*, dense.cuh): tile counts, offsets and
 // the list's size, keys.  out->n must hold the expected count.
-gdl_status launch_list(gdl_engine *e, const u32 *bm, u64 words, int rs, DArr *out) {
+gdl_status launch_list(gdl_engine *e, const u32 *bm, u64 words, int rs, DArr *out,
+                       int check_n) {
   const u64 tiles = words / kBmTileWords;
   TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, tiles + 2));
   k_bm_list_count<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(bm, tiles, e->lb_list.flag,
                                                                    e->d_ctl);
   k_bm_list_offsets<<<1, kListScanBlock, 0, e->s>>>(e->lb_list.flag, tiles, e->lb_list.agg, out,
-                                                    e->d_ctl);
+                                                    check_n, e->d_ctl);
   k_bm_list_write<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(
       bm, tiles, rs, e->lb_list.flag, e->lb_list.agg, out, &e->recs[8], e->d_ctl);
   CK(e, cudaGetLastError());
@@ -2367,7 +2401,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     k_ctl_resume<<<1, 32, 0, e->s>>>(e->d_ctl);
     for (int r : L.update)
       if (e->h[r].full_lazy)
-        TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full));
+        TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, 1));
     CK(e, cudaGetLastError());
     CK(e, cudaMemcpyAsync(e->h_ctl2, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->s));
     CK(e, cudaEventRecord(e->ev1, e->s));
@@ -2628,7 +2662,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         if (!e->h[r].full_lazy) continue;
         if (!e->instances) {
           // square domain (k_bm_list_*)
-          TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full));
+          TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, 1));
           continue;
         }
         BmScanArgs a = scan_none(L.map);
@@ -2675,7 +2709,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
           rows = h.bmG;
         }
-        TRY(launch_list(e, rows, L.map.words, L.dk - 5, &e->d_rels[r].delta));
+        TRY(launch_list(e, rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, 1));
         if (!plan.delta_n[r]) CK(e, cudaMemsetAsync(h.bmG, 0, L.map.words * 4, e->s));
       }
       CK(e, cudaGetLastError());
@@ -3772,7 +3806,8 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
       t->row_gather > 3 || t->spin_limit_log2 < 0 || t->spin_limit_log2 > 30 ||
       (t->radix_bits && t->radix_bits != 6 && t->radix_bits != 8 && t->radix_bits != 10) ||
       (t->join_block && t->join_block != 128 && t->join_block != 256 && t->join_block != 512) ||
-      (t->rows_piece && t->rows_piece != 8 && t->rows_piece != 16 && t->rows_piece != 32))
+      (t->rows_piece && t->rows_piece != 8 && t->rows_piece != 16 && t->rows_piece != 32) ||
+      t->load_dedup < 0 || t->load_dedup > 2)
     return fail(e, GDL_E_INVALID, "tuning value out of range");
   e->dedup_mode = t->dedup;
   if (t->dense_max_bits) e->dense_max_bits = t->dense_max_bits;
@@ -3788,6 +3823,7 @@ gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t) {
   if (t->radix_bits) e->radix_bits = t->radix_bits;
   if (t->join_block) e->join_block = t->join_block;
   if (t->rows_piece) e->rows_piece = t->rows_piece;
+  if (t->load_dedup) e->load_dedup = t->load_dedup;
   for (LieHost &L : e->lies) L.graph_dirty = true;
   return GDL_OK;
 }
@@ -3809,6 +3845,7 @@ gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t) {
   t->radix_bits = e->radix_bits;
   t->join_block = e->join_block;
   t->rows_piece = e->rows_piece;
+  t->load_dedup = e->load_dedup;
   return GDL_OK;
 }
 

@@ -222,9 +222,21 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(SortArgs a) {
   (void)words;
   for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (u64)gridDim.x * blockDim.x) {
-    u64 k = a.buf0[i];
+  // four keys in flight per thread: their loads are issued together ahead
+  // of the shared-memory counts
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    u64 k[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) k[j] = a.buf0[i + j * stride];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      for (int p = 0; p < a.passes; p++)
+        atomicAdd(&s_hist[p][sort_vkey_digit<BITS>(k[j], a.kbits, p)], 1u);
+  }
+  for (; i < n; i += stride) {
+    const u64 k = a.buf0[i];
     for (int p = 0; p < a.passes; p++)
       atomicAdd(&s_hist[p][sort_vkey_digit<BITS>(k, a.kbits, p)], 1u);
   }

@@ -63,7 +63,8 @@ class Tuning(C.Structure):
                 ("dense_join_passes", C.c_int32), ("join_aggregate", C.c_int32),
                 ("pull_joins", C.c_int32), ("row_gather", C.c_int32),
                 ("spin_limit_log2", C.c_int32), ("radix_bits", C.c_int32),
-                ("join_block", C.c_int32), ("rows_piece", C.c_int32)]
+                ("join_block", C.c_int32), ("rows_piece", C.c_int32),
+                ("load_dedup", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

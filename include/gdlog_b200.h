@@ -166,6 +166,11 @@ typedef struct gdl_tuning {
                                   bitmaps: 128, 256 (default) or 512 */
   int32_t rows_piece;          /* row-gather joins: in-edges of one output row
                                   per unit of work, 8, 16 or 32 (default) */
+  int32_t load_dedup;          /* load_relation's sort + unique: 1 = radix sort
+                                  and merge; 2 = set the rows' bits in a bitmap
+                                  over the key domain and list it, when the ids
+                                  are below 2^15 and the load has more than
+                                  4096 rows (default; same result) */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);

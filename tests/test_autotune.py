@@ -39,14 +39,16 @@ def test_tuning_values_validated():
             g.set_tuning(index_slots_per_key=3)
         with pytest.raises(GdlError):
             g.set_tuning(dense_max_bits=40)
-        for bad in ({"radix_bits": 7}, {"join_block": 64}, {"rows_piece": 64}):
+        for bad in ({"radix_bits": 7}, {"join_block": 64}, {"rows_piece": 64},
+                    {"load_dedup": 3}):
             with pytest.raises(GdlError):
                 g.set_tuning(**bad)
         g.set_tuning(join_ctas_per_sm=16, dedup="sort", radix_bits=10, join_block=512,
-                     rows_piece=8)
+                     rows_piece=8, load_dedup=1)
         t = g.get_tuning().as_dict()
         assert t["join_ctas_per_sm"] == 16 and t["dedup"] == 1
         assert (t["radix_bits"], t["join_block"], t["rows_piece"]) == (10, 512, 8)
+        assert t["load_dedup"] == 1
 
 
 @pytest.mark.gpu
