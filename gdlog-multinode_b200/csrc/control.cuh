@@ -33,32 +33,62 @@ struct LieDev {
   u64 *trace;                 // [trace rows][n_update][3]
 };
 
+// A lane's entries of the LIE's lists (entries lane and lane + 32; every
+// list holds at most kMaxRels = 64), read once with all their loads in
+// flight together: the control kernels are one warp whose time is its
+// chains of dependent loads.
+constexpr int kListPerLane = kMaxRels / 32;
+static_assert(kMaxOps <= kMaxRels, "ops per lane");
+struct LaneLists {
+  int nu, ns, nt, no;
+  int upd[kListPerLane], sta[kListPerLane], tmp[kListPerLane];
+};
+__device__ __forceinline__ LaneLists lane_lists(const LieDev *L, int lane) {
+  LaneLists x;
+  x.nu = L->n_update;
+  x.ns = L->n_static;
+  x.nt = L->n_tmp;
+  x.no = L->n_ops;
+#pragma unroll
+  for (int j = 0; j < kListPerLane; j++) {
+    // (every slot is inside the arrays; slots past a list's length unused)
+    x.upd[j] = L->update[lane + 32 * j];
+    x.sta[j] = L->statics[lane + 32 * j];
+    x.tmp[j] = L->tmps[lane + 32 * j];
+  }
+  return x;
+}
+
 // Open an iteration: working visibilities from the committed ones, NEWT
 // emptied, this iteration's Copy-once flags cleared.  Run by one warp, lane
-// l taking entries l, l + 32, ... of each list (each relation is in one
+// l taking entries l and l + 32 of each list (each relation is in one
 // list; k_commit gives every entry to the same lane).
-__device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L, int lane) {
-  const int nu = L->n_update, ns = L->n_static, nt = L->n_tmp, no = L->n_ops;
-  for (int i = lane; i < nu; i += 32) {
-    RelDev &r = rels[L->update[i]];
-    r.w_full_vis = r.full_vis;
-    r.w_delta_vis = r.delta_vis;
-    r.newt.n = 0;
-  }
-  for (int i = lane; i < ns; i += 32) {
-    RelDev &r = rels[L->statics[i]];
-    r.w_full_vis = r.full_vis;
-    r.w_delta_vis = r.delta_vis;
-  }
-  for (int i = lane; i < nt; i += 32) {
-    RelDev &r = rels[L->tmps[i]];
-    r.w_full_vis = r.full_vis;
-    r.w_delta_vis = r.delta_vis;
-    r.newt.n = 0;
-  }
-  for (int i = lane; i < no; i += 32) {
-    L->once_pending[i] = 0;
-    L->jonce_pending[i] = 0;
+__device__ __forceinline__ void begin_iteration(RelDev *rels, LieDev *L, const LaneLists &x,
+                                                int lane) {
+#pragma unroll
+  for (int j = 0; j < kListPerLane; j++) {
+    const int i = lane + 32 * j;
+    if (i < x.nu) {
+      RelDev &r = rels[x.upd[j]];
+      r.w_full_vis = r.full_vis;
+      r.w_delta_vis = r.delta_vis;
+      r.newt.n = 0;
+    }
+    if (i < x.ns) {
+      RelDev &r = rels[x.sta[j]];
+      r.w_full_vis = r.full_vis;
+      r.w_delta_vis = r.delta_vis;
+    }
+    if (i < x.nt) {
+      RelDev &r = rels[x.tmp[j]];
+      r.w_full_vis = r.full_vis;
+      r.w_delta_vis = r.delta_vis;
+      r.newt.n = 0;
+    }
+    if (i < x.no) {
+      L->once_pending[i] = 0;
+      L->jonce_pending[i] = 0;
+    }
   }
 }
 
@@ -79,7 +109,7 @@ __global__ void k_begin(RelDev *rels, LieDev *L, Ctl *ctl) {
     }
   }
   if (!__shfl_sync(0xffffffffu, ok, 0)) return;
-  begin_iteration(rels, L, lane);
+  begin_iteration(rels, L, lane_lists(L, lane), lane);
 }
 
 template <class T>
@@ -96,16 +126,23 @@ __device__ __forceinline__ void dswap(T &a, T &b) {
 __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
   const int lane = threadIdx.x;
   if (lane >= 32) return;
+  // the control words and the lists, all loads in flight together
   bool stop = ctl->done | ctl->pause | ctl->overflow | ctl->timeout;
+  const u64 it = ctl->iteration, trace_base = ctl->trace_base;
+  const u64 trace_rows = ctl->trace_rows, max_it = ctl->max_iteration, stop_at = ctl->stop_at;
+  const u32 cond_set = ctl->cond_set;
+  const unsigned long long cond_handle = ctl->cond_handle;
+  const LaneLists x = lane_lists(L, lane);
+  u64 *trace = L->trace;
   if (!stop) {
-    const u64 it = ctl->iteration;
-    const u64 row = it - ctl->trace_base;
-    const u64 trace_rows = ctl->trace_rows, max_it = ctl->max_iteration, stop_at = ctl->stop_at;
-    const int nu = L->n_update;
-    u64 *trace = L->trace;
+    const u64 row = it - trace_base;
+    const int nu = x.nu;
     bool grew = false;
-    for (int i = lane; i < nu; i += 32) {
-      RelDev &r = rels[L->update[i]];
+#pragma unroll
+    for (int j = 0; j < kListPerLane; j++) {
+      const int i = lane + 32 * j;
+      if (i >= nu) continue;
+      RelDev &r = rels[x.upd[j]];
       u64 *tr = (trace && row < trace_rows) ? trace + (row * nu + i) * 3 : 0;
       // (Dense form: the update scan has already merged NEWT into the FULL
       // bitmap in place, dense.cuh.)
@@ -147,18 +184,19 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
       r.newt_phantom = 0;
     }
     const bool fixpoint = !__any_sync(0xffffffffu, grew);
-    for (int i = lane; i < L->n_static; i += 32) {
-      RelDev &r = rels[L->statics[i]];
-      r.full_vis = r.w_full_vis;
-      r.delta_vis = r.w_delta_vis;
-    }
-    for (int i = lane; i < L->n_tmp; i += 32) {
-      RelDev &r = rels[L->tmps[i]];
-      r.newt.n = 0;  // src/lie.cu:85-87
-    }
-    for (int i = lane; i < L->n_ops; i += 32) {
-      L->once[i] |= L->once_pending[i];
-      L->jonce[i] |= L->jonce_pending[i];
+#pragma unroll
+    for (int j = 0; j < kListPerLane; j++) {
+      const int i = lane + 32 * j;
+      if (i < x.ns) {
+        RelDev &r = rels[x.sta[j]];
+        r.full_vis = r.w_full_vis;
+        r.delta_vis = r.w_delta_vis;
+      }
+      if (i < x.nt) rels[x.tmp[j]].newt.n = 0;  // src/lie.cu:85-87
+      if (i < x.no) {
+        L->once[i] |= L->once_pending[i];
+        L->jonce[i] |= L->jonce_pending[i];
+      }
     }
     const u64 next = it + 1;
     const bool done = fixpoint || next > max_it;
@@ -173,11 +211,11 @@ __global__ void k_commit(RelDev *rels, LieDev *L, Ctl *ctl, int begin_next) {
     }
     stop = done || pause;
     __syncwarp();
-    if (begin_next && !stop) begin_iteration(rels, L, lane);
+    if (begin_next && !stop) begin_iteration(rels, L, x, lane);
     __threadfence();
   }
-  if (lane == 0 && ctl->cond_set)
-    cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond_handle, stop ? 0u : 1u);
+  if (lane == 0 && cond_set)
+    cudaGraphSetConditional((cudaGraphConditionalHandle)cond_handle, stop ? 0u : 1u);
 }
 
 // Point the control block at a graph's while-node condition: the loop's

@@ -155,9 +155,8 @@ struct RelHost {
   // A load committed on the device that the host mirror has not read back
   // (its FULL count is known on the device only).
   bool stale = false;
-  u32 *inv_off = nullptr, *inv_cur = nullptr, *inv_keys = nullptr;
-  u32 *inv_poff = nullptr;   // pieces of work per y, then their offsets (2^dk + 1)
-  uint4 *inv_pieces = nullptr;  // {first edge, end edge, y, whole}
+  u32 *inv_off = nullptr, *inv_cur = nullptr;
+  u32 *inv_keys = nullptr, *inv_ys = nullptr;  // per in-edge: source, y
   u64 inv_cap = 0;
   int inv_dk = 0;
 };
@@ -197,8 +196,8 @@ struct gdl_engine {
   int sort_status_passes = 0;
   int sort_status_radix = 0;
   // Tuned shapes (gdl_tuning): radix sort digit width, block size of the
-  // probe-and-expand join (k_join_bm), in-edges per piece of a row-gather
-  // join (k_join_rows_bm).
+  // probe-and-expand join (k_join_bm), in-edges per unit of work of a
+  // row-gather join (k_join_rows_bm).
   int radix_bits = kRadixBits;
   int join_block = 256;
   int rows_piece = 32;
@@ -1280,28 +1279,24 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   const u64 n = e->h[r].full.n;
   const u32 ids = 1u << dk;
   if (rh.inv_dk != dk || rh.inv_cap < std::max<u64>(n, 1)) {
-    for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_poff, &rh.inv_keys}) {
+    for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_keys, &rh.inv_ys}) {
       dfree(e, *q);
       *q = nullptr;
     }
-    dfree(e, rh.inv_pieces);
-    rh.inv_pieces = nullptr;
     rh.inv_cap = std::max<u64>(n, 1);
     rh.inv_dk = dk;
     TRY(dalloc(e, (void **)&rh.inv_off, (ids + 1) * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_cur, ids * sizeof(u32)));
-    TRY(dalloc(e, (void **)&rh.inv_poff, (ids + 1) * sizeof(u32)));
     TRY(dalloc(e, (void **)&rh.inv_keys, rh.inv_cap * sizeof(u32)));
-    // pieces: at most one per in-edge, and one per y
-    TRY(dalloc(e, (void **)&rh.inv_pieces, (rh.inv_cap + ids) * sizeof(uint4)));
+    TRY(dalloc(e, (void **)&rh.inv_ys, rh.inv_cap * sizeof(u32)));
   }
   CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
   const DArr *list = &e->d_rels[r].full;
   k_inv_count<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, dk, e->d_ctl);
-  // edge offsets, fill cursors and the pieces of work, in one block
-  k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, rh.inv_poff,
-                                           rh.inv_pieces, dk, (u32)e->rows_piece);
-  k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, dk);
+  // edge offsets and fill cursors, in one block
+  k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
+  k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
+                                                       dk);
   CK(e, cudaGetLastError());
   return GDL_OK;
 }
@@ -1435,8 +1430,9 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         ra.outer_clear = op.outer_ver == GDL_NEWT ? oh.bmG : nullptr;
         const RelHost &ih = e->rels[op.inner];
         ra.inv_keys = ih.inv_keys;
-        ra.pieces_off = ih.inv_poff;
-        ra.pieces = ih.inv_pieces;
+        ra.inv_ys = ih.inv_ys;
+        ra.inv_off = ih.inv_off;
+        ra.unit = (u32)e->rows_piece;
         const RelDev &out = e->h[op.out];
         ra.dst = plan.out_twin[oi] ? out.bmOT : out.bmG;
         ra.dirty = plan.out_twin[oi] ? nullptr : out.dirty;
@@ -2911,9 +2907,8 @@ static void release_program(gdl_engine *e) {
     dfree(e, r.bmD);
     dfree(e, r.tile_prefix);
     const RelHost &rh = e->rels[i];
-    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_poff, rh.inv_keys})
+    for (u32 *q : {rh.inv_off, rh.inv_cur, rh.inv_keys, rh.inv_ys})
       dfree(e, q);
-    dfree(e, rh.inv_pieces);
     if (!e->rels[i].raw_is_full) dfree(e, e->rels[i].raw);
   }
   for (LieHost &L : e->lies) {

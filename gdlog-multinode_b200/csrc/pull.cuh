@@ -59,14 +59,22 @@ constexpr int kPullAutoBits = 10;  // the pull form by default from 2^10 ids on
 // Lane l holds row l of a 32 x 32 bit block (bit j = column j); afterwards
 // lane j holds column j (bit l = row l).  Each round swaps the off-diagonal
 // quarters of the blocks of side 2s between lane pairs l, l ^ s.
+// A lane keeps the bits of `keep` (m in the lower lane of a pair, ~m in
+// the upper) and takes the others from its partner's word rotated into
+// place: left by s in the lower lane, right by s in the upper.  The bits
+// that wrap around in the rotation fall outside the taken mask (m = ~m >> s
+// and ~m = m << s for these masks), so one funnel shift and one select do
+// a round.
 __device__ __forceinline__ u32 transpose32(u32 x, int lane) {
   const u32 masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
 #pragma unroll
   for (int i = 0; i < 5; i++) {
     const int s = 16 >> i;
-    const u32 m = masks[i];
+    const bool up = (lane & s) != 0;
+    const u32 keep = up ? ~masks[i] : masks[i];
     const u32 y = __shfl_xor_sync(0xffffffffu, x, s);
-    x = (lane & s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
+    const u32 r = __funnelshift_l(y, y, up ? 32 - s : s);
+    x = (x & keep) | (r & ~keep);
   }
   return x;
 }
@@ -499,9 +507,11 @@ __global__ void __launch_bounds__(256) k_inv_count(const DArr *list, u32 *cnt, i
   }
 }
 
-// Scatter: the in-edges of y at [off[y], off[y+1]) (the order inside a y
-// does not matter: the gather ORs).
-__global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, int dk) {
+// Scatter: the in-edges of y at [off[y], off[y+1]), each edge's source in
+// keys and its y in ys (the order inside a y does not matter: the gather
+// ORs).
+__global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u32 *keys, u32 *ys,
+                                                  int dk) {
   const u64 n = list->n;
   const u32 lim = 1u << dk;
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
@@ -510,29 +520,22 @@ __global__ void __launch_bounds__(256) k_inv_fill(const DArr *list, u32 *cur, u3
     if (y >= lim || k >= lim) continue;
     const u32 pos = atomicAdd(&cur[y], 1u);
     keys[pos] = k;
+    ys[pos] = y;
   }
 }
 
-// Units of work of the row-gather join: the in-edges of one y, cut into
-// pieces of at most `piece` (<= 32, a tuning choice; a y with more in-edges
-// than that is shared by several warps, which OR their parts into the
-// output row).  A piece is {first edge, end edge, y, whole}: whole when it
-// holds all of y's in-edges.
 constexpr int kInvBlock = 1024;
 constexpr int kInvPer = 8;  // consecutive ids per thread and chunk
 
 // One block: from the in-degree counts cnt[y] (2^dk of them), the edge
-// offsets off[0..2^dk] (and the fill cursors cur, a copy; cur may be cnt),
-// the piece offsets poff[0..2^dk] and the pieces themselves (the poff
-// array is no longer read by the join: a piece names its y).  Chunks of kInvBlock x kInvPer ids, each thread
-// kInvPer consecutive ones read and written as 16-byte vectors; the two
-// prefix sums (edges low, pieces high) share one 64-bit block scan.
+// offsets off[0..2^dk] and the fill cursors cur (a copy; cur may be cnt).
+// Chunks of kInvBlock x kInvPer ids, each thread kInvPer consecutive ones
+// read and written as 16-byte vectors.
 __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *off, u32 *cur,
-                                                           u32 *poff, uint4 *pieces, int dk,
-                                                           u32 piece) {
+                                                           int dk) {
   __shared__ u64 s_warp[kInvBlock / 32];
   const u32 n = 1u << dk;  // a multiple of kInvPer
-  u64 carry = 0;           // (pieces << 32) | edges of the chunks before
+  u64 carry = 0;           // edges of the chunks before
   for (u32 c0 = 0; c0 < n; c0 += kInvBlock * kInvPer) {
     const u32 b = c0 + kInvPer * threadIdx.x;
     u32 v[kInvPer];
@@ -547,45 +550,35 @@ __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *
     }
     u64 local = 0;
 #pragma unroll
-    for (int i = 0; i < kInvPer; i++)
-      local += ((u64)((v[i] + piece - 1) / piece) << 32) | v[i];
+    for (int i = 0; i < kInvPer; i++) local += v[i];
     u64 tot;
     const u64 ex = block_excl_scan<kInvBlock>(local, s_warp, &tot) + carry;
     carry += tot;
     if (b >= n) continue;
-    u32 e = (u32)ex, p = (u32)(ex >> 32);
-    u32 o[kInvPer], po[kInvPer];
+    u32 e = (u32)ex;
+    u32 o[kInvPer];
 #pragma unroll
     for (int i = 0; i < kInvPer; i++) {
       o[i] = e;
-      po[i] = p;
-      const u32 end = e + v[i];
-      for (u32 s = e; s < end; s += piece)
-        pieces[p++] = make_uint4(s, min(s + piece, end), b + i, v[i] <= piece ? 1u : 0u);
-      e = end;
+      e += v[i];
     }
-    uint4 *po4 = reinterpret_cast<uint4 *>(off + b), *pc4 = reinterpret_cast<uint4 *>(cur + b),
-          *pp4 = reinterpret_cast<uint4 *>(poff + b);
+    uint4 *po4 = reinterpret_cast<uint4 *>(off + b), *pc4 = reinterpret_cast<uint4 *>(cur + b);
     po4[0] = make_uint4(o[0], o[1], o[2], o[3]);
     po4[1] = make_uint4(o[4], o[5], o[6], o[7]);
     pc4[0] = make_uint4(o[0], o[1], o[2], o[3]);
     pc4[1] = make_uint4(o[4], o[5], o[6], o[7]);
-    pp4[0] = make_uint4(po[0], po[1], po[2], po[3]);
-    pp4[1] = make_uint4(po[4], po[5], po[6], po[7]);
   }
-  if (threadIdx.x == 0) {
-    off[n] = (u32)carry;
-    poff[n] = (u32)(carry >> 32);
-  }
+  if (threadIdx.x == 0) off[n] = (u32)carry;
 }
 
 struct RowsArgs {
   JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record
   const u32 *O;        // the outer's rows: DELTA (non-transposed copy) or a tmp NEWT
   u32 *outer_clear;    // bitmap to clear if an empty inner zeroes a NEWT outer
-  const u32 *inv_keys;    // in-edge sources, grouped by y
-  const u32 *pieces_off;  // pieces_off[2^dk]: the number of pieces
-  const uint4 *pieces;    // {first edge, end edge, y, whole}
+  const u32 *inv_keys;  // in-edge sources, grouped by y
+  const u32 *inv_ys;    // the y of each in-edge
+  const u32 *inv_off;   // inv_off[2^dk]: the number of in-edges
+  u32 unit;             // in-edges per unit of work (8, 16 or 32)
   u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
   u8 *dirty;           // dirty map of dst, or null
   int dst_zero;        // dst is all zero when the launch starts
@@ -630,19 +623,6 @@ __device__ __forceinline__ void rows_flush(const RowsArgs &a, u32 y, bool whole,
 }
 
 template <int V>
-__device__ __forceinline__ void rows_or(uint4 *acc, const u32 *O, u32 k, int rs, int lane) {
-  const uint4 *row = reinterpret_cast<const uint4 *>(O + ((u64)k << rs));
-#pragma unroll
-  for (int j = 0; j < V; j++) {
-    const uint4 v = row[j * 32 + lane];
-    acc[j].x |= v.x;
-    acc[j].y |= v.y;
-    acc[j].z |= v.z;
-    acc[j].w |= v.w;
-  }
-}
-
-template <int V>
 __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   if (ctl_stop(a.j.ctl)) return;
   if (eff_count(a.j.inner, a.j.inner_vis) == 0) {
@@ -666,38 +646,73 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   if (a.j.outer_vis && eff_count(a.j.outer, a.j.outer_vis) == 0) return;
   const int lane = threadIdx.x & 31;
   const int rs = a.dk - 5;
-  // the pieces actually built (values outside the domain are skipped by
+  // the in-edges actually listed (values outside the domain are skipped by
   // k_inv_fill and reported by the fixpoint)
-  const u32 n_pieces = a.pieces_off[1u << a.dk];
+  const u32 n_edges = a.inv_off[1u << a.dk];
   u64 words_out = 0, edges = 0;
-  // Pieces are bounded (<= 32 rows), so warps take them round robin; the
-  // next piece's descriptor and keys load while this one's rows are read.
+  // Units are runs of U consecutive in-edges (grouped by y, so a unit holds
+  // the in-edges of a few consecutive y's), taken round robin: every warp
+  // reads the same number of rows, kFly at a time, and flushes its
+  // accumulator where y changes.  A y none of whose in-edges lie just
+  // before or just after the unit has them all here: its row is this
+  // warp's alone.  The next unit's ids load while this unit's rows are read.
+  // U follows from the edge count: each warp takes k units of U <= a.unit
+  // edges (k = ceil(edges per warp / a.unit)), so no warp takes one unit
+  // more than the others (that unit would be the launch's tail).
   const u32 nw = (gridDim.x * blockDim.x) >> 5;
-  u32 c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint4 pc = c < n_pieces ? a.pieces[c] : make_uint4(0, 0, 0, 0);
-  u32 my_k = (c < n_pieces && lane < (int)(pc.y - pc.x)) ? a.inv_keys[pc.x + lane] : 0;
+  const u32 per_warp = (n_edges + nw - 1) / nw;
+  const u32 k_units = max(1u, (per_warp + a.unit - 1) / a.unit);
+  const u32 U = max(1u, (per_warp + k_units - 1) / k_units);
+  const u32 n_units = (n_edges + U - 1) / U;
+  const uint4 none = make_uint4(0, 0, 0, 0);
   constexpr int kFly = V <= 4 ? 4 : 2;
-  while (c < n_pieces) {
-    const u32 cn = c + nw;
-    const uint4 pn = cn < n_pieces ? a.pieces[cn] : make_uint4(0, 0, 0, 0);
+  u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  u32 my_k = 0, my_y = ~0u;
+  if (u < n_units && u * U + lane < n_edges && lane < (int)U) {
+    my_k = a.inv_keys[u * U + lane];
+    my_y = a.inv_ys[u * U + lane];
+  }
+  while (u < n_units) {
+    const u32 base = u * U;
+    const u32 m = min(U, n_edges - base);
+    // the y's of the edges just before and just after this unit
+    u32 edge_y = ~0u;
+    if (lane == 0 && base > 0) edge_y = a.inv_ys[base - 1];
+    if (lane == 1 && base + m < n_edges) edge_y = a.inv_ys[base + m];
+    // the next unit's ids
+    const u32 un = u + nw;
+    u32 nk = 0, ny = ~0u;
+    if (un < n_units && un * U + lane < n_edges && lane < (int)U) {
+      nk = a.inv_keys[un * U + lane];
+      ny = a.inv_ys[un * U + lane];
+    }
+    const u32 y_before = __shfl_sync(0xffffffffu, edge_y, 0);
+    const u32 y_after = __shfl_sync(0xffffffffu, edge_y, 1);
     uint4 acc[V];
 #pragma unroll
-    for (int j = 0; j < V; j++) acc[j] = make_uint4(0, 0, 0, 0);
-    // this piece's keys, one per lane; kFly rows in flight per step (all
-    // their loads issued before the ORs)
-    const u32 m = pc.y - pc.x;
-    u32 i = 0;
-    for (; i + kFly <= m; i += kFly) {
+    for (int j = 0; j < V; j++) acc[j] = none;
+    u32 cur_y = __shfl_sync(0xffffffffu, my_y, 0);
+    for (u32 i = 0; i < m; i += kFly) {
+      // kFly rows in flight: all their loads issued before the ORs (a slot
+      // past the unit's end reads row 0, inside the bitmap, and is unused)
       uint4 b[kFly][V];
 #pragma unroll
       for (int f = 0; f < kFly; f++) {
-        const u32 k = __shfl_sync(0xffffffffu, my_k, i + f);
-        const uint4 *row = reinterpret_cast<const uint4 *>(a.O + ((u64)k << rs));
+        const u32 k = __shfl_sync(0xffffffffu, my_k, (int)((i + f) & 31u));
+        const uint4 *row = reinterpret_cast<const uint4 *>(a.O + ((u64)(i + f < m ? k : 0u) << rs));
 #pragma unroll
         for (int j = 0; j < V; j++) b[f][j] = row[j * 32 + lane];
       }
 #pragma unroll
-      for (int f = 0; f < kFly; f++)
+      for (int f = 0; f < kFly; f++) {
+        const u32 yf = __shfl_sync(0xffffffffu, my_y, (int)((i + f) & 31u));
+        if (i + f >= m) break;
+        if (yf != cur_y) {
+          rows_flush<V>(a, cur_y, cur_y != y_before && cur_y != y_after, acc, words_out);
+#pragma unroll
+          for (int j = 0; j < V; j++) acc[j] = none;
+          cur_y = yf;
+        }
 #pragma unroll
         for (int j = 0; j < V; j++) {
           acc[j].x |= b[f][j].x;
@@ -705,16 +720,13 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
           acc[j].z |= b[f][j].z;
           acc[j].w |= b[f][j].w;
         }
+      }
     }
-    for (; i < m; i++) rows_or<V>(acc, a.O, __shfl_sync(0xffffffffu, my_k, i), rs, lane);
-    // the next piece's keys (its descriptor has arrived)
-    const u32 kn = (cn < n_pieces && lane < (int)(pn.y - pn.x)) ? a.inv_keys[pn.x + lane] : 0;
-    // a y whose in-edges are all in this piece is this warp's alone
-    rows_flush<V>(a, pc.z, pc.w != 0, acc, words_out);
+    rows_flush<V>(a, cur_y, cur_y != y_before && cur_y != y_after, acc, words_out);
     edges += m;
-    c = cn;
-    pc = pn;
-    my_k = kn;
+    u = un;
+    my_k = nk;
+    my_y = ny;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) words_out += __shfl_xor_sync(0xffffffffu, words_out, o);

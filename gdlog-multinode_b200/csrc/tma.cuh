@@ -211,25 +211,34 @@ __global__ void __launch_bounds__(kTrBlock, 2)
     const bool any_n = any8(v);
     if (gt) {
       // the twin's rows are NEWT's columns: transpose (lane j of warp w,
-      // word i: NEWT row 32 i + j, word w)
+      // word i: NEWT row 32 i + j, word w), unless the whole tile is zero
+      // (the barrier also orders the last tile's reads of s_t)
+      if (__syncthreads_or(any_n)) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
-      __syncthreads();
+        for (int i = 0; i < 8; i++) s_t[i * 32 + lane][wid] = transpose32(v[i], lane);
+        __syncthreads();
 #pragma unroll
-      for (int i = 0; i < 8; i++) g[i] = s_t[tid][i];
+        for (int i = 0; i < 8; i++) g[i] = s_t[tid][i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) g[i] = 0;
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < 8; i++) g[i] = v[i];
     }
     lds8(in_f(st) + tid * 8, f);
     const bool any_g = any8(g);
+    u32 nd = 0, ng = 0;  // (at most 256 bits a thread)
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       d[i] = g[i] & ~f[i];
-      n_delta += __popc(d[i]);
-      n_newt += __popc(g[i]);
+      nd += __popc(d[i]);
+      ng += __popc(g[i]);
       f[i] |= g[i];
     }
+    n_delta += nd;
+    n_newt += ng;
     sts8(out_f(slot) + tid * 8, f);
     if (has_dn) sts8(out_dn(slot) + tid * 8, d);
     if (has_dt) {

@@ -27,11 +27,13 @@ same-generation queries grows fast); a batch the engine refuses for size
 (GDL_E_UNSUPPORTED list limit, GDL_E_NOMEM) is split in halves and each half
 run again, down to single queries.
 
-A same-generation query on 2^12 or more nodes is served alone through the
-plain engine instead (`plain_min_nodes`): there its joins run gathered by
-output row (pull form, csrc/pull.cuh), which the block-diagonal batched
-layout does not have, and a large query no longer sets the pace of a batch
-of small ones.
+A query on 2^12 or more nodes is served alone through the plain engine
+instead (`plain_min_nodes`), and so is a batch that holds one query: there
+the joins run gathered by output row or along the inner's in-edges
+(csrc/pull.cuh), which the block-diagonal batched layout does not have, so
+one query runs faster alone than as a batch of one, and a large query no
+longer sets the pace of a batch of small ones.  Batches form when queries
+queue up behind the slots.
 
 The plain baseline serves the same stream one query at a time through the
 plain (unbatched) engine.  Both report p50 / p99 latency (finish - arrival)
@@ -192,7 +194,7 @@ class Server:
 
     def _alone(self, r) -> bool:
         """Served alone through the plain engine (see the module docstring)."""
-        return r.kind == "sg" and self.plain_min_nodes and r.nodes >= self.plain_min_nodes
+        return bool(self.plain_min_nodes) and r.nodes >= self.plain_min_nodes
 
     def _worker(self, t0):
         try:
@@ -231,7 +233,7 @@ class Server:
     def _run(self, eng, prog, reqs) -> list:
         """Results of one batch (or, unbatched, of each query in turn); a
         batch refused for its size is split in halves."""
-        if not self.batched or (len(reqs) == 1 and self._alone(reqs[0])):
+        if not self.batched or len(reqs) == 1:
             return B.run_plain_loop(eng, prog, [r.inputs for r in reqs]).results
         try:
             return B.run_batched(eng, prog, [r.inputs for r in reqs],

@@ -164,8 +164,10 @@ typedef struct gdl_tuning {
                                   falls back to 8 */
   int32_t join_block;          /* threads per block of the one-pass join into
                                   bitmaps: 128, 256 (default) or 512 */
-  int32_t rows_piece;          /* row-gather joins: in-edges of one output row
-                                  per unit of work, 8, 16 or 32 (default) */
+  int32_t rows_piece;          /* row-gather joins: at most this many consecutive
+                                  in-edges (grouped by output row) per unit of
+                                  work, 8, 16 or 32 (default); every warp takes
+                                  the same number of units */
   int32_t load_dedup;          /* load_relation's sort + unique: 1 = radix sort
                                   and merge; 2 = set the rows' bits in a bitmap
                                   over the key domain and list it, when the ids

@@ -3,6 +3,7 @@ GPU are batched with continuous admission; every request's result (size,
 digest of its sorted tuples, loop passes) is the same in the mix as when
 it runs alone through the plain engine."""
 import copy
+import types
 
 import pytest
 
@@ -48,21 +49,45 @@ def test_take_batches_one_kind_within_budget():
     assert len(srv.queue) == len(reqs) - len(first)
 
 
-def test_large_sg_queries_are_taken_alone():
-    """A same-generation query on plain_min_nodes nodes or more is served
+def test_large_queries_are_taken_alone():
+    """A query on plain_min_nodes nodes or more, of either program, is served
     alone (plain engine); no batch holds one with other queries."""
-    reqs = S.make_stream(60, rate=2000.0, seed=4, min_scale=10, max_scale=13, l_range=(3, 9),
-                         w_range=(3, 9))
-    assert any(r.kind == "sg" and r.nodes >= 1 << 12 for r in reqs)
-    srv = S.Server(slots=1, budget_bytes=1 << 40, max_batch=64, plain_min_nodes=1 << 12)
+    reqs = S.make_stream(60, rate=2000.0, seed=4, min_scale=5, max_scale=8, l_range=(3, 16),
+                         w_range=(3, 16))
+    lim = 1 << 7
+    assert any(r.kind == "sg" and r.nodes >= lim for r in reqs)
+    assert any(r.kind == "tc" and r.nodes >= lim for r in reqs)
+    srv = S.Server(slots=1, budget_bytes=1 << 40, max_batch=64, plain_min_nodes=lim)
     srv.queue.extend(reqs)
     sizes = []
     while srv.queue:
         batch = srv._take()
-        big = [r for r in batch if r.kind == "sg" and r.nodes >= 1 << 12]
+        big = [r for r in batch if r.nodes >= lim]
         assert not big or len(batch) == 1
         sizes.append(len(batch))
     assert max(sizes) > 1
+
+
+def test_single_query_batches_run_on_the_plain_engine(monkeypatch):
+    """A batch of one runs through the plain engine (faster than a batch of
+    one in the block-diagonal layout); larger batches run batched."""
+    calls = []
+
+    def plain(eng, prog, instances):
+        calls.append(("plain", len(instances)))
+        return types.SimpleNamespace(results=[None] * len(instances))
+
+    def batched(eng, prog, instances, node_counts=None):
+        calls.append(("batched", len(instances)))
+        return types.SimpleNamespace(results=[None] * len(instances))
+
+    monkeypatch.setattr(B, "run_plain_loop", plain)
+    monkeypatch.setattr(B, "run_batched", batched)
+    reqs = small_stream(6, seed=2)
+    srv = S.Server(slots=1)
+    srv._run(None, S.PROGRAMS["tc"], reqs[:1])
+    srv._run(None, S.PROGRAMS["tc"], reqs[:3])
+    assert calls == [("plain", 1), ("batched", 3)]
 
 
 def test_count_pass_estimate_matches_degrees_on_the_oracle():
