@@ -942,7 +942,12 @@ __global__ void __launch_bounds__(kBmBlock) k_bm_list_write(const u32 *bm, u64 t
       const u64 pos0 = base + sm.seg_off[i];
       u64 *o = dst + pos0;
       moved += 8 * (u64)(threadIdx.x == 0 ? st : 0);
-      if (pos0 + st <= cap) {
+      if (pos0 + st <= cap && rs >= 8) {
+        // rows of 256 words or more: the segment lies in one row, so its
+        // keys are the segment's first key plus their positions
+        const u64 kb = ((ws >> rs) << 32) | ((ws & row_mask) << 5);
+        for (u32 j = threadIdx.x; j < st; j += kBmBlock) o[j] = kb + stg[j];
+      } else if (pos0 + st <= cap) {
         for (u32 j = threadIdx.x; j < st; j += kBmBlock) {
           const u32 q = stg[j];
           const u64 w = ws + (q >> 5);

@@ -159,6 +159,10 @@ struct RelHost {
   u32 *inv_keys = nullptr, *inv_ys = nullptr;  // per in-edge: source, y
   u64 inv_cap = 0;
   int inv_dk = 0;
+  // the in-edge lists hold FULL's current rows (inv_n of them, 2^inv_dk
+  // ids): cleared by a load and when a LIE updates the relation
+  bool inv_ready = false;
+  u64 inv_n = 0;
 };
 
 }  // namespace
@@ -732,6 +736,27 @@ gdl_status ensure_bitmaps(gdl_engine *e, int r, u64 words, bool with_full) {
   return GDL_OK;
 }
 
+// The FULL bitmap of a static relation read as a row-gather join's outer
+// (its FULL does not change during the LIE): that bitmap alone, sized as
+// ensure_bitmaps sizes them.
+gdl_status ensure_static_bitmap(gdl_engine *e, int r, u64 words) {
+  RelHost &rh = e->rels[r];
+  RelDev &h = e->h[r];
+  if (rh.bm_words != words) {
+    for (u32 **p : {&h.bmF, &h.bmG, &h.bmDT, &h.bmGT, &h.bmOT, &h.bmDN}) {
+      dfree(e, *p);
+      *p = nullptr;
+    }
+    dfree(e, h.bmD);
+    h.bmD = nullptr;
+    dfree(e, h.tile_prefix);
+    h.tile_prefix = nullptr;
+    rh.bm_words = words;
+  }
+  if (!h.bmF) TRY(dalloc(e, (void **)&h.bmF, words * 4));
+  return GDL_OK;
+}
+
 gdl_status ensure_dense_scratch(gdl_engine *e, u64 words) {
   // look-back units: tiles / kScanChunk, or in listed mode dirty chunks /
   // kDirtyUnit and chunk groups / kScanChunk (the largest of the three)
@@ -807,6 +832,7 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   RelDev &r = e->h[rel];
   rh.bm_valid = false;
   rh.full_resident = false;
+  rh.inv_ready = false;
   // raw := keys in load order
   if (rh.raw && !rh.raw_is_full) dfree(e, rh.raw);
   rh.raw = nullptr;
@@ -928,6 +954,10 @@ struct Plan {
   // per op: a row-gather join whose output bitmap (a transposed twin) is
   // all zero when it starts (pull.cuh, RowsArgs::dst_zero)
   std::vector<char> twin_zero;
+  // per op: a row-gather join writing an update relation's NEWT directly,
+  // first of the iteration's ops to write that relation (the update step
+  // leaves NEWT zero, so its rows are zero when the join starts)
+  std::vector<char> g_zero;
 };
 
 Plan make_plan(gdl_engine *e, const LieHost &L) {
@@ -953,6 +983,7 @@ Plan make_plan(gdl_engine *e, const LieHost &L) {
   p.tmp_overwritten.assign(n, 0);
   p.static_once.assign(L.ops.size(), 0);
   p.twin_zero.assign(L.ops.size(), 0);
+  p.g_zero.assign(L.ops.size(), 0);
   {
     std::vector<char> is_static(n, 0), is_update(n, 0), newt_read(n, 0);
     for (int r : L.statics) is_static[r] = 1;
@@ -1009,6 +1040,15 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   std::vector<char> is_update(e->rels.size(), 0), is_tmp(e->rels.size(), 0);
   for (int r : L.update) is_update[r] = 1;
   for (int r : L.tmps) is_tmp[r] = 1;
+  std::vector<char> is_static_r(e->rels.size(), 0);
+  for (int r : L.statics) is_static_r[r] = 1;
+  // the row-gather form's size rule (below), for joins that have no other
+  // bitmap form
+  auto rows_fit = [&](const OpHost &op) {
+    if (e->row_gather == 1 || L.dk < kRowsMinBits || op.hook) return false;
+    const u64 bytes = e->h[op.inner].full.n * (4ull << (L.dk - 5));
+    return e->row_gather == 3 || bytes <= kRowsBudget;
+  };
   std::fill(p.newt_list.begin(), p.newt_list.end(), 0);
   std::fill(p.delta_list.begin(), p.delta_list.end(), 0);
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
@@ -1016,11 +1056,18 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     if (op.kind != 0) continue;
     // (outer column 1, inner column 1), or its transpose (inner column 1,
     // outer column 1): gathered into a transposed twin of the output
-    const bool plain = !op.generic && op.pred.kind == 0;
+    // a join of two static FULLs (same generation's first rule,
+    // test/sg.cu:147-151) takes the row-gather form, and with it the
+    // predicate t[0] != t[1] (the output row's diagonal bit)
+    const bool statics = op.outer_ver == GDL_FULL && op.inner_ver == GDL_FULL &&
+                         is_static_r[op.outer] && is_static_r[op.inner] && rows_fit(op);
+    const bool diag = op.pred.kind == GDL_PRED_NE &&
+                      ((op.pred.a == 0 && op.pred.b == 1) || (op.pred.a == 1 && op.pred.b == 0));
+    const bool plain = !op.generic && (op.pred.kind == 0 || (statics && diag));
     const bool fwd = plain && op.sel.s0 == 3 && op.sel.s1 == 1;
     const bool rev = plain && op.sel.s0 == 1 && op.sel.s1 == 3;
     const bool outer_ok = (op.outer_ver == GDL_DELTA && is_update[op.outer]) ||
-                          (op.outer_ver == GDL_NEWT && is_tmp[op.outer]);
+                          (op.outer_ver == GDL_NEWT && is_tmp[op.outer]) || statics;
     if ((fwd || rev) && outer_ok) {
       p.pull[oi] = 1;
       if (rev) p.pull_t[oi] = 1;
@@ -1085,6 +1132,17 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
     for (size_t oi = 0; oi < L.ops.size(); oi++) {
       const int r = L.ops[oi].out;
       p.twin_zero[oi] = p.out_twin[oi] && p.rows[oi] && (!p.fold_late[r] || twin_writers[r] == 1);
+    }
+  }
+  // row-gather joins that write an update relation's NEWT directly and are
+  // the first of the iteration's ops to write it: the update step leaves
+  // NEWT zero, so the join's rows start zero
+  {
+    std::vector<char> written(e->rels.size(), 0);
+    for (size_t oi = 0; oi < L.ops.size(); oi++) {
+      const int r = L.ops[oi].out;
+      if (p.rows[oi] && !p.out_twin[oi] && is_update[r] && !written[r]) p.g_zero[oi] = 1;
+      written[r] = 1;
     }
   }
   // tmp relations whose first op in the iteration writes them through a
@@ -1278,6 +1336,7 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   RelHost &rh = e->rels[r];
   const u64 n = e->h[r].full.n;
   const u32 ids = 1u << dk;
+  if (rh.inv_ready && rh.inv_dk == dk && rh.inv_n == n) return GDL_OK;
   if (rh.inv_dk != dk || rh.inv_cap < std::max<u64>(n, 1)) {
     for (u32 **q : {&rh.inv_off, &rh.inv_cur, &rh.inv_keys, &rh.inv_ys}) {
       dfree(e, *q);
@@ -1297,6 +1356,8 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
   k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
                                                        dk);
+  rh.inv_ready = true;
+  rh.inv_n = n;
   CK(e, cudaGetLastError());
   return GDL_OK;
 }
@@ -1426,8 +1487,15 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         memset(&ra, 0, sizeof ra);
         ra.j = a;
         ra.j.rec = &e->recs[6];
-        ra.O = op.outer_ver == GDL_DELTA ? oh.bmDN : oh.bmG;
+        ra.O = op.outer_ver == GDL_DELTA ? oh.bmDN : op.outer_ver == GDL_FULL ? oh.bmF : oh.bmG;
         ra.outer_clear = op.outer_ver == GDL_NEWT ? oh.bmG : nullptr;
+        ra.clear_diag = op.pred.kind == GDL_PRED_NE;
+        if (plan.static_once[oi]) {
+          ra.j.once = &L.d_lie->jonce[oi];
+          ra.j.once_pending = &L.d_lie->jonce_pending[oi];
+          ra.j.produced = &L.d_lie->produced[oi];
+          ra.j.phantom = &R[op.out].newt_phantom;
+        }
         const RelHost &ih = e->rels[op.inner];
         ra.inv_keys = ih.inv_keys;
         ra.inv_ys = ih.inv_ys;
@@ -1436,7 +1504,7 @@ void enqueue_iteration(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc, 
         const RelDev &out = e->h[op.out];
         ra.dst = plan.out_twin[oi] ? out.bmOT : out.bmG;
         ra.dirty = plan.out_twin[oi] ? nullptr : out.dirty;
-        ra.dst_zero = plan.twin_zero[oi];
+        ra.dst_zero = plan.twin_zero[oi] || plan.g_zero[oi];
         ra.dk = L.dk;
         launch_rows(e, ra, kc);
         if (plan.out_twin[oi] && !plan.fold_late[op.out])
@@ -2177,6 +2245,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     }
     const u64 words = L.map.words;
     for (int r : L.update) {
+      e->rels[r].inv_ready = false;  // (its FULL changes during the LIE)
       TRY(ensure_bitmaps(e, r, words, true));
       RelDev &h = e->h[r];
       h.dense = 1;
@@ -2260,6 +2329,21 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     for (auto *v : {&L.update, &L.tmps})
       for (int r : *v)
         if (plan.out_t[r]) CK(e, cudaMemsetAsync(e->h[r].bmOT, 0, words * 4, e->s));
+    // the FULL bitmaps of the static outers of row-gather joins
+    {
+      std::vector<char> built_o(e->rels.size(), 0);
+      for (size_t oi = 0; oi < L.ops.size(); oi++) {
+        const OpHost &op = L.ops[oi];
+        if (!plan.rows[oi] || op.outer_ver != GDL_FULL || built_o[op.outer]) continue;
+        TRY(ensure_static_bitmap(e, op.outer, words));
+        const RelDev &h = e->h[op.outer];
+        CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
+        if (h.full.n)
+          k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
+              &e->d_rels[op.outer].full, h.bmF, L.map, e->d_ctl);
+        built_o[op.outer] = 1;
+      }
+    }
     // the in-edges of the static inners of row-gather joins
     std::vector<char> built(e->rels.size(), 0);
     for (size_t oi = 0; oi < L.ops.size(); oi++) {

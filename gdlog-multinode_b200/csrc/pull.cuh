@@ -572,8 +572,10 @@ __global__ void __launch_bounds__(kInvBlock) k_inv_offsets(const u32 *cnt, u32 *
 }
 
 struct RowsArgs {
-  JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record
-  const u32 *O;        // the outer's rows: DELTA (non-transposed copy) or a tmp NEWT
+  JoinArgs j;          // outer / inner descriptors (emptiness rules), ctl, launch record,
+                       // the run-once flags of a join over static FULLs
+  const u32 *O;        // the outer's rows: DELTA (non-transposed copy), a tmp NEWT, or a
+                       // static FULL's bitmap
   u32 *outer_clear;    // bitmap to clear if an empty inner zeroes a NEWT outer
   const u32 *inv_keys;  // in-edge sources, grouped by y
   const u32 *inv_ys;    // the y of each in-edge
@@ -582,6 +584,7 @@ struct RowsArgs {
   u32 *dst;            // output rows y (the output's NEWT or its transposed twin)
   u8 *dirty;           // dirty map of dst, or null
   int dst_zero;        // dst is all zero when the launch starts
+  int clear_diag;      // predicate t[0] != t[1]: bit (y, y) dropped from row y
   int dk;
 };
 
@@ -594,6 +597,19 @@ __device__ __forceinline__ void rows_flush(const RowsArgs &a, u32 y, bool whole,
   const int lane = threadIdx.x & 31;
   const int rs = a.dk - 5;
   uint4 *d = reinterpret_cast<uint4 *>(a.dst + ((u64)y << rs));
+  if (a.clear_diag) {
+    // word y / 32 of the row is component (y / 32) % 4 of uint4 y / 128,
+    // held by lane (y / 128) % 32 as its entry (y / 128) / 32
+    const u32 q = y >> 7, c = (y >> 5) & 3u, m = ~(1u << (y & 31));
+#pragma unroll
+    for (int j = 0; j < V; j++)
+      if (q == (u32)(j * 32 + lane)) {
+        if (c == 0) acc[j].x &= m;
+        else if (c == 1) acc[j].y &= m;
+        else if (c == 2) acc[j].z &= m;
+        else acc[j].w &= m;
+      }
+  }
 #pragma unroll
   for (int j = 0; j < V; j++) {
     const uint4 v = acc[j];
@@ -644,6 +660,15 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   }
   // a DELTA outer zeroed earlier in the iteration reads as empty
   if (a.j.outer_vis && eff_count(a.j.outer, a.j.outer_vis) == 0) return;
+  if (a.j.once) {
+    // a join over static FULLs that an earlier iteration ran with both
+    // sides non-empty: the same tuples, all in the output's FULL already
+    if (*a.j.once) {
+      if (blockIdx.x == 0 && threadIdx.x == 0 && *a.j.produced) *a.j.phantom = 1;
+      return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.j.once_pending = 1;
+  }
   const int lane = threadIdx.x & 31;
   const int rs = a.dk - 5;
   // the in-edges actually listed (values outside the domain are skipped by
@@ -658,11 +683,13 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   // warp's alone.  The next unit's ids load while this unit's rows are read.
   // U follows from the edge count: each warp takes k units of U <= a.unit
   // edges (k = ceil(edges per warp / a.unit)), so no warp takes one unit
-  // more than the others (that unit would be the launch's tail).
+  // more than the others (that unit would be the launch's tail).  U stays
+  // at least a.unit / 2: shorter units would cut most y's in-edges apart,
+  // and a y split between units is written with reductions.
   const u32 nw = (gridDim.x * blockDim.x) >> 5;
   const u32 per_warp = (n_edges + nw - 1) / nw;
   const u32 k_units = max(1u, (per_warp + a.unit - 1) / a.unit);
-  const u32 U = max(1u, (per_warp + k_units - 1) / k_units);
+  const u32 U = max(max(1u, a.unit / 2), (per_warp + k_units - 1) / k_units);
   const u32 n_units = (n_edges + U - 1) / U;
   const uint4 none = make_uint4(0, 0, 0, 0);
   constexpr int kFly = V <= 4 ? 4 : 2;
@@ -734,6 +761,7 @@ __global__ void __launch_bounds__(256) k_join_rows_bm(RowsArgs a) {
   // in-edge, and each output word written (read and written back)
   if (lane == 0)
     prof_add(a.j.ctl, kPJoinMat, edges * ((4ull << rs) + 8) + 8 * words_out);
+  if (lane == 0 && words_out && a.j.produced) *a.j.produced = 1;
   launch_rec_finish(a.j.rec);
 }
 

@@ -11,9 +11,10 @@ other batches are on the GPU are admitted as soon as a slot and memory
 free up, and their kernels overlap with the batches in flight (other
 streams).  Relations live on the device from load to result.
 
-Admission uses an HBM estimate per query: the bitmaps of its relations
-(n^2 / 8 bytes each, three per updated relation plus NEWT of the tmp
-relation) plus 16 bytes per candidate of its first join.  The candidates
+Admission uses an HBM estimate per query that can join a batch: the
+bitmaps of its relations (n^2 / 8 bytes each, three per updated relation
+plus NEWT of the tmp relation) plus 16 bytes per candidate of its first
+join.  The candidates
 come from that join's count pass on the device (gdl_join_count: the
 query's relations are loaded into an estimator engine as its program loads
 them, and k_join_count sums, per outer row, the length of the inner run it
@@ -260,7 +261,8 @@ class Server:
                 if delay > 0:
                     time.sleep(delay)
                 r.arrival = r.arrival * time_scale
-                if est is not None:
+                if est is not None and not self._alone(r):
+                    # (a query served alone is admitted whatever its size)
                     r.est_bytes, r.est_tuples = device_estimate(est, r)
                 with self.cv:
                     if self.error is not None:

@@ -144,6 +144,52 @@ def rows_quirks(eng, sync=None):
     return it, a.size(), a.digest(), c.size(), c.digest(), lie.trace().tolist()
 
 
+def static_outer_quirks(eng, sync=None):
+    """Joins of two static FULLs in the row-gather form, over 2^13 ids: the
+    predicate t[0] != t[1] in both column orders (inputs with self-loops, so
+    diagonal candidates exist), output rows written directly and through a
+    transposed twin, run once per fixpoint while a recursive join keeps the
+    loop going, and an empty static inner that zeroes a static outer's
+    count for the rest of the LIE (src/join.cu:38-45)."""
+    rng = np.random.default_rng(13)
+    e = eng.relation("e")
+    f = eng.relation("f")
+    z = eng.relation("z")
+    s = eng.relation("s", index_flag=False)
+    w = eng.relation("w", index_flag=False)
+    ev = rng.integers(0, 5000, size=(3000, 2)).astype(np.uint64)
+    ev[:200, 1] = ev[:200, 0]
+    fv = rng.integers(0, 5000, size=(2500, 2)).astype(np.uint64)
+    fv[:200, 1] = fv[:200, 0]
+    eng.load(e, ev)
+    eng.load(f, fv)
+    eng.load(z, None)
+    eng.load(s, None)
+    eng.load(w, None)
+    lie = eng.lie()
+    lie.add_relations(e, True)
+    lie.add_relations(f, True)
+    lie.add_relations(z, True)
+    lie.add_relations(s, False)
+    lie.add_relations(w, False)
+    lie.add_join(e, FULL, f, FULL, s, (INNER(1), OUTER(1)), pred=(PRED_NE, 0, 1))
+    lie.add_join(f, FULL, e, FULL, w, (OUTER(1), INNER(1)), pred=(PRED_NE, 1, 0))
+    lie.add_join(e, FULL, s, DELTA, s, (OUTER(1), INNER(1)))   # s(b, y) :- s(k, b), e(k, y)
+    lie.add_join(z, FULL, f, FULL, w, (OUTER(1), INNER(1)))    # empty inner: f's count zeroed
+    it = lie.fixpoint()
+    return it, s.size(), s.digest(), w.size(), w.digest(), lie.trace().tolist()
+
+
+def test_static_outer_row_gather_matches_oracle():
+    got = []
+    for mode in ("dense_rows", "dense_pull", "dense_push"):
+        with Engine("gpu", dedup=mode) as g:
+            got.append(static_outer_quirks(g))
+    with Engine("oracle") as o:
+        want = static_outer_quirks(o)
+    assert got[0] == got[1] == got[2] == want
+
+
 def test_row_gather_quirks_match_oracle():
     got = []
     for mode in ("dense_rows", "dense_pull", "dense_push"):
