@@ -850,8 +850,13 @@ gdl_status load_keys(gdl_engine *e, int rel, const u64 *keys_dev, u64 n) {
   TRY(ensure_arr(e, r.full, n, false));
   TRY(ensure_arr(e, r.full_next, n, false));
   const int ldk = std::max(e->kbits, kPullMinBits);
+  // the bitmap's bytes are streamed twice (cleared, then counted): worth it
+  // up to 32 MB, or with at least one row per KB of bitmap (measured: 40,000
+  // rows over 2^14 ids load faster this way; 20,000-60,000 over 2^15 ids,
+  // 128 MB, slower)
+  const u64 bm_bytes = 1ull << (2 * ldk - 3);
   if (n > (u64)kSortTile && e->load_dedup == 2 && !e->wide && rh.arity == 2 &&
-      ldk <= kLoadBitmapMaxBits) {
+      ldk <= kLoadBitmapMaxBits && (bm_bytes <= (32ull << 20) || n >= bm_bytes / 1024)) {
     // Sort + unique through a bitmap over the key domain (2^(2 ldk) bits,
     // at most 128 MB): the rows' bits set, then listed in key order into
     // full_next, which k_load_commit swaps in.  Five streaming launches in

@@ -171,8 +171,9 @@ typedef struct gdl_tuning {
   int32_t load_dedup;          /* load_relation's sort + unique: 1 = radix sort
                                   and merge; 2 = set the rows' bits in a bitmap
                                   over the key domain and list it, when the ids
-                                  are below 2^15 and the load has more than
-                                  4096 rows (default; same result) */
+                                  are below 2^15, the load has more than 4096
+                                  rows, and the bitmap is at most 32 MB or 1 KB
+                                  a row (default; same result) */
 } gdl_tuning;
 gdl_status gdl_engine_set_tuning(gdl_engine *e, const gdl_tuning *t);
 gdl_status gdl_engine_get_tuning(gdl_engine *e, gdl_tuning *t);
