@@ -94,9 +94,16 @@ def measure(eng, prog, inputs, cfg, reps=2) -> float:
 
 
 def measure_runner(eng, run, cfg, reps=2) -> float:
-    """Best of `reps` calls of run(eng) -> device milliseconds under cfg."""
+    """Best of `reps` calls of run(eng) -> device milliseconds under cfg; a
+    configuration the engine refuses for the workload (a status such as the
+    list limit) scores as infinitely slow, and the engine is cleared."""
+    from gdlog_b200 import GdlError
     eng.set_tuning(**cfg)
-    return min(run(eng) for _ in range(reps))
+    try:
+        return min(run(eng) for _ in range(reps))
+    except GdlError:
+        eng.clear()
+        return math.inf
 
 
 def batch_bucket(program: str, instances) -> str:

@@ -103,3 +103,32 @@ def test_every_configuration_gives_the_same_result(tmp_path):
         assert rec["ms"] <= min(rec["default_ms"], rec["ms"]) + 1e-9
         assert json.load(open(tmp_path / "cache.json"))
         assert A.Tuner(str(tmp_path / "cache.json")).lookup("sg", (e,))["config"] == rec["config"]
+
+
+def test_refused_configuration_scores_infinite(tmp_path):
+    """A configuration the engine refuses (a GdlError from the run) loses
+    instead of aborting the tune, and the engine is cleared after it."""
+    from gdlog_b200 import GdlError
+
+    class Fake:
+        def __init__(self):
+            self.cfg, self.cleared = {}, 0
+
+        def set_tuning(self, **kw):
+            self.cfg = kw
+
+        def clear(self):
+            self.cleared += 1
+
+    def run(e):
+        if e.cfg.get("dense_join_passes") == 2:
+            raise GdlError(4, "list limit")
+        return 1.0 + e.cfg.get("join_ctas_per_sm", 0) / 100
+
+    eng = Fake()
+    assert A.measure_runner(eng, run, {"dense_join_passes": 2}) == float("inf")
+    assert eng.cleared == 1
+    t = A.Tuner(cache_path=str(tmp_path / "cache.json"))
+    space = {"dense_join_passes": [2, 1], "join_ctas_per_sm": [8, 4]}
+    rec = t.tune_runner(eng, "k", run, space=space, reps=1, save=False)
+    assert rec["config"]["dense_join_passes"] == 1 and rec["config"]["join_ctas_per_sm"] == 4
