@@ -1028,8 +1028,9 @@ bool fused_update(const Plan &p, int r) { return p.fused[r] != 0; }
 // Pull-form joins (pull.cuh), decided once the LIE's dense form is known: a
 // join into bitmaps over the square domain whose output is (outer column 1,
 // inner column 1), without predicate, over the DELTA of an update relation
-// or the NEWT of a tmp relation.  A NEWT read only by such joins needs no
-// list.
+// or the NEWT of a tmp relation, or (row-gather form only) a join of two
+// static FULLs, which may carry the predicate t[0] != t[1].  A NEWT read
+// only by such joins needs no list.
 // An update relation whose DELTA no op reads as a list and whose FULL is not
 // read as a list either has the fused update step; it keeps DELTA as the
 // bitmaps its readers need (transposed, rows), at least one of them, from
@@ -1091,7 +1092,8 @@ void plan_pull(const gdl_engine *e, const LieHost &L, Plan &p) {
   // a static inner FULL small enough that reading one outer row per in-edge
   // beats expanding candidates: |inner| rows of 2^(dk-5) words within
   // kRowsBudget bytes (any size with row_gather = 3).  A DELTA outer must be
-  // a relation whose update step is the fused pass (it writes DELTA's rows).
+  // a relation whose update step is the fused pass (it writes DELTA's rows);
+  // a static FULL outer is set as a bitmap at LIE start.
   std::vector<char> is_static(e->rels.size(), 0);
   for (int r : L.statics) is_static[r] = 1;
   for (size_t oi = 0; oi < L.ops.size(); oi++) {
@@ -1260,7 +1262,7 @@ void enqueue_update_step(gdl_engine *e, LieHost &L, const Plan &plan, Counts *kc
 // host opens with a k_begin before each launch and whose k_commit opens
 // the next iteration; otherwise the iteration opens itself.
 void launch_rows(gdl_engine *e, const RowsArgs &ra, Counts *kc) {
-  // one resident wave (warps take the pieces round robin): 4 blocks an SM
+  // one resident wave (warps take the units round robin): 4 blocks an SM
   // at 2^12 ids, 2 at 2^13..2^15 (the row accumulators hold 2^(dk-5)
   // words a warp), 1 from 2^16
   const int g = (int)e->sms * (ra.dk >= 16 ? 1 : ra.dk >= 13 ? 2 : 4);

@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(kPullBlock, 8) k_join_pull_bm(JoinArgs a, u32 
 // whatever the number of candidate tuples (which the pull form expands one
 // shared-memory atomic each: 4-8x more work on same generation's dense
 // iterations).  It fits a small inner kept static through the LIE (an edge
-// relation): its in-edges are listed once per LIE (k_inv_*).  The output is
+// relation): its in-edges are listed once (k_inv_*) and kept until the
+// relation is loaded again or a LIE updates it.  The output is
 // the transpose of the pull form's, so the two forms swap the roles of the
 // output's NEWT and its transposed twin.
 // ---------------------------------------------------------------------------
