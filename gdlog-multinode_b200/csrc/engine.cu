@@ -205,6 +205,9 @@ struct gdl_engine {
   int radix_bits = kRadixBits;
   int join_block = 256;
   int rows_piece = 32;
+  // launches of this engine's kernels outside the loop's counted ones (LIE
+  // setup, listings): a fixpoint adds those in its span to its kernel count
+  u64 aux_launches = 0;
   int load_dedup = 2;  // loads: 1 radix sort + merge, 2 bitmap listing where it fits
   u64 *crow_off = nullptr, *crow_key = nullptr;
   u32 *crow_start = nullptr, *crow_len = nullptr;
@@ -1284,6 +1287,7 @@ gdl_status launch_list(gdl_engine *e, const u32 *bm, u64 words, int rs, DArr *ou
   TRY(ensure_lb(e, e->lb_list, e->lb_list_tiles, tiles + 2));
   k_bm_list_count<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(bm, tiles, e->lb_list.flag,
                                                                    e->d_ctl);
+  e->aux_launches += 3;  // (count, offsets, write)
   k_bm_list_offsets<<<1, kListScanBlock, 0, e->s>>>(e->lb_list.flag, tiles, e->lb_list.agg, out,
                                                     check_n, e->d_ctl);
   k_bm_list_write<<<grid_for(e, tiles, 1, 8), kBmBlock, 0, e->s>>>(
@@ -1359,6 +1363,7 @@ gdl_status build_inverse(gdl_engine *e, int r, int dk) {
   CK(e, cudaMemsetAsync(rh.inv_cur, 0, ids * sizeof(u32), e->s));
   const DArr *list = &e->d_rels[r].full;
   k_inv_count<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, dk, e->d_ctl);
+  e->aux_launches += 3;  // (count, offsets, fill)
   // edge offsets and fill cursors, in one block
   k_inv_offsets<<<1, kInvBlock, 0, e->s>>>(rh.inv_cur, rh.inv_off, rh.inv_cur, dk);
   k_inv_fill<<<grid_for(e, n, 256, 8), 256, 0, e->s>>>(list, rh.inv_cur, rh.inv_keys, rh.inv_ys,
@@ -2162,6 +2167,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   // The timed span is the whole call, as the reference's drivers time the
   // whole fixpoint_loop (test/tc.cu:120-140): setup, loop and finish.
   CK(e, cudaEventRecord(e->ev0, e->s));
+  const u64 aux0 = e->aux_launches;
   const auto t_setup = std::chrono::steady_clock::now();
   // GDLOG_TRACE_SETUP=1: host time of each setup phase on stderr
   static const bool trace_setup = getenv("GDLOG_TRACE_SETUP") != nullptr;
@@ -2310,22 +2316,28 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
       CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(h.bmG, 0, words * 4, e->s));
       CK(e, cudaMemsetAsync(h.bmD, 0, words / kBmChunkWords, e->s));
-      if (h.full.n)
+      if (h.full.n) {
         k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
             &e->d_rels[r].full, h.bmF, L.map, e->d_ctl);
+        e->aux_launches++;
+      }
       if (plan.delta_t[r]) {
         // the first DELTA, transposed, for the pull-form joins that read it
         CK(e, cudaMemsetAsync(h.bmDT, 0, words * 4, e->s));
-        if (h.delta.n)
+        if (h.delta.n) {
           k_bm_from_list_t<<<grid_for(e, h.delta.n, 256, 8), 256, 0, e->s>>>(
               &e->d_rels[r].delta, h.bmDT, L.dk, e->d_ctl);
+          e->aux_launches++;
+        }
       }
       if (plan.delta_n[r]) {
         // ... and as rows, for the row-gather joins
         CK(e, cudaMemsetAsync(h.bmDN, 0, words * 4, e->s));
-        if (h.delta.n)
+        if (h.delta.n) {
           k_bm_from_list<<<grid_for(e, h.delta.n, 256, 8), 256, 0, e->s>>>(
               &e->d_rels[r].delta, h.bmDN, L.map, e->d_ctl);
+          e->aux_launches++;
+        }
       }
       e->rels[r].bm_valid = true;
     }
@@ -2345,9 +2357,11 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
         TRY(ensure_static_bitmap(e, op.outer, words));
         const RelDev &h = e->h[op.outer];
         CK(e, cudaMemsetAsync(h.bmF, 0, words * 4, e->s));
-        if (h.full.n)
+        if (h.full.n) {
           k_bm_from_list<<<grid_for(e, h.full.n, 256, 8), 256, 0, e->s>>>(
               &e->d_rels[op.outer].full, h.bmF, L.map, e->d_ctl);
+          e->aux_launches++;
+        }
         built_o[op.outer] = 1;
       }
     }
@@ -2412,6 +2426,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
                           e->s>>>(dv ? &e->d_rels[r].delta : &e->d_rels[r].full,
                                   dv ? &e->d_rels[r].delta_idx : &e->d_rels[r].full_idx, nullptr,
                                   e->d_ctl);
+          e->aux_launches++;
         }
       CK(e, cudaGetLastError());
     }
@@ -2486,6 +2501,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
     }
     if (!spec_list) return GDL_OK;
     k_ctl_resume<<<1, 32, 0, e->s>>>(e->d_ctl);
+    e->aux_launches++;
     for (int r : L.update)
       if (e->h[r].full_lazy)
         TRY(launch_list(e, e->h[r].bmF, L.map.words, L.dk - 5, &e->d_rels[r].full, 1));
@@ -2794,6 +2810,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
           TransposeArgs t = transpose_args(h.bmDT, nullptr, h.bmG, L.dk, nullptr, nullptr,
                                            &e->recs[7], e->d_ctl);
           k_bm_transpose<<<grid_for(e, side * side, 1, 8), kTrBlock, 0, e->s>>>(t);
+          e->aux_launches++;
           rows = h.bmG;
         }
         TRY(launch_list(e, rows, L.map.words, L.dk - 5, &e->d_rels[r].delta, 1));
@@ -2826,6 +2843,7 @@ gdl_status fixpoint(gdl_engine *e, LieHost &L, uint64_t *out_iters) {
   CK(e, cudaEventElapsedTime(&ms, e->ev0, e->ev1));
   L.ms = ms;
   L.iterations = c.iteration;
+  L.kernels += e->aux_launches - aux0;  // (setup and listings, between ev0 and ev1)
   e->kernels_launched += L.kernels;
   for (int k = 0; k < kPKinds; k++) e->prof_bytes[k] += c.prof[k];
   // Finish (src/lie.cu:217-260).
